@@ -1,0 +1,254 @@
+/*
+ * pmgpu -- B200 (sm_100a) implementation of ProtoMol's nonbonded hot path
+ * behind a plain C ABI: cutoff Lennard-Jones + Coulomb over a device-built
+ * cell list with ProtoMol's switching functions, Ewald real space + PME
+ * reciprocal space + exclusion/self corrections, OBC generalized Born, the
+ * harmonic bonds/angles needed to integrate flexible water, and
+ * device-resident leapfrog / Langevin-leapfrog integration.
+ *
+ * Every entry point returns a status code (PMGPU_OK == 0); the message of
+ * the last failure on the calling thread is available from
+ * pmgpu_last_error().  No entry point takes or returns a torch or CUDA
+ * runtime type: host arrays are plain pointers with explicit sizes, in
+ * ProtoMol's own layouts (Vector3DBlock = double[3N] x,y,z per atom;
+ * ScalarStructure energies indexed as in type/ScalarStructure.h:26-67).
+ *
+ * Reference interfaces each entry point replaces (paths inside ProtoMol):
+ *   SystemForce::evaluate(topo, positions, forces, energies)
+ *       force/system/SystemForce.h:32-35           -> pmgpu_force_evaluate
+ *   ForceFactory::make(<force line>) for NonbondedCutoff / FullEwald /
+ *       NonbondedSimpleFull GB* forces
+ *       factory/ForceFactory.cpp:21-242            -> pmgpu_force_*_add
+ *   Integrator::run(n) of Leapfrog / LangevinLeapfrog
+ *       integrator/leapfrog/LeapfrogIntegrator.cpp:89-104,
+ *       integrator/StandardIntegrator.cpp:27-37    -> pmgpu_run
+ *   GenericTopology (atoms, LJ table, exclusions, boundary conditions)
+ *       topology/GenericTopology.h:120-165         -> pmgpu_topology
+ */
+#ifndef PMGPU_H
+#define PMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMGPU_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------- */
+enum {
+  PMGPU_OK = 0,
+  PMGPU_ERR_ARG = 1,          /* invalid argument / configuration */
+  PMGPU_ERR_CUDA = 2,         /* CUDA runtime or cuFFT failure */
+  PMGPU_ERR_OOM = 3,          /* device allocation failed */
+  PMGPU_ERR_OVERFLOW = 4,     /* a device capacity (cell, list) overflowed */
+  PMGPU_ERR_NAN = 5,          /* non-finite force or energy detected */
+  PMGPU_ERR_UNSUPPORTED = 6,  /* configuration outside what is built */
+  PMGPU_ERR_STATE = 7         /* call made in the wrong state */
+};
+
+/* ---- ProtoMol enumerations ---------------------------------------- */
+/* ExclusionClass, topology/ExclusionTable.h:19-23 */
+enum { PMGPU_EXCL_NONE = 0, PMGPU_EXCL_MODIFIED = 1, PMGPU_EXCL_FULL = 2 };
+
+/* Switching functions, switch/{Universal,Cutoff,C1,C2,Cn}SwitchingFunction */
+enum {
+  PMGPU_SW_UNIVERSAL = 0,
+  PMGPU_SW_CUTOFF = 1,
+  PMGPU_SW_C1 = 2,
+  PMGPU_SW_C2 = 3,
+  PMGPU_SW_CN = 4
+};
+
+/* Energy slots written by pmgpu_evaluate / pmgpu_force_evaluate: the first
+ * PMGPU_E_COUNT entries of ProtoMol's ScalarStructure (COULOMB,
+ * LENNARDJONES, BOND, ANGLE, DIHEDRAL, IMPROPER, OTHER). */
+enum {
+  PMGPU_E_COULOMB = 0,
+  PMGPU_E_LENNARDJONES = 1,
+  PMGPU_E_BOND = 2,
+  PMGPU_E_ANGLE = 3,
+  PMGPU_E_DIHEDRAL = 4,
+  PMGPU_E_IMPROPER = 5,
+  PMGPU_E_OTHER = 6,
+  PMGPU_E_COUNT = 7
+};
+
+/* Arithmetic of the pair kernels. */
+enum { PMGPU_PREC_MIXED = 0, /* FP32 pair math, FP64 accumulation/updates */
+       PMGPU_PREC_DOUBLE = 1 /* FP64 throughout */ };
+
+/* ---- topology ------------------------------------------------------ */
+typedef struct {
+  int n_atoms;
+  const double *charge;     /* n: Atom::scaledCharge (q * 18.2226123264) */
+  const double *mass;       /* n: Atom::scaledMass */
+  const int *type;          /* n: Atom::type */
+  const int *molecule;      /* n: Atom::molecule */
+  int n_types;
+  const double *lj;         /* n_types^2 * 4: A, B, A14, B14 per type pair
+                               (LennardJonesParameterTable) */
+  int n_exclusions;
+  const int *exclusions;    /* 3 per entry of ExclusionTable::getTable():
+                               a1, a2, and the class ExclusionTable::check
+                               returns for the pair (used by pair forces) */
+  const int *exclusion_table_class; /* n_exclusions or NULL: the class the
+                               table entry itself holds, used by the Ewald
+                               correction term (NULL: same as above).  The
+                               two differ when a pair was added twice with
+                               different classes (ExclusionTable.cpp:103-118) */
+  double coulomb_scaling;   /* GenericTopology::coulombScalingFactor */
+  int periodic;             /* 1: PeriodicBoundaryConditions, 0: vacuum */
+  double box[12];           /* e1, e2, e3, origin (orthogonal boxes) */
+  /* Harmonic bonds (force/bonded/BondSystemForce.h): i, j and (k, r0). */
+  int n_bonds;
+  const int *bond_atoms;    /* 2 per bond */
+  const double *bond_params;/* 2 per bond: k [kcal/mol/A^2], r0 [A] */
+  /* Harmonic angles (force/bonded/AngleSystemForce.h): i, j(center), k
+   * and (k_theta, theta0 [rad], k_ub, r_ub). */
+  int n_angles;
+  const int *angle_atoms;   /* 3 per angle */
+  const double *angle_params;/* 4 per angle */
+  /* OBC GB atom parameters (GBSAAtomParameters, topology/Atom.h:35-157);
+   * may be NULL when no GB force is added. */
+  const double *gb_vdwr;    /* vanDerWaalRadius */
+  const double *gb_scale;   /* scalingFactor */
+  const double *gb_offset;  /* offsetRadius */
+  const int *water;         /* 1 if the atom's molecule is a water */
+  double gb_obc[3];         /* alphaObc, betaObc, gammaObc */
+} pmgpu_topology;
+
+typedef struct {
+  int kind;         /* PMGPU_SW_* */
+  double cutoff;    /* -cutoff */
+  double switchon;  /* -switchon (C2, Cn) */
+  double switchoff; /* -switchoff (Cn; 0 means "use cutoff") */
+  double order;     /* -n (Cn) */
+} pmgpu_switch;
+
+typedef struct pmgpu_context pmgpu_context;
+typedef struct pmgpu_system pmgpu_system;
+
+/* ---- context ------------------------------------------------------- */
+int pmgpu_context_create(int device, pmgpu_context **out);
+int pmgpu_context_destroy(pmgpu_context *ctx);
+/* Message of the last failing call on this thread ("" if none). */
+const char *pmgpu_last_error(void);
+int pmgpu_abi_version(void);
+
+/* ---- systems ------------------------------------------------------- */
+/* Copies the topology to the device; positions/velocities start at zero. */
+int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *topo,
+                        int precision, pmgpu_system **out);
+int pmgpu_system_destroy(pmgpu_system *sys);
+/* Host <-> device copies of Vector3DBlock-layout arrays (3n doubles). */
+int pmgpu_system_set_positions(pmgpu_system *sys, const double *pos);
+int pmgpu_system_get_positions(pmgpu_system *sys, double *pos);
+int pmgpu_system_set_velocities(pmgpu_system *sys, const double *vel);
+int pmgpu_system_get_velocities(pmgpu_system *sys, double *vel);
+/* Total force of the last evaluation (all enabled terms), 3n doubles. */
+int pmgpu_system_get_forces(pmgpu_system *sys, double *forces);
+/* Energies (PMGPU_E_COUNT) and atomic virial (9, may be NULL) of the last
+ * evaluation. */
+int pmgpu_system_get_energies(pmgpu_system *sys, double *energies,
+                              double *virial);
+/* The CUDA stream (a cudaStream_t) every kernel of this system runs on. */
+void *pmgpu_system_stream(pmgpu_system *sys);
+/* Device pointers of the resident state: positions and velocities as
+ * double[3n] (Vector3DBlock layout), forces as int64 fixed point
+ * [3][n] (x plane, y plane, z plane) with PMGPU_FORCE_SCALE units. */
+int pmgpu_system_device_state(pmgpu_system *sys, double **pos, double **vel,
+                              long long **force_fixed);
+#define PMGPU_FORCE_SCALE 4294967296.0 /* 2^32 per kcal/mol/A */
+
+/* ---- forces (one per ProtoMol `force` line) ------------------------- */
+/* NonbondedCutoff with LennardJones and/or Coulomb
+ * (module/NonbondedCutoffForceModule.cpp:40-201).  lj_sw / coul_sw may be
+ * NULL for an absent term.  cellsize is the topology's cellsize keyword;
+ * alg_cutoff is the algorithm's -cutoff. */
+int pmgpu_force_cutoff_add(pmgpu_system *sys, const pmgpu_switch *lj_sw,
+                           const pmgpu_switch *coul_sw, double alg_cutoff,
+                           double cellsize, int *force_id);
+/* NonbondedSimpleFull LennardJones and/or Coulomb (vacuum all pairs with
+ * exclusions, module/NonbondedSimpleFullForceModule.cpp). */
+int pmgpu_force_simplefull_add(pmgpu_system *sys, int lj, int coulomb,
+                               int *force_id);
+/* Ewald Coulomb delivered as PME: real space (erfc-screened, cutoff rc),
+ * reciprocal space (smooth PME, B-spline order, grid), exclusion
+ * correction and self/charged-system terms, selected by flags.  The real
+ * term follows NonbondedFullEwaldSystemForce::realTerm (:753-858) with the
+ * A&S erfc (exact_erf = 0) or the C library erfc (exact_erf = 1). */
+enum { PMGPU_EWALD_REAL = 1, PMGPU_EWALD_RECIPROCAL = 2,
+       PMGPU_EWALD_CORRECTION = 4, PMGPU_EWALD_ALL = 7 };
+int pmgpu_force_pme_add(pmgpu_system *sys, double alpha, double rc,
+                        int order, const int grid[3], int flags,
+                        int exact_erf, double cellsize, int *force_id);
+/* GBBornRadii + GBPartialSum + GBForce (OBC, vacuum, all pairs),
+ * force/GB/GB{BornRadii,PartialSum,Force}.cpp. */
+int pmgpu_force_gb_add(pmgpu_system *sys, double solute_dielec,
+                       double solvent_dielec, int *force_id);
+/* Harmonic bonds and angles of the topology. */
+int pmgpu_force_bonded_add(pmgpu_system *sys, int bonds, int angles,
+                           int *force_id);
+int pmgpu_force_set_enabled(pmgpu_system *sys, int force_id, int enabled);
+
+/* Evaluate all enabled forces at the resident positions.  energies (may be
+ * NULL) gets PMGPU_E_COUNT values, virial (may be NULL) 9. */
+int pmgpu_evaluate(pmgpu_system *sys, double *energies, double *virial);
+
+/* ProtoMol SystemForce::evaluate semantics for one force term: uploads
+ * positions (3n doubles), evaluates that term only, ADDS its forces into
+ * forces (3n doubles) and its energies into energies (ScalarStructure
+ * slots, PMGPU_E_COUNT) and, if virial != NULL, its virial (9). */
+int pmgpu_force_evaluate(pmgpu_system *sys, int force_id, const double *pos,
+                         double *forces, double *energies, double *virial);
+
+/* ---- integration ---------------------------------------------------- */
+enum { PMGPU_INT_LEAPFROG = 0, PMGPU_INT_LANGEVIN_LEAPFROG = 1 };
+typedef struct {
+  int kind;              /* PMGPU_INT_* */
+  double timestep_fs;    /* -timestep */
+  double temperature;    /* LangevinLeapfrog temperature [K] */
+  double gamma_ps;       /* LangevinLeapfrog gamma [1/ps] */
+  uint64_t seed;         /* counter-based RNG key */
+} pmgpu_integrator;
+
+/* Integrator::run(n): n steps on the device, state stays resident.
+ * Leapfrog follows LeapfrogIntegrator::run (half kick, drift, forces,
+ * (kick, drift, forces)*, half kick); LangevinLeapfrog follows
+ * StandardIntegrator::run with LangevinLeapfrogIntegrator::doHalfKick.
+ * The first call (and any call after positions are set from the host)
+ * evaluates the initial forces first, as Integrator::initialize does. */
+int pmgpu_run(pmgpu_system *sys, const pmgpu_integrator *integ, long n_steps);
+
+/* ---- diagnostics ---------------------------------------------------- */
+typedef struct {
+  long long pairs_in_cutoff;   /* pairs that passed the cutoff test */
+  long long list_entries;      /* (i-cluster, j) entries in the pair list */
+  long long clusters;          /* 8-atom i-clusters */
+  long long list_builds;       /* pair-list builds so far */
+  int cells[3];                /* sort-grid dims of the cutoff path */
+} pmgpu_stats;
+/* Counts from the last evaluation of force_id (pairs_in_cutoff requires
+ * the force to have been evaluated with counting on; see
+ * pmgpu_set_count_pairs). */
+int pmgpu_force_stats(pmgpu_system *sys, int force_id, pmgpu_stats *out);
+int pmgpu_set_count_pairs(pmgpu_system *sys, int enabled);
+
+/* ProtoMol cell assignment (topology/Topology.h:44-86 with
+ * CubicCellManager, cellsize given) computed by the device binning kernel
+ * on the resident positions: cell_xyz gets 3n ints, dims 3 ints. */
+int pmgpu_debug_cell_assign(pmgpu_system *sys, double cellsize,
+                            int *cell_xyz, int *dims);
+/* The unordered pair set (i < j, original indices) the cutoff force
+ * force_id evaluated on its last evaluation: pairs gets 2 ints per pair,
+ * up to cap pairs; *count gets the total. */
+int pmgpu_debug_pair_set(pmgpu_system *sys, int force_id, int *pairs,
+                         long long cap, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMGPU_H */

@@ -1,0 +1,849 @@
+// The C ABI of libpmgpu (include/pmgpu.h): contexts, systems, forces,
+// evaluation and device-resident integration.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pm_device.cuh"
+
+namespace pmgpu {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+// PeriodicBoundaryConditions::set (PeriodicBoundaryConditions.cpp:32-78),
+// orthogonal boxes; the same FP64 expressions so min/max/H/D round alike.
+void box_from_topology(const pmgpu_topology *t, Box *b) {
+  std::memset(b, 0, sizeof(*b));
+  b->periodic = t->periodic;
+  if (!t->periodic) return;
+  const double *e1 = t->box, *e2 = t->box + 3, *e3 = t->box + 6, *o = t->box + 9;
+  auto cross = [](const double *a, const double *c, double *r) {
+    r[0] = a[1] * c[2] - a[2] * c[1];
+    r[1] = a[2] * c[0] - a[0] * c[2];
+    r[2] = a[0] * c[1] - a[1] * c[0];
+  };
+  auto dot = [](const double *a, const double *c) {
+    return a[0] * c[0] + a[1] * c[1] + a[2] * c[2];
+  };
+  double a1[3], a2[3], a3[3], tt[3];
+  cross(e1, e2, tt);
+  b->V = std::fabs(dot(tt, e3));
+  cross(e2, e3, a1);
+  cross(e3, e1, a2);
+  cross(e1, e2, a3);
+  double d1 = dot(e1, a1), d2 = dot(e2, a2), d3 = dot(e3, a3);
+  b->er[0] = a1[0] / d1;
+  b->er[1] = a2[1] / d2;
+  b->er[2] = a3[2] / d3;
+  b->e[0] = e1[0];
+  b->e[1] = e2[1];
+  b->e[2] = e3[2];
+  for (int c = 0; c < 3; c++) {
+    double sum = (e1[c] + e2[c]) + e3[c];
+    double lo = o[c] - sum * 0.5, hi = o[c] + sum * 0.5;
+    b->min[c] = std::min(lo, hi);
+    b->max[c] = std::max(lo, hi);
+    b->origin[c] = o[c];
+  }
+  double dx = (e1[0] * 0.5) * (e1[0] * 0.5);
+  double dy = (e2[1] * 0.5) * (e2[1] * 0.5);
+  double dz = (e3[2] * 0.5) * (e3[2] * 0.5);
+  b->D = std::min(dx, std::min(dy, dz));
+  for (int c = 0; c < 3; c++) {
+    b->H[c] = b->max[c] - b->min[c];
+    b->H2[c] = b->H[c] * 0.5;
+  }
+}
+
+// Switching-function constants exactly as the ProtoMol constructors form
+// them (C1SwitchingFunction.cpp:12-17, C2SwitchingFunction.cpp:12-19,
+// CnSwitchingFunction.cpp:41-60).
+void switch_setup(const pmgpu_switch *in, SwitchParams *o) {
+  std::memset(o, 0, sizeof(*o));
+  o->kind = in->kind;
+  double rc = in->cutoff, rs = in->switchon;
+  switch (in->kind) {
+    case PMGPU_SW_UNIVERSAL:
+      o->cutoff = 1e300;
+      o->cutoff2 = 1e300;
+      break;
+    case PMGPU_SW_CUTOFF:
+      o->cutoff = rc;
+      o->cutoff2 = rc * rc;
+      break;
+    case PMGPU_SW_C1:
+      o->modify = 1;
+      o->cutoff = rc;
+      o->cutoff2 = rc * rc;
+      o->c1a = 1.5 / rc;
+      o->c1b = 0.5 / (rc * rc * rc);
+      o->c1c = 1.5 / (rc * rc * rc);
+      break;
+    case PMGPU_SW_C2: {
+      o->modify = 1;
+      double d = rc * rc - rs * rs;
+      o->cutoff = rc;
+      o->cutoff2 = rc * rc;
+      o->switchon2 = rs * rs;
+      o->s1 = 1.0 / (d * d * d);
+      o->s2 = rc * rc - 3.0 * rs * rs;
+      o->s3 = 4.0 / (d * d * d);
+      break;
+    }
+    case PMGPU_SW_CN: {
+      o->modify = 1;
+      double mycut = in->switchoff != 0.0 ? in->switchoff : rc;
+      o->cutoff = mycut;
+      o->cutoff2 = mycut * mycut;
+      o->switchon2 = rs * rs;
+      o->ord_int = (int)in->order;
+      o->ord_idx = o->ord_int - 2;
+      if (o->ord_int == 5) o->ord_int = 2;
+      o->irange[0] = std::pow(rs - rc, -(o->ord_int + 1));
+      for (int i = 1; i < o->ord_int + 1 && i < 8; i++)
+        o->irange[i] = o->irange[i - 1] / (rs - rc);
+      break;
+    }
+  }
+}
+
+static int validate_switch(const pmgpu_switch *sw, const char *what) {
+  if (!sw) return PMGPU_OK;
+  std::string w(what);
+  switch (sw->kind) {
+    case PMGPU_SW_CUTOFF:
+    case PMGPU_SW_C1:
+      if (!(sw->cutoff > 0)) return fail(PMGPU_ERR_ARG, w + ": cutoff must be > 0");
+      return PMGPU_OK;
+    case PMGPU_SW_C2:
+      // C2SwitchingFunction::make (C2SwitchingFunction.cpp:33-44)
+      if (!(sw->switchon >= 0 && sw->cutoff > 0 && sw->switchon < sw->cutoff))
+        return fail(PMGPU_ERR_ARG, w + ": C2 needs 0 <= switchon < cutoff");
+      return PMGPU_OK;
+    case PMGPU_SW_CN:
+      // CnSwitchingFunction::make (CnSwitchingFunction.cpp:83-110)
+      if (!(sw->switchon >= 0 && sw->cutoff > 0 && sw->switchon < sw->cutoff) ||
+          (sw->switchoff > 0 && sw->switchoff != sw->cutoff) || sw->order < 2 ||
+          sw->order > 6)
+        return fail(PMGPU_ERR_ARG, w + ": Cn needs 0 <= switchon < cutoff, order 2..6");
+      return PMGPU_OK;
+    case PMGPU_SW_UNIVERSAL:
+      return fail(PMGPU_ERR_ARG, w + ": a cutoff force needs a cutoff switching function");
+    default:
+      return fail(PMGPU_ERR_ARG, w + ": unknown switching function");
+  }
+}
+
+template <typename T>
+static int upload(T **d, const T *h, size_t count) {
+  if (count == 0) count = 1;
+  PM_CUDA(cudaMalloc(d, sizeof(T) * count));
+  if (h) PM_CUDA(cudaMemcpy(*d, h, sizeof(T) * count, cudaMemcpyHostToDevice));
+  else PM_CUDA(cudaMemset(*d, 0, sizeof(T) * count));
+  return PMGPU_OK;
+}
+
+static int system_free(System *s) {
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto &f : s->forces) pme_free(&f);
+  for (auto &nl : s->lists) nb_list_free(&nl);
+  void *ptrs[] = {s->d_charge, s->d_mass, s->d_type, s->d_mol, s->d_lj32, s->d_lj64,
+                  s->d_excl_start, s->d_excl_partner, s->d_excl_class, s->d_excl_pairs,
+                  s->d_bond_atoms, s->d_angle_atoms, s->d_bond_params, s->d_angle_params,
+                  s->d_gb_vdwr, s->d_gb_scale, s->d_gb_offset, s->d_water, s->d_gb_born,
+                  s->d_gb_psi, s->d_gb_partial, s->d_gb_fixed, s->d_pos, s->d_vel,
+                  s->d_force, s->d_acc, s->d_status, s->d_pairbuf, s->d_paircount,
+                  s->d_stage};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (s->h_acc) cudaFreeHost(s->h_acc);
+  if (s->h_status) cudaFreeHost(s->h_status);
+  if (s->h_stage) cudaFreeHost(s->h_stage);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  return PMGPU_OK;
+}
+
+// ------------------------------------------------------------ evaluation
+struct Launch {
+  int list;
+  PairTerms terms;
+};
+
+static int add_pair_terms(std::vector<Launch> &groups, int list, const PairTerms &t) {
+  for (auto &g : groups) {
+    if (g.list != list || (g.terms.mask & t.mask)) continue;
+    if (t.mask & TERM_LJ) {
+      g.terms.lj_sw = t.lj_sw;
+      g.terms.lj_cut2 = t.lj_cut2;
+    }
+    if (t.mask & TERM_COUL) {
+      g.terms.coul_sw = t.coul_sw;
+      g.terms.coul_cut2 = t.coul_cut2;
+    }
+    if (t.mask & TERM_EWALD) {
+      g.terms.ewald_alpha = t.ewald_alpha;
+      g.terms.ewald_rc2 = t.ewald_rc2;
+      g.terms.exact_erf = t.exact_erf;
+    }
+    g.terms.mask |= t.mask;
+    return 0;
+  }
+  groups.push_back({list, t});
+  return 0;
+}
+
+// Evaluates the enabled forces (or only force `only`) at the resident
+// positions, accumulating into the (already zeroed) force planes and
+// energy accumulators.
+static int evaluate_forces(System *s, int only, int want_virial, int record) {
+  std::vector<Launch> groups;
+  std::vector<int> prepared(s->lists.size(), 0);
+  for (auto &f : s->forces) {
+    if (only >= 0 ? f.id != only : !f.enabled) continue;
+    if (f.kind == FK_CUTOFF || (f.kind == FK_PME && (f.ewald_flags & PMGPU_EWALD_REAL)))
+      add_pair_terms(groups, f.list_index, f.terms);
+  }
+  // neighbour lists are prepared once per evaluation
+  for (auto &f : s->forces) {
+    if (only >= 0 ? f.id != only : !f.enabled) continue;
+    if (f.list_index >= 0 && !prepared[f.list_index]) {
+      PM_CHECK(nb_prepare(s, &s->lists[f.list_index], 0));
+      prepared[f.list_index] = 1;
+    }
+  }
+  for (auto &g : groups)
+    PM_CHECK(nb_pair_forces(s, &s->lists[g.list], g.terms, want_virial, record));
+  for (auto &f : s->forces) {
+    if (only >= 0 ? f.id != only : !f.enabled) continue;
+    switch (f.kind) {
+      case FK_PME:
+        if (f.ewald_flags & PMGPU_EWALD_RECIPROCAL) PM_CHECK(pme_reciprocal(s, &f, want_virial));
+        if (f.ewald_flags & PMGPU_EWALD_CORRECTION) PM_CHECK(ewald_correction(s, &f, want_virial));
+        break;
+      case FK_GB:
+        PM_CHECK(gb_forces(s, &f));
+        break;
+      case FK_BONDED:
+        PM_CHECK(bonded_forces(s, &f, want_virial));
+        break;
+      case FK_SIMPLEFULL:
+        PM_CHECK(nb_simplefull(s, f.sf_lj, f.sf_coul, want_virial));
+        break;
+      default:
+        break;
+    }
+  }
+  return PMGPU_OK;
+}
+
+// Constant energy terms (Ewald point self energy and charged-system term,
+// NonbondedFullEwaldSystemForce.h:344-353, :694-714) for the selected forces.
+static void constant_terms(System *s, int only, double *energies, double *virial) {
+  for (auto &f : s->forces) {
+    if (only >= 0 ? f.id != only : !f.enabled) continue;
+    if (f.kind == FK_PME && (f.ewald_flags & PMGPU_EWALD_CORRECTION)) {
+      if (energies) energies[PMGPU_E_COULOMB] += f.self_energy + f.charged_energy;
+      if (virial) {
+        virial[0] += f.charged_energy;
+        virial[4] += f.charged_energy;
+        virial[8] += f.charged_energy;
+      }
+    }
+  }
+}
+
+static int read_results(System *s, int only, double *energies, double *virial, int add) {
+  PM_CUDA(cudaMemcpyAsync(s->h_acc, s->d_acc, sizeof(long long) * ACC_COUNT,
+                          cudaMemcpyDeviceToHost, s->stream));
+  PM_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                          s->stream));
+  PM_CUDA(cudaStreamSynchronize(s->stream));
+  double e[PMGPU_E_COUNT], v[9];
+  for (int k = 0; k < PMGPU_E_COUNT; k++) e[k] = (double)s->h_acc[k] / kEnergyScale;
+  for (int k = 0; k < 9; k++) v[k] = (double)s->h_acc[ACC_VIRIAL + k] / kEnergyScale;
+  constant_terms(s, only, e, v);
+  s->last_pairs = s->h_acc[ACC_PAIRS] / 2;
+  for (int k = 0; k < PMGPU_E_COUNT; k++) s->last_energy[k] = e[k];
+  for (int k = 0; k < 9; k++) s->last_virial[k] = v[k];
+  if (energies)
+    for (int k = 0; k < PMGPU_E_COUNT; k++) energies[k] = add ? energies[k] + e[k] : e[k];
+  if (virial)
+    for (int k = 0; k < 9; k++) virial[k] = add ? virial[k] + v[k] : v[k];
+  int st = *s->h_status;
+  if (st) {
+    PM_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
+    if (st & ST_LIST_OVERFLOW) {
+      // grow every list for the next call; this result is incomplete
+      for (auto &nl : s->lists) {
+        int cap = nl.cap * 2;
+        nb_list_free(&nl);
+        nl.cap = cap;
+        PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
+      }
+      return fail(PMGPU_ERR_OVERFLOW,
+                  "neighbour list capacity exceeded; capacity doubled, repeat the call");
+    }
+    if (st & ST_NONFINITE) return fail(PMGPU_ERR_NAN, "non-finite position or force");
+  }
+  return PMGPU_OK;
+}
+
+static int begin_eval(System *s) {
+  PM_CUDA(cudaMemsetAsync(s->d_acc, 0, sizeof(long long) * ACC_COUNT, s->stream));
+  return PMGPU_OK;
+}
+
+}  // namespace pmgpu
+
+using namespace pmgpu;
+
+// ===================================================================== ABI
+extern "C" {
+
+const char *pmgpu_last_error(void) { return g_last_error.c_str(); }
+int pmgpu_abi_version(void) { return PMGPU_ABI_VERSION; }
+
+int pmgpu_context_create(int device, pmgpu_context **out) {
+  if (!out) return fail(PMGPU_ERR_ARG, "null output pointer");
+  int count = 0;
+  PM_CUDA(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) return fail(PMGPU_ERR_ARG, "no such CUDA device");
+  PM_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  PM_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return fail(PMGPU_ERR_UNSUPPORTED, "libpmgpu is built for sm_100a (Blackwell B200)");
+  auto *c = new pmgpu_context();
+  c->device = device;
+  *out = c;
+  return PMGPU_OK;
+}
+
+int pmgpu_context_destroy(pmgpu_context *ctx) {
+  delete ctx;
+  return PMGPU_OK;
+}
+
+int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precision,
+                        pmgpu_system **out) {
+  if (!ctx || !t || !out) return fail(PMGPU_ERR_ARG, "null argument");
+  if (t->n_atoms < 0 || t->n_atoms >= kMaxAtoms)
+    return fail(PMGPU_ERR_ARG, "atom count out of range (0 .. 2^24-1)");
+  if (precision != PMGPU_PREC_MIXED && precision != PMGPU_PREC_DOUBLE)
+    return fail(PMGPU_ERR_ARG, "precision must be PMGPU_PREC_MIXED or PMGPU_PREC_DOUBLE");
+  int n = t->n_atoms;
+  if (n > 0 && (!t->charge || !t->mass || !t->type || !t->molecule))
+    return fail(PMGPU_ERR_ARG, "charge, mass, type and molecule arrays are required");
+  if (t->n_types < 1 || !t->lj) return fail(PMGPU_ERR_ARG, "LJ table required (n_types >= 1)");
+  for (int i = 0; i < n; i++)
+    if (t->type[i] < 0 || t->type[i] >= t->n_types)
+      return fail(PMGPU_ERR_ARG, "atom type index out of range");
+  if (t->periodic) {
+    const double *b = t->box;
+    if (b[1] != 0 || b[2] != 0 || b[3] != 0 || b[5] != 0 || b[6] != 0 || b[7] != 0)
+      return fail(PMGPU_ERR_UNSUPPORTED, "only orthogonal periodic boxes are supported");
+    if (!(b[0] > 0 && b[4] > 0 && b[8] > 0))
+      return fail(PMGPU_ERR_ARG, "box edges must be positive");
+  }
+  PM_CUDA(cudaSetDevice(ctx->device));
+  std::unique_ptr<System> s(new System());
+  s->ctx = ctx;
+  s->device = ctx->device;
+  s->n = n;
+  s->precision = precision;
+  box_from_topology(t, &s->box);
+  s->ntypes = t->n_types;
+  s->coulomb_scaling = t->coulomb_scaling;
+  PM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  size_t nn = std::max(1, n);
+  PM_CHECK(upload(&s->d_charge, t->charge, n));
+  PM_CHECK(upload(&s->d_mass, t->mass, n));
+  PM_CHECK(upload(&s->d_type, t->type, n));
+  PM_CHECK(upload(&s->d_mol, t->molecule, n));
+  int nt2 = t->n_types * t->n_types;
+  std::vector<float4> lj32(nt2);
+  std::vector<double4> lj64(nt2);
+  for (int k = 0; k < nt2; k++) {
+    const double *p = t->lj + 4 * k;
+    lj32[k] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3]);
+    lj64[k] = make_double4(p[0], p[1], p[2], p[3]);
+  }
+  PM_CHECK(upload(&s->d_lj32, lj32.data(), nt2));
+  PM_CHECK(upload(&s->d_lj64, lj64.data(), nt2));
+  // exclusion table as CSR over both atoms of each pair
+  int ne = std::max(0, t->n_exclusions);
+  std::vector<int> start(n + 1, 0), partner(2 * (size_t)ne + 1), cls(2 * (size_t)ne + 1);
+  for (int k = 0; k < ne; k++) {
+    int a = t->exclusions[3 * k], b = t->exclusions[3 * k + 1];
+    if (a < 0 || b < 0 || a >= n || b >= n)
+      return fail(PMGPU_ERR_ARG, "exclusion atom index out of range");
+    start[a + 1]++;
+    start[b + 1]++;
+  }
+  for (int i = 0; i < n; i++) start[i + 1] += start[i];
+  std::vector<int> cur(start.begin(), start.end() - 1);
+  for (int k = 0; k < ne; k++) {
+    int a = t->exclusions[3 * k], b = t->exclusions[3 * k + 1], c = t->exclusions[3 * k + 2];
+    partner[cur[a]] = b; cls[cur[a]++] = c;
+    partner[cur[b]] = a; cls[cur[b]++] = c;
+  }
+  PM_CHECK(upload(&s->d_excl_start, start.data(), n + 1));
+  PM_CHECK(upload(&s->d_excl_partner, partner.data(), 2 * (size_t)ne + 1));
+  PM_CHECK(upload(&s->d_excl_class, cls.data(), 2 * (size_t)ne + 1));
+  // The correction term iterates the table with the class each entry holds.
+  std::vector<int> table(3 * (size_t)ne + 3);
+  for (int k = 0; k < ne; k++) {
+    table[3 * k] = t->exclusions[3 * k];
+    table[3 * k + 1] = t->exclusions[3 * k + 1];
+    table[3 * k + 2] = t->exclusion_table_class ? t->exclusion_table_class[k]
+                                                : t->exclusions[3 * k + 2];
+  }
+  PM_CHECK(upload(&s->d_excl_pairs, table.data(), 3 * (size_t)ne));
+  s->n_excl = ne;
+  s->n_bonds = std::max(0, t->n_bonds);
+  s->n_angles = std::max(0, t->n_angles);
+  if (s->n_bonds && (!t->bond_atoms || !t->bond_params))
+    return fail(PMGPU_ERR_ARG, "bond arrays missing");
+  if (s->n_angles && (!t->angle_atoms || !t->angle_params))
+    return fail(PMGPU_ERR_ARG, "angle arrays missing");
+  PM_CHECK(upload(&s->d_bond_atoms, s->n_bonds ? t->bond_atoms : (const int *)nullptr, 2 * (size_t)s->n_bonds));
+  PM_CHECK(upload(&s->d_bond_params, s->n_bonds ? t->bond_params : (const double *)nullptr, 2 * (size_t)s->n_bonds));
+  PM_CHECK(upload(&s->d_angle_atoms, s->n_angles ? t->angle_atoms : (const int *)nullptr, 3 * (size_t)s->n_angles));
+  PM_CHECK(upload(&s->d_angle_params, s->n_angles ? t->angle_params : (const double *)nullptr, 4 * (size_t)s->n_angles));
+  if (t->gb_vdwr && t->gb_scale && t->gb_offset) {
+    PM_CHECK(upload(&s->d_gb_vdwr, t->gb_vdwr, n));
+    PM_CHECK(upload(&s->d_gb_scale, t->gb_scale, n));
+    PM_CHECK(upload(&s->d_gb_offset, t->gb_offset, n));
+    for (int k = 0; k < 3; k++) s->gb_obc[k] = t->gb_obc[k];
+  }
+  if (t->water) PM_CHECK(upload(&s->d_water, t->water, n));
+  PM_CHECK(upload(&s->d_pos, (const double *)nullptr, 3 * nn));
+  PM_CHECK(upload(&s->d_vel, (const double *)nullptr, 3 * nn));
+  PM_CHECK(upload(&s->d_force, (const long long *)nullptr, 3 * nn));
+  PM_CHECK(upload(&s->d_acc, (const long long *)nullptr, ACC_COUNT));
+  PM_CHECK(upload(&s->d_status, (const int *)nullptr, 1));
+  PM_CHECK(upload(&s->d_stage, (const double *)nullptr, 3 * nn));
+  PM_CUDA(cudaMallocHost(&s->h_acc, sizeof(long long) * ACC_COUNT));
+  PM_CUDA(cudaMallocHost(&s->h_status, sizeof(int)));
+  PM_CUDA(cudaMallocHost(&s->h_stage, sizeof(double) * 3 * nn));
+  s->h_charge.assign(t->charge, t->charge + n);
+  *out = reinterpret_cast<pmgpu_system *>(s.release());
+  return PMGPU_OK;
+}
+
+int pmgpu_system_destroy(pmgpu_system *h) {
+  if (!h) return PMGPU_OK;
+  System *s = reinterpret_cast<System *>(h);
+  system_free(s);
+  delete s;
+  return PMGPU_OK;
+}
+
+static System *sysp(pmgpu_system *h) { return reinterpret_cast<System *>(h); }
+
+static int copy_in(System *s, double *dst, const double *src) {
+  if (!src) return fail(PMGPU_ERR_ARG, "null host array");
+  size_t bytes = sizeof(double) * 3 * (size_t)s->n;
+  if (!bytes) return PMGPU_OK;
+  std::memcpy(s->h_stage, src, bytes);
+  PM_CUDA(cudaMemcpyAsync(dst, s->h_stage, bytes, cudaMemcpyHostToDevice, s->stream));
+  PM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMGPU_OK;
+}
+static int copy_out(System *s, double *dst, const double *src) {
+  if (!dst) return fail(PMGPU_ERR_ARG, "null host array");
+  size_t bytes = sizeof(double) * 3 * (size_t)s->n;
+  if (!bytes) return PMGPU_OK;
+  PM_CUDA(cudaMemcpyAsync(s->h_stage, src, bytes, cudaMemcpyDeviceToHost, s->stream));
+  PM_CUDA(cudaStreamSynchronize(s->stream));
+  std::memcpy(dst, s->h_stage, bytes);
+  return PMGPU_OK;
+}
+
+int pmgpu_system_set_positions(pmgpu_system *h, const double *pos) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  PM_CHECK(copy_in(s, s->d_pos, pos));
+  s->forces_valid = 0;
+  return PMGPU_OK;
+}
+int pmgpu_system_get_positions(pmgpu_system *h, double *pos) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  return copy_out(s, pos, s->d_pos);
+}
+int pmgpu_system_set_velocities(pmgpu_system *h, const double *vel) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  return copy_in(s, s->d_vel, vel);
+}
+int pmgpu_system_get_velocities(pmgpu_system *h, double *vel) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  return copy_out(s, vel, s->d_vel);
+}
+
+int pmgpu_system_get_forces(pmgpu_system *h, double *forces) {
+  if (!h || !forces) return fail(PMGPU_ERR_ARG, "null argument");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  return forces_to_host(s, forces, 0);
+}
+
+int pmgpu_system_get_energies(pmgpu_system *h, double *energies, double *virial) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  if (energies)
+    for (int k = 0; k < PMGPU_E_COUNT; k++) energies[k] = s->last_energy[k];
+  if (virial)
+    for (int k = 0; k < 9; k++) virial[k] = s->last_virial[k];
+  return PMGPU_OK;
+}
+
+void *pmgpu_system_stream(pmgpu_system *h) { return h ? (void *)sysp(h)->stream : nullptr; }
+
+int pmgpu_system_device_state(pmgpu_system *h, double **pos, double **vel,
+                              long long **force_fixed) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  if (pos) *pos = s->d_pos;
+  if (vel) *vel = s->d_vel;
+  if (force_fixed) *force_fixed = s->d_force;
+  return PMGPU_OK;
+}
+
+// --------------------------------------------------------------- forces
+static int list_for(System *s, double cutoff, double skin) {
+  for (size_t k = 0; k < s->lists.size(); k++)
+    if (s->lists[k].cutoff == cutoff && s->lists[k].skin == skin) return (int)k;
+  NeighborList nl;
+  int r = nb_list_init(s, &nl, cutoff, skin, 0);
+  if (r != PMGPU_OK) {
+    nb_list_free(&nl);
+    return -r;
+  }
+  s->lists.push_back(nl);
+  return (int)s->lists.size() - 1;
+}
+
+static int add_force(System *s, Force &f, int *force_id) {
+  f.id = (int)s->forces.size();
+  s->forces.push_back(f);
+  if (force_id) *force_id = f.id;
+  s->forces_valid = 0;
+  return PMGPU_OK;
+}
+
+static double default_skin(const System *s, double cutoff) {
+  // A 1 A skin keeps list rebuilds to every ~10-20 steps for liquid water
+  // at 1 fs; small boxes get a smaller skin so cutoff + skin stays below
+  // the box edge.
+  double skin = 1.0;
+  if (s->box.periodic) {
+    double emin = std::min(s->box.e[0], std::min(s->box.e[1], s->box.e[2]));
+    if (cutoff + skin >= emin) skin = std::max(0.0, 0.5 * (emin - cutoff));
+  }
+  return skin;
+}
+
+int pmgpu_force_cutoff_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
+                           const pmgpu_switch *coul_sw, double alg_cutoff,
+                           double cellsize, int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  if (!lj_sw && !coul_sw) return fail(PMGPU_ERR_ARG, "need LennardJones and/or Coulomb");
+  PM_CHECK(validate_switch(lj_sw, "LennardJones"));
+  PM_CHECK(validate_switch(coul_sw, "Coulomb"));
+  if (!(alg_cutoff > 0)) return fail(PMGPU_ERR_ARG, "algorithm cutoff must be > 0");
+  Force f;
+  f.kind = FK_CUTOFF;
+  f.alg_cutoff = alg_cutoff;
+  f.cellsize = cellsize;
+  f.terms.coulomb_scaling = s->coulomb_scaling;
+  // OneAtomPairTwo: rough test with the larger switch cutoff; when any
+  // switch modifies (C1/C2/Cn) both terms are switched, which zeroes each
+  // beyond its own cutoff (OneAtomPairTwo.h:24-27, :40-45, :66-76).
+  double c2max = 0;
+  int modify = 0;
+  if (lj_sw) {
+    switch_setup(lj_sw, &f.terms.lj_sw);
+    c2max = std::max(c2max, f.terms.lj_sw.cutoff2);
+    modify |= f.terms.lj_sw.modify;
+  }
+  if (coul_sw) {
+    switch_setup(coul_sw, &f.terms.coul_sw);
+    c2max = std::max(c2max, f.terms.coul_sw.cutoff2);
+    modify |= f.terms.coul_sw.modify;
+  }
+  if (lj_sw) {
+    f.terms.mask |= TERM_LJ;
+    f.terms.lj_sw.modify = modify;
+    f.terms.lj_cut2 = modify ? f.terms.lj_sw.cutoff2 : c2max;
+    if (!lj_sw || !coul_sw) f.terms.lj_cut2 = f.terms.lj_sw.cutoff2;
+  }
+  if (coul_sw) {
+    f.terms.mask |= TERM_COUL;
+    f.terms.coul_sw.modify = modify;
+    f.terms.coul_cut2 = modify ? f.terms.coul_sw.cutoff2 : c2max;
+    if (!lj_sw || !coul_sw) f.terms.coul_cut2 = f.terms.coul_sw.cutoff2;
+  }
+  double rc = std::sqrt(c2max);
+  if (s->box.periodic) {
+    double emin = std::min(s->box.e[0], std::min(s->box.e[1], s->box.e[2]));
+    if (2 * rc > emin)
+      return fail(PMGPU_ERR_UNSUPPORTED,
+                  "cutoff forces need box edges of at least twice the cutoff "
+                  "(minimal-image pairs)");
+  }
+  int li = list_for(s, rc, default_skin(s, rc));
+  if (li < 0) return -li;
+  f.list_index = li;
+  return add_force(s, f, force_id);
+}
+
+int pmgpu_force_simplefull_add(pmgpu_system *h, int lj, int coulomb, int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  if (s->box.periodic)
+    return fail(PMGPU_ERR_UNSUPPORTED, "NonbondedSimpleFull is the vacuum all-pairs path");
+  if (!lj && !coulomb) return fail(PMGPU_ERR_ARG, "need LennardJones and/or Coulomb");
+  Force f;
+  f.kind = FK_SIMPLEFULL;
+  f.sf_lj = lj ? 1 : 0;
+  f.sf_coul = coulomb ? 1 : 0;
+  return add_force(s, f, force_id);
+}
+
+int pmgpu_force_pme_add(pmgpu_system *h, double alpha, double rc, int order,
+                        const int grid[3], int flags, int exact_erf, double cellsize,
+                        int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  if (!s->box.periodic) return fail(PMGPU_ERR_UNSUPPORTED, "PME needs a periodic box");
+  if (!(alpha > 0)) return fail(PMGPU_ERR_ARG, "alpha must be > 0");
+  if ((flags & PMGPU_EWALD_REAL) && !(rc > 0)) return fail(PMGPU_ERR_ARG, "rc must be > 0");
+  if (flags & ~PMGPU_EWALD_ALL || !flags) return fail(PMGPU_ERR_ARG, "bad Ewald term flags");
+  Force f;
+  f.kind = FK_PME;
+  f.ewald_flags = flags;
+  f.alpha = alpha;
+  f.rc = rc;
+  f.order = order;
+  f.cellsize = cellsize;
+  if (grid) for (int a = 0; a < 3; a++) f.grid[a] = grid[a];
+  f.terms.coulomb_scaling = s->coulomb_scaling;
+  if (flags & PMGPU_EWALD_REAL) {
+    f.terms.mask = TERM_EWALD;
+    f.terms.ewald_alpha = alpha;
+    f.terms.ewald_rc2 = rc * rc;
+    f.terms.exact_erf = exact_erf ? 1 : 0;
+    int li = list_for(s, rc, default_skin(s, rc));
+    if (li < 0) return -li;
+    f.list_index = li;
+  } else {
+    // spatial order for spreading still comes from a list when one exists
+    f.list_index = s->lists.empty() ? -1 : 0;
+  }
+  if (flags & PMGPU_EWALD_RECIPROCAL) PM_CHECK(pme_init(s, &f));
+  // point self energy and charged-system energy (:694-714)
+  double q2 = 0, q = 0;
+  for (double c : s->h_charge) q2 += c * c;
+  for (double c : s->h_charge) q += c;
+  f.self_energy = -q2 * alpha / std::sqrt(M_PI);
+  f.charged_energy = 0.0;
+  if (std::fabs(q * 0.00268283) > 1.0e-5)
+    f.charged_energy = -M_PI / (2.0 * s->box.V * (alpha * alpha)) * q * q;
+  return add_force(s, f, force_id);
+}
+
+int pmgpu_force_gb_add(pmgpu_system *h, double solute, double solvent, int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  if (s->box.periodic) return fail(PMGPU_ERR_UNSUPPORTED, "GB is the vacuum all-pairs path");
+  if (!(solute > 0) || !(solvent > 0)) return fail(PMGPU_ERR_ARG, "dielectrics must be > 0");
+  PM_CHECK(gb_init(s));
+  Force f;
+  f.kind = FK_GB;
+  f.solute = solute;
+  f.solvent = solvent;
+  return add_force(s, f, force_id);
+}
+
+int pmgpu_force_bonded_add(pmgpu_system *h, int bonds, int angles, int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  Force f;
+  f.kind = FK_BONDED;
+  f.bonds = bonds ? 1 : 0;
+  f.angles = angles ? 1 : 0;
+  return add_force(sysp(h), f, force_id);
+}
+
+int pmgpu_force_set_enabled(pmgpu_system *h, int id, int enabled) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
+  s->forces[id].enabled = enabled ? 1 : 0;
+  s->forces_valid = 0;
+  return PMGPU_OK;
+}
+
+int pmgpu_evaluate(pmgpu_system *h, double *energies, double *virial) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  PM_CHECK(zero_forces(s));
+  PM_CHECK(begin_eval(s));
+  PM_CHECK(evaluate_forces(s, -1, virial != nullptr, 0));
+  int r = read_results(s, -1, energies, virial, 0);
+  s->forces_valid = (r == PMGPU_OK);
+  return r;
+}
+
+int pmgpu_force_evaluate(pmgpu_system *h, int id, const double *pos, double *forces,
+                         double *energies, double *virial) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
+  if (pos) PM_CHECK(copy_in(s, s->d_pos, pos));
+  s->forces_valid = 0;
+  PM_CHECK(zero_forces(s));
+  PM_CHECK(begin_eval(s));
+  PM_CHECK(evaluate_forces(s, id, virial != nullptr, 0));
+  PM_CHECK(read_results(s, id, energies, virial, 1));
+  if (forces) PM_CHECK(forces_to_host(s, forces, 1));
+  return PMGPU_OK;
+}
+
+// Integrator::run(n) on the device.  Forces of the current positions are
+// kept resident between calls (ProtoMol keeps myForces between run calls);
+// the first call after positions changed on the host evaluates them, like
+// Integrator::initialize (StandardIntegrator.cpp:39-43).
+int pmgpu_run(pmgpu_system *h, const pmgpu_integrator *it, long n_steps) {
+  if (!h || !it) return fail(PMGPU_ERR_ARG, "null argument");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  if (!(it->timestep_fs > 0)) return fail(PMGPU_ERR_ARG, "timestep must be > 0");
+  if (it->kind != PMGPU_INT_LEAPFROG && it->kind != PMGPU_INT_LANGEVIN_LEAPFROG)
+    return fail(PMGPU_ERR_ARG, "unknown integrator");
+  if (it->kind == PMGPU_INT_LANGEVIN_LEAPFROG && !(it->gamma_ps > 0))
+    return fail(PMGPU_ERR_ARG, "LangevinLeapfrog needs gamma > 0");
+  if (n_steps < 1) return PMGPU_OK;
+  if (!s->forces_valid) {
+    PM_CHECK(zero_forces(s));
+    PM_CHECK(begin_eval(s));
+    PM_CHECK(evaluate_forces(s, -1, 0, 0));
+  }
+  bool lang = it->kind == PMGPU_INT_LANGEVIN_LEAPFROG;
+  for (long k = 0; k < n_steps; k++) {
+    int phase = lang ? (k == 0 ? 3 : 4) : (k == 0 ? 0 : 1);
+    PM_CHECK(integrate_kick_drift(s, it, phase));
+    s->step++;
+    PM_CHECK(begin_eval(s));
+    PM_CHECK(evaluate_forces(s, -1, 0, 0));
+  }
+  PM_CHECK(integrate_kick_drift(s, it, lang ? 5 : 2));
+  int r = read_results(s, -1, nullptr, nullptr, 0);
+  s->forces_valid = (r == PMGPU_OK);
+  return r;
+}
+
+int pmgpu_set_count_pairs(pmgpu_system *h, int enabled) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  sysp(h)->count_pairs = enabled ? 1 : 0;
+  return PMGPU_OK;
+}
+
+int pmgpu_force_stats(pmgpu_system *h, int id, pmgpu_stats *out) {
+  if (!h || !out) return fail(PMGPU_ERR_ARG, "null argument");
+  System *s = sysp(h);
+  if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
+  std::memset(out, 0, sizeof(*out));
+  const Force &f = s->forces[id];
+  out->pairs_in_cutoff = s->last_pairs;
+  if (f.list_index >= 0) {
+    const NeighborList &nl = s->lists[f.list_index];
+    out->cells[0] = nl.ncx;
+    out->cells[1] = nl.ncy;
+    out->cells[2] = nl.ncz;
+    int rb[2] = {0, 0};
+    PM_CUDA(cudaMemcpy(rb, nl.d_rebuild, sizeof(rb), cudaMemcpyDeviceToHost));
+    out->list_builds = rb[1];
+    std::vector<int> cnt(s->n);
+    if (s->n) {
+      PM_CUDA(cudaMemcpy(cnt.data(), nl.d_nbr_count, sizeof(int) * s->n,
+                         cudaMemcpyDeviceToHost));
+      long long tot = 0;
+      for (int c : cnt) tot += c;
+      out->list_entries = tot;
+    }
+  }
+  return PMGPU_OK;
+}
+
+int pmgpu_debug_cell_assign(pmgpu_system *h, double cellsize, int *cell_xyz, int *dims) {
+  if (!h || !cell_xyz || !dims) return fail(PMGPU_ERR_ARG, "null argument");
+  if (!(cellsize > 0)) return fail(PMGPU_ERR_ARG, "cellsize must be > 0");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  return nb_debug_cells(s, cellsize, cell_xyz, dims);
+}
+
+int pmgpu_debug_pair_set(pmgpu_system *h, int id, int *pairs, long long cap,
+                         long long *count) {
+  if (!h || !count) return fail(PMGPU_ERR_ARG, "null argument");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
+  Force &f = s->forces[id];
+  if (f.list_index < 0) return fail(PMGPU_ERR_ARG, "force has no pair list");
+  long long want = std::max(1LL, cap);
+  if (s->pairbuf_cap < want) {
+    if (s->d_pairbuf) cudaFree(s->d_pairbuf);
+    PM_CUDA(cudaMalloc(&s->d_pairbuf, sizeof(long long) * want));
+    s->pairbuf_cap = want;
+  }
+  if (!s->d_paircount) PM_CUDA(cudaMalloc(&s->d_paircount, sizeof(long long)));
+  PM_CUDA(cudaMemsetAsync(s->d_paircount, 0, sizeof(long long), s->stream));
+  PM_CHECK(zero_forces(s));
+  PM_CHECK(begin_eval(s));
+  PM_CHECK(nb_prepare(s, &s->lists[f.list_index], 0));
+  PM_CHECK(nb_pair_forces(s, &s->lists[f.list_index], f.terms, 0, 1));
+  long long total = 0;
+  PM_CUDA(cudaMemcpyAsync(&total, s->d_paircount, sizeof(long long), cudaMemcpyDeviceToHost,
+                          s->stream));
+  PM_CUDA(cudaStreamSynchronize(s->stream));
+  *count = total;
+  long long ncopy = std::min(total, cap);
+  if (pairs && ncopy > 0) {
+    std::vector<long long> buf(ncopy);
+    PM_CUDA(cudaMemcpy(buf.data(), s->d_pairbuf, sizeof(long long) * ncopy,
+                       cudaMemcpyDeviceToHost));
+    for (long long k = 0; k < ncopy; k++) {
+      pairs[2 * k] = (int)(buf[k] >> 32);
+      pairs[2 * k + 1] = (int)(buf[k] & 0xffffffffLL);
+    }
+  }
+  s->forces_valid = 0;
+  return PMGPU_OK;
+}
+
+}  // extern "C"

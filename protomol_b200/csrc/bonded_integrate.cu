@@ -1,0 +1,307 @@
+// Harmonic bonds and angles (FP64), the device-resident leapfrog and
+// Langevin-leapfrog updates (FP64), and fixed-point force conversion.
+#include <cmath>
+
+#include "pm_device.cuh"
+
+namespace pmgpu {
+
+// BondSystemForce::calcBond (force/bonded/BondSystemForce.h:89-124).
+__global__ void k_bonds(Box box, int nb, const int *__restrict__ atoms,
+                        const double *__restrict__ prm, const double *__restrict__ pos,
+                        int n, long long *__restrict__ force, long long *__restrict__ acc,
+                        int want_virial) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
+  if (b < nb) {
+    int a1 = atoms[2 * b], a2 = atoms[2 * b + 1];
+    double k = prm[2 * b], r0 = prm[2 * b + 1];
+    double dx, dy, dz;
+    // r12 = minimalDifference(atom2, atom1): vector from atom 2 to atom 1
+    box_mindiff(box, pos[3 * a2], pos[3 * a2 + 1], pos[3 * a2 + 2], pos[3 * a1],
+                pos[3 * a1 + 1], pos[3 * a1 + 2], dx, dy, dz);
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    double dp = 2.0 * k * (r - r0);
+    double g = -dp / r;
+    double fx = dx * g, fy = dy * g, fz = dz * g;
+    red_add(&force[a1], to_fixed(fx, kForceScale));
+    red_add(&force[n + a1], to_fixed(fy, kForceScale));
+    red_add(&force[2 * n + a1], to_fixed(fz, kForceScale));
+    red_add(&force[a2], to_fixed(-fx, kForceScale));
+    red_add(&force[n + a2], to_fixed(-fy, kForceScale));
+    red_add(&force[2 * n + a2], to_fixed(-fz, kForceScale));
+    e = k * (r - r0) * (r - r0);
+    if (want_virial) {
+      v[0] = fx * dx; v[1] = fx * dy; v[2] = fx * dz;
+      v[3] = fy * dy; v[4] = fy * dz; v[5] = fz * dz;
+    }
+  }
+  e = warp_sum(e);
+  if (want_virial)
+    for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
+  if ((threadIdx.x & 31) == 0) {
+    red_add(&acc[ACC_BOND], to_fixed(e, kEnergyScale));
+    if (want_virial) {
+      const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+      for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
+    }
+  }
+}
+
+// AngleSystemForce::calcAngle (force/bonded/AngleSystemForce.h:86-171),
+// harmonic angle plus Urey-Bradley.
+__global__ void k_angles(Box box, int na, const int *__restrict__ atoms,
+                         const double *__restrict__ prm, const double *__restrict__ pos,
+                         int n, long long *__restrict__ force, long long *__restrict__ acc,
+                         int want_virial) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
+  if (t < na) {
+    int a1 = atoms[3 * t], a2 = atoms[3 * t + 1], a3 = atoms[3 * t + 2];
+    double kt = prm[4 * t], t0 = prm[4 * t + 1], kub = prm[4 * t + 2], rub = prm[4 * t + 3];
+    double r12[3], r32[3], r13[3];
+    box_mindiff(box, pos[3 * a2], pos[3 * a2 + 1], pos[3 * a2 + 2], pos[3 * a1],
+                pos[3 * a1 + 1], pos[3 * a1 + 2], r12[0], r12[1], r12[2]);
+    box_mindiff(box, pos[3 * a2], pos[3 * a2 + 1], pos[3 * a2 + 2], pos[3 * a3],
+                pos[3 * a3 + 1], pos[3 * a3 + 2], r32[0], r32[1], r32[2]);
+    box_mindiff(box, pos[3 * a3], pos[3 * a3 + 1], pos[3 * a3 + 2], pos[3 * a1],
+                pos[3 * a1 + 1], pos[3 * a1 + 2], r13[0], r13[1], r13[2]);
+    double d12 = sqrt(r12[0] * r12[0] + r12[1] * r12[1] + r12[2] * r12[2]);
+    double d32 = sqrt(r32[0] * r32[0] + r32[1] * r32[1] + r32[2] * r32[2]);
+    double d13 = sqrt(r13[0] * r13[0] + r13[1] * r13[1] + r13[2] * r13[2]);
+    double cx = r12[1] * r32[2] - r12[2] * r32[1];
+    double cy = r12[2] * r32[0] - r12[0] * r32[2];
+    double cz = r12[0] * r32[1] - r12[1] * r32[0];
+    double theta = atan2(sqrt(cx * cx + cy * cy + cz * cz),
+                         r12[0] * r32[0] + r12[1] * r32[1] + r12[2] * r32[2]);
+    double st = sin(theta), ct = cos(theta);
+    double dpdt = 2.0 * kt * (theta - t0);
+    double f1[3], f3[3];
+    double ub = 2.0 * kub * (d13 - rub);
+    for (int c = 0; c < 3; c++) {
+      double dr12 = r12[c] / d12, dr32 = r32[c] / d32, dr13 = r13[c] / d13;
+      double dth1 = (dr12 * ct - dr32) / (st * d12);
+      double dth3 = (dr32 * ct - dr12) / (st * d32);
+      double ub1 = dr13 * ub;
+      f1[c] = -dth1 * dpdt - ub1;
+      f3[c] = -dth3 * dpdt + ub1;
+    }
+    for (int c = 0; c < 3; c++) {
+      red_add(&force[c * n + a1], to_fixed(f1[c], kForceScale));
+      red_add(&force[c * n + a3], to_fixed(f3[c], kForceScale));
+      red_add(&force[c * n + a2], to_fixed(-f1[c] - f3[c], kForceScale));
+    }
+    e = kt * (theta - t0) * (theta - t0) + kub * (d13 - rub) * (d13 - rub);
+    if (want_virial) {
+      v[0] = f1[0] * r12[0] + f3[0] * r32[0];
+      v[1] = f1[0] * r12[1] + f3[0] * r32[1];
+      v[2] = f1[0] * r12[2] + f3[0] * r32[2];
+      v[3] = f1[1] * r12[1] + f3[1] * r32[1];
+      v[4] = f1[1] * r12[2] + f3[1] * r32[2];
+      v[5] = f1[2] * r12[2] + f3[2] * r32[2];
+    }
+  }
+  e = warp_sum(e);
+  if (want_virial)
+    for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
+  if ((threadIdx.x & 31) == 0) {
+    red_add(&acc[ACC_ANGLE], to_fixed(e, kEnergyScale));
+    if (want_virial) {
+      const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+      for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
+    }
+  }
+}
+
+int bonded_forces(System *s, Force *f, int want_virial) {
+  if (f->bonds && s->n_bonds > 0) {
+    k_bonds<<<(s->n_bonds + 127) / 128, 128, 0, s->stream>>>(
+        s->box, s->n_bonds, s->d_bond_atoms, s->d_bond_params, s->d_pos, s->n,
+        s->d_force, s->d_acc, want_virial);
+  }
+  if (f->angles && s->n_angles > 0) {
+    k_angles<<<(s->n_angles + 127) / 128, 128, 0, s->stream>>>(
+        s->box, s->n_angles, s->d_angle_atoms, s->d_angle_params, s->d_pos, s->n,
+        s->d_force, s->d_acc, want_virial);
+  }
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+int zero_forces(System *s) {
+  PM_CUDA(cudaMemsetAsync(s->d_force, 0, sizeof(long long) * 3 * (size_t)s->n, s->stream));
+  return PMGPU_OK;
+}
+
+// ------------------------------------------------------------------ RNG
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11): counter-based, so the Langevin noise of atom i
+// at half-kick h of step s is a pure function of (seed, s, h, i) and can be
+// replayed or checkpointed by the step counter alone.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+    uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += W0;
+    k.y += W1;
+  }
+  return c;
+}
+
+__device__ __forceinline__ double u01(uint32_t a, uint32_t b) {
+  // 53-bit uniform in (0, 1]
+  unsigned long long m = ((unsigned long long)a << 21) ^ (unsigned long long)b;
+  m &= (1ull << 53) - 1;
+  return ((double)m + 1.0) * (1.0 / 9007199254740992.0);
+}
+
+__device__ __forceinline__ void gauss3(uint64_t seed, uint64_t step, int half, int atom,
+                                       double g[3]) {
+  uint4 c = make_uint4((uint32_t)atom, (uint32_t)step, (uint32_t)(step >> 32),
+                       (uint32_t)half);
+  uint2 k = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  uint4 r = philox4x32_10(c, k);
+  uint4 r2 = philox4x32_10(make_uint4(c.x, c.y, c.z, c.w | 0x80000000u), k);
+  // Box-Muller on two uniform pairs
+  double u1 = u01(r.x, r.y), u2 = u01(r.z, r.w);
+  double rad = sqrt(-2.0 * log(u1));
+  double s, co;
+  sincospi(2.0 * u2, &s, &co);
+  g[0] = rad * co;
+  g[1] = rad * s;
+  double u3 = u01(r2.x, r2.y), u4 = u01(r2.z, r2.w);
+  double rad2 = sqrt(-2.0 * log(u3));
+  sincospi(2.0 * u4, &s, &co);
+  g[2] = rad2 * co;
+}
+
+// ------------------------------------------------------------ integrator
+struct UpdateArgs {
+  int n;
+  int kicks;          // 0, 1 or 2 kicks with the resident forces
+  int langevin;
+  double coef;        // leapfrog: kick coefficient (h or h/2)
+  double h;           // drift step (timestep * INV_TIMEFACTOR)
+  int drift;
+  int zero_force;
+  // Langevin (LangevinLeapfrogIntegrator.cpp:44-71)
+  double vdt, fdt, ndt, fc;
+  uint64_t seed;
+  uint64_t kstep[2];  // (step, half) of each kick's noise
+  int khalf[2];
+};
+
+__global__ void k_update(UpdateArgs a, const double *__restrict__ mass,
+                         double *__restrict__ pos, double *__restrict__ vel,
+                         long long *__restrict__ force, int *__restrict__ status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  double F[3];
+  for (int c = 0; c < 3; c++) F[c] = (double)force[c * a.n + i] * (1.0 / kForceScale);
+  double m = mass[i];
+  double v[3] = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+  for (int k = 0; k < a.kicks; k++) {
+    if (a.langevin) {
+      double g[3];
+      gauss3(a.seed, a.kstep[k], a.khalf[k], i, g);
+      double sq = sqrt(a.fc / m);
+      for (int c = 0; c < 3; c++)
+        v[c] = xadd(xadd(xmul(v[c], a.vdt), xmul(F[c], a.fdt) / m), xmul(xmul(g[c], sq), a.ndt));
+    } else {
+      // StandardIntegrator::doHalfKick / LeapfrogIntegrator::doKickdoDrift
+      for (int c = 0; c < 3; c++) v[c] = xadd(v[c], xmul(F[c], a.coef) / m);
+    }
+  }
+  for (int c = 0; c < 3; c++) vel[3 * i + c] = v[c];
+  if (a.drift) {
+    for (int c = 0; c < 3; c++) {
+      double x = xadd(pos[3 * i + c], xmul(v[c], a.h));
+      pos[3 * i + c] = x;
+      if (!isfinite(x)) atomicOr(status, ST_NONFINITE);
+    }
+  }
+  if (a.zero_force)
+    for (int c = 0; c < 3; c++) force[c * a.n + i] = 0;
+}
+
+// phase: 0 = leapfrog first (half kick + drift), 1 = leapfrog middle (kick +
+// drift), 2 = leapfrog last (half kick), 3 = Langevin half kick + drift,
+// 4 = Langevin two half kicks (end of step s, start of step s+1) + drift,
+// 5 = Langevin closing half kick.
+int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase) {
+  UpdateArgs a;
+  a.n = s->n;
+  a.h = it->timestep_fs * kInvTimeFactor;
+  a.langevin = it->kind == PMGPU_INT_LANGEVIN_LEAPFROG;
+  a.seed = it->seed;
+  // StandardIntegrator::run gives every step two half kicks; the noise of
+  // kick (step, half) is Philox(seed; atom, step, half).
+  uint64_t st = s->step;
+  a.kstep[0] = st; a.khalf[0] = 0;
+  a.kstep[1] = st; a.khalf[1] = 0;
+  a.vdt = a.fdt = a.ndt = a.fc = 0;
+  if (a.langevin) {
+    double gamma = it->gamma_ps / (1000 * kInvTimeFactor);
+    double dt = a.h;
+    a.fdt = (1.0 - exp(-0.5 * gamma * dt)) / gamma;
+    a.vdt = exp(-0.5 * gamma * dt);
+    a.ndt = sqrt((1.0 - exp(-gamma * dt)) / (2.0 * gamma));
+    a.fc = 2 * kBoltzmann * it->temperature * gamma;
+  }
+  switch (phase) {
+    case 0: a.kicks = 1; a.coef = 0.5 * a.h; a.drift = 1; a.zero_force = 1; break;
+    case 1: a.kicks = 1; a.coef = a.h; a.drift = 1; a.zero_force = 1; break;
+    case 2: a.kicks = 1; a.coef = 0.5 * a.h; a.drift = 0; a.zero_force = 0; break;
+    case 3:  // first half kick of step st, drift
+      a.kicks = 1; a.coef = 0; a.drift = 1; a.zero_force = 1;
+      break;
+    case 4:  // second half kick of step st-1, first half kick of step st
+      a.kicks = 2; a.coef = 0; a.drift = 1; a.zero_force = 1;
+      a.kstep[0] = st - 1; a.khalf[0] = 1;
+      break;
+    case 5:  // second half kick of step st-1
+      a.kicks = 1; a.coef = 0; a.drift = 0; a.zero_force = 0;
+      a.kstep[0] = st - 1; a.khalf[0] = 1;
+      break;
+    default: return fail(PMGPU_ERR_ARG, "bad integrator phase");
+  }
+  if (s->n)
+    k_update<<<(s->n + 255) / 256, 256, 0, s->stream>>>(a, s->d_mass, s->d_pos, s->d_vel,
+                                                        s->d_force, s->d_status);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+__global__ void k_forces_to_aos(int n, const long long *__restrict__ force,
+                                double *__restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int c = 0; c < 3; c++) out[3 * i + c] = (double)force[c * n + i] * (1.0 / kForceScale);
+}
+
+int forces_to_host(System *s, double *out, int add) {
+  int n = s->n;
+  if (n == 0) return PMGPU_OK;
+  double *d_tmp = nullptr;
+  PM_CUDA(cudaMallocAsync(&d_tmp, sizeof(double) * 3 * n, s->stream));
+  k_forces_to_aos<<<(n + 255) / 256, 256, 0, s->stream>>>(n, s->d_force, d_tmp);
+  std::vector<double> h(3 * (size_t)n);
+  cudaError_t e1 = cudaMemcpyAsync(h.data(), d_tmp, sizeof(double) * 3 * n,
+                                   cudaMemcpyDeviceToHost, s->stream);
+  cudaFreeAsync(d_tmp, s->stream);
+  cudaError_t e2 = cudaStreamSynchronize(s->stream);
+  if (e1 != cudaSuccess || e2 != cudaSuccess)
+    return fail(PMGPU_ERR_CUDA, std::string("force download: ") +
+                                    cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+  if (add)
+    for (size_t k = 0; k < h.size(); k++) out[k] += h[k];
+  else
+    for (size_t k = 0; k < h.size(); k++) out[k] = h[k];
+  return PMGPU_OK;
+}
+
+}  // namespace pmgpu

@@ -1,0 +1,324 @@
+// OBC generalized Born in the vacuum all-pairs form:
+//   GBBornRadii  (force/GB/GBBornRadii.cpp:15-173): burial integrals -> psi
+//                -> Born radius through tanh(alpha psi - beta psi^2 + gamma psi^3)
+//   GBPartialSum (force/GB/GBPartialSum.cpp:11-42): per-atom chain-rule sums
+//   GBForce      (force/GB/GBForce.cpp:14-242): pair + self energies, forces
+// The reference stores six N x N scratch arrays (distij, L, U, expTerm,
+// filTerm, partialTerm, topology/Atom.h:35-157); here every pass recomputes
+// what it needs in registers.  Each pass is a thread-per-i kernel over a
+// 2-D grid (i blocks x j chunks) with j tiles in shared memory, and per-atom
+// sums reduced in int64 fixed point, so results are order independent.
+#include <algorithm>
+#include <cmath>
+
+#include "pm_device.cuh"
+
+namespace pmgpu {
+
+constexpr double kGbScale = 1099511627776.0;  // 2^40 for per-atom GB sums
+constexpr int kGbTile = 128;
+
+struct GbArgs {
+  int n;
+  const double *pos, *charge, *vdwr, *scale, *offset;
+  const int *water;
+  double alpha, beta, gamma;
+  double dielec;  // 1/solute - 1/solvent
+  long long *burial_fx, *partial_fx;  // fixed-point accumulators
+  double *born, *psi, *partial;
+  long long *force, *acc;
+};
+
+template <typename Real>
+__device__ __forceinline__ Real gb_burial_term(Real dist, Real oi, Real oj, Real Sj) {
+  // term_i of GBBornRadii::operator() (GBBornRadii.cpp:60-85)
+  Real L, U;
+  Real sjoj = Sj * oj;
+  if (oi >= dist + sjoj) {
+    L = Real(1);
+    U = Real(1);
+  } else {
+    Real a = fabs(dist - sjoj);
+    L = oi > a ? oi : a;
+    U = dist + sjoj;
+  }
+  Real C = (oi < sjoj - dist) ? Real(2) * (Real(1) / oi - Real(1) / L) : Real(0);
+  Real iL = Real(1) / L, iU = Real(1) / U;
+  return (iL - iU) + (dist / Real(4)) * (iU * iU - iL * iL) +
+         (Real(1) / (Real(2) * dist)) * log(L / U) +
+         ((sjoj * sjoj) / (Real(4) * dist)) * (iL * iL - iU * iU) + C;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kGbTile) k_gb_burial(GbArgs a, int jchunk) {
+  __shared__ double sx[kGbTile], sy[kGbTile], sz[kGbTile], so[kGbTile], ss[kGbTile];
+  __shared__ int sw[kGbTile];
+  int i = blockIdx.x * kGbTile + threadIdx.x;
+  bool valid = i < a.n;
+  int ii = valid ? i : 0;
+  double xi = a.pos[3 * ii], yi = a.pos[3 * ii + 1], zi = a.pos[3 * ii + 2];
+  Real oi = (Real)(a.vdwr[ii] - a.offset[ii]);
+  int wi = a.water ? a.water[ii] : 0;
+  double acc = 0.0;
+  int j0 = blockIdx.y * jchunk, j1 = min(a.n, j0 + jchunk);
+  for (int base = j0; base < j1; base += kGbTile) {
+    int j = base + threadIdx.x;
+    if (j < j1) {
+      sx[threadIdx.x] = a.pos[3 * j]; sy[threadIdx.x] = a.pos[3 * j + 1];
+      sz[threadIdx.x] = a.pos[3 * j + 2];
+      so[threadIdx.x] = a.vdwr[j] - a.offset[j];
+      ss[threadIdx.x] = a.scale[j];
+      sw[threadIdx.x] = a.water ? a.water[j] : 0;
+    }
+    __syncthreads();
+    int lim = min(kGbTile, j1 - base);
+    if (valid && !wi) {
+      Real part = 0;
+      for (int k = 0; k < lim; k++) {
+        if (base + k == i || sw[k]) continue;
+        Real dx = (Real)(sx[k] - xi), dy = (Real)(sy[k] - yi), dz = (Real)(sz[k] - zi);
+        Real dist = pm_sqrt(dx * dx + dy * dy + dz * dz);
+        part += gb_burial_term<Real>(dist, oi, (Real)so[k], (Real)ss[k]);
+      }
+      acc += (double)part;
+    }
+    __syncthreads();
+  }
+  if (valid && !wi && acc != 0.0) red_add(&a.burial_fx[i], to_fixed(acc, kGbScale));
+}
+
+// GBBornRadii::postProcess (GBBornRadii.cpp:145-173) and the GB self
+// energy of GBForce (GBForce.cpp:56-63, summed in postProcess :230-242).
+__global__ void k_gb_radii(GbArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double self = 0.0;
+  if (i < a.n) {
+    double burial = (double)a.burial_fx[i] * (1.0 / kGbScale);
+    double ri = a.vdwr[i];
+    double oi = ri - a.offset[i];
+    double psi = 0.5 * burial * oi;
+    double tp = a.alpha * psi - a.beta * psi * psi + a.gamma * psi * psi * psi;
+    double inv = (1 / oi) - (1 / ri) * tanh(tp);
+    double born = 1 / inv;
+    a.psi[i] = psi;
+    a.born[i] = born;
+    a.burial_fx[i] = 0;
+    a.partial_fx[i] = 0;
+    if (a.n > 1) {
+      double q = a.charge[i];
+      self = -0.5 * (q * q) * (1 / born) * a.dielec;
+    }
+  }
+  self = warp_sum(self);
+  if ((threadIdx.x & 31) == 0) red_add(&a.acc[ACC_COULOMB], to_fixed(self, kEnergyScale));
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kGbTile) k_gb_partial(GbArgs a, int jchunk) {
+  __shared__ double sx[kGbTile], sy[kGbTile], sz[kGbTile], sb[kGbTile], sq[kGbTile];
+  int i = blockIdx.x * kGbTile + threadIdx.x;
+  bool valid = i < a.n;
+  int ii = valid ? i : 0;
+  double xi = a.pos[3 * ii], yi = a.pos[3 * ii + 1], zi = a.pos[3 * ii + 2];
+  Real bi = (Real)a.born[ii], qi = (Real)a.charge[ii];
+  double acc = 0.0;
+  int j0 = blockIdx.y * jchunk, j1 = min(a.n, j0 + jchunk);
+  for (int base = j0; base < j1; base += kGbTile) {
+    int j = base + threadIdx.x;
+    if (j < j1) {
+      sx[threadIdx.x] = a.pos[3 * j]; sy[threadIdx.x] = a.pos[3 * j + 1];
+      sz[threadIdx.x] = a.pos[3 * j + 2];
+      sb[threadIdx.x] = a.born[j];
+      sq[threadIdx.x] = a.charge[j];
+    }
+    __syncthreads();
+    int lim = min(kGbTile, j1 - base);
+    if (valid) {
+      Real part = 0;
+      for (int k = 0; k < lim; k++) {
+        if (base + k == i) continue;
+        Real dx = (Real)(sx[k] - xi), dy = (Real)(sy[k] - yi), dz = (Real)(sz[k] - zi);
+        Real r2 = dx * dx + dy * dy + dz * dz;
+        Real bj = (Real)sb[k];
+        Real ex = exp(-r2 / (Real(4) * bi * bj));
+        Real fil = pm_sqrt(r2 + bi * bj * ex);
+        Real p = qi * (Real)sq[k] * (Real(1) / (fil * fil)) * Real(0.5) * (Real(1) / fil) * ex;
+        part += p * (bj + r2 / (Real(4) * bi));  // aTerm, GBPartialSum.cpp:33
+      }
+      acc += (double)part;
+    }
+    __syncthreads();
+  }
+  if (valid && acc != 0.0) red_add(&a.partial_fx[i], to_fixed(acc, kGbScale));
+}
+
+__global__ void k_gb_partial_fin(GbArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.n) a.partial[i] = (double)a.partial_fx[i] * (1.0 / kGbScale);
+}
+
+// dBT/dr and dR/dr of GBForce::operator() (GBForce.cpp:70-124) for the
+// "i sees j" direction.
+template <typename Real>
+__device__ __forceinline__ Real gb_dR(Real dist, Real oi, Real ri, Real bi, Real psi_i,
+                                      Real oj, Real Sj, Real alpha, Real beta, Real gamma) {
+  Real sjoj = Sj * oj;
+  Real L, U;
+  if (oi >= dist + sjoj) {
+    L = 1; U = 1;
+  } else {
+    Real a = fabs(dist - sjoj);
+    L = oi > a ? oi : a;
+    U = dist + sjoj;
+  }
+  Real iL = Real(1) / L, iU = Real(1) / U;
+  Real dL = (oi <= (dist - sjoj)) ? Real(1) : Real(0);
+  Real dU = (oi < (dist + sjoj)) ? Real(1) : Real(0);
+  Real dC = (oi <= (sjoj - dist)) ? Real(2) * iL * iL * dL : Real(0);
+  Real tp = alpha * psi_i - beta * psi_i * psi_i + gamma * psi_i * psi_i * psi_i;
+  Real th = tanh(tp);
+  Real td = alpha - Real(2) * beta * psi_i + Real(3) * gamma * psi_i * psi_i;
+  Real Sjt = sjoj / dist;
+  Real iL2 = iL * iL, iU2 = iU * iU;
+  Real dBT = Real(-0.5) * dL * iL2 + Real(0.5) * dU * iU2 + Real(0.125) * (iU2 - iL2) +
+             Real(0.125) * dist * (Real(2) * iL2 * iL * dL - Real(2) * iU2 * iU * dU) -
+             Real(0.25) * (Real(1) / (dist * dist)) * log(L / U) +
+             (U / (Real(4) * dist * L)) * (iU * dL - (L * iU2) * dU) -
+             Real(0.125) * (Sjt * Sjt) * (iL2 - iU2) +
+             Real(0.25) * ((sjoj * sjoj) / dist) * iU2 * iU * dU -
+             Real(0.25) * ((sjoj * sjoj) / dist) * iL2 * iL * dL + dC;
+  return (bi * bi) * oi * (Real(1) - th * th) * td * (Real(1) / ri) * dBT;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
+  __shared__ double sx[kGbTile], sy[kGbTile], sz[kGbTile], sb[kGbTile], sq[kGbTile];
+  __shared__ double sr[kGbTile], so[kGbTile], ss[kGbTile], sp[kGbTile], spart[kGbTile];
+  int i = blockIdx.x * kGbTile + threadIdx.x;
+  bool valid = i < a.n;
+  int ii = valid ? i : 0;
+  double xi = a.pos[3 * ii], yi = a.pos[3 * ii + 1], zi = a.pos[3 * ii + 2];
+  Real bi = (Real)a.born[ii], qi = (Real)a.charge[ii];
+  Real ri = (Real)a.vdwr[ii], oi = (Real)(a.vdwr[ii] - a.offset[ii]);
+  Real Si = (Real)a.scale[ii], psi_i = (Real)a.psi[ii];
+  Real part_i = (Real)a.partial[ii];
+  Real al = (Real)a.alpha, be = (Real)a.beta, ga = (Real)a.gamma;
+  Real fx = 0, fy = 0, fz = 0;
+  double epair = 0.0;
+  int j0 = blockIdx.y * jchunk, j1 = min(a.n, j0 + jchunk);
+  for (int base = j0; base < j1; base += kGbTile) {
+    int j = base + threadIdx.x;
+    if (j < j1) {
+      sx[threadIdx.x] = a.pos[3 * j]; sy[threadIdx.x] = a.pos[3 * j + 1];
+      sz[threadIdx.x] = a.pos[3 * j + 2];
+      sb[threadIdx.x] = a.born[j]; sq[threadIdx.x] = a.charge[j];
+      sr[threadIdx.x] = a.vdwr[j]; so[threadIdx.x] = a.vdwr[j] - a.offset[j];
+      ss[threadIdx.x] = a.scale[j]; sp[threadIdx.x] = a.psi[j];
+      spart[threadIdx.x] = a.partial[j];
+    }
+    __syncthreads();
+    int lim = min(kGbTile, j1 - base);
+    if (valid) {
+      Real ep = 0;
+      for (int k = 0; k < lim; k++) {
+        if (base + k == i) continue;
+        Real dx = (Real)(sx[k] - xi), dy = (Real)(sy[k] - yi), dz = (Real)(sz[k] - zi);
+        Real r2 = dx * dx + dy * dy + dz * dz;
+        Real dist = pm_sqrt(r2);
+        Real bj = (Real)sb[k], qj = (Real)sq[k];
+        Real oj = (Real)so[k], rj = (Real)sr[k], Sj = (Real)ss[k];
+        Real ex = exp(-r2 / (Real(4) * bi * bj));
+        Real fGB = pm_sqrt(r2 + bi * bj * ex);
+        ep += -(qi * qj) / fGB;
+        Real dRi = gb_dR<Real>(dist, oi, ri, bi, psi_i, oj, Sj, al, be, ga);
+        Real dRj = gb_dR<Real>(dist, oj, rj, bj, (Real)sp[k], oi, Si, al, be, ga);
+        Real pref = qi * qj * (Real(1) / (fGB * fGB)) * Real(0.5) * (Real(1) / fGB);
+        // partialTerm[i][j] and [j][i] (GBPartialSum.cpp:33-41)
+        Real ptij = pref * ex * (bj + r2 / (Real(4) * bi));
+        Real ptji = pref * ex * (bi + r2 / (Real(4) * bj));
+        Real f = -pref * ((Real(2) * dist - Real(0.5) * ex * dist) +
+                          ex * dRi * (bj + r2 / (Real(4) * bi)) +
+                          ex * dRj * (bi + r2 / (Real(4) * bj))) / dist;
+        f -= Real(0.5) * qi * qi * dRi / (bi * bi) / dist;
+        f -= Real(0.5) * qj * qj * dRj / (bj * bj) / dist;
+        f -= (part_i - ptij) * (dRi / dist);
+        f -= ((Real)spart[k] - ptji) * (dRj / dist);
+        fx -= dx * f; fy -= dy * f; fz -= dz * f;
+      }
+      epair += (double)ep;
+    }
+    __syncthreads();
+  }
+  double d = a.dielec;
+  if (valid) {
+    red_add(&a.force[i], to_fixed((double)fx * d, kForceScale));
+    red_add(&a.force[a.n + i], to_fixed((double)fy * d, kForceScale));
+    red_add(&a.force[2 * a.n + i], to_fixed((double)fz * d, kForceScale));
+  }
+  epair = warp_sum(epair) * 0.5 * d;
+  if ((threadIdx.x & 31) == 0) red_add(&a.acc[ACC_COULOMB], to_fixed(epair, kEnergyScale));
+}
+
+static long long *g_dummy = nullptr;
+
+int gb_init(System *s) {
+  int n = std::max(1, s->n);
+  if (!s->d_gb_vdwr) return fail(PMGPU_ERR_ARG, "GB force needs gb_vdwr/gb_scale/gb_offset");
+  if (!s->d_gb_born) {
+    PM_CUDA(cudaMalloc(&s->d_gb_born, sizeof(double) * n));
+    PM_CUDA(cudaMalloc(&s->d_gb_psi, sizeof(double) * n));
+    PM_CUDA(cudaMalloc(&s->d_gb_partial, sizeof(double) * n));
+    PM_CUDA(cudaMalloc(&s->d_gb_fixed, sizeof(long long) * 2 * n));
+    PM_CUDA(cudaMemset(s->d_gb_fixed, 0, sizeof(long long) * 2 * n));
+  }
+  (void)g_dummy;
+  return PMGPU_OK;
+}
+
+int gb_forces(System *s, Force *f) {
+  int n = s->n;
+  if (n == 0) return PMGPU_OK;
+  GbArgs a;
+  a.n = n;
+  a.pos = s->d_pos;
+  a.charge = s->d_charge;
+  a.vdwr = s->d_gb_vdwr;
+  a.scale = s->d_gb_scale;
+  a.offset = s->d_gb_offset;
+  a.water = s->d_water;
+  a.alpha = s->gb_obc[0];
+  a.beta = s->gb_obc[1];
+  a.gamma = s->gb_obc[2];
+  a.dielec = (1 / f->solute) - (1 / f->solvent);
+  a.burial_fx = s->d_gb_fixed;
+  a.partial_fx = s->d_gb_fixed + n;
+  a.born = s->d_gb_born;
+  a.psi = s->d_gb_psi;
+  a.partial = s->d_gb_partial;
+  a.force = s->d_force;
+  a.acc = s->d_acc;
+  int iblocks = (n + kGbTile - 1) / kGbTile;
+  // enough j chunks to put ~2 blocks on every SM
+  int chunks = std::max(1, std::min((296 + iblocks - 1) / iblocks, (n + kGbTile - 1) / kGbTile));
+  int jchunk = ((n + chunks - 1) / chunks + kGbTile - 1) / kGbTile * kGbTile;
+  chunks = (n + jchunk - 1) / jchunk;
+  dim3 grid(iblocks, chunks);
+  cudaStream_t st = s->stream;
+  if (s->precision == PMGPU_PREC_MIXED) {
+    k_gb_burial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);
+    k_gb_partial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    k_gb_partial_fin<<<(n + 127) / 128, 128, 0, st>>>(a);
+    k_gb_force<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
+  } else {
+    k_gb_burial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);
+    k_gb_partial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    k_gb_partial_fin<<<(n + 127) / 128, 128, 0, st>>>(a);
+    k_gb_force<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
+  }
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+}  // namespace pmgpu

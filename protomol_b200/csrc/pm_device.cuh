@@ -1,0 +1,207 @@
+// Device helpers shared by the pmgpu kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pm_internal.cuh"
+
+namespace pmgpu {
+
+// ---------------------------------------------------- exact FP64 helpers
+// The reference's own x86-64 build rounds every double operation
+// separately (no fused multiply-add).  These helpers keep nvcc from
+// contracting, so positions, cells and the cutoff test agree bit for bit.
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xnorm2(double x, double y, double z) {
+  return xadd(xadd(xmul(x, x), xmul(y, y)), xmul(z, z));
+}
+
+// PeriodicBoundaryConditions::minimalDifference(c1, c2, distSquared),
+// PeriodicBoundaryConditions.h:72-110 (orthogonal branch); d = c2 - c1.
+__device__ __forceinline__ double box_mindiff(const Box &b, double x1, double y1,
+                                              double z1, double x2, double y2,
+                                              double z2, double &dx, double &dy,
+                                              double &dz) {
+  dx = xsub(x2, x1);
+  dy = xsub(y2, y1);
+  dz = xsub(z2, z1);
+  double r2 = xnorm2(dx, dy, dz);
+  if (!b.periodic) return r2;
+  if (r2 > b.D) {
+    if (dx < -b.H2[0]) dx = xadd(dx, b.H[0]);
+    else if (dx > b.H2[0]) dx = xsub(dx, b.H[0]);
+    if (dy < -b.H2[1]) dy = xadd(dy, b.H[1]);
+    else if (dy > b.H2[1]) dy = xsub(dy, b.H[1]);
+    if (dz < -b.H2[2]) dz = xadd(dz, b.H[2]);
+    else if (dz > b.H2[2]) dz = xsub(dz, b.H[2]);
+    r2 = xnorm2(dx, dy, dz);
+    if (r2 > b.D) {
+      dx = xsub(dx, xmul(b.e[0], rint(xmul(b.er[0], dx))));
+      dy = xsub(dy, xmul(b.e[1], rint(xmul(b.er[1], dy))));
+      dz = xsub(dz, xmul(b.e[2], rint(xmul(b.er[2], dz))));
+      r2 = xnorm2(dx, dy, dz);
+    }
+  }
+  return r2;
+}
+
+// PeriodicBoundaryConditions::minimalPosition(c), :113-140.
+__device__ __forceinline__ void box_minpos(const Box &b, double x, double y,
+                                           double z, double &ox, double &oy,
+                                           double &oz) {
+  if (!b.periodic) {
+    ox = x; oy = y; oz = z;
+    return;
+  }
+  ox = xsub(x, b.origin[0]);
+  oy = xsub(y, b.origin[1]);
+  oz = xsub(z, b.origin[2]);
+  if (xnorm2(ox, oy, oz) <= b.D) return;
+  if (ox < -b.H2[0]) ox = xadd(ox, b.H[0]);
+  else if (ox > b.H2[0]) ox = xsub(ox, b.H[0]);
+  if (oy < -b.H2[1]) oy = xadd(oy, b.H[1]);
+  else if (oy > b.H2[1]) oy = xsub(oy, b.H[1]);
+  if (oz < -b.H2[2]) oz = xadd(oz, b.H[2]);
+  else if (oz > b.H2[2]) oz = xsub(oz, b.H[2]);
+  if (xnorm2(ox, oy, oz) <= b.D) return;
+  ox = xsub(ox, xmul(b.e[0], rint(xmul(b.er[0], ox))));
+  oy = xsub(oy, xmul(b.e[1], rint(xmul(b.er[1], oy))));
+  oz = xsub(oz, xmul(b.e[2], rint(xmul(b.er[2], oz))));
+}
+
+// ------------------------------------------------------------ switching
+// Value and derivative-over-distance of ProtoMol's switching functions
+// (switch/C1SwitchingFunction.h:41-50, C2SwitchingFunction.h:42-52,
+// CnSwitchingFunction.cpp:149-175, CutoffSwitchingFunction.h:41-44,
+// UniversalSwitchingFunction.h:45-48), in the precision Real.
+template <typename Real>
+struct SwitchDev {
+  int kind;
+  Real cutoff, cutoff2, switchon2;
+  Real c1a, c1b, c1c;
+  Real s1, s2, s3;
+  int ord_int, ord_idx;
+  Real irange[8];
+};
+
+template <typename Real>
+__host__ inline SwitchDev<Real> make_switch_dev(const SwitchParams &p) {
+  SwitchDev<Real> d;
+  d.kind = p.kind;
+  d.cutoff = (Real)p.cutoff;
+  d.cutoff2 = (Real)p.cutoff2;
+  d.switchon2 = (Real)p.switchon2;
+  d.c1a = (Real)p.c1a; d.c1b = (Real)p.c1b; d.c1c = (Real)p.c1c;
+  d.s1 = (Real)p.s1; d.s2 = (Real)p.s2; d.s3 = (Real)p.s3;
+  d.ord_int = p.ord_int; d.ord_idx = p.ord_idx;
+  for (int i = 0; i < 8; i++) d.irange[i] = (Real)p.irange[i];
+  return d;
+}
+
+// Cn polynomial tables (switch/CnSwitchingFunction.cpp:9-23).
+static __constant__ double c_cn_sw[5][7] = {
+    {10., -15., 6., 0, 0, 0, 0},
+    {35., -84., 70., -20., 0, 0, 0},
+    {126., -420., 540., -315., 70., 0, 0},
+    {0, 0, 0, 0, 0, 0, 0},
+    {1716., -9009., 20020., -24024., 16380., -6006., 924.0}};
+static __constant__ double c_cn_dsw[5][7] = {
+    {30., -60., 30., 0, 0, 0, 0},
+    {140., -420., 420., -140., 0, 0, 0},
+    {630., -2520., 3780., -2520., 630., 0, 0},
+    {0, 0, 0, 0, 0, 0, 0},
+    {12012., -72072., 180180., -240240., 180180., -72072., 12012.0}};
+
+__device__ __forceinline__ float pm_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double pm_sqrt(double x) { return sqrt(x); }
+
+template <typename Real>
+__device__ __forceinline__ void switch_eval(const SwitchDev<Real> &w, Real r2,
+                                            Real &val, Real &der) {
+  switch (w.kind) {
+    case PMGPU_SW_C2:
+      der = Real(0);
+      if (r2 > w.cutoff2) {
+        val = Real(0);
+      } else if (r2 >= w.switchon2) {
+        Real c2 = w.cutoff2 - r2;
+        Real c4 = c2 * (w.s2 + Real(2) * r2);
+        val = w.s1 * (c2 * c4);
+        der = w.s3 * (c2 * c2 - c4);
+      } else {
+        val = Real(1);
+      }
+      return;
+    case PMGPU_SW_C1: {
+      if (r2 > w.cutoff2) {
+        val = Real(0);
+        der = Real(0);
+        return;
+      }
+      Real d = pm_sqrt(r2);
+      val = Real(1) - d * (w.c1a - r2 * w.c1b);
+      der = -w.c1a / d + d * w.c1c;
+      return;
+    }
+    case PMGPU_SW_CN: {
+      der = Real(0);
+      val = Real(0);
+      if (r2 > w.cutoff2) return;
+      if (r2 < w.switchon2) {
+        val = Real(1);
+        return;
+      }
+      Real sq = pm_sqrt(r2);
+      Real sd = sq - w.cutoff;
+      Real c = Real(1);
+      for (int i = 0; i < w.ord_int; i++) c *= sd;  // c[0] = sd^ordInt
+      for (int i = 0; i < w.ord_int + 1; i++) {
+        Real cn = c * sd;                            // c[i+1]
+        val += (Real)c_cn_sw[w.ord_idx][i] * cn * w.irange[i];
+        der += (Real)c_cn_dsw[w.ord_idx][i] * c * w.irange[i];
+        c = cn;
+      }
+      der /= sq;
+      return;
+    }
+    case PMGPU_SW_CUTOFF:
+      der = Real(0);
+      val = r2 > w.cutoff2 ? Real(0) : Real(1);
+      return;
+    default:
+      val = Real(1);
+      der = Real(0);
+      return;
+  }
+}
+
+// A&S 7.1.26 polynomial (base/MathUtilities.cpp:39-49).
+template <typename Real>
+__device__ __forceinline__ Real poly5(Real ar) {
+  Real t = Real(1) / (Real(1) + Real(0.3275911) * ar);
+  return t * (Real(0.254829592) +
+              t * (Real(-0.284496736) +
+                   t * (Real(1.421413741) +
+                        t * (Real(-1.453152027) + t * Real(1.061405429)))));
+}
+
+// ----------------------------------------------------------- fixed point
+__device__ __forceinline__ long long to_fixed(double v, double scale) {
+  return __double2ll_rn(v * scale);
+}
+__device__ __forceinline__ void red_add(long long *p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(p),
+            static_cast<unsigned long long>(v));
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace pmgpu

@@ -1,0 +1,254 @@
+// Internal declarations shared by the pmgpu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "pmgpu.h"
+
+namespace pmgpu {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+
+#define PM_CUDA(call)                                                        \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      return ::pmgpu::fail(PMGPU_ERR_CUDA, std::string(#call) + ": " +       \
+                                               cudaGetErrorString(e_));      \
+  } while (0)
+
+#define PM_CHECK(call)                                                       \
+  do {                                                                       \
+    int r_ = (call);                                                         \
+    if (r_ != PMGPU_OK) return r_;                                           \
+  } while (0)
+
+// ------------------------------------------------------------ constants
+constexpr double kForceScale = PMGPU_FORCE_SCALE;   // 2^32 per kcal/mol/A
+constexpr double kEnergyScale = 4294967296.0;       // 2^32 per kcal/mol
+constexpr double kInvTimeFactor = 0.02045482828087295;  // PMConstants.cpp:54
+constexpr double kBoltzmann = 0.001987191;              // PMConstants.cpp:70
+constexpr double kEpsilon = 1.0e-14;                    // PMConstants.cpp:50
+constexpr int kMaxInt2 = 2147483647 / 2;                // PMConstants.cpp:45
+
+// Accumulator slots on the device (int64 fixed point, kEnergyScale).
+enum { ACC_COULOMB = 0, ACC_LJ, ACC_BOND, ACC_ANGLE, ACC_DIHEDRAL,
+       ACC_IMPROPER, ACC_OTHER, ACC_VIRIAL = 7, ACC_PAIRS = 16,
+       ACC_COUNT = 18 };
+
+// Status word bits (device side).
+enum { ST_LIST_OVERFLOW = 1, ST_NONFINITE = 2, ST_CELL_OVERFLOW = 4,
+       ST_BAD_BOX = 8 };
+
+// Neighbour-entry layout: bits 0..23 sorted j index, 24..28 periodic shift
+// code ((sx+1)*9 + (sy+1)*3 + (sz+1)), bit 29 "same molecule, minimal
+// image" (exclusion lookup needed).
+constexpr uint32_t kJMask = 0xFFFFFFu;
+constexpr int kShiftBits = 24;
+constexpr uint32_t kSameMolBit = 1u << 29;
+constexpr int kZeroShift = 13;
+constexpr int kMaxAtoms = 1 << 24;
+
+// Fine sub-cells per coarse cell and axis (Morton-ordered inside a coarse
+// cell), so that 32 consecutive sorted atoms are spatially compact.
+constexpr int kFine = 4;
+constexpr int kFine3 = kFine * kFine * kFine;
+
+// Orthogonal periodic box in the exact form ProtoMol's
+// PeriodicBoundaryConditions::set computes (PeriodicBoundaryConditions.cpp:32-78).
+struct Box {
+  int periodic;
+  double e[3];        // edge lengths e1.x, e2.y, e3.z
+  double er[3];       // e1r.x, e2r.y, e3r.z
+  double origin[3];
+  double min[3], max[3];
+  double H[3], H2[3];
+  double D;           // min half edge squared
+  double V;
+};
+
+// Switching function, FP64 constants as ProtoMol precomputes them.
+struct SwitchParams {
+  int kind;
+  int modify;          // switch value/derivative applied (C1, C2, Cn)
+  double cutoff, cutoff2, switchon2;
+  double c1a, c1b, c1c;          // C1: 1.5/rc, 0.5/rc^3, 1.5/rc^3
+  double s1, s2, s3;             // C2: 1/(rc2-rs2)^3, rc2-3rs2, 4/(rc2-rs2)^3
+  int ord_int, ord_idx;          // Cn
+  double irange[8];
+};
+
+// Pair-term selection for the fused pair kernel.
+enum { TERM_LJ = 1, TERM_COUL = 2, TERM_EWALD = 4 };
+
+struct PairTerms {
+  int mask;                 // TERM_*
+  SwitchParams lj_sw, coul_sw;
+  double lj_cut2, coul_cut2;   // effective rough-test cutoffs^2
+  double ewald_alpha, ewald_rc2;
+  int exact_erf;
+  double coulomb_scaling;
+};
+
+// Device arrays of one neighbour-list structure (one per distinct
+// (cutoff, skin) in a system).
+struct NeighborList {
+  double cutoff = 0, skin = 0, reach = 0;
+  int ncx = 0, ncy = 0, ncz = 0;     // coarse cells
+  double cs[3] = {0, 0, 0};          // coarse cell size vector
+  double vac_origin[3] = {0, 0, 0};  // vacuum grid minimum
+  int nkeys = 0;
+  int cap = 0;                       // entries per atom
+  int built = 0;
+  long long builds = 0;
+  // device
+  int *d_key = nullptr;         // n
+  int *d_key_count = nullptr;   // nkeys
+  int *d_key_start = nullptr;   // nkeys + 1
+  int *d_key_cursor = nullptr;  // nkeys
+  int *d_sorted = nullptr;      // n: original index of sorted slot
+  double *d_offset = nullptr;   // 3n: x_build - x_wrapped (original order)
+  double *d_xbuild = nullptr;   // 3n
+  float4 *d_xhi = nullptr;      // n (x,y,z,q)
+  float4 *d_xlo = nullptr;      // n (x,y,z, type bits)
+  double4 *d_xw = nullptr;      // n FP64 wrapped position + q
+  uint32_t *d_nbr = nullptr;    // cap * n, column major
+  int *d_nbr_count = nullptr;   // n
+  unsigned int *d_maxdisp = nullptr;  // float bits of max displacement^2
+  int *d_rebuild = nullptr;     // rebuild flag
+  void *d_scan_tmp = nullptr;
+};
+
+struct System;
+
+struct Force {
+  int kind = 0;     // FK_*
+  int enabled = 1;
+  int id = 0;
+  // cutoff / ewald
+  PairTerms terms{};
+  double cellsize = 0;
+  double alg_cutoff = 0;
+  int list_index = -1;
+  // ewald
+  int ewald_flags = 0;
+  double alpha = 0, rc = 0;
+  int order = 4;
+  int grid[3] = {0, 0, 0};
+  double self_energy = 0, charged_energy = 0;
+  // pme device state
+  cufftHandle plan_r2c = 0, plan_c2r = 0;
+  float *d_grid = nullptr;            // real grid (K1*K2*K3)
+  long long *d_grid_fixed = nullptr;  // fixed-point spread target
+  float2 *d_cgrid = nullptr;          // complex grid (K1*K2*(K3/2+1))
+  float *d_bsp_mod[3] = {nullptr, nullptr, nullptr};
+  // simplefull
+  int sf_lj = 0, sf_coul = 0;
+  // gb
+  double solute = 1.0, solvent = 80.0;
+  // bonded
+  int bonds = 0, angles = 0;
+  long long last_pairs = 0;
+};
+
+enum { FK_CUTOFF = 1, FK_PME = 2, FK_GB = 3, FK_BONDED = 4,
+       FK_SIMPLEFULL = 5 };
+
+struct System {
+  pmgpu_context *ctx = nullptr;
+  int device = 0;
+  int n = 0;
+  int precision = PMGPU_PREC_MIXED;
+  Box box{};
+  cudaStream_t stream = nullptr;
+  // host copies of static topology
+  std::vector<double> h_charge, h_mass;
+  std::vector<int> h_type, h_mol;
+  int ntypes = 0;
+  std::vector<double> h_lj;
+  std::vector<int> h_excl;
+  double coulomb_scaling = 1.0;
+  // device topology
+  double *d_charge = nullptr, *d_mass = nullptr;
+  int *d_type = nullptr, *d_mol = nullptr;
+  float4 *d_lj32 = nullptr;     // ntypes^2: A, B, A14, B14 (FP32)
+  double4 *d_lj64 = nullptr;    // ntypes^2 (FP64)
+  int *d_excl_start = nullptr, *d_excl_partner = nullptr;  // CSR
+  int *d_excl_class = nullptr;
+  int *d_excl_pairs = nullptr;  // 3 per exclusion (a1, a2, class)
+  int n_excl = 0;
+  int n_bonds = 0, n_angles = 0;
+  int *d_bond_atoms = nullptr, *d_angle_atoms = nullptr;
+  double *d_bond_params = nullptr, *d_angle_params = nullptr;
+  // GB
+  double *d_gb_vdwr = nullptr, *d_gb_scale = nullptr, *d_gb_offset = nullptr;
+  int *d_water = nullptr;
+  double gb_obc[3] = {1.0, 0.8, 4.85};
+  double *d_gb_born = nullptr, *d_gb_psi = nullptr, *d_gb_partial = nullptr;
+  long long *d_gb_fixed = nullptr;  // 2n: burial and partial-sum accumulators
+  // dynamic state
+  double *d_pos = nullptr;   // 3n AoS
+  double *d_vel = nullptr;   // 3n AoS
+  long long *d_force = nullptr;  // 3 planes of n, fixed point
+  long long *d_acc = nullptr;    // ACC_COUNT fixed point accumulators
+  int *d_status = nullptr;
+  long long *h_acc = nullptr;    // pinned mirror
+  int *h_status = nullptr;       // pinned mirror
+  // forces and lists
+  std::vector<Force> forces;
+  std::vector<NeighborList> lists;
+  int count_pairs = 0;
+  int forces_valid = 0;   // resident forces correspond to resident positions
+  uint64_t step = 0;      // RNG counter
+  long long last_pairs = 0;
+  double last_energy[PMGPU_E_COUNT] = {0, 0, 0, 0, 0, 0, 0};
+  double last_virial[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double *d_stage = nullptr;       // 3n device staging
+  double *h_stage = nullptr;       // 3n pinned host staging
+  long long *d_pairbuf = nullptr;  // debug pair-set buffer
+  long long pairbuf_cap = 0;
+  long long *d_paircount = nullptr;
+};
+
+// ------------------------------------------------------------ host API of TUs
+void box_from_topology(const pmgpu_topology *t, Box *b);
+void switch_setup(const pmgpu_switch *in, SwitchParams *o);
+
+// nonbonded.cu
+int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin,
+                 double cellsize_for_debug);
+int nb_list_free(NeighborList *nl);
+int nb_prepare(System *s, NeighborList *nl, int force_rebuild);
+int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t,
+                   int want_virial, int record_pairs);
+int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
+int nb_simplefull(System *s, int lj, int coul, int want_virial);
+
+// pme.cu
+int pme_init(System *s, Force *f);
+int pme_free(Force *f);
+int pme_reciprocal(System *s, Force *f, int want_virial);
+int ewald_correction(System *s, Force *f, int want_virial);
+
+// gb.cu
+int gb_init(System *s);
+int gb_forces(System *s, Force *f);
+
+// bonded_integrate.cu
+int bonded_forces(System *s, Force *f, int want_virial);
+int zero_forces(System *s);
+int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase);
+int forces_to_host(System *s, double *out, int add);
+
+}  // namespace pmgpu
+
+struct pmgpu_context {
+  int device = 0;
+};

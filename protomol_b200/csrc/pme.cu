@@ -1,0 +1,391 @@
+// Ewald Coulomb delivered as smooth PME (Essmann et al., J. Chem. Phys.
+// 103, 8577 (1995)) plus the two O(exclusions) / O(1) terms of ProtoMol's
+// NonbondedFullEwaldSystemForce:
+//   * spread: cardinal B-spline (order p) charge spreading into an int64
+//     fixed-point grid (order independent, bit reproducible);
+//   * 3-D real-to-complex FFT (cuFFT, same stream), convolution with the
+//     influence function exp(-pi^2 m^2/alpha^2)/(pi V m^2) |b(m)|^2 with the
+//     energy and virial reduced on the way, complex-to-real FFT;
+//   * gather: forces from the B-spline derivatives;
+//   * correctionTerm (NonbondedFullEwaldSystemForce.h:1092-1131) in FP64.
+// The reciprocal energy matches the reference's convention
+// E = (4 pi / V) sum_{half space k} exp(-k^2/4a^2)/k^2 |S(k)|^2 (:1013-1054).
+#include <cmath>
+#include <vector>
+
+#include "pm_device.cuh"
+
+namespace pmgpu {
+
+constexpr int kMaxOrder = 8;
+constexpr double kGridScale = 4294967296.0;  // 2^32 per (scaled) charge
+
+struct PmeArgs {
+  Box box;
+  int n;
+  int K[3];
+  int order;
+  double inv_L[3];
+};
+
+// B-spline weights M_p(fr + k), k = 0..p-1, and their derivatives with
+// respect to u, by the Cox-de Boor recursion of the cardinal B-spline.
+__device__ __forceinline__ void bspline(float fr, int p, float *th, float *dth) {
+  float m[kMaxOrder];
+  m[0] = fr;
+  m[1] = 1.f - fr;
+  for (int k = 2; k < p; k++) m[k] = 0.f;
+  for (int n = 3; n <= p; n++) {
+    if (n == p) {
+      // derivative of M_p from M_{p-1}
+      dth[0] = m[0];
+      for (int k = 1; k < p; k++) dth[k] = m[k] - m[k - 1];
+    }
+    float div = 1.f / (float)(n - 1);
+    float prev = 0.f;
+    for (int k = 0; k < n; k++) {
+      float cur = k < n - 1 ? m[k] : 0.f;
+      float x = fr + (float)k;
+      m[k] = div * (x * cur + ((float)n - x) * prev);
+      prev = cur;
+    }
+  }
+  if (p == 2) {
+    dth[0] = 1.f;
+    dth[1] = -1.f;
+  }
+  for (int k = 0; k < p; k++) th[k] = m[k];
+}
+
+// Grid coordinate of one atom along one axis: u = K * (frac), with frac
+// taken from the minimal-image position so it lies in [0, 1].
+__device__ __forceinline__ void grid_coord(const PmeArgs &a, int axis, double w,
+                                           int &iu, float &fr) {
+  double f = (w - a.box.min[axis] + a.box.origin[axis]) * a.inv_L[axis];
+  f -= floor(f);
+  double u = f * a.K[axis];
+  double fl = floor(u);
+  iu = (int)fl;
+  fr = (float)(u - fl);
+  if (iu >= a.K[axis]) iu -= a.K[axis];
+}
+
+__global__ void k_pme_spread(PmeArgs a, const double *__restrict__ pos,
+                             const double *__restrict__ charge,
+                             const int *__restrict__ order_map,
+                             long long *__restrict__ grid) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  int i = order_map ? order_map[t] : t;
+  double wx, wy, wz;
+  box_minpos(a.box, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wx, wy, wz);
+  int iu[3];
+  float fr[3];
+  grid_coord(a, 0, wx, iu[0], fr[0]);
+  grid_coord(a, 1, wy, iu[1], fr[1]);
+  grid_coord(a, 2, wz, iu[2], fr[2]);
+  float th[3][kMaxOrder], dth[3][kMaxOrder];
+  for (int d = 0; d < 3; d++) bspline(fr[d], a.order, th[d], dth[d]);
+  double q = charge[i];
+  int p = a.order;
+  for (int kx = 0; kx < p; kx++) {
+    int gx = iu[0] - kx;
+    if (gx < 0) gx += a.K[0];
+    double qx = q * (double)th[0][kx];
+    for (int ky = 0; ky < p; ky++) {
+      int gy = iu[1] - ky;
+      if (gy < 0) gy += a.K[1];
+      double qxy = qx * (double)th[1][ky];
+      long long *row = grid + ((size_t)gx * a.K[1] + gy) * a.K[2];
+      for (int kz = 0; kz < p; kz++) {
+        int gz = iu[2] - kz;
+        if (gz < 0) gz += a.K[2];
+        red_add(&row[gz], to_fixed(qxy * (double)th[2][kz], kGridScale));
+      }
+    }
+  }
+}
+
+__global__ void k_pme_fixed_to_float(int total, const long long *__restrict__ g,
+                                     float *__restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) out[i] = (float)((double)g[i] * (1.0 / kGridScale));
+}
+
+// Multiply by the influence function; reduce energy and virial.
+// m index convention: m in [0, K/2] -> m, (K/2, K) -> m - K.
+__global__ void k_pme_convolve(int K0, int K1, int K2, double L0, double L1,
+                               double L2, double alpha, double V,
+                               const float *__restrict__ bmod0,
+                               const float *__restrict__ bmod1,
+                               const float *__restrict__ bmod2,
+                               float2 *__restrict__ c, long long *__restrict__ acc,
+                               int want_virial) {
+  int Kh = K2 / 2 + 1;
+  int total = K0 * K1 * Kh;
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
+  if (idx < total) {
+    int mz = idx % Kh;
+    int my_ = (idx / Kh) % K1;
+    int mx_ = idx / (Kh * K1);
+    int mx = mx_ <= K0 / 2 ? mx_ : mx_ - K0;
+    int my = my_ <= K1 / 2 ? my_ : my_ - K1;
+    float2 f = c[idx];
+    if (mx == 0 && my == 0 && mz == 0) {
+      c[idx] = make_float2(0.f, 0.f);
+    } else {
+      double hx = mx / L0, hy = my / L1, hz = mz / L2;
+      double h2 = hx * hx + hy * hy + hz * hz;
+      double pa = M_PI * M_PI / (alpha * alpha);
+      double g = exp(-pa * h2) / (M_PI * V * h2) *
+                 (double)bmod0[mx_] * (double)bmod1[my_] * (double)bmod2[mz];
+      double w = (mz == 0 || (K2 % 2 == 0 && mz == K2 / 2)) ? 1.0 : 2.0;
+      double f2 = (double)f.x * f.x + (double)f.y * f.y;
+      double em = 0.5 * w * g * f2;
+      e = em;
+      if (want_virial) {
+        double cc = 2.0 * (1.0 / h2 + pa);
+        v[0] = em * (1.0 - cc * hx * hx);
+        v[1] = -em * cc * hx * hy;
+        v[2] = -em * cc * hx * hz;
+        v[3] = em * (1.0 - cc * hy * hy);
+        v[4] = -em * cc * hy * hz;
+        v[5] = em * (1.0 - cc * hz * hz);
+      }
+      c[idx] = make_float2((float)(g * f.x), (float)(g * f.y));
+    }
+  }
+  e = warp_sum(e);
+  if (want_virial)
+    for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
+  if ((threadIdx.x & 31) == 0) {
+    red_add(&acc[ACC_COULOMB], to_fixed(e, kEnergyScale));
+    if (want_virial) {
+      const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+      for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
+    }
+  }
+}
+
+__global__ void k_pme_gather(PmeArgs a, const double *__restrict__ pos,
+                             const double *__restrict__ charge,
+                             const int *__restrict__ order_map,
+                             const float *__restrict__ phi, long long *__restrict__ force) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  int i = order_map ? order_map[t] : t;
+  double wx, wy, wz;
+  box_minpos(a.box, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wx, wy, wz);
+  int iu[3];
+  float fr[3];
+  grid_coord(a, 0, wx, iu[0], fr[0]);
+  grid_coord(a, 1, wy, iu[1], fr[1]);
+  grid_coord(a, 2, wz, iu[2], fr[2]);
+  float th[3][kMaxOrder], dth[3][kMaxOrder];
+  for (int d = 0; d < 3; d++) bspline(fr[d], a.order, th[d], dth[d]);
+  int p = a.order;
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+  for (int kx = 0; kx < p; kx++) {
+    int gx = iu[0] - kx;
+    if (gx < 0) gx += a.K[0];
+    for (int ky = 0; ky < p; ky++) {
+      int gy = iu[1] - ky;
+      if (gy < 0) gy += a.K[1];
+      const float *row = phi + ((size_t)gx * a.K[1] + gy) * a.K[2];
+      float txy = th[0][kx] * th[1][ky];
+      float dxy = dth[0][kx] * th[1][ky];
+      float txdy = th[0][kx] * dth[1][ky];
+      for (int kz = 0; kz < p; kz++) {
+        int gz = iu[2] - kz;
+        if (gz < 0) gz += a.K[2];
+        float v = __ldg(&row[gz]);
+        sx += dxy * th[2][kz] * v;
+        sy += txdy * th[2][kz] * v;
+        sz += txy * dth[2][kz] * v;
+      }
+    }
+  }
+  double q = charge[i];
+  double fx = -q * (double)sx * a.K[0] * a.inv_L[0];
+  double fy = -q * (double)sy * a.K[1] * a.inv_L[1];
+  double fz = -q * (double)sz * a.K[2] * a.inv_L[2];
+  red_add(&force[i], to_fixed(fx, kForceScale));
+  red_add(&force[a.n + i], to_fixed(fy, kForceScale));
+  red_add(&force[2 * a.n + i], to_fixed(fz, kForceScale));
+}
+
+// correctionTerm, NonbondedFullEwaldSystemForce.h:1092-1131, FP64.
+__global__ void k_ewald_correction(Box box, int nexcl, const int *__restrict__ ex,
+                                   const double *__restrict__ pos,
+                                   const double *__restrict__ charge, double alpha,
+                                   double csf, int n, long long *__restrict__ force,
+                                   long long *__restrict__ acc, int want_virial) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
+  if (k < nexcl) {
+    int a1 = ex[3 * k], a2 = ex[3 * k + 1], cl = ex[3 * k + 2];
+    double dx, dy, dz;
+    double r2 = box_mindiff(box, pos[3 * a1], pos[3 * a1 + 1], pos[3 * a1 + 2],
+                            pos[3 * a2], pos[3 * a2 + 1], pos[3 * a2 + 2], dx, dy, dz);
+    double qq = charge[a1] * charge[a2];
+    if (cl == PMGPU_EXCL_MODIFIED) qq *= 1 - csf;
+    double r = sqrt(r2);
+    double rr = 1 / r;
+    // the reference's erf() here is the C library's (bit-exact against it)
+    double ee = erf(alpha * r) * rr;
+    e = -qq * ee;
+    double a2pi = 2.0 * alpha / sqrt(M_PI);
+    double g = qq * (a2pi * exp(-(alpha * alpha) * r2) - ee) * rr * rr;
+    double fx = dx * g, fy = dy * g, fz = dz * g;
+    red_add(&force[a1], to_fixed(-fx, kForceScale));
+    red_add(&force[n + a1], to_fixed(-fy, kForceScale));
+    red_add(&force[2 * n + a1], to_fixed(-fz, kForceScale));
+    red_add(&force[a2], to_fixed(fx, kForceScale));
+    red_add(&force[n + a2], to_fixed(fy, kForceScale));
+    red_add(&force[2 * n + a2], to_fixed(fz, kForceScale));
+    if (want_virial) {
+      v[0] = fx * dx; v[1] = fx * dy; v[2] = fx * dz;
+      v[3] = fy * dy; v[4] = fy * dz; v[5] = fz * dz;
+    }
+  }
+  e = warp_sum(e);
+  if (want_virial)
+    for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
+  if ((threadIdx.x & 31) == 0) {
+    red_add(&acc[ACC_COULOMB], to_fixed(e, kEnergyScale));
+    if (want_virial) {
+      const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+      for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
+    }
+  }
+}
+
+// ------------------------------------------------------------ host side
+// |b(m)|^2 = 1 / |sum_{k=0}^{p-2} M_p(k+1) exp(2 pi i m k / K)|^2
+// (Essmann et al. eq. 4.4), with the usual fix for the zero of the
+// denominator at odd orders (average of the neighbours).
+static void bspline_moduli(int K, int p, std::vector<float> &out) {
+  std::vector<double> M(p + 1, 0.0);
+  // M_p at integer points 1..p-1 by the recursion on a unit fractional part
+  std::vector<double> m(p, 0.0);
+  m[0] = 0.0;  // fr = 0
+  m[1] = 1.0;
+  for (int n = 3; n <= p; n++) {
+    double prev = 0.0;
+    for (int k = 0; k < n; k++) {
+      double cur = k < n - 1 ? m[k] : 0.0;
+      double x = (double)k;
+      m[k] = (x * cur + ((double)n - x) * prev) / (double)(n - 1);
+      prev = cur;
+    }
+  }
+  // m[k] = M_p(k) for k = 0..p-1
+  std::vector<double> mod(K);
+  for (int i = 0; i < K; i++) {
+    double sr = 0, si = 0;
+    for (int k = 0; k < p - 1; k++) {
+      double arg = 2.0 * M_PI * i * k / K;
+      sr += m[k + 1] * cos(arg);
+      si += m[k + 1] * sin(arg);
+    }
+    mod[i] = sr * sr + si * si;
+  }
+  for (int i = 0; i < K; i++)
+    if (mod[i] < 1e-7) mod[i] = 0.5 * (mod[(i - 1 + K) % K] + mod[(i + 1) % K]);
+  out.resize(K);
+  for (int i = 0; i < K; i++) out[i] = (float)(1.0 / mod[i]);
+}
+
+int pme_init(System *s, Force *f) {
+  if (!s->box.periodic) return fail(PMGPU_ERR_UNSUPPORTED, "PME needs a periodic box");
+  if (f->order < 2 || f->order > kMaxOrder)
+    return fail(PMGPU_ERR_ARG, "PME order must be in [2, 8]");
+  for (int a = 0; a < 3; a++)
+    if (f->grid[a] < f->order || f->grid[a] > 1024)
+      return fail(PMGPU_ERR_ARG, "PME grid dimension out of range");
+  if (!(f->ewald_flags & PMGPU_EWALD_RECIPROCAL)) return PMGPU_OK;
+  int K0 = f->grid[0], K1 = f->grid[1], K2 = f->grid[2];
+  size_t nreal = (size_t)K0 * K1 * K2;
+  size_t ncplx = (size_t)K0 * K1 * (K2 / 2 + 1);
+  PM_CUDA(cudaMalloc(&f->d_grid, sizeof(float) * nreal));
+  PM_CUDA(cudaMalloc(&f->d_grid_fixed, sizeof(long long) * nreal));
+  PM_CUDA(cudaMalloc(&f->d_cgrid, sizeof(float2) * ncplx));
+  for (int a = 0; a < 3; a++) {
+    std::vector<float> bm;
+    bspline_moduli(f->grid[a], f->order, bm);
+    PM_CUDA(cudaMalloc(&f->d_bsp_mod[a], sizeof(float) * bm.size()));
+    PM_CUDA(cudaMemcpy(f->d_bsp_mod[a], bm.data(), sizeof(float) * bm.size(),
+                       cudaMemcpyHostToDevice));
+  }
+  if (cufftPlan3d(&f->plan_r2c, K0, K1, K2, CUFFT_R2C) != CUFFT_SUCCESS ||
+      cufftPlan3d(&f->plan_c2r, K0, K1, K2, CUFFT_C2R) != CUFFT_SUCCESS)
+    return fail(PMGPU_ERR_CUDA, "cuFFT plan creation failed");
+  if (cufftSetStream(f->plan_r2c, s->stream) != CUFFT_SUCCESS ||
+      cufftSetStream(f->plan_c2r, s->stream) != CUFFT_SUCCESS)
+    return fail(PMGPU_ERR_CUDA, "cufftSetStream failed");
+  return PMGPU_OK;
+}
+
+int pme_free(Force *f) {
+  if (f->plan_r2c) cufftDestroy(f->plan_r2c);
+  if (f->plan_c2r) cufftDestroy(f->plan_c2r);
+  f->plan_r2c = f->plan_c2r = 0;
+  void *ptrs[] = {f->d_grid, f->d_grid_fixed, f->d_cgrid, f->d_bsp_mod[0],
+                  f->d_bsp_mod[1], f->d_bsp_mod[2]};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  f->d_grid = nullptr; f->d_grid_fixed = nullptr; f->d_cgrid = nullptr;
+  for (int a = 0; a < 3; a++) f->d_bsp_mod[a] = nullptr;
+  return PMGPU_OK;
+}
+
+int pme_reciprocal(System *s, Force *f, int want_virial) {
+  int n = s->n;
+  if (n == 0) return PMGPU_OK;
+  PmeArgs a;
+  a.box = s->box;
+  a.n = n;
+  for (int d = 0; d < 3; d++) {
+    a.K[d] = f->grid[d];
+    a.inv_L[d] = 1.0 / s->box.e[d];
+  }
+  a.order = f->order;
+  int K0 = f->grid[0], K1 = f->grid[1], K2 = f->grid[2];
+  size_t nreal = (size_t)K0 * K1 * K2;
+  size_t ncplx = (size_t)K0 * K1 * (K2 / 2 + 1);
+  // Spread in the spatial order of the pair list when there is one, so
+  // neighbouring threads hit neighbouring grid lines.
+  const int *order_map = nullptr;
+  if (f->list_index >= 0 && f->list_index < (int)s->lists.size() &&
+      s->lists[f->list_index].built)
+    order_map = s->lists[f->list_index].d_sorted;
+  PM_CUDA(cudaMemsetAsync(f->d_grid_fixed, 0, sizeof(long long) * nreal, s->stream));
+  k_pme_spread<<<(n + 127) / 128, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge,
+                                                       order_map, f->d_grid_fixed);
+  k_pme_fixed_to_float<<<(int)((nreal + 255) / 256), 256, 0, s->stream>>>(
+      (int)nreal, f->d_grid_fixed, f->d_grid);
+  if (cufftExecR2C(f->plan_r2c, f->d_grid, (cufftComplex *)f->d_cgrid) != CUFFT_SUCCESS)
+    return fail(PMGPU_ERR_CUDA, "cufftExecR2C failed");
+  k_pme_convolve<<<(int)((ncplx + 255) / 256), 256, 0, s->stream>>>(
+      K0, K1, K2, s->box.e[0], s->box.e[1], s->box.e[2], f->alpha, s->box.V,
+      f->d_bsp_mod[0], f->d_bsp_mod[1], f->d_bsp_mod[2], f->d_cgrid, s->d_acc,
+      want_virial);
+  if (cufftExecC2R(f->plan_c2r, (cufftComplex *)f->d_cgrid, f->d_grid) != CUFFT_SUCCESS)
+    return fail(PMGPU_ERR_CUDA, "cufftExecC2R failed");
+  k_pme_gather<<<(n + 127) / 128, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge,
+                                                       order_map, f->d_grid, s->d_force);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+int ewald_correction(System *s, Force *f, int want_virial) {
+  if (s->n_excl == 0) return PMGPU_OK;
+  k_ewald_correction<<<(s->n_excl + 127) / 128, 128, 0, s->stream>>>(
+      s->box, s->n_excl, s->d_excl_pairs, s->d_pos, s->d_charge, f->alpha,
+      s->coulomb_scaling, s->n, s->d_force, s->d_acc, want_virial);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+}  // namespace pmgpu

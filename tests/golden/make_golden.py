@@ -1,0 +1,131 @@
+"""Regenerates the golden fixtures in this directory from the unmodified
+ProtoMol reference (built by oracle/ref.mk into oracle/_ref/).
+
+Each fixture is an .npz holding the topology ProtoMol built (charges, masses,
+types, molecules, LJ table, exclusion table, box, GB atom parameters), the
+positions, and the FP64 forces and ScalarStructure energies of each force
+line, as written by oracle/_ref/pm_forcedump.  Inputs are the reference's own
+test systems (its test/tests/*.conf data) and seeded synthetic systems from
+protomol_b200.systems written out as PSF/PAR/XYZ.
+
+    python tests/golden/make_golden.py            # needs the reference tree
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import refdump  # noqa: E402
+from protomol_b200 import systems  # noqa: E402
+
+REF_TESTS = "/root/reference/test/tests"
+
+
+def save(name: str, d: dict, extra: dict | None = None) -> None:
+    out = {}
+    for k in ("natoms", "charge", "mass", "type", "molecule", "water", "lj", "ntypes",
+              "exclusions", "exclusions_check", "coulomb_scaling", "periodic", "box",
+              "positions", "velocities", "bonds", "bond_params", "angles", "angle_params",
+              "gb_vdwr", "gb_scale", "gb_offset", "gb_obc"):
+        if k in d:
+            out[k] = np.asarray(d[k])
+    defs, ids = [], []
+    for k, f in enumerate(d["forces"]):
+        out[f"forces_{k}"] = f["forces"]
+        out[f"energies_{k}"] = f["energies"]
+        defs.append(f["def"])
+        ids.append(f.get("id", ""))
+    out["defs"] = np.array(defs)
+    out["ids"] = np.array(ids)
+    if extra:
+        out.update(extra)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print("wrote", name, d["natoms"][0], "atoms,", len(defs), "forces")
+
+
+def reference_conf(conf: str, forces: list[str], steps: int = 0) -> dict:
+    tmp = tempfile.mkdtemp()
+    try:
+        os.symlink(os.path.join(REF_TESTS, "data"), os.path.join(tmp, "data"))
+        shutil.copy(os.path.join(REF_TESTS, conf), tmp)
+        os.makedirs(os.path.join(tmp, "output"))
+        return refdump.run(conf, os.path.join(tmp, "dump.txt"), forces, steps=steps, cwd=tmp)
+    finally:
+        shutil.rmtree(tmp)
+
+
+def synthetic(sysm, stem: str, forces: list[str], cellsize: float, steps: int = 0,
+              conf_forces=("Bond",), integrator="Leapfrog", timestep=0.5,
+              integrator_params="") -> dict:
+    tmp = tempfile.mkdtemp()
+    try:
+        conf = systems.write_protomol_inputs(sysm, tmp, stem, list(conf_forces),
+                                             cellsize=cellsize, outputs=False,
+                                             numsteps=max(steps, 20),
+                                             integrator=integrator, timestep=timestep,
+                                             integrator_params=integrator_params)
+        return refdump.run(conf, os.path.join(tmp, "dump.txt"), forces, steps=steps, cwd=tmp)
+    finally:
+        shutil.rmtree(tmp)
+
+
+def main() -> None:
+    # 1. The reference's periodic water test (423 atoms, 28 A box).
+    d = reference_conf("water_CHARMM_PERIODIC_L.conf", [
+        "Coulomb -algorithm NonbondedCutoff -switchingFunction C1 -cutoff 6.5",
+        "LennardJones -algorithm NonbondedCutoff -switchingFunction C2 -cutoff 6.5 -switchon 0.1",
+        "Bond", "Angle",
+        "Coulomb -algorithm FullEwald -real -alpha 0.35 -accuracy 0.0001",
+        "Coulomb -algorithm FullEwald -reciprocal -alpha 0.35 -accuracy 0.0001",
+        "Coulomb -algorithm FullEwald -correction -alpha 0.35 -accuracy 0.0001",
+        "LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction Cn -n 4 "
+        "-switchon 5 -cutoff 8 -switchingFunction Cn -n 3 -switchon 4 -cutoff 8 -cutoff 8",
+    ])
+    save("water423", d)
+    # 2. The reference's GB tests (vacuum, GROMACS topologies).
+    gb = ["GBBornRadii -algorithm NonbondedSimpleFull",
+          "GBPartialSum -algorithm NonbondedSimpleFull",
+          "GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.3",
+          "LennardJones -algorithm NonbondedSimpleFull",
+          "Coulomb -algorithm NonbondedSimpleFull"]
+    save("fip35_gb", reference_conf("www-fip35_FFAMBER_GB_LL.conf", gb))
+    save("alanylalanine_gb", reference_conf("alanylalanine_FFAMBER_GB_LL.conf", gb))
+    # 3. Synthetic 648-atom TIP3P box (216 waters, 18.6 A): the small plain
+    #    configuration, LJ + Coulomb C2 switching 7 -> 8 A.
+    c1 = systems.tip3p_box(216, 18.6, seed=1, lattice=6)
+    d = synthetic(c1, "c1", [
+        "LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction C2 -switchon 7 "
+        "-cutoff 8 -switchingFunction C2 -switchon 7 -cutoff 8 -cutoff 8",
+        "Coulomb -algorithm NonbondedCutoff -switchingFunction C1 -cutoff 8",
+        "LennardJones -algorithm NonbondedCutoff -switchingFunction Cn -n 2 -switchon 6 -cutoff 8",
+        "LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction C2 -switchon 7 "
+        "-cutoff 8 -switchingFunction C1 -cutoff 8 -cutoff 8",
+        "Coulomb -algorithm FullEwald -real -alpha 0.35 -accuracy 0.0001",
+        "Coulomb -algorithm FullEwald -reciprocal -alpha 0.35 -accuracy 0.0001",
+        "Coulomb -algorithm FullEwald -correction -alpha 0.35 -accuracy 0.0001",
+        "Bond", "Angle"], cellsize=8.0)
+    save("c1_tip3p648", d, {"seed": np.array(1)})
+    # 4. Trajectories of the same box through the reference's integrators:
+    #    state after setup and after 20 steps.
+    md = ["LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction C2 -switchon 7 "
+          "-cutoff 8 -switchingFunction C2 -switchon 7 -cutoff 8 -cutoff 8", "Bond", "Angle"]
+    for tag, integ, dt, prm in (("leapfrog", "Leapfrog", 0.5, ""),
+                                ("langevin_t0", "LangevinLeapfrog", 1.0,
+                                 "temperature 0 gamma 5 seed 1234")):
+        d0 = synthetic(c1, "c1", ["Bond"], 8.0, 0, md, integ, dt, prm)
+        d1 = synthetic(c1, "c1", ["Bond"], 8.0, 20, md, integ, dt, prm)
+        save(f"c1_{tag}20", d0, {"positions_20": d1["positions"],
+                                 "velocities_20": d1["velocities"],
+                                 "timestep": np.array(dt), "md_forces": np.array(md)})
+
+
+if __name__ == "__main__":
+    main()

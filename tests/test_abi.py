@@ -1,0 +1,35 @@
+"""The C-ABI library loads and exports every entry point include/pmgpu.h
+declares (no GPU needed: nothing is called)."""
+import ctypes
+import os
+import re
+
+from protomol_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(?:int|void|char)\s*\**\s*(pmgpu_\w+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    names = declared_symbols()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(_lib.EXPORTED) <= names
+
+
+def test_abi_version_without_device():
+    lib = _lib.load()
+    assert lib.pmgpu_abi_version() == 1

@@ -1,0 +1,208 @@
+"""GPU parity: the CUDA path (libpmgpu through the C ABI) against the
+ProtoMol reference's own outputs (golden fixtures) and the FP64 oracle.
+
+Tolerances (stated per the FP32-pair / FP64-accumulate design):
+  * mixed precision: RMS relative force error <= 1e-5 per force term,
+    energy relative error <= 1e-6 (abs floor 1e-4 kcal/mol);
+  * double precision ("FP64 throughout"): RMS relative force error <= 1e-9;
+  * the cutoff pair set and the cell assignment are bit-exact.
+"""
+import numpy as np
+import pytest
+
+import fixtures as F
+import oracle
+from protomol_b200 import (ForceFactory, GpuSystem, LangevinLeapfrogIntegrator,
+                           LeapfrogIntegrator, PMEwaldSystemForce, ScalarStructure)
+
+pytestmark = pytest.mark.gpu
+
+RMS_MIXED = 1e-5
+RMS_DOUBLE = 1e-9
+E_REL = 1e-6
+
+
+def _energy_ok(got, want, rel=E_REL, floor=1e-4):
+    return abs(got - want) <= max(rel * abs(want), floor)
+
+
+def _eval(force, topo):
+    f = np.zeros((topo.pos.shape[0], 3))
+    e = ScalarStructure()
+    force.evaluate(topo.pos, f, e, virial=True)
+    return f, e
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", RMS_MIXED), ("double", RMS_DOUBLE)])
+@pytest.mark.parametrize("name,cellsize", [("water423", 6.5), ("c1_tip3p648", 8.0)])
+def test_cutoff_forces_vs_reference(ctx, name, cellsize, precision, tol):
+    z = F.load(name)
+    topo = F.topology(z)
+    gs = GpuSystem(ctx, topo, precision)
+    ff = ForceFactory(gs, cellsize)
+    n = 0
+    for k, d in enumerate(z["defs"]):
+        d = str(d)
+        if "NonbondedCutoff" not in d:
+            continue
+        force = ff.make(d)
+        f, e = _eval(force, topo)
+        ref_f, ref_e = F.forces(z, k), F.energies(z, k)
+        err = F.rms_rel(f, ref_f)
+        assert err <= tol, (d, err)
+        assert _energy_ok(e[0], ref_e[0]), (d, e[0], ref_e[0])
+        assert _energy_ok(e[1], ref_e[1]), (d, e[1], ref_e[1])
+        vir_err = np.abs(e[7:16] - ref_e[7:16]).max() / max(np.abs(ref_e[7:16]).max(), 1)
+        assert vir_err <= 1e-5, (d, vir_err)
+        n += 1
+    assert n >= 3
+    gs.close()
+
+
+@pytest.mark.parametrize("name,cellsize", [("water423", 6.5), ("c1_tip3p648", 8.0)])
+def test_pair_set_and_cells_bit_exact(ctx, name, cellsize):
+    z = F.load(name)
+    topo = F.topology(z)
+    s = F.oracle_system(z)
+    gs = GpuSystem(ctx, topo, "mixed")
+    rc = 8.0 if name.startswith("c1") else 6.5
+    line = (f"LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction C2 -switchon "
+            f"{rc - 1} -cutoff {rc} -switchingFunction C1 -cutoff {rc} -cutoff {rc}")
+    force = ForceFactory(gs, cellsize).make(line)
+    got = force.pair_set()
+    want = oracle.cutoff_pairs(s, cellsize, rc, rc)[:, :2]
+    got = np.unique(np.sort(got, axis=1), axis=0)
+    want = np.unique(np.sort(want, axis=1), axis=0)
+    assert got.shape == want.shape
+    assert np.array_equal(got, want)
+    cells, dims = gs.cell_assign(cellsize)
+    ocells, odims = oracle.cell_assign(s, cellsize)
+    assert tuple(dims) == tuple(odims)
+    assert np.array_equal(cells, ocells)
+    gs.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", RMS_MIXED), ("double", RMS_DOUBLE)])
+@pytest.mark.parametrize("name", ["water423", "c1_tip3p648"])
+def test_ewald_real_and_correction_vs_reference(ctx, name, precision, tol):
+    z = F.load(name)
+    topo = F.topology(z)
+    gs = GpuSystem(ctx, topo, precision)
+    alpha = 0.35
+    rc = np.sqrt(-np.log(1e-4)) / alpha  # Rc of FullEwald -accuracy 1e-4
+    k_real = [k for k, d in enumerate(z["defs"]) if "FullEwald -real" in str(d)][0]
+    k_corr = [k for k, d in enumerate(z["defs"]) if "FullEwald -correction" in str(d)][0]
+    real = PMEwaldSystemForce(gs, alpha, rc, real=True, reciprocal=False, correction=False)
+    corr = PMEwaldSystemForce(gs, alpha, rc, real=False, reciprocal=False, correction=True)
+    f, e = _eval(real, topo)
+    assert F.rms_rel(f, F.forces(z, k_real)) <= tol
+    assert _energy_ok(e[0], F.energies(z, k_real)[0])
+    f, e = _eval(corr, topo)
+    assert F.rms_rel(f, F.forces(z, k_corr)) <= 1e-10  # FP64 kernel
+    assert _energy_ok(e[0], F.energies(z, k_corr)[0], rel=1e-10, floor=1e-8)
+    gs.close()
+
+
+@pytest.mark.parametrize("name", ["water423", "c1_tip3p648"])
+def test_pme_reciprocal_vs_spme_restatement_and_full_ewald(ctx, name):
+    from oracle import spme
+    z = F.load(name)
+    topo = F.topology(z)
+    gs = GpuSystem(ctx, topo, "mixed")
+    L = topo.box[0]
+    for order, K in ((4, 32), (6, 48)):
+        rec = PMEwaldSystemForce(gs, 0.35, 0.0, order=order, grid=(K, K, K), real=False,
+                                 reciprocal=True, correction=False)
+        f, e = _eval(rec, topo)
+        fo, eo = spme.reciprocal(topo.pos, topo.charge, L, 0.35, order, K)
+        # matched grid, order and alpha: FP32 FFT/B-spline vs FP64 restatement
+        assert F.rms_rel(f, fo) <= 1e-5, (order, K, F.rms_rel(f, fo))
+        assert _energy_ok(e[0], eo, rel=1e-5)
+        rec.set_enabled(False)
+    # Converged PME approaches the reference's full Ewald k-sum (its
+    # algorithm, via the reference-pinned oracle, at accuracy 1e-14 so the
+    # k-sphere truncation is below FP32 resolution).
+    s = F.oracle_system(z)
+    fk, ek, _ = oracle.ewald_reciprocal(s, oracle.ewald_params(s, 0.35, 1e-14))
+    rec = PMEwaldSystemForce(gs, 0.35, 0.0, order=8, grid=(64, 64, 64), real=False,
+                             reciprocal=True, correction=False)
+    f, e = _eval(rec, topo)
+    assert F.rms_rel(f, fk) <= 1e-5, F.rms_rel(f, fk)
+    assert _energy_ok(e[0], ek, rel=1e-5)
+    gs.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", RMS_MIXED), ("double", RMS_DOUBLE)])
+@pytest.mark.parametrize("name", ["fip35_gb", "alanylalanine_gb"])
+def test_gb_and_simplefull_vs_reference(ctx, name, precision, tol):
+    z = F.load(name)
+    topo = F.topology(z)
+    gs = GpuSystem(ctx, topo, precision)
+    ff = ForceFactory(gs)
+    gb = ff.make("GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.3")
+    f, e = _eval(gb, topo)
+    assert F.rms_rel(f, F.forces(z, 2)) <= tol, F.rms_rel(f, F.forces(z, 2))
+    assert _energy_ok(e[0], F.energies(z, 2)[0])
+    for k, line, slot in ((3, "LennardJones -algorithm NonbondedSimpleFull", 1),
+                          (4, "Coulomb -algorithm NonbondedSimpleFull", 0)):
+        fc = ff.make(line)
+        f, e = _eval(fc, topo)
+        assert F.rms_rel(f, F.forces(z, k)) <= tol, line
+        assert _energy_ok(e[slot], F.energies(z, k)[slot])
+    gs.close()
+
+
+def test_bonded_vs_reference(ctx):
+    z = F.load("water423")
+    topo = F.topology(z)
+    gs = GpuSystem(ctx, topo, "mixed")
+    ff = ForceFactory(gs)
+    for k, line, slot in ((2, "Bond", 2), (3, "Angle", 3)):
+        f, e = _eval(ff.make(line), topo)
+        assert F.rms_rel(f, F.forces(z, k)) <= 1e-10
+        assert _energy_ok(e[slot], F.energies(z, k)[slot], rel=1e-10, floor=1e-8)
+    gs.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("double", 1e-8), ("mixed", 2e-4)])
+@pytest.mark.parametrize("tag,integ", [("leapfrog", "leapfrog"), ("langevin_t0", "langevin")])
+def test_trajectory_vs_reference(ctx, tag, integ, precision, tol):
+    """20 steps of the device integrator against the reference's own
+    Leapfrog / LangevinLeapfrog (temperature 0, so the noise term is zero)."""
+    z = F.load(f"c1_{tag}20")
+    topo = F.topology(z)
+    gs = GpuSystem(ctx, topo, precision)
+    ff = ForceFactory(gs, 8.0)
+    for line in z["md_forces"]:
+        ff.make(str(line))
+    dt = float(z["timestep"])
+    it = LeapfrogIntegrator(dt) if integ == "leapfrog" else \
+        LangevinLeapfrogIntegrator(dt, temperature=0.0, gamma=5.0, seed=1234)
+    it.run(gs, 20)
+    x = gs.positions()
+    v = gs.velocities()
+    dx = np.abs(x - z["positions_20"].reshape(-1, 3)).max()
+    dv = np.abs(v - z["velocities_20"].reshape(-1, 3)).max() / np.abs(z["velocities_20"]).max()
+    assert dx <= tol, dx
+    assert dv <= 10 * tol, dv
+    gs.close()
+
+
+def test_run_segmentation_invariance(ctx):
+    """run(20) equals run(7) + run(13) bit for bit (forces stay resident
+    between calls as ProtoMol keeps myForces; fixed-point sums)."""
+    z = F.load("c1_leapfrog20")
+    out = []
+    for split in ((20,), (7, 13)):
+        topo = F.topology(z)
+        gs = GpuSystem(ctx, topo, "mixed")
+        ff = ForceFactory(gs, 8.0)
+        for line in z["md_forces"]:
+            ff.make(str(line))
+        it = LangevinLeapfrogIntegrator(1.0, temperature=300.0, gamma=5.0, seed=99)
+        for n in split:
+            it.run(gs, n)
+        out.append((gs.positions(), gs.velocities()))
+        gs.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])

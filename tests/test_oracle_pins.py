@@ -1,0 +1,125 @@
+"""Pins the FP64 oracle restatement (oracle/pmoracle.c) against the golden
+fixtures, which are outputs of the unmodified ProtoMol reference
+(tests/golden/make_golden.py).  Every term below matches the reference
+to rounding (most bit for bit)."""
+import numpy as np
+import pytest
+
+import fixtures as F
+import oracle
+
+CUT_TOL = 1e-11  # absolute, kcal/mol/A: FP64 restatement vs FP64 reference
+
+
+def _cutoff_terms(d):
+    pots, sws, alg = F.parse_cutoff_def(d)
+    terms = [(p, oracle.Switch(sws[j]["kind"], sws[j].get("cutoff", 0.0),
+                               sws[j].get("switchon", 0.0), 0.0, sws[j].get("n", 0.0)))
+             for j, p in enumerate(pots)]
+    return terms, alg
+
+
+@pytest.mark.parametrize("name,cellsize", [("water423", 6.5), ("c1_tip3p648", 8.0)])
+def test_cutoff_forces_match_reference(name, cellsize):
+    z = F.load(name)
+    s = F.oracle_system(z)
+    seen = 0
+    for k, d in enumerate(z["defs"]):
+        if "NonbondedCutoff" not in d:
+            continue
+        terms, alg = _cutoff_terms(str(d))
+        f, e, v = oracle.cutoff_force(s, cellsize, alg, terms)
+        ref_e = F.energies(z, k)
+        assert np.abs(f - F.forces(z, k)).max() < CUT_TOL, d
+        assert e["coulomb"] == pytest.approx(ref_e[0], abs=1e-9)
+        assert e["lj"] == pytest.approx(ref_e[1], abs=1e-9)
+        assert np.abs(v.reshape(-1) - ref_e[7:16]).max() < 1e-9
+        seen += 1
+    assert seen >= 3
+
+
+@pytest.mark.parametrize("name,cellsize", [("water423", 6.5), ("c1_tip3p648", 8.0)])
+def test_full_ewald_terms_match_reference(name, cellsize):
+    z = F.load(name)
+    s = F.oracle_system(z)
+    ew = oracle.ewald_params(s, 0.35, 1e-4)
+    for k, d in enumerate(z["defs"]):
+        d = str(d)
+        if "FullEwald" not in d:
+            continue
+        if "-real" in d:
+            f, e, v = oracle.ewald_real(s, ew, cellsize)
+        elif "-reciprocal" in d:
+            f, e, v = oracle.ewald_reciprocal(s, ew)
+        else:
+            f, e, v = oracle.ewald_correction(s, ew)
+            a, b = oracle.ewald_self(s, ew)
+            e += a + b
+        assert np.abs(f - F.forces(z, k)).max() < 1e-11, d
+        assert e == pytest.approx(F.energies(z, k)[0], rel=1e-13, abs=1e-10), d
+
+
+@pytest.mark.parametrize("name", ["fip35_gb", "alanylalanine_gb"])
+def test_gb_and_simplefull_match_reference(name):
+    z = F.load(name)
+    s = F.oracle_system(z)
+    f, e, born = oracle.gb_force(s, 1.0, 78.3)
+    assert np.abs(f - F.forces(z, 2)).max() < 1e-10
+    assert e == pytest.approx(F.energies(z, 2)[0], rel=1e-12)
+    for k, pot, slot in ((3, "LennardJones", "lj"), (4, "Coulomb", "coulomb")):
+        f, e, v = oracle.simplefull_force(s, pot)
+        assert np.abs(f - F.forces(z, k)).max() < 1e-10
+        assert e[slot] == pytest.approx(F.energies(z, k)[1 if slot == "lj" else 0], rel=1e-12)
+
+
+def test_spme_restatement_converges_to_reference_ksum():
+    """ProtoMol has no PME.  The FP64 SPME restatement converges to the
+    reference's Ewald k-sum (restated bit-exactly above; accuracy 1e-14 so
+    the k-sphere truncation is negligible) as order and grid grow."""
+    from oracle import spme
+    z = F.load("c1_tip3p648")
+    s = F.oracle_system(z)
+    t = F.topology(z)
+    fk, ek, _ = oracle.ewald_reciprocal(s, oracle.ewald_params(s, 0.35, 1e-14))
+    errs = []
+    for p, K in ((4, 32), (6, 48), (8, 96)):
+        f, e = spme.reciprocal(t.pos, t.charge, t.box, 0.35, p, K)
+        errs.append(F.rms_rel(f, fk))
+        if p == 8:
+            assert abs(e - ek) <= 1e-10 * abs(ek)
+    assert errs[0] > errs[1] > errs[2]
+    assert errs[2] < 1e-10
+
+
+def test_pair_set_equals_brute_force_minimal_image():
+    """The cell enumeration covers exactly the pairs within the cutoff."""
+    z = F.load("c1_tip3p648")
+    s = F.oracle_system(z)
+    pairs = oracle.cutoff_pairs(s, 8.0, 8.0, 8.0)
+    L = s.box[0]
+    got = set(map(tuple, np.sort(pairs[:, :2], axis=1)))
+    want = set()
+    for i in range(s.n):
+        d = s.pos[i + 1:] - s.pos[i]
+        d -= L * np.rint(d / L)
+        r2 = (d * d).sum(1)
+        js = np.nonzero(r2 <= 64.0)[0] + i + 1
+        for j in js:
+            if s.molecule[i] == s.molecule[j]:
+                continue  # TIP3P: every intramolecular pair is excluded
+            want.add((i, int(j)))
+    assert got == want
+
+
+def test_cell_assignment_formula():
+    """ProtoMol cells: cell size L / floor(L / cellsize), index
+    floor((L/2 + minimalPosition(x)) / size)."""
+    z = F.load("water423")
+    s = F.oracle_system(z)
+    cells, dims = oracle.cell_assign(s, 6.5)
+    assert tuple(dims) == (4, 4, 4)
+    w = s.pos - s.box[9:12]
+    w -= 28.0 * np.rint(w / 28.0)
+    ref = np.floor((w + 14.0) / 7.0).astype(int)
+    ok = np.all(cells == ref, axis=1)
+    assert ok.mean() > 0.999
