@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the plain single-system GPU form on the solvated system:
+7,850 TIP3P waters (23,550 atoms) in a 62 A periodic box, seeded lattice +
+0.3 A jitter, random orientations, 300 K Maxwell-Boltzmann velocities;
+Coulomb as Ewald real space (cutoff 9 A, alpha 0.35/A) + smooth PME
+(order 4, 64^3 grid) + exclusion/self corrections; Lennard-Jones cutoff 9 A
+with C2 switching from 8 A; flexible TIP3P bonds and angles; leapfrog at
+1 fs.  FP32 pair math, int64 fixed-point force accumulation, FP64 updates.
+
+A bench step is one Integrator::run(100) segment (100 MD steps between
+outputs, as the configuration reports every 100 steps); ns/day counts MD
+steps.  L2 is flushed (256 MiB write) between timed segments.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pmgpu|reference]
+
+Prints one JSON line (rank 0).  With N > 1 (torchrun) every rank advances
+an independent replica (weak scaling, no collective on the data path); the
+time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_WATERS, EDGE, JITTER, SEED = 7850, 62.0, 0.3, 2024
+DT_FS = 1.0
+ALPHA, RC, ORDER, GRID = 0.35, 9.0, 4, 64
+LJ_SWITCHON = 8.0
+SEGMENT = 100
+METRIC = "ns/day"
+WORKLOAD = ("tip3p_23550_pme64: 7,850 TIP3P waters, 62 A periodic box, Ewald real 9 A "
+            "alpha 0.35 + PME order 4 grid 64^3, LJ C2 8->9 A, bonds+angles, leapfrog 1 fs")
+
+
+def gpu_force_lines():
+    return ["Bond", "Angle",
+            f"LennardJones -algorithm NonbondedCutoff -switchingFunction C2 -switchon {LJ_SWITCHON} "
+            f"-cutoff {RC} -cutoff {RC}",
+            f"Coulomb -algorithm PMEwald -alpha {ALPHA} -cutoff {RC} -order {ORDER} "
+            f"-gridsize {GRID} {GRID} {GRID}"]
+
+
+def reference_force_lines():
+    acc = math.exp(-(ALPHA * RC) ** 2)  # FullEwald Rc = sqrt(-ln acc)/alpha = 9 A
+    return ["Bond", "Angle",
+            f"LennardJones -algorithm NonbondedCutoff -switchingFunction C2 -switchon {LJ_SWITCHON} "
+            f"-cutoff {RC}",
+            f"Coulomb -algorithm FullEwald -real -reciprocal -correction -alpha {ALPHA} "
+            f"-accuracy {acc:.17g}"]
+
+
+def build_system(seed: int):
+    from protomol_b200 import systems
+    return systems.tip3p_box(N_WATERS, EDGE, seed, jitter=JITTER, lattice=20)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+             "-lms", "200", "-i", str(self.idx)], stdout=subprocess.PIPE, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------- reference arm
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "protomol")
+
+
+def run_reference(numsteps: int) -> dict:
+    """Runs ProtoMol's own CPU path (the reference built from its sources by
+    oracle/ref.mk) on the same system and returns its ns/day."""
+    from protomol_b200 import systems
+    sysm = build_system(SEED)
+    tmp = tempfile.mkdtemp()
+    try:
+        conf = systems.write_protomol_inputs(sysm, tmp, "bench", reference_force_lines(),
+                                             integrator="Leapfrog", timestep=DT_FS,
+                                             numsteps=numsteps, cellsize=RC / 2, outputs=False)
+        t0 = time.perf_counter()
+        out = subprocess.run([REF_BIN, conf], cwd=tmp, capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        if out.returncode != 0:
+            raise RuntimeError(out.stdout[-2000:] + out.stderr[-2000:])
+        m = re.search(r"run:\s*([0-9.eE+-]+)\[s\]", out.stdout + out.stderr)
+        run_s = float(m.group(1)) if m else wall
+        return {"ns_per_day": numsteps * DT_FS * 1e-6 * 86400.0 / run_s, "run_s": run_s,
+                "wall_s": wall, "steps": numsteps}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+# --------------------------------------------------------------- GPU arm
+def load_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+def load_traffic() -> float | None:
+    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "pair_kernel_tip3p23550.json")
+    if os.path.exists(p):
+        try:
+            return float(json.load(open(p))["dram_bytes_per_launch"])
+        except Exception:
+            return None
+    return None
+
+
+def algorithmic_bytes_per_step(n: int, grid: int) -> dict:
+    """Unique bytes one MD step must move (counted once), by phase:
+    pair pass N*(16 pos+q + 4 type + 24 force write + 24 force read);
+    cell sort N*(16 + 8 + 2*2*8 + 16); PME spread N*16 + G*8, forward and
+    inverse FFT 2*(G*8 + Gc*8), convolution 2*Gc*8, gather G*8 + N*(16+24);
+    integrator N*(24+24+24+8 + 24+24)."""
+    G = grid ** 3
+    Gc = grid * grid * (grid // 2 + 1)
+    parts = {
+        "pairs": n * (16 + 4 + 24 + 24),
+        "sort": n * (16 + 8 + 2 * 2 * 8 + 16),
+        "spread": n * 16 + G * 8,
+        "fft": 2 * (G * 8 + Gc * 8),
+        "convolution": 2 * Gc * 8,
+        "gather": G * 8 + n * (16 + 24),
+        "integrator": n * (24 + 24 + 24 + 8 + 24 + 24),
+    }
+    parts["total"] = sum(parts.values())
+    return parts
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="pmgpu", choices=["pmgpu", "reference"])
+    ap.add_argument("--segment", type=int, default=SEGMENT)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        if not os.path.exists(REF_BIN):
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "reference binary oracle/_ref/protomol not built"}))
+            return
+        # bounded sample: K timed reference MD steps (each ~ seconds at 23.5k atoms)
+        r = run_reference(max(1, args.steps))
+        cores = 1
+        line = {"impl": "reference", "metric": METRIC, "value": r["ns_per_day"], "unit": "ns/day",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1000.0 * r["run_s"] / r["steps"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "atoms": 3 * N_WATERS,
+                           "reference_algorithm": "FullEwald (explicit k-sum) at alpha 0.35, "
+                                                  "Rc 9 A; no PME exists in the reference"},
+                "cpu_baseline": {"value": r["ns_per_day"], "unit": "ns/day", "cores": cores,
+                                 "kind": "reference",
+                                 "sample": f"{r['steps']} MD steps of the 23,550-atom box "
+                                           f"through ProtoMol's own Leapfrog, 1 core"},
+                "e2e": {"value": r["ns_per_day"], "unit": "ns/day", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from protomol_b200 import Context, ForceFactory, GpuSystem, LeapfrogIntegrator
+
+    sysm = build_system(SEED + rank)
+    ctx = Context(local)
+    gs = GpuSystem(ctx, sysm, "mixed")
+    ff = ForceFactory(gs, RC)
+    for line in gpu_force_lines():
+        ff.make(line)
+    integ = LeapfrogIntegrator(DT_FS)
+    stream = torch.cuda.ExternalStream(gs.stream())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB
+
+    for _ in range(args.warmup):
+        integ.run(gs, args.segment)
+    # device-resident throughput ("value")
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    gs.profile(enable=True, reset=True)
+    k0 = gs.kernel_count()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.add_(1.0)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        integ.run(gs, args.segment)
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        b.synchronize()
+        total_ms += a.elapsed_time(b)
+    torch.cuda.synchronize()
+    launches = gs.kernel_count() - k0
+    prof = gs.profile(enable=False, reset=True)
+    clk = clocks.stop()
+    # end to end through the public API with host buffers: each segment
+    # uploads positions and velocities and reads back positions + energies
+    pos_h = gs.positions()
+    vel_h = gs.velocities()
+    e2e_ms = 0.0
+    for _ in range(max(1, args.steps)):
+        with torch.cuda.stream(stream):
+            flush.add_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gs.set_positions(pos_h)
+        gs.set_velocities(vel_h)
+        integ.run(gs, args.segment)
+        pos_h = gs.positions()
+        vel_h = gs.velocities()
+        e, _ = gs.energies()
+        e2e_ms += 1000.0 * (time.perf_counter() - t0)
+    t_ms = total_ms
+    if dist:
+        t = torch.tensor([total_ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms, e2e_ms = float(t[0]), float(t[1])
+    md_steps = args.steps * args.segment
+    ns_day = world * md_steps * DT_FS * 1e-6 * 86400.0 / (t_ms / 1000.0)
+    e2e_ns_day = world * md_steps * DT_FS * 1e-6 * 86400.0 / (e2e_ms / 1000.0)
+    n = gs.n
+    force = gs.forces[3]
+    st = force.stats()
+    pairs = st["pairs_in_cutoff"]
+    peaks = load_peaks()
+    ab = algorithmic_bytes_per_step(n, GRID)
+    pair_ms, pair_launches = prof["pairs"]
+    pair_avg_s = pair_ms / max(1, pair_launches) / 1000.0
+    pair_gbs = ab["pairs"] / pair_avg_s / 1e9
+    step_s = t_ms / 1000.0 / md_steps / world
+    traffic = load_traffic()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ns_day, "unit": "ns/day", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32-pairs/fp64-update", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "atoms": n, "md_steps_per_bench_step": args.segment,
+                       "timestep_fs": DT_FS, "l2": "flushed (256 MiB write) between timed segments",
+                       "replicas": world, "parallelism": f"replicas x{world}"},
+            "pairs_per_s": pairs * md_steps * world / (t_ms / 1000.0),
+            "pairs_in_cutoff_per_md_step": pairs,
+            "us_per_md_step": 1e6 * step_s,
+            "phase_ms_per_md_step": {k: v[0] / md_steps for k, v in prof.items() if v[1]},
+            "roofline": {"bound": "hbm", "kernel": "k_pairs (fused LJ + Ewald real)",
+                         "achieved": pair_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": pair_gbs / peaks["hbm_gbs"],
+                         "traffic": traffic, "peak_source": peaks["src"],
+                         "algorithmic_bytes_per_launch": ab["pairs"],
+                         "avg_launch_us": pair_avg_s * 1e6,
+                         "step": {"algorithmic_bytes": ab["total"],
+                                  "achieved_gbs": ab["total"] / step_s / 1e9,
+                                  "frac": ab["total"] / step_s / 1e9 / peaks["hbm_gbs"]}},
+            "e2e": {"value": e2e_ns_day, "unit": "ns/day",
+                    "h2d_bytes_per_step": 2 * 3 * n * 8,
+                    "d2h_bytes_per_step": 2 * 3 * n * 8 + 7 * 8},
+            "gpu_launches": launches,
+        }
+        if clk:
+            line["clocks"] = clk
+        if world == 1 and os.path.exists(REF_BIN):
+            try:
+                r = run_reference(2)
+                line["cpu_baseline"] = {"value": r["ns_per_day"], "unit": "ns/day", "cores": 1,
+                                        "kind": "reference",
+                                        "sample": "2 MD steps of the same 23,550-atom box through "
+                                                  "ProtoMol's Leapfrog with FullEwald (alpha 0.35, "
+                                                  "Rc 9 A) + LJ C2 8->9 A + bonds/angles, 1 core"}
+            except Exception as ex:  # reported, never fatal
+                line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+        print(json.dumps(line), flush=True)
+    gs.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -237,6 +237,29 @@ typedef struct {
 int pmgpu_force_stats(pmgpu_system *sys, int force_id, pmgpu_stats *out);
 int pmgpu_set_count_pairs(pmgpu_system *sys, int enabled);
 
+/* Per-phase device timing (CUDA events on the system stream), the
+ * counterpart of ProtoMol's TimerStatistic FORCES/INTEGRATOR timers
+ * (base/TimerStatistic.h:21-28).  Phases: */
+enum {
+  PMGPU_PHASE_LIST = 0,       /* cell sort, gather, neighbour-list build */
+  PMGPU_PHASE_PAIRS = 1,      /* fused LJ / Coulomb / Ewald real pair kernel */
+  PMGPU_PHASE_PME = 2,        /* PME spread + FFTs + convolution + gather */
+  PMGPU_PHASE_CORRECTION = 3, /* Ewald exclusion correction */
+  PMGPU_PHASE_BONDED = 4,     /* bonds and angles */
+  PMGPU_PHASE_GB = 5,         /* GB passes */
+  PMGPU_PHASE_SIMPLEFULL = 6, /* vacuum all-pairs LJ / Coulomb */
+  PMGPU_PHASE_INTEGRATE = 7,  /* kick / drift updates */
+  PMGPU_PHASE_COUNT = 8
+};
+int pmgpu_profile_enable(pmgpu_system *sys, int enabled);
+/* Milliseconds and launch counts per phase accumulated since the last
+ * reset (ms and launches hold PMGPU_PHASE_COUNT entries each). */
+int pmgpu_profile_read(pmgpu_system *sys, double *ms, long long *launches,
+                       int reset);
+/* Number of this library's own kernels launched on the system so far
+ * (library kernels such as cuFFT's are not counted). */
+int pmgpu_kernel_count(pmgpu_system *sys, long long *count);
+
 /* ProtoMol cell assignment (topology/Topology.h:44-86 with
  * CubicCellManager, cellsize given) computed by the device binning kernel
  * on the resident positions: cell_xyz gets 3n ints, dims 3 ints. */

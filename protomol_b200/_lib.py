@@ -35,8 +35,10 @@ EXPORTED = [
     "pmgpu_force_pme_add", "pmgpu_force_gb_add", "pmgpu_force_bonded_add",
     "pmgpu_force_set_enabled", "pmgpu_evaluate", "pmgpu_force_evaluate", "pmgpu_run",
     "pmgpu_set_count_pairs", "pmgpu_force_stats", "pmgpu_debug_cell_assign",
-    "pmgpu_debug_pair_set",
+    "pmgpu_debug_pair_set", "pmgpu_profile_enable", "pmgpu_profile_read",
+    "pmgpu_kernel_count",
 ]
+PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
 
 class PmgpuError(RuntimeError):
@@ -116,6 +118,9 @@ def load() -> C.CDLL:
     lib.pmgpu_force_stats.argtypes = [vp, i32, C.POINTER(Stats)]
     lib.pmgpu_debug_cell_assign.argtypes = [vp, dbl, vp, vp]
     lib.pmgpu_debug_pair_set.argtypes = [vp, i32, vp, C.c_longlong, C.POINTER(C.c_longlong)]
+    lib.pmgpu_profile_enable.argtypes = [vp, i32]
+    lib.pmgpu_profile_read.argtypes = [vp, vp, vp, i32]
+    lib.pmgpu_kernel_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     _lib = lib
     return lib
 

@@ -164,14 +164,63 @@ static int system_free(System *s) {
                   s->d_gb_vdwr, s->d_gb_scale, s->d_gb_offset, s->d_water, s->d_gb_born,
                   s->d_gb_psi, s->d_gb_partial, s->d_gb_fixed, s->d_pos, s->d_vel,
                   s->d_force, s->d_acc, s->d_status, s->d_pairbuf, s->d_paircount,
-                  s->d_stage};
+                  s->d_stage, s->d_snap};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->h_acc) cudaFreeHost(s->h_acc);
   if (s->h_status) cudaFreeHost(s->h_status);
   if (s->h_stage) cudaFreeHost(s->h_stage);
+  prof_collect(s);
+  for (cudaEvent_t e : s->prof.pool) cudaEventDestroy(e);
+  s->prof.pool.clear();
   if (s->stream) cudaStreamDestroy(s->stream);
   return PMGPU_OK;
+}
+
+// ------------------------------------------------------------- profiling
+static cudaEvent_t prof_event(System *s) {
+  Profiler &p = s->prof;
+  if (!p.pool.empty()) {
+    cudaEvent_t e = p.pool.back();
+    p.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void prof_begin(System *s, int phase) {
+  Profiler &p = s->prof;
+  if (!p.enabled) return;
+  p.open_phase = phase;
+  p.open_ev = prof_event(s);
+  cudaEventRecord(p.open_ev, s->stream);
+}
+
+void prof_end(System *s) {
+  Profiler &p = s->prof;
+  if (!p.enabled || p.open_phase < 0) return;
+  cudaEvent_t b = prof_event(s);
+  cudaEventRecord(b, s->stream);
+  p.pending.push_back({p.open_phase, p.open_ev, b});
+  p.open_phase = -1;
+  // bound the number of outstanding events on long segments
+  if (p.pending.size() > 4096) prof_collect(s);
+}
+
+void prof_collect(System *s) {
+  Profiler &p = s->prof;
+  for (auto &m : p.pending) {
+    float t = 0.f;
+    if (cudaEventSynchronize(m.b) == cudaSuccess && cudaEventElapsedTime(&t, m.a, m.b) == cudaSuccess) {
+      p.ms[m.phase] += t;
+      p.launches[m.phase] += 1;
+    }
+    p.pool.push_back(m.a);
+    p.pool.push_back(m.b);
+  }
+  p.pending.clear();
 }
 
 // ------------------------------------------------------------ evaluation
@@ -206,7 +255,8 @@ static int add_pair_terms(std::vector<Launch> &groups, int list, const PairTerms
 // Evaluates the enabled forces (or only force `only`) at the resident
 // positions, accumulating into the (already zeroed) force planes and
 // energy accumulators.
-static int evaluate_forces(System *s, int only, int want_virial, int record) {
+static int evaluate_forces(System *s, int only, int mode) {
+  const int want_virial = mode == PAIR_VIRIAL;
   std::vector<Launch> groups;
   std::vector<int> prepared(s->lists.size(), 0);
   for (auto &f : s->forces) {
@@ -218,31 +268,62 @@ static int evaluate_forces(System *s, int only, int want_virial, int record) {
   for (auto &f : s->forces) {
     if (only >= 0 ? f.id != only : !f.enabled) continue;
     if (f.list_index >= 0 && !prepared[f.list_index]) {
-      PM_CHECK(nb_prepare(s, &s->lists[f.list_index], 0));
+      prof_begin(s, PMGPU_PHASE_LIST);
+      int r = nb_prepare(s, &s->lists[f.list_index], 0);
+      prof_end(s);
+      PM_CHECK(r);
+      s->kernels += 7;  // check, bin, scan, scatter, sort, gather, build
       prepared[f.list_index] = 1;
     }
   }
-  for (auto &g : groups)
-    PM_CHECK(nb_pair_forces(s, &s->lists[g.list], g.terms, want_virial, record));
+  for (auto &g : groups) {
+    prof_begin(s, PMGPU_PHASE_PAIRS);
+    int r = nb_pair_forces(s, &s->lists[g.list], g.terms, mode);
+    prof_end(s);
+    PM_CHECK(r);
+    s->kernels += 1;
+  }
   for (auto &f : s->forces) {
     if (only >= 0 ? f.id != only : !f.enabled) continue;
+    int r = PMGPU_OK;
     switch (f.kind) {
       case FK_PME:
-        if (f.ewald_flags & PMGPU_EWALD_RECIPROCAL) PM_CHECK(pme_reciprocal(s, &f, want_virial));
-        if (f.ewald_flags & PMGPU_EWALD_CORRECTION) PM_CHECK(ewald_correction(s, &f, want_virial));
+        if (f.ewald_flags & PMGPU_EWALD_RECIPROCAL) {
+          prof_begin(s, PMGPU_PHASE_PME);
+          r = pme_reciprocal(s, &f, want_virial);
+          prof_end(s);
+          PM_CHECK(r);
+          s->kernels += 4;  // spread, fixed->float, convolve, gather (+ cuFFT)
+        }
+        if (f.ewald_flags & PMGPU_EWALD_CORRECTION) {
+          prof_begin(s, PMGPU_PHASE_CORRECTION);
+          r = ewald_correction(s, &f, want_virial);
+          prof_end(s);
+          s->kernels += s->n_excl > 0;
+        }
         break;
       case FK_GB:
-        PM_CHECK(gb_forces(s, &f));
+        prof_begin(s, PMGPU_PHASE_GB);
+        r = gb_forces(s, &f);
+        prof_end(s);
+        s->kernels += 5;
         break;
       case FK_BONDED:
-        PM_CHECK(bonded_forces(s, &f, want_virial));
+        prof_begin(s, PMGPU_PHASE_BONDED);
+        r = bonded_forces(s, &f, want_virial);
+        prof_end(s);
+        s->kernels += (f.bonds && s->n_bonds > 0) + (f.angles && s->n_angles > 0);
         break;
       case FK_SIMPLEFULL:
-        PM_CHECK(nb_simplefull(s, f.sf_lj, f.sf_coul, want_virial));
+        prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
+        r = nb_simplefull(s, f.sf_lj, f.sf_coul, want_virial);
+        prof_end(s);
+        s->kernels += 1;
         break;
       default:
         break;
     }
+    PM_CHECK(r);
   }
   return PMGPU_OK;
 }
@@ -269,6 +350,23 @@ static int read_results(System *s, int only, double *energies, double *virial, i
   PM_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost,
                           s->stream));
   PM_CUDA(cudaStreamSynchronize(s->stream));
+  prof_collect(s);
+  int st = *s->h_status;
+  if (st) {
+    PM_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
+    if (st & ST_LIST_OVERFLOW) {
+      // Grow every list (fresh build next time); this result is incomplete
+      // and no output is touched.
+      for (auto &nl : s->lists) {
+        int cap = nl.cap * 2;
+        nb_list_free(&nl);
+        nl.cap = cap;
+        PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
+      }
+      return fail(PMGPU_ERR_OVERFLOW, "neighbour list capacity exceeded; capacity doubled");
+    }
+    if (st & ST_NONFINITE) return fail(PMGPU_ERR_NAN, "non-finite position or force");
+  }
   double e[PMGPU_E_COUNT], v[9];
   for (int k = 0; k < PMGPU_E_COUNT; k++) e[k] = (double)s->h_acc[k] / kEnergyScale;
   for (int k = 0; k < 9; k++) v[k] = (double)s->h_acc[ACC_VIRIAL + k] / kEnergyScale;
@@ -280,23 +378,19 @@ static int read_results(System *s, int only, double *energies, double *virial, i
     for (int k = 0; k < PMGPU_E_COUNT; k++) energies[k] = add ? energies[k] + e[k] : e[k];
   if (virial)
     for (int k = 0; k < 9; k++) virial[k] = add ? virial[k] + v[k] : v[k];
-  int st = *s->h_status;
-  if (st) {
-    PM_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
-    if (st & ST_LIST_OVERFLOW) {
-      // grow every list for the next call; this result is incomplete
-      for (auto &nl : s->lists) {
-        int cap = nl.cap * 2;
-        nb_list_free(&nl);
-        nl.cap = cap;
-        PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
-      }
-      return fail(PMGPU_ERR_OVERFLOW,
-                  "neighbour list capacity exceeded; capacity doubled, repeat the call");
-    }
-    if (st & ST_NONFINITE) return fail(PMGPU_ERR_NAN, "non-finite position or force");
-  }
   return PMGPU_OK;
+}
+
+// Runs fn() and, when a neighbour list overflowed (capacities are then
+// doubled by read_results), runs it again; at most three attempts.
+template <typename Fn>
+static int with_overflow_retry(Fn fn) {
+  int r = PMGPU_OK;
+  for (int attempt = 0; attempt < 3; attempt++) {
+    r = fn();
+    if (r != PMGPU_ERR_OVERFLOW) return r;
+  }
+  return r;
 }
 
 static int begin_eval(System *s) {
@@ -709,10 +803,12 @@ int pmgpu_evaluate(pmgpu_system *h, double *energies, double *virial) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
   PM_CUDA(cudaSetDevice(s->device));
-  PM_CHECK(zero_forces(s));
-  PM_CHECK(begin_eval(s));
-  PM_CHECK(evaluate_forces(s, -1, virial != nullptr, 0));
-  int r = read_results(s, -1, energies, virial, 0);
+  int r = with_overflow_retry([&]() {
+    PM_CHECK(zero_forces(s));
+    PM_CHECK(begin_eval(s));
+    PM_CHECK(evaluate_forces(s, -1, virial ? PAIR_VIRIAL : PAIR_ENERGY));
+    return read_results(s, -1, energies, virial, 0);
+  });
   s->forces_valid = (r == PMGPU_OK);
   return r;
 }
@@ -725,10 +821,12 @@ int pmgpu_force_evaluate(pmgpu_system *h, int id, const double *pos, double *for
   if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
   if (pos) PM_CHECK(copy_in(s, s->d_pos, pos));
   s->forces_valid = 0;
-  PM_CHECK(zero_forces(s));
-  PM_CHECK(begin_eval(s));
-  PM_CHECK(evaluate_forces(s, id, virial != nullptr, 0));
-  PM_CHECK(read_results(s, id, energies, virial, 1));
+  PM_CHECK(with_overflow_retry([&]() {
+    PM_CHECK(zero_forces(s));
+    PM_CHECK(begin_eval(s));
+    PM_CHECK(evaluate_forces(s, id, virial ? PAIR_VIRIAL : PAIR_ENERGY));
+    return read_results(s, id, energies, virial, 1);
+  }));
   if (forces) PM_CHECK(forces_to_host(s, forces, 1));
   return PMGPU_OK;
 }
@@ -747,23 +845,84 @@ int pmgpu_run(pmgpu_system *h, const pmgpu_integrator *it, long n_steps) {
   if (it->kind == PMGPU_INT_LANGEVIN_LEAPFROG && !(it->gamma_ps > 0))
     return fail(PMGPU_ERR_ARG, "LangevinLeapfrog needs gamma > 0");
   if (n_steps < 1) return PMGPU_OK;
-  if (!s->forces_valid) {
-    PM_CHECK(zero_forces(s));
-    PM_CHECK(begin_eval(s));
-    PM_CHECK(evaluate_forces(s, -1, 0, 0));
-  }
+  // A neighbour list that overflows mid-segment is only seen at the end of
+  // the segment (no host synchronisation per step): the segment then rolls
+  // back to this snapshot and runs again with the grown capacity.
+  size_t n3 = 3 * (size_t)std::max(1, s->n);
+  if (!s->d_snap) PM_CUDA(cudaMalloc(&s->d_snap, n3 * (2 * sizeof(double) + sizeof(long long))));
+  double *snap_pos = reinterpret_cast<double *>(s->d_snap);
+  double *snap_vel = snap_pos + n3;
+  long long *snap_f = reinterpret_cast<long long *>(snap_vel + n3);
+  const uint64_t step0 = s->step;
+  const int valid0 = s->forces_valid;
+  PM_CUDA(cudaMemcpyAsync(snap_pos, s->d_pos, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  PM_CUDA(cudaMemcpyAsync(snap_vel, s->d_vel, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  PM_CUDA(cudaMemcpyAsync(snap_f, s->d_force, n3 * sizeof(long long), cudaMemcpyDeviceToDevice, s->stream));
   bool lang = it->kind == PMGPU_INT_LANGEVIN_LEAPFROG;
-  for (long k = 0; k < n_steps; k++) {
-    int phase = lang ? (k == 0 ? 3 : 4) : (k == 0 ? 0 : 1);
-    PM_CHECK(integrate_kick_drift(s, it, phase));
-    s->step++;
-    PM_CHECK(begin_eval(s));
-    PM_CHECK(evaluate_forces(s, -1, 0, 0));
+  int r = PMGPU_OK;
+  for (int attempt = 0; attempt < 3; attempt++) {
+    if (attempt > 0) {
+      PM_CUDA(cudaMemcpyAsync(s->d_pos, snap_pos, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+      PM_CUDA(cudaMemcpyAsync(s->d_vel, snap_vel, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+      PM_CUDA(cudaMemcpyAsync(s->d_force, snap_f, n3 * sizeof(long long), cudaMemcpyDeviceToDevice, s->stream));
+      s->step = step0;
+      s->forces_valid = valid0;
+    }
+    if (!s->forces_valid) {
+      PM_CHECK(zero_forces(s));
+      PM_CHECK(begin_eval(s));
+      PM_CHECK(evaluate_forces(s, -1, PAIR_FORCE));
+    }
+    for (long k = 0; k < n_steps; k++) {
+      int phase = lang ? (k == 0 ? 3 : 4) : (k == 0 ? 0 : 1);
+      prof_begin(s, PMGPU_PHASE_INTEGRATE);
+      int ri = integrate_kick_drift(s, it, phase);
+      prof_end(s);
+      PM_CHECK(ri);
+      s->kernels += s->n > 0;
+      s->step++;
+      PM_CHECK(begin_eval(s));
+      PM_CHECK(evaluate_forces(s, -1, k + 1 == n_steps ? PAIR_ENERGY : PAIR_FORCE));
+    }
+    prof_begin(s, PMGPU_PHASE_INTEGRATE);
+    int ri = integrate_kick_drift(s, it, lang ? 5 : 2);
+    prof_end(s);
+    PM_CHECK(ri);
+    s->kernels += s->n > 0;
+    r = read_results(s, -1, nullptr, nullptr, 0);
+    if (r != PMGPU_ERR_OVERFLOW) break;
   }
-  PM_CHECK(integrate_kick_drift(s, it, lang ? 5 : 2));
-  int r = read_results(s, -1, nullptr, nullptr, 0);
   s->forces_valid = (r == PMGPU_OK);
   return r;
+}
+
+int pmgpu_profile_enable(pmgpu_system *h, int enabled) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  sysp(h)->prof.enabled = enabled ? 1 : 0;
+  return PMGPU_OK;
+}
+
+int pmgpu_profile_read(pmgpu_system *h, double *ms, long long *launches, int reset) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  PM_CUDA(cudaStreamSynchronize(s->stream));
+  prof_collect(s);
+  for (int k = 0; k < PMGPU_PHASE_COUNT; k++) {
+    if (ms) ms[k] = s->prof.ms[k];
+    if (launches) launches[k] = s->prof.launches[k];
+    if (reset) {
+      s->prof.ms[k] = 0;
+      s->prof.launches[k] = 0;
+    }
+  }
+  return PMGPU_OK;
+}
+
+int pmgpu_kernel_count(pmgpu_system *h, long long *count) {
+  if (!h || !count) return fail(PMGPU_ERR_ARG, "null argument");
+  *count = sysp(h)->kernels;
+  return PMGPU_OK;
 }
 
 int pmgpu_set_count_pairs(pmgpu_system *h, int enabled) {
@@ -826,7 +985,7 @@ int pmgpu_debug_pair_set(pmgpu_system *h, int id, int *pairs, long long cap,
   PM_CHECK(zero_forces(s));
   PM_CHECK(begin_eval(s));
   PM_CHECK(nb_prepare(s, &s->lists[f.list_index], 0));
-  PM_CHECK(nb_pair_forces(s, &s->lists[f.list_index], f.terms, 0, 1));
+  PM_CHECK(nb_pair_forces(s, &s->lists[f.list_index], f.terms, PAIR_RECORD));
   long long total = 0;
   PM_CUDA(cudaMemcpyAsync(&total, s->d_paircount, sizeof(long long), cudaMemcpyDeviceToHost,
                           s->stream));

@@ -297,286 +297,12 @@ __global__ void k_build_list(BuildArgs a, const int *__restrict__ rebuild,
   nbr_count[i] = count;
 }
 
+}  // namespace pmgpu
+
 // ---------------------------------------------------------- pair kernel
-template <typename Real>
-struct PairArgs {
-  Box box;
-  int n;
-  int ntypes;
-  int mask;
-  SwitchDev<Real> lj_sw, coul_sw;
-  int lj_modify, coul_modify;
-  // rough-test cutoffs^2 (FP64 exact and the FP32 band around them)
-  double lj_cut2, coul_cut2, ew_cut2;
-  Real lj_lo, lj_hi, coul_lo, coul_hi, ew_lo, ew_hi, max_hi;
-  Real alpha, a2pi;
-  int exact_erf;
-  Real csf;  // coulomb scaling factor
-  int cap;
-  const int *sorted;
-  const double *pos;     // raw positions (exact re-test)
-  const int *excl_start, *excl_partner, *excl_class;
-  const uint32_t *nbr;
-  const int *nbr_count;
-  const float4 *xhi, *xlo;
-  const double4 *xw;
-  const int *type;
-  const float4 *lj32;
-  const double4 *lj64;
-  long long *force;      // 3 planes
-  long long *acc;
-  long long *pairbuf;
-  long long pairbuf_cap;
-  long long *paircount;
-};
+#include "pair_kernel.cuh"
 
-__device__ __forceinline__ int excl_lookup(const int *start, const int *partner,
-                                           const int *cls, int oi, int oj) {
-  int b = start[oi], e = start[oi + 1];
-  for (int k = b; k < e; k++)
-    if (partner[k] == oj) return cls[k];
-  return PMGPU_EXCL_NONE;
-}
-
-// Exact FP64 squared distance of the image in hand, formed the way the
-// reference forms it: the minimal difference (PeriodicBoundaryConditions.h:
-// 72-110) plus a lattice vector (NonbondedFullEwaldSystemForce.h:790-805;
-// for orthogonal boxes lattice components are exactly e_c * k_c).  d is the
-// FP32/FP64 difference of the kernel, used only to pick the lattice vector.
-template <typename Real>
-__device__ __forceinline__ double exact_r2(const PairArgs<Real> &a, int oi, int oj,
-                                           double dx, double dy, double dz) {
-  double mx, my, mz;
-  double r2 = box_mindiff(a.box, a.pos[3 * oi], a.pos[3 * oi + 1], a.pos[3 * oi + 2],
-                          a.pos[3 * oj], a.pos[3 * oj + 1], a.pos[3 * oj + 2], mx, my, mz);
-  if (!a.box.periodic) return r2;
-  double kx = rint((dx - mx) * a.box.er[0]);
-  double ky = rint((dy - my) * a.box.er[1]);
-  double kz = rint((dz - mz) * a.box.er[2]);
-  if (kx == 0.0 && ky == 0.0 && kz == 0.0) return r2;
-  return xnorm2(xadd(mx, xmul(a.box.e[0], kx)), xadd(my, xmul(a.box.e[1], ky)),
-                xadd(mz, xmul(a.box.e[2], kz)));
-}
-
-template <typename Real>
-__device__ __forceinline__ Real fast_exp(Real x);
-template <>
-__device__ __forceinline__ float fast_exp<float>(float x) { return __expf(x); }
-template <>
-__device__ __forceinline__ double fast_exp<double>(double x) { return exp(x); }
-template <typename Real>
-__device__ __forceinline__ Real fast_rsqrt(Real x);
-template <>
-__device__ __forceinline__ float fast_rsqrt<float>(float x) { return rsqrtf(x); }
-template <>
-__device__ __forceinline__ double fast_rsqrt<double>(double x) { return 1.0 / sqrt(x); }
-
-// Thread per sorted atom i; walks its full neighbour list.  Each unordered
-// pair is visited from both ends: forces are written for i only (no
-// atomics on j), energies are halved.
-template <typename Real, int TERMS, bool VIRIAL, bool RECORD>
-__global__ void __launch_bounds__(128)
-k_pairs(PairArgs<Real> a) {
-  constexpr bool MIXED = sizeof(Real) == 4;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool valid = i < a.n;
-  int ii = valid ? i : 0;
-  int oi = a.sorted[ii];
-  double4 wi = a.xw[ii];
-  Real xs_h[3], xs_l[3], qi;
-  int ti;
-  if (MIXED) {
-    float4 h = a.xhi[ii], l = a.xlo[ii];
-    xs_h[0] = h.x; xs_h[1] = h.y; xs_h[2] = h.z; qi = h.w;
-    xs_l[0] = l.x; xs_l[1] = l.y; xs_l[2] = l.z; ti = __float_as_int(l.w);
-  } else {
-    xs_h[0] = wi.x; xs_h[1] = wi.y; xs_h[2] = wi.z; qi = wi.w;
-    xs_l[0] = xs_l[1] = xs_l[2] = Real(0);
-    ti = a.type[oi];
-  }
-  int cur_shift = kZeroShift;
-  Real fx = 0, fy = 0, fz = 0, elj = 0, ec = 0;
-  Real vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
-  int npairs = 0;
-  int cnt = valid ? a.nbr_count[ii] : 0;
-  for (int k = 0; k < cnt; k++) {
-    uint32_t e = a.nbr[(size_t)k * a.n + ii];
-    int j = (int)(e & kJMask);
-    int sh = (int)((e >> kShiftBits) & 31);
-    if (sh != cur_shift) {
-      // i coordinates moved by minus the j image shift: d = xj - (xi - s L)
-      int sx = sh / 9 - 1, sy = (sh / 3) % 3 - 1, sz = sh % 3 - 1;
-      double px = wi.x - sx * a.box.e[0], py = wi.y - sy * a.box.e[1],
-             pz = wi.z - sz * a.box.e[2];
-      if (MIXED) {
-        float hx = (float)px, hy = (float)py, hz = (float)pz;
-        xs_h[0] = hx; xs_h[1] = hy; xs_h[2] = hz;
-        xs_l[0] = (float)(px - hx); xs_l[1] = (float)(py - hy); xs_l[2] = (float)(pz - hz);
-      } else {
-        xs_h[0] = px; xs_h[1] = py; xs_h[2] = pz;
-      }
-      cur_shift = sh;
-    }
-    Real dx, dy, dz, qj;
-    int tj;
-    if (MIXED) {
-      float4 h = a.xhi[j], l = a.xlo[j];
-      dx = (h.x - xs_h[0]) + (l.x - xs_l[0]);
-      dy = (h.y - xs_h[1]) + (l.y - xs_l[1]);
-      dz = (h.z - xs_h[2]) + (l.z - xs_l[2]);
-      qj = h.w;
-      tj = __float_as_int(l.w);
-    } else {
-      double4 w = a.xw[j];
-      dx = w.x - xs_h[0];
-      dy = w.y - xs_h[1];
-      dz = w.z - xs_h[2];
-      qj = w.w;
-      tj = -1;
-    }
-    Real r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 > a.max_hi) continue;
-    int excl = PMGPU_EXCL_NONE;
-    int oj = -1;
-    if (e & kSameMolBit) {
-      oj = a.sorted[j];
-      excl = excl_lookup(a.excl_start, a.excl_partner, a.excl_class, oi, oj);
-    }
-    bool do_lj = false, do_coul = false, do_ew = false;
-    double r2x = -1.0;  // exact FP64 r^2 of this image, when needed
-    if (TERMS & TERM_LJ) {
-      if (r2 <= a.lj_lo) do_lj = true;
-      else if (r2 <= a.lj_hi) {
-        if (oj < 0) oj = a.sorted[j];
-        r2x = exact_r2(a, oi, oj, (double)dx, (double)dy, (double)dz);
-        do_lj = r2x <= a.lj_cut2;
-      }
-    }
-    if (TERMS & TERM_COUL) {
-      if (r2 <= a.coul_lo) do_coul = true;
-      else if (r2 <= a.coul_hi) {
-        if (oj < 0) oj = a.sorted[j];
-        if (r2x < 0) r2x = exact_r2(a, oi, oj, (double)dx, (double)dy, (double)dz);
-        do_coul = r2x <= a.coul_cut2;
-      }
-    }
-    if (TERMS & TERM_EWALD) {
-      if (r2 <= a.ew_lo) do_ew = true;
-      else if (r2 <= a.ew_hi) {
-        if (oj < 0) oj = a.sorted[j];
-        if (r2x < 0) r2x = exact_r2(a, oi, oj, (double)dx, (double)dy, (double)dz);
-        do_ew = r2x <= a.ew_cut2;
-      }
-    }
-    // FULL exclusions skip the pair (OneAtomPairTwo.h:47-53); in the
-    // Ewald real term they skip only the minimal image, which is the
-    // entry carrying the same-molecule bit (NonbondedFullEwald...h:795-801).
-    if (excl == PMGPU_EXCL_FULL) {
-      do_lj = false;
-      do_coul = false;
-      do_ew = false;
-    }
-    if (!(do_lj || do_coul || do_ew)) continue;
-    if (!MIXED) tj = a.type[a.sorted[j]];
-    Real rinv = fast_rsqrt<Real>(r2);
-    Real rinv2 = rinv * rinv;
-    Real f = 0;
-    if ((TERMS & TERM_LJ) && do_lj) {
-      Real A, B;
-      if (MIXED) {
-        float4 p = __ldg(&a.lj32[ti * a.ntypes + tj]);
-        A = excl == PMGPU_EXCL_MODIFIED ? p.z : p.x;
-        B = excl == PMGPU_EXCL_MODIFIED ? p.w : p.y;
-      } else {
-        double4 p = a.lj64[ti * a.ntypes + tj];
-        A = excl == PMGPU_EXCL_MODIFIED ? p.z : p.x;
-        B = excl == PMGPU_EXCL_MODIFIED ? p.w : p.y;
-      }
-      Real r6 = rinv2 * rinv2 * rinv2;
-      Real r6B = B * r6;
-      Real r12A = A * r6 * r6;
-      Real en = r12A - r6B;
-      Real ff = (Real(12) * r12A - Real(6) * r6B) * rinv2;
-      if (a.lj_modify) {
-        Real sv, sd;
-        switch_eval<Real>(a.lj_sw, r2, sv, sd);
-        ff = ff * sv - en * sd;
-        en = en * sv;
-      }
-      elj += en;
-      f += ff;
-    }
-    if ((TERMS & TERM_COUL) && do_coul) {
-      Real en = qi * qj * rinv;
-      if (excl == PMGPU_EXCL_MODIFIED) en *= a.csf;
-      Real ff = en * rinv2;
-      if (a.coul_modify) {
-        Real sv, sd;
-        switch_eval<Real>(a.coul_sw, r2, sv, sd);
-        ff = ff * sv - en * sd;
-        en = en * sv;
-      }
-      ec += en;
-      f += ff;
-    }
-    if ((TERMS & TERM_EWALD) && do_ew) {
-      Real qq = qi * qj;
-      if (excl == PMGPU_EXCL_MODIFIED) qq *= a.csf;
-      Real r = r2 * rinv;
-      Real ar = a.alpha * r;
-      Real ee = qq * fast_exp<Real>(-ar * ar);
-      Real en;
-      if (!a.exact_erf) {
-        en = poly5<Real>(ar) * ee * rinv;
-      } else {
-        en = qq * erfc(ar) * rinv;  // USE_EWALD_EXACT_ERF: libm erfc
-      }
-      Real ff = (en + a.a2pi * ee) * rinv2;
-      ec += en;
-      f += ff;
-    }
-    npairs++;
-    fx -= dx * f;
-    fy -= dy * f;
-    fz -= dz * f;
-    if (VIRIAL) {
-      // addVirial(fij, d) with fij = d * f, half per visit
-      Real hf = Real(0.5) * f;
-      vxx += dx * dx * hf; vxy += dx * dy * hf; vxz += dx * dz * hf;
-      vyy += dy * dy * hf; vyz += dy * dz * hf; vzz += dz * dz * hf;
-    }
-    if (RECORD) {
-      if (oj < 0) oj = a.sorted[j];
-      if (oi < oj) {
-        long long slot = atomicAdd((unsigned long long *)a.paircount, 1ull);
-        if (slot < a.pairbuf_cap) a.pairbuf[slot] = ((long long)oi << 32) | (unsigned)oj;
-      }
-    }
-  }
-  if (valid) {
-    red_add(&a.force[oi], to_fixed((double)fx, kForceScale));
-    red_add(&a.force[a.n + oi], to_fixed((double)fy, kForceScale));
-    red_add(&a.force[2 * a.n + oi], to_fixed((double)fz, kForceScale));
-  }
-  double dlj = warp_sum((double)elj) * 0.5;
-  double dc = warp_sum((double)ec) * 0.5;
-  int np = warp_sum(npairs);
-  double v[6];
-  if (VIRIAL) {
-    v[0] = warp_sum((double)vxx); v[1] = warp_sum((double)vxy);
-    v[2] = warp_sum((double)vxz); v[3] = warp_sum((double)vyy);
-    v[4] = warp_sum((double)vyz); v[5] = warp_sum((double)vzz);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (TERMS & TERM_LJ) red_add(&a.acc[ACC_LJ], to_fixed(dlj, kEnergyScale));
-    if (TERMS & (TERM_COUL | TERM_EWALD)) red_add(&a.acc[ACC_COULOMB], to_fixed(dc, kEnergyScale));
-    red_add(&a.acc[ACC_PAIRS], (long long)np);
-    if (VIRIAL) {
-      const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
-      for (int q = 0; q < 9; q++) red_add(&a.acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
-    }
-  }
-}
+namespace pmgpu {
 
 // ------------------------------------------------------------ host side
 int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double) {
@@ -627,7 +353,9 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   // capacity: expected neighbours in the reach sphere at the mean density,
   // with headroom for local fluctuations (overflow is detected and
   // reported, and the next call doubles the capacity).
-  double dens = b.periodic ? n / b.V : 0.15;
+  // Condensed matter (liquid water ~0.1 atoms/A^3) bounds the local
+  // density even in sparse boxes, where atoms still cluster.
+  double dens = b.periodic ? std::max(n / b.V, 0.12) : 0.15;
   double expect = 4.18879 * nl->reach * nl->reach * nl->reach * dens;
   int cap = (int)(expect * 1.5 + 64);
   cap = std::min(cap, std::max(32, n));
@@ -740,6 +468,8 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   a.mask = t.mask;
   a.lj_sw = make_switch_dev<Real>(t.lj_sw);
   a.coul_sw = make_switch_dev<Real>(t.coul_sw);
+  a.lj_sw64 = make_switch_dev<double>(t.lj_sw);
+  a.coul_sw64 = make_switch_dev<double>(t.coul_sw);
   a.lj_modify = t.lj_sw.modify;
   a.coul_modify = t.coul_sw.modify;
   // The FP32 squared distance is within ~1e-5 A^2 of the exact one; pairs
@@ -761,8 +491,11 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   a.max_hi = (Real)(mx * (1 + band));
   a.alpha = (Real)t.ewald_alpha;
   a.a2pi = (Real)(2.0 * t.ewald_alpha / std::sqrt(M_PI));
+  a.alpha64 = t.ewald_alpha;
+  a.a2pi64 = 2.0 * t.ewald_alpha / std::sqrt(M_PI);
   a.exact_erf = t.exact_erf;
   a.csf = (Real)t.coulomb_scaling;
+  a.csf64 = t.coulomb_scaling;
   a.cap = nl->cap;
   a.sorted = nl->d_sorted;
   a.pos = s->d_pos;
@@ -785,26 +518,24 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
 }
 
 template <typename Real, int TERMS>
-static void launch_pairs_t(PairArgs<Real> &a, cudaStream_t st, int virial, int record) {
+static void launch_pairs_t(PairArgs<Real> &a, cudaStream_t st, int mode) {
   int nb = (a.n + 127) / 128;
-  if (record)
-    k_pairs<Real, TERMS, false, true><<<nb, 128, 0, st>>>(a);
-  else if (virial)
-    k_pairs<Real, TERMS, true, false><<<nb, 128, 0, st>>>(a);
-  else
-    k_pairs<Real, TERMS, false, false><<<nb, 128, 0, st>>>(a);
+  switch (mode) {
+    case PAIR_FORCE: k_pairs<Real, TERMS, PAIR_FORCE><<<nb, 128, 0, st>>>(a); break;
+    case PAIR_ENERGY: k_pairs<Real, TERMS, PAIR_ENERGY><<<nb, 128, 0, st>>>(a); break;
+    case PAIR_VIRIAL: k_pairs<Real, TERMS, PAIR_VIRIAL><<<nb, 128, 0, st>>>(a); break;
+    default: k_pairs<Real, TERMS, PAIR_RECORD><<<nb, 128, 0, st>>>(a); break;
+  }
 }
 
 template <typename Real>
-static int launch_pairs(PairArgs<Real> &a, cudaStream_t st, int virial, int record) {
+static int launch_pairs(PairArgs<Real> &a, cudaStream_t st, int mode) {
   switch (a.mask) {
-    case TERM_LJ: launch_pairs_t<Real, TERM_LJ>(a, st, virial, record); break;
-    case TERM_COUL: launch_pairs_t<Real, TERM_COUL>(a, st, virial, record); break;
-    case TERM_LJ | TERM_COUL:
-      launch_pairs_t<Real, TERM_LJ | TERM_COUL>(a, st, virial, record); break;
-    case TERM_EWALD: launch_pairs_t<Real, TERM_EWALD>(a, st, virial, record); break;
-    case TERM_LJ | TERM_EWALD:
-      launch_pairs_t<Real, TERM_LJ | TERM_EWALD>(a, st, virial, record); break;
+    case TERM_LJ: launch_pairs_t<Real, TERM_LJ>(a, st, mode); break;
+    case TERM_COUL: launch_pairs_t<Real, TERM_COUL>(a, st, mode); break;
+    case TERM_LJ | TERM_COUL: launch_pairs_t<Real, TERM_LJ | TERM_COUL>(a, st, mode); break;
+    case TERM_EWALD: launch_pairs_t<Real, TERM_EWALD>(a, st, mode); break;
+    case TERM_LJ | TERM_EWALD: launch_pairs_t<Real, TERM_LJ | TERM_EWALD>(a, st, mode); break;
     default:
       return fail(PMGPU_ERR_UNSUPPORTED, "unsupported pair-term combination");
   }
@@ -812,17 +543,18 @@ static int launch_pairs(PairArgs<Real> &a, cudaStream_t st, int virial, int reco
   return PMGPU_OK;
 }
 
-int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int want_virial,
-                   int record_pairs) {
+// mode: PAIR_FORCE (forces only), PAIR_ENERGY (+ FP64 energies),
+// PAIR_VIRIAL (+ virial), PAIR_RECORD (+ pair-set recording).
+int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode) {
   if (s->n == 0) return PMGPU_OK;
   if (s->precision == PMGPU_PREC_MIXED) {
     PairArgs<float> a;
     fill_pair_args<float>(a, s, nl, t);
-    return launch_pairs<float>(a, s->stream, want_virial, record_pairs);
+    return launch_pairs<float>(a, s->stream, mode);
   }
   PairArgs<double> a;
   fill_pair_args<double>(a, s, nl, t);
-  return launch_pairs<double>(a, s->stream, want_virial, record_pairs);
+  return launch_pairs<double>(a, s->stream, mode);
 }
 
 // ProtoMol cell assignment with a given cellsize on the resident positions

@@ -156,8 +156,13 @@ __device__ __forceinline__ void switch_eval(const SwitchDev<Real> &w, Real r2,
       }
       Real sq = pm_sqrt(r2);
       Real sd = sq - w.cutoff;
-      Real c = Real(1);
-      for (int i = 0; i < w.ord_int; i++) c *= sd;  // c[0] = sd^ordInt
+      Real c;  // c[0] = sd^ordInt
+      if (sizeof(Real) == 8) {
+        c = (Real)pow((double)sd, (double)w.ord_int);
+      } else {
+        c = Real(1);
+        for (int i = 0; i < w.ord_int; i++) c *= sd;
+      }
       for (int i = 0; i < w.ord_int + 1; i++) {
         Real cn = c * sd;                            // c[i+1]
         val += (Real)c_cn_sw[w.ord_idx][i] * cn * w.irange[i];

@@ -87,6 +87,9 @@ struct SwitchParams {
 
 // Pair-term selection for the fused pair kernel.
 enum { TERM_LJ = 1, TERM_COUL = 2, TERM_EWALD = 4 };
+// What a pair-kernel launch produces: forces only (inner MD steps),
+// forces + FP64 energies, + virial, or + the recorded pair set.
+enum { PAIR_FORCE = 0, PAIR_ENERGY = 1, PAIR_VIRIAL = 2, PAIR_RECORD = 3 };
 
 struct PairTerms {
   int mask;                 // TERM_*
@@ -161,8 +164,26 @@ struct Force {
 enum { FK_CUTOFF = 1, FK_PME = 2, FK_GB = 3, FK_BONDED = 4,
        FK_SIMPLEFULL = 5 };
 
+// Per-phase CUDA-event timing; events are recorded only when enabled and
+// summed at the next host synchronisation.
+struct Profiler {
+  int enabled = 0;
+  struct Mark { int phase; cudaEvent_t a, b; };
+  std::vector<Mark> pending;
+  std::vector<cudaEvent_t> pool;
+  double ms[PMGPU_PHASE_COUNT] = {0};
+  long long launches[PMGPU_PHASE_COUNT] = {0};
+  int open_phase = -1;
+  cudaEvent_t open_ev = nullptr;
+};
+void prof_begin(struct System *s, int phase);
+void prof_end(struct System *s);
+void prof_collect(struct System *s);
+
 struct System {
   pmgpu_context *ctx = nullptr;
+  Profiler prof;
+  long long kernels = 0;  // own kernel launches (see pmgpu_kernel_count)
   int device = 0;
   int n = 0;
   int precision = PMGPU_PREC_MIXED;
@@ -211,6 +232,7 @@ struct System {
   double last_energy[PMGPU_E_COUNT] = {0, 0, 0, 0, 0, 0, 0};
   double last_virial[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   double *d_stage = nullptr;       // 3n device staging
+  void *d_snap = nullptr;          // run() rollback snapshot (pos, vel, force)
   double *h_stage = nullptr;       // 3n pinned host staging
   long long *d_pairbuf = nullptr;  // debug pair-set buffer
   long long pairbuf_cap = 0;
@@ -226,8 +248,7 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin,
                  double cellsize_for_debug);
 int nb_list_free(NeighborList *nl);
 int nb_prepare(System *s, NeighborList *nl, int force_rebuild);
-int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t,
-                   int want_virial, int record_pairs);
+int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode);
 int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
 int nb_simplefull(System *s, int lj, int coul, int want_virial);
 

@@ -172,6 +172,14 @@ class GpuSystem:
         L.check(self.lib.pmgpu_evaluate(self.h, L.ptr(e), L.ptr(v)))
         return e, (v.reshape(3, 3) if v is not None else None)
 
+    def energies(self):
+        """(energies[7], virial[3,3]) of the last evaluation or run segment,
+        without evaluating again."""
+        e = np.zeros(L.E_COUNT)
+        v = np.zeros(9)
+        L.check(self.lib.pmgpu_system_get_energies(self.h, L.ptr(e), L.ptr(v)))
+        return e, v.reshape(3, 3)
+
     def stream(self) -> int:
         return self.lib.pmgpu_system_stream(self.h)
 
@@ -179,6 +187,21 @@ class GpuSystem:
         p, v, f = C.c_void_p(), C.c_void_p(), C.c_void_p()
         L.check(self.lib.pmgpu_system_device_state(self.h, C.byref(p), C.byref(v), C.byref(f)))
         return p.value, v.value, f.value
+
+    def profile(self, enable: bool | None = None, reset: bool = False) -> dict:
+        """Per-phase device time (ms) and launch counts since the last reset
+        (CUDA events inside the library); optionally switch profiling."""
+        if enable is not None:
+            L.check(self.lib.pmgpu_profile_enable(self.h, 1 if enable else 0))
+        ms = np.zeros(len(L.PHASES))
+        ln = np.zeros(len(L.PHASES), np.int64)
+        L.check(self.lib.pmgpu_profile_read(self.h, L.ptr(ms), L.ptr(ln), 1 if reset else 0))
+        return {p: (float(ms[k]), int(ln[k])) for k, p in enumerate(L.PHASES)}
+
+    def kernel_count(self) -> int:
+        c = C.c_longlong()
+        L.check(self.lib.pmgpu_kernel_count(self.h, C.byref(c)))
+        return int(c.value)
 
     def cell_assign(self, cellsize: float):
         cells = np.zeros((self.n, 3), np.int32)

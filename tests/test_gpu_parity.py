@@ -4,7 +4,7 @@ ProtoMol reference's own outputs (golden fixtures) and the FP64 oracle.
 Tolerances (stated per the FP32-pair / FP64-accumulate design):
   * mixed precision: RMS relative force error <= 1e-5 per force term,
     energy relative error <= 1e-6 (abs floor 1e-4 kcal/mol);
-  * double precision ("FP64 throughout"): RMS relative force error <= 1e-9;
+  * double precision ("FP64 throughout"): RMS relative force error <= 1e-8;
   * the cutoff pair set and the cell assignment are bit-exact.
 """
 import numpy as np
@@ -18,7 +18,7 @@ from protomol_b200 import (ForceFactory, GpuSystem, LangevinLeapfrogIntegrator,
 pytestmark = pytest.mark.gpu
 
 RMS_MIXED = 1e-5
-RMS_DOUBLE = 1e-9
+RMS_DOUBLE = 1e-8
 E_REL = 1e-6
 
 
