@@ -164,7 +164,9 @@ static int system_free(System *s) {
                   s->d_gb_vdwr, s->d_gb_scale, s->d_gb_offset, s->d_water, s->d_gb_born,
                   s->d_gb_psi, s->d_gb_partial, s->d_gb_fixed, s->d_pos, s->d_vel,
                   s->d_force, s->d_acc, s->d_status, s->d_pairbuf, s->d_paircount,
-                  s->d_stage, s->d_snap};
+                  s->d_stage, s->d_snap, s->d_step};
+  for (auto &g : s->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->h_acc) cudaFreeHost(s->h_acc);
@@ -362,6 +364,7 @@ static int read_results(System *s, int only, double *energies, double *virial, i
         nb_list_free(&nl);
         nl.cap = cap;
         PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
+        s->graph_version++;  // captured graphs hold the old list buffers
       }
       return fail(PMGPU_ERR_OVERFLOW, "neighbour list capacity exceeded; capacity doubled");
     }
@@ -527,6 +530,7 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   PM_CHECK(upload(&s->d_force, (const long long *)nullptr, 3 * nn));
   PM_CHECK(upload(&s->d_acc, (const long long *)nullptr, ACC_COUNT));
   PM_CHECK(upload(&s->d_status, (const int *)nullptr, 1));
+  PM_CHECK(upload(&s->d_step, (const unsigned long long *)nullptr, 1));
   PM_CHECK(upload(&s->d_stage, (const double *)nullptr, 3 * nn));
   PM_CUDA(cudaMallocHost(&s->h_acc, sizeof(long long) * ACC_COUNT));
   PM_CUDA(cudaMallocHost(&s->h_status, sizeof(int)));
@@ -640,6 +644,7 @@ static int add_force(System *s, Force &f, int *force_id) {
   s->forces.push_back(f);
   if (force_id) *force_id = f.id;
   s->forces_valid = 0;
+  s->graph_version++;
   return PMGPU_OK;
 }
 
@@ -795,6 +800,7 @@ int pmgpu_force_set_enabled(pmgpu_system *h, int id, int enabled) {
   System *s = sysp(h);
   if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
   s->forces[id].enabled = enabled ? 1 : 0;
+  s->graph_version++;
   s->forces_valid = 0;
   return PMGPU_OK;
 }
@@ -828,6 +834,65 @@ int pmgpu_force_evaluate(pmgpu_system *h, int id, const double *pos, double *for
     return read_results(s, id, energies, virial, 1);
   }));
   if (forces) PM_CHECK(forces_to_host(s, forces, 1));
+  return PMGPU_OK;
+}
+
+// One MD step body: kick + drift (+ device step counter), then the force
+// evaluation at the new positions.
+static int one_step(System *s, const pmgpu_integrator *it, int phase, int mode) {
+  prof_begin(s, PMGPU_PHASE_INTEGRATE);
+  int ri = integrate_kick_drift(s, it, phase);
+  prof_end(s);
+  PM_CHECK(ri);
+  s->kernels += (s->n > 0) + 1;  // update + step counter
+  PM_CHECK(begin_eval(s));
+  return evaluate_forces(s, -1, mode);
+}
+
+static bool same_integrator(const pmgpu_integrator &a, const pmgpu_integrator &b) {
+  return a.kind == b.kind && a.timestep_fs == b.timestep_fs &&
+         a.temperature == b.temperature && a.gamma_ps == b.gamma_ps && a.seed == b.seed;
+}
+
+// Replays (capturing on first use) a CUDA graph of g inner steps.  *used is
+// 0 when capture is not possible, in which case the caller runs eagerly.
+static int run_graph(System *s, const pmgpu_integrator *it, long g, int *used) {
+  *used = 0;
+  System::StepGraph &sg = s->graphs[g == 1 ? 1 : 0];
+  const int phase = it->kind == PMGPU_INT_LANGEVIN_LEAPFROG ? 4 : 1;
+  if (!(sg.exec && sg.version == s->graph_version && sg.steps == g &&
+        same_integrator(sg.key, *it))) {
+    if (sg.exec) cudaGraphExecDestroy(sg.exec);
+    sg.exec = nullptr;
+    long long k0 = s->kernels;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      s->graphs_disabled = 1;
+      return PMGPU_OK;
+    }
+    int r = PMGPU_OK;
+    for (long k = 0; k < g && r == PMGPU_OK; k++) r = one_step(s, it, phase, PAIR_FORCE);
+    cudaError_t ec = cudaStreamEndCapture(s->stream, &graph);
+    const long long per_launch = s->kernels - k0;
+    s->kernels = k0;
+    if (r != PMGPU_OK || ec != cudaSuccess || !graph ||
+        cudaGraphInstantiate(&sg.exec, graph, 0) != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      sg.exec = nullptr;
+      s->graphs_disabled = 1;  // fall back to eager launches from now on
+      return PMGPU_OK;
+    }
+    cudaGraphDestroy(graph);
+    sg.version = s->graph_version;
+    sg.steps = g;
+    sg.key = *it;
+    sg.kernels = per_launch;
+  }
+  PM_CUDA(cudaGraphLaunch(sg.exec, s->stream));
+  s->kernels += sg.kernels;
+  *used = 1;
   return PMGPU_OK;
 }
 
@@ -868,21 +933,30 @@ int pmgpu_run(pmgpu_system *h, const pmgpu_integrator *it, long n_steps) {
       s->step = step0;
       s->forces_valid = valid0;
     }
+    PM_CHECK(set_device_step(s));
     if (!s->forces_valid) {
       PM_CHECK(zero_forces(s));
       PM_CHECK(begin_eval(s));
       PM_CHECK(evaluate_forces(s, -1, PAIR_FORCE));
     }
-    for (long k = 0; k < n_steps; k++) {
+    for (long k = 0; k < n_steps;) {
+      // Inner steps (not the first, not the last) replay a captured graph
+      // of several steps when possible; the rest run eagerly.
+      const long inner_left = (n_steps - 1) - k;
+      if (k > 0 && inner_left > 0 && !s->prof.enabled && !s->graphs_disabled) {
+        const long g = inner_left >= kGraphSteps ? kGraphSteps : 1;
+        int used = 0;
+        PM_CHECK(run_graph(s, it, g, &used));
+        if (used) {
+          s->step += g;
+          k += g;
+          continue;
+        }
+      }
       int phase = lang ? (k == 0 ? 3 : 4) : (k == 0 ? 0 : 1);
-      prof_begin(s, PMGPU_PHASE_INTEGRATE);
-      int ri = integrate_kick_drift(s, it, phase);
-      prof_end(s);
-      PM_CHECK(ri);
-      s->kernels += s->n > 0;
+      PM_CHECK(one_step(s, it, phase, k + 1 == n_steps ? PAIR_ENERGY : PAIR_FORCE));
       s->step++;
-      PM_CHECK(begin_eval(s));
-      PM_CHECK(evaluate_forces(s, -1, k + 1 == n_steps ? PAIR_ENERGY : PAIR_FORCE));
+      k++;
     }
     prof_begin(s, PMGPU_PHASE_INTEGRATE);
     int ri = integrate_kick_drift(s, it, lang ? 5 : 2);

@@ -191,9 +191,22 @@ struct UpdateArgs {
   // Langevin (LangevinLeapfrogIntegrator.cpp:44-71)
   double vdt, fdt, ndt, fc;
   uint64_t seed;
-  uint64_t kstep[2];  // (step, half) of each kick's noise
+  // (step, half) of each kick's noise: step = *step_ptr + kstep_off[k].  The
+  // step counter lives in device memory so captured graphs stay valid.
+  const unsigned long long *step_ptr;
+  int kstep_off[2];
   int khalf[2];
 };
+
+// Advances the device step counter (after the drift of a step).
+__global__ void k_step_inc(unsigned long long *step) { *step += 1ull; }
+__global__ void k_step_set(unsigned long long *step, unsigned long long v) { *step = v; }
+
+int set_device_step(System *s) {
+  k_step_set<<<1, 1, 0, s->stream>>>(s->d_step, (unsigned long long)s->step);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
 
 __global__ void k_update(UpdateArgs a, const double *__restrict__ mass,
                          double *__restrict__ pos, double *__restrict__ vel,
@@ -207,7 +220,7 @@ __global__ void k_update(UpdateArgs a, const double *__restrict__ mass,
   for (int k = 0; k < a.kicks; k++) {
     if (a.langevin) {
       double g[3];
-      gauss3(a.seed, a.kstep[k], a.khalf[k], i, g);
+      gauss3(a.seed, *a.step_ptr + (long long)a.kstep_off[k], a.khalf[k], i, g);
       double sq = sqrt(a.fc / m);
       for (int c = 0; c < 3; c++)
         v[c] = xadd(xadd(xmul(v[c], a.vdt), xmul(F[c], a.fdt) / m), xmul(xmul(g[c], sq), a.ndt));
@@ -240,9 +253,9 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase) {
   a.seed = it->seed;
   // StandardIntegrator::run gives every step two half kicks; the noise of
   // kick (step, half) is Philox(seed; atom, step, half).
-  uint64_t st = s->step;
-  a.kstep[0] = st; a.khalf[0] = 0;
-  a.kstep[1] = st; a.khalf[1] = 0;
+  a.step_ptr = s->d_step;
+  a.kstep_off[0] = 0; a.khalf[0] = 0;
+  a.kstep_off[1] = 0; a.khalf[1] = 0;
   a.vdt = a.fdt = a.ndt = a.fc = 0;
   if (a.langevin) {
     double gamma = it->gamma_ps / (1000 * kInvTimeFactor);
@@ -261,17 +274,18 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase) {
       break;
     case 4:  // second half kick of step st-1, first half kick of step st
       a.kicks = 2; a.coef = 0; a.drift = 1; a.zero_force = 1;
-      a.kstep[0] = st - 1; a.khalf[0] = 1;
+      a.kstep_off[0] = -1; a.khalf[0] = 1;
       break;
     case 5:  // second half kick of step st-1
       a.kicks = 1; a.coef = 0; a.drift = 0; a.zero_force = 0;
-      a.kstep[0] = st - 1; a.khalf[0] = 1;
+      a.kstep_off[0] = -1; a.khalf[0] = 1;
       break;
     default: return fail(PMGPU_ERR_ARG, "bad integrator phase");
   }
   if (s->n)
     k_update<<<(s->n + 255) / 256, 256, 0, s->stream>>>(a, s->d_mass, s->d_pos, s->d_vel,
                                                         s->d_force, s->d_status);
+  if (a.drift) k_step_inc<<<1, 1, 0, s->stream>>>(s->d_step);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }

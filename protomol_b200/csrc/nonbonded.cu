@@ -13,6 +13,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <cooperative_groups.h>
+
 #include "pm_device.cuh"
 
 namespace pmgpu {
@@ -226,24 +228,34 @@ struct BuildArgs {
   int periodic;
 };
 
-__global__ void k_build_list(BuildArgs a, const int *__restrict__ rebuild,
-                             const int *__restrict__ key, const int *__restrict__ sorted,
-                             const int *__restrict__ start, const double4 *__restrict__ xw,
-                             const int *__restrict__ mol, uint32_t *__restrict__ nbr,
-                             int *__restrict__ nbr_count, int *__restrict__ status) {
+// kBuildLanes lanes per atom scan the 27 neighbour cells; candidates are
+// tested in FP32 against (reach + margin)^2 and compacted with a tile ballot,
+// so every row is written in a fixed (cell, index) order.
+__global__ void __launch_bounds__(128)
+k_build_list(BuildArgs a, const int *__restrict__ rebuild, const int *__restrict__ key,
+             const int *__restrict__ sorted, const int *__restrict__ start,
+             const double4 *__restrict__ xw, const int *__restrict__ mol,
+             uint32_t *__restrict__ nbr, int *__restrict__ nbr_count,
+             int *__restrict__ status) {
   if (!*rebuild) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n) return;
-  int oi = sorted[i];
-  double4 pi = xw[i];
-  int mi = mol[oi];
-  int cell = key[oi] / kFine3;
-  int cz = cell % a.ncz, cy = (cell / a.ncz) % a.ncy, cx = cell / (a.ncz * a.ncy);
+  namespace cg = cooperative_groups;
+  auto tile = cg::tiled_partition<kBuildLanes>(cg::this_thread_block());
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = tile.thread_rank();
+  const int i = gt / kBuildLanes;
+  if (i >= a.n) return;  // whole tiles exit together
+  const int oi = sorted[i];
+  const double4 pi = xw[i];
+  const int mi = mol[oi];
+  const int cell = key[oi] / kFine3;
+  const int cz = cell % a.ncz, cy = (cell / a.ncz) % a.ncy, cx = cell / (a.ncz * a.ncy);
+  const int dims[3] = {a.ncx, a.ncy, a.ncz};
+  const float reach2 = (float)a.reach2;
+  uint32_t *row = nbr + (size_t)i * a.cap;
   int count = 0;
-  int dims[3] = {a.ncx, a.ncy, a.ncz};
-  // In a non-periodic box, cells beyond the grid do not exist; in a
-  // periodic box with fewer than 3 cells per axis the same cell is visited
-  // under different images, which is what the Ewald image sum needs.
+  // With one or two cells on an axis the -1/0/+1 neighbours name the same
+  // cells under different images; every (cell, image) pair is distinct and
+  // the box edge exceeds the reach, so no pair appears twice under one image.
   for (int ddx = -1; ddx <= 1; ddx++) {
     int nx = cx + ddx, sx = 0;
     if (a.periodic) {
@@ -262,39 +274,49 @@ __global__ void k_build_list(BuildArgs a, const int *__restrict__ rebuild,
           if (nz < 0) { nz += dims[2]; sz = -1; }
           else if (nz >= dims[2]) { nz -= dims[2]; sz = 1; }
         } else if (nz < 0 || nz >= dims[2]) continue;
-        // With one or two cells on an axis the -1/0/+1 neighbours name the
-        // same cells under different images; every (cell, image) pair is
-        // still distinct, and the box edge exceeds the reach, so no pair
-        // is visited twice under the same image.
-        int shift = (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1);
-        double ox = sx * a.box.e[0], oy = sy * a.box.e[1], oz = sz * a.box.e[2];
-        int c2 = (nx * dims[1] + ny) * dims[2] + nz;
-        int jb = start[c2 * kFine3], je = start[c2 * kFine3 + kFine3];
-        for (int j = jb; j < je; j++) {
-          if (j == i && shift == kZeroShift) continue;
-          double4 pj = xw[j];
-          double dx = (pj.x + ox) - pi.x, dy = (pj.y + oy) - pi.y, dz = (pj.z + oz) - pi.z;
-          double r2 = dx * dx + dy * dy + dz * dz;
-          if (r2 >= a.reach2) continue;
-          uint32_t e = (uint32_t)j | ((uint32_t)shift << kShiftBits);
-          int oj = sorted[j];
-          if (mol[oj] == mi) {
-            bool minimal = !a.periodic ||
-                           (fabs(dx) <= a.box.H2[0] && fabs(dy) <= a.box.H2[1] &&
-                            fabs(dz) <= a.box.H2[2]);
-            if (minimal) e |= kSameMolBit;
+        const int shift = (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1);
+        const float ox = (float)(pi.x - sx * a.box.e[0]);
+        const float oy = (float)(pi.y - sy * a.box.e[1]);
+        const float oz = (float)(pi.z - sz * a.box.e[2]);
+        const int c2 = (nx * dims[1] + ny) * dims[2] + nz;
+        const int jb = start[c2 * kFine3], je = start[c2 * kFine3 + kFine3];
+        for (int j0 = jb; j0 < je; j0 += kBuildLanes) {
+          const int j = j0 + lane;
+          bool pass = false;
+          float dx = 0.f, dy = 0.f, dz = 0.f;
+          if (j < je && !(j == i && shift == kZeroShift)) {
+            const double4 pj = xw[j];
+            dx = (float)pj.x - ox;
+            dy = (float)pj.y - oy;
+            dz = (float)pj.z - oz;
+            pass = dx * dx + dy * dy + dz * dz < reach2;
           }
-          if (count < a.cap) nbr[(size_t)count * a.n + i] = e;
-          count++;
+          const unsigned m = tile.ballot(pass);
+          if (pass) {
+            const int slot = count + __popc(m & ((1u << lane) - 1u));
+            uint32_t e = (uint32_t)j | ((uint32_t)shift << kShiftBits);
+            const int oj = sorted[j];
+            if (mol[oj] == mi) {
+              const bool minimal = !a.periodic ||
+                                   (fabsf(dx) <= (float)a.box.H2[0] &&
+                                    fabsf(dy) <= (float)a.box.H2[1] &&
+                                    fabsf(dz) <= (float)a.box.H2[2]);
+              if (minimal) e |= kSameMolBit;
+            }
+            if (slot < a.cap) row[slot] = e;
+          }
+          count += __popc(m);
         }
       }
     }
   }
-  if (count > a.cap) {
-    atomicOr(status, ST_LIST_OVERFLOW);
-    count = a.cap;
+  if (lane == 0) {
+    if (count > a.cap) {
+      atomicOr(status, ST_LIST_OVERFLOW);
+      count = a.cap;
+    }
+    nbr_count[i] = count;
   }
-  nbr_count[i] = count;
 }
 
 }  // namespace pmgpu
@@ -447,10 +469,11 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
   ba.box = s->box;
   ba.n = n;
   ba.ncx = nl->ncx; ba.ncy = nl->ncy; ba.ncz = nl->ncz;
-  ba.reach2 = nl->reach * nl->reach;
+  // FP32 candidate test with a margin well above its rounding error
+  ba.reach2 = (nl->reach + 0.01) * (nl->reach + 0.01);
   ba.cap = nl->cap;
   ba.periodic = s->box.periodic;
-  k_build_list<<<(n + 127) / 128, 128, 0, st>>>(ba, nl->d_rebuild, nl->d_key,
+  k_build_list<<<(int)(((long long)n * kBuildLanes + 127) / 128), 128, 0, st>>>(ba, nl->d_rebuild, nl->d_key,
                                                 nl->d_sorted, nl->d_key_start, nl->d_xw,
                                                 s->d_mol, nl->d_nbr, nl->d_nbr_count,
                                                 s->d_status);
@@ -519,12 +542,13 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
 
 template <typename Real, int TERMS>
 static void launch_pairs_t(PairArgs<Real> &a, cudaStream_t st, int mode) {
-  int nb = (a.n + 127) / 128;
+  constexpr int TPA = kPairLanes;
+  int nb = (int)(((long long)a.n * TPA + 127) / 128);
   switch (mode) {
-    case PAIR_FORCE: k_pairs<Real, TERMS, PAIR_FORCE><<<nb, 128, 0, st>>>(a); break;
-    case PAIR_ENERGY: k_pairs<Real, TERMS, PAIR_ENERGY><<<nb, 128, 0, st>>>(a); break;
-    case PAIR_VIRIAL: k_pairs<Real, TERMS, PAIR_VIRIAL><<<nb, 128, 0, st>>>(a); break;
-    default: k_pairs<Real, TERMS, PAIR_RECORD><<<nb, 128, 0, st>>>(a); break;
+    case PAIR_FORCE: k_pairs<Real, TERMS, PAIR_FORCE, TPA><<<nb, 128, 0, st>>>(a); break;
+    case PAIR_ENERGY: k_pairs<Real, TERMS, PAIR_ENERGY, TPA><<<nb, 128, 0, st>>>(a); break;
+    case PAIR_VIRIAL: k_pairs<Real, TERMS, PAIR_VIRIAL, TPA><<<nb, 128, 0, st>>>(a); break;
+    default: k_pairs<Real, TERMS, PAIR_RECORD, TPA><<<nb, 128, 0, st>>>(a); break;
   }
 }
 

@@ -115,13 +115,19 @@ __device__ __forceinline__ void apply_switch(const SwitchDev<Real> &sw,
 // Thread per sorted atom i; walks its full neighbour list.  Each unordered
 // pair is visited from both ends: forces are written for i only (no atomics
 // on j), energies and virial are halved.
-template <typename Real, int TERMS, int MODE>
+// TPA lanes (a warp-aligned tile) share one atom: lane l walks entries
+// l, l + TPA, ... of the atom's neighbour row, so 23.5k atoms still fill the
+// GPU, and the tile reduces its forces with shuffles at the end.
+template <typename Real, int TERMS, int MODE, int TPA>
 __global__ void __launch_bounds__(128) k_pairs(PairArgs<Real> a) {
+  static_assert(TPA >= 1 && TPA <= 32 && (TPA & (TPA - 1)) == 0, "TPA: power of two");
   constexpr bool MIXED = sizeof(Real) == 4;
   constexpr bool ENERGY = MODE != PAIR_FORCE;
   constexpr bool VIRIAL = MODE == PAIR_VIRIAL;
   constexpr bool RECORD = MODE == PAIR_RECORD;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = gt & (TPA - 1);
+  int i = gt / TPA;
   bool valid = i < a.n;
   int ii = valid ? i : 0;
   int oi = a.sorted[ii];
@@ -148,10 +154,11 @@ __global__ void __launch_bounds__(128) k_pairs(PairArgs<Real> a) {
   constexpr int kPairChunk = 16;
   double Fx = 0, Fy = 0, Fz = 0, Elj = 0, Ec = 0;
   double V[6] = {0, 0, 0, 0, 0, 0};
-  for (int k0 = 0; k0 < cnt; k0 += kPairChunk) {
-    const int k1 = min(cnt, k0 + kPairChunk);
-    for (int k = k0; k < k1; k++) {
-      uint32_t e = a.nbr[(size_t)k * a.n + ii];
+  const uint32_t *row = a.nbr + (size_t)ii * a.cap;
+  for (int k0 = lane; k0 < cnt; k0 += kPairChunk * TPA) {
+    const int k1 = min(cnt, k0 + kPairChunk * TPA);
+    for (int k = k0; k < k1; k += TPA) {
+      uint32_t e = row[k];
       int j = (int)(e & kJMask);
       int sh = (int)((e >> kShiftBits) & 31);
       if (sh != cur_shift) {
@@ -350,7 +357,14 @@ __global__ void __launch_bounds__(128) k_pairs(PairArgs<Real> a) {
       vxx = vxy = vxz = vyy = vyz = vzz = Real(0);
     }
   }
-  if (valid) {
+  // reduce the atom's force over its TPA lanes (fixed lane order)
+#pragma unroll
+  for (int o = TPA / 2; o > 0; o >>= 1) {
+    Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
+    Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
+    Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+  }
+  if (valid && lane == 0) {
     red_add(&a.force[oi], to_fixed(Fx, kForceScale));
     red_add(&a.force[a.n + oi], to_fixed(Fy, kForceScale));
     red_add(&a.force[2 * a.n + oi], to_fixed(Fz, kForceScale));

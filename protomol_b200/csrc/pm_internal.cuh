@@ -61,6 +61,16 @@ constexpr int kMaxAtoms = 1 << 24;
 constexpr int kFine = 4;
 constexpr int kFine3 = kFine * kFine * kFine;
 
+// Lanes per atom in the pair kernel and in the list build (a power of two
+// <= 32): enough threads to fill 148 SMs at ~20k atoms.
+#ifndef PMGPU_PAIR_LANES
+#define PMGPU_PAIR_LANES 8
+#endif
+constexpr int kPairLanes = PMGPU_PAIR_LANES;
+constexpr int kBuildLanes = 8;
+// Inner MD steps captured per CUDA graph in pmgpu_run.
+constexpr long kGraphSteps = 10;
+
 // Orthogonal periodic box in the exact form ProtoMol's
 // PeriodicBoundaryConditions::set computes (PeriodicBoundaryConditions.cpp:32-78).
 struct Box {
@@ -227,7 +237,18 @@ struct System {
   std::vector<NeighborList> lists;
   int count_pairs = 0;
   int forces_valid = 0;   // resident forces correspond to resident positions
-  uint64_t step = 0;      // RNG counter
+  uint64_t step = 0;      // RNG counter (host mirror of *d_step)
+  unsigned long long *d_step = nullptr;
+  // captured multi-step graphs of pmgpu_run (invalidated by graph_version)
+  int graph_version = 0;
+  int graphs_disabled = 0;
+  struct StepGraph {
+    int version = -1;
+    long steps = 0;
+    pmgpu_integrator key{};
+    cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;  // own kernels per replay
+  } graphs[2];
   long long last_pairs = 0;
   double last_energy[PMGPU_E_COUNT] = {0, 0, 0, 0, 0, 0, 0};
   double last_virial[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -266,6 +287,7 @@ int gb_forces(System *s, Force *f);
 int bonded_forces(System *s, Force *f, int want_virial);
 int zero_forces(System *s);
 int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase);
+int set_device_step(System *s);
 int forces_to_host(System *s, double *out, int add);
 
 }  // namespace pmgpu

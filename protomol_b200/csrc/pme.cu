@@ -70,12 +70,15 @@ __device__ __forceinline__ void grid_coord(const PmeArgs &a, int axis, double w,
   if (iu >= a.K[axis]) iu -= a.K[axis];
 }
 
-__global__ void k_pme_spread(PmeArgs a, const double *__restrict__ pos,
-                             const double *__restrict__ charge,
-                             const int *__restrict__ order_map,
-                             long long *__restrict__ grid) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.n) return;
+// Spread: P2 lanes per atom (P2 = order rounded up to a power of two);
+// lane kx < order adds the order^2 points of its x plane.
+template <int P2>
+__global__ void __launch_bounds__(128)
+k_pme_spread(PmeArgs a, const double *__restrict__ pos, const double *__restrict__ charge,
+             const int *__restrict__ order_map, long long *__restrict__ grid) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = gt / P2, kx = gt & (P2 - 1);
+  if (t >= a.n || kx >= a.order) return;
   int i = order_map ? order_map[t] : t;
   double wx, wy, wz;
   box_minpos(a.box, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wx, wy, wz);
@@ -86,22 +89,19 @@ __global__ void k_pme_spread(PmeArgs a, const double *__restrict__ pos,
   grid_coord(a, 2, wz, iu[2], fr[2]);
   float th[3][kMaxOrder], dth[3][kMaxOrder];
   for (int d = 0; d < 3; d++) bspline(fr[d], a.order, th[d], dth[d]);
-  double q = charge[i];
-  int p = a.order;
-  for (int kx = 0; kx < p; kx++) {
-    int gx = iu[0] - kx;
-    if (gx < 0) gx += a.K[0];
-    double qx = q * (double)th[0][kx];
-    for (int ky = 0; ky < p; ky++) {
-      int gy = iu[1] - ky;
-      if (gy < 0) gy += a.K[1];
-      double qxy = qx * (double)th[1][ky];
-      long long *row = grid + ((size_t)gx * a.K[1] + gy) * a.K[2];
-      for (int kz = 0; kz < p; kz++) {
-        int gz = iu[2] - kz;
-        if (gz < 0) gz += a.K[2];
-        red_add(&row[gz], to_fixed(qxy * (double)th[2][kz], kGridScale));
-      }
+  const int p = a.order;
+  int gx = iu[0] - kx;
+  if (gx < 0) gx += a.K[0];
+  const double qx = charge[i] * (double)th[0][kx];
+  for (int ky = 0; ky < p; ky++) {
+    int gy = iu[1] - ky;
+    if (gy < 0) gy += a.K[1];
+    const double qxy = qx * (double)th[1][ky];
+    long long *row = grid + ((size_t)gx * a.K[1] + gy) * a.K[2];
+    for (int kz = 0; kz < p; kz++) {
+      int gz = iu[2] - kz;
+      if (gz < 0) gz += a.K[2];
+      red_add(&row[gz], to_fixed(qxy * (double)th[2][kz], kGridScale));
     }
   }
 }
@@ -168,51 +168,63 @@ __global__ void k_pme_convolve(int K0, int K1, int K2, double L0, double L1,
   }
 }
 
-__global__ void k_pme_gather(PmeArgs a, const double *__restrict__ pos,
-                             const double *__restrict__ charge,
-                             const int *__restrict__ order_map,
-                             const float *__restrict__ phi, long long *__restrict__ force) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.n) return;
-  int i = order_map ? order_map[t] : t;
-  double wx, wy, wz;
-  box_minpos(a.box, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wx, wy, wz);
-  int iu[3];
-  float fr[3];
-  grid_coord(a, 0, wx, iu[0], fr[0]);
-  grid_coord(a, 1, wy, iu[1], fr[1]);
-  grid_coord(a, 2, wz, iu[2], fr[2]);
-  float th[3][kMaxOrder], dth[3][kMaxOrder];
-  for (int d = 0; d < 3; d++) bspline(fr[d], a.order, th[d], dth[d]);
-  int p = a.order;
+// Gather: P2 lanes per atom, lane kx < order sums its x plane; the partial
+// forces are reduced over the lanes with shuffles.
+template <int P2>
+__global__ void __launch_bounds__(128)
+k_pme_gather(PmeArgs a, const double *__restrict__ pos, const double *__restrict__ charge,
+             const int *__restrict__ order_map, const float *__restrict__ phi,
+             long long *__restrict__ force) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = gt / P2, kx = gt & (P2 - 1);
+  const bool valid = t < a.n;
   float sx = 0.f, sy = 0.f, sz = 0.f;
-  for (int kx = 0; kx < p; kx++) {
-    int gx = iu[0] - kx;
-    if (gx < 0) gx += a.K[0];
-    for (int ky = 0; ky < p; ky++) {
-      int gy = iu[1] - ky;
-      if (gy < 0) gy += a.K[1];
-      const float *row = phi + ((size_t)gx * a.K[1] + gy) * a.K[2];
-      float txy = th[0][kx] * th[1][ky];
-      float dxy = dth[0][kx] * th[1][ky];
-      float txdy = th[0][kx] * dth[1][ky];
-      for (int kz = 0; kz < p; kz++) {
-        int gz = iu[2] - kz;
-        if (gz < 0) gz += a.K[2];
-        float v = __ldg(&row[gz]);
-        sx += dxy * th[2][kz] * v;
-        sy += txdy * th[2][kz] * v;
-        sz += txy * dth[2][kz] * v;
+  int i = 0;
+  if (valid) {
+    i = order_map ? order_map[t] : t;
+    double wx, wy, wz;
+    box_minpos(a.box, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wx, wy, wz);
+    int iu[3];
+    float fr[3];
+    grid_coord(a, 0, wx, iu[0], fr[0]);
+    grid_coord(a, 1, wy, iu[1], fr[1]);
+    grid_coord(a, 2, wz, iu[2], fr[2]);
+    float th[3][kMaxOrder], dth[3][kMaxOrder];
+    for (int d = 0; d < 3; d++) bspline(fr[d], a.order, th[d], dth[d]);
+    const int p = a.order;
+    if (kx < p) {
+      int gx = iu[0] - kx;
+      if (gx < 0) gx += a.K[0];
+      for (int ky = 0; ky < p; ky++) {
+        int gy = iu[1] - ky;
+        if (gy < 0) gy += a.K[1];
+        const float *row = phi + ((size_t)gx * a.K[1] + gy) * a.K[2];
+        const float txy = th[0][kx] * th[1][ky];
+        const float dxy = dth[0][kx] * th[1][ky];
+        const float txdy = th[0][kx] * dth[1][ky];
+        for (int kz = 0; kz < p; kz++) {
+          int gz = iu[2] - kz;
+          if (gz < 0) gz += a.K[2];
+          const float v = __ldg(&row[gz]);
+          sx += dxy * th[2][kz] * v;
+          sy += txdy * th[2][kz] * v;
+          sz += txy * dth[2][kz] * v;
+        }
       }
     }
   }
-  double q = charge[i];
-  double fx = -q * (double)sx * a.K[0] * a.inv_L[0];
-  double fy = -q * (double)sy * a.K[1] * a.inv_L[1];
-  double fz = -q * (double)sz * a.K[2] * a.inv_L[2];
-  red_add(&force[i], to_fixed(fx, kForceScale));
-  red_add(&force[a.n + i], to_fixed(fy, kForceScale));
-  red_add(&force[2 * a.n + i], to_fixed(fz, kForceScale));
+#pragma unroll
+  for (int o = P2 / 2; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    sz += __shfl_xor_sync(0xffffffffu, sz, o);
+  }
+  if (valid && kx == 0) {
+    const double q = charge[i];
+    red_add(&force[i], to_fixed(-q * (double)sx * a.K[0] * a.inv_L[0], kForceScale));
+    red_add(&force[a.n + i], to_fixed(-q * (double)sy * a.K[1] * a.inv_L[1], kForceScale));
+    red_add(&force[2 * a.n + i], to_fixed(-q * (double)sz * a.K[2] * a.inv_L[2], kForceScale));
+  }
 }
 
 // correctionTerm, NonbondedFullEwaldSystemForce.h:1092-1131, FP64.
@@ -361,8 +373,14 @@ int pme_reciprocal(System *s, Force *f, int want_virial) {
       s->lists[f->list_index].built)
     order_map = s->lists[f->list_index].d_sorted;
   PM_CUDA(cudaMemsetAsync(f->d_grid_fixed, 0, sizeof(long long) * nreal, s->stream));
-  k_pme_spread<<<(n + 127) / 128, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge,
-                                                       order_map, f->d_grid_fixed);
+  const int lanes = f->order <= 4 ? 4 : 8;
+  const int nb = (int)(((long long)n * lanes + 127) / 128);
+  if (lanes == 4)
+    k_pme_spread<4><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
+                                               f->d_grid_fixed);
+  else
+    k_pme_spread<8><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
+                                               f->d_grid_fixed);
   k_pme_fixed_to_float<<<(int)((nreal + 255) / 256), 256, 0, s->stream>>>(
       (int)nreal, f->d_grid_fixed, f->d_grid);
   if (cufftExecR2C(f->plan_r2c, f->d_grid, (cufftComplex *)f->d_cgrid) != CUFFT_SUCCESS)
@@ -373,8 +391,12 @@ int pme_reciprocal(System *s, Force *f, int want_virial) {
       want_virial);
   if (cufftExecC2R(f->plan_c2r, (cufftComplex *)f->d_cgrid, f->d_grid) != CUFFT_SUCCESS)
     return fail(PMGPU_ERR_CUDA, "cufftExecC2R failed");
-  k_pme_gather<<<(n + 127) / 128, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge,
-                                                       order_map, f->d_grid, s->d_force);
+  if (lanes == 4)
+    k_pme_gather<4><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
+                                               f->d_grid, s->d_force);
+  else
+    k_pme_gather<8><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
+                                               f->d_grid, s->d_force);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
