@@ -189,6 +189,34 @@ int pmgpu_force_pme_add(pmgpu_system *sys, double alpha, double rc,
  * force/GB/GB{BornRadii,PartialSum,Force}.cpp. */
 int pmgpu_force_gb_add(pmgpu_system *sys, double solute_dielec,
                        double solvent_dielec, int *force_id);
+/* GB forces (the same three passes as pmgpu_force_gb_add) for callers that
+ * must not allocate device memory: a host that has given all of HBM to its
+ * own pool, a plugin that may only use the buffers it is handed, or a loop
+ * that cannot take the device-wide synchronisation cudaMalloc/cudaFree
+ * imply.  This entry point has no counterpart in the reference.
+ *
+ * Every array is device memory on the current device, owned by the caller:
+ * pos (3n, Vector3DBlock layout), charge, gb_vdwr, gb_scale, gb_offset (n
+ * each), water (n, or NULL), forces (3n, OVERWRITTEN, kcal/mol/A) and
+ * energy (1 double, overwritten with the GB energy).  obc is a host array
+ * {alpha, beta, gamma}.  stream is a cudaStream_t (NULL: default stream);
+ * the call only enqueues work on it.
+ *
+ * Scratch lives in one statically sized device array inside the library,
+ * so n_atoms above PMGPU_GB_STATIC_MAX_ATOMS is rejected with
+ * PMGPU_ERR_ARG.  The first call on each device (with that device current)
+ * looks up the array's device address; make that first call before any
+ * stream capture.  All calls on a device share the array and it keeps the
+ * previous call's contents (the call clears what must start at zero): two
+ * calls whose work overlaps on the GPU race and both results are wrong, so
+ * issue them on one stream or otherwise serialise them. */
+#define PMGPU_GB_STATIC_MAX_ATOMS 16384
+int pmgpu_gb_forces_noalloc(int n_atoms, const double *pos, const double *charge,
+                            const double *gb_vdwr, const double *gb_scale,
+                            const double *gb_offset, const int *water,
+                            const double obc[3], double solute_dielec,
+                            double solvent_dielec, int precision,
+                            double *forces, double *energy, void *stream);
 /* Harmonic bonds and angles of the topology. */
 int pmgpu_force_bonded_add(pmgpu_system *sys, int bonds, int angles,
                            int *force_id);

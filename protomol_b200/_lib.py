@@ -24,6 +24,7 @@ PREC_MIXED, PREC_DOUBLE = 0, 1
 EWALD_REAL, EWALD_RECIPROCAL, EWALD_CORRECTION, EWALD_ALL = 1, 2, 4, 7
 INT_LEAPFROG, INT_LANGEVIN_LEAPFROG = 0, 1
 FORCE_SCALE = 4294967296.0
+GB_STATIC_MAX_ATOMS = 16384
 
 EXPORTED = [
     "pmgpu_context_create", "pmgpu_context_destroy", "pmgpu_last_error",
@@ -36,7 +37,7 @@ EXPORTED = [
     "pmgpu_force_set_enabled", "pmgpu_evaluate", "pmgpu_force_evaluate", "pmgpu_run",
     "pmgpu_set_count_pairs", "pmgpu_force_stats", "pmgpu_debug_cell_assign",
     "pmgpu_debug_pair_set", "pmgpu_profile_enable", "pmgpu_profile_read",
-    "pmgpu_kernel_count",
+    "pmgpu_kernel_count", "pmgpu_gb_forces_noalloc",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -121,6 +122,8 @@ def load() -> C.CDLL:
     lib.pmgpu_profile_enable.argtypes = [vp, i32]
     lib.pmgpu_profile_read.argtypes = [vp, vp, vp, i32]
     lib.pmgpu_kernel_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.pmgpu_gb_forces_noalloc.argtypes = [i32, vp, vp, vp, vp, vp, vp, C.POINTER(dbl),
+                                            dbl, dbl, i32, vp, vp, vp]
     _lib = lib
     return lib
 

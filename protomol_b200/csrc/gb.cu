@@ -10,6 +10,8 @@
 // sums reduced in int64 fixed point, so results are order independent.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 
 #include "pm_device.cuh"
 
@@ -322,3 +324,168 @@ int gb_forces(System *s, Force *f) {
 }
 
 }  // namespace pmgpu
+
+// ---------------------------------------------------------------------------
+// GB forces without any device allocation.
+//
+// Some callers cannot allocate device memory at the moment they need GB
+// forces: a host program that has handed all of HBM to its own pool
+// allocator, a plugin that only ever receives buffers from its host and must
+// not grow the device footprint, or a loop that cannot afford the implicit
+// device-wide synchronisation that cudaMalloc/cudaFree bring.  For them this
+// path keeps its scratch (Born radii, psi, partial sums and the fixed-point
+// accumulators) in one statically sized __device__ array that lives as long
+// as the library is loaded.  The price is a hard size limit and a single
+// shared scratch: every call on a device uses the same array, so two calls
+// whose kernels overlap on the GPU (different streams, or different host
+// threads on one device) race on it and both results are garbage.  Callers
+// serialise their calls, for instance by issuing them all on one stream.
+// ---------------------------------------------------------------------------
+namespace pmgpu {
+namespace {
+
+constexpr int kGbStaticMaxAtoms = PMGPU_GB_STATIC_MAX_ATOMS;
+constexpr int kGbStaticAccWords = 32;
+static_assert(ACC_COUNT <= kGbStaticAccWords, "accumulator block too small");
+// per atom: born, psi, partial (double), burial and partial sums (int64),
+// three force planes (int64); then the energy/virial accumulator block
+constexpr size_t kGbStaticWords = 8 * (size_t)kGbStaticMaxAtoms + kGbStaticAccWords;
+constexpr int kGbStaticMaxDevices = 64;
+
+// In host code this name is only a stand-in for the symbol; the device
+// address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) long long g_gb_scratch[kGbStaticWords];
+
+std::mutex g_gb_scratch_mu;
+long long *g_gb_scratch_dev[kGbStaticMaxDevices] = {};
+
+// Device address of g_gb_scratch on the current device, looked up on the
+// first call made with that device current.
+int gb_scratch_address(long long **out) {
+  int dev = -1;
+  PM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kGbStaticMaxDevices)
+    return fail(PMGPU_ERR_UNSUPPORTED, "device ordinal beyond the static scratch table");
+  std::lock_guard<std::mutex> lock(g_gb_scratch_mu);
+  if (!g_gb_scratch_dev[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_gb_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(PMGPU_ERR_CUDA, std::string("cudaGetSymbolAddress(GB scratch): ") +
+                                      cudaGetErrorString(e));
+    g_gb_scratch_dev[dev] = static_cast<long long *>(p);
+  }
+  *out = g_gb_scratch_dev[dev];
+  return PMGPU_OK;
+}
+
+// The caller's arrays must be device (or managed) memory of the current
+// device: a host pointer here would fault inside the kernels.
+int check_device_ptr(const void *p, const char *what) {
+  if (!p) return fail(PMGPU_ERR_ARG, std::string(what) + " is NULL");
+  cudaPointerAttributes at;
+  cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(PMGPU_ERR_ARG, std::string(what) + " is not a CUDA pointer");
+  }
+  if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+    return fail(PMGPU_ERR_ARG, std::string(what) + " is not device memory");
+  int dev = -1;
+  PM_CUDA(cudaGetDevice(&dev));
+  if (at.type == cudaMemoryTypeDevice && at.device != dev)
+    return fail(PMGPU_ERR_ARG, std::string(what) + " lives on another device");
+  return PMGPU_OK;
+}
+
+__global__ void k_gb_static_out(int n, const long long *__restrict__ force,
+                                const long long *__restrict__ acc, double *__restrict__ out,
+                                double *__restrict__ energy) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    for (int c = 0; c < 3; c++) out[3 * i + c] = (double)force[c * n + i] * (1.0 / kForceScale);
+  if (i == 0) *energy = (double)acc[ACC_COULOMB] / kEnergyScale;
+}
+
+}  // namespace
+}  // namespace pmgpu
+
+extern "C" int pmgpu_gb_forces_noalloc(int n_atoms, const double *pos, const double *charge,
+                                       const double *gb_vdwr, const double *gb_scale,
+                                       const double *gb_offset, const int *water,
+                                       const double obc[3], double solute_dielec,
+                                       double solvent_dielec, int precision, double *forces,
+                                       double *energy, void *stream) {
+  using namespace pmgpu;
+  const int n = n_atoms;
+  if (n < 0) return fail(PMGPU_ERR_ARG, "n_atoms < 0");
+  if (n > kGbStaticMaxAtoms)
+    return fail(PMGPU_ERR_ARG, "n_atoms = " + std::to_string(n) +
+                                   " exceeds the static GB scratch limit of " +
+                                   std::to_string(kGbStaticMaxAtoms) + " atoms");
+  if (precision != PMGPU_PREC_MIXED && precision != PMGPU_PREC_DOUBLE)
+    return fail(PMGPU_ERR_ARG, "precision must be PMGPU_PREC_MIXED or PMGPU_PREC_DOUBLE");
+  if (!obc) return fail(PMGPU_ERR_ARG, "obc is NULL");
+  if (!(solute_dielec != 0.0) || !(solvent_dielec != 0.0))
+    return fail(PMGPU_ERR_ARG, "dielectric constants must be non-zero");
+  PM_CHECK(check_device_ptr(energy, "energy"));
+  long long *scratch = nullptr;
+  PM_CHECK(gb_scratch_address(&scratch));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n == 0) {
+    PM_CUDA(cudaMemsetAsync(energy, 0, sizeof(double), st));
+    return PMGPU_OK;
+  }
+  PM_CHECK(check_device_ptr(pos, "pos"));
+  PM_CHECK(check_device_ptr(charge, "charge"));
+  PM_CHECK(check_device_ptr(gb_vdwr, "gb_vdwr"));
+  PM_CHECK(check_device_ptr(gb_scale, "gb_scale"));
+  PM_CHECK(check_device_ptr(gb_offset, "gb_offset"));
+  PM_CHECK(check_device_ptr(forces, "forces"));
+  if (water) PM_CHECK(check_device_ptr(water, "water"));
+
+  // carve the scratch for this n; what accumulates starts at zero
+  GbArgs a;
+  a.n = n;
+  a.pos = pos;
+  a.charge = charge;
+  a.vdwr = gb_vdwr;
+  a.scale = gb_scale;
+  a.offset = gb_offset;
+  a.water = water;
+  a.alpha = obc[0];
+  a.beta = obc[1];
+  a.gamma = obc[2];
+  a.dielec = (1 / solute_dielec) - (1 / solvent_dielec);
+  a.born = reinterpret_cast<double *>(scratch);
+  a.psi = reinterpret_cast<double *>(scratch + n);
+  a.partial = reinterpret_cast<double *>(scratch + 2 * (size_t)n);
+  a.burial_fx = scratch + 3 * (size_t)n;
+  a.partial_fx = scratch + 4 * (size_t)n;
+  a.force = scratch + 5 * (size_t)n;
+  a.acc = scratch + 8 * (size_t)n;
+  PM_CUDA(cudaMemsetAsync(a.burial_fx, 0, sizeof(long long) * (5 * (size_t)n + kGbStaticAccWords),
+                          st));
+
+  int iblocks = (n + kGbTile - 1) / kGbTile;
+  int chunks = std::max(1, std::min((296 + iblocks - 1) / iblocks, (n + kGbTile - 1) / kGbTile));
+  int jchunk = ((n + chunks - 1) / chunks + kGbTile - 1) / kGbTile * kGbTile;
+  chunks = (n + jchunk - 1) / jchunk;
+  dim3 grid(iblocks, chunks);
+  if (precision == PMGPU_PREC_MIXED) {
+    k_gb_burial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);
+    k_gb_partial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    k_gb_partial_fin<<<(n + 127) / 128, 128, 0, st>>>(a);
+    k_gb_force<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
+  } else {
+    k_gb_burial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);
+    k_gb_partial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    k_gb_partial_fin<<<(n + 127) / 128, 128, 0, st>>>(a);
+    k_gb_force<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
+  }
+  k_gb_static_out<<<(n + 255) / 256, 256, 0, st>>>(n, a.force, a.acc, forces, energy);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
