@@ -248,11 +248,20 @@ def main():
         ff.make(line)
     integ = LeapfrogIntegrator(DT_FS)
     if args.mode == "profile":
-        gs.profile(enable=True)  # eager launches, one kernel of each kind per step
-        for _ in range(args.steps):
-            integ.run(gs, 1)
+        # steady state: warm-up segments, then --steps MD steps as one run()
+        # (graphs on) between cudaProfilerStart/Stop, for
+        # `ncu --profile-from-start off`
+        for _ in range(args.warmup):
+            integ.run(gs, args.segment)
+        b0 = gs.forces[3].stats()["list_builds"]
         torch.cuda.synchronize()
-        print(json.dumps({"mode": "profile", "md_steps": args.steps, "atoms": gs.n}))
+        torch.cuda.profiler.start()
+        integ.run(gs, args.steps)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        b1 = gs.forces[3].stats()["list_builds"]
+        print(json.dumps({"mode": "profile", "md_steps": args.steps, "atoms": gs.n,
+                          "list_builds": b1 - b0}))
         gs.close()
         return
     stream = torch.cuda.ExternalStream(gs.stream())
@@ -272,6 +281,7 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     k0 = gs.kernel_count()
+    builds0 = gs.forces[3].stats()["list_builds"]
     total_ms = 0.0
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
@@ -286,6 +296,7 @@ def main():
         total_ms += a.elapsed_time(b)
     torch.cuda.synchronize()
     launches = gs.kernel_count() - k0
+    builds = gs.forces[3].stats()["list_builds"] - builds0
     clk = clocks.stop()
     # end to end through the public API with host buffers: each segment
     # uploads positions and velocities and reads back positions + energies
@@ -334,6 +345,7 @@ def main():
                        "replicas": world, "parallelism": f"replicas x{world}"},
             "pairs_per_s": pairs * md_steps * world / (t_ms / 1000.0),
             "pairs_in_cutoff_per_md_step": pairs,
+            "list_builds_per_100_md_steps": 100.0 * builds / max(1, args.steps * args.segment),
             "us_per_md_step": 1e6 * step_s,
             "phase_ms_per_md_step_eager": {k: v[0] / args.segment for k, v in prof.items()
                                            if v[1]},

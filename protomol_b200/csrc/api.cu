@@ -259,6 +259,9 @@ static int add_pair_terms(std::vector<Launch> &groups, int list, const PairTerms
 // energy accumulators.
 static int evaluate_forces(System *s, int only, int mode) {
   const int want_virial = mode == PAIR_VIRIAL;
+  // energy mode of the non-pair terms: 0 forces only (inner MD steps),
+  // 1 + energies, 2 + energies and virial
+  const int em = mode == PAIR_FORCE ? 0 : (want_virial ? 2 : 1);
   std::vector<Launch> groups;
   std::vector<int> prepared(s->lists.size(), 0);
   for (auto &f : s->forces) {
@@ -292,14 +295,14 @@ static int evaluate_forces(System *s, int only, int mode) {
       case FK_PME:
         if (f.ewald_flags & PMGPU_EWALD_RECIPROCAL) {
           prof_begin(s, PMGPU_PHASE_PME);
-          r = pme_reciprocal(s, &f, want_virial);
+          r = pme_reciprocal(s, &f, em);
           prof_end(s);
           PM_CHECK(r);
           s->kernels += 4;  // spread, fixed->float, convolve, gather (+ cuFFT)
         }
         if (f.ewald_flags & PMGPU_EWALD_CORRECTION) {
           prof_begin(s, PMGPU_PHASE_CORRECTION);
-          r = ewald_correction(s, &f, want_virial);
+          r = ewald_correction(s, &f, em);
           prof_end(s);
           s->kernels += s->n_excl > 0;
         }
@@ -312,7 +315,7 @@ static int evaluate_forces(System *s, int only, int mode) {
         break;
       case FK_BONDED:
         prof_begin(s, PMGPU_PHASE_BONDED);
-        r = bonded_forces(s, &f, want_virial);
+        r = bonded_forces(s, &f, em);
         prof_end(s);
         s->kernels += (f.bonds && s->n_bonds > 0) + (f.angles && s->n_angles > 0);
         break;
@@ -844,7 +847,8 @@ static int one_step(System *s, const pmgpu_integrator *it, int phase, int mode) 
   int ri = integrate_kick_drift(s, it, phase);
   prof_end(s);
   PM_CHECK(ri);
-  s->kernels += (s->n > 0) + 1;  // update + step counter
+  // update (+ step counter for the Langevin noise)
+  s->kernels += (s->n > 0) + (it->kind == PMGPU_INT_LANGEVIN_LEAPFROG);
   PM_CHECK(begin_eval(s));
   return evaluate_forces(s, -1, mode);
 }

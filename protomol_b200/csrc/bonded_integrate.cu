@@ -10,7 +10,7 @@ namespace pmgpu {
 __global__ void k_bonds(Box box, int nb, const int *__restrict__ atoms,
                         const double *__restrict__ prm, const double *__restrict__ pos,
                         int n, long long *__restrict__ force, long long *__restrict__ acc,
-                        int want_virial) {
+                        int em) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
   if (b < nb) {
@@ -31,17 +31,18 @@ __global__ void k_bonds(Box box, int nb, const int *__restrict__ atoms,
     red_add(&force[n + a2], to_fixed(-fy, kForceScale));
     red_add(&force[2 * n + a2], to_fixed(-fz, kForceScale));
     e = k * (r - r0) * (r - r0);
-    if (want_virial) {
+    if (em == 2) {
       v[0] = fx * dx; v[1] = fx * dy; v[2] = fx * dz;
       v[3] = fy * dy; v[4] = fy * dz; v[5] = fz * dz;
     }
   }
+  if (!em) return;
   e = warp_sum(e);
-  if (want_virial)
+  if (em == 2)
     for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
   if ((threadIdx.x & 31) == 0) {
     red_add(&acc[ACC_BOND], to_fixed(e, kEnergyScale));
-    if (want_virial) {
+    if (em == 2) {
       const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
       for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
     }
@@ -53,7 +54,7 @@ __global__ void k_bonds(Box box, int nb, const int *__restrict__ atoms,
 __global__ void k_angles(Box box, int na, const int *__restrict__ atoms,
                          const double *__restrict__ prm, const double *__restrict__ pos,
                          int n, long long *__restrict__ force, long long *__restrict__ acc,
-                         int want_virial) {
+                         int em) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
   if (t < na) {
@@ -92,7 +93,7 @@ __global__ void k_angles(Box box, int na, const int *__restrict__ atoms,
       red_add(&force[c * n + a2], to_fixed(-f1[c] - f3[c], kForceScale));
     }
     e = kt * (theta - t0) * (theta - t0) + kub * (d13 - rub) * (d13 - rub);
-    if (want_virial) {
+    if (em == 2) {
       v[0] = f1[0] * r12[0] + f3[0] * r32[0];
       v[1] = f1[0] * r12[1] + f3[0] * r32[1];
       v[2] = f1[0] * r12[2] + f3[0] * r32[2];
@@ -101,28 +102,29 @@ __global__ void k_angles(Box box, int na, const int *__restrict__ atoms,
       v[5] = f1[2] * r12[2] + f3[2] * r32[2];
     }
   }
+  if (!em) return;
   e = warp_sum(e);
-  if (want_virial)
+  if (em == 2)
     for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
   if ((threadIdx.x & 31) == 0) {
     red_add(&acc[ACC_ANGLE], to_fixed(e, kEnergyScale));
-    if (want_virial) {
+    if (em == 2) {
       const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
       for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
     }
   }
 }
 
-int bonded_forces(System *s, Force *f, int want_virial) {
+int bonded_forces(System *s, Force *f, int em) {
   if (f->bonds && s->n_bonds > 0) {
     k_bonds<<<(s->n_bonds + 127) / 128, 128, 0, s->stream>>>(
         s->box, s->n_bonds, s->d_bond_atoms, s->d_bond_params, s->d_pos, s->n,
-        s->d_force, s->d_acc, want_virial);
+        s->d_force, s->d_acc, em);
   }
   if (f->angles && s->n_angles > 0) {
     k_angles<<<(s->n_angles + 127) / 128, 128, 0, s->stream>>>(
         s->box, s->n_angles, s->d_angle_atoms, s->d_angle_params, s->d_pos, s->n,
-        s->d_force, s->d_acc, want_virial);
+        s->d_force, s->d_acc, em);
   }
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
@@ -285,7 +287,9 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase) {
   if (s->n)
     k_update<<<(s->n + 255) / 256, 256, 0, s->stream>>>(a, s->d_mass, s->d_pos, s->d_vel,
                                                         s->d_force, s->d_status);
-  if (a.drift) k_step_inc<<<1, 1, 0, s->stream>>>(s->d_step);
+  // only the Langevin noise reads the device step counter (every run sets
+  // it from the host counter first)
+  if (a.drift && a.langevin) k_step_inc<<<1, 1, 0, s->stream>>>(s->d_step);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }

@@ -13,8 +13,6 @@
 #include <cmath>
 #include <cstring>
 
-#include <cooperative_groups.h>
-
 #include "pm_device.cuh"
 
 namespace pmgpu {
@@ -30,15 +28,23 @@ struct GridArgs {
   double vmin[3];    // vacuum: grid minimum (positions clamp into the grid)
 };
 
-__device__ __forceinline__ int morton3(int x, int y, int z) {
+// Sort key of an atom: coarse xy column, then the global fine z layer
+// (kFine layers per coarse cell), then a Morton-ordered kFine x kFine xy
+// sub-cell.  Every column is one contiguous z-sorted range, so the list
+// build reads the atoms of a neighbour column within the reach in z as one
+// slice.
+__device__ __forceinline__ int morton2(int x, int y) {
   int m = 0;
 #pragma unroll
   for (int b = 0; b < 2; b++) {
-    m |= ((x >> b) & 1) << (3 * b + 2);
-    m |= ((y >> b) & 1) << (3 * b + 1);
-    m |= ((z >> b) & 1) << (3 * b);
+    m |= ((x >> b) & 1) << (2 * b + 1);
+    m |= ((y >> b) & 1) << (2 * b);
   }
   return m;
+}
+__device__ __forceinline__ int sort_key(int cx, int cy, int layer, int fx, int fy, int ncy,
+                                        int nlayers) {
+  return ((cx * ncy + cy) * nlayers + layer) * (kFine * kFine) + morton2(fx, fy);
 }
 
 // Cell of one atom: floor((delta + minimalPosition(x)) * inv) per axis
@@ -80,8 +86,7 @@ __global__ void k_bin(GridArgs g, const double *__restrict__ pos,
     f[a] = k < 0 ? 0 : (k >= kFine ? kFine - 1 : k);
   }
   if (!isfinite(x) || !isfinite(y) || !isfinite(z)) atomicOr(status, ST_NONFINITE);
-  int cell = (c[0] * g.ncy + c[1]) * g.ncz + c[2];
-  int k = cell * kFine3 + morton3(f[0], f[1], f[2]);
+  int k = sort_key(c[0], c[1], c[2] * kFine + f[2], f[0], f[1], g.ncy, g.ncz * kFine);
   key[i] = k;
   atomicAdd(&key_count[k], 1);
   offset[3 * i] = x - w[0];
@@ -171,14 +176,17 @@ __global__ void k_sort_keys(const int *__restrict__ rebuild, int nkeys,
 
 // Per-step gather of the sorted coordinates: xw = x - offset keeps every
 // atom in the image it had at the last build, so list shifts stay valid.
+// xhi (FP32 position + charge) feeds the list build in both precisions;
+// xlo (the FP32 residue + type) only the mixed-precision pair kernel.
 template <bool MIXED>
 __global__ void k_gather(int n, const double *__restrict__ pos,
                          const double *__restrict__ offset,
                          const double *__restrict__ xbuild,
                          const int *__restrict__ sorted,
                          const double *__restrict__ charge,
-                         const int *__restrict__ type, float4 *__restrict__ xhi,
-                         float4 *__restrict__ xlo, double4 *__restrict__ xw,
+                         const int *__restrict__ type, const int *__restrict__ mol,
+                         float4 *__restrict__ xhi, float4 *__restrict__ xlo,
+                         double4 *__restrict__ xw, int *__restrict__ mol_s,
                          unsigned int *__restrict__ maxdisp) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.f;
@@ -188,12 +196,12 @@ __global__ void k_gather(int n, const double *__restrict__ pos,
     double wx = x - offset[3 * i], wy = y - offset[3 * i + 1], wz = z - offset[3 * i + 2];
     double q = charge[i];
     xw[s] = make_double4(wx, wy, wz, q);
-    if (MIXED) {
-      float hx = (float)wx, hy = (float)wy, hz = (float)wz;
-      xhi[s] = make_float4(hx, hy, hz, (float)q);
+    float hx = (float)wx, hy = (float)wy, hz = (float)wz;
+    xhi[s] = make_float4(hx, hy, hz, (float)q);
+    if (MIXED)
       xlo[s] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
                            (float)(wz - (double)hz), __int_as_float(type[i]));
-    }
+    mol_s[s] = mol[i];
     double dx = x - xbuild[3 * i], dy = y - xbuild[3 * i + 1], dz = z - xbuild[3 * i + 2];
     d2 = (float)(dx * dx + dy * dy + dz * dz);
     if (!(d2 == d2)) d2 = 3.0e38f;  // NaN forces a rebuild / status check
@@ -223,90 +231,141 @@ struct BuildArgs {
   Box box;
   int n;
   int ncx, ncy, ncz;
-  double reach2;
+  float reach2;       // FP32 candidate radius^2 (reach plus a rounding margin)
+  float cull2;        // column culling radius^2 (wider margin)
+  float cell_lo[3];   // lower corner of cell 0 in the xw frame
+  float cs[3];        // coarse cell size
+  float inv_layer;    // 1 / fine z-layer thickness
+  int nlayers;        // fine z layers per column
+  float L[3];         // box edges
+  float H2[3];        // half box edges (minimal-image test)
   int cap;
   int periodic;
+  const int *excl_start, *excl_partner, *excl_class;
 };
 
-// kBuildLanes lanes per atom scan the 27 neighbour cells; candidates are
-// tested in FP32 against (reach + margin)^2 and compacted with a tile ballot,
-// so every row is written in a fixed (cell, index) order.
-__global__ void __launch_bounds__(128)
+__device__ __forceinline__ int excl_class_of(const int *start, const int *partner,
+                                             const int *cls, int oi, int oj) {
+  int b = start[oi], e = start[oi + 1];
+  for (int k = b; k < e; k++)
+    if (partner[k] == oj) return cls[k];
+  return PMGPU_EXCL_NONE;
+}
+
+// One warp per sorted atom: for each of the 9 neighbour columns (skipping
+// columns whose xy box lies beyond the reach) the warp reads the slice of
+// fine z layers within the reach (split where it wraps through the periodic
+// z face), tests 32 candidates at a time in FP32 against (reach + margin)^2
+// and compacts passing entries with a warp ballot, so every row is written
+// in a fixed (column, layer, index) order.  Exclusions are resolved here
+// (ExclusionTable::check, topology/ExclusionTable.h:116-130, consulted only
+// for same-molecule minimal-image pairs as in OneAtomPairTwo.h:47-53):
+// fully excluded pairs are dropped, modified pairs flagged.
+__global__ void __launch_bounds__(kBuildWarps * 32)
 k_build_list(BuildArgs a, const int *__restrict__ rebuild, const int *__restrict__ key,
              const int *__restrict__ sorted, const int *__restrict__ start,
-             const double4 *__restrict__ xw, const int *__restrict__ mol,
+             const float4 *__restrict__ xhi, const int *__restrict__ mol_s,
              uint32_t *__restrict__ nbr, int *__restrict__ nbr_count,
              int *__restrict__ status) {
   if (!*rebuild) return;
-  namespace cg = cooperative_groups;
-  auto tile = cg::tiled_partition<kBuildLanes>(cg::this_thread_block());
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = tile.thread_rank();
-  const int i = gt / kBuildLanes;
-  if (i >= a.n) return;  // whole tiles exit together
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kBuildWarps + (threadIdx.x >> 5);
+  if (i >= a.n) return;  // whole warps exit together
+  const unsigned lt_mask = (1u << lane) - 1u;
   const int oi = sorted[i];
-  const double4 pi = xw[i];
-  const int mi = mol[oi];
-  const int cell = key[oi] / kFine3;
-  const int cz = cell % a.ncz, cy = (cell / a.ncz) % a.ncy, cx = cell / (a.ncz * a.ncy);
-  const int dims[3] = {a.ncx, a.ncy, a.ncz};
-  const float reach2 = (float)a.reach2;
+  const float4 pi = xhi[i];
+  const int mi = mol_s[i];
+  const int col = key[oi] / (a.nlayers * kFine * kFine);
+  const int cy = col % a.ncy, cx = col / a.ncy;
+  const int nl = a.nlayers;
   uint32_t *row = nbr + (size_t)i * a.cap;
   int count = 0;
-  // With one or two cells on an axis the -1/0/+1 neighbours name the same
-  // cells under different images; every (cell, image) pair is distinct and
-  // the box edge exceeds the reach, so no pair appears twice under one image.
+
+  // candidates of one contiguous slice [jb, je) seen under image (sx, sy, sz)
+  auto scan = [&](int jb, int je, int sx, int sy, int sz) {
+    const uint32_t sbits = (uint32_t)shift_code(sx, sy, sz) << kShiftBits;
+    const bool zero = (sx | sy | sz) == 0;
+    const float ox = pi.x - sx * a.L[0];
+    const float oy = pi.y - sy * a.L[1];
+    const float oz = pi.z - sz * a.L[2];
+    for (int j0 = jb; j0 < je; j0 += 32) {
+      const int j = j0 + lane;
+      bool pass = false;
+      uint32_t flags = 0;
+      if (j < je && !(j == i && zero)) {
+        const float4 pj = xhi[j];
+        const float dx = pj.x - ox, dy = pj.y - oy, dz = pj.z - oz;
+        pass = dx * dx + dy * dy + dz * dz < a.reach2;
+        if (pass && mol_s[j] == mi) {
+          const bool minimal = !a.periodic || (fabsf(dx) <= a.H2[0] &&
+                                               fabsf(dy) <= a.H2[1] && fabsf(dz) <= a.H2[2]);
+          if (minimal) {
+            const int cls = excl_class_of(a.excl_start, a.excl_partner, a.excl_class, oi,
+                                          sorted[j]);
+            if (cls == PMGPU_EXCL_FULL) pass = false;
+            else if (cls == PMGPU_EXCL_MODIFIED) flags = kModifiedBit;
+          }
+        }
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, pass);
+      if (pass) {
+        const int slot = count + __popc(m & lt_mask);
+        if (slot < a.cap) row[slot] = (uint32_t)j | sbits | flags;
+      }
+      count += __popc(m);
+    }
+  };
+  auto slice = [&](int c2, int l0, int l1) {  // layers l0..l1 of column c2
+    const int base = c2 * nl * (kFine * kFine);
+    return make_int2(start[base + l0 * (kFine * kFine)],
+                     start[base + (l1 + 1) * (kFine * kFine)]);
+  };
+
+  // With one or two columns on an axis the -1/0/+1 neighbours name the same
+  // columns under different images; every (column, image) pair is distinct
+  // and the box edge exceeds the reach, so no pair appears twice under one
+  // image.
   for (int ddx = -1; ddx <= 1; ddx++) {
     int nx = cx + ddx, sx = 0;
     if (a.periodic) {
-      if (nx < 0) { nx += dims[0]; sx = -1; }
-      else if (nx >= dims[0]) { nx -= dims[0]; sx = 1; }
-    } else if (nx < 0 || nx >= dims[0]) continue;
+      if (nx < 0) { nx += a.ncx; sx = -1; }
+      else if (nx >= a.ncx) { nx -= a.ncx; sx = 1; }
+    } else if (nx < 0 || nx >= a.ncx) continue;
     for (int ddy = -1; ddy <= 1; ddy++) {
       int ny = cy + ddy, sy = 0;
       if (a.periodic) {
-        if (ny < 0) { ny += dims[1]; sy = -1; }
-        else if (ny >= dims[1]) { ny -= dims[1]; sy = 1; }
-      } else if (ny < 0 || ny >= dims[1]) continue;
-      for (int ddz = -1; ddz <= 1; ddz++) {
-        int nz = cz + ddz, sz = 0;
-        if (a.periodic) {
-          if (nz < 0) { nz += dims[2]; sz = -1; }
-          else if (nz >= dims[2]) { nz -= dims[2]; sz = 1; }
-        } else if (nz < 0 || nz >= dims[2]) continue;
-        const int shift = (sx + 1) * 9 + (sy + 1) * 3 + (sz + 1);
-        const float ox = (float)(pi.x - sx * a.box.e[0]);
-        const float oy = (float)(pi.y - sy * a.box.e[1]);
-        const float oz = (float)(pi.z - sz * a.box.e[2]);
-        const int c2 = (nx * dims[1] + ny) * dims[2] + nz;
-        const int jb = start[c2 * kFine3], je = start[c2 * kFine3 + kFine3];
-        for (int j0 = jb; j0 < je; j0 += kBuildLanes) {
-          const int j = j0 + lane;
-          bool pass = false;
-          float dx = 0.f, dy = 0.f, dz = 0.f;
-          if (j < je && !(j == i && shift == kZeroShift)) {
-            const double4 pj = xw[j];
-            dx = (float)pj.x - ox;
-            dy = (float)pj.y - oy;
-            dz = (float)pj.z - oz;
-            pass = dx * dx + dy * dy + dz * dz < reach2;
-          }
-          const unsigned m = tile.ballot(pass);
-          if (pass) {
-            const int slot = count + __popc(m & ((1u << lane) - 1u));
-            uint32_t e = (uint32_t)j | ((uint32_t)shift << kShiftBits);
-            const int oj = sorted[j];
-            if (mol[oj] == mi) {
-              const bool minimal = !a.periodic ||
-                                   (fabsf(dx) <= (float)a.box.H2[0] &&
-                                    fabsf(dy) <= (float)a.box.H2[1] &&
-                                    fabsf(dz) <= (float)a.box.H2[2]);
-              if (minimal) e |= kSameMolBit;
-            }
-            if (slot < a.cap) row[slot] = e;
-          }
-          count += __popc(m);
-        }
+        if (ny < 0) { ny += a.ncy; sy = -1; }
+        else if (ny >= a.ncy) { ny -= a.ncy; sy = 1; }
+      } else if (ny < 0 || ny >= a.ncy) continue;
+      const int c2 = nx * a.ncy + ny;
+      if (!a.periodic) {  // vacuum: atoms may be clamped into edge cells
+        int2 r = slice(c2, 0, nl - 1);
+        scan(r.x, r.y, 0, 0, 0);
+        continue;
+      }
+      // xy distance from the atom to this column's box (in this image)
+      const float lox = a.cell_lo[0] + (cx + ddx) * a.cs[0];
+      const float loy = a.cell_lo[1] + (cy + ddy) * a.cs[1];
+      const float gx = fmaxf(fmaxf(lox - pi.x, pi.x - (lox + a.cs[0])), 0.f);
+      const float gy = fmaxf(fmaxf(loy - pi.y, pi.y - (loy + a.cs[1])), 0.f);
+      const float g2 = gx * gx + gy * gy;
+      if (g2 > a.cull2) continue;
+      const float hz = sqrtf(a.cull2 - g2);  // z half-range of the reach sphere
+      const int l0 = (int)floorf((pi.z - hz - a.cell_lo[2]) * a.inv_layer);
+      const int l1 = (int)floorf((pi.z + hz - a.cell_lo[2]) * a.inv_layer);
+      // layers below 0 are the top of the box seen one box length down
+      // (j image sz = -1); layers past the top the bottom one length up
+      if (l0 < 0) {
+        int2 r = slice(c2, max(nl + l0, 0), nl - 1);
+        scan(r.x, r.y, sx, sy, -1);
+      }
+      {
+        int2 r = slice(c2, max(l0, 0), min(l1, nl - 1));
+        scan(r.x, r.y, sx, sy, 0);
+      }
+      if (l1 >= nl) {
+        int2 r = slice(c2, 0, min(l1 - nl, nl - 1));
+        scan(r.x, r.y, sx, sy, 1);
       }
     }
   }
@@ -396,6 +455,7 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   PM_CUDA(cudaMalloc(&nl->d_xhi, sizeof(float4) * nn));
   PM_CUDA(cudaMalloc(&nl->d_xlo, sizeof(float4) * nn));
   PM_CUDA(cudaMalloc(&nl->d_xw, sizeof(double4) * nn));
+  PM_CUDA(cudaMalloc(&nl->d_mol_s, sizeof(int) * nn));
   PM_CUDA(cudaMalloc(&nl->d_nbr, sizeof(uint32_t) * (size_t)cap * nn));
   PM_CUDA(cudaMalloc(&nl->d_nbr_count, sizeof(int) * nn));
   PM_CUDA(cudaMemset(nl->d_nbr_count, 0, sizeof(int) * nn));
@@ -410,14 +470,15 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
 int nb_list_free(NeighborList *nl) {
   void *ptrs[] = {nl->d_key, nl->d_key_count, nl->d_key_start, nl->d_key_cursor,
                   nl->d_sorted, nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo,
-                  nl->d_xw, nl->d_nbr, nl->d_nbr_count, nl->d_maxdisp, nl->d_rebuild};
+                  nl->d_xw, nl->d_nbr, nl->d_nbr_count, nl->d_maxdisp, nl->d_rebuild,
+                  nl->d_mol_s};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   nl->d_key = nullptr; nl->d_key_count = nullptr; nl->d_key_start = nullptr;
   nl->d_key_cursor = nullptr; nl->d_sorted = nullptr; nl->d_offset = nullptr;
   nl->d_xbuild = nullptr; nl->d_xhi = nullptr; nl->d_xlo = nullptr;
   nl->d_xw = nullptr; nl->d_nbr = nullptr; nl->d_nbr_count = nullptr;
-  nl->d_maxdisp = nullptr; nl->d_rebuild = nullptr;
+  nl->d_maxdisp = nullptr; nl->d_rebuild = nullptr; nl->d_mol_s = nullptr;
   return PMGPU_OK;
 }
 
@@ -459,24 +520,39 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
                                                     nl->d_key_count);
   if (s->precision == PMGPU_PREC_MIXED)
     k_gather<true><<<nb, T, 0, st>>>(n, s->d_pos, nl->d_offset, nl->d_xbuild,
-                                     nl->d_sorted, s->d_charge, s->d_type, nl->d_xhi,
-                                     nl->d_xlo, nl->d_xw, nl->d_maxdisp);
+                                     nl->d_sorted, s->d_charge, s->d_type, s->d_mol,
+                                     nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
+                                     nl->d_maxdisp);
   else
     k_gather<false><<<nb, T, 0, st>>>(n, s->d_pos, nl->d_offset, nl->d_xbuild,
-                                      nl->d_sorted, s->d_charge, s->d_type, nl->d_xhi,
-                                      nl->d_xlo, nl->d_xw, nl->d_maxdisp);
+                                      nl->d_sorted, s->d_charge, s->d_type, s->d_mol,
+                                      nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
+                                      nl->d_maxdisp);
   BuildArgs ba;
   ba.box = s->box;
   ba.n = n;
   ba.ncx = nl->ncx; ba.ncy = nl->ncy; ba.ncz = nl->ncz;
   // FP32 candidate test with a margin well above its rounding error
-  ba.reach2 = (nl->reach + 0.01) * (nl->reach + 0.01);
+  const double r1 = nl->reach + 0.01, r2 = nl->reach + 0.05;
+  ba.reach2 = (float)(r1 * r1);
+  ba.cull2 = (float)(r2 * r2);
+  for (int c = 0; c < 3; c++) {
+    ba.cell_lo[c] = (float)(s->box.periodic ? s->box.min[c] - s->box.origin[c]
+                                            : nl->vac_origin[c]);
+    ba.cs[c] = (float)nl->cs[c];
+    ba.L[c] = (float)s->box.e[c];
+    ba.H2[c] = (float)s->box.H2[c];
+  }
+  ba.inv_layer = (float)(kFine / nl->cs[2]);
+  ba.nlayers = nl->ncz * kFine;
   ba.cap = nl->cap;
   ba.periodic = s->box.periodic;
-  k_build_list<<<(int)(((long long)n * kBuildLanes + 127) / 128), 128, 0, st>>>(ba, nl->d_rebuild, nl->d_key,
-                                                nl->d_sorted, nl->d_key_start, nl->d_xw,
-                                                s->d_mol, nl->d_nbr, nl->d_nbr_count,
-                                                s->d_status);
+  ba.excl_start = s->d_excl_start;
+  ba.excl_partner = s->d_excl_partner;
+  ba.excl_class = s->d_excl_class;
+  k_build_list<<<(n + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, st>>>(
+      ba, nl->d_rebuild, nl->d_key, nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s,
+      nl->d_nbr, nl->d_nbr_count, s->d_status);
   PM_CUDA(cudaGetLastError());
   nl->built = 1;
   return PMGPU_OK;
@@ -512,6 +588,11 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   if (t.mask & TERM_COUL) mx = std::max(mx, t.coul_cut2);
   if (t.mask & TERM_EWALD) mx = std::max(mx, t.ewald_rc2);
   a.max_hi = (Real)(mx * (1 + band));
+  a.max_lo = (Real)(mx * (1 - band));
+  a.same_cut = 1;
+  if ((t.mask & TERM_LJ) && t.lj_cut2 != mx) a.same_cut = 0;
+  if ((t.mask & TERM_COUL) && t.coul_cut2 != mx) a.same_cut = 0;
+  if ((t.mask & TERM_EWALD) && t.ewald_rc2 != mx) a.same_cut = 0;
   a.alpha = (Real)t.ewald_alpha;
   a.a2pi = (Real)(2.0 * t.ewald_alpha / std::sqrt(M_PI));
   a.alpha64 = t.ewald_alpha;
@@ -538,28 +619,64 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   a.pairbuf = s->d_pairbuf;
   a.pairbuf_cap = s->pairbuf_cap;
   a.paircount = s->d_paircount;
+  a.count_pairs = s->count_pairs;
 }
 
-template <typename Real, int TERMS>
-static void launch_pairs_t(PairArgs<Real> &a, cudaStream_t st, int mode) {
-  constexpr int TPA = kPairLanes;
-  int nb = (int)(((long long)a.n * TPA + 127) / 128);
+// Compile-time switch kind of a term for the specialised force-only
+// kernel: -2 when the configuration has no specialisation.
+static int spec_kind(const SwitchParams &sw) {
+  if (!sw.modify) return kSwNone;
+  if (sw.kind == PMGPU_SW_C2 || sw.kind == PMGPU_SW_C1) return sw.kind;
+  return -2;
+}
+
+template <typename Real, int TERMS, typename SPEC>
+static void launch_pairs_spec(PairArgs<Real> &a, cudaStream_t st, int mode) {
+  const int nb = (a.n + kPairWarps - 1) / kPairWarps;
+  const int T = kPairWarps * 32;
   switch (mode) {
-    case PAIR_FORCE: k_pairs<Real, TERMS, PAIR_FORCE, TPA><<<nb, 128, 0, st>>>(a); break;
-    case PAIR_ENERGY: k_pairs<Real, TERMS, PAIR_ENERGY, TPA><<<nb, 128, 0, st>>>(a); break;
-    case PAIR_VIRIAL: k_pairs<Real, TERMS, PAIR_VIRIAL, TPA><<<nb, 128, 0, st>>>(a); break;
-    default: k_pairs<Real, TERMS, PAIR_RECORD, TPA><<<nb, 128, 0, st>>>(a); break;
+    case PAIR_FORCE: k_pairs<Real, TERMS, PAIR_FORCE, SPEC><<<nb, T, 0, st>>>(a); break;
+    case PAIR_ENERGY: k_pairs<Real, TERMS, PAIR_ENERGY, SPEC><<<nb, T, 0, st>>>(a); break;
+    case PAIR_VIRIAL: k_pairs<Real, TERMS, PAIR_VIRIAL, SPEC><<<nb, T, 0, st>>>(a); break;
+    default: k_pairs<Real, TERMS, PAIR_RECORD, SPEC><<<nb, T, 0, st>>>(a); break;
   }
 }
 
+template <typename Real, int TERMS, typename SPEC>
+static void launch_force_spec(PairArgs<Real> &a, cudaStream_t st) {
+  const int nb = (a.n + kPairWarps - 1) / kPairWarps;
+  k_pairs<Real, TERMS, PAIR_FORCE, SPEC><<<nb, kPairWarps * 32, 0, st>>>(a);
+}
+
+template <typename Real, int TERMS>
+static void launch_pairs_t(PairArgs<Real> &a, cudaStream_t st, int mode, const PairTerms &t) {
+  // specialised force-only FP32 kernels of the common configurations
+  if (sizeof(Real) == 4 && mode == PAIR_FORCE) {
+    const int lk = spec_kind(t.lj_sw), ck = spec_kind(t.coul_sw);
+    if (TERMS == (TERM_LJ | TERM_EWALD) && !t.exact_erf && lk == PMGPU_SW_C2) {
+      launch_force_spec<Real, TERM_LJ | TERM_EWALD, PairSpec<PMGPU_SW_C2, -1, 0>>(a, st);
+      return;
+    }
+    if (TERMS == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C2) {
+      launch_force_spec<Real, TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C2, -1>>(a, st);
+      return;
+    }
+    if (TERMS == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C1) {
+      launch_force_spec<Real, TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C1, -1>>(a, st);
+      return;
+    }
+  }
+  launch_pairs_spec<Real, TERMS, GenericSpec>(a, st, mode);
+}
+
 template <typename Real>
-static int launch_pairs(PairArgs<Real> &a, cudaStream_t st, int mode) {
+static int launch_pairs(PairArgs<Real> &a, cudaStream_t st, int mode, const PairTerms &t) {
   switch (a.mask) {
-    case TERM_LJ: launch_pairs_t<Real, TERM_LJ>(a, st, mode); break;
-    case TERM_COUL: launch_pairs_t<Real, TERM_COUL>(a, st, mode); break;
-    case TERM_LJ | TERM_COUL: launch_pairs_t<Real, TERM_LJ | TERM_COUL>(a, st, mode); break;
-    case TERM_EWALD: launch_pairs_t<Real, TERM_EWALD>(a, st, mode); break;
-    case TERM_LJ | TERM_EWALD: launch_pairs_t<Real, TERM_LJ | TERM_EWALD>(a, st, mode); break;
+    case TERM_LJ: launch_pairs_t<Real, TERM_LJ>(a, st, mode, t); break;
+    case TERM_COUL: launch_pairs_t<Real, TERM_COUL>(a, st, mode, t); break;
+    case TERM_LJ | TERM_COUL: launch_pairs_t<Real, TERM_LJ | TERM_COUL>(a, st, mode, t); break;
+    case TERM_EWALD: launch_pairs_t<Real, TERM_EWALD>(a, st, mode, t); break;
+    case TERM_LJ | TERM_EWALD: launch_pairs_t<Real, TERM_LJ | TERM_EWALD>(a, st, mode, t); break;
     default:
       return fail(PMGPU_ERR_UNSUPPORTED, "unsupported pair-term combination");
   }
@@ -574,11 +691,11 @@ int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode) {
   if (s->precision == PMGPU_PREC_MIXED) {
     PairArgs<float> a;
     fill_pair_args<float>(a, s, nl, t);
-    return launch_pairs<float>(a, s->stream, mode);
+    return launch_pairs<float>(a, s->stream, mode, t);
   }
   PairArgs<double> a;
   fill_pair_args<double>(a, s, nl, t);
-  return launch_pairs<double>(a, s->stream, mode);
+  return launch_pairs<double>(a, s->stream, mode, t);
 }
 
 // ProtoMol cell assignment with a given cellsize on the resident positions
@@ -690,7 +807,7 @@ k_simplefull(int n, const double *__restrict__ pos, const double *__restrict__ c
         if (jj == i) continue;
         int excl = PMGPU_EXCL_NONE;
         if (sm[k] == mi) {
-          excl = excl_lookup(ex_start, ex_partner, ex_class, i, jj);
+          excl = excl_class_of(ex_start, ex_partner, ex_class, i, jj);
           if (excl == PMGPU_EXCL_FULL) continue;
         }
         Real dx = (Real)(sx[k] - xi), dy = (Real)(sy[k] - yi), dz = (Real)(sz[k] - zi);

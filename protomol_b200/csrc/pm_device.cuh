@@ -193,6 +193,19 @@ __device__ __forceinline__ Real poly5(Real ar) {
                         t * (Real(-1.453152027) + t * Real(1.061405429)))));
 }
 
+// The same polynomial with the reciprocal from the fast hardware
+// approximation (about 2 ulp) in FP32; FP64 keeps the exact division.
+template <typename Real>
+__device__ __forceinline__ Real poly5_fast(Real ar) {
+  return poly5<Real>(ar);
+}
+template <>
+__device__ __forceinline__ float poly5_fast<float>(float ar) {
+  float t = __fdividef(1.0f, 1.0f + 0.3275911f * ar);
+  return t * (0.254829592f +
+              t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f))));
+}
+
 // ----------------------------------------------------------- fixed point
 __device__ __forceinline__ long long to_fixed(double v, double scale) {
   return __double2ll_rn(v * scale);

@@ -47,13 +47,17 @@ enum { ACC_COULOMB = 0, ACC_LJ, ACC_BOND, ACC_ANGLE, ACC_DIHEDRAL,
 enum { ST_LIST_OVERFLOW = 1, ST_NONFINITE = 2, ST_CELL_OVERFLOW = 4,
        ST_BAD_BOX = 8 };
 
-// Neighbour-entry layout: bits 0..23 sorted j index, 24..28 periodic shift
-// code ((sx+1)*9 + (sy+1)*3 + (sz+1)), bit 29 "same molecule, minimal
-// image" (exclusion lookup needed).
+// Neighbour-entry layout: bits 0..23 sorted j index, 24..29 periodic image
+// of j as three 2-bit fields (sx+1, sy+1, sz+1), bit 30 "modified (scaled
+// 1-4) pair".  Fully excluded minimal-image pairs never enter the list.
 constexpr uint32_t kJMask = 0xFFFFFFu;
 constexpr int kShiftBits = 24;
-constexpr uint32_t kSameMolBit = 1u << 29;
-constexpr int kZeroShift = 13;
+constexpr uint32_t kShiftMask = 0x3Fu;
+constexpr uint32_t kModifiedBit = 1u << 30;
+constexpr int kZeroShift = 1 | (1 << 2) | (1 << 4);
+__host__ __device__ constexpr int shift_code(int sx, int sy, int sz) {
+  return (sx + 1) | ((sy + 1) << 2) | ((sz + 1) << 4);
+}
 constexpr int kMaxAtoms = 1 << 24;
 
 // Fine sub-cells per coarse cell and axis (Morton-ordered inside a coarse
@@ -61,13 +65,9 @@ constexpr int kMaxAtoms = 1 << 24;
 constexpr int kFine = 4;
 constexpr int kFine3 = kFine * kFine * kFine;
 
-// Lanes per atom in the pair kernel and in the list build (a power of two
-// <= 32): enough threads to fill 148 SMs at ~20k atoms.
-#ifndef PMGPU_PAIR_LANES
-#define PMGPU_PAIR_LANES 8
-#endif
-constexpr int kPairLanes = PMGPU_PAIR_LANES;
-constexpr int kBuildLanes = 8;
+// Warps per block of the warp-per-atom pair kernel and list build.
+constexpr int kPairWarps = 8;
+constexpr int kBuildWarps = 8;
 // Inner MD steps captured per CUDA graph in pmgpu_run.
 constexpr long kGraphSteps = 10;
 
@@ -132,7 +132,8 @@ struct NeighborList {
   float4 *d_xhi = nullptr;      // n (x,y,z,q)
   float4 *d_xlo = nullptr;      // n (x,y,z, type bits)
   double4 *d_xw = nullptr;      // n FP64 wrapped position + q
-  uint32_t *d_nbr = nullptr;    // cap * n, column major
+  int *d_mol_s = nullptr;       // n molecule of each sorted slot
+  uint32_t *d_nbr = nullptr;    // n rows of cap entries (row per sorted atom)
   int *d_nbr_count = nullptr;   // n
   unsigned int *d_maxdisp = nullptr;  // float bits of max displacement^2
   int *d_rebuild = nullptr;     // rebuild flag
@@ -161,7 +162,7 @@ struct Force {
   float *d_grid = nullptr;            // real grid (K1*K2*K3)
   long long *d_grid_fixed = nullptr;  // fixed-point spread target
   float2 *d_cgrid = nullptr;          // complex grid (K1*K2*(K3/2+1))
-  float *d_bsp_mod[3] = {nullptr, nullptr, nullptr};
+  float *d_influence = nullptr;       // K1*K2*(K3/2+1) influence function
   // simplefull
   int sf_lj = 0, sf_coul = 0;
   // gb
@@ -276,15 +277,15 @@ int nb_simplefull(System *s, int lj, int coul, int want_virial);
 // pme.cu
 int pme_init(System *s, Force *f);
 int pme_free(Force *f);
-int pme_reciprocal(System *s, Force *f, int want_virial);
-int ewald_correction(System *s, Force *f, int want_virial);
+int pme_reciprocal(System *s, Force *f, int em);
+int ewald_correction(System *s, Force *f, int em);
 
 // gb.cu
 int gb_init(System *s);
 int gb_forces(System *s, Force *f);
 
 // bonded_integrate.cu
-int bonded_forces(System *s, Force *f, int want_virial);
+int bonded_forces(System *s, Force *f, int em);
 int zero_forces(System *s);
 int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase);
 int set_device_step(System *s);

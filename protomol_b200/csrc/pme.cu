@@ -29,20 +29,27 @@ struct PmeArgs {
 };
 
 // B-spline weights M_p(fr + k), k = 0..p-1, and their derivatives with
-// respect to u, by the Cox-de Boor recursion of the cardinal B-spline.
-__device__ __forceinline__ void bspline(float fr, int p, float *th, float *dth) {
-  float m[kMaxOrder];
+// respect to u, by the Cox-de Boor recursion of the cardinal B-spline
+// (fully unrolled for a compile-time order, so the weights stay in
+// registers).
+template <int P>
+__device__ __forceinline__ void bspline(float fr, float *th, float *dth) {
+  float m[P];
   m[0] = fr;
   m[1] = 1.f - fr;
-  for (int k = 2; k < p; k++) m[k] = 0.f;
-  for (int n = 3; n <= p; n++) {
-    if (n == p) {
+#pragma unroll
+  for (int k = 2; k < P; k++) m[k] = 0.f;
+#pragma unroll
+  for (int n = 3; n <= P; n++) {
+    if (n == P) {
       // derivative of M_p from M_{p-1}
       dth[0] = m[0];
-      for (int k = 1; k < p; k++) dth[k] = m[k] - m[k - 1];
+#pragma unroll
+      for (int k = 1; k < P; k++) dth[k] = m[k] - m[k - 1];
     }
-    float div = 1.f / (float)(n - 1);
+    const float div = 1.f / (float)(n - 1);
     float prev = 0.f;
+#pragma unroll
     for (int k = 0; k < n; k++) {
       float cur = k < n - 1 ? m[k] : 0.f;
       float x = fr + (float)k;
@@ -50,11 +57,12 @@ __device__ __forceinline__ void bspline(float fr, int p, float *th, float *dth) 
       prev = cur;
     }
   }
-  if (p == 2) {
+  if (P == 2) {
     dth[0] = 1.f;
     dth[1] = -1.f;
   }
-  for (int k = 0; k < p; k++) th[k] = m[k];
+#pragma unroll
+  for (int k = 0; k < P; k++) th[k] = m[k];
 }
 
 // Grid coordinate of one atom along one axis: u = K * (frac), with frac
@@ -70,15 +78,15 @@ __device__ __forceinline__ void grid_coord(const PmeArgs &a, int axis, double w,
   if (iu >= a.K[axis]) iu -= a.K[axis];
 }
 
-// Spread: P2 lanes per atom (P2 = order rounded up to a power of two);
-// lane kx < order adds the order^2 points of its x plane.
-template <int P2>
+// Spread: L lanes per atom (L = order rounded up to a power of two); lane
+// kx < P adds the P^2 points of its x plane.
+template <int P, int L>
 __global__ void __launch_bounds__(128)
 k_pme_spread(PmeArgs a, const double *__restrict__ pos, const double *__restrict__ charge,
              const int *__restrict__ order_map, long long *__restrict__ grid) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int t = gt / P2, kx = gt & (P2 - 1);
-  if (t >= a.n || kx >= a.order) return;
+  const int t = gt / L, kx = gt & (L - 1);
+  if (t >= a.n || kx >= P) return;
   int i = order_map ? order_map[t] : t;
   double wx, wy, wz;
   box_minpos(a.box, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wx, wy, wz);
@@ -87,21 +95,29 @@ k_pme_spread(PmeArgs a, const double *__restrict__ pos, const double *__restrict
   grid_coord(a, 0, wx, iu[0], fr[0]);
   grid_coord(a, 1, wy, iu[1], fr[1]);
   grid_coord(a, 2, wz, iu[2], fr[2]);
-  float th[3][kMaxOrder], dth[3][kMaxOrder];
-  for (int d = 0; d < 3; d++) bspline(fr[d], a.order, th[d], dth[d]);
-  const int p = a.order;
+  float thx[P], thy[P], thz[P], d[P];
+  bspline<P>(fr[0], thx, d);
+  bspline<P>(fr[1], thy, d);
+  bspline<P>(fr[2], thz, d);
+  // this lane's x weight without a dynamically indexed array
+  float tx = thx[0];
+#pragma unroll
+  for (int k = 1; k < P; k++)
+    if (kx == k) tx = thx[k];
   int gx = iu[0] - kx;
   if (gx < 0) gx += a.K[0];
-  const double qx = charge[i] * (double)th[0][kx];
-  for (int ky = 0; ky < p; ky++) {
+  const double qx = charge[i] * (double)tx;
+#pragma unroll
+  for (int ky = 0; ky < P; ky++) {
     int gy = iu[1] - ky;
     if (gy < 0) gy += a.K[1];
-    const double qxy = qx * (double)th[1][ky];
+    const double qxy = qx * (double)thy[ky];
     long long *row = grid + ((size_t)gx * a.K[1] + gy) * a.K[2];
-    for (int kz = 0; kz < p; kz++) {
+#pragma unroll
+    for (int kz = 0; kz < P; kz++) {
       int gz = iu[2] - kz;
       if (gz < 0) gz += a.K[2];
-      red_add(&row[gz], to_fixed(qxy * (double)th[2][kz], kGridScale));
+      red_add(&row[gz], to_fixed(qxy * (double)thz[kz], kGridScale));
     }
   }
 }
@@ -112,71 +128,66 @@ __global__ void k_pme_fixed_to_float(int total, const long long *__restrict__ g,
   if (i < total) out[i] = (float)((double)g[i] * (1.0 / kGridScale));
 }
 
-// Multiply by the influence function; reduce energy and virial.
+// Multiply by the influence function (precomputed for the box:
+// exp(-pi^2 m^2/alpha^2)/(pi V m^2) |b(m)|^2, zero at m = 0); with em >= 1
+// reduce the energy, with em == 2 also the virial.
 // m index convention: m in [0, K/2] -> m, (K/2, K) -> m - K.
-__global__ void k_pme_convolve(int K0, int K1, int K2, double L0, double L1,
-                               double L2, double alpha, double V,
-                               const float *__restrict__ bmod0,
-                               const float *__restrict__ bmod1,
-                               const float *__restrict__ bmod2,
-                               float2 *__restrict__ c, long long *__restrict__ acc,
-                               int want_virial) {
-  int Kh = K2 / 2 + 1;
-  int total = K0 * K1 * Kh;
-  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_pme_convolve(int K0, int K1, int K2, double L0, double L1, double L2,
+                               double alpha, const float *__restrict__ infl,
+                               float2 *__restrict__ c, long long *__restrict__ acc, int em) {
+  const int Kh = K2 / 2 + 1;
+  const int total = K0 * K1 * Kh;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
   if (idx < total) {
-    int mz = idx % Kh;
-    int my_ = (idx / Kh) % K1;
-    int mx_ = idx / (Kh * K1);
-    int mx = mx_ <= K0 / 2 ? mx_ : mx_ - K0;
-    int my = my_ <= K1 / 2 ? my_ : my_ - K1;
-    float2 f = c[idx];
-    if (mx == 0 && my == 0 && mz == 0) {
-      c[idx] = make_float2(0.f, 0.f);
-    } else {
-      double hx = mx / L0, hy = my / L1, hz = mz / L2;
-      double h2 = hx * hx + hy * hy + hz * hz;
-      double pa = M_PI * M_PI / (alpha * alpha);
-      double g = exp(-pa * h2) / (M_PI * V * h2) *
-                 (double)bmod0[mx_] * (double)bmod1[my_] * (double)bmod2[mz];
-      double w = (mz == 0 || (K2 % 2 == 0 && mz == K2 / 2)) ? 1.0 : 2.0;
-      double f2 = (double)f.x * f.x + (double)f.y * f.y;
-      double em = 0.5 * w * g * f2;
-      e = em;
-      if (want_virial) {
-        double cc = 2.0 * (1.0 / h2 + pa);
-        v[0] = em * (1.0 - cc * hx * hx);
-        v[1] = -em * cc * hx * hy;
-        v[2] = -em * cc * hx * hz;
-        v[3] = em * (1.0 - cc * hy * hy);
-        v[4] = -em * cc * hy * hz;
-        v[5] = em * (1.0 - cc * hz * hz);
+    const float g = infl[idx];
+    const float2 f = c[idx];
+    c[idx] = make_float2(g * f.x, g * f.y);
+    if (em) {
+      const int mz = idx % Kh;
+      const double w = (mz == 0 || (K2 % 2 == 0 && mz == K2 / 2)) ? 1.0 : 2.0;
+      const double f2 = (double)f.x * f.x + (double)f.y * f.y;
+      const double emode = 0.5 * w * (double)g * f2;
+      e = emode;
+      if (em == 2 && g != 0.f) {
+        const int my_ = (idx / Kh) % K1, mx_ = idx / (Kh * K1);
+        const int mx = mx_ <= K0 / 2 ? mx_ : mx_ - K0;
+        const int my = my_ <= K1 / 2 ? my_ : my_ - K1;
+        const double hx = mx / L0, hy = my / L1, hz = mz / L2;
+        const double h2 = hx * hx + hy * hy + hz * hz;
+        const double pa = M_PI * M_PI / (alpha * alpha);
+        const double cc = 2.0 * (1.0 / h2 + pa);
+        v[0] = emode * (1.0 - cc * hx * hx);
+        v[1] = -emode * cc * hx * hy;
+        v[2] = -emode * cc * hx * hz;
+        v[3] = emode * (1.0 - cc * hy * hy);
+        v[4] = -emode * cc * hy * hz;
+        v[5] = emode * (1.0 - cc * hz * hz);
       }
-      c[idx] = make_float2((float)(g * f.x), (float)(g * f.y));
     }
   }
+  if (!em) return;
   e = warp_sum(e);
-  if (want_virial)
+  if (em == 2)
     for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
   if ((threadIdx.x & 31) == 0) {
     red_add(&acc[ACC_COULOMB], to_fixed(e, kEnergyScale));
-    if (want_virial) {
+    if (em == 2) {
       const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
       for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
     }
   }
 }
 
-// Gather: P2 lanes per atom, lane kx < order sums its x plane; the partial
+// Gather: L lanes per atom, lane kx < P sums its x plane; the partial
 // forces are reduced over the lanes with shuffles.
-template <int P2>
+template <int P, int L>
 __global__ void __launch_bounds__(128)
 k_pme_gather(PmeArgs a, const double *__restrict__ pos, const double *__restrict__ charge,
              const int *__restrict__ order_map, const float *__restrict__ phi,
              long long *__restrict__ force) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int t = gt / P2, kx = gt & (P2 - 1);
+  const int t = gt / L, kx = gt & (L - 1);
   const bool valid = t < a.n;
   float sx = 0.f, sy = 0.f, sz = 0.f;
   int i = 0;
@@ -189,32 +200,42 @@ k_pme_gather(PmeArgs a, const double *__restrict__ pos, const double *__restrict
     grid_coord(a, 0, wx, iu[0], fr[0]);
     grid_coord(a, 1, wy, iu[1], fr[1]);
     grid_coord(a, 2, wz, iu[2], fr[2]);
-    float th[3][kMaxOrder], dth[3][kMaxOrder];
-    for (int d = 0; d < 3; d++) bspline(fr[d], a.order, th[d], dth[d]);
-    const int p = a.order;
-    if (kx < p) {
+    float thx[P], dthx[P], thy[P], dthy[P], thz[P], dthz[P];
+    bspline<P>(fr[0], thx, dthx);
+    bspline<P>(fr[1], thy, dthy);
+    bspline<P>(fr[2], thz, dthz);
+    if (kx < P) {
+      float tx = thx[0], dtx = dthx[0];
+#pragma unroll
+      for (int k = 1; k < P; k++)
+        if (kx == k) {
+          tx = thx[k];
+          dtx = dthx[k];
+        }
       int gx = iu[0] - kx;
       if (gx < 0) gx += a.K[0];
-      for (int ky = 0; ky < p; ky++) {
+#pragma unroll
+      for (int ky = 0; ky < P; ky++) {
         int gy = iu[1] - ky;
         if (gy < 0) gy += a.K[1];
         const float *row = phi + ((size_t)gx * a.K[1] + gy) * a.K[2];
-        const float txy = th[0][kx] * th[1][ky];
-        const float dxy = dth[0][kx] * th[1][ky];
-        const float txdy = th[0][kx] * dth[1][ky];
-        for (int kz = 0; kz < p; kz++) {
+        const float txy = tx * thy[ky];
+        const float dxy = dtx * thy[ky];
+        const float txdy = tx * dthy[ky];
+#pragma unroll
+        for (int kz = 0; kz < P; kz++) {
           int gz = iu[2] - kz;
           if (gz < 0) gz += a.K[2];
           const float v = __ldg(&row[gz]);
-          sx += dxy * th[2][kz] * v;
-          sy += txdy * th[2][kz] * v;
-          sz += txy * dth[2][kz] * v;
+          sx += dxy * thz[kz] * v;
+          sy += txdy * thz[kz] * v;
+          sz += txy * dthz[kz] * v;
         }
       }
     }
   }
 #pragma unroll
-  for (int o = P2 / 2; o > 0; o >>= 1) {
+  for (int o = L / 2; o > 0; o >>= 1) {
     sx += __shfl_xor_sync(0xffffffffu, sx, o);
     sy += __shfl_xor_sync(0xffffffffu, sy, o);
     sz += __shfl_xor_sync(0xffffffffu, sz, o);
@@ -232,7 +253,7 @@ __global__ void k_ewald_correction(Box box, int nexcl, const int *__restrict__ e
                                    const double *__restrict__ pos,
                                    const double *__restrict__ charge, double alpha,
                                    double csf, int n, long long *__restrict__ force,
-                                   long long *__restrict__ acc, int want_virial) {
+                                   long long *__restrict__ acc, int em) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
   if (k < nexcl) {
@@ -256,17 +277,18 @@ __global__ void k_ewald_correction(Box box, int nexcl, const int *__restrict__ e
     red_add(&force[a2], to_fixed(fx, kForceScale));
     red_add(&force[n + a2], to_fixed(fy, kForceScale));
     red_add(&force[2 * n + a2], to_fixed(fz, kForceScale));
-    if (want_virial) {
+    if (em == 2) {
       v[0] = fx * dx; v[1] = fx * dy; v[2] = fx * dz;
       v[3] = fy * dy; v[4] = fy * dz; v[5] = fz * dz;
     }
   }
+  if (!em) return;
   e = warp_sum(e);
-  if (want_virial)
+  if (em == 2)
     for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
   if ((threadIdx.x & 31) == 0) {
     red_add(&acc[ACC_COULOMB], to_fixed(e, kEnergyScale));
-    if (want_virial) {
+    if (em == 2) {
       const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
       for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
     }
@@ -323,12 +345,31 @@ int pme_init(System *s, Force *f) {
   PM_CUDA(cudaMalloc(&f->d_grid, sizeof(float) * nreal));
   PM_CUDA(cudaMalloc(&f->d_grid_fixed, sizeof(long long) * nreal));
   PM_CUDA(cudaMalloc(&f->d_cgrid, sizeof(float2) * ncplx));
-  for (int a = 0; a < 3; a++) {
-    std::vector<float> bm;
-    bspline_moduli(f->grid[a], f->order, bm);
-    PM_CUDA(cudaMalloc(&f->d_bsp_mod[a], sizeof(float) * bm.size()));
-    PM_CUDA(cudaMemcpy(f->d_bsp_mod[a], bm.data(), sizeof(float) * bm.size(),
-                       cudaMemcpyHostToDevice));
+  {
+    // influence function of the box (fixed for the life of the system)
+    std::vector<float> bm[3];
+    for (int a = 0; a < 3; a++) bspline_moduli(f->grid[a], f->order, bm[a]);
+    const int Kh = K2 / 2 + 1;
+    const double L0 = s->box.e[0], L1 = s->box.e[1], L2 = s->box.e[2], V = s->box.V;
+    const double pa = M_PI * M_PI / (f->alpha * f->alpha);
+    std::vector<float> g(ncplx);
+    for (int mx_ = 0; mx_ < K0; mx_++)
+      for (int my_ = 0; my_ < K1; my_++)
+        for (int mz = 0; mz < Kh; mz++) {
+          const int mx = mx_ <= K0 / 2 ? mx_ : mx_ - K0;
+          const int my = my_ <= K1 / 2 ? my_ : my_ - K1;
+          const size_t idx = ((size_t)mx_ * K1 + my_) * Kh + mz;
+          if (mx == 0 && my == 0 && mz == 0) {
+            g[idx] = 0.f;
+            continue;
+          }
+          const double hx = mx / L0, hy = my / L1, hz = mz / L2;
+          const double h2 = hx * hx + hy * hy + hz * hz;
+          g[idx] = (float)(std::exp(-pa * h2) / (M_PI * V * h2) * (double)bm[0][mx_] *
+                           (double)bm[1][my_] * (double)bm[2][mz]);
+        }
+    PM_CUDA(cudaMalloc(&f->d_influence, sizeof(float) * ncplx));
+    PM_CUDA(cudaMemcpy(f->d_influence, g.data(), sizeof(float) * ncplx, cudaMemcpyHostToDevice));
   }
   if (cufftPlan3d(&f->plan_r2c, K0, K1, K2, CUFFT_R2C) != CUFFT_SUCCESS ||
       cufftPlan3d(&f->plan_c2r, K0, K1, K2, CUFFT_C2R) != CUFFT_SUCCESS)
@@ -343,16 +384,42 @@ int pme_free(Force *f) {
   if (f->plan_r2c) cufftDestroy(f->plan_r2c);
   if (f->plan_c2r) cufftDestroy(f->plan_c2r);
   f->plan_r2c = f->plan_c2r = 0;
-  void *ptrs[] = {f->d_grid, f->d_grid_fixed, f->d_cgrid, f->d_bsp_mod[0],
-                  f->d_bsp_mod[1], f->d_bsp_mod[2]};
+  void *ptrs[] = {f->d_grid, f->d_grid_fixed, f->d_cgrid, f->d_influence};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   f->d_grid = nullptr; f->d_grid_fixed = nullptr; f->d_cgrid = nullptr;
-  for (int a = 0; a < 3; a++) f->d_bsp_mod[a] = nullptr;
+  f->d_influence = nullptr;
   return PMGPU_OK;
 }
 
-int pme_reciprocal(System *s, Force *f, int want_virial) {
+template <int P>
+static void launch_spread_gather(const PmeArgs &a, System *s, Force *f, const int *order_map,
+                                 int gather) {
+  constexpr int L = P <= 4 ? 4 : 8;
+  const int nb = (int)(((long long)a.n * L + 127) / 128);
+  if (!gather)
+    k_pme_spread<P, L><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
+                                                  f->d_grid_fixed);
+  else
+    k_pme_gather<P, L><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
+                                                  f->d_grid, s->d_force);
+}
+
+static void spread_gather(const PmeArgs &a, System *s, Force *f, const int *order_map,
+                          int gather) {
+  switch (f->order) {
+    case 2: launch_spread_gather<2>(a, s, f, order_map, gather); break;
+    case 3: launch_spread_gather<3>(a, s, f, order_map, gather); break;
+    case 4: launch_spread_gather<4>(a, s, f, order_map, gather); break;
+    case 5: launch_spread_gather<5>(a, s, f, order_map, gather); break;
+    case 6: launch_spread_gather<6>(a, s, f, order_map, gather); break;
+    case 7: launch_spread_gather<7>(a, s, f, order_map, gather); break;
+    default: launch_spread_gather<8>(a, s, f, order_map, gather); break;
+  }
+}
+
+// em: 0 forces only, 1 + energy, 2 + energy and virial.
+int pme_reciprocal(System *s, Force *f, int em) {
   int n = s->n;
   if (n == 0) return PMGPU_OK;
   PmeArgs a;
@@ -373,39 +440,26 @@ int pme_reciprocal(System *s, Force *f, int want_virial) {
       s->lists[f->list_index].built)
     order_map = s->lists[f->list_index].d_sorted;
   PM_CUDA(cudaMemsetAsync(f->d_grid_fixed, 0, sizeof(long long) * nreal, s->stream));
-  const int lanes = f->order <= 4 ? 4 : 8;
-  const int nb = (int)(((long long)n * lanes + 127) / 128);
-  if (lanes == 4)
-    k_pme_spread<4><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
-                                               f->d_grid_fixed);
-  else
-    k_pme_spread<8><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
-                                               f->d_grid_fixed);
+  spread_gather(a, s, f, order_map, 0);
   k_pme_fixed_to_float<<<(int)((nreal + 255) / 256), 256, 0, s->stream>>>(
       (int)nreal, f->d_grid_fixed, f->d_grid);
   if (cufftExecR2C(f->plan_r2c, f->d_grid, (cufftComplex *)f->d_cgrid) != CUFFT_SUCCESS)
     return fail(PMGPU_ERR_CUDA, "cufftExecR2C failed");
   k_pme_convolve<<<(int)((ncplx + 255) / 256), 256, 0, s->stream>>>(
-      K0, K1, K2, s->box.e[0], s->box.e[1], s->box.e[2], f->alpha, s->box.V,
-      f->d_bsp_mod[0], f->d_bsp_mod[1], f->d_bsp_mod[2], f->d_cgrid, s->d_acc,
-      want_virial);
+      K0, K1, K2, s->box.e[0], s->box.e[1], s->box.e[2], f->alpha, f->d_influence,
+      f->d_cgrid, s->d_acc, em);
   if (cufftExecC2R(f->plan_c2r, (cufftComplex *)f->d_cgrid, f->d_grid) != CUFFT_SUCCESS)
     return fail(PMGPU_ERR_CUDA, "cufftExecC2R failed");
-  if (lanes == 4)
-    k_pme_gather<4><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
-                                               f->d_grid, s->d_force);
-  else
-    k_pme_gather<8><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
-                                               f->d_grid, s->d_force);
+  spread_gather(a, s, f, order_map, 1);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
 
-int ewald_correction(System *s, Force *f, int want_virial) {
+int ewald_correction(System *s, Force *f, int em) {
   if (s->n_excl == 0) return PMGPU_OK;
   k_ewald_correction<<<(s->n_excl + 127) / 128, 128, 0, s->stream>>>(
       s->box, s->n_excl, s->d_excl_pairs, s->d_pos, s->d_charge, f->alpha,
-      s->coulomb_scaling, s->n, s->d_force, s->d_acc, want_virial);
+      s->coulomb_scaling, s->n, s->d_force, s->d_acc, em);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
