@@ -190,6 +190,37 @@ def algorithmic_bytes_per_step(n: int, grid: int) -> dict:
     return parts
 
 
+def served_line(args, ctx, world: int, rank: int) -> dict:
+    """Aggregate ns/day of the served (or batched) form beside the plain
+    form on the same requests: plain = one request at a time, served = up
+    to --slots requests in flight with continuous admission.  Every rank
+    serves its own seeded stream (replicas)."""
+    from protomol_b200 import serve
+    if args.mode == "served":
+        # 500-50,000 atoms log-uniform, 30 % single evaluations, 70 % Langevin
+        # segments; all requests queued at t = 0 (a saturating stream)
+        mk = lambda: serve.request_stream(args.requests, 7 + rank, steps=args.md_steps)
+        workload = (f"served stream: {args.requests} requests, TIP3P boxes of 500-50,000 atoms "
+                    f"(log-uniform), 30% energy+force evaluations, 70% {args.md_steps}-step "
+                    f"LangevinLeapfrog segments (1 fs, 5/ps, 300 K), PME order 4 spacing <= 1 A, "
+                    f"rc 9 A")
+    else:
+        steps = 50
+        mk = lambda: serve.ensemble(args.requests, 9 + rank, steps=steps)
+        workload = (f"batched ensemble: {args.requests} TIP3P boxes of 100-1,000 waters "
+                    f"(log-uniform), 0.0334 waters/A^3, one {steps}-step leapfrog segment each, "
+                    f"PME order 4 spacing <= 1 A, rc 9 A")
+    serve.execute(ctx, serve.Request(rid=-1, n_waters=300, seed=1, steps=20))  # warm-up
+    plain = serve.Server(ctx, slots=1).run(mk(), realtime=False)
+    served = serve.Server(ctx, slots=args.slots).run(mk(), realtime=False)
+    return {"metric": "ns/day (" + args.mode + " form)", "impl": "pmgpu", "mode": args.mode,
+            "value": served["ns_per_day"] * world, "unit": "ns/day", "n_gpus": world,
+            "higher_is_better": True, "scaling": "weak", "data": "synthetic",
+            "config": {"workload": workload, "replicas": world},
+            "served": served, "plain": plain,
+            "served_over_plain": served["ns_per_day"] / max(plain["ns_per_day"], 1e-30)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,9 +228,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pmgpu", choices=["pmgpu", "reference"])
     ap.add_argument("--segment", type=int, default=SEGMENT)
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile"],
-                    help="profile: run --steps single MD steps eagerly and exit "
-                         "(a plain workload for ncu captures)")
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "served", "batched"],
+                    help="profile: warm-up segments, then --steps MD steps between "
+                         "cudaProfilerStart/Stop (for ncu); served: a mixed request stream "
+                         "served plain (one slot) and with continuous batching; batched: "
+                         "an ensemble of small boxes, one MD segment each")
+    ap.add_argument("--requests", type=int, default=48,
+                    help="served/batched: requests (boxes) in the stream")
+    ap.add_argument("--slots", type=int, default=32,
+                    help="served/batched: requests in flight at once")
+    ap.add_argument("--md-steps", type=int, default=1000,
+                    help="served: MD steps per segment request (batched: 50)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -240,8 +279,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from protomol_b200 import Context, ForceFactory, GpuSystem, LeapfrogIntegrator
 
-    sysm = build_system(SEED + rank)
     ctx = Context(local)
+    if args.mode in ("served", "batched"):
+        print(json.dumps(served_line(args, ctx, world, rank)), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    sysm = build_system(SEED + rank)
     gs = GpuSystem(ctx, sysm, "mixed")
     ff = ForceFactory(gs, RC)
     for line in gpu_force_lines():

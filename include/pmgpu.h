@@ -251,6 +251,26 @@ typedef struct {
  * evaluates the initial forces first, as Integrator::initialize does. */
 int pmgpu_run(pmgpu_system *sys, const pmgpu_integrator *integ, long n_steps);
 
+/* ---- asynchronous segments (serving many systems at once) ----------- */
+/* pmgpu_run split in two: pmgpu_run_async enqueues the segment on the
+ * system's stream and returns at once; pmgpu_run_wait waits for it and
+ * returns what pmgpu_run would have (a list overflow found there re-runs
+ * the segment from its start before returning).  pmgpu_run_query sets
+ * *done without blocking.  Every other call on the system first waits for
+ * a pending segment.  Segments of different systems run concurrently on
+ * the device.  No counterpart in the reference (ProtoMol runs one system
+ * per process). */
+int pmgpu_run_async(pmgpu_system *sys, const pmgpu_integrator *integ, long n_steps);
+int pmgpu_run_query(pmgpu_system *sys, int *done);
+int pmgpu_run_wait(pmgpu_system *sys);
+/* Free and total device memory of the context's GPU (admission control). */
+int pmgpu_mem_info(pmgpu_context *ctx, long long *free_bytes, long long *total_bytes);
+/* Estimated device bytes of a periodic system of n_atoms with edges
+ * box[3], a pair list of the given reach (cutoff + skin; 0: none) and a
+ * PME grid (NULL: none). */
+int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
+                             const int grid[3], long long *bytes);
+
 /* ---- diagnostics ---------------------------------------------------- */
 typedef struct {
   long long pairs_in_cutoff;   /* pairs that passed the cutoff test */

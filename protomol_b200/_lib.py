@@ -37,7 +37,8 @@ EXPORTED = [
     "pmgpu_force_set_enabled", "pmgpu_evaluate", "pmgpu_force_evaluate", "pmgpu_run",
     "pmgpu_set_count_pairs", "pmgpu_force_stats", "pmgpu_debug_cell_assign",
     "pmgpu_debug_pair_set", "pmgpu_profile_enable", "pmgpu_profile_read",
-    "pmgpu_kernel_count", "pmgpu_gb_forces_noalloc",
+    "pmgpu_kernel_count", "pmgpu_gb_forces_noalloc", "pmgpu_run_async", "pmgpu_run_query",
+    "pmgpu_run_wait", "pmgpu_mem_info", "pmgpu_footprint_estimate",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -122,6 +123,11 @@ def load() -> C.CDLL:
     lib.pmgpu_profile_enable.argtypes = [vp, i32]
     lib.pmgpu_profile_read.argtypes = [vp, vp, vp, i32]
     lib.pmgpu_kernel_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.pmgpu_run_async.argtypes = [vp, C.POINTER(Integrator), C.c_long]
+    lib.pmgpu_run_query.argtypes = [vp, C.POINTER(i32)]
+    lib.pmgpu_run_wait.argtypes = [vp]
+    lib.pmgpu_mem_info.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.pmgpu_footprint_estimate.argtypes = [i32, vp, dbl, vp, C.POINTER(C.c_longlong)]
     lib.pmgpu_gb_forces_noalloc.argtypes = [i32, vp, vp, vp, vp, vp, vp, C.POINTER(dbl),
                                             dbl, dbl, i32, vp, vp, vp]
     _lib = lib

@@ -144,20 +144,38 @@ static int validate_switch(const pmgpu_switch *sw, const char *what) {
   }
 }
 
+int dev_alloc(System *s, void **p, size_t bytes) {
+  cudaError_t e = cudaMallocAsync(p, std::max<size_t>(bytes, 1), s->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(e == cudaErrorMemoryAllocation ? PMGPU_ERR_OOM : PMGPU_ERR_CUDA,
+                std::string("device allocation of ") + std::to_string(bytes) +
+                    " bytes: " + cudaGetErrorString(e));
+  }
+  return PMGPU_OK;
+}
+
+void dev_free(System *s, void *p) {
+  if (p) cudaFreeAsync(p, s->stream);
+}
+
+// Allocates count elements on the system's stream and fills them from h
+// (or with zeros).
 template <typename T>
-static int upload(T **d, const T *h, size_t count) {
+static int upload(System *s, T **d, const T *h, size_t count) {
   if (count == 0) count = 1;
-  PM_CUDA(cudaMalloc(d, sizeof(T) * count));
-  if (h) PM_CUDA(cudaMemcpy(*d, h, sizeof(T) * count, cudaMemcpyHostToDevice));
-  else PM_CUDA(cudaMemset(*d, 0, sizeof(T) * count));
+  PM_CHECK(dev_alloc(s, d, sizeof(T) * count));
+  if (h) PM_CUDA(cudaMemcpyAsync(*d, h, sizeof(T) * count, cudaMemcpyHostToDevice, s->stream));
+  else PM_CUDA(cudaMemsetAsync(*d, 0, sizeof(T) * count, s->stream));
   return PMGPU_OK;
 }
 
 static int system_free(System *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
-  for (auto &f : s->forces) pme_free(&f);
-  for (auto &nl : s->lists) nb_list_free(&nl);
+  for (auto &f : s->forces) pme_free(s, &f);
+  for (auto &nl : s->lists) nb_list_free(s, &nl);
   void *ptrs[] = {s->d_charge, s->d_mass, s->d_type, s->d_mol, s->d_lj32, s->d_lj64,
                   s->d_excl_start, s->d_excl_partner, s->d_excl_class, s->d_excl_pairs,
                   s->d_bond_atoms, s->d_angle_atoms, s->d_bond_params, s->d_angle_params,
@@ -167,8 +185,8 @@ static int system_free(System *s) {
                   s->d_stage, s->d_snap, s->d_step};
   for (auto &g : s->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
+  for (void *p : ptrs) dev_free(s, p);
+  if (s->stream) cudaStreamSynchronize(s->stream);
   if (s->h_acc) cudaFreeHost(s->h_acc);
   if (s->h_status) cudaFreeHost(s->h_status);
   if (s->h_stage) cudaFreeHost(s->h_stage);
@@ -248,6 +266,7 @@ static int add_pair_terms(std::vector<Launch> &groups, int list, const PairTerms
       g.terms.exact_erf = t.exact_erf;
     }
     g.terms.mask |= t.mask;
+    g.terms.minimal_image |= t.minimal_image;
     return 0;
   }
   groups.push_back({list, t});
@@ -364,7 +383,7 @@ static int read_results(System *s, int only, double *energies, double *virial, i
       // and no output is touched.
       for (auto &nl : s->lists) {
         int cap = nl.cap * 2;
-        nb_list_free(&nl);
+        nb_list_free(s, &nl);
         nl.cap = cap;
         PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
         s->graph_version++;  // captured graphs hold the old list buffers
@@ -411,6 +430,8 @@ using namespace pmgpu;
 // ===================================================================== ABI
 extern "C" {
 
+static int run_finish(System *s);
+
 const char *pmgpu_last_error(void) { return g_last_error.c_str(); }
 int pmgpu_abi_version(void) { return PMGPU_ABI_VERSION; }
 
@@ -424,6 +445,13 @@ int pmgpu_context_create(int device, pmgpu_context **out) {
   PM_CUDA(cudaGetDeviceProperties(&prop, device));
   if (prop.major < 10)
     return fail(PMGPU_ERR_UNSUPPORTED, "libpmgpu is built for sm_100a (Blackwell B200)");
+  // Stream-ordered allocations of freed systems stay in this process's
+  // default pool for the next system instead of going back to the driver.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   auto *c = new pmgpu_context();
   c->device = device;
   *out = c;
@@ -467,10 +495,10 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   s->coulomb_scaling = t->coulomb_scaling;
   PM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   size_t nn = std::max(1, n);
-  PM_CHECK(upload(&s->d_charge, t->charge, n));
-  PM_CHECK(upload(&s->d_mass, t->mass, n));
-  PM_CHECK(upload(&s->d_type, t->type, n));
-  PM_CHECK(upload(&s->d_mol, t->molecule, n));
+  PM_CHECK(upload(s.get(), &s->d_charge, t->charge, n));
+  PM_CHECK(upload(s.get(), &s->d_mass, t->mass, n));
+  PM_CHECK(upload(s.get(), &s->d_type, t->type, n));
+  PM_CHECK(upload(s.get(), &s->d_mol, t->molecule, n));
   int nt2 = t->n_types * t->n_types;
   std::vector<float4> lj32(nt2);
   std::vector<double4> lj64(nt2);
@@ -479,8 +507,8 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
     lj32[k] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3]);
     lj64[k] = make_double4(p[0], p[1], p[2], p[3]);
   }
-  PM_CHECK(upload(&s->d_lj32, lj32.data(), nt2));
-  PM_CHECK(upload(&s->d_lj64, lj64.data(), nt2));
+  PM_CHECK(upload(s.get(), &s->d_lj32, lj32.data(), nt2));
+  PM_CHECK(upload(s.get(), &s->d_lj64, lj64.data(), nt2));
   // exclusion table as CSR over both atoms of each pair
   int ne = std::max(0, t->n_exclusions);
   std::vector<int> start(n + 1, 0), partner(2 * (size_t)ne + 1), cls(2 * (size_t)ne + 1);
@@ -498,9 +526,9 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
     partner[cur[a]] = b; cls[cur[a]++] = c;
     partner[cur[b]] = a; cls[cur[b]++] = c;
   }
-  PM_CHECK(upload(&s->d_excl_start, start.data(), n + 1));
-  PM_CHECK(upload(&s->d_excl_partner, partner.data(), 2 * (size_t)ne + 1));
-  PM_CHECK(upload(&s->d_excl_class, cls.data(), 2 * (size_t)ne + 1));
+  PM_CHECK(upload(s.get(), &s->d_excl_start, start.data(), n + 1));
+  PM_CHECK(upload(s.get(), &s->d_excl_partner, partner.data(), 2 * (size_t)ne + 1));
+  PM_CHECK(upload(s.get(), &s->d_excl_class, cls.data(), 2 * (size_t)ne + 1));
   // The correction term iterates the table with the class each entry holds.
   std::vector<int> table(3 * (size_t)ne + 3);
   for (int k = 0; k < ne; k++) {
@@ -509,7 +537,7 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
     table[3 * k + 2] = t->exclusion_table_class ? t->exclusion_table_class[k]
                                                 : t->exclusions[3 * k + 2];
   }
-  PM_CHECK(upload(&s->d_excl_pairs, table.data(), 3 * (size_t)ne));
+  PM_CHECK(upload(s.get(), &s->d_excl_pairs, table.data(), 3 * (size_t)ne));
   s->n_excl = ne;
   s->n_bonds = std::max(0, t->n_bonds);
   s->n_angles = std::max(0, t->n_angles);
@@ -517,27 +545,28 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
     return fail(PMGPU_ERR_ARG, "bond arrays missing");
   if (s->n_angles && (!t->angle_atoms || !t->angle_params))
     return fail(PMGPU_ERR_ARG, "angle arrays missing");
-  PM_CHECK(upload(&s->d_bond_atoms, s->n_bonds ? t->bond_atoms : (const int *)nullptr, 2 * (size_t)s->n_bonds));
-  PM_CHECK(upload(&s->d_bond_params, s->n_bonds ? t->bond_params : (const double *)nullptr, 2 * (size_t)s->n_bonds));
-  PM_CHECK(upload(&s->d_angle_atoms, s->n_angles ? t->angle_atoms : (const int *)nullptr, 3 * (size_t)s->n_angles));
-  PM_CHECK(upload(&s->d_angle_params, s->n_angles ? t->angle_params : (const double *)nullptr, 4 * (size_t)s->n_angles));
+  PM_CHECK(upload(s.get(), &s->d_bond_atoms, s->n_bonds ? t->bond_atoms : (const int *)nullptr, 2 * (size_t)s->n_bonds));
+  PM_CHECK(upload(s.get(), &s->d_bond_params, s->n_bonds ? t->bond_params : (const double *)nullptr, 2 * (size_t)s->n_bonds));
+  PM_CHECK(upload(s.get(), &s->d_angle_atoms, s->n_angles ? t->angle_atoms : (const int *)nullptr, 3 * (size_t)s->n_angles));
+  PM_CHECK(upload(s.get(), &s->d_angle_params, s->n_angles ? t->angle_params : (const double *)nullptr, 4 * (size_t)s->n_angles));
   if (t->gb_vdwr && t->gb_scale && t->gb_offset) {
-    PM_CHECK(upload(&s->d_gb_vdwr, t->gb_vdwr, n));
-    PM_CHECK(upload(&s->d_gb_scale, t->gb_scale, n));
-    PM_CHECK(upload(&s->d_gb_offset, t->gb_offset, n));
+    PM_CHECK(upload(s.get(), &s->d_gb_vdwr, t->gb_vdwr, n));
+    PM_CHECK(upload(s.get(), &s->d_gb_scale, t->gb_scale, n));
+    PM_CHECK(upload(s.get(), &s->d_gb_offset, t->gb_offset, n));
     for (int k = 0; k < 3; k++) s->gb_obc[k] = t->gb_obc[k];
   }
-  if (t->water) PM_CHECK(upload(&s->d_water, t->water, n));
-  PM_CHECK(upload(&s->d_pos, (const double *)nullptr, 3 * nn));
-  PM_CHECK(upload(&s->d_vel, (const double *)nullptr, 3 * nn));
-  PM_CHECK(upload(&s->d_force, (const long long *)nullptr, 3 * nn));
-  PM_CHECK(upload(&s->d_acc, (const long long *)nullptr, ACC_COUNT));
-  PM_CHECK(upload(&s->d_status, (const int *)nullptr, 1));
-  PM_CHECK(upload(&s->d_step, (const unsigned long long *)nullptr, 1));
-  PM_CHECK(upload(&s->d_stage, (const double *)nullptr, 3 * nn));
+  if (t->water) PM_CHECK(upload(s.get(), &s->d_water, t->water, n));
+  PM_CHECK(upload(s.get(), &s->d_pos, (const double *)nullptr, 3 * nn));
+  PM_CHECK(upload(s.get(), &s->d_vel, (const double *)nullptr, 3 * nn));
+  PM_CHECK(upload(s.get(), &s->d_force, (const long long *)nullptr, 3 * nn));
+  PM_CHECK(upload(s.get(), &s->d_acc, (const long long *)nullptr, ACC_COUNT));
+  PM_CHECK(upload(s.get(), &s->d_status, (const int *)nullptr, 1));
+  PM_CHECK(upload(s.get(), &s->d_step, (const unsigned long long *)nullptr, 1));
+  PM_CHECK(upload(s.get(), &s->d_stage, (const double *)nullptr, 3 * nn));
   PM_CUDA(cudaMallocHost(&s->h_acc, sizeof(long long) * ACC_COUNT));
   PM_CUDA(cudaMallocHost(&s->h_status, sizeof(int)));
   PM_CUDA(cudaMallocHost(&s->h_stage, sizeof(double) * 3 * nn));
+  PM_CUDA(cudaStreamSynchronize(s->stream));
   s->h_charge.assign(t->charge, t->charge + n);
   *out = reinterpret_cast<pmgpu_system *>(s.release());
   return PMGPU_OK;
@@ -575,6 +604,7 @@ static int copy_out(System *s, double *dst, const double *src) {
 int pmgpu_system_set_positions(pmgpu_system *h, const double *pos) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   PM_CHECK(copy_in(s, s->d_pos, pos));
   s->forces_valid = 0;
@@ -583,18 +613,21 @@ int pmgpu_system_set_positions(pmgpu_system *h, const double *pos) {
 int pmgpu_system_get_positions(pmgpu_system *h, double *pos) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   return copy_out(s, pos, s->d_pos);
 }
 int pmgpu_system_set_velocities(pmgpu_system *h, const double *vel) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   return copy_in(s, s->d_vel, vel);
 }
 int pmgpu_system_get_velocities(pmgpu_system *h, double *vel) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   return copy_out(s, vel, s->d_vel);
 }
@@ -602,6 +635,7 @@ int pmgpu_system_get_velocities(pmgpu_system *h, double *vel) {
 int pmgpu_system_get_forces(pmgpu_system *h, double *forces) {
   if (!h || !forces) return fail(PMGPU_ERR_ARG, "null argument");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   return forces_to_host(s, forces, 0);
 }
@@ -609,6 +643,7 @@ int pmgpu_system_get_forces(pmgpu_system *h, double *forces) {
 int pmgpu_system_get_energies(pmgpu_system *h, double *energies, double *virial) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   if (energies)
     for (int k = 0; k < PMGPU_E_COUNT; k++) energies[k] = s->last_energy[k];
   if (virial)
@@ -635,7 +670,7 @@ static int list_for(System *s, double cutoff, double skin) {
   NeighborList nl;
   int r = nb_list_init(s, &nl, cutoff, skin, 0);
   if (r != PMGPU_OK) {
-    nb_list_free(&nl);
+    nb_list_free(s, &nl);
     return -r;
   }
   s->lists.push_back(nl);
@@ -643,6 +678,7 @@ static int list_for(System *s, double cutoff, double skin) {
 }
 
 static int add_force(System *s, Force &f, int *force_id) {
+  PM_CHECK(run_finish(s));
   f.id = (int)s->forces.size();
   s->forces.push_back(f);
   if (force_id) *force_id = f.id;
@@ -668,6 +704,7 @@ int pmgpu_force_cutoff_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
                            double cellsize, int *force_id) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   if (!lj_sw && !coul_sw) return fail(PMGPU_ERR_ARG, "need LennardJones and/or Coulomb");
   PM_CHECK(validate_switch(lj_sw, "LennardJones"));
@@ -708,10 +745,12 @@ int pmgpu_force_cutoff_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
   double rc = std::sqrt(c2max);
   if (s->box.periodic) {
     double emin = std::min(s->box.e[0], std::min(s->box.e[1], s->box.e[2]));
-    if (2 * rc > emin)
-      return fail(PMGPU_ERR_UNSUPPORTED,
-                  "cutoff forces need box edges of at least twice the cutoff "
-                  "(minimal-image pairs)");
+    if (rc >= emin)
+      return fail(PMGPU_ERR_UNSUPPORTED, "cutoff forces need box edges longer than the cutoff");
+    // Below twice the cutoff a pair can be inside it under two images; the
+    // reference's minimalDifference (PeriodicBoundaryConditions.h:72-110)
+    // keeps only the minimal one, and so does the pair kernel.
+    f.terms.minimal_image = 2 * rc > emin;
   }
   int li = list_for(s, rc, default_skin(s, rc));
   if (li < 0) return -li;
@@ -722,6 +761,7 @@ int pmgpu_force_cutoff_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
 int pmgpu_force_simplefull_add(pmgpu_system *h, int lj, int coulomb, int *force_id) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   if (s->box.periodic)
     return fail(PMGPU_ERR_UNSUPPORTED, "NonbondedSimpleFull is the vacuum all-pairs path");
   if (!lj && !coulomb) return fail(PMGPU_ERR_ARG, "need LennardJones and/or Coulomb");
@@ -737,6 +777,7 @@ int pmgpu_force_pme_add(pmgpu_system *h, double alpha, double rc, int order,
                         int *force_id) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   if (!s->box.periodic) return fail(PMGPU_ERR_UNSUPPORTED, "PME needs a periodic box");
   if (!(alpha > 0)) return fail(PMGPU_ERR_ARG, "alpha must be > 0");
@@ -778,6 +819,7 @@ int pmgpu_force_pme_add(pmgpu_system *h, double alpha, double rc, int order,
 int pmgpu_force_gb_add(pmgpu_system *h, double solute, double solvent, int *force_id) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   if (s->box.periodic) return fail(PMGPU_ERR_UNSUPPORTED, "GB is the vacuum all-pairs path");
   if (!(solute > 0) || !(solvent > 0)) return fail(PMGPU_ERR_ARG, "dielectrics must be > 0");
@@ -801,6 +843,7 @@ int pmgpu_force_bonded_add(pmgpu_system *h, int bonds, int angles, int *force_id
 int pmgpu_force_set_enabled(pmgpu_system *h, int id, int enabled) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
   s->forces[id].enabled = enabled ? 1 : 0;
   s->graph_version++;
@@ -811,6 +854,7 @@ int pmgpu_force_set_enabled(pmgpu_system *h, int id, int enabled) {
 int pmgpu_evaluate(pmgpu_system *h, double *energies, double *virial) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   int r = with_overflow_retry([&]() {
     PM_CHECK(zero_forces(s));
@@ -826,6 +870,7 @@ int pmgpu_force_evaluate(pmgpu_system *h, int id, const double *pos, double *for
                          double *energies, double *virial) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
   if (pos) PM_CHECK(copy_in(s, s->d_pos, pos));
@@ -900,78 +945,191 @@ static int run_graph(System *s, const pmgpu_integrator *it, long g, int *used) {
   return PMGPU_OK;
 }
 
-// Integrator::run(n) on the device.  Forces of the current positions are
+// Integrator::run(n) on the device, split into the part that only enqueues
+// work on the system's stream (run_enqueue) and the part that waits for it
+// and checks the status (run_finish).  Forces of the current positions are
 // kept resident between calls (ProtoMol keeps myForces between run calls);
 // the first call after positions changed on the host evaluates them, like
 // Integrator::initialize (StandardIntegrator.cpp:39-43).
-int pmgpu_run(pmgpu_system *h, const pmgpu_integrator *it, long n_steps) {
-  if (!h || !it) return fail(PMGPU_ERR_ARG, "null argument");
-  System *s = sysp(h);
-  PM_CUDA(cudaSetDevice(s->device));
+static int check_integrator(const pmgpu_integrator *it) {
   if (!(it->timestep_fs > 0)) return fail(PMGPU_ERR_ARG, "timestep must be > 0");
   if (it->kind != PMGPU_INT_LEAPFROG && it->kind != PMGPU_INT_LANGEVIN_LEAPFROG)
     return fail(PMGPU_ERR_ARG, "unknown integrator");
   if (it->kind == PMGPU_INT_LANGEVIN_LEAPFROG && !(it->gamma_ps > 0))
     return fail(PMGPU_ERR_ARG, "LangevinLeapfrog needs gamma > 0");
-  if (n_steps < 1) return PMGPU_OK;
-  // A neighbour list that overflows mid-segment is only seen at the end of
-  // the segment (no host synchronisation per step): the segment then rolls
-  // back to this snapshot and runs again with the grown capacity.
+  return PMGPU_OK;
+}
+
+// Snapshot of the state a segment starts from: a neighbour list that
+// overflows mid-segment is only seen at the end of the segment (no host
+// synchronisation per step), and the segment then runs again from here
+// with the grown capacity.
+static int run_snapshot(System *s, int restore) {
   size_t n3 = 3 * (size_t)std::max(1, s->n);
-  if (!s->d_snap) PM_CUDA(cudaMalloc(&s->d_snap, n3 * (2 * sizeof(double) + sizeof(long long))));
+  if (!s->d_snap) PM_CHECK(dev_alloc(s, &s->d_snap, n3 * (2 * sizeof(double) + sizeof(long long))));
   double *snap_pos = reinterpret_cast<double *>(s->d_snap);
   double *snap_vel = snap_pos + n3;
   long long *snap_f = reinterpret_cast<long long *>(snap_vel + n3);
-  const uint64_t step0 = s->step;
-  const int valid0 = s->forces_valid;
-  PM_CUDA(cudaMemcpyAsync(snap_pos, s->d_pos, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-  PM_CUDA(cudaMemcpyAsync(snap_vel, s->d_vel, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-  PM_CUDA(cudaMemcpyAsync(snap_f, s->d_force, n3 * sizeof(long long), cudaMemcpyDeviceToDevice, s->stream));
-  bool lang = it->kind == PMGPU_INT_LANGEVIN_LEAPFROG;
+  const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+  if (!restore) {
+    PM_CUDA(cudaMemcpyAsync(snap_pos, s->d_pos, n3 * sizeof(double), k, s->stream));
+    PM_CUDA(cudaMemcpyAsync(snap_vel, s->d_vel, n3 * sizeof(double), k, s->stream));
+    PM_CUDA(cudaMemcpyAsync(snap_f, s->d_force, n3 * sizeof(long long), k, s->stream));
+  } else {
+    PM_CUDA(cudaMemcpyAsync(s->d_pos, snap_pos, n3 * sizeof(double), k, s->stream));
+    PM_CUDA(cudaMemcpyAsync(s->d_vel, snap_vel, n3 * sizeof(double), k, s->stream));
+    PM_CUDA(cudaMemcpyAsync(s->d_force, snap_f, n3 * sizeof(long long), k, s->stream));
+  }
+  return PMGPU_OK;
+}
+
+static int run_enqueue(System *s, const pmgpu_integrator *it, long n_steps) {
+  const bool lang = it->kind == PMGPU_INT_LANGEVIN_LEAPFROG;
+  PM_CHECK(set_device_step(s));
+  if (!s->forces_valid) {
+    PM_CHECK(zero_forces(s));
+    PM_CHECK(begin_eval(s));
+    PM_CHECK(evaluate_forces(s, -1, PAIR_FORCE));
+  }
+  for (long k = 0; k < n_steps;) {
+    // Inner steps (not the first, not the last) replay a captured graph
+    // of several steps when possible; the rest run eagerly.
+    const long inner_left = (n_steps - 1) - k;
+    if (k > 0 && inner_left > 0 && !s->prof.enabled && !s->graphs_disabled) {
+      const long g = inner_left >= kGraphSteps ? kGraphSteps : 1;
+      int used = 0;
+      PM_CHECK(run_graph(s, it, g, &used));
+      if (used) {
+        s->step += g;
+        k += g;
+        continue;
+      }
+    }
+    int phase = lang ? (k == 0 ? 3 : 4) : (k == 0 ? 0 : 1);
+    PM_CHECK(one_step(s, it, phase, k + 1 == n_steps ? PAIR_ENERGY : PAIR_FORCE));
+    s->step++;
+    k++;
+  }
+  prof_begin(s, PMGPU_PHASE_INTEGRATE);
+  int ri = integrate_kick_drift(s, it, lang ? 5 : 2);
+  prof_end(s);
+  PM_CHECK(ri);
+  s->kernels += s->n > 0;
+  return PMGPU_OK;
+}
+
+static int run_start(System *s, const pmgpu_integrator *it, long n_steps) {
+  s->pending.integ = *it;
+  s->pending.n_steps = n_steps;
+  s->pending.step0 = s->step;
+  s->pending.valid0 = s->forces_valid;
+  s->pending.active = 1;
+  PM_CHECK(run_snapshot(s, 0));
+  return run_enqueue(s, it, n_steps);
+}
+
+// Waits for the pending segment; on a list overflow (capacity already
+// doubled by read_results) restores the snapshot and runs the segment
+// again, at most three attempts in all.
+static int run_finish(System *s) {
+  if (!s->pending.active) return PMGPU_OK;
+  PM_CUDA(cudaSetDevice(s->device));
   int r = PMGPU_OK;
   for (int attempt = 0; attempt < 3; attempt++) {
     if (attempt > 0) {
-      PM_CUDA(cudaMemcpyAsync(s->d_pos, snap_pos, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-      PM_CUDA(cudaMemcpyAsync(s->d_vel, snap_vel, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-      PM_CUDA(cudaMemcpyAsync(s->d_force, snap_f, n3 * sizeof(long long), cudaMemcpyDeviceToDevice, s->stream));
-      s->step = step0;
-      s->forces_valid = valid0;
+      PM_CHECK(run_snapshot(s, 1));
+      s->step = s->pending.step0;
+      s->forces_valid = s->pending.valid0;
+      PM_CHECK(run_enqueue(s, &s->pending.integ, s->pending.n_steps));
     }
-    PM_CHECK(set_device_step(s));
-    if (!s->forces_valid) {
-      PM_CHECK(zero_forces(s));
-      PM_CHECK(begin_eval(s));
-      PM_CHECK(evaluate_forces(s, -1, PAIR_FORCE));
-    }
-    for (long k = 0; k < n_steps;) {
-      // Inner steps (not the first, not the last) replay a captured graph
-      // of several steps when possible; the rest run eagerly.
-      const long inner_left = (n_steps - 1) - k;
-      if (k > 0 && inner_left > 0 && !s->prof.enabled && !s->graphs_disabled) {
-        const long g = inner_left >= kGraphSteps ? kGraphSteps : 1;
-        int used = 0;
-        PM_CHECK(run_graph(s, it, g, &used));
-        if (used) {
-          s->step += g;
-          k += g;
-          continue;
-        }
-      }
-      int phase = lang ? (k == 0 ? 3 : 4) : (k == 0 ? 0 : 1);
-      PM_CHECK(one_step(s, it, phase, k + 1 == n_steps ? PAIR_ENERGY : PAIR_FORCE));
-      s->step++;
-      k++;
-    }
-    prof_begin(s, PMGPU_PHASE_INTEGRATE);
-    int ri = integrate_kick_drift(s, it, lang ? 5 : 2);
-    prof_end(s);
-    PM_CHECK(ri);
-    s->kernels += s->n > 0;
     r = read_results(s, -1, nullptr, nullptr, 0);
     if (r != PMGPU_ERR_OVERFLOW) break;
   }
+  s->pending.active = 0;
   s->forces_valid = (r == PMGPU_OK);
   return r;
+}
+
+int pmgpu_run(pmgpu_system *h, const pmgpu_integrator *it, long n_steps) {
+  if (!h || !it) return fail(PMGPU_ERR_ARG, "null argument");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  PM_CHECK(check_integrator(it));
+  PM_CHECK(run_finish(s));  // a segment still pending from pmgpu_run_async
+  if (n_steps < 1) return PMGPU_OK;
+  PM_CHECK(run_start(s, it, n_steps));
+  return run_finish(s);
+}
+
+int pmgpu_run_async(pmgpu_system *h, const pmgpu_integrator *it, long n_steps) {
+  if (!h || !it) return fail(PMGPU_ERR_ARG, "null argument");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  PM_CHECK(check_integrator(it));
+  if (s->pending.active) return fail(PMGPU_ERR_STATE, "a segment is already pending");
+  if (n_steps < 1) return PMGPU_OK;
+  return run_start(s, it, n_steps);
+}
+
+int pmgpu_run_query(pmgpu_system *h, int *done) {
+  if (!h || !done) return fail(PMGPU_ERR_ARG, "null argument");
+  System *s = sysp(h);
+  if (!s->pending.active) {
+    *done = 1;
+    return PMGPU_OK;
+  }
+  PM_CUDA(cudaSetDevice(s->device));
+  cudaError_t e = cudaStreamQuery(s->stream);
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return PMGPU_OK;
+  }
+  if (e != cudaSuccess) return fail(PMGPU_ERR_CUDA, cudaGetErrorString(e));
+  *done = 1;
+  return PMGPU_OK;
+}
+
+int pmgpu_run_wait(pmgpu_system *h) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null argument");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  return run_finish(s);
+}
+
+int pmgpu_mem_info(pmgpu_context *ctx, long long *free_bytes, long long *total_bytes) {
+  if (!ctx || !free_bytes || !total_bytes) return fail(PMGPU_ERR_ARG, "null argument");
+  PM_CUDA(cudaSetDevice(ctx->device));
+  size_t f = 0, t = 0;
+  PM_CUDA(cudaMemGetInfo(&f, &t));
+  *free_bytes = (long long)f;
+  *total_bytes = (long long)t;
+  return PMGPU_OK;
+}
+
+// Device bytes a periodic system of n atoms and edge lengths box[3] needs
+// with a pair list of the given reach and a PME grid (grid may be NULL):
+// the resident state, the sorted coordinates, the list at its initial
+// capacity and the PME grids (cuFFT work areas are estimated as one more
+// complex grid).
+int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
+                             const int grid[3], long long *bytes) {
+  if (!box || !bytes || n_atoms < 0 || !(reach >= 0)) return fail(PMGPU_ERR_ARG, "bad argument");
+  const double n = std::max(1, n_atoms);
+  const double V = box[0] * box[1] * box[2];
+  double b = n * (24 * 3 + 24 + 24 + 8 + 8 + 8);        // pos, vel, snapshot, force, q, m, ids
+  b += n * (16 + 16 + 32 + 4 + 4 + 24 + 24 + 8);       // sorted coordinates, offsets, keys
+  if (reach > 0) {
+    double dens = V > 0 ? std::max(n / V, 0.12) : 0.15;
+    double cap = std::min(4.18879 * reach * reach * reach * dens * 1.5 + 64, n);
+    b += n * 4 * (cap + 32) + 4.0 * 64 * std::max(1.0, V / (reach * reach * reach));
+  }
+  if (grid) {
+    double G = (double)grid[0] * grid[1] * grid[2];
+    double Gc = (double)grid[0] * grid[1] * (grid[2] / 2 + 1);
+    b += G * (8 + 4) + Gc * (8 + 4) + Gc * 8;
+  }
+  *bytes = (long long)(b + (1 << 20));
+  return PMGPU_OK;
 }
 
 int pmgpu_profile_enable(pmgpu_system *h, int enabled) {
@@ -1012,6 +1170,7 @@ int pmgpu_set_count_pairs(pmgpu_system *h, int enabled) {
 int pmgpu_force_stats(pmgpu_system *h, int id, pmgpu_stats *out) {
   if (!h || !out) return fail(PMGPU_ERR_ARG, "null argument");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
   std::memset(out, 0, sizeof(*out));
   const Force &f = s->forces[id];
@@ -1022,12 +1181,14 @@ int pmgpu_force_stats(pmgpu_system *h, int id, pmgpu_stats *out) {
     out->cells[1] = nl.ncy;
     out->cells[2] = nl.ncz;
     int rb[2] = {0, 0};
-    PM_CUDA(cudaMemcpy(rb, nl.d_rebuild, sizeof(rb), cudaMemcpyDeviceToHost));
+    PM_CUDA(cudaMemcpyAsync(rb, nl.d_rebuild, sizeof(rb), cudaMemcpyDeviceToHost, s->stream));
+    PM_CUDA(cudaStreamSynchronize(s->stream));
     out->list_builds = rb[1];
     std::vector<int> cnt(s->n);
     if (s->n) {
-      PM_CUDA(cudaMemcpy(cnt.data(), nl.d_nbr_count, sizeof(int) * s->n,
-                         cudaMemcpyDeviceToHost));
+      PM_CUDA(cudaMemcpyAsync(cnt.data(), nl.d_nbr_count, sizeof(int) * s->n,
+                              cudaMemcpyDeviceToHost, s->stream));
+      PM_CUDA(cudaStreamSynchronize(s->stream));
       long long tot = 0;
       for (int c : cnt) tot += c;
       out->list_entries = tot;
@@ -1040,6 +1201,7 @@ int pmgpu_debug_cell_assign(pmgpu_system *h, double cellsize, int *cell_xyz, int
   if (!h || !cell_xyz || !dims) return fail(PMGPU_ERR_ARG, "null argument");
   if (!(cellsize > 0)) return fail(PMGPU_ERR_ARG, "cellsize must be > 0");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   return nb_debug_cells(s, cellsize, cell_xyz, dims);
 }
@@ -1048,17 +1210,18 @@ int pmgpu_debug_pair_set(pmgpu_system *h, int id, int *pairs, long long cap,
                          long long *count) {
   if (!h || !count) return fail(PMGPU_ERR_ARG, "null argument");
   System *s = sysp(h);
+  PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
   Force &f = s->forces[id];
   if (f.list_index < 0) return fail(PMGPU_ERR_ARG, "force has no pair list");
   long long want = std::max(1LL, cap);
   if (s->pairbuf_cap < want) {
-    if (s->d_pairbuf) cudaFree(s->d_pairbuf);
-    PM_CUDA(cudaMalloc(&s->d_pairbuf, sizeof(long long) * want));
+    dev_free(s, s->d_pairbuf);
+    PM_CHECK(dev_alloc(s, &s->d_pairbuf, sizeof(long long) * want));
     s->pairbuf_cap = want;
   }
-  if (!s->d_paircount) PM_CUDA(cudaMalloc(&s->d_paircount, sizeof(long long)));
+  if (!s->d_paircount) PM_CHECK(dev_alloc(s, &s->d_paircount, sizeof(long long)));
   PM_CUDA(cudaMemsetAsync(s->d_paircount, 0, sizeof(long long), s->stream));
   PM_CHECK(zero_forces(s));
   PM_CHECK(begin_eval(s));
@@ -1072,8 +1235,9 @@ int pmgpu_debug_pair_set(pmgpu_system *h, int id, int *pairs, long long cap,
   long long ncopy = std::min(total, cap);
   if (pairs && ncopy > 0) {
     std::vector<long long> buf(ncopy);
-    PM_CUDA(cudaMemcpy(buf.data(), s->d_pairbuf, sizeof(long long) * ncopy,
-                       cudaMemcpyDeviceToHost));
+    PM_CUDA(cudaMemcpyAsync(buf.data(), s->d_pairbuf, sizeof(long long) * ncopy,
+                            cudaMemcpyDeviceToHost, s->stream));
+    PM_CUDA(cudaStreamSynchronize(s->stream));
     for (long long k = 0; k < ncopy; k++) {
       pairs[2 * k] = (int)(buf[k] >> 32);
       pairs[2 * k + 1] = (int)(buf[k] & 0xffffffffLL);

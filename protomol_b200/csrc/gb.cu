@@ -267,11 +267,11 @@ int gb_init(System *s) {
   int n = std::max(1, s->n);
   if (!s->d_gb_vdwr) return fail(PMGPU_ERR_ARG, "GB force needs gb_vdwr/gb_scale/gb_offset");
   if (!s->d_gb_born) {
-    PM_CUDA(cudaMalloc(&s->d_gb_born, sizeof(double) * n));
-    PM_CUDA(cudaMalloc(&s->d_gb_psi, sizeof(double) * n));
-    PM_CUDA(cudaMalloc(&s->d_gb_partial, sizeof(double) * n));
-    PM_CUDA(cudaMalloc(&s->d_gb_fixed, sizeof(long long) * 2 * n));
-    PM_CUDA(cudaMemset(s->d_gb_fixed, 0, sizeof(long long) * 2 * n));
+    PM_CHECK(dev_alloc(s, &s->d_gb_born, sizeof(double) * n));
+    PM_CHECK(dev_alloc(s, &s->d_gb_psi, sizeof(double) * n));
+    PM_CHECK(dev_alloc(s, &s->d_gb_partial, sizeof(double) * n));
+    PM_CHECK(dev_alloc(s, &s->d_gb_fixed, sizeof(long long) * 2 * n));
+    PM_CUDA(cudaMemsetAsync(s->d_gb_fixed, 0, sizeof(long long) * 2 * n, s->stream));
   }
   (void)g_dummy;
   return PMGPU_OK;

@@ -412,8 +412,11 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
     // one reach; atoms that later leave it clamp into the edge cells
     // (cells only accelerate the search, they never drop a pair).
     std::vector<double> h(3 * (size_t)std::max(n, 1), 0.0);
-    if (n) PM_CUDA(cudaMemcpy(h.data(), s->d_pos, sizeof(double) * 3 * n,
-                              cudaMemcpyDeviceToHost));
+    if (n) {
+      PM_CUDA(cudaMemcpyAsync(h.data(), s->d_pos, sizeof(double) * 3 * n,
+                              cudaMemcpyDeviceToHost, s->stream));
+      PM_CUDA(cudaStreamSynchronize(s->stream));
+    }
     double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
     for (int a = 0; a < 3; a++) { mn[a] = h[a]; mx[a] = h[a]; }
     for (int i = 1; i < n; i++)
@@ -444,36 +447,35 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   if (nl->cap > cap) cap = nl->cap;
   nl->cap = cap;
   size_t nn = std::max(1, n);
-  PM_CUDA(cudaMalloc(&nl->d_key, sizeof(int) * nn));
-  PM_CUDA(cudaMalloc(&nl->d_key_count, sizeof(int) * nl->nkeys));
-  PM_CUDA(cudaMemset(nl->d_key_count, 0, sizeof(int) * nl->nkeys));
-  PM_CUDA(cudaMalloc(&nl->d_key_start, sizeof(int) * (nl->nkeys + 1)));
-  PM_CUDA(cudaMalloc(&nl->d_key_cursor, sizeof(int) * nl->nkeys));
-  PM_CUDA(cudaMalloc(&nl->d_sorted, sizeof(int) * nn));
-  PM_CUDA(cudaMalloc(&nl->d_offset, sizeof(double) * 3 * nn));
-  PM_CUDA(cudaMalloc(&nl->d_xbuild, sizeof(double) * 3 * nn));
-  PM_CUDA(cudaMalloc(&nl->d_xhi, sizeof(float4) * nn));
-  PM_CUDA(cudaMalloc(&nl->d_xlo, sizeof(float4) * nn));
-  PM_CUDA(cudaMalloc(&nl->d_xw, sizeof(double4) * nn));
-  PM_CUDA(cudaMalloc(&nl->d_mol_s, sizeof(int) * nn));
-  PM_CUDA(cudaMalloc(&nl->d_nbr, sizeof(uint32_t) * (size_t)cap * nn));
-  PM_CUDA(cudaMalloc(&nl->d_nbr_count, sizeof(int) * nn));
-  PM_CUDA(cudaMemset(nl->d_nbr_count, 0, sizeof(int) * nn));
-  PM_CUDA(cudaMalloc(&nl->d_maxdisp, sizeof(unsigned int)));
-  PM_CUDA(cudaMemset(nl->d_maxdisp, 0, sizeof(unsigned int)));
-  PM_CUDA(cudaMalloc(&nl->d_rebuild, 2 * sizeof(int)));
-  PM_CUDA(cudaMemset(nl->d_rebuild, 0, 2 * sizeof(int)));
+  PM_CHECK(dev_alloc(s, &nl->d_key, sizeof(int) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_key_count, sizeof(int) * nl->nkeys));
+  PM_CUDA(cudaMemsetAsync(nl->d_key_count, 0, sizeof(int) * nl->nkeys, s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_key_start, sizeof(int) * (nl->nkeys + 1)));
+  PM_CHECK(dev_alloc(s, &nl->d_key_cursor, sizeof(int) * nl->nkeys));
+  PM_CHECK(dev_alloc(s, &nl->d_sorted, sizeof(int) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_offset, sizeof(double) * 3 * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_xbuild, sizeof(double) * 3 * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_xhi, sizeof(float4) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_xlo, sizeof(float4) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_xw, sizeof(double4) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_mol_s, sizeof(int) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_nbr, sizeof(uint32_t) * (size_t)cap * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_nbr_count, sizeof(int) * nn));
+  PM_CUDA(cudaMemsetAsync(nl->d_nbr_count, 0, sizeof(int) * nn, s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_maxdisp, sizeof(unsigned int)));
+  PM_CUDA(cudaMemsetAsync(nl->d_maxdisp, 0, sizeof(unsigned int), s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_rebuild, 2 * sizeof(int)));
+  PM_CUDA(cudaMemsetAsync(nl->d_rebuild, 0, 2 * sizeof(int), s->stream));
   nl->built = 0;
   return PMGPU_OK;
 }
 
-int nb_list_free(NeighborList *nl) {
+int nb_list_free(System *s, NeighborList *nl) {
   void *ptrs[] = {nl->d_key, nl->d_key_count, nl->d_key_start, nl->d_key_cursor,
                   nl->d_sorted, nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo,
                   nl->d_xw, nl->d_nbr, nl->d_nbr_count, nl->d_maxdisp, nl->d_rebuild,
                   nl->d_mol_s};
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
+  for (void *p : ptrs) dev_free(s, p);
   nl->d_key = nullptr; nl->d_key_count = nullptr; nl->d_key_start = nullptr;
   nl->d_key_cursor = nullptr; nl->d_sorted = nullptr; nl->d_offset = nullptr;
   nl->d_xbuild = nullptr; nl->d_xhi = nullptr; nl->d_xlo = nullptr;
@@ -589,6 +591,8 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   if (t.mask & TERM_EWALD) mx = std::max(mx, t.ewald_rc2);
   a.max_hi = (Real)(mx * (1 + band));
   a.max_lo = (Real)(mx * (1 - band));
+  a.minimal_image = t.minimal_image;
+  for (int c = 0; c < 3; c++) a.half_edge[c] = (Real)s->box.H2[c];
   a.same_cut = 1;
   if ((t.mask & TERM_LJ) && t.lj_cut2 != mx) a.same_cut = 0;
   if ((t.mask & TERM_COUL) && t.coul_cut2 != mx) a.same_cut = 0;
@@ -724,8 +728,11 @@ int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims) {
     for (int a = 0; a < 3; a++) { mn[a] = s->box.min[a]; mx[a] = s->box.max[a]; }
   } else {
     std::vector<double> h(3 * (size_t)std::max(n, 1), 0.0);
-    if (n) PM_CUDA(cudaMemcpy(h.data(), s->d_pos, sizeof(double) * 3 * n,
-                              cudaMemcpyDeviceToHost));
+    if (n) {
+      PM_CUDA(cudaMemcpyAsync(h.data(), s->d_pos, sizeof(double) * 3 * n,
+                              cudaMemcpyDeviceToHost, s->stream));
+      PM_CUDA(cudaStreamSynchronize(s->stream));
+    }
     // Vector3DBlock::boundingbox (type/Vector3DBlock.cpp:9-35)
     for (int a = 0; a < 3; a++) mn[a] = mx[a] = h[a];
     for (int i = 1; i < n; i++)
@@ -754,12 +761,12 @@ int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims) {
   }
   g.ncx = d[0]; g.ncy = d[1]; g.ncz = d[2];
   int *dout = nullptr;
-  PM_CUDA(cudaMalloc(&dout, sizeof(int) * 3 * std::max(n, 1)));
+  PM_CHECK(dev_alloc(s, &dout, sizeof(int) * 3 * std::max(n, 1)));
   if (n) k_cells_debug<<<(n + 255) / 256, 256, 0, s->stream>>>(g, s->d_pos, dout);
   cudaError_t e = cudaMemcpyAsync(cell_xyz, dout, sizeof(int) * 3 * n,
                                   cudaMemcpyDeviceToHost, s->stream);
+  dev_free(s, dout);
   cudaError_t e2 = cudaStreamSynchronize(s->stream);
-  cudaFree(dout);
   if (e != cudaSuccess || e2 != cudaSuccess)
     return fail(PMGPU_ERR_CUDA, "debug cell assignment failed");
   dims[0] = d[0]; dims[1] = d[1]; dims[2] = d[2];

@@ -35,6 +35,8 @@ struct PairArgs {
   double lj_cut2, coul_cut2, ew_cut2;
   Real lj_lo, lj_hi, coul_lo, coul_hi, ew_lo, ew_hi, max_lo, max_hi;
   int same_cut;          // all active terms share one cutoff
+  int minimal_image;     // LJ / Coulomb cutoff terms only for the minimal image
+  Real half_edge[3];
   Real alpha, a2pi;
   double alpha64, a2pi64;
   int exact_erf;
@@ -448,6 +450,12 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE>::bl
         if ((TERMS & TERM_EWALD) && r2 > a.ew_lo && r2x <= a.ew_cut2) flags |= kQEwald;
       }
     }
+    // boxes below twice the cutoff: cutoff terms take the minimal image only
+    // (Ewald real space sums every image, NonbondedFullEwaldSystemForce.h:790)
+    if ((TERMS & (TERM_LJ | TERM_COUL)) && a.minimal_image && (flags & (kQLJ | kQCoul)) &&
+        !(fabs(dx) <= a.half_edge[0] && fabs(dy) <= a.half_edge[1] &&
+          fabs(dz) <= a.half_edge[2]))
+      flags &= ~(kQLJ | kQCoul);
     const bool pass = flags != 0;
     const unsigned mk = __ballot_sync(kAll, pass);
     if (pass) {

@@ -108,6 +108,7 @@ struct PairTerms {
   double ewald_alpha, ewald_rc2;
   int exact_erf;
   double coulomb_scaling;
+  int minimal_image;        // cutoff terms see only the minimal image
 };
 
 // Device arrays of one neighbour-list structure (one per distinct
@@ -163,6 +164,7 @@ struct Force {
   long long *d_grid_fixed = nullptr;  // fixed-point spread target
   float2 *d_cgrid = nullptr;          // complex grid (K1*K2*(K3/2+1))
   float *d_influence = nullptr;       // K1*K2*(K3/2+1) influence function
+  void *d_fft_work = nullptr;         // cuFFT work area shared by both plans
   // simplefull
   int sf_lj = 0, sf_coul = 0;
   // gb
@@ -250,6 +252,13 @@ struct System {
     cudaGraphExec_t exec = nullptr;
     long long kernels = 0;  // own kernels per replay
   } graphs[2];
+  struct PendingRun {
+    int active = 0;
+    pmgpu_integrator integ{};
+    long n_steps = 0;
+    uint64_t step0 = 0;
+    int valid0 = 0;
+  } pending;  // segment enqueued by pmgpu_run_async, not yet waited for
   long long last_pairs = 0;
   double last_energy[PMGPU_E_COUNT] = {0, 0, 0, 0, 0, 0, 0};
   double last_virial[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -261,6 +270,16 @@ struct System {
   long long *d_paircount = nullptr;
 };
 
+// Device buffers are stream-ordered (cudaMallocAsync / cudaFreeAsync on the
+// system's stream): creating and destroying a system never synchronises the
+// whole device, so systems served side by side do not stall one another.
+int dev_alloc(System *s, void **p, size_t bytes);
+template <typename T>
+inline int dev_alloc(System *s, T **p, size_t bytes) {
+  return dev_alloc(s, reinterpret_cast<void **>(p), bytes);
+}
+void dev_free(System *s, void *p);
+
 // ------------------------------------------------------------ host API of TUs
 void box_from_topology(const pmgpu_topology *t, Box *b);
 void switch_setup(const pmgpu_switch *in, SwitchParams *o);
@@ -268,7 +287,7 @@ void switch_setup(const pmgpu_switch *in, SwitchParams *o);
 // nonbonded.cu
 int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin,
                  double cellsize_for_debug);
-int nb_list_free(NeighborList *nl);
+int nb_list_free(System *s, NeighborList *nl);
 int nb_prepare(System *s, NeighborList *nl, int force_rebuild);
 int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode);
 int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
@@ -276,7 +295,7 @@ int nb_simplefull(System *s, int lj, int coul, int want_virial);
 
 // pme.cu
 int pme_init(System *s, Force *f);
-int pme_free(Force *f);
+int pme_free(System *s, Force *f);
 int pme_reciprocal(System *s, Force *f, int em);
 int ewald_correction(System *s, Force *f, int em);
 

@@ -10,6 +10,7 @@
 //   * correctionTerm (NonbondedFullEwaldSystemForce.h:1092-1131) in FP64.
 // The reciprocal energy matches the reference's convention
 // E = (4 pi / V) sum_{half space k} exp(-k^2/4a^2)/k^2 |S(k)|^2 (:1013-1054).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -342,9 +343,9 @@ int pme_init(System *s, Force *f) {
   int K0 = f->grid[0], K1 = f->grid[1], K2 = f->grid[2];
   size_t nreal = (size_t)K0 * K1 * K2;
   size_t ncplx = (size_t)K0 * K1 * (K2 / 2 + 1);
-  PM_CUDA(cudaMalloc(&f->d_grid, sizeof(float) * nreal));
-  PM_CUDA(cudaMalloc(&f->d_grid_fixed, sizeof(long long) * nreal));
-  PM_CUDA(cudaMalloc(&f->d_cgrid, sizeof(float2) * ncplx));
+  PM_CHECK(dev_alloc(s, &f->d_grid, sizeof(float) * nreal));
+  PM_CHECK(dev_alloc(s, &f->d_grid_fixed, sizeof(long long) * nreal));
+  PM_CHECK(dev_alloc(s, &f->d_cgrid, sizeof(float2) * ncplx));
   {
     // influence function of the box (fixed for the life of the system)
     std::vector<float> bm[3];
@@ -368,27 +369,38 @@ int pme_init(System *s, Force *f) {
           g[idx] = (float)(std::exp(-pa * h2) / (M_PI * V * h2) * (double)bm[0][mx_] *
                            (double)bm[1][my_] * (double)bm[2][mz]);
         }
-    PM_CUDA(cudaMalloc(&f->d_influence, sizeof(float) * ncplx));
-    PM_CUDA(cudaMemcpy(f->d_influence, g.data(), sizeof(float) * ncplx, cudaMemcpyHostToDevice));
+    PM_CHECK(dev_alloc(s, &f->d_influence, sizeof(float) * ncplx));
+    PM_CUDA(cudaMemcpyAsync(f->d_influence, g.data(), sizeof(float) * ncplx,
+                            cudaMemcpyHostToDevice, s->stream));
+    PM_CUDA(cudaStreamSynchronize(s->stream));
   }
-  if (cufftPlan3d(&f->plan_r2c, K0, K1, K2, CUFFT_R2C) != CUFFT_SUCCESS ||
-      cufftPlan3d(&f->plan_c2r, K0, K1, K2, CUFFT_C2R) != CUFFT_SUCCESS)
+  // cuFFT plans without their own work area: one stream-ordered work area
+  // serves both (they run back to back on the system's stream)
+  size_t ws_r2c = 0, ws_c2r = 0;
+  if (cufftCreate(&f->plan_r2c) != CUFFT_SUCCESS || cufftCreate(&f->plan_c2r) != CUFFT_SUCCESS ||
+      cufftSetAutoAllocation(f->plan_r2c, 0) != CUFFT_SUCCESS ||
+      cufftSetAutoAllocation(f->plan_c2r, 0) != CUFFT_SUCCESS ||
+      cufftMakePlan3d(f->plan_r2c, K0, K1, K2, CUFFT_R2C, &ws_r2c) != CUFFT_SUCCESS ||
+      cufftMakePlan3d(f->plan_c2r, K0, K1, K2, CUFFT_C2R, &ws_c2r) != CUFFT_SUCCESS)
     return fail(PMGPU_ERR_CUDA, "cuFFT plan creation failed");
-  if (cufftSetStream(f->plan_r2c, s->stream) != CUFFT_SUCCESS ||
+  PM_CHECK(dev_alloc(s, &f->d_fft_work, std::max(ws_r2c, ws_c2r)));
+  if (cufftSetWorkArea(f->plan_r2c, f->d_fft_work) != CUFFT_SUCCESS ||
+      cufftSetWorkArea(f->plan_c2r, f->d_fft_work) != CUFFT_SUCCESS ||
+      cufftSetStream(f->plan_r2c, s->stream) != CUFFT_SUCCESS ||
       cufftSetStream(f->plan_c2r, s->stream) != CUFFT_SUCCESS)
-    return fail(PMGPU_ERR_CUDA, "cufftSetStream failed");
+    return fail(PMGPU_ERR_CUDA, "cuFFT work area / stream set-up failed");
   return PMGPU_OK;
 }
 
-int pme_free(Force *f) {
+int pme_free(System *s, Force *f) {
   if (f->plan_r2c) cufftDestroy(f->plan_r2c);
   if (f->plan_c2r) cufftDestroy(f->plan_c2r);
   f->plan_r2c = f->plan_c2r = 0;
-  void *ptrs[] = {f->d_grid, f->d_grid_fixed, f->d_cgrid, f->d_influence};
-  for (void *p : ptrs)
-    if (p) cudaFree(p);
+  void *ptrs[] = {f->d_grid, f->d_grid_fixed, f->d_cgrid, f->d_influence, f->d_fft_work};
+  for (void *p : ptrs) dev_free(s, p);
   f->d_grid = nullptr; f->d_grid_fixed = nullptr; f->d_cgrid = nullptr;
   f->d_influence = nullptr;
+  f->d_fft_work = nullptr;
   return PMGPU_OK;
 }
 

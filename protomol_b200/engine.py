@@ -35,6 +35,17 @@ def ScalarStructure() -> np.ndarray:
     return np.zeros(SCALAR_LAST)
 
 
+def footprint_estimate(n_atoms: int, box, reach: float, grid=None) -> int:
+    """Device bytes a periodic system needs (admission control)."""
+    lib = L.load()
+    b = np.ascontiguousarray(np.asarray(box, dtype=np.float64)[:3])
+    g = None if grid is None else np.ascontiguousarray(np.asarray(grid, dtype=np.int32))
+    out = C.c_longlong()
+    L.check(lib.pmgpu_footprint_estimate(int(n_atoms), L.ptr(b), float(reach), L.ptr(g),
+                                         C.byref(out)))
+    return int(out.value)
+
+
 class Context:
     """One CUDA device."""
 
@@ -44,6 +55,12 @@ class Context:
         L.check(self.lib.pmgpu_context_create(device, C.byref(h)))
         self.h = h
         self.device = device
+
+    def mem_info(self) -> tuple[int, int]:
+        """(free, total) device bytes."""
+        f, t = C.c_longlong(), C.c_longlong()
+        L.check(self.lib.pmgpu_mem_info(self.h, C.byref(f), C.byref(t)))
+        return int(f.value), int(t.value)
 
     def close(self):
         if self.h:
@@ -454,6 +471,21 @@ class _Integrator:
     def run(self, system: GpuSystem, n_steps: int) -> None:
         """Integrator::run(n): all steps on the device."""
         L.check(system.lib.pmgpu_run(system.h, C.byref(self.p), int(n_steps)))
+
+    def run_async(self, system: GpuSystem, n_steps: int) -> None:
+        """Enqueue run(n) on the system's stream and return at once; finish
+        with wait()."""
+        L.check(system.lib.pmgpu_run_async(system.h, C.byref(self.p), int(n_steps)))
+
+    @staticmethod
+    def done(system: GpuSystem) -> bool:
+        d = C.c_int()
+        L.check(system.lib.pmgpu_run_query(system.h, C.byref(d)))
+        return bool(d.value)
+
+    @staticmethod
+    def wait(system: GpuSystem) -> None:
+        L.check(system.lib.pmgpu_run_wait(system.h))
 
 
 class LeapfrogIntegrator(_Integrator):

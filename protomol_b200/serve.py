@@ -1,0 +1,260 @@
+"""Batched and served forms: many independent water boxes advanced at once
+on one GPU.
+
+Every admitted request owns a GpuSystem (its own CUDA stream, resident
+coordinates, velocities, neighbour list and PME grids).  A request is either
+one energy + force evaluation or an MD segment (LangevinLeapfrog by default).
+Admission is continuous: a request is started as soon as a slot is free and
+its footprint estimate fits in the device-memory budget, while the segments
+already admitted keep running; their kernels overlap on the device because
+each system runs on its own stream and the library releases the GIL inside
+every blocking call.  The plain form is the same loop with one slot.
+
+Each result is a pure function of the request (fixed-point force sums and a
+counter-based Langevin noise), so it is bit-identical alone and in the mix.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import queue
+import threading
+import time
+
+import numpy as np
+
+from . import systems
+from .engine import (Context, ForceFactory, GpuSystem, LangevinLeapfrogIntegrator,
+                     LeapfrogIntegrator, footprint_estimate)
+
+WATER_DENSITY = 0.0334  # waters per A^3
+RC, ALPHA, ORDER, LJ_SWITCHON, SPACING, SKIN = 9.0, 0.35, 4, 8.0, 1.0, 1.0
+
+
+def fft_size(n: int) -> int:
+    """Smallest 2^a 3^b 5^c >= n."""
+    m = max(1, n)
+    while True:
+        k = m
+        for p in (2, 3, 5):
+            while k % p == 0:
+                k //= p
+        if k == 1:
+            return m
+        m += 1
+
+
+@dataclasses.dataclass
+class Request:
+    """One unit of served work on a seeded TIP3P box."""
+    rid: int
+    n_waters: int
+    seed: int
+    kind: str = "segment"        # "segment" | "evaluate"
+    steps: int = 1000
+    integrator: str = "langevin"  # "langevin" | "leapfrog"
+    timestep: float = 1.0
+    temperature: float = 300.0
+    gamma: float = 5.0
+    arrival: float = 0.0          # seconds after the stream starts
+    system: systems.MolecularSystem | None = None  # the client's input
+    # filled in by the server
+    t_start: float = 0.0
+    t_done: float = 0.0
+    energies: np.ndarray | None = None
+    positions: np.ndarray | None = None
+    forces: np.ndarray | None = None
+    error: str | None = None
+
+    @property
+    def n_atoms(self) -> int:
+        return 3 * self.n_waters
+
+    @property
+    def edge(self) -> float:
+        return (self.n_waters / WATER_DENSITY) ** (1.0 / 3.0)
+
+    @property
+    def grid(self) -> int:
+        return fft_size(int(math.ceil(self.edge / SPACING)))
+
+    def footprint(self) -> int:
+        L = self.edge
+        g = self.grid
+        return footprint_estimate(self.n_atoms, (L, L, L), RC + SKIN, (g, g, g))
+
+    def latency(self) -> float:
+        return self.t_done - self.arrival
+
+    def prepare(self) -> "Request":
+        """Builds the request's input system (the client's side of a
+        request: the server receives a ready topology and coordinates)."""
+        if self.system is None:
+            self.system = systems.water_box_for_density(self.n_waters, WATER_DENSITY, self.seed,
+                                                        jitter=0.2)
+        return self
+
+
+def force_lines(grid: int) -> list[str]:
+    return ["Bond", "Angle",
+            f"LennardJones -algorithm NonbondedCutoff -switchingFunction C2 "
+            f"-switchon {LJ_SWITCHON} -cutoff {RC} -cutoff {RC}",
+            f"Coulomb -algorithm PMEwald -alpha {ALPHA} -cutoff {RC} -order {ORDER} "
+            f"-gridsize {grid} {grid} {grid}"]
+
+
+def build(ctx: Context, req: Request, precision: str = "mixed") -> GpuSystem:
+    gs = GpuSystem(ctx, req.prepare().system, precision)
+    ff = ForceFactory(gs, RC)
+    for line in force_lines(req.grid):
+        ff.make(line)
+    return gs
+
+
+def execute(ctx: Context, req: Request, keep_positions: bool = True) -> Request:
+    """Runs one request to completion on the calling thread."""
+    gs = build(ctx, req)
+    try:
+        if req.kind == "evaluate":
+            e, _ = gs.evaluate()
+            req.energies = e
+            req.forces = gs.forces_total()
+        else:
+            if req.integrator == "langevin":
+                integ = LangevinLeapfrogIntegrator(req.timestep, req.temperature, req.gamma,
+                                                   seed=req.seed)
+            else:
+                integ = LeapfrogIntegrator(req.timestep)
+            integ.run(gs, req.steps)
+            req.energies = gs.energies()[0]
+            if keep_positions:
+                req.positions = gs.positions()
+    finally:
+        gs.close()
+    return req
+
+
+class Server:
+    """Continuous-batching request loop over one device.
+
+    slots: requests in flight at once (one worker thread each);
+    mem_fraction: share of the device memory free at start-up that admitted
+    requests may hold (by their footprint estimates)."""
+
+    def __init__(self, ctx: Context, slots: int = 16, mem_fraction: float = 0.8):
+        self.ctx = ctx
+        self.slots = slots
+        free, _ = ctx.mem_info()
+        self.budget = int(free * mem_fraction)
+        self.in_use = 0
+        self.lock = threading.Condition()
+        self.admit_q: queue.Queue = queue.Queue()
+        self.done: list[Request] = []
+        self.peak_in_flight = 0
+        self.in_flight = 0
+        self.peak_in_use = 0
+
+    def _worker(self):
+        while True:
+            req = self.admit_q.get()
+            if req is None:
+                return
+            try:
+                execute(self.ctx, req)
+            except Exception as ex:  # reported per request, the loop goes on
+                req.error = str(ex)[:300]
+            req.t_done = time.perf_counter() - self.t0
+            with self.lock:
+                self.in_use -= req._fp
+                self.in_flight -= 1
+                self.done.append(req)
+                self.lock.notify_all()
+
+    def run(self, requests: list[Request], realtime: bool = True) -> dict:
+        """Serves the requests (in arrival order; with realtime the arrival
+        times are honoured) and returns throughput and latency figures."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        for r in reqs:
+            r.prepare()  # inputs arrive ready-made; building them is not timed
+            r._fp = r.footprint()
+            if r._fp > self.budget:
+                raise ValueError(f"request {r.rid} needs {r._fp} B, over the budget {self.budget}")
+        workers = [threading.Thread(target=self._worker, daemon=True) for _ in range(self.slots)]
+        for w in workers:
+            w.start()
+        self.t0 = time.perf_counter()
+        for r in reqs:
+            if realtime:
+                wait = r.arrival - (time.perf_counter() - self.t0)
+                if wait > 0:
+                    time.sleep(wait)
+            with self.lock:
+                # admit when a slot and the memory are free
+                while self.in_flight >= self.slots or self.in_use + r._fp > self.budget:
+                    self.lock.wait()
+                self.in_use += r._fp
+                self.in_flight += 1
+                self.peak_in_flight = max(self.peak_in_flight, self.in_flight)
+                self.peak_in_use = max(self.peak_in_use, self.in_use)
+            r.t_start = time.perf_counter() - self.t0
+            self.admit_q.put(r)
+        with self.lock:
+            while len(self.done) < len(reqs):
+                self.lock.wait()
+        wall = time.perf_counter() - self.t0
+        for _ in workers:
+            self.admit_q.put(None)
+        for w in workers:
+            w.join()
+        out = summarize(reqs, wall, self.slots, self.peak_in_flight)
+        out["peak_footprint_bytes"] = self.peak_in_use
+        out["budget_bytes"] = self.budget
+        return out
+
+
+def summarize(reqs: list[Request], wall: float, slots: int, peak: int) -> dict:
+    ok = [r for r in reqs if r.error is None]
+    lat = np.array([r.latency() for r in ok]) if ok else np.zeros(1)
+    md_ns = sum(r.steps * r.timestep * 1e-6 for r in ok if r.kind == "segment")
+    atom_steps = sum(r.n_atoms * (r.steps if r.kind == "segment" else 1) for r in ok)
+    return {
+        "requests": len(reqs), "failed": len(reqs) - len(ok), "slots": slots,
+        "peak_in_flight": peak, "wall_s": wall,
+        "ns_per_day": md_ns * 86400.0 / wall,
+        "atom_steps_per_s": atom_steps / wall,
+        "p50_latency_s": float(np.percentile(lat, 50)),
+        "p99_latency_s": float(np.percentile(lat, 99)),
+    }
+
+
+def request_stream(n: int, seed: int, min_atoms: int = 500, max_atoms: int = 50000,
+                   eval_fraction: float = 0.3, steps: int = 1000,
+                   rate_per_s: float | None = None) -> list[Request]:
+    """A seeded request stream: atom counts log-uniform in [min, max]
+    (rounded to whole waters), a share of single evaluations, the rest MD
+    segments; Poisson arrivals at rate_per_s (None: all at time 0)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    for k in range(n):
+        atoms = math.exp(rng.uniform(math.log(min_atoms), math.log(max_atoms)))
+        nw = max(1, int(round(atoms / 3)))
+        kind = "evaluate" if rng.uniform() < eval_fraction else "segment"
+        if rate_per_s:
+            t += rng.exponential(1.0 / rate_per_s)
+        out.append(Request(rid=k, n_waters=nw, seed=int(rng.integers(1 << 31)), kind=kind,
+                           steps=steps if kind == "segment" else 0, arrival=t))
+    return out
+
+
+def ensemble(n_boxes: int, seed: int, min_waters: int = 100, max_waters: int = 1000,
+             steps: int = 50) -> list[Request]:
+    """The batched ensemble: boxes with water counts log-uniform in
+    [min_waters, max_waters], one MD segment each, all available at once."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_boxes):
+        nw = int(round(math.exp(rng.uniform(math.log(min_waters), math.log(max_waters)))))
+        out.append(Request(rid=k, n_waters=nw, seed=int(rng.integers(1 << 31)), steps=steps,
+                           integrator="leapfrog"))
+    return out

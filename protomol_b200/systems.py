@@ -90,6 +90,18 @@ def _random_rotation(rng: np.random.Generator) -> np.ndarray:
         [2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d]])
 
 
+def _random_rotations(rng: np.random.Generator, count: int) -> np.ndarray:
+    """count rotation matrices from unit quaternions, (count, 3, 3)."""
+    q = rng.normal(size=(count, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    a, b, c, d = q.T
+    return np.stack([
+        np.stack([a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)], -1),
+        np.stack([2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)], -1),
+        np.stack([2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d], -1)],
+        1)
+
+
 def mb_velocities(mass: np.ndarray, temperature: float, rng) -> np.ndarray:
     """Maxwell-Boltzmann velocities in ProtoMol units (A per internal time
     unit, so that 0.5 m v^2 is in kcal/mol), zero total momentum."""
@@ -109,8 +121,8 @@ def tip3p_box(n_waters: int, edge: float, seed: int, jitter: float = 0.0,
     rng = np.random.default_rng(seed)
     if lattice is None:
         lattice = int(math.ceil(n_waters ** (1.0 / 3.0) - 1e-9))
-    sites = np.array([(i, j, k) for i in range(lattice) for j in range(lattice)
-                      for k in range(lattice)], dtype=np.float64)
+    g = np.arange(lattice, dtype=np.float64)
+    sites = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
     if len(sites) < n_waters:
         raise ValueError("lattice too small")
     if len(sites) > n_waters:
@@ -124,10 +136,10 @@ def tip3p_box(n_waters: int, edge: float, seed: int, jitter: float = 0.0,
                       [p["r_oh"] * math.sin(half), 0.0, p["r_oh"] * math.cos(half)],
                       [-p["r_oh"] * math.sin(half), 0.0, p["r_oh"] * math.cos(half)]])
     n = 3 * n_waters
-    pos = np.zeros((n, 3))
-    for w in range(n_waters):
-        R = _random_rotation(rng)
-        pos[3 * w:3 * w + 3] = centers[w] + local @ R.T
+    # one random rotation per water (the same draws, in the same order, as
+    # n_waters calls of _random_rotation)
+    R = _random_rotations(rng, n_waters)
+    pos = (centers[:, None, :] + np.einsum("ak,wjk->waj", local, R)).reshape(n, 3)
     raw_q = np.tile([p["q_o"], p["q_h"], p["q_h"]], n_waters)
     mass = np.tile([p["m_o"], p["m_h"], p["m_h"]], n_waters)
     typ = np.tile(np.array([0, 1, 1], np.int32), n_waters)
