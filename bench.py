@@ -234,6 +234,108 @@ def served_line(args, ctx, world: int, rank: int, dist=None) -> dict:
                                                                    1e-30)}
 
 
+GB_ATOMS, GB_SEED, GB_SEGMENT = 2000, 3, 500
+GB_WORKLOAD = ("gb_polymer2000: linear heteropolymer of 2,000 atoms, vacuum, GB OBC2 "
+               "(solute 1, solvent 78.5) + LJ + Coulomb all pairs, bonds/angles/dihedrals, "
+               "LangevinLeapfrog 1 fs, gamma 5/ps, 300 K")
+
+
+def gb_force_lines():
+    return ["GBBornRadii -algorithm NonbondedSimpleFull",
+            "GBPartialSum -algorithm NonbondedSimpleFull",
+            "GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.5",
+            "LennardJones -algorithm NonbondedSimpleFull",
+            "Coulomb -algorithm NonbondedSimpleFull", "Bond", "Angle", "Dihedral"]
+
+
+def gb_cpu_baseline(sysm, evals: int = 3) -> dict:
+    """The oracle's FP64 restatement (one core) timed on the same polymer:
+    GB + LJ + Coulomb all pairs + torsions per MD step (the integrator and
+    bonds are negligible beside the O(N^2) passes)."""
+    import oracle
+    s = oracle.System(pos=sysm.pos, charge=sysm.charge, type=sysm.type, molecule=sysm.molecule,
+                      lj=sysm.lj, excl=sysm.exclusions, periodic=False, box=sysm.box,
+                      mass=sysm.mass, water=sysm.water, gb_vdwr=sysm.gb_vdwr,
+                      gb_scale=sysm.gb_scale, gb_offset=sysm.gb_offset, gb_obc=sysm.gb_obc)
+    t0 = time.perf_counter()
+    for _ in range(evals):
+        oracle.gb_force(s, 1.0, 78.5)
+        oracle.simplefull_force(s, "LennardJones")
+        oracle.simplefull_force(s, "Coulomb")
+        oracle.torsion_force(s, sysm.dihedrals, sysm.dihedral_params)
+    dt = (time.perf_counter() - t0) / evals
+    return {"value": DT_FS * 1e-6 * 86400.0 / dt, "unit": "ns/day", "cores": 1, "kind": "port",
+            "sample": f"{evals} force evaluations of the 2,000-atom polymer by the FP64 oracle "
+                      f"restatement (GB + LJ + Coulomb all pairs + torsions), 1 core"}
+
+
+def gb_line(args, ctx, world: int, rank: int, dist=None) -> dict:
+    """The implicit-solvent configuration: Langevin segments of the GB
+    polymer (one replica per rank), device-timed, plus the end-to-end run
+    through the public API with host buffers."""
+    import torch
+    from protomol_b200 import ForceFactory, GpuSystem, LangevinLeapfrogIntegrator, systems
+    sysm = systems.gb_polymer(GB_ATOMS, GB_SEED + rank)
+    gs = GpuSystem(ctx, sysm, "mixed")
+    ff = ForceFactory(gs)
+    for line in gb_force_lines():
+        ff.make(line)
+    integ = LangevinLeapfrogIntegrator(DT_FS, 300.0, 5.0, seed=GB_SEED)
+    seg = args.segment if args.segment != SEGMENT else GB_SEGMENT
+    stream = torch.cuda.ExternalStream(gs.stream())
+    for _ in range(args.warmup):
+        integ.run(gs, seg)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    k0 = gs.kernel_count()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        integ.run(gs, seg)
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        b.synchronize()
+        total_ms += a.elapsed_time(b)
+    launches = gs.kernel_count() - k0
+    pos_h, vel_h = gs.positions(), gs.velocities()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        gs.set_positions(pos_h)
+        gs.set_velocities(vel_h)
+        integ.run(gs, seg)
+        pos_h, vel_h = gs.positions(), gs.velocities()
+        gs.energies()
+    e2e_ms = 1000.0 * (time.perf_counter() - t0)
+    gs.close()
+    from protomol_b200 import replicas
+    t_ms = replicas.max_over_ranks(total_ms, dist)
+    e2e_ms = replicas.max_over_ranks(e2e_ms, dist)
+    md = args.steps * seg
+    n = GB_ATOMS
+    line = {"metric": "ns/day", "value": world * md * DT_FS * 1e-6 * 86400.0 / (t_ms / 1e3),
+            "unit": "ns/day", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32-pairs/fp64-update", "data": "synthetic",
+            "mode": "gb",
+            "config": {"workload": GB_WORKLOAD, "atoms": n, "md_steps_per_bench_step": seg,
+                       "replicas": world},
+            "pairs_per_s": world * md * 3 * n * (n - 1) / 2 / (t_ms / 1e3),
+            "us_per_md_step": 1e3 * t_ms / md,
+            "e2e": {"value": world * md * DT_FS * 1e-6 * 86400.0 / (e2e_ms / 1e3), "unit": "ns/day",
+                    "h2d_bytes_per_step": 2 * 3 * n * 8, "d2h_bytes_per_step": 2 * 3 * n * 8 + 7 * 8},
+            "gpu_launches": launches}
+    if world == 1:
+        try:
+            line["cpu_baseline"] = gb_cpu_baseline(sysm)
+        except Exception as ex:  # reported, never fatal
+            line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -241,7 +343,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pmgpu", choices=["pmgpu", "reference"])
     ap.add_argument("--segment", type=int, default=SEGMENT)
-    ap.add_argument("--mode", default="bench", choices=["bench", "profile", "served", "batched"],
+    ap.add_argument("--mode", default="bench",
+                    choices=["bench", "profile", "served", "batched", "gb"],
                     help="profile: warm-up segments, then --steps MD steps between "
                          "cudaProfilerStart/Stop (for ncu); served: a mixed request stream "
                          "served plain (one slot) and with continuous batching; batched: "
@@ -293,8 +396,11 @@ def main():
     from protomol_b200 import Context, ForceFactory, GpuSystem, LeapfrogIntegrator
 
     ctx = Context(local)
-    if args.mode in ("served", "batched"):
-        line = served_line(args, ctx, world, rank, dist)
+    if args.mode in ("served", "batched", "gb"):
+        if args.mode == "gb":
+            line = gb_line(args, ctx, world, rank, dist)
+        else:
+            line = served_line(args, ctx, world, rank, dist)
         if rank == 0:
             print(json.dumps(line), flush=True)
         if dist:

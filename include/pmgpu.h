@@ -118,6 +118,16 @@ typedef struct {
   const double *gb_offset;  /* offsetRadius */
   const int *water;         /* 1 if the atom's molecule is a water */
   double gb_obc[3];         /* alphaObc, betaObc, gammaObc */
+  /* Torsions (topology/Torsion.h; MTorsionSystemForce): 4 atoms and
+   * (k [kcal/mol], periodicity n, phase [rad]) per term, a torsion of
+   * multiplicity m given as m terms.  n > 0: k (1 + cos(n phi + phase));
+   * n == 0: k (phi - phase)^2.  NULL arrays: none. */
+  int n_dihedrals;
+  const int *dihedral_atoms;
+  const double *dihedral_params;
+  int n_impropers;
+  const int *improper_atoms;
+  const double *improper_params;
 } pmgpu_topology;
 
 typedef struct {
@@ -220,6 +230,11 @@ int pmgpu_gb_forces_noalloc(int n_atoms, const double *pos, const double *charge
 /* Harmonic bonds and angles of the topology. */
 int pmgpu_force_bonded_add(pmgpu_system *sys, int bonds, int angles,
                            int *force_id);
+/* Dihedral and/or Improper torsions of the topology
+ * (force/bonded/DihedralSystemForce.h, ImproperSystemForce.h); energies go
+ * to PMGPU_E_DIHEDRAL / PMGPU_E_IMPROPER. */
+int pmgpu_force_torsion_add(pmgpu_system *sys, int dihedrals, int impropers,
+                            int *force_id);
 int pmgpu_force_set_enabled(pmgpu_system *sys, int force_id, int enabled);
 
 /* Evaluate all enabled forces at the resident positions.  energies (may be

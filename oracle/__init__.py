@@ -211,6 +211,20 @@ def simplefull_force(sysm: System, potential: str, sw: Switch | None = None):
     return f, {"coulomb": e[0], "lj": e[1]}, v.reshape(3, 3)
 
 
+def torsion_force(sysm: System, atoms: np.ndarray, params: np.ndarray):
+    """Torsion terms (4 atoms; k, periodicity, phase [rad]) ->
+    (forces (n,3), energy, virial (3,3))."""
+    cs = sysm.c()
+    a = np.ascontiguousarray(atoms, dtype=np.int32).reshape(-1)
+    p = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
+    f = np.zeros((sysm.n, 3))
+    e = C.c_double(0)
+    v = np.zeros(9)
+    assert lib().orc_torsion_force(C.byref(cs), len(a) // 4, _ptr(a), _ptr(p), _ptr(f),
+                                   C.byref(e), _ptr(v)) == 0
+    return f, e.value, v.reshape(3, 3)
+
+
 def ewald_params(sysm: System, alpha: float, accuracy: float, exact_erf: bool = False):
     cs = sysm.c()
     e = _Ewald()

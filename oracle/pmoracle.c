@@ -1147,6 +1147,117 @@ int orc_gb_force(const orc_system *s, const orc_gb *g, double *born,
 }
 
 /* ------------------------------------------------------------------ */
+/* ---------------------------------------------------------- torsions */
+static void cross_to(const double *u, const double *v, double *o) {
+  o[0] = u[1] * v[2] - u[2] * v[1];
+  o[1] = u[2] * v[0] - u[0] * v[2];
+  o[2] = u[0] * v[1] - u[1] * v[0];
+}
+
+/* MTorsionSystemForce::calcTorsion (MTorsionSystemForce.h:40-204): the
+ * dihedral angle from the normals of the (1,2,3) and (2,3,4) planes, and
+ * the gradient through d cos(phi) when |sin phi| > 0.1, else through
+ * d sin(phi), which avoids dividing by a small sine or cosine. */
+int orc_torsion_force(const orc_system *s, int nt, const int *atoms,
+                      const double *params, double *forces, double *energy,
+                      double *virial) {
+  pbc_t p;
+  int t, c;
+  double e = 0.0, v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  pbc_set(s, &p);
+  for (t = 0; t < nt; t++) {
+    const int a1 = atoms[4 * t], a2 = atoms[4 * t + 1], a3 = atoms[4 * t + 2],
+              a4 = atoms[4 * t + 3];
+    const double k = params[3 * t], delta = params[3 * t + 2];
+    const int per = (int)params[3 * t + 1];
+    double r12[3], r23[3], r34[3], na[3], nb[3], nc[3], r2;
+    double f1[3], f2[3], f3[3];
+    pbc_mindiff(&p, s->pos + 3 * a2, s->pos + 3 * a1, r12, &r2);
+    pbc_mindiff(&p, s->pos + 3 * a3, s->pos + 3 * a2, r23, &r2);
+    pbc_mindiff(&p, s->pos + 3 * a4, s->pos + 3 * a3, r34, &r2);
+    cross_to(r12, r23, na);
+    cross_to(r23, r34, nb);
+    cross_to(r23, na, nc);
+    const double ia = 1.0 / sqrt(norm2(na)), ib = 1.0 / sqrt(norm2(nb)),
+                 ic = 1.0 / sqrt(norm2(nc));
+    for (c = 0; c < 3; c++) {
+      na[c] *= ia;
+      nb[c] *= ib;
+      nc[c] *= ic;
+    }
+    const double cphi = dot3(na, nb), sphi = dot3(nc, nb);
+    const double phi = -atan2(sphi, cphi);
+    double dvdphi;
+    if (per > 0) {
+      dvdphi = -per * k * sin(per * phi + delta);
+      e += k * (1.0 + cos(per * phi + delta));
+    } else {
+      double diff = phi - delta;
+      if (diff < -M_PI) diff += 2 * M_PI;
+      else if (diff > M_PI) diff -= 2 * M_PI;
+      dvdphi = 2.0 * k * diff;
+      e += k * diff * diff;
+    }
+    if (fabs(sphi) > 0.1) {
+      double ga[3], gb[3];
+      const double g = dvdphi / sphi;
+      for (c = 0; c < 3; c++) {
+        ga[c] = (na[c] * cphi - nb[c]) * ia;
+        gb[c] = (nb[c] * cphi - na[c]) * ib;
+      }
+      /* f1 = g (r23 x ga), f3 = g (gb x r23), f2 = g (ga x r12 + r34 x gb) */
+      double t1[3], t2[3];
+      cross_to(r23, ga, t1);
+      cross_to(gb, r23, t2);
+      for (c = 0; c < 3; c++) {
+        f1[c] = g * t1[c];
+        f3[c] = g * t2[c];
+      }
+      cross_to(ga, r12, t1);
+      cross_to(r34, gb, t2);
+      for (c = 0; c < 3; c++) f2[c] = g * (t1[c] + t2[c]);
+    } else {
+      double gc[3], gb[3], t1[3];
+      const double g = -dvdphi / cphi;
+      for (c = 0; c < 3; c++) {
+        gc[c] = (nc[c] * sphi - nb[c]) * ic;
+        gb[c] = (nb[c] * sphi - nc[c]) * ib;
+      }
+      /* f1 = g (|r23|^2 gc - r23 (r23 . gc)) */
+      const double r23sq = norm2(r23), r23gc = dot3(r23, gc);
+      for (c = 0; c < 3; c++) f1[c] = g * (r23sq * gc[c] - r23[c] * r23gc);
+      cross_to(gb, r23, t1);
+      for (c = 0; c < 3; c++) f3[c] = g * t1[c];
+      /* f2 = g (-(r23 . r12) gc + 2 r23 (r12 . gc) - r12 (r23 . gc) + r34 x gb)
+       *      with the diagonal terms as the reference groups them */
+      for (c = 0; c < 3; c++) {
+        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+        f2[c] = g * (-(r23[c1] * r12[c1] + r23[c2] * r12[c2]) * gc[c] +
+                     (2.0 * r23[c] * r12[c1] - r12[c] * r23[c1]) * gc[c1] +
+                     (2.0 * r23[c] * r12[c2] - r12[c] * r23[c2]) * gc[c2] +
+                     gb[c2] * r34[c1] - gb[c1] * r34[c2]);
+      }
+    }
+    for (c = 0; c < 3; c++) {
+      forces[3 * a1 + c] += f1[c];
+      forces[3 * a2 + c] += f2[c] - f1[c];
+      forces[3 * a3 + c] += f3[c] - f2[c];
+      forces[3 * a4 + c] -= f3[c];
+    }
+    /* the upper triangle, mirrored (the reference adds xy to YX etc.) */
+    for (int i = 0; i < 3; i++)
+      for (int j = i; j < 3; j++) {
+        const double w = f1[i] * r12[j] + f2[i] * r23[j] + f3[i] * r34[j];
+        v[3 * i + j] += w;
+        if (j != i) v[3 * j + i] += w;
+      }
+  }
+  *energy = e;
+  if (virial)
+    for (c = 0; c < 9; c++) virial[c] = v[c];
+  return 0;
+}
+
 void orc_kick(int n, const double *mass, const double *forces, double h,
               double *vel) {
   int i, c;

@@ -124,6 +124,15 @@ int orc_gb_force(const orc_system *s, const orc_gb *g, double *born,
  *   first step: v += F*h/2/m; x += v*h; F = f(x); then per step
  *   v += F*h/m; x += v*h; F = f(x); last: v += F*h/2/m.
  * These expose the single operations; the drivers live in Python. */
+/* Torsions (MTorsionSystemForce::calcTorsion, force/bonded/
+ * MTorsionSystemForce.h:40-204): nt terms, atoms 4 per term, params 3 per
+ * term (k, periodicity n, phase delta [rad]); n > 0 is the cosine form
+ * k (1 + cos(n phi + delta)), n == 0 the harmonic k (phi - delta)^2.
+ * Forces are added; energy and virial (may be NULL) are set. */
+int orc_torsion_force(const orc_system *s, int nt, const int *atoms,
+                      const double *params, double *forces, double *energy,
+                      double *virial);
+
 void orc_kick(int n, const double *mass, const double *forces, double h,
               double *vel);
 void orc_drift(int n, const double *vel, double h, double *pos);

@@ -170,6 +170,25 @@ int main(int argc, char *argv[]) {
     putv(f, "bond_params", bprm);
     puti(f, "angles", aidx);
     putv(f, "angle_params", aprm);
+    // Torsions (topology/Torsion.h): one row per term (atoms, k, n, delta),
+    // a torsion of multiplicity m giving m rows.
+    for (int kind = 0; kind < 2; kind++) {
+      const std::vector<Torsion> &ts = kind == 0 ? topo->dihedrals : topo->impropers;
+      std::vector<long> tidx;
+      std::vector<double> tprm;
+      for (size_t k = 0; k < ts.size(); k++)
+        for (int m = 0; m < ts[k].multiplicity; m++) {
+          tidx.push_back(ts[k].atom1);
+          tidx.push_back(ts[k].atom2);
+          tidx.push_back(ts[k].atom3);
+          tidx.push_back(ts[k].atom4);
+          tprm.push_back(ts[k].forceConstant[m]);
+          tprm.push_back((double)ts[k].periodicity[m]);
+          tprm.push_back(ts[k].phaseShift[m]);
+        }
+      puti(f, kind == 0 ? "dihedrals" : "impropers", tidx);
+      putv(f, kind == 0 ? "dihedral_params" : "improper_params", tprm);
+    }
     vector<double> csf(1, topo->coulombScalingFactor);
     putv(f, "coulomb_scaling", csf);
 

@@ -46,7 +46,7 @@ def parse(path: str) -> dict:
                 out["forces"].append(cur)
                 continue
             if key in ("type", "molecule", "water", "exclusions", "exclusions_check", "bonds",
-                       "angles"):
+                       "angles", "dihedrals", "impropers"):
                 arr = np.array([int(v) for v in vals], dtype=np.int64)
             else:
                 arr = np.array([float(v) for v in vals], dtype=np.float64)

@@ -10,5 +10,5 @@ from .engine import (  # noqa: F401
     ANGLE, BOND, COULOMB, LENNARDJONES, VIRIALXX, BondedSystemForce, Context, ForceFactory,
     GBForce, GpuSystem, LangevinLeapfrogIntegrator, LeapfrogIntegrator,
     NonbondedCutoffSystemForce, NonbondedSimpleFullSystemForce, PMEwaldSystemForce,
-    ScalarStructure, SystemForce)
+    ScalarStructure, SystemForce, TorsionSystemForce)
 from ._lib import PmgpuError, load  # noqa: F401

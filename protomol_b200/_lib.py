@@ -38,7 +38,7 @@ EXPORTED = [
     "pmgpu_set_count_pairs", "pmgpu_force_stats", "pmgpu_debug_cell_assign",
     "pmgpu_debug_pair_set", "pmgpu_profile_enable", "pmgpu_profile_read",
     "pmgpu_kernel_count", "pmgpu_gb_forces_noalloc", "pmgpu_run_async", "pmgpu_run_query",
-    "pmgpu_run_wait", "pmgpu_mem_info", "pmgpu_footprint_estimate",
+    "pmgpu_run_wait", "pmgpu_mem_info", "pmgpu_footprint_estimate", "pmgpu_force_torsion_add",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -60,6 +60,8 @@ class Topology(C.Structure):
         ("n_angles", C.c_int), ("angle_atoms", C.c_void_p), ("angle_params", C.c_void_p),
         ("gb_vdwr", C.c_void_p), ("gb_scale", C.c_void_p), ("gb_offset", C.c_void_p),
         ("water", C.c_void_p), ("gb_obc", C.c_double * 3),
+        ("n_dihedrals", C.c_int), ("dihedral_atoms", C.c_void_p), ("dihedral_params", C.c_void_p),
+        ("n_impropers", C.c_int), ("improper_atoms", C.c_void_p), ("improper_params", C.c_void_p),
     ]
 
 
@@ -112,6 +114,7 @@ def load() -> C.CDLL:
     lib.pmgpu_force_pme_add.argtypes = [vp, dbl, dbl, i32, vp, i32, i32, dbl, C.POINTER(i32)]
     lib.pmgpu_force_gb_add.argtypes = [vp, dbl, dbl, C.POINTER(i32)]
     lib.pmgpu_force_bonded_add.argtypes = [vp, i32, i32, C.POINTER(i32)]
+    lib.pmgpu_force_torsion_add.argtypes = [vp, i32, i32, C.POINTER(i32)]
     lib.pmgpu_force_set_enabled.argtypes = [vp, i32, i32]
     lib.pmgpu_evaluate.argtypes = [vp, vp, vp]
     lib.pmgpu_force_evaluate.argtypes = [vp, i32, vp, vp, vp, vp]

@@ -1,6 +1,7 @@
 // The C ABI of libpmgpu (include/pmgpu.h): contexts, systems, forces,
 // evaluation and device-resident integration.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -178,7 +179,10 @@ static int system_free(System *s) {
   for (auto &nl : s->lists) nb_list_free(s, &nl);
   void *ptrs[] = {s->d_charge, s->d_mass, s->d_type, s->d_mol, s->d_lj32, s->d_lj64,
                   s->d_excl_start, s->d_excl_partner, s->d_excl_class, s->d_excl_pairs,
+                  s->d_excl_range,
                   s->d_bond_atoms, s->d_angle_atoms, s->d_bond_params, s->d_angle_params,
+                  s->d_dihedral_atoms, s->d_dihedral_params, s->d_improper_atoms,
+                  s->d_improper_params,
                   s->d_gb_vdwr, s->d_gb_scale, s->d_gb_offset, s->d_water, s->d_gb_born,
                   s->d_gb_psi, s->d_gb_partial, s->d_gb_fixed, s->d_pos, s->d_vel,
                   s->d_force, s->d_acc, s->d_status, s->d_pairbuf, s->d_paircount,
@@ -283,6 +287,12 @@ static int evaluate_forces(System *s, int only, int mode) {
   const int em = mode == PAIR_FORCE ? 0 : (want_virial ? 2 : 1);
   std::vector<Launch> groups;
   std::vector<int> prepared(s->lists.size(), 0);
+  int sf_lj = 0, sf_coul = 0, sf_done = 0;
+  for (auto &f : s->forces)
+    if (f.kind == FK_SIMPLEFULL && f.enabled) {
+      sf_lj |= f.sf_lj;
+      sf_coul |= f.sf_coul;
+    }
   for (auto &f : s->forces) {
     if (only >= 0 ? f.id != only : !f.enabled) continue;
     if (f.kind == FK_CUTOFF || (f.kind == FK_PME && (f.ewald_flags & PMGPU_EWALD_REAL)))
@@ -338,9 +348,18 @@ static int evaluate_forces(System *s, int only, int mode) {
         prof_end(s);
         s->kernels += (f.bonds && s->n_bonds > 0) + (f.angles && s->n_angles > 0);
         break;
+      case FK_TORSION:
+        prof_begin(s, PMGPU_PHASE_BONDED);
+        r = torsion_forces(s, &f, em);
+        prof_end(s);
+        s->kernels += (f.dihedrals && s->n_dihedrals > 0) + (f.impropers && s->n_impropers > 0);
+        break;
       case FK_SIMPLEFULL:
+        // all enabled simple-full terms share one all-pairs pass
+        if (sf_done) break;
+        sf_done = 1;
         prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
-        r = nb_simplefull(s, f.sf_lj, f.sf_coul, want_virial);
+        r = nb_simplefull(s, only >= 0 ? f.sf_lj : sf_lj, only >= 0 ? f.sf_coul : sf_coul, em);
         prof_end(s);
         s->kernels += 1;
         break;
@@ -526,6 +545,15 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
     partner[cur[a]] = b; cls[cur[a]++] = c;
     partner[cur[b]] = a; cls[cur[b]++] = c;
   }
+  // index range of each atom's exclusion partners: pair loops consult the
+  // table only for partners inside it
+  std::vector<int2> range(std::max(1, n), make_int2(INT_MAX, -1));
+  for (int i = 0; i < n; i++)
+    for (int k = start[i]; k < start[i + 1]; k++) {
+      range[i].x = std::min(range[i].x, partner[k]);
+      range[i].y = std::max(range[i].y, partner[k]);
+    }
+  PM_CHECK(upload(s.get(), &s->d_excl_range, range.data(), (size_t)std::max(1, n)));
   PM_CHECK(upload(s.get(), &s->d_excl_start, start.data(), n + 1));
   PM_CHECK(upload(s.get(), &s->d_excl_partner, partner.data(), 2 * (size_t)ne + 1));
   PM_CHECK(upload(s.get(), &s->d_excl_class, cls.data(), 2 * (size_t)ne + 1));
@@ -549,6 +577,18 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   PM_CHECK(upload(s.get(), &s->d_bond_params, s->n_bonds ? t->bond_params : (const double *)nullptr, 2 * (size_t)s->n_bonds));
   PM_CHECK(upload(s.get(), &s->d_angle_atoms, s->n_angles ? t->angle_atoms : (const int *)nullptr, 3 * (size_t)s->n_angles));
   PM_CHECK(upload(s.get(), &s->d_angle_params, s->n_angles ? t->angle_params : (const double *)nullptr, 4 * (size_t)s->n_angles));
+  s->n_dihedrals = t->dihedral_atoms ? t->n_dihedrals : 0;
+  s->n_impropers = t->improper_atoms ? t->n_impropers : 0;
+  for (int k = 0; k < 4 * s->n_dihedrals; k++)
+    if (t->dihedral_atoms[k] < 0 || t->dihedral_atoms[k] >= n)
+      return fail(PMGPU_ERR_ARG, "dihedral atom index out of range");
+  for (int k = 0; k < 4 * s->n_impropers; k++)
+    if (t->improper_atoms[k] < 0 || t->improper_atoms[k] >= n)
+      return fail(PMGPU_ERR_ARG, "improper atom index out of range");
+  PM_CHECK(upload(s.get(), &s->d_dihedral_atoms, s->n_dihedrals ? t->dihedral_atoms : (const int *)nullptr, 4 * (size_t)s->n_dihedrals));
+  PM_CHECK(upload(s.get(), &s->d_dihedral_params, s->n_dihedrals ? t->dihedral_params : (const double *)nullptr, 3 * (size_t)s->n_dihedrals));
+  PM_CHECK(upload(s.get(), &s->d_improper_atoms, s->n_impropers ? t->improper_atoms : (const int *)nullptr, 4 * (size_t)s->n_impropers));
+  PM_CHECK(upload(s.get(), &s->d_improper_params, s->n_impropers ? t->improper_params : (const double *)nullptr, 3 * (size_t)s->n_impropers));
   if (t->gb_vdwr && t->gb_scale && t->gb_offset) {
     PM_CHECK(upload(s.get(), &s->d_gb_vdwr, t->gb_vdwr, n));
     PM_CHECK(upload(s.get(), &s->d_gb_scale, t->gb_scale, n));
@@ -837,6 +877,15 @@ int pmgpu_force_bonded_add(pmgpu_system *h, int bonds, int angles, int *force_id
   f.kind = FK_BONDED;
   f.bonds = bonds ? 1 : 0;
   f.angles = angles ? 1 : 0;
+  return add_force(sysp(h), f, force_id);
+}
+
+int pmgpu_force_torsion_add(pmgpu_system *h, int dihedrals, int impropers, int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  Force f;
+  f.kind = FK_TORSION;
+  f.dihedrals = dihedrals ? 1 : 0;
+  f.impropers = impropers ? 1 : 0;
   return add_force(sysp(h), f, force_id);
 }
 

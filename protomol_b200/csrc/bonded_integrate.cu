@@ -115,6 +115,137 @@ __global__ void k_angles(Box box, int na, const int *__restrict__ atoms,
   }
 }
 
+__device__ __forceinline__ void dcross(const double *u, const double *v, double *o) {
+  o[0] = u[1] * v[2] - u[2] * v[1];
+  o[1] = u[2] * v[0] - u[0] * v[2];
+  o[2] = u[0] * v[1] - u[1] * v[0];
+}
+__device__ __forceinline__ double ddot(const double *u, const double *v) {
+  return u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+}
+
+// MTorsionSystemForce::calcTorsion (force/bonded/MTorsionSystemForce.h:40-204),
+// one term per thread: the dihedral angle from the normals of the (1,2,3)
+// and (2,3,4) planes; the gradient goes through d cos(phi) when
+// |sin phi| > 0.1 and through d sin(phi) otherwise.  params: k,
+// periodicity n, phase delta; n > 0 cosine form, n == 0 harmonic.
+__global__ void k_torsions(Box box, int nt, const int *__restrict__ atoms,
+                           const double *__restrict__ prm, const double *__restrict__ pos,
+                           int n, long long *__restrict__ force, long long *__restrict__ acc,
+                           int slot, int em) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
+  if (t < nt) {
+    const int a1 = atoms[4 * t], a2 = atoms[4 * t + 1], a3 = atoms[4 * t + 2],
+              a4 = atoms[4 * t + 3];
+    const double k = prm[3 * t], delta = prm[3 * t + 2];
+    const int per = (int)prm[3 * t + 1];
+    double r12[3], r23[3], r34[3];
+    box_mindiff(box, pos[3 * a2], pos[3 * a2 + 1], pos[3 * a2 + 2], pos[3 * a1],
+                pos[3 * a1 + 1], pos[3 * a1 + 2], r12[0], r12[1], r12[2]);
+    box_mindiff(box, pos[3 * a3], pos[3 * a3 + 1], pos[3 * a3 + 2], pos[3 * a2],
+                pos[3 * a2 + 1], pos[3 * a2 + 2], r23[0], r23[1], r23[2]);
+    box_mindiff(box, pos[3 * a4], pos[3 * a4 + 1], pos[3 * a4 + 2], pos[3 * a3],
+                pos[3 * a3 + 1], pos[3 * a3 + 2], r34[0], r34[1], r34[2]);
+    double na[3], nb[3], nc[3];
+    dcross(r12, r23, na);
+    dcross(r23, r34, nb);
+    dcross(r23, na, nc);
+    const double ia = 1.0 / sqrt(ddot(na, na)), ib = 1.0 / sqrt(ddot(nb, nb)),
+                 ic = 1.0 / sqrt(ddot(nc, nc));
+    for (int c = 0; c < 3; c++) {
+      na[c] *= ia;
+      nb[c] *= ib;
+      nc[c] *= ic;
+    }
+    const double cphi = ddot(na, nb), sphi = ddot(nc, nb);
+    const double phi = -atan2(sphi, cphi);
+    double dvdphi;
+    if (per > 0) {
+      dvdphi = -per * k * sin(per * phi + delta);
+      e = k * (1.0 + cos(per * phi + delta));
+    } else {
+      double diff = phi - delta;
+      if (diff < -M_PI) diff += 2 * M_PI;
+      else if (diff > M_PI) diff -= 2 * M_PI;
+      dvdphi = 2.0 * k * diff;
+      e = k * diff * diff;
+    }
+    double f1[3], f2[3], f3[3], t1[3], t2[3];
+    if (fabs(sphi) > 0.1) {
+      double ga[3], gb[3];
+      const double g = dvdphi / sphi;
+      for (int c = 0; c < 3; c++) {
+        ga[c] = (na[c] * cphi - nb[c]) * ia;
+        gb[c] = (nb[c] * cphi - na[c]) * ib;
+      }
+      dcross(r23, ga, t1);
+      dcross(gb, r23, t2);
+      for (int c = 0; c < 3; c++) {
+        f1[c] = g * t1[c];
+        f3[c] = g * t2[c];
+      }
+      dcross(ga, r12, t1);
+      dcross(r34, gb, t2);
+      for (int c = 0; c < 3; c++) f2[c] = g * (t1[c] + t2[c]);
+    } else {
+      double gc[3], gb[3];
+      const double g = -dvdphi / cphi;
+      for (int c = 0; c < 3; c++) {
+        gc[c] = (nc[c] * sphi - nb[c]) * ic;
+        gb[c] = (nb[c] * sphi - nc[c]) * ib;
+      }
+      const double r23sq = ddot(r23, r23), r23gc = ddot(r23, gc);
+      for (int c = 0; c < 3; c++) f1[c] = g * (r23sq * gc[c] - r23[c] * r23gc);
+      dcross(gb, r23, t1);
+      for (int c = 0; c < 3; c++) f3[c] = g * t1[c];
+      for (int c = 0; c < 3; c++) {
+        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+        f2[c] = g * (-(r23[c1] * r12[c1] + r23[c2] * r12[c2]) * gc[c] +
+                     (2.0 * r23[c] * r12[c1] - r12[c] * r23[c1]) * gc[c1] +
+                     (2.0 * r23[c] * r12[c2] - r12[c] * r23[c2]) * gc[c2] +
+                     gb[c2] * r34[c1] - gb[c1] * r34[c2]);
+      }
+    }
+    for (int c = 0; c < 3; c++) {
+      red_add(&force[c * n + a1], to_fixed(f1[c], kForceScale));
+      red_add(&force[c * n + a2], to_fixed(f2[c] - f1[c], kForceScale));
+      red_add(&force[c * n + a3], to_fixed(f3[c] - f2[c], kForceScale));
+      red_add(&force[c * n + a4], to_fixed(-f3[c], kForceScale));
+    }
+    if (em == 2) {
+      // upper triangle (xx, xy, xz, yy, yz, zz), mirrored below
+      int q = 0;
+      for (int i = 0; i < 3; i++)
+        for (int j = i; j < 3; j++) v[q++] = f1[i] * r12[j] + f2[i] * r23[j] + f3[i] * r34[j];
+    }
+  }
+  if (!em) return;
+  e = warp_sum(e);
+  if (em == 2)
+    for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
+  if ((threadIdx.x & 31) == 0) {
+    red_add(&acc[slot], to_fixed(e, kEnergyScale));
+    if (em == 2) {
+      const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+      for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
+    }
+  }
+}
+
+int torsion_forces(System *s, Force *f, int em) {
+  if (f->dihedrals && s->n_dihedrals > 0)
+    k_torsions<<<(s->n_dihedrals + 127) / 128, 128, 0, s->stream>>>(
+        s->box, s->n_dihedrals, s->d_dihedral_atoms, s->d_dihedral_params, s->d_pos, s->n,
+        s->d_force, s->d_acc, ACC_DIHEDRAL, em);
+  if (f->impropers && s->n_impropers > 0)
+    k_torsions<<<(s->n_impropers + 127) / 128, 128, 0, s->stream>>>(
+        s->box, s->n_impropers, s->d_improper_atoms, s->d_improper_params, s->d_pos, s->n,
+        s->d_force, s->d_acc, ACC_IMPROPER, em);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
 int bonded_forces(System *s, Force *f, int em) {
   if (f->bonds && s->n_bonds > 0) {
     k_bonds<<<(s->n_bonds + 127) / 128, 128, 0, s->stream>>>(

@@ -18,7 +18,17 @@
 namespace pmgpu {
 
 constexpr double kGbScale = 1099511627776.0;  // 2^40 for per-atom GB sums
-constexpr int kGbTile = 128;
+constexpr int kGbTile = 64;
+
+// 2-D launch shape of the all-pairs passes: enough j chunks (whole tiles)
+// that about eight blocks land on every SM.
+static void gb_grid(int n, dim3 *grid, int *jchunk) {
+  const int iblocks = (n + kGbTile - 1) / kGbTile;
+  int chunks = std::max(1, std::min((148 * 8 + iblocks - 1) / iblocks, iblocks));
+  *jchunk = ((n + chunks - 1) / chunks + kGbTile - 1) / kGbTile * kGbTile;
+  chunks = (n + *jchunk - 1) / *jchunk;
+  *grid = dim3(iblocks, chunks);
+}
 
 struct GbArgs {
   int n;
@@ -27,7 +37,8 @@ struct GbArgs {
   double alpha, beta, gamma;
   double dielec;  // 1/solute - 1/solvent
   long long *burial_fx, *partial_fx;  // fixed-point accumulators
-  double *born, *psi, *partial;
+  double *born, *partial;
+  double *psi;  // per atom dR/d(burial sum) factor of the force pass
   long long *force, *acc;
 };
 
@@ -100,9 +111,13 @@ __global__ void k_gb_radii(GbArgs a) {
     double oi = ri - a.offset[i];
     double psi = 0.5 * burial * oi;
     double tp = a.alpha * psi - a.beta * psi * psi + a.gamma * psi * psi * psi;
-    double inv = (1 / oi) - (1 / ri) * tanh(tp);
+    double th = tanh(tp);
+    double inv = (1 / oi) - (1 / ri) * th;
     double born = 1 / inv;
-    a.psi[i] = psi;
+    // dR_i/d(burial sum) (GBForce.cpp:108-118 without the pair factor dBT):
+    // R_i^2 rho~_i (1 - tanh^2) (alpha - 2 beta psi + 3 gamma psi^2) / rho_i
+    double td = a.alpha - 2.0 * a.beta * psi + 3.0 * a.gamma * psi * psi;
+    a.psi[i] = born * born * oi * (1.0 - th * th) * td / ri;
     a.born[i] = born;
     a.burial_fx[i] = 0;
     a.partial_fx[i] = 0;
@@ -159,11 +174,10 @@ __global__ void k_gb_partial_fin(GbArgs a) {
   if (i < a.n) a.partial[i] = (double)a.partial_fx[i] * (1.0 / kGbScale);
 }
 
-// dBT/dr and dR/dr of GBForce::operator() (GBForce.cpp:70-124) for the
-// "i sees j" direction.
+// dBT/dr of GBForce::operator() (GBForce.cpp:70-124) for the "i sees j"
+// direction; dR_i/dr is this times the per-atom factor k_gb_radii stores.
 template <typename Real>
-__device__ __forceinline__ Real gb_dR(Real dist, Real oi, Real ri, Real bi, Real psi_i,
-                                      Real oj, Real Sj, Real alpha, Real beta, Real gamma) {
+__device__ __forceinline__ Real gb_dBT(Real dist, Real oi, Real oj, Real Sj) {
   Real sjoj = Sj * oj;
   Real L, U;
   if (oi >= dist + sjoj) {
@@ -177,34 +191,29 @@ __device__ __forceinline__ Real gb_dR(Real dist, Real oi, Real ri, Real bi, Real
   Real dL = (oi <= (dist - sjoj)) ? Real(1) : Real(0);
   Real dU = (oi < (dist + sjoj)) ? Real(1) : Real(0);
   Real dC = (oi <= (sjoj - dist)) ? Real(2) * iL * iL * dL : Real(0);
-  Real tp = alpha * psi_i - beta * psi_i * psi_i + gamma * psi_i * psi_i * psi_i;
-  Real th = tanh(tp);
-  Real td = alpha - Real(2) * beta * psi_i + Real(3) * gamma * psi_i * psi_i;
   Real Sjt = sjoj / dist;
   Real iL2 = iL * iL, iU2 = iU * iU;
-  Real dBT = Real(-0.5) * dL * iL2 + Real(0.5) * dU * iU2 + Real(0.125) * (iU2 - iL2) +
-             Real(0.125) * dist * (Real(2) * iL2 * iL * dL - Real(2) * iU2 * iU * dU) -
-             Real(0.25) * (Real(1) / (dist * dist)) * log(L / U) +
-             (U / (Real(4) * dist * L)) * (iU * dL - (L * iU2) * dU) -
-             Real(0.125) * (Sjt * Sjt) * (iL2 - iU2) +
-             Real(0.25) * ((sjoj * sjoj) / dist) * iU2 * iU * dU -
-             Real(0.25) * ((sjoj * sjoj) / dist) * iL2 * iL * dL + dC;
-  return (bi * bi) * oi * (Real(1) - th * th) * td * (Real(1) / ri) * dBT;
+  return Real(-0.5) * dL * iL2 + Real(0.5) * dU * iU2 + Real(0.125) * (iU2 - iL2) +
+         Real(0.125) * dist * (Real(2) * iL2 * iL * dL - Real(2) * iU2 * iU * dU) -
+         Real(0.25) * (Real(1) / (dist * dist)) * log(L / U) +
+         (U / (Real(4) * dist * L)) * (iU * dL - (L * iU2) * dU) -
+         Real(0.125) * (Sjt * Sjt) * (iL2 - iU2) +
+         Real(0.25) * ((sjoj * sjoj) / dist) * iU2 * iU * dU -
+         Real(0.25) * ((sjoj * sjoj) / dist) * iL2 * iL * dL + dC;
 }
 
 template <typename Real>
 __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
   __shared__ double sx[kGbTile], sy[kGbTile], sz[kGbTile], sb[kGbTile], sq[kGbTile];
-  __shared__ double sr[kGbTile], so[kGbTile], ss[kGbTile], sp[kGbTile], spart[kGbTile];
+  __shared__ double so[kGbTile], ss[kGbTile], sp[kGbTile], spart[kGbTile];
   int i = blockIdx.x * kGbTile + threadIdx.x;
   bool valid = i < a.n;
   int ii = valid ? i : 0;
   double xi = a.pos[3 * ii], yi = a.pos[3 * ii + 1], zi = a.pos[3 * ii + 2];
   Real bi = (Real)a.born[ii], qi = (Real)a.charge[ii];
-  Real ri = (Real)a.vdwr[ii], oi = (Real)(a.vdwr[ii] - a.offset[ii]);
-  Real Si = (Real)a.scale[ii], psi_i = (Real)a.psi[ii];
+  Real oi = (Real)(a.vdwr[ii] - a.offset[ii]);
+  Real Si = (Real)a.scale[ii], dfac_i = (Real)a.psi[ii];
   Real part_i = (Real)a.partial[ii];
-  Real al = (Real)a.alpha, be = (Real)a.beta, ga = (Real)a.gamma;
   Real fx = 0, fy = 0, fz = 0;
   double epair = 0.0;
   int j0 = blockIdx.y * jchunk, j1 = min(a.n, j0 + jchunk);
@@ -214,7 +223,7 @@ __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
       sx[threadIdx.x] = a.pos[3 * j]; sy[threadIdx.x] = a.pos[3 * j + 1];
       sz[threadIdx.x] = a.pos[3 * j + 2];
       sb[threadIdx.x] = a.born[j]; sq[threadIdx.x] = a.charge[j];
-      sr[threadIdx.x] = a.vdwr[j]; so[threadIdx.x] = a.vdwr[j] - a.offset[j];
+      so[threadIdx.x] = a.vdwr[j] - a.offset[j];
       ss[threadIdx.x] = a.scale[j]; sp[threadIdx.x] = a.psi[j];
       spart[threadIdx.x] = a.partial[j];
     }
@@ -227,24 +236,25 @@ __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
         Real dx = (Real)(sx[k] - xi), dy = (Real)(sy[k] - yi), dz = (Real)(sz[k] - zi);
         Real r2 = dx * dx + dy * dy + dz * dz;
         Real dist = pm_sqrt(r2);
+        Real idist = Real(1) / dist;
         Real bj = (Real)sb[k], qj = (Real)sq[k];
-        Real oj = (Real)so[k], rj = (Real)sr[k], Sj = (Real)ss[k];
+        Real oj = (Real)so[k], Sj = (Real)ss[k];
         Real ex = exp(-r2 / (Real(4) * bi * bj));
         Real fGB = pm_sqrt(r2 + bi * bj * ex);
         ep += -(qi * qj) / fGB;
-        Real dRi = gb_dR<Real>(dist, oi, ri, bi, psi_i, oj, Sj, al, be, ga);
-        Real dRj = gb_dR<Real>(dist, oj, rj, bj, (Real)sp[k], oi, Si, al, be, ga);
+        Real dRi = dfac_i * gb_dBT<Real>(dist, oi, oj, Sj);
+        Real dRj = (Real)sp[k] * gb_dBT<Real>(dist, oj, oi, Si);
         Real pref = qi * qj * (Real(1) / (fGB * fGB)) * Real(0.5) * (Real(1) / fGB);
         // partialTerm[i][j] and [j][i] (GBPartialSum.cpp:33-41)
         Real ptij = pref * ex * (bj + r2 / (Real(4) * bi));
         Real ptji = pref * ex * (bi + r2 / (Real(4) * bj));
         Real f = -pref * ((Real(2) * dist - Real(0.5) * ex * dist) +
                           ex * dRi * (bj + r2 / (Real(4) * bi)) +
-                          ex * dRj * (bi + r2 / (Real(4) * bj))) / dist;
-        f -= Real(0.5) * qi * qi * dRi / (bi * bi) / dist;
-        f -= Real(0.5) * qj * qj * dRj / (bj * bj) / dist;
-        f -= (part_i - ptij) * (dRi / dist);
-        f -= ((Real)spart[k] - ptji) * (dRj / dist);
+                          ex * dRj * (bi + r2 / (Real(4) * bj))) * idist;
+        f -= Real(0.5) * qi * qi * dRi / (bi * bi) * idist;
+        f -= Real(0.5) * qj * qj * dRj / (bj * bj) * idist;
+        f -= (part_i - ptij) * (dRi * idist);
+        f -= ((Real)spart[k] - ptji) * (dRj * idist);
         fx -= dx * f; fy -= dy * f; fz -= dz * f;
       }
       epair += (double)ep;
@@ -261,8 +271,6 @@ __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
   if ((threadIdx.x & 31) == 0) red_add(&a.acc[ACC_COULOMB], to_fixed(epair, kEnergyScale));
 }
 
-static long long *g_dummy = nullptr;
-
 int gb_init(System *s) {
   int n = std::max(1, s->n);
   if (!s->d_gb_vdwr) return fail(PMGPU_ERR_ARG, "GB force needs gb_vdwr/gb_scale/gb_offset");
@@ -273,7 +281,6 @@ int gb_init(System *s) {
     PM_CHECK(dev_alloc(s, &s->d_gb_fixed, sizeof(long long) * 2 * n));
     PM_CUDA(cudaMemsetAsync(s->d_gb_fixed, 0, sizeof(long long) * 2 * n, s->stream));
   }
-  (void)g_dummy;
   return PMGPU_OK;
 }
 
@@ -299,12 +306,9 @@ int gb_forces(System *s, Force *f) {
   a.partial = s->d_gb_partial;
   a.force = s->d_force;
   a.acc = s->d_acc;
-  int iblocks = (n + kGbTile - 1) / kGbTile;
-  // enough j chunks to put ~2 blocks on every SM
-  int chunks = std::max(1, std::min((296 + iblocks - 1) / iblocks, (n + kGbTile - 1) / kGbTile));
-  int jchunk = ((n + chunks - 1) / chunks + kGbTile - 1) / kGbTile * kGbTile;
-  chunks = (n + jchunk - 1) / jchunk;
-  dim3 grid(iblocks, chunks);
+  dim3 grid;
+  int jchunk;
+  gb_grid(n, &grid, &jchunk);
   cudaStream_t st = s->stream;
   if (s->precision == PMGPU_PREC_MIXED) {
     k_gb_burial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
@@ -467,11 +471,9 @@ extern "C" int pmgpu_gb_forces_noalloc(int n_atoms, const double *pos, const dou
   PM_CUDA(cudaMemsetAsync(a.burial_fx, 0, sizeof(long long) * (5 * (size_t)n + kGbStaticAccWords),
                           st));
 
-  int iblocks = (n + kGbTile - 1) / kGbTile;
-  int chunks = std::max(1, std::min((296 + iblocks - 1) / iblocks, (n + kGbTile - 1) / kGbTile));
-  int jchunk = ((n + chunks - 1) / chunks + kGbTile - 1) / kGbTile * kGbTile;
-  chunks = (n + jchunk - 1) / jchunk;
-  dim3 grid(iblocks, chunks);
+  dim3 grid;
+  int jchunk;
+  gb_grid(n, &grid, &jchunk);
   if (precision == PMGPU_PREC_MIXED) {
     k_gb_burial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
     k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);

@@ -775,70 +775,80 @@ int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims) {
 
 // --------------------------------------------------- NonbondedSimpleFull
 // Vacuum all pairs with exclusions (NonbondedSimpleFullSystemForce.h:125-150
-// with OneAtomPair<Vacuum, Universal, LennardJones|Coulomb>): block tiles of
-// 128 i atoms against j tiles staged in shared memory; every i sees every
-// j != i, energies halved.
+// with OneAtomPair<Vacuum, Universal, LennardJones|Coulomb>): a 2-D grid of
+// (128 i atoms) x (a chunk of j) blocks, j tiles staged in shared memory;
+// every i sees every j != i (forces for i only), energies halved.  The
+// exclusion table is consulted only for j inside i's partner-index range.
+constexpr int kSfTile = 128;
+
 template <typename Real, bool LJ, bool COUL>
-__global__ void __launch_bounds__(128)
-k_simplefull(int n, const double *__restrict__ pos, const double *__restrict__ charge,
-             const int *__restrict__ type, const int *__restrict__ mol, int ntypes,
-             const double4 *__restrict__ lj64, const int *__restrict__ ex_start,
-             const int *__restrict__ ex_partner, const int *__restrict__ ex_class,
-             Real csf, long long *__restrict__ force, long long *__restrict__ acc,
-             int want_virial) {
-  __shared__ double sx[128], sy[128], sz[128], sq[128];
-  __shared__ int st[128], sm[128];
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool valid = i < n;
-  double xi = 0, yi = 0, zi = 0, qi = 0;
-  int ti = 0, mi = -1;
-  if (valid) {
-    xi = pos[3 * i]; yi = pos[3 * i + 1]; zi = pos[3 * i + 2];
-    qi = charge[i]; ti = type[i]; mi = mol[i];
-  }
+__global__ void __launch_bounds__(kSfTile)
+k_simplefull(int n, int jchunk, const double *__restrict__ pos,
+             const double *__restrict__ charge, const int *__restrict__ type, int ntypes,
+             const float4 *__restrict__ lj32, const double4 *__restrict__ lj64,
+             const int2 *__restrict__ ex_range, const int *__restrict__ ex_start,
+             const int *__restrict__ ex_partner, const int *__restrict__ ex_class, Real csf,
+             long long *__restrict__ force, long long *__restrict__ acc, int em) {
+  __shared__ double sx[kSfTile], sy[kSfTile], sz[kSfTile], sq[kSfTile];
+  __shared__ int st[kSfTile];
+  const int i = blockIdx.x * kSfTile + threadIdx.x;
+  const bool valid = i < n;
+  const int ii = valid ? i : 0;
+  const double xi = pos[3 * ii], yi = pos[3 * ii + 1], zi = pos[3 * ii + 2];
+  const double qi = charge[ii];
+  const int ti = type[ii];
+  const int2 er = ex_range[ii];
   Real fx = 0, fy = 0, fz = 0;
   double elj = 0, ec = 0;
   double v[6] = {0, 0, 0, 0, 0, 0};
-  for (int base = 0; base < n; base += 128) {
-    int j = base + threadIdx.x;
-    if (j < n) {
+  const int j0 = blockIdx.y * jchunk, j1 = min(n, j0 + jchunk);
+  for (int base = j0; base < j1; base += kSfTile) {
+    const int j = base + threadIdx.x;
+    if (j < j1) {
       sx[threadIdx.x] = pos[3 * j]; sy[threadIdx.x] = pos[3 * j + 1];
       sz[threadIdx.x] = pos[3 * j + 2]; sq[threadIdx.x] = charge[j];
-      st[threadIdx.x] = type[j]; sm[threadIdx.x] = mol[j];
+      st[threadIdx.x] = type[j];
     }
     __syncthreads();
-    int lim = min(128, n - base);
+    const int lim = min(kSfTile, j1 - base);
     if (valid) {
       for (int k = 0; k < lim; k++) {
-        int jj = base + k;
+        const int jj = base + k;
         if (jj == i) continue;
         int excl = PMGPU_EXCL_NONE;
-        if (sm[k] == mi) {
+        if (jj >= er.x && jj <= er.y) {
           excl = excl_class_of(ex_start, ex_partner, ex_class, i, jj);
           if (excl == PMGPU_EXCL_FULL) continue;
         }
-        Real dx = (Real)(sx[k] - xi), dy = (Real)(sy[k] - yi), dz = (Real)(sz[k] - zi);
-        Real r2 = dx * dx + dy * dy + dz * dz;
-        Real rr2 = Real(1) / r2;
+        const Real dx = (Real)(sx[k] - xi), dy = (Real)(sy[k] - yi), dz = (Real)(sz[k] - zi);
+        const Real r2 = dx * dx + dy * dy + dz * dz;
+        const Real rr2 = Real(1) / r2;
         Real f = 0;
         if (LJ) {
-          double4 p = lj64[ti * ntypes + st[k]];
-          Real A = (Real)(excl == PMGPU_EXCL_MODIFIED ? p.z : p.x);
-          Real B = (Real)(excl == PMGPU_EXCL_MODIFIED ? p.w : p.y);
-          Real r6 = rr2 * rr2 * rr2;
-          Real r6B = B * r6, r12A = A * r6 * r6;
-          elj += (double)(r12A - r6B);
+          Real A, B;
+          if (sizeof(Real) == 4) {
+            const float4 p = __ldg(&lj32[ti * ntypes + st[k]]);
+            A = excl == PMGPU_EXCL_MODIFIED ? p.z : p.x;
+            B = excl == PMGPU_EXCL_MODIFIED ? p.w : p.y;
+          } else {
+            const double4 p = lj64[ti * ntypes + st[k]];
+            A = excl == PMGPU_EXCL_MODIFIED ? p.z : p.x;
+            B = excl == PMGPU_EXCL_MODIFIED ? p.w : p.y;
+          }
+          const Real r6 = rr2 * rr2 * rr2;
+          const Real r6B = B * r6, r12A = A * r6 * r6;
+          if (em) elj += (double)(r12A - r6B);
           f += (Real(12) * r12A - Real(6) * r6B) * rr2;
         }
         if (COUL) {
           Real en = (Real)(qi * sq[k]) * pm_sqrt(rr2);
           if (excl == PMGPU_EXCL_MODIFIED) en *= csf;
-          ec += (double)en;
+          if (em) ec += (double)en;
           f += en * rr2;
         }
         fx -= dx * f; fy -= dy * f; fz -= dz * f;
-        if (want_virial) {
-          double hf = 0.5 * (double)f;
+        if (em == 2) {
+          const double hf = 0.5 * (double)f;
           v[0] += dx * dx * hf; v[1] += dx * dy * hf; v[2] += dx * dz * hf;
           v[3] += dy * dy * hf; v[4] += dy * dz * hf; v[5] += dz * dz * hf;
         }
@@ -851,36 +861,44 @@ k_simplefull(int n, const double *__restrict__ pos, const double *__restrict__ c
     red_add(&force[n + i], to_fixed((double)fy, kForceScale));
     red_add(&force[2 * n + i], to_fixed((double)fz, kForceScale));
   }
+  if (!em) return;
   elj = warp_sum(elj) * 0.5;
   ec = warp_sum(ec) * 0.5;
-  for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
+  if (em == 2)
+    for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
   if ((threadIdx.x & 31) == 0) {
     if (LJ) red_add(&acc[ACC_LJ], to_fixed(elj, kEnergyScale));
     if (COUL) red_add(&acc[ACC_COULOMB], to_fixed(ec, kEnergyScale));
-    if (want_virial) {
+    if (em == 2) {
       const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
       for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
     }
   }
 }
 
-int nb_simplefull(System *s, int lj, int coul, int want_virial) {
-  int n = s->n;
+// em: 0 forces only, 1 + energies, 2 + energies and virial.
+int nb_simplefull(System *s, int lj, int coul, int em) {
+  const int n = s->n;
   if (n == 0 || !(lj || coul)) return PMGPU_OK;
-  int nb = (n + 127) / 128;
+  // enough j chunks for ~2 blocks per SM
+  const int iblocks = (n + kSfTile - 1) / kSfTile;
+  int chunks = std::max(1, std::min((296 + iblocks - 1) / iblocks, iblocks));
+  const int jchunk = ((n + chunks - 1) / chunks + kSfTile - 1) / kSfTile * kSfTile;
+  chunks = (n + jchunk - 1) / jchunk;
+  const dim3 grid(iblocks, chunks);
   auto go = [&](auto kern, auto csf) {
-    kern<<<nb, 128, 0, s->stream>>>(n, s->d_pos, s->d_charge, s->d_type, s->d_mol,
-                                    s->ntypes, s->d_lj64, s->d_excl_start,
-                                    s->d_excl_partner, s->d_excl_class, csf, s->d_force,
-                                    s->d_acc, want_virial);
+    kern<<<grid, kSfTile, 0, s->stream>>>(n, jchunk, s->d_pos, s->d_charge, s->d_type,
+                                          s->ntypes, s->d_lj32, s->d_lj64, s->d_excl_range,
+                                          s->d_excl_start, s->d_excl_partner, s->d_excl_class,
+                                          csf, s->d_force, s->d_acc, em);
   };
   if (s->precision == PMGPU_PREC_MIXED) {
-    float csf = (float)s->coulomb_scaling;
+    const float csf = (float)s->coulomb_scaling;
     if (lj && coul) go(k_simplefull<float, true, true>, csf);
     else if (lj) go(k_simplefull<float, true, false>, csf);
     else go(k_simplefull<float, false, true>, csf);
   } else {
-    double csf = s->coulomb_scaling;
+    const double csf = s->coulomb_scaling;
     if (lj && coul) go(k_simplefull<double, true, true>, csf);
     else if (lj) go(k_simplefull<double, true, false>, csf);
     else go(k_simplefull<double, false, true>, csf);

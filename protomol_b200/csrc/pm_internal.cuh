@@ -171,11 +171,12 @@ struct Force {
   double solute = 1.0, solvent = 80.0;
   // bonded
   int bonds = 0, angles = 0;
+  int dihedrals = 0, impropers = 0;
   long long last_pairs = 0;
 };
 
 enum { FK_CUTOFF = 1, FK_PME = 2, FK_GB = 3, FK_BONDED = 4,
-       FK_SIMPLEFULL = 5 };
+       FK_SIMPLEFULL = 5, FK_TORSION = 6 };
 
 // Per-phase CUDA-event timing; events are recorded only when enabled and
 // summed at the next host synchronisation.
@@ -217,10 +218,14 @@ struct System {
   int *d_excl_start = nullptr, *d_excl_partner = nullptr;  // CSR
   int *d_excl_class = nullptr;
   int *d_excl_pairs = nullptr;  // 3 per exclusion (a1, a2, class)
+  int2 *d_excl_range = nullptr; // per atom: lowest and highest partner index
   int n_excl = 0;
   int n_bonds = 0, n_angles = 0;
   int *d_bond_atoms = nullptr, *d_angle_atoms = nullptr;
   double *d_bond_params = nullptr, *d_angle_params = nullptr;
+  int n_dihedrals = 0, n_impropers = 0;
+  int *d_dihedral_atoms = nullptr, *d_improper_atoms = nullptr;
+  double *d_dihedral_params = nullptr, *d_improper_params = nullptr;
   // GB
   double *d_gb_vdwr = nullptr, *d_gb_scale = nullptr, *d_gb_offset = nullptr;
   int *d_water = nullptr;
@@ -291,7 +296,7 @@ int nb_list_free(System *s, NeighborList *nl);
 int nb_prepare(System *s, NeighborList *nl, int force_rebuild);
 int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode);
 int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
-int nb_simplefull(System *s, int lj, int coul, int want_virial);
+int nb_simplefull(System *s, int lj, int coul, int em);
 
 // pme.cu
 int pme_init(System *s, Force *f);
@@ -305,6 +310,7 @@ int gb_forces(System *s, Force *f);
 
 // bonded_integrate.cu
 int bonded_forces(System *s, Force *f, int em);
+int torsion_forces(System *s, Force *f, int em);
 int zero_forces(System *s);
 int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase);
 int set_device_step(System *s);

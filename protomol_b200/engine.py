@@ -122,6 +122,15 @@ class GpuSystem:
         if len(angles):
             t.angle_atoms = arr("angles", angles, np.int32)
             t.angle_params = arr("anglep", topo.angle_params, np.float64)
+        for kind in ("dihedral", "improper"):
+            atoms = getattr(topo, kind + "s", None)
+            if atoms is not None and len(np.asarray(atoms).reshape(-1)):
+                atoms = np.asarray(atoms).reshape(-1, 4)
+                setattr(t, "n_" + kind + "s", len(atoms))
+                setattr(t, kind + "_atoms", arr(kind + "a", atoms, np.int32))
+                setattr(t, kind + "_params",
+                        arr(kind + "p", np.asarray(getattr(topo, kind + "_params")).reshape(-1, 3),
+                            np.float64))
         if getattr(topo, "gb_vdwr", None) is not None:
             t.gb_vdwr = arr("vdwr", topo.gb_vdwr, np.float64)
             t.gb_scale = arr("scale", topo.gb_scale, np.float64)
@@ -346,6 +355,18 @@ class GBForce(SystemForce):
         super().__init__(system, fid.value)
 
 
+class TorsionSystemForce(SystemForce):
+    """``Dihedral`` and/or ``Improper`` (MTorsionSystemForce: cosine
+    torsions for periodicity > 0, harmonic for periodicity 0)."""
+    keyword = "Torsion"
+
+    def __init__(self, system: GpuSystem, dihedrals: bool = True, impropers: bool = True):
+        fid = C.c_int()
+        L.check(system.lib.pmgpu_force_torsion_add(system.h, int(dihedrals), int(impropers),
+                                                   C.byref(fid)))
+        super().__init__(system, fid.value)
+
+
 class BondedSystemForce(SystemForce):
     """``Bond`` and/or ``Angle`` (harmonic, with Urey-Bradley)."""
     keyword = "Bonded"
@@ -413,6 +434,8 @@ class ForceFactory:
         s = self.system
         if names and all(n in ("bond", "angle") for n in names):
             return BondedSystemForce(s, "bond" in names, "angle" in names)
+        if names and all(n in ("dihedral", "improper") for n in names):
+            return TorsionSystemForce(s, "dihedral" in names, "improper" in names)
         if algn == "nonbondedcutoff":
             if not switches:
                 raise ValueError("NonbondedCutoff needs -switchingFunction")

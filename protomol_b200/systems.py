@@ -51,6 +51,11 @@ class MolecularSystem:
     gb_scale: np.ndarray | None = None
     gb_offset: np.ndarray | None = None
     gb_obc: tuple = (1.0, 0.8, 4.85)
+    # torsions: (m,4) atoms and (m,3) k, periodicity, phase [rad]
+    dihedrals: np.ndarray | None = None
+    dihedral_params: np.ndarray | None = None
+    impropers: np.ndarray | None = None
+    improper_params: np.ndarray | None = None
     # PSF bookkeeping
     atom_names: list | None = None
     resnames: list | None = None
@@ -218,6 +223,10 @@ def gb_polymer(n_atoms: int, seed: int, temperature: float = 300.0) -> Molecular
     angles = np.stack([np.arange(n_atoms - 2), np.arange(1, n_atoms - 1),
                        np.arange(2, n_atoms)], 1).astype(np.int32)
     angle_params = np.tile([50.0, math.radians(109.5), 0.0, 0.0], (len(angles), 1))
+    # periodic dihedrals n = 3, k = 0.2 kcal/mol, phase 0 along the backbone
+    dih = np.stack([np.arange(n_atoms - 3), np.arange(1, n_atoms - 2),
+                    np.arange(2, n_atoms - 1), np.arange(3, n_atoms)], 1).astype(np.int32)
+    dih_params = np.tile([0.2, 3.0, 0.0], (len(dih), 1))
     # exclude scaled1-4: 1-2, 1-3 full; 1-4 modified
     ex = [(i, i + 1, 2) for i in range(n_atoms - 1)] + \
          [(i, i + 2, 2) for i in range(n_atoms - 2)] + \
@@ -229,6 +238,7 @@ def gb_polymer(n_atoms: int, seed: int, temperature: float = 300.0) -> Molecular
         lj=lj, exclusions=np.array(ex, np.int32).reshape(-1, 3), bonds=bonds,
         bond_params=bond_params, angles=angles, angle_params=angle_params, periodic=False,
         box=np.zeros(12), water=np.zeros(n_atoms, np.int32),
+        dihedrals=dih, dihedral_params=dih_params,
         gb_vdwr=rng.uniform(1.2, 1.9, n_atoms), gb_scale=gb_scale,
         gb_offset=np.full(n_atoms, 0.09), raw_charge=q, eps=eps, rmin2=rmin2,
         atom_names=[f"{e}{i % 100}" for i, e in enumerate(elem)], resnames=["POL"] * n_atoms)
@@ -257,8 +267,15 @@ def write_psf(sysm: MolecularSystem, path: str) -> None:
             f.write(f"{a + 1:8d}{b + 1:8d}{c + 1:8d}")
             if k % 3 == 2:
                 f.write("\n")
-        f.write("\n\n       0 !NPHI: dihedrals\n\n\n       0 !NIMPHI: impropers\n\n\n"
-                "       0 !NDON: donors\n\n\n       0 !NACC: acceptors\n\n\n"
+        for title, key in (("NPHI: dihedrals", "dihedrals"), ("NIMPHI: impropers", "impropers")):
+            quads = getattr(sysm, key)
+            quads = np.zeros((0, 4), np.int32) if quads is None else quads
+            f.write(f"\n\n{len(quads):8d} !{title}\n")
+            for k, q in enumerate(quads):
+                f.write("".join(f"{a + 1:8d}" for a in q))
+                if k % 2 == 1:
+                    f.write("\n")
+        f.write("\n\n       0 !NDON: donors\n\n\n       0 !NACC: acceptors\n\n\n"
                 "       0 !NNB\n\n\n       0       0 !NGRP\n\n")
 
 
@@ -283,7 +300,22 @@ def write_par(sysm: MolecularSystem, path: str) -> None:
             seen.add(key)
             f.write(f"{key[0]:<6s} {key[1]:<6s} {key[2]:<6s} {prm[0]:.17g} "
                     f"{math.degrees(prm[1]):.17g}\n")
-        f.write("\nDIHEDRALS\n\nIMPROPER\n\nNONBONDED nbxmod 5 atom cdiel shift vatom "
+        for title, key in (("DIHEDRALS", "dihedral"), ("IMPROPER", "improper")):
+            f.write(f"\n{title}\n")
+            quads, prms = getattr(sysm, key + "s"), getattr(sysm, key + "_params")
+            seen = set()
+            for q, prm in zip(quads if quads is not None else [], prms if prms is not None else []):
+                key4 = tuple(tn[sysm.type[a]] for a in q)
+                if key4 in seen:
+                    continue
+                seen.add(key4)
+                if title == "DIHEDRALS":
+                    f.write(" ".join(f"{t:<6s}" for t in key4) +
+                            f" {prm[0]:.17g} {int(prm[1])} {math.degrees(prm[2]):.17g}\n")
+                else:
+                    f.write(" ".join(f"{t:<6s}" for t in key4) +
+                            f" {prm[0]:.17g} 0 {math.degrees(prm[2]):.17g}\n")
+        f.write("\nNONBONDED nbxmod 5 atom cdiel shift vatom "
                 "vdistance vswitch -\ncutnb 14.0 ctofnb 12.0 ctonnb 10.0 eps 1.0 e14fac 1.0 "
                 "wmin 1.5\n\n")
         for t, name in enumerate(tn):

@@ -36,6 +36,10 @@ def topology(z: dict) -> SimpleNamespace:
         bond_params=z["bond_params"].reshape(-1, 2) if "bond_params" in z else np.zeros((0, 2)),
         angles=z["angles"].reshape(-1, 3).astype(np.int32) if "angles" in z else np.zeros((0, 3), np.int32),
         angle_params=z["angle_params"].reshape(-1, 4) if "angle_params" in z else np.zeros((0, 4)))
+    for kind in ("dihedral", "improper"):
+        if kind + "s" in z and len(z[kind + "s"]):
+            setattr(t, kind + "s", z[kind + "s"].reshape(-1, 4).astype(np.int32))
+            setattr(t, kind + "_params", z[kind + "_params"].reshape(-1, 3).copy())
     if "gb_vdwr" in z:
         t.gb_vdwr = z["gb_vdwr"].copy()
         t.gb_scale = z["gb_scale"].copy()

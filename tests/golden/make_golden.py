@@ -34,6 +34,7 @@ def save(name: str, d: dict, extra: dict | None = None) -> None:
     for k in ("natoms", "charge", "mass", "type", "molecule", "water", "lj", "ntypes",
               "exclusions", "exclusions_check", "coulomb_scaling", "periodic", "box",
               "positions", "velocities", "bonds", "bond_params", "angles", "angle_params",
+              "dihedrals", "dihedral_params", "impropers", "improper_params",
               "gb_vdwr", "gb_scale", "gb_offset", "gb_obc"):
         if k in d:
             out[k] = np.asarray(d[k])
@@ -77,7 +78,24 @@ def synthetic(sysm, stem: str, forces: list[str], cellsize: float, steps: int = 
         shutil.rmtree(tmp)
 
 
-def main() -> None:
+def torsions() -> None:
+    """The reference's GB test proteins through its Dihedral and Improper
+    forces (periodic cosine torsions and harmonic impropers)."""
+    for conf, name in (("www-fip35_FFAMBER_GB_LL.conf", "fip35_torsions"),
+                       ("alanylalanine_FFAMBER_GB_LL.conf", "alanylalanine_torsions")):
+        save(name, reference_conf(conf, ["Dihedral", "Improper"]))
+    # the synthetic heteropolymer (n = 3 backbone dihedrals) through the
+    # reference's PSF/PAR reader and its Dihedral/Bond/Angle forces
+    poly = systems.gb_polymer(200, seed=3)
+    save("polymer200_torsions", synthetic(poly, "poly", ["Dihedral", "Bond", "Angle"],
+                                          cellsize=5.0), {"seed": np.array(3)})
+
+
+def main(which: str = "all") -> None:
+    if which == "torsions":
+        torsions()
+        return
+    torsions()
     # 1. The reference's periodic water test (423 atoms, 28 A box).
     d = reference_conf("water_CHARMM_PERIODIC_L.conf", [
         "Coulomb -algorithm NonbondedCutoff -switchingFunction C1 -cutoff 6.5",
@@ -128,4 +146,4 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else "all")

@@ -226,3 +226,17 @@ def test_graph_replay_equals_eager(ctx):
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
     assert np.array_equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("name", ["fip35_torsions", "alanylalanine_torsions", "polymer200_torsions"])
+def test_torsions_vs_reference(ctx, name):
+    """Dihedral force (FP64 kernel) against the reference's own output."""
+    z = F.load(name)
+    topo = F.topology(z)
+    gs = GpuSystem(ctx, topo, "mixed")
+    f, e = _eval(ForceFactory(gs).make("Dihedral"), topo)
+    # FP64 arithmetic; the int64 fixed-point force sums resolve 2^-32
+    # kcal/mol/A, about 1e-9 of these small torsion forces
+    assert F.rms_rel(f, F.forces(z, 0)) <= 1e-8
+    assert _energy_ok(e[4], F.energies(z, 0)[4], rel=1e-10, floor=1e-8)
+    gs.close()

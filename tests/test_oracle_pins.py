@@ -123,3 +123,17 @@ def test_cell_assignment_formula():
     ref = np.floor((w + 14.0) / 7.0).astype(int)
     ok = np.all(cells == ref, axis=1)
     assert ok.mean() > 0.999
+
+
+@pytest.mark.parametrize("name", ["fip35_torsions", "alanylalanine_torsions", "polymer200_torsions"])
+def test_torsion_oracle_matches_reference(name):
+    """MTorsionSystemForce::calcTorsion (Dihedral force) restated in the
+    oracle against the reference's own forces and DIHEDRAL energy."""
+    z = F.load(name)
+    s = F.oracle_system(z)
+    atoms = z["dihedrals"].reshape(-1, 4)
+    prm = z["dihedral_params"].reshape(-1, 3)
+    f, e, _ = oracle.torsion_force(s, atoms, prm)
+    ref_f = F.forces(z, 0)
+    assert np.abs(f - ref_f).max() <= 1e-10 * max(1.0, np.abs(ref_f).max())
+    assert abs(e - F.energies(z, 0)[4]) <= 1e-10 * max(1.0, abs(e))
