@@ -36,6 +36,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# hardware work queues for the many per-system streams of the batched and
+# served forms (read when this process creates its CUDA context)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 N_WATERS, EDGE, JITTER, SEED = 7850, 62.0, 0.3, 2024
 DT_FS = 1.0
@@ -190,6 +193,44 @@ def algorithmic_bytes_per_step(n: int, grid: int) -> dict:
     return parts
 
 
+def ensemble_line(args, ctx, world: int, rank: int, dist=None) -> dict:
+    """The batched ensemble: --requests resident TIP3P boxes (100-1,000 waters
+    log-uniform, split over the ranks), each advanced in 50-step leapfrog
+    segments.  Set-up and the first segment (graph capture) are untimed;
+    then --steps segments are timed with all members in flight at once
+    (batched) and one member at a time (plain)."""
+    from protomol_b200 import replicas, serve
+    seg = 50
+    reqs = replicas.my_share(serve.ensemble(args.requests, 9, steps=seg), world, rank,
+                            cost=lambda r: float(r.n_atoms))
+    ens = serve.Ensemble(ctx, reqs)
+    for _ in range(max(1, args.warmup)):
+        ens.run(seg)
+    out = {}
+    for name, plain in (("plain", True), ("batched", False)):
+        if dist:
+            dist.barrier()
+        wall = sum(ens.run(seg, plain=plain) for _ in range(args.steps))
+        wall = replicas.max_over_ranks(wall, dist)
+        members = args.requests
+        md_ns = members * seg * args.steps * 1e-6  # 1 fs steps
+        atoms = sum(p for p in replicas.gather_summaries(ens.atoms, dist))
+        out[name] = {"wall_s": wall, "ns_per_day": md_ns * 86400.0 / wall,
+                     "atom_steps_per_s": atoms * seg * args.steps / wall,
+                     "segments_per_member": args.steps}
+    ens.close()
+    workload = (f"batched ensemble: {args.requests} resident TIP3P boxes of 100-1,000 waters "
+                f"(log-uniform), 0.0334 waters/A^3, {seg}-step leapfrog segments (inner steps "
+                f"as CUDA graphs), PME order 4 spacing <= 1 A, rc 9 A, LJ C2 8->9 A")
+    return {"metric": "ns/day (batched form)", "impl": "pmgpu", "mode": "batched",
+            "value": out["batched"]["ns_per_day"], "unit": "ns/day", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "strong", "data": "synthetic",
+            "config": {"workload": workload, "partition": f"boxes over {world} GPU(s)"},
+            "batched": out["batched"], "plain": out["plain"],
+            "batched_over_plain": out["batched"]["ns_per_day"] / out["plain"]["ns_per_day"]}
+
+
 def served_line(args, ctx, world: int, rank: int, dist=None) -> dict:
     """Aggregate ns/day of the served (or batched) form beside the plain
     form on the same requests: plain = one request at a time, served = up
@@ -207,11 +248,7 @@ def served_line(args, ctx, world: int, rank: int, dist=None) -> dict:
                     f"LangevinLeapfrog segments (1 fs, 5/ps, 300 K), PME order 4 spacing <= 1 A, "
                     f"rc 9 A")
     else:
-        steps = 50
-        mk = lambda: serve.ensemble(args.requests, 9, steps=steps)
-        workload = (f"batched ensemble: {args.requests} TIP3P boxes of 100-1,000 waters "
-                    f"(log-uniform), 0.0334 waters/A^3, one {steps}-step leapfrog segment each, "
-                    f"PME order 4 spacing <= 1 A, rc 9 A")
+        return ensemble_line(args, ctx, world, rank, dist)
     serve.execute(ctx, serve.Request(rid=-1, n_waters=300, seed=1, steps=20))  # warm-up
     out = {}
     for name, slots in (("plain", 1), ("served", args.slots)):
@@ -336,6 +373,44 @@ def gb_line(args, ctx, world: int, rank: int, dist=None) -> dict:
     return line
 
 
+def run_forms(args, ctx, world: int, rank: int, dist=None) -> dict:
+    """Short runs of the other forms for the summary in the main line: the
+    batched ensemble (256 boxes), the served stream (32 requests) and the
+    GB polymer; each reports its own ns/day and its ratio to the plain form.
+    Failures are reported in place, never fatal."""
+    import copy
+    legs = (("batched", dict(requests=256, steps=2, warmup=1)),
+            ("served", dict(requests=32, md_steps=1000, slots=32)),
+            ("gb", dict(steps=2, warmup=2, segment=GB_SEGMENT)))
+    out = {}
+    for mode, kw in legs:
+        a = copy.copy(args)
+        a.mode = mode
+        for k, v in kw.items():
+            setattr(a, k, v)
+        try:
+            r = gb_line(a, ctx, world, rank, dist) if mode == "gb" else \
+                served_line(a, ctx, world, rank, dist)
+        except Exception as ex:  # reported, never fatal
+            out[mode] = {"error": str(ex)[:200]}
+            continue
+        if mode == "batched":
+            out[mode] = {"value": r["value"], "unit": "ns/day", "workload": r["config"]["workload"],
+                         "plain_ns_per_day": r["plain"]["ns_per_day"],
+                         "batched_over_plain": r["batched_over_plain"]}
+        elif mode == "served":
+            sv = r["served"]
+            out[mode] = {"value": r["value"], "unit": "ns/day", "workload": r["config"]["workload"],
+                         "plain_ns_per_day": r["plain"]["ns_per_day"],
+                         "served_over_plain": r["served_over_plain"],
+                         "p50_latency_s": sv["p50_latency_s"], "p99_latency_s": sv["p99_latency_s"]}
+        else:
+            out[mode] = {"value": r["value"], "unit": "ns/day", "workload": r["config"]["workload"],
+                         "us_per_md_step": r["us_per_md_step"], "e2e": r["e2e"]["value"],
+                         "cpu_baseline": r.get("cpu_baseline")}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -353,6 +428,8 @@ def main():
                     help="served/batched: requests (boxes) in the stream")
     ap.add_argument("--slots", type=int, default=32,
                     help="served/batched: requests in flight at once")
+    ap.add_argument("--no-forms", dest="forms", action="store_false",
+                    help="bench: skip the short batched / served / GB summaries")
     ap.add_argument("--md-steps", type=int, default=1000,
                     help="served: MD steps per segment request (batched: 50)")
     args = ap.parse_args()
@@ -500,6 +577,7 @@ def main():
     pair_gbs = ab["pairs"] / pair_avg_s / 1e9
     step_s = t_ms / 1000.0 / md_steps / world
     traffic = load_traffic()
+    forms = run_forms(args, ctx, world, rank, dist) if args.forms else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": ns_day, "unit": "ns/day", "n_gpus": world,
@@ -531,6 +609,8 @@ def main():
         }
         if clk:
             line["clocks"] = clk
+        if forms:
+            line["forms"] = forms
         if world == 1 and os.path.exists(REF_BIN):
             try:
                 r = run_reference(2)

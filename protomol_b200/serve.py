@@ -212,6 +212,49 @@ class Server:
         return out
 
 
+class Ensemble:
+    """The batched form: many resident boxes advanced together.  Every
+    member keeps its state on the device between segments; a segment is
+    enqueued on every member's stream (inner steps replay each member's
+    captured CUDA graph) before any is waited for, so the members' kernels
+    overlap on the device.  `plain` advances the members one at a time."""
+
+    def __init__(self, ctx: Context, requests: list[Request]):
+        self.requests = requests
+        self.members = [build(ctx, r.prepare()) for r in requests]
+        self.integ = [LeapfrogIntegrator(r.timestep) if r.integrator == "leapfrog" else
+                      LangevinLeapfrogIntegrator(r.timestep, r.temperature, r.gamma, seed=r.seed)
+                      for r in requests]
+
+    def run(self, steps: int, plain: bool = False) -> float:
+        """One segment of `steps` MD steps for every member; wall seconds."""
+        t0 = time.perf_counter()
+        if plain:
+            for gs, it in zip(self.members, self.integ):
+                it.run(gs, steps)
+        else:
+            for gs, it in zip(self.members, self.integ):
+                it.run_async(gs, steps)
+            for gs, it in zip(self.members, self.integ):
+                it.wait(gs)
+        return time.perf_counter() - t0
+
+    def energies(self) -> list[np.ndarray]:
+        return [gs.energies()[0] for gs in self.members]
+
+    def positions(self) -> list[np.ndarray]:
+        return [gs.positions() for gs in self.members]
+
+    def close(self):
+        for gs in self.members:
+            gs.close()
+        self.members = []
+
+    @property
+    def atoms(self) -> int:
+        return sum(r.n_atoms for r in self.requests)
+
+
 def summarize(reqs: list[Request], wall: float, slots: int, peak: int) -> dict:
     ok = [r for r in reqs if r.error is None]
     lat = np.array([r.latency() for r in ok]) if ok else np.zeros(1)
