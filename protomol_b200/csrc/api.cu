@@ -197,6 +197,10 @@ static int system_free(System *s) {
   prof_collect(s);
   for (cudaEvent_t e : s->prof.pool) cudaEventDestroy(e);
   s->prof.pool.clear();
+  if (s->side) cudaStreamSynchronize(s->side);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->side) cudaStreamDestroy(s->side);
   if (s->stream) cudaStreamDestroy(s->stream);
   return PMGPU_OK;
 }
@@ -310,13 +314,30 @@ static int evaluate_forces(System *s, int only, int mode) {
       prepared[f.list_index] = 1;
     }
   }
-  for (auto &g : groups) {
-    prof_begin(s, PMGPU_PHASE_PAIRS);
-    int r = nb_pair_forces(s, &s->lists[g.list], g.terms, mode);
-    prof_end(s);
-    PM_CHECK(r);
-    s->kernels += 1;
+  // The other terms (PME, corrections, bonded, GB, all-pairs) only read the
+  // positions and add into the fixed-point forces and energies, so they run
+  // on the system's second stream beside the pair kernels and join before
+  // the evaluation ends (not while profiling, which times phases in order).
+  // That stream has the higher priority and is enqueued first, so its short
+  // dependent kernels are not queued behind the pair kernel's blocks.
+  const bool fork = s->side && !s->prof.enabled;
+  const cudaStream_t main_stream = s->stream;
+  if (fork) {
+    PM_CUDA(cudaEventRecord(s->ev_fork, main_stream));
+    PM_CUDA(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
+    s->stream = s->side;
   }
+  struct Join {  // back on the main stream, joined, on every exit path
+    System *s;
+    cudaStream_t main_stream;
+    bool on;
+    ~Join() {
+      s->stream = main_stream;
+      if (!on) return;
+      cudaEventRecord(s->ev_join, s->side);
+      cudaStreamWaitEvent(main_stream, s->ev_join, 0);
+    }
+  } join{s, main_stream, fork};
   for (auto &f : s->forces) {
     if (only >= 0 ? f.id != only : !f.enabled) continue;
     int r = PMGPU_OK;
@@ -367,6 +388,14 @@ static int evaluate_forces(System *s, int only, int mode) {
         break;
     }
     PM_CHECK(r);
+  }
+  s->stream = main_stream;
+  for (auto &g : groups) {
+    prof_begin(s, PMGPU_PHASE_PAIRS);
+    int r = nb_pair_forces(s, &s->lists[g.list], g.terms, mode);
+    prof_end(s);
+    PM_CHECK(r);
+    s->kernels += 1;
   }
   return PMGPU_OK;
 }
@@ -513,6 +542,11 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   s->ntypes = t->n_types;
   s->coulomb_scaling = t->coulomb_scaling;
   PM_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  int prio_low = 0, prio_high = 0;
+  PM_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+  PM_CUDA(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, prio_high));
+  PM_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+  PM_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
   size_t nn = std::max(1, n);
   PM_CHECK(upload(s.get(), &s->d_charge, t->charge, n));
   PM_CHECK(upload(s.get(), &s->d_mass, t->mass, n));

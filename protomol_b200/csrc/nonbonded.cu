@@ -634,22 +634,45 @@ static int spec_kind(const SwitchParams &sw) {
   return -2;
 }
 
+// Blocks of the pair kernel: one warp per atom, except the force-only FP32
+// kernel of the inner MD steps, whose grid is capped at three blocks per SM
+// (warps stride over the atoms) so that the PME / bonded chain on the
+// system's second stream always finds room beside it.
+static int pair_blocks(int n, bool persistent) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        sms <= 0)
+      sms = 148;
+  }
+  const int nb = (n + kPairWarps - 1) / kPairWarps;
+  return persistent ? std::max(1, std::min(nb, 3 * sms)) : nb;
+}
+
 template <typename Real, int TERMS, typename SPEC>
 static void launch_pairs_spec(PairArgs<Real> &a, cudaStream_t st, int mode) {
-  const int nb = (a.n + kPairWarps - 1) / kPairWarps;
   const int T = kPairWarps * 32;
   switch (mode) {
-    case PAIR_FORCE: k_pairs<Real, TERMS, PAIR_FORCE, SPEC><<<nb, T, 0, st>>>(a); break;
-    case PAIR_ENERGY: k_pairs<Real, TERMS, PAIR_ENERGY, SPEC><<<nb, T, 0, st>>>(a); break;
-    case PAIR_VIRIAL: k_pairs<Real, TERMS, PAIR_VIRIAL, SPEC><<<nb, T, 0, st>>>(a); break;
-    default: k_pairs<Real, TERMS, PAIR_RECORD, SPEC><<<nb, T, 0, st>>>(a); break;
+    case PAIR_FORCE:
+      k_pairs<Real, TERMS, PAIR_FORCE, SPEC><<<pair_blocks(a.n, sizeof(Real) == 4), T, 0, st>>>(a);
+      break;
+    case PAIR_ENERGY:
+      k_pairs<Real, TERMS, PAIR_ENERGY, SPEC><<<pair_blocks(a.n, false), T, 0, st>>>(a);
+      break;
+    case PAIR_VIRIAL:
+      k_pairs<Real, TERMS, PAIR_VIRIAL, SPEC><<<pair_blocks(a.n, false), T, 0, st>>>(a);
+      break;
+    default:
+      k_pairs<Real, TERMS, PAIR_RECORD, SPEC><<<pair_blocks(a.n, false), T, 0, st>>>(a);
+      break;
   }
 }
 
 template <typename Real, int TERMS, typename SPEC>
 static void launch_force_spec(PairArgs<Real> &a, cudaStream_t st) {
-  const int nb = (a.n + kPairWarps - 1) / kPairWarps;
-  k_pairs<Real, TERMS, PAIR_FORCE, SPEC><<<nb, kPairWarps * 32, 0, st>>>(a);
+  k_pairs<Real, TERMS, PAIR_FORCE, SPEC><<<pair_blocks(a.n, true), kPairWarps * 32, 0, st>>>(a);
 }
 
 template <typename Real, int TERMS>

@@ -309,183 +309,187 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE>::bl
   __shared__ PairQueue<Real> Q;
   const int w = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const int ii = blockIdx.x * kPairWarps + w;
-  if (ii >= a.n) return;  // whole warps exit; no block-wide barrier below
   const unsigned lt_mask = (1u << lane) - 1u;
-  const int cnt = a.nbr_count[ii];
-  const uint32_t *row = a.nbr + (size_t)ii * a.cap;
-  uint32_t e_next = lane < cnt ? __ldg(row + lane) : 0u;
-  const int oi = a.sorted[ii];
-  const double4 wi = a.xw[ii];
-  Real xi_h[3], xi_l[3], qi;
-  int ti;
-  if (MIXED) {
-    float4 h = a.xhi[ii], l = a.xlo[ii];
-    xi_h[0] = h.x; xi_h[1] = h.y; xi_h[2] = h.z; qi = h.w;
-    xi_l[0] = l.x; xi_l[1] = l.y; xi_l[2] = l.z; ti = __float_as_int(l.w);
-  } else {
-    xi_h[0] = wi.x; xi_h[1] = wi.y; xi_h[2] = wi.z; qi = wi.w;
-    xi_l[0] = xi_l[1] = xi_l[2] = Real(0);
-    ti = a.type[oi];
-  }
-  const Real *ljrow = MIXED ? reinterpret_cast<const Real *>(a.lj32 + ti * a.ntypes)
-                            : reinterpret_cast<const Real *>(a.lj64 + ti * a.ntypes);
-  // i as seen from the current entry's image of j (d = xj - (xi - s L))
-  int cur = kZeroShift;
-  Real xs_h[3] = {xi_h[0], xi_h[1], xi_h[2]};
-  Real xs_l[3] = {xi_l[0], xi_l[1], xi_l[2]};
-  Real fx = 0, fy = 0, fz = 0;
   Real vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
   double Elj = 0, Ec = 0;
   double V64[6] = {0, 0, 0, 0, 0, 0};
   int npairs = 0;
-  int head = 0, queued = 0;
-
-  auto process = [&](int p) {
-    const auto d = Q.d[w][p];
-    const int4 m = Q.m[w][p];
-    const int flags = m.w & 15;
-    Real en_lj = 0, en_c = 0;
-    const Real f = pair_force<Real, TERMS, SPEC>(a, ljrow, d.w, qi * Q.qj[w][p], m.y, flags,
-                                           en_lj, en_c);
-    fx -= d.x * f;
-    fy -= d.y * f;
-    fz -= d.z * f;
-    npairs++;
-    if (ENERGY) {
-      if (MIXED) {
-        pair_energy64<Real, TERMS, VIRIAL>(a, wi, a.xw[m.x], m.w >> 4, ti, m.y, flags, Elj,
-                                           Ec, V64);
-      } else {
-        Elj += (double)en_lj;
-        Ec += (double)en_c;
-      }
-    }
-    if (VIRIAL && !MIXED) {
-      // addVirial(fij, d) with fij = d * f, half per visit
-      Real hf = Real(0.5) * f;
-      vxx += d.x * d.x * hf; vxy += d.x * d.y * hf; vxz += d.x * d.z * hf;
-      vyy += d.y * d.y * hf; vyz += d.y * d.z * hf; vzz += d.z * d.z * hf;
-    }
-    if (RECORD) {
-      int oj = a.sorted[m.x];
-      if (oi < oj) {
-        long long slot = atomicAdd((unsigned long long *)a.paircount, 1ull);
-        if (slot < a.pairbuf_cap) a.pairbuf[slot] = ((long long)oi << 32) | (unsigned)oj;
-      }
-    }
-  };
-
-  for (int k0 = 0; k0 < cnt; k0 += 32) {
-    const int k = k0 + lane;
-    const bool have = k < cnt;
-    const uint32_t e = e_next;
-    // the next round's entry is fetched while this round computes
-    e_next = (k + 32 < cnt) ? __ldg(row + k + 32) : 0u;
-    const int j = (int)(e & kJMask);
-    const int sh = (int)((e >> kShiftBits) & kShiftMask);
-    // image changes are rare (atoms near a face of the box): a real branch
-    if (__any_sync(kAll, have && sh != cur)) {
-      if (have && sh != cur) {
-        const int sx = (sh & 3) - 1, sy = ((sh >> 2) & 3) - 1, sz = ((sh >> 4) & 3) - 1;
-        const double xs64[3] = {wi.x - sx * a.box.e[0], wi.y - sy * a.box.e[1],
-                                wi.z - sz * a.box.e[2]};
-        for (int c = 0; c < 3; c++) {
-          if (MIXED) {
-            float h = (float)xs64[c];
-            xs_h[c] = h;
-            xs_l[c] = (float)(xs64[c] - (double)h);
-          } else {
-            xs_h[c] = xs64[c];
-          }
-        }
-        cur = sh;
-      }
-    }
-    Real dx, dy, dz, qj;
-    int tj = 0;
+  // Warps stride over the sorted atoms (the grid may be smaller than one
+  // warp per atom, which leaves room on every SM for the work of the other
+  // stream); no block-wide barrier below.
+  for (int ii = blockIdx.x * kPairWarps + w; ii < a.n; ii += gridDim.x * kPairWarps) {
+    const int cnt = a.nbr_count[ii];
+    const uint32_t *row = a.nbr + (size_t)ii * a.cap;
+    uint32_t e_next = lane < cnt ? __ldg(row + lane) : 0u;
+    const int oi = a.sorted[ii];
+    const double4 wi = a.xw[ii];
+    Real xi_h[3], xi_l[3], qi;
+    int ti;
     if (MIXED) {
-      const float4 h = a.xhi[j], l = a.xlo[j];
-      dx = (h.x - xs_h[0]) + (l.x - xs_l[0]);
-      dy = (h.y - xs_h[1]) + (l.y - xs_l[1]);
-      dz = (h.z - xs_h[2]) + (l.z - xs_l[2]);
-      qj = h.w;
-      tj = __float_as_int(l.w);
+      float4 h = a.xhi[ii], l = a.xlo[ii];
+      xi_h[0] = h.x; xi_h[1] = h.y; xi_h[2] = h.z; qi = h.w;
+      xi_l[0] = l.x; xi_l[1] = l.y; xi_l[2] = l.z; ti = __float_as_int(l.w);
     } else {
-      const double4 wj = a.xw[j];
-      dx = wj.x - xs_h[0];
-      dy = wj.y - xs_h[1];
-      dz = wj.z - xs_h[2];
-      qj = wj.w;
+      xi_h[0] = wi.x; xi_h[1] = wi.y; xi_h[2] = wi.z; qi = wi.w;
+      xi_l[0] = xi_l[1] = xi_l[2] = Real(0);
+      ti = a.type[oi];
     }
-    const Real r2 = dx * dx + dy * dy + dz * dz;
-    constexpr int kAllTerms = ((TERMS & TERM_LJ) ? kQLJ : 0) | ((TERMS & TERM_COUL) ? kQCoul : 0) |
-                              ((TERMS & TERM_EWALD) ? kQEwald : 0);
-    int flags = 0;
-    bool band = false;
-    if (have && a.same_cut) {  // every term shares one cutoff
-      if (r2 <= a.max_lo) flags = kAllTerms;
-      else band = r2 <= a.max_hi;
-    } else if (have) {
-      if (TERMS & TERM_LJ) {
-        if (r2 <= a.lj_lo) flags |= kQLJ;
-        else band |= r2 <= a.lj_hi;
+    const Real *ljrow = MIXED ? reinterpret_cast<const Real *>(a.lj32 + ti * a.ntypes)
+                              : reinterpret_cast<const Real *>(a.lj64 + ti * a.ntypes);
+    // i as seen from the current entry's image of j (d = xj - (xi - s L))
+    int cur = kZeroShift;
+    Real xs_h[3] = {xi_h[0], xi_h[1], xi_h[2]};
+    Real xs_l[3] = {xi_l[0], xi_l[1], xi_l[2]};
+    Real fx = 0, fy = 0, fz = 0;
+    int head = 0, queued = 0;
+
+    auto process = [&](int p) {
+      const auto d = Q.d[w][p];
+      const int4 m = Q.m[w][p];
+      const int flags = m.w & 15;
+      Real en_lj = 0, en_c = 0;
+      const Real f = pair_force<Real, TERMS, SPEC>(a, ljrow, d.w, qi * Q.qj[w][p], m.y, flags,
+                                             en_lj, en_c);
+      fx -= d.x * f;
+      fy -= d.y * f;
+      fz -= d.z * f;
+      npairs++;
+      if (ENERGY) {
+        if (MIXED) {
+          pair_energy64<Real, TERMS, VIRIAL>(a, wi, a.xw[m.x], m.w >> 4, ti, m.y, flags, Elj,
+                                             Ec, V64);
+        } else {
+          Elj += (double)en_lj;
+          Ec += (double)en_c;
+        }
       }
-      if (TERMS & TERM_COUL) {
-        if (r2 <= a.coul_lo) flags |= kQCoul;
-        else band |= r2 <= a.coul_hi;
+      if (VIRIAL && !MIXED) {
+        // addVirial(fij, d) with fij = d * f, half per visit
+        Real hf = Real(0.5) * f;
+        vxx += d.x * d.x * hf; vxy += d.x * d.y * hf; vxz += d.x * d.z * hf;
+        vyy += d.y * d.y * hf; vyz += d.y * d.z * hf; vzz += d.z * d.z * hf;
       }
-      if (TERMS & TERM_EWALD) {
-        if (r2 <= a.ew_lo) flags |= kQEwald;
-        else band |= r2 <= a.ew_hi;
+      if (RECORD) {
+        int oj = a.sorted[m.x];
+        if (oi < oj) {
+          long long slot = atomicAdd((unsigned long long *)a.paircount, 1ull);
+          if (slot < a.pairbuf_cap) a.pairbuf[slot] = ((long long)oi << 32) | (unsigned)oj;
+        }
+      }
+    };
+
+    for (int k0 = 0; k0 < cnt; k0 += 32) {
+      const int k = k0 + lane;
+      const bool have = k < cnt;
+      const uint32_t e = e_next;
+      // the next round's entry is fetched while this round computes
+      e_next = (k + 32 < cnt) ? __ldg(row + k + 32) : 0u;
+      const int j = (int)(e & kJMask);
+      const int sh = (int)((e >> kShiftBits) & kShiftMask);
+      // image changes are rare (atoms near a face of the box): a real branch
+      if (__any_sync(kAll, have && sh != cur)) {
+        if (have && sh != cur) {
+          const int sx = (sh & 3) - 1, sy = ((sh >> 2) & 3) - 1, sz = ((sh >> 4) & 3) - 1;
+          const double xs64[3] = {wi.x - sx * a.box.e[0], wi.y - sy * a.box.e[1],
+                                  wi.z - sz * a.box.e[2]};
+          for (int c = 0; c < 3; c++) {
+            if (MIXED) {
+              float h = (float)xs64[c];
+              xs_h[c] = h;
+              xs_l[c] = (float)(xs64[c] - (double)h);
+            } else {
+              xs_h[c] = xs64[c];
+            }
+          }
+          cur = sh;
+        }
+      }
+      Real dx, dy, dz, qj;
+      int tj = 0;
+      if (MIXED) {
+        const float4 h = a.xhi[j], l = a.xlo[j];
+        dx = (h.x - xs_h[0]) + (l.x - xs_l[0]);
+        dy = (h.y - xs_h[1]) + (l.y - xs_l[1]);
+        dz = (h.z - xs_h[2]) + (l.z - xs_l[2]);
+        qj = h.w;
+        tj = __float_as_int(l.w);
+      } else {
+        const double4 wj = a.xw[j];
+        dx = wj.x - xs_h[0];
+        dy = wj.y - xs_h[1];
+        dz = wj.z - xs_h[2];
+        qj = wj.w;
+      }
+      const Real r2 = dx * dx + dy * dy + dz * dz;
+      constexpr int kAllTerms = ((TERMS & TERM_LJ) ? kQLJ : 0) | ((TERMS & TERM_COUL) ? kQCoul : 0) |
+                                ((TERMS & TERM_EWALD) ? kQEwald : 0);
+      int flags = 0;
+      bool band = false;
+      if (have && a.same_cut) {  // every term shares one cutoff
+        if (r2 <= a.max_lo) flags = kAllTerms;
+        else band = r2 <= a.max_hi;
+      } else if (have) {
+        if (TERMS & TERM_LJ) {
+          if (r2 <= a.lj_lo) flags |= kQLJ;
+          else band |= r2 <= a.lj_hi;
+        }
+        if (TERMS & TERM_COUL) {
+          if (r2 <= a.coul_lo) flags |= kQCoul;
+          else band |= r2 <= a.coul_hi;
+        }
+        if (TERMS & TERM_EWALD) {
+          if (r2 <= a.ew_lo) flags |= kQEwald;
+          else band |= r2 <= a.ew_hi;
+        }
+      }
+      // pairs within a rounding band of a cutoff take the reference's exact
+      // FP64 test (rare: a real branch)
+      if (__any_sync(kAll, band)) {
+        if (band) {
+          const double r2x = exact_r2(a, oi, a.sorted[j], (double)dx, (double)dy, (double)dz);
+          if ((TERMS & TERM_LJ) && r2 > a.lj_lo && r2x <= a.lj_cut2) flags |= kQLJ;
+          if ((TERMS & TERM_COUL) && r2 > a.coul_lo && r2x <= a.coul_cut2) flags |= kQCoul;
+          if ((TERMS & TERM_EWALD) && r2 > a.ew_lo && r2x <= a.ew_cut2) flags |= kQEwald;
+        }
+      }
+      // boxes below twice the cutoff: cutoff terms take the minimal image only
+      // (Ewald real space sums every image, NonbondedFullEwaldSystemForce.h:790)
+      if ((TERMS & (TERM_LJ | TERM_COUL)) && a.minimal_image && (flags & (kQLJ | kQCoul)) &&
+          !(fabs(dx) <= a.half_edge[0] && fabs(dy) <= a.half_edge[1] &&
+            fabs(dz) <= a.half_edge[2]))
+        flags &= ~(kQLJ | kQCoul);
+      const bool pass = flags != 0;
+      const unsigned mk = __ballot_sync(kAll, pass);
+      if (pass) {
+        if (!MIXED) tj = a.type[a.sorted[j]];
+        if (e & kModifiedBit) flags |= kQModified;
+        const int p = (head + queued + __popc(mk & lt_mask)) & (kQueue - 1);
+        typename QueueVec<Real>::T d;
+        d.x = dx; d.y = dy; d.z = dz; d.w = r2;
+        Q.d[w][p] = d;
+        Q.m[w][p] = make_int4(j, tj, 0, flags | (sh << 4));
+        Q.qj[w][p] = qj;
+      }
+      queued += __popc(mk);
+      if (queued >= 32) {
+        __syncwarp();
+        process((head + lane) & (kQueue - 1));
+        head += 32;
+        queued -= 32;
+        __syncwarp();
       }
     }
-    // pairs within a rounding band of a cutoff take the reference's exact
-    // FP64 test (rare: a real branch)
-    if (__any_sync(kAll, band)) {
-      if (band) {
-        const double r2x = exact_r2(a, oi, a.sorted[j], (double)dx, (double)dy, (double)dz);
-        if ((TERMS & TERM_LJ) && r2 > a.lj_lo && r2x <= a.lj_cut2) flags |= kQLJ;
-        if ((TERMS & TERM_COUL) && r2 > a.coul_lo && r2x <= a.coul_cut2) flags |= kQCoul;
-        if ((TERMS & TERM_EWALD) && r2 > a.ew_lo && r2x <= a.ew_cut2) flags |= kQEwald;
-      }
-    }
-    // boxes below twice the cutoff: cutoff terms take the minimal image only
-    // (Ewald real space sums every image, NonbondedFullEwaldSystemForce.h:790)
-    if ((TERMS & (TERM_LJ | TERM_COUL)) && a.minimal_image && (flags & (kQLJ | kQCoul)) &&
-        !(fabs(dx) <= a.half_edge[0] && fabs(dy) <= a.half_edge[1] &&
-          fabs(dz) <= a.half_edge[2]))
-      flags &= ~(kQLJ | kQCoul);
-    const bool pass = flags != 0;
-    const unsigned mk = __ballot_sync(kAll, pass);
-    if (pass) {
-      if (!MIXED) tj = a.type[a.sorted[j]];
-      if (e & kModifiedBit) flags |= kQModified;
-      const int p = (head + queued + __popc(mk & lt_mask)) & (kQueue - 1);
-      typename QueueVec<Real>::T d;
-      d.x = dx; d.y = dy; d.z = dz; d.w = r2;
-      Q.d[w][p] = d;
-      Q.m[w][p] = make_int4(j, tj, 0, flags | (sh << 4));
-      Q.qj[w][p] = qj;
-    }
-    queued += __popc(mk);
-    if (queued >= 32) {
+    if (queued > 0) {
       __syncwarp();
-      process((head + lane) & (kQueue - 1));
-      head += 32;
-      queued -= 32;
-      __syncwarp();
+      if (lane < queued) process((head + lane) & (kQueue - 1));
     }
-  }
-  if (queued > 0) {
-    __syncwarp();
-    if (lane < queued) process((head + lane) & (kQueue - 1));
-  }
-  double Fx = warp_sum((double)fx), Fy = warp_sum((double)fy), Fz = warp_sum((double)fz);
-  if (lane == 0) {
-    red_add(&a.force[oi], to_fixed(Fx, kForceScale));
-    red_add(&a.force[a.n + oi], to_fixed(Fy, kForceScale));
-    red_add(&a.force[2 * a.n + oi], to_fixed(Fz, kForceScale));
+    __syncwarp();  // the ring is refilled by the next atom
+    double Fx = warp_sum((double)fx), Fy = warp_sum((double)fy), Fz = warp_sum((double)fz);
+    if (lane == 0) {
+      red_add(&a.force[oi], to_fixed(Fx, kForceScale));
+      red_add(&a.force[a.n + oi], to_fixed(Fy, kForceScale));
+      red_add(&a.force[2 * a.n + oi], to_fixed(Fz, kForceScale));
+    }
   }
   if (ENERGY || a.count_pairs) {
     int np = warp_sum(npairs);

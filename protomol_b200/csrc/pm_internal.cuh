@@ -203,6 +203,8 @@ struct System {
   int precision = PMGPU_PREC_MIXED;
   Box box{};
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;     // second stream for the non-pair terms
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // host copies of static topology
   std::vector<double> h_charge, h_mass;
   std::vector<int> h_type, h_mol;

@@ -451,6 +451,10 @@ int pme_reciprocal(System *s, Force *f, int em) {
   if (f->list_index >= 0 && f->list_index < (int)s->lists.size() &&
       s->lists[f->list_index].built)
     order_map = s->lists[f->list_index].d_sorted;
+  // the plans run on whichever stream this evaluation uses
+  if (cufftSetStream(f->plan_r2c, s->stream) != CUFFT_SUCCESS ||
+      cufftSetStream(f->plan_c2r, s->stream) != CUFFT_SUCCESS)
+    return fail(PMGPU_ERR_CUDA, "cufftSetStream failed");
   PM_CUDA(cudaMemsetAsync(f->d_grid_fixed, 0, sizeof(long long) * nreal, s->stream));
   spread_gather(a, s, f, order_map, 0);
   k_pme_fixed_to_float<<<(int)((nreal + 255) / 256), 256, 0, s->stream>>>(
