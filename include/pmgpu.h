@@ -289,7 +289,8 @@ int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
 /* ---- diagnostics ---------------------------------------------------- */
 typedef struct {
   long long pairs_in_cutoff;   /* pairs that passed the cutoff test */
-  long long list_entries;      /* (i-cluster, j) entries in the pair list */
+  long long list_entries;      /* tiles in the pair list: (8-atom i cluster,
+                                  4-atom j cluster, image) entries */
   long long clusters;          /* 8-atom i-clusters */
   long long list_builds;       /* pair-list builds so far */
   int cells[3];                /* sort-grid dims of the cutoff path */

@@ -439,12 +439,14 @@ static int read_results(System *s, int only, double *energies, double *virial, i
       return fail(PMGPU_ERR_OVERFLOW, "neighbour list capacity exceeded; capacity doubled");
     }
     if (st & ST_NONFINITE) return fail(PMGPU_ERR_NAN, "non-finite position or force");
+    if (st & ST_CELL_OVERFLOW)
+      return fail(PMGPU_ERR_UNSUPPORTED, "more atoms in one pair-list column than the sort holds");
   }
   double e[PMGPU_E_COUNT], v[9];
   for (int k = 0; k < PMGPU_E_COUNT; k++) e[k] = (double)s->h_acc[k] / kEnergyScale;
   for (int k = 0; k < 9; k++) v[k] = (double)s->h_acc[ACC_VIRIAL + k] / kEnergyScale;
   constant_terms(s, only, e, v);
-  s->last_pairs = s->h_acc[ACC_PAIRS] / 2;
+  s->last_pairs = s->h_acc[ACC_PAIRS];
   for (int k = 0; k < PMGPU_E_COUNT; k++) s->last_energy[k] = e[k];
   for (int k = 0; k < 9; k++) s->last_virial[k] = v[k];
   if (energies)
@@ -1200,11 +1202,18 @@ int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
   const double n = std::max(1, n_atoms);
   const double V = box[0] * box[1] * box[2];
   double b = n * (24 * 3 + 24 + 24 + 8 + 8 + 8);        // pos, vel, snapshot, force, q, m, ids
-  b += n * (16 + 16 + 32 + 4 + 4 + 24 + 24 + 8);       // sorted coordinates, offsets, keys
   if (reach > 0) {
-    double dens = V > 0 ? std::max(n / V, 0.12) : 0.15;
-    double cap = std::min(4.18879 * reach * reach * reach * dens * 1.5 + 64, n);
-    b += n * 4 * (cap + 32) + 4.0 * 64 * std::max(1.0, V / (reach * reach * reach));
+    // cluster-pair list: padded slots, cluster boxes, sort keys, tile rows
+    // (the same sizing as the list set-up)
+    const double ncol = std::max(1.0, std::floor(box[0] / kColumnWidth)) *
+                        std::max(1.0, std::floor(box[1] / kColumnWidth));
+    const double nkeys = ncol * std::max(1.0, std::floor(box[2] / kZBin));
+    const double ns = n + 7 * ncol + 8, ncl = ns / 8;
+    const double dens = V > 0 ? std::max(n / V, 0.12) : 0.15;
+    const double r = reach + 5.0;
+    const double cap = 4.18879 * r * r * r * dens / 8.0 * 1.4 + 64;
+    b += ns * (16 + 16 + 32 + 4 + 4 + 8) + n * (4 + 4 + 4 + 24 + 24) + nkeys * 4 + ncol * 16 +
+         ncl * (16 * cap + 4);
   }
   if (grid) {
     double G = (double)grid[0] * grid[1] * grid[2];
@@ -1262,18 +1271,20 @@ int pmgpu_force_stats(pmgpu_system *h, int id, pmgpu_stats *out) {
     const NeighborList &nl = s->lists[f.list_index];
     out->cells[0] = nl.ncx;
     out->cells[1] = nl.ncy;
-    out->cells[2] = nl.ncz;
+    out->cells[2] = nl.nzb;
+    out->clusters = nl.nclusters;
     int rb[2] = {0, 0};
     PM_CUDA(cudaMemcpyAsync(rb, nl.d_rebuild, sizeof(rb), cudaMemcpyDeviceToHost, s->stream));
     PM_CUDA(cudaStreamSynchronize(s->stream));
     out->list_builds = rb[1];
-    std::vector<int> cnt(s->n);
-    if (s->n) {
-      PM_CUDA(cudaMemcpyAsync(cnt.data(), nl.d_nbr_count, sizeof(int) * s->n,
+    // list entries: tiles (8 x 4 atom pairs each) over all i clusters
+    std::vector<int> cnt(std::max(1, nl.nclusters));
+    if (nl.nclusters) {
+      PM_CUDA(cudaMemcpyAsync(cnt.data(), nl.d_tile_count, sizeof(int) * nl.nclusters,
                               cudaMemcpyDeviceToHost, s->stream));
       PM_CUDA(cudaStreamSynchronize(s->stream));
       long long tot = 0;
-      for (int c : cnt) tot += c;
+      for (int k = 0; k < nl.nclusters; k++) tot += cnt[k];
       out->list_entries = tot;
     }
   }

@@ -28,25 +28,6 @@ struct GridArgs {
   double vmin[3];    // vacuum: grid minimum (positions clamp into the grid)
 };
 
-// Sort key of an atom: coarse xy column, then the global fine z layer
-// (kFine layers per coarse cell), then a Morton-ordered kFine x kFine xy
-// sub-cell.  Every column is one contiguous z-sorted range, so the list
-// build reads the atoms of a neighbour column within the reach in z as one
-// slice.
-__device__ __forceinline__ int morton2(int x, int y) {
-  int m = 0;
-#pragma unroll
-  for (int b = 0; b < 2; b++) {
-    m |= ((x >> b) & 1) << (2 * b + 1);
-    m |= ((y >> b) & 1) << (2 * b);
-  }
-  return m;
-}
-__device__ __forceinline__ int sort_key(int cx, int cy, int layer, int fx, int fy, int ncy,
-                                        int nlayers) {
-  return ((cx * ncy + cy) * nlayers + layer) * (kFine * kFine) + morton2(fx, fy);
-}
-
 // Cell of one atom: floor((delta + minimalPosition(x)) * inv) per axis
 // (Topology.h:67-70, CubicCellManager.cpp:40-44); also returns the wrapped
 // position and the fractional position inside the cell.
@@ -66,29 +47,45 @@ __device__ __forceinline__ void cell_of(const GridArgs &g, double x, double y,
   }
 }
 
-__global__ void k_bin(GridArgs g, const double *__restrict__ pos,
+// ------------------------------------------------------ list sort grid
+// The cluster-pair list sorts atoms into ncx x ncy columns of the xy plane
+// and, within a column, by z (ties by atom index, so the order is
+// deterministic).  Eight consecutive atoms of a column then form a compact
+// cluster of about kColumnWidth on each side.
+struct ListGrid {
+  Box box;
+  int n, periodic;
+  int ncx, ncy, nzb;
+  double lo[3];    // grid corner in the wrapped frame
+  double inv[3];   // 1 / column width (x, y), 1 / z-bin height
+};
+
+__global__ void k_bin(ListGrid g, const double *__restrict__ pos,
                       const int *__restrict__ rebuild, int *__restrict__ key,
-                      int *__restrict__ key_count, double *__restrict__ offset,
-                      double *__restrict__ xbuild, int *__restrict__ status) {
+                      unsigned *__restrict__ zkey, int *__restrict__ col_count,
+                      double *__restrict__ offset, double *__restrict__ xbuild,
+                      int *__restrict__ status) {
   if (!*rebuild) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.n) return;
-  double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-  int c[3];
-  double w[3], fr[3];
-  cell_of(g, x, y, z, c, w, fr);
-  int dims[3] = {g.ncx, g.ncy, g.ncz};
-  int f[3];
-  for (int a = 0; a < 3; a++) {
-    if (c[a] < 0) { c[a] = 0; fr[a] = 0.0; }
-    if (c[a] >= dims[a]) { c[a] = dims[a] - 1; fr[a] = 0.999999; }
-    int k = (int)(fr[a] * kFine);
-    f[a] = k < 0 ? 0 : (k >= kFine ? kFine - 1 : k);
+  const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+  double w[3];
+  box_minpos(g.box, x, y, z, w[0], w[1], w[2]);
+  const int dims[2] = {g.ncx, g.ncy};
+  int c[2];
+  const bool finite = isfinite(x) && isfinite(y) && isfinite(z);
+  for (int a = 0; a < 2; a++) {
+    const double q = finite ? (w[a] - g.lo[a]) * g.inv[a] : 0.0;
+    int k = (int)floor(fmin(fmax(q, -1.0), (double)dims[a]));
+    c[a] = k < 0 ? 0 : (k >= dims[a] ? dims[a] - 1 : k);
   }
-  if (!isfinite(x) || !isfinite(y) || !isfinite(z)) atomicOr(status, ST_NONFINITE);
-  int k = sort_key(c[0], c[1], c[2] * kFine + f[2], f[0], f[1], g.ncy, g.ncz * kFine);
-  key[i] = k;
-  atomicAdd(&key_count[k], 1);
+  if (!finite) atomicOr(status, ST_NONFINITE);
+  const int col = c[0] * g.ncy + c[1];
+  key[i] = col;
+  // non-negative FP32 bits order like the values
+  const float zf = finite ? (float)fmin(fmax(w[2] - g.lo[2], 0.0), 1.0e30) : 0.f;
+  zkey[i] = __float_as_uint(zf);
+  atomicAdd(&col_count[col], 1);
   offset[3 * i] = x - w[0];
   offset[3 * i + 1] = y - w[1];
   offset[3 * i + 2] = z - w[2];
@@ -97,89 +94,152 @@ __global__ void k_bin(GridArgs g, const double *__restrict__ pos,
   xbuild[3 * i + 2] = z;
 }
 
-// Single-block exclusive scan of the key counts (nkeys is at most a few
-// hundred thousand); also zeroes the scatter cursors.
-__global__ void k_scan(const int *__restrict__ rebuild, const int *__restrict__ count,
-                       int *__restrict__ start, int *__restrict__ cursor, int nkeys) {
-  if (!*rebuild) return;
-  __shared__ int warp_tot[32];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
+// Exclusive scan of value(k), k < count, by one block; write(k, prefix)
+// receives each prefix and the return value is the total.
+template <typename V, typename W>
+__device__ int block_scan(int count, V value, W write, int *warp_tot, int *carry) {
+  if (threadIdx.x == 0) *carry = 0;
   __syncthreads();
-  for (int base = 0; base < nkeys; base += blockDim.x) {
-    int i = base + threadIdx.x;
-    int v = i < nkeys ? count[i] : 0;
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < count; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int v = i < count ? value(i) : 0;
     int incl = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(0xffffffffu, incl, o);
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += t;
     }
     if (lane == 31) warp_tot[wid] = incl;
     __syncthreads();
     if (wid == 0) {
-      int nw = blockDim.x >> 5;
-      int t = lane < nw ? warp_tot[lane] : 0;
+      const int t = lane < nw ? warp_tot[lane] : 0;
       int ti = t;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-        int u = __shfl_up_sync(0xffffffffu, ti, o);
+        const int u = __shfl_up_sync(0xffffffffu, ti, o);
         if (lane >= o) ti += u;
       }
-      if (lane < nw) warp_tot[lane] = ti - t;  // exclusive warp offsets
+      if (lane < nw) warp_tot[lane] = ti - t;
     }
     __syncthreads();
-    int excl = carry + warp_tot[wid] + incl - v;
-    if (i < nkeys) {
-      start[i] = excl;
-      cursor[i] = 0;
-    }
+    const int excl = *carry + warp_tot[wid] + incl - v;
+    if (i < count) write(i, excl);
     __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+    if (threadIdx.x == blockDim.x - 1) *carry = excl + v;
     __syncthreads();
   }
-  if (threadIdx.x == 0) start[nkeys] = carry;
+  return *carry;
+}
+
+// One block: column starts (unpadded, for the scatter) and padded column
+// bases (every column a whole number of 8-atom clusters); slots past the
+// padded total are marked empty.
+__global__ void __launch_bounds__(1024)
+k_scan_cols(const int *__restrict__ rebuild, const int *__restrict__ col_count, int ncol,
+            int *__restrict__ col_u, int *__restrict__ cursor, int *__restrict__ col_base,
+            int *__restrict__ key_start, int nkeys, int *__restrict__ sorted, int ns_max) {
+  if (!*rebuild) return;
+  __shared__ int warp_tot[32];
+  __shared__ int carry;
+  block_scan(
+      ncol, [&](int c) { return col_count[c]; },
+      [&](int c, int p) {
+        col_u[c] = p;
+        cursor[c] = 0;
+      },
+      warp_tot, &carry);
+  const int padded = block_scan(
+      ncol, [&](int c) { return (col_count[c] + 7) & ~7; },
+      [&](int c, int p) { col_base[c] = p; }, warp_tot, &carry);
+  if (threadIdx.x == 0) {
+    col_base[ncol] = padded;
+    key_start[nkeys] = padded;
+  }
+  for (int s = padded + threadIdx.x; s < ns_max; s += blockDim.x) sorted[s] = -1;
 }
 
 __global__ void k_scatter(const int *__restrict__ rebuild, int n,
-                          const int *__restrict__ key, const int *__restrict__ start,
-                          int *__restrict__ cursor, int *__restrict__ sorted) {
+                          const int *__restrict__ key, const int *__restrict__ col_u,
+                          int *__restrict__ cursor, int *__restrict__ unsorted) {
   if (!*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  int k = key[i];
-  int slot = start[k] + atomicAdd(&cursor[k], 1);
-  sorted[slot] = i;
+  const int c = key[i];
+  unsorted[col_u[c] + atomicAdd(&cursor[c], 1)] = i;
 }
 
-// Deterministic order inside each fine cell: ascending atom index (the
-// order ProtoMol's linked cell lists have, Topology.h:72-83).
-__global__ void k_sort_keys(const int *__restrict__ rebuild, int nkeys,
-                            const int *__restrict__ start, int *__restrict__ sorted,
-                            int *__restrict__ key_count) {
+// One block per column: bitonic sort of (z, atom) in shared memory, the
+// column's padded slots written in that order, and the column's z-bin
+// index (first slot of every bin).  A column above kColCap atoms flags
+// ST_CELL_OVERFLOW and is left empty.
+constexpr int kSortThreads = 256;
+__global__ void __launch_bounds__(kSortThreads)
+k_sort_cols(const int *__restrict__ rebuild, int nzb, float inv_z,
+            int *__restrict__ col_count, const int *__restrict__ col_u,
+            const int *__restrict__ col_base, const int *__restrict__ unsorted,
+            const unsigned *__restrict__ zkey, int *__restrict__ sorted,
+            int *__restrict__ key_start, int *__restrict__ status) {
   if (!*rebuild) return;
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nkeys) return;
-  int b = start[k], e = start[k + 1];
-  for (int i = b + 1; i < e; i++) {
-    int v = sorted[i];
-    int j = i - 1;
-    while (j >= b && sorted[j] > v) {
-      sorted[j + 1] = sorted[j];
-      j--;
-    }
-    sorted[j + 1] = v;
+  __shared__ unsigned long long keys[kColCap];
+  const int col = blockIdx.x;
+  int m = col_count[col];
+  const int base = col_base[col], pend = col_base[col + 1];
+  if (m > kColCap) {
+    if (threadIdx.x == 0) atomicOr(status, ST_CELL_OVERFLOW);
+    m = 0;
   }
-  key_count[k] = 0;  // ready for the next build
+  int P = 1;
+  while (P < m) P <<= 1;
+  const int u = col_u[col];
+  for (int k = threadIdx.x; k < P; k += kSortThreads) {
+    if (k < m) {
+      const int i = unsorted[u + k];
+      keys[k] = ((unsigned long long)zkey[i] << 32) | (unsigned)i;
+    } else {
+      keys[k] = ~0ull;
+    }
+  }
+  __syncthreads();
+  for (int size = 2; size <= P; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int k = threadIdx.x; k < P; k += kSortThreads) {
+        const int l = k ^ stride;
+        if (l > k) {
+          const unsigned long long x = keys[k], y = keys[l];
+          const bool up = (k & size) == 0;
+          if ((x > y) == up) {
+            keys[k] = y;
+            keys[l] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  auto bin_of = [&](int k) {
+    const float zf = __uint_as_float((unsigned)(keys[k] >> 32));
+    const int b = (int)(zf * inv_z);
+    return b < 0 ? 0 : (b >= nzb ? nzb - 1 : b);
+  };
+  int *ks = key_start + (size_t)col * nzb;
+  for (int k = threadIdx.x; k < pend - base; k += kSortThreads)
+    sorted[base + k] = k < m ? (int)(keys[k] & 0xffffffffu) : -1;
+  for (int k = threadIdx.x; k < m; k += kSortThreads) {
+    const int b = bin_of(k), prev = k ? bin_of(k - 1) : -1;
+    for (int q = prev + 1; q <= b; q++) ks[q] = base + k;
+  }
+  const int last = m ? bin_of(m - 1) : -1;
+  for (int q = last + 1 + threadIdx.x; q < nzb; q += kSortThreads) ks[q] = base + m;
+  __syncthreads();
+  if (threadIdx.x == 0) col_count[col] = 0;  // ready for the next build
 }
 
 // Per-step gather of the sorted coordinates: xw = x - offset keeps every
-// atom in the image it had at the last build, so list shifts stay valid.
-// xhi (FP32 position + charge) feeds the list build in both precisions;
-// xlo (the FP32 residue + type) only the mixed-precision pair kernel.
+// atom in the image it had at the last build, so tile images stay valid.
+// Padding slots get far-away positions and no charge; no tile pairs them.
 template <bool MIXED>
-__global__ void k_gather(int n, const double *__restrict__ pos,
+__global__ void k_gather(int ns, const double *__restrict__ pos,
                          const double *__restrict__ offset,
                          const double *__restrict__ xbuild,
                          const int *__restrict__ sorted,
@@ -190,21 +250,29 @@ __global__ void k_gather(int n, const double *__restrict__ pos,
                          unsigned int *__restrict__ maxdisp) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.f;
-  if (s < n) {
-    int i = sorted[s];
-    double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-    double wx = x - offset[3 * i], wy = y - offset[3 * i + 1], wz = z - offset[3 * i + 2];
-    double q = charge[i];
-    xw[s] = make_double4(wx, wy, wz, q);
-    float hx = (float)wx, hy = (float)wy, hz = (float)wz;
-    xhi[s] = make_float4(hx, hy, hz, (float)q);
-    if (MIXED)
-      xlo[s] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
-                           (float)(wz - (double)hz), __int_as_float(type[i]));
-    mol_s[s] = mol[i];
-    double dx = x - xbuild[3 * i], dy = y - xbuild[3 * i + 1], dz = z - xbuild[3 * i + 2];
-    d2 = (float)(dx * dx + dy * dy + dz * dz);
-    if (!(d2 == d2)) d2 = 3.0e38f;  // NaN forces a rebuild / status check
+  if (s < ns) {
+    const int i = sorted[s];
+    if (i < 0) {
+      const double far = 1.0e5 + 16.0 * s;
+      xw[s] = make_double4(far, 1.0e5, 1.0e5, 0.0);
+      xhi[s] = make_float4((float)far, 1.0e5f, 1.0e5f, 0.f);
+      if (MIXED) xlo[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+      mol_s[s] = -1;
+    } else {
+      double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+      double wx = x - offset[3 * i], wy = y - offset[3 * i + 1], wz = z - offset[3 * i + 2];
+      double q = charge[i];
+      xw[s] = make_double4(wx, wy, wz, q);
+      float hx = (float)wx, hy = (float)wy, hz = (float)wz;
+      xhi[s] = make_float4(hx, hy, hz, (float)q);
+      if (MIXED)
+        xlo[s] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
+                             (float)(wz - (double)hz), __int_as_float(type[i]));
+      mol_s[s] = mol[i];
+      double dx = x - xbuild[3 * i], dy = y - xbuild[3 * i + 1], dz = z - xbuild[3 * i + 2];
+      d2 = (float)(dx * dx + dy * dy + dz * dz);
+      if (!(d2 == d2)) d2 = 3.0e38f;  // NaN forces a rebuild / status check
+    }
   }
   float m = d2;
 #pragma unroll
@@ -226,21 +294,42 @@ __global__ void k_check_rebuild(unsigned int *maxdisp, int *rebuild, float half_
   }
 }
 
+// Bounding box of every 4-atom cluster at the build (lower corner with the
+// number of atoms in .w, upper corner).
+__global__ void k_bbox(const int *__restrict__ rebuild, int nhalf,
+                       const int *__restrict__ sorted, const float4 *__restrict__ xhi,
+                       float4 *__restrict__ bb) {
+  if (!*rebuild) return;
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= nhalf) return;
+  float lo[3] = {3.0e38f, 3.0e38f, 3.0e38f}, hi[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
+  int m = 0;
+  for (int k = 0; k < 4; k++) {
+    if (sorted[4 * h + k] < 0) continue;
+    const float4 p = xhi[4 * h + k];
+    const float c[3] = {p.x, p.y, p.z};
+    for (int a = 0; a < 3; a++) {
+      lo[a] = fminf(lo[a], c[a]);
+      hi[a] = fmaxf(hi[a], c[a]);
+    }
+    m++;
+  }
+  bb[2 * h] = make_float4(lo[0], lo[1], lo[2], (float)m);
+  bb[2 * h + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
+}
+
 // ---------------------------------------------------------- list build
-struct BuildArgs {
-  Box box;
-  int n;
-  int ncx, ncy, ncz;
-  float reach2;       // FP32 candidate radius^2 (reach plus a rounding margin)
-  float cull2;        // column culling radius^2 (wider margin)
-  float cell_lo[3];   // lower corner of cell 0 in the xw frame
-  float cs[3];        // coarse cell size
-  float inv_layer;    // 1 / fine z-layer thickness
-  int nlayers;        // fine z layers per column
-  float L[3];         // box edges
-  float H2[3];        // half box edges (minimal-image test)
-  int cap;
+struct TileBuildArgs {
+  int nclusters;
   int periodic;
+  int ncx, ncy, nzb;
+  float lo[3];       // grid corner in the wrapped frame
+  float cs[3];       // column widths (x, y), z-bin height
+  float L[3];        // box edges
+  float H2[3];       // half box edges (minimal-image test)
+  float reach2;      // FP32 pair test radius^2 (reach plus a rounding margin)
+  float cull;        // cluster / column culling radius (wider margin)
+  int cap;
   const int *excl_start, *excl_partner, *excl_class;
 };
 
@@ -252,120 +341,173 @@ __device__ __forceinline__ int excl_class_of(const int *start, const int *partne
   return PMGPU_EXCL_NONE;
 }
 
-// One warp per sorted atom: for each of the 9 neighbour columns (skipping
-// columns whose xy box lies beyond the reach) the warp reads the slice of
-// fine z layers within the reach (split where it wraps through the periodic
-// z face), tests 32 candidates at a time in FP32 against (reach + margin)^2
-// and compacts passing entries with a warp ballot, so every row is written
-// in a fixed (column, layer, index) order.  Exclusions are resolved here
-// (ExclusionTable::check, topology/ExclusionTable.h:116-130, consulted only
-// for same-molecule minimal-image pairs as in OneAtomPairTwo.h:47-53):
-// fully excluded pairs are dropped, modified pairs flagged.
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ int floor_div(int a, int b) {
+  return a >= 0 ? a / b : -((-a + b - 1) / b);
+}
+
+// One warp per 8-atom i cluster.  Candidate 4-atom j clusters come from the
+// columns (and periodic images) whose box lies within the reach of the i
+// cluster's box, taking the z slice within the reach; a candidate is kept
+// if its box (in that image) lies within the reach.  Each unordered pair
+// is listed once: j clusters of a later i cluster are taken in every
+// image, those of the same i cluster in the zero image (pairs with the i
+// atom before the j atom) and in one half of the other images.  The 32
+// lanes then test the tile's 8 x 4 atom pairs at once: pairs beyond the
+// reach or with padding are masked off, and ExclusionTable::check
+// (topology/ExclusionTable.h:116-130; consulted for same-molecule
+// minimal-image pairs as in OneAtomPairTwo.h:47-53) clears fully excluded
+// pairs and marks modified ones.  Tiles are appended in a fixed order
+// (column image, z slice, cluster index), so the list is deterministic.
 __global__ void __launch_bounds__(kBuildWarps * 32)
-k_build_list(BuildArgs a, const int *__restrict__ rebuild, const int *__restrict__ key,
-             const int *__restrict__ sorted, const int *__restrict__ start,
-             const float4 *__restrict__ xhi, const int *__restrict__ mol_s,
-             uint32_t *__restrict__ nbr, int *__restrict__ nbr_count,
-             int *__restrict__ status) {
+k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__restrict__ sorted,
+              const int *__restrict__ start, const float4 *__restrict__ xhi,
+              const int *__restrict__ mol_s, const float4 *__restrict__ bb,
+              uint4 *__restrict__ tiles, int *__restrict__ tile_count,
+              int *__restrict__ status) {
   if (!*rebuild) return;
   const int lane = threadIdx.x & 31;
-  const int i = blockIdx.x * kBuildWarps + (threadIdx.x >> 5);
-  if (i >= a.n) return;  // whole warps exit together
-  const unsigned lt_mask = (1u << lane) - 1u;
-  const int oi = sorted[i];
-  const float4 pi = xhi[i];
-  const int mi = mol_s[i];
-  const int col = key[oi] / (a.nlayers * kFine * kFine);
-  const int cy = col % a.ncy, cx = col / a.ncy;
-  const int nl = a.nlayers;
-  uint32_t *row = nbr + (size_t)i * a.cap;
+  const int ci = blockIdx.x * kBuildWarps + (threadIdx.x >> 5);
+  if (ci >= a.nclusters) return;  // whole warps exit together
+  const float4 l0 = bb[4 * ci], h0 = bb[4 * ci + 1], l1 = bb[4 * ci + 2], h1 = bb[4 * ci + 3];
+  if (l0.w + l1.w == 0.f) {
+    if (lane == 0) tile_count[ci] = 0;
+    return;
+  }
+  float ilo[3] = {fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z)};
+  float ihi[3] = {fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z)};
+  // non-finite coordinates (already flagged by the binning), or periodic
+  // coordinates outside the box: no tiles, no unbounded window
+  bool sane = true;
+  for (int c = 0; c < 3; c++) {
+    const float span = (c < 2 ? (c ? a.ncy : a.ncx) : a.nzb) * a.cs[c];
+    sane = sane && isfinite(ilo[c]) && isfinite(ihi[c]) &&
+           (!a.periodic || (fabsf(ilo[c] - a.lo[c]) < 2.f * span &&
+                            fabsf(ihi[c] - a.lo[c]) < 2.f * span));
+  }
+  if (!sane) {
+    if (lane == 0) {
+      tile_count[ci] = 0;
+      atomicOr(status, ST_NONFINITE);
+    }
+    return;
+  }
+  const int islot = 8 * ci + (lane & 7);
+  const int jl = lane >> 3;
+  const int oi = sorted[islot];
+  const float4 pi = xhi[islot];
+  const int mi = mol_s[islot];
+  const float R = a.cull, R2 = a.cull * a.cull;
+  uint4 *row = tiles + (size_t)ci * a.cap;
   int count = 0;
 
-  // candidates of one contiguous slice [jb, je) seen under image (sx, sy, sz)
-  auto scan = [&](int jb, int je, int sx, int sy, int sz) {
-    const uint32_t sbits = (uint32_t)shift_code(sx, sy, sz) << kShiftBits;
-    const bool zero = (sx | sy | sz) == 0;
-    const float ox = pi.x - sx * a.L[0];
-    const float oy = pi.y - sy * a.L[1];
-    const float oz = pi.z - sz * a.L[2];
-    for (int j0 = jb; j0 < je; j0 += 32) {
-      const int j = j0 + lane;
-      bool pass = false;
-      uint32_t flags = 0;
-      if (j < je && !(j == i && zero)) {
-        const float4 pj = xhi[j];
-        const float dx = pj.x - ox, dy = pj.y - oy, dz = pj.z - oz;
-        pass = dx * dx + dy * dy + dz * dz < a.reach2;
-        if (pass && mol_s[j] == mi) {
+  // the j clusters of slots [s0, s1) seen under image (sx, sy, sz)
+  auto scan = [&](int s0, int s1, int sx, int sy, int sz) {
+    if (s1 <= s0) return;
+    const int code = shift_code(sx, sy, sz);
+    const float S[3] = {sx * a.L[0], sy * a.L[1], sz * a.L[2]};
+    const int hb = s0 >> 2, he = (s1 - 1) >> 2;
+    for (int h0 = hb; h0 <= he; h0 += 32) {
+      const int h = h0 + lane;
+      bool cand = false;
+      if (h <= he) {
+        const int parent = h >> 1;
+        cand = parent > ci || (parent == ci && code >= kZeroShift);
+        if (cand) {
+          const float4 jl4 = bb[2 * h], jh4 = bb[2 * h + 1];
+          const float jlo[3] = {jl4.x + S[0], jl4.y + S[1], jl4.z + S[2]};
+          const float jhi[3] = {jh4.x + S[0], jh4.y + S[1], jh4.z + S[2]};
+          float g2 = 0.f;
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            const float g = fmaxf(fmaxf(jlo[c] - ihi[c], ilo[c] - jhi[c]), 0.f);
+            g2 += g * g;
+          }
+          cand = jl4.w > 0.f && g2 <= R2;
+        }
+      }
+      unsigned cm = __ballot_sync(0xffffffffu, cand);
+      // the 8 x 4 atom pairs of a candidate tile (ci, hj) in this image
+      auto test = [&](int hj, int jslot, int oj, float4 pj, int mj) {
+        const float dx = pj.x + S[0] - pi.x, dy = pj.y + S[1] - pi.y, dz = pj.z + S[2] - pi.z;
+        bool pass = oi >= 0 && oj >= 0 && dx * dx + dy * dy + dz * dz < a.reach2;
+        if ((hj >> 1) == ci && code == kZeroShift) pass = pass && islot < jslot;
+        bool mod = false;
+        if (pass && mj == mi) {
           const bool minimal = !a.periodic || (fabsf(dx) <= a.H2[0] &&
                                                fabsf(dy) <= a.H2[1] && fabsf(dz) <= a.H2[2]);
           if (minimal) {
-            const int cls = excl_class_of(a.excl_start, a.excl_partner, a.excl_class, oi,
-                                          sorted[j]);
+            const int cls = excl_class_of(a.excl_start, a.excl_partner, a.excl_class, oi, oj);
             if (cls == PMGPU_EXCL_FULL) pass = false;
-            else if (cls == PMGPU_EXCL_MODIFIED) flags = kModifiedBit;
+            else if (cls == PMGPU_EXCL_MODIFIED) mod = true;
           }
         }
+        const unsigned im = __ballot_sync(0xffffffffu, pass);
+        const unsigned mm = __ballot_sync(0xffffffffu, mod);
+        if (im) {
+          if (lane == 0 && count < a.cap)
+            row[count] = make_uint4((uint32_t)hj | ((uint32_t)code << kShiftBits), im, mm, 0u);
+          count++;
+        }
+      };
+      // two candidates per round: both tiles' loads are in flight together
+      while (cm) {
+        const int bA = __ffs(cm) - 1;
+        cm &= cm - 1;
+        const int bB = cm ? __ffs(cm) - 1 : bA;
+        const bool two = cm != 0;
+        if (two) cm &= cm - 1;
+        const int hA = h0 + bA, hB = h0 + bB;
+        const int jA = 4 * hA + jl, jB = 4 * hB + jl;
+        const int oA = sorted[jA], oB = sorted[jB];
+        const float4 pA = xhi[jA], pB = xhi[jB];
+        const int mA = mol_s[jA], mB = mol_s[jB];
+        test(hA, jA, oA, pA, mA);
+        if (two) test(hB, jB, oB, pB, mB);
       }
-      const unsigned m = __ballot_sync(0xffffffffu, pass);
-      if (pass) {
-        const int slot = count + __popc(m & lt_mask);
-        if (slot < a.cap) row[slot] = (uint32_t)j | sbits | flags;
-      }
-      count += __popc(m);
     }
   };
-  auto slice = [&](int c2, int l0, int l1) {  // layers l0..l1 of column c2
-    const int base = c2 * nl * (kFine * kFine);
-    return make_int2(start[base + l0 * (kFine * kFine)],
-                     start[base + (l1 + 1) * (kFine * kFine)]);
+  auto slots = [&](int col, int b0, int b1) {  // z bins b0..b1 of a column
+    return make_int2(start[col * a.nzb + b0], start[col * a.nzb + b1 + 1]);
   };
 
-  // With one or two columns on an axis the -1/0/+1 neighbours name the same
-  // columns under different images; every (column, image) pair is distinct
-  // and the box edge exceeds the reach, so no pair appears twice under one
-  // image.
-  for (int ddx = -1; ddx <= 1; ddx++) {
-    int nx = cx + ddx, sx = 0;
-    if (a.periodic) {
-      if (nx < 0) { nx += a.ncx; sx = -1; }
-      else if (nx >= a.ncx) { nx -= a.ncx; sx = 1; }
-    } else if (nx < 0 || nx >= a.ncx) continue;
-    for (int ddy = -1; ddy <= 1; ddy++) {
-      int ny = cy + ddy, sy = 0;
-      if (a.periodic) {
-        if (ny < 0) { ny += a.ncy; sy = -1; }
-        else if (ny >= a.ncy) { ny -= a.ncy; sy = 1; }
-      } else if (ny < 0 || ny >= a.ncy) continue;
-      const int c2 = nx * a.ncy + ny;
-      if (!a.periodic) {  // vacuum: atoms may be clamped into edge cells
-        int2 r = slice(c2, 0, nl - 1);
+  const int ux0 = (int)floorf((ilo[0] - R - a.lo[0]) / a.cs[0]);
+  const int ux1 = (int)floorf((ihi[0] + R - a.lo[0]) / a.cs[0]);
+  const int uy0 = (int)floorf((ilo[1] - R - a.lo[1]) / a.cs[1]);
+  const int uy1 = (int)floorf((ihi[1] + R - a.lo[1]) / a.cs[1]);
+  const int b0 = (int)floorf((ilo[2] - R - a.lo[2]) / a.cs[2]);
+  const int b1 = (int)floorf((ihi[2] + R - a.lo[2]) / a.cs[2]);
+  if (!a.periodic) {
+    // vacuum: atoms outside the grid sit in its edge columns and bins;
+    // clamping the window the same way keeps every atom within the reach
+    for (int cx = clampi(ux0, 0, a.ncx - 1); cx <= clampi(ux1, 0, a.ncx - 1); cx++)
+      for (int cy = clampi(uy0, 0, a.ncy - 1); cy <= clampi(uy1, 0, a.ncy - 1); cy++) {
+        const int2 r = slots(cx * a.ncy + cy, clampi(b0, 0, a.nzb - 1),
+                             clampi(b1, 0, a.nzb - 1));
         scan(r.x, r.y, 0, 0, 0);
-        continue;
       }
-      // xy distance from the atom to this column's box (in this image)
-      const float lox = a.cell_lo[0] + (cx + ddx) * a.cs[0];
-      const float loy = a.cell_lo[1] + (cy + ddy) * a.cs[1];
-      const float gx = fmaxf(fmaxf(lox - pi.x, pi.x - (lox + a.cs[0])), 0.f);
-      const float gy = fmaxf(fmaxf(loy - pi.y, pi.y - (loy + a.cs[1])), 0.f);
-      const float g2 = gx * gx + gy * gy;
-      if (g2 > a.cull2) continue;
-      const float hz = sqrtf(a.cull2 - g2);  // z half-range of the reach sphere
-      const int l0 = (int)floorf((pi.z - hz - a.cell_lo[2]) * a.inv_layer);
-      const int l1 = (int)floorf((pi.z + hz - a.cell_lo[2]) * a.inv_layer);
-      // layers below 0 are the top of the box seen one box length down
-      // (j image sz = -1); layers past the top the bottom one length up
-      if (l0 < 0) {
-        int2 r = slice(c2, max(nl + l0, 0), nl - 1);
-        scan(r.x, r.y, sx, sy, -1);
-      }
-      {
-        int2 r = slice(c2, max(l0, 0), min(l1, nl - 1));
-        scan(r.x, r.y, sx, sy, 0);
-      }
-      if (l1 >= nl) {
-        int2 r = slice(c2, 0, min(l1 - nl, nl - 1));
-        scan(r.x, r.y, sx, sy, 1);
+  } else {
+    // the box edge exceeds the culling radius, so the window spans images
+    // -1, 0, 1 only
+    for (int ux = ux0; ux <= ux1; ux++) {
+      const int sx = floor_div(ux, a.ncx), cx = ux - sx * a.ncx;
+      const float clx = a.lo[0] + ux * a.cs[0];
+      const float gx = fmaxf(fmaxf(clx - ihi[0], ilo[0] - (clx + a.cs[0])), 0.f);
+      for (int uy = uy0; uy <= uy1; uy++) {
+        const int sy = floor_div(uy, a.ncy), cy = uy - sy * a.ncy;
+        const float cly = a.lo[1] + uy * a.cs[1];
+        const float gy = fmaxf(fmaxf(cly - ihi[1], ilo[1] - (cly + a.cs[1])), 0.f);
+        if (gx * gx + gy * gy > R2) continue;
+        const int col = cx * a.ncy + cy;
+        // z bins of the window in images sz = -1, 0, 1 (bin b of image sz
+        // lies at unwrapped bin b + sz * nzb)
+        for (int sz = -1; sz <= 1; sz++) {
+          const int lo = max(b0 - sz * a.nzb, 0), hi = min(b1 - sz * a.nzb, a.nzb - 1);
+          if (lo > hi) continue;
+          const int2 r = slots(col, lo, hi);
+          scan(r.x, r.y, sx, sy, sz);
+        }
       }
     }
   }
@@ -374,7 +516,7 @@ k_build_list(BuildArgs a, const int *__restrict__ rebuild, const int *__restrict
       atomicOr(status, ST_LIST_OVERFLOW);
       count = a.cap;
     }
-    nbr_count[i] = count;
+    tile_count[ci] = count;
   }
 }
 
@@ -390,78 +532,86 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   nl->cutoff = cutoff;
   nl->skin = skin;
   nl->reach = cutoff + skin;
-  int n = s->n;
+  const int n = s->n;
   const Box &b = s->box;
+  double lo[3], span[3];
   if (b.periodic) {
     for (int a = 0; a < 3; a++)
-      if (b.e[a] <= nl->reach)
+      if (b.e[a] <= nl->reach + 0.1)
         return fail(PMGPU_ERR_UNSUPPORTED,
-                    "box edge must exceed cutoff + list skin on the cell-list path");
-    // CubicCellManager::initialize (CubicCellManager.cpp:46-65) and
-    // ArrayCellListStructure::initialize (ArrayCellListStructure.cpp:40-42)
-    int dims[3];
+                    "box edge must exceed cutoff + list skin on the pair-list path");
     for (int a = 0; a < 3; a++) {
-      double vd = b.max[a] - b.min[a];
-      double f = std::floor(vd / nl->reach);
-      nl->cs[a] = vd / std::max(1.0, f);
-      dims[a] = std::max(1, (int)std::floor(vd / nl->cs[a] + kEpsilon));
+      lo[a] = b.min[a] - b.origin[a];
+      span[a] = b.max[a] - b.min[a];
     }
-    nl->ncx = dims[0]; nl->ncy = dims[1]; nl->ncz = dims[2];
   } else {
     // Vacuum: a fixed grid over the current bounding box plus a margin of
-    // one reach; atoms that later leave it clamp into the edge cells
-    // (cells only accelerate the search, they never drop a pair).
+    // one reach; atoms that later leave it clamp into the edge columns
+    // (the grid only orders atoms; cluster boxes decide the pairs).
     std::vector<double> h(3 * (size_t)std::max(n, 1), 0.0);
     if (n) {
       PM_CUDA(cudaMemcpyAsync(h.data(), s->d_pos, sizeof(double) * 3 * n,
                               cudaMemcpyDeviceToHost, s->stream));
       PM_CUDA(cudaStreamSynchronize(s->stream));
     }
-    double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
-    for (int a = 0; a < 3; a++) { mn[a] = h[a]; mx[a] = h[a]; }
+    double mn[3] = {h[0], h[1], h[2]}, mx[3] = {h[0], h[1], h[2]};
     for (int i = 1; i < n; i++)
       for (int a = 0; a < 3; a++) {
         mn[a] = std::min(mn[a], h[3 * i + a]);
         mx[a] = std::max(mx[a], h[3 * i + a]);
       }
-    int dims[3];
     for (int a = 0; a < 3; a++) {
-      double span = (mx[a] - mn[a]) + 2 * nl->reach;
-      dims[a] = std::max(1, std::min(128, (int)std::floor(span / nl->reach)));
-      nl->cs[a] = span / dims[a];
-      nl->vac_origin[a] = mn[a] - nl->reach;
+      lo[a] = mn[a] - nl->reach;
+      span[a] = (mx[a] - mn[a]) + 2 * nl->reach;
     }
-    nl->ncx = dims[0]; nl->ncy = dims[1]; nl->ncz = dims[2];
   }
-  nl->nkeys = nl->ncx * nl->ncy * nl->ncz * kFine3;
-  // capacity: expected neighbours in the reach sphere at the mean density,
-  // with headroom for local fluctuations (overflow is detected and
-  // reported, and the next call doubles the capacity).
-  // Condensed matter (liquid water ~0.1 atoms/A^3) bounds the local
-  // density even in sparse boxes, where atoms still cluster.
-  double dens = b.periodic ? std::max(n / b.V, 0.12) : 0.15;
-  double expect = 4.18879 * nl->reach * nl->reach * nl->reach * dens;
-  int cap = (int)(expect * 1.5 + 64);
-  cap = std::min(cap, std::max(32, n));
+  nl->ncx = std::max(1, std::min(256, (int)std::floor(span[0] / kColumnWidth)));
+  nl->ncy = std::max(1, std::min(256, (int)std::floor(span[1] / kColumnWidth)));
+  nl->nzb = std::max(1, std::min(1024, (int)std::floor(span[2] / kZBin)));
+  nl->cs[0] = span[0] / nl->ncx;
+  nl->cs[1] = span[1] / nl->ncy;
+  nl->cs[2] = span[2] / nl->nzb;
+  for (int a = 0; a < 3; a++) nl->lo[a] = lo[a];
+  nl->ncol = nl->ncx * nl->ncy;
+  nl->nkeys = nl->ncol * nl->nzb;
+  // slots: every column padded to whole 8-atom clusters
+  nl->ns_max = ((n + 7 * nl->ncol) + 7) & ~7;
+  nl->nclusters = nl->ns_max / 8;
+  // capacity: j clusters within (reach + cluster extent) of an i cluster at
+  // the mean density (condensed matter bounds the local density even in
+  // sparse boxes), half of them by the one-tile-per-pair rule, with
+  // headroom; an overflow is detected and the capacity doubled
+  const double dens = b.periodic ? std::max(n / b.V, 0.12) : 0.15;
+  const double r = nl->reach + 5.0;
+  const double expect = 4.18879 * r * r * r * dens / 4.0 / 2.0;
+  int cap = (int)(expect * 1.4 + 32);
+  cap = std::min(cap, std::max(32, nl->ns_max / 4 * 27));
   cap = (cap + 31) & ~31;
   if (nl->cap > cap) cap = nl->cap;
   nl->cap = cap;
-  size_t nn = std::max(1, n);
+  const size_t nn = std::max(1, n), ns = std::max(8, nl->ns_max);
   PM_CHECK(dev_alloc(s, &nl->d_key, sizeof(int) * nn));
-  PM_CHECK(dev_alloc(s, &nl->d_key_count, sizeof(int) * nl->nkeys));
-  PM_CUDA(cudaMemsetAsync(nl->d_key_count, 0, sizeof(int) * nl->nkeys, s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_zkey, sizeof(unsigned) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_unsorted, sizeof(int) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_col_count, sizeof(int) * nl->ncol));
+  PM_CUDA(cudaMemsetAsync(nl->d_col_count, 0, sizeof(int) * nl->ncol, s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_col_u, sizeof(int) * nl->ncol));
+  PM_CHECK(dev_alloc(s, &nl->d_col_cursor, sizeof(int) * nl->ncol));
+  PM_CHECK(dev_alloc(s, &nl->d_col_base, sizeof(int) * (nl->ncol + 1)));
   PM_CHECK(dev_alloc(s, &nl->d_key_start, sizeof(int) * (nl->nkeys + 1)));
-  PM_CHECK(dev_alloc(s, &nl->d_key_cursor, sizeof(int) * nl->nkeys));
-  PM_CHECK(dev_alloc(s, &nl->d_sorted, sizeof(int) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_sorted, sizeof(int) * ns));
+  PM_CUDA(cudaMemsetAsync(nl->d_sorted, 0xff, sizeof(int) * ns, s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_offset, sizeof(double) * 3 * nn));
   PM_CHECK(dev_alloc(s, &nl->d_xbuild, sizeof(double) * 3 * nn));
-  PM_CHECK(dev_alloc(s, &nl->d_xhi, sizeof(float4) * nn));
-  PM_CHECK(dev_alloc(s, &nl->d_xlo, sizeof(float4) * nn));
-  PM_CHECK(dev_alloc(s, &nl->d_xw, sizeof(double4) * nn));
-  PM_CHECK(dev_alloc(s, &nl->d_mol_s, sizeof(int) * nn));
-  PM_CHECK(dev_alloc(s, &nl->d_nbr, sizeof(uint32_t) * (size_t)cap * nn));
-  PM_CHECK(dev_alloc(s, &nl->d_nbr_count, sizeof(int) * nn));
-  PM_CUDA(cudaMemsetAsync(nl->d_nbr_count, 0, sizeof(int) * nn, s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_xhi, sizeof(float4) * ns));
+  PM_CHECK(dev_alloc(s, &nl->d_xlo, sizeof(float4) * ns));
+  PM_CHECK(dev_alloc(s, &nl->d_xw, sizeof(double4) * ns));
+  PM_CHECK(dev_alloc(s, &nl->d_mol_s, sizeof(int) * ns));
+  PM_CHECK(dev_alloc(s, &nl->d_bb, sizeof(float4) * 2 * (ns / 4)));
+  PM_CHECK(dev_alloc(s, &nl->d_tiles, sizeof(uint4) * (size_t)cap * nl->nclusters));
+  PM_CHECK(dev_alloc(s, &nl->d_tile_count, sizeof(int) * std::max(1, nl->nclusters)));
+  PM_CUDA(cudaMemsetAsync(nl->d_tile_count, 0, sizeof(int) * std::max(1, nl->nclusters),
+                          s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_maxdisp, sizeof(unsigned int)));
   PM_CUDA(cudaMemsetAsync(nl->d_maxdisp, 0, sizeof(unsigned int), s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_rebuild, 2 * sizeof(int)));
@@ -471,94 +621,95 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
 }
 
 int nb_list_free(System *s, NeighborList *nl) {
-  void *ptrs[] = {nl->d_key, nl->d_key_count, nl->d_key_start, nl->d_key_cursor,
-                  nl->d_sorted, nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo,
-                  nl->d_xw, nl->d_nbr, nl->d_nbr_count, nl->d_maxdisp, nl->d_rebuild,
-                  nl->d_mol_s};
+  void *ptrs[] = {nl->d_key, nl->d_zkey, nl->d_unsorted, nl->d_col_count, nl->d_col_u,
+                  nl->d_col_cursor, nl->d_col_base, nl->d_key_start, nl->d_sorted,
+                  nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
+                  nl->d_bb, nl->d_tiles, nl->d_tile_count, nl->d_maxdisp, nl->d_rebuild};
   for (void *p : ptrs) dev_free(s, p);
-  nl->d_key = nullptr; nl->d_key_count = nullptr; nl->d_key_start = nullptr;
-  nl->d_key_cursor = nullptr; nl->d_sorted = nullptr; nl->d_offset = nullptr;
-  nl->d_xbuild = nullptr; nl->d_xhi = nullptr; nl->d_xlo = nullptr;
-  nl->d_xw = nullptr; nl->d_nbr = nullptr; nl->d_nbr_count = nullptr;
-  nl->d_maxdisp = nullptr; nl->d_rebuild = nullptr; nl->d_mol_s = nullptr;
+  nl->d_key = nl->d_unsorted = nl->d_col_count = nl->d_col_u = nl->d_col_cursor = nullptr;
+  nl->d_col_base = nl->d_key_start = nl->d_sorted = nl->d_mol_s = nl->d_tile_count = nullptr;
+  nl->d_zkey = nullptr;
+  nl->d_rebuild = nullptr;
+  nl->d_offset = nl->d_xbuild = nullptr;
+  nl->d_xhi = nl->d_xlo = nl->d_bb = nullptr;
+  nl->d_xw = nullptr;
+  nl->d_tiles = nullptr;
+  nl->d_maxdisp = nullptr;
   return PMGPU_OK;
-}
-
-static GridArgs make_grid(const System *s, const NeighborList *nl) {
-  GridArgs g;
-  g.box = s->box;
-  g.n = s->n;
-  g.ncx = nl->ncx; g.ncy = nl->ncy; g.ncz = nl->ncz;
-  for (int a = 0; a < 3; a++) {
-    g.cs[a] = nl->cs[a];
-    g.inv[a] = 1.0 / nl->cs[a];
-    g.delta[a] = s->box.periodic ? s->box.origin[a] - s->box.min[a] : 0.0;
-    g.vmin[a] = s->box.periodic ? 0.0 : nl->vac_origin[a];
-  }
-  return g;
 }
 
 // Sort + (conditional) list build + per-step gather.  Never synchronises
 // with the host: the rebuild decision lives in device memory.
 int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
-  int n = s->n;
+  const int n = s->n;
   if (n == 0) return PMGPU_OK;
   cudaStream_t st = s->stream;
   const int T = 256;
-  int nb = (n + T - 1) / T;
-  int first = !nl->built;
-  float hs = (float)(0.5 * nl->skin);
+  const int nb = (n + T - 1) / T, nbs = (nl->ns_max + T - 1) / T;
+  const int first = !nl->built;
+  const float hs = (float)(0.5 * nl->skin);
   k_check_rebuild<<<1, 1, 0, st>>>(nl->d_maxdisp, nl->d_rebuild, hs * hs,
                                    (force_rebuild || first) ? 1 : 0);
-  GridArgs g = make_grid(s, nl);
-  k_bin<<<nb, T, 0, st>>>(g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_key_count,
+  ListGrid g;
+  g.box = s->box;
+  g.n = n;
+  g.periodic = s->box.periodic;
+  g.ncx = nl->ncx; g.ncy = nl->ncy; g.nzb = nl->nzb;
+  for (int a = 0; a < 3; a++) {
+    g.lo[a] = nl->lo[a];
+    g.inv[a] = 1.0 / nl->cs[a];
+  }
+  k_bin<<<nb, T, 0, st>>>(g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_zkey, nl->d_col_count,
                           nl->d_offset, nl->d_xbuild, s->d_status);
-  k_scan<<<1, 1024, 0, st>>>(nl->d_rebuild, nl->d_key_count, nl->d_key_start,
-                             nl->d_key_cursor, nl->nkeys);
-  k_scatter<<<nb, T, 0, st>>>(nl->d_rebuild, n, nl->d_key, nl->d_key_start,
-                              nl->d_key_cursor, nl->d_sorted);
-  k_sort_keys<<<(nl->nkeys + T - 1) / T, T, 0, st>>>(nl->d_rebuild, nl->nkeys,
-                                                    nl->d_key_start, nl->d_sorted,
-                                                    nl->d_key_count);
+  k_scan_cols<<<1, 1024, 0, st>>>(nl->d_rebuild, nl->d_col_count, nl->ncol, nl->d_col_u,
+                                  nl->d_col_cursor, nl->d_col_base, nl->d_key_start,
+                                  nl->nkeys, nl->d_sorted, nl->ns_max);
+  k_scatter<<<nb, T, 0, st>>>(nl->d_rebuild, n, nl->d_key, nl->d_col_u, nl->d_col_cursor,
+                              nl->d_unsorted);
+  k_sort_cols<<<nl->ncol, kSortThreads, 0, st>>>(
+      nl->d_rebuild, nl->nzb, (float)(1.0 / nl->cs[2]), nl->d_col_count, nl->d_col_u,
+      nl->d_col_base, nl->d_unsorted, nl->d_zkey, nl->d_sorted, nl->d_key_start, s->d_status);
   if (s->precision == PMGPU_PREC_MIXED)
-    k_gather<true><<<nb, T, 0, st>>>(n, s->d_pos, nl->d_offset, nl->d_xbuild,
-                                     nl->d_sorted, s->d_charge, s->d_type, s->d_mol,
-                                     nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
-                                     nl->d_maxdisp);
-  else
-    k_gather<false><<<nb, T, 0, st>>>(n, s->d_pos, nl->d_offset, nl->d_xbuild,
+    k_gather<true><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_xbuild,
                                       nl->d_sorted, s->d_charge, s->d_type, s->d_mol,
                                       nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
                                       nl->d_maxdisp);
-  BuildArgs ba;
-  ba.box = s->box;
-  ba.n = n;
-  ba.ncx = nl->ncx; ba.ncy = nl->ncy; ba.ncz = nl->ncz;
-  // FP32 candidate test with a margin well above its rounding error
-  const double r1 = nl->reach + 0.01, r2 = nl->reach + 0.05;
-  ba.reach2 = (float)(r1 * r1);
-  ba.cull2 = (float)(r2 * r2);
+  else
+    k_gather<false><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_xbuild,
+                                       nl->d_sorted, s->d_charge, s->d_type, s->d_mol,
+                                       nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
+                                       nl->d_maxdisp);
+  const int nhalf = nl->ns_max / 4;
+  k_bbox<<<(nhalf + T - 1) / T, T, 0, st>>>(nl->d_rebuild, nhalf, nl->d_sorted, nl->d_xhi,
+                                           nl->d_bb);
+  TileBuildArgs ba;
+  ba.nclusters = nl->nclusters;
+  ba.periodic = s->box.periodic;
+  ba.ncx = nl->ncx; ba.ncy = nl->ncy; ba.nzb = nl->nzb;
   for (int c = 0; c < 3; c++) {
-    ba.cell_lo[c] = (float)(s->box.periodic ? s->box.min[c] - s->box.origin[c]
-                                            : nl->vac_origin[c]);
+    ba.lo[c] = (float)nl->lo[c];
     ba.cs[c] = (float)nl->cs[c];
     ba.L[c] = (float)s->box.e[c];
     ba.H2[c] = (float)s->box.H2[c];
   }
-  ba.inv_layer = (float)(kFine / nl->cs[2]);
-  ba.nlayers = nl->ncz * kFine;
+  // FP32 pair test with a margin well above its rounding error; wider for
+  // the box culling
+  const double r1 = nl->reach + 0.01;
+  ba.reach2 = (float)(r1 * r1);
+  ba.cull = (float)(nl->reach + 0.05);
   ba.cap = nl->cap;
-  ba.periodic = s->box.periodic;
   ba.excl_start = s->d_excl_start;
   ba.excl_partner = s->d_excl_partner;
   ba.excl_class = s->d_excl_class;
-  k_build_list<<<(n + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, st>>>(
-      ba, nl->d_rebuild, nl->d_key, nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s,
-      nl->d_nbr, nl->d_nbr_count, s->d_status);
+  k_build_tiles<<<(nl->nclusters + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, st>>>(
+      ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s, nl->d_bb,
+      nl->d_tiles, nl->d_tile_count, s->d_status);
   PM_CUDA(cudaGetLastError());
   nl->built = 1;
   return PMGPU_OK;
 }
+
+static int pair_splits(int nclusters);
 
 template <typename Real>
 static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
@@ -589,6 +740,7 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   if (t.mask & TERM_LJ) mx = std::max(mx, t.lj_cut2);
   if (t.mask & TERM_COUL) mx = std::max(mx, t.coul_cut2);
   if (t.mask & TERM_EWALD) mx = std::max(mx, t.ewald_rc2);
+  a.max_cut2 = mx;
   a.max_hi = (Real)(mx * (1 + band));
   a.max_lo = (Real)(mx * (1 - band));
   a.minimal_image = t.minimal_image;
@@ -605,13 +757,15 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   a.csf = (Real)t.coulomb_scaling;
   a.csf64 = t.coulomb_scaling;
   a.cap = nl->cap;
+  a.nclusters = nl->nclusters;
+  a.splits = pair_splits(nl->nclusters);
   a.sorted = nl->d_sorted;
   a.pos = s->d_pos;
   a.excl_start = s->d_excl_start;
   a.excl_partner = s->d_excl_partner;
   a.excl_class = s->d_excl_class;
-  a.nbr = nl->d_nbr;
-  a.nbr_count = nl->d_nbr_count;
+  a.tiles = nl->d_tiles;
+  a.tile_count = nl->d_tile_count;
   a.xhi = nl->d_xhi;
   a.xlo = nl->d_xlo;
   a.xw = nl->d_xw;
@@ -634,11 +788,12 @@ static int spec_kind(const SwitchParams &sw) {
   return -2;
 }
 
-// Blocks of the pair kernel: one warp per atom, except the force-only FP32
-// kernel of the inner MD steps, whose grid is capped at three blocks per SM
-// (warps stride over the atoms) so that the PME / bonded chain on the
-// system's second stream always finds room beside it.
-static int pair_blocks(int n, bool persistent) {
+// Warps per i cluster row of the tile kernel: about four waves of the
+// force-only kernel's resident warps (five blocks of kPairWarps per SM),
+// at most 8 per row, so blocks that finish early are refilled and the
+// tail stays short.  The split depends only on the system, so every launch
+// of a system sums its forces in the same order.
+static int pair_splits(int nclusters) {
   static int sms = 0;
   if (!sms) {
     int dev = 0;
@@ -647,38 +802,33 @@ static int pair_blocks(int n, bool persistent) {
         sms <= 0)
       sms = 148;
   }
-  const int nb = (n + kPairWarps - 1) / kPairWarps;
-  return persistent ? std::max(1, std::min(nb, 3 * sms)) : nb;
+  const long long want = 4LL * sms * 5 * kPairWarps;
+  return (int)std::max(1LL, std::min(8LL, (want + nclusters / 2) / std::max(1, nclusters)));
 }
 
 template <typename Real, int TERMS, typename SPEC>
 static void launch_pairs_spec(PairArgs<Real> &a, cudaStream_t st, int mode) {
   const int T = kPairWarps * 32;
+  const int nb = (int)(((long long)a.nclusters * a.splits + kPairWarps - 1) / kPairWarps);
+  if (nb == 0) return;
   switch (mode) {
-    case PAIR_FORCE:
-      k_pairs<Real, TERMS, PAIR_FORCE, SPEC><<<pair_blocks(a.n, sizeof(Real) == 4), T, 0, st>>>(a);
-      break;
-    case PAIR_ENERGY:
-      k_pairs<Real, TERMS, PAIR_ENERGY, SPEC><<<pair_blocks(a.n, false), T, 0, st>>>(a);
-      break;
-    case PAIR_VIRIAL:
-      k_pairs<Real, TERMS, PAIR_VIRIAL, SPEC><<<pair_blocks(a.n, false), T, 0, st>>>(a);
-      break;
-    default:
-      k_pairs<Real, TERMS, PAIR_RECORD, SPEC><<<pair_blocks(a.n, false), T, 0, st>>>(a);
-      break;
+    case PAIR_FORCE: k_pairs<Real, TERMS, PAIR_FORCE, SPEC><<<nb, T, 0, st>>>(a); break;
+    case PAIR_ENERGY: k_pairs<Real, TERMS, PAIR_ENERGY, SPEC><<<nb, T, 0, st>>>(a); break;
+    case PAIR_VIRIAL: k_pairs<Real, TERMS, PAIR_VIRIAL, SPEC><<<nb, T, 0, st>>>(a); break;
+    default: k_pairs<Real, TERMS, PAIR_RECORD, SPEC><<<nb, T, 0, st>>>(a); break;
   }
 }
 
 template <typename Real, int TERMS, typename SPEC>
 static void launch_force_spec(PairArgs<Real> &a, cudaStream_t st) {
-  k_pairs<Real, TERMS, PAIR_FORCE, SPEC><<<pair_blocks(a.n, true), kPairWarps * 32, 0, st>>>(a);
+  launch_pairs_spec<Real, TERMS, SPEC>(a, st, PAIR_FORCE);
 }
 
 template <typename Real, int TERMS>
 static void launch_pairs_t(PairArgs<Real> &a, cudaStream_t st, int mode, const PairTerms &t) {
   // specialised force-only FP32 kernels of the common configurations
-  if (sizeof(Real) == 4 && mode == PAIR_FORCE) {
+  // (every term with one cutoff, box edges at least twice the cutoff)
+  if (sizeof(Real) == 4 && mode == PAIR_FORCE && a.same_cut && !a.minimal_image) {
     const int lk = spec_kind(t.lj_sw), ck = spec_kind(t.coul_sw);
     if (TERMS == (TERM_LJ | TERM_EWALD) && !t.exact_erf && lk == PMGPU_SW_C2) {
       launch_force_spec<Real, TERM_LJ | TERM_EWALD, PairSpec<PMGPU_SW_C2, -1, 0>>(a, st);

@@ -1,8 +1,9 @@
 // The fused nonbonded pair kernel: Lennard-Jones and Coulomb with
 // ProtoMol's switching functions (OneAtomPair / OneAtomPairTwo,
 // force/OneAtomPairTwo.h:30-100) and the Ewald real-space term
-// (NonbondedFullEwaldSystemForce::realTerm, .h:753-858), over full Verlet
-// lists (warp per sorted atom, accepted pairs compacted in shared memory).
+// (NonbondedFullEwaldSystemForce::realTerm, .h:753-858), over the
+// cluster-pair list (8 x 4 atom tiles, one pair per lane, each unordered
+// pair listed once).
 //
 // Arithmetic:
 //   * forces: the kernel precision Real (FP32 in the mixed mode) from
@@ -32,7 +33,7 @@ struct PairArgs {
   SwitchDev<double> lj_sw64, coul_sw64;
   int lj_modify, coul_modify;
   // rough-test cutoffs^2 (FP64 exact and the kernel-precision band)
-  double lj_cut2, coul_cut2, ew_cut2;
+  double lj_cut2, coul_cut2, ew_cut2, max_cut2;
   Real lj_lo, lj_hi, coul_lo, coul_hi, ew_lo, ew_hi, max_lo, max_hi;
   int same_cut;          // all active terms share one cutoff
   int minimal_image;     // LJ / Coulomb cutoff terms only for the minimal image
@@ -42,12 +43,14 @@ struct PairArgs {
   int exact_erf;
   Real csf;  // coulomb scaling factor
   double csf64;
-  int cap;
+  int cap;              // tiles per i cluster row
+  int nclusters;        // 8-atom i clusters
+  int splits;           // warps per i cluster row
   const int *sorted;
   const double *pos;     // raw positions (exact re-test)
   const int *excl_start, *excl_partner, *excl_class;
-  const uint32_t *nbr;
-  const int *nbr_count;
+  const uint4 *tiles;
+  const int *tile_count;
   const float4 *xhi, *xlo;
   const double4 *xw;
   const int *type;
@@ -206,6 +209,72 @@ __device__ __forceinline__ Real pair_force(const PairArgs<Real> &a, const Real *
   return f;
 }
 
+// Switch of a force-only specialised kernel, without branches: the value
+// and derivative of every region are formed and the region's selected
+// (C2SwitchingFunction.h:42-52, C1SwitchingFunction.h:41-50).  rinv is
+// 1/sqrt(r2).
+template <typename Real, int KIND>
+__device__ __forceinline__ void switch_fast(const SwitchDev<Real> &sw, Real r2, Real rinv,
+                                            Real &ff, Real en) {
+  if (KIND == PMGPU_SW_C2) {
+    const Real c2 = sw.cutoff2 - r2;
+    const Real c4 = c2 * (sw.s2 + Real(2) * r2);
+    const bool on = r2 >= sw.switchon2, off = r2 > sw.cutoff2;
+    const Real val = off ? Real(0) : (on ? sw.s1 * (c2 * c4) : Real(1));
+    const Real der = (on && !off) ? sw.s3 * (c2 * c2 - c4) : Real(0);
+    ff = ff * val - en * der;
+  } else if (KIND == PMGPU_SW_C1) {
+    const Real d = r2 * rinv;
+    const bool off = r2 > sw.cutoff2;
+    const Real val = off ? Real(0) : Real(1) - d * (sw.c1a - r2 * sw.c1b);
+    const Real der = off ? Real(0) : -sw.c1a * rinv + d * sw.c1c;
+    ff = ff * val - en * der;
+  }
+}
+
+// Pair force of the force-only specialised kernels: every term inside its
+// (common) cutoff, no energies, no branches.  Same arithmetic as
+// pair_force.
+template <typename Real, int TERMS, typename SPEC>
+__device__ __forceinline__ Real pair_force_fast(const PairArgs<Real> &a, const Real *ljrow,
+                                                Real r2, Real qq, int tj, bool modified) {
+  const Real rinv = rsqrt_nr(r2);
+  const Real rinv2 = rinv * rinv;
+  Real f = 0;
+  if (TERMS & TERM_LJ) {
+    Real A, B;
+    if (sizeof(Real) == 4) {
+      const float4 p = __ldg(reinterpret_cast<const float4 *>(ljrow) + tj);
+      A = modified ? p.z : p.x;
+      B = modified ? p.w : p.y;
+    } else {
+      const double4 p = reinterpret_cast<const double4 *>(ljrow)[tj];
+      A = modified ? p.z : p.x;
+      B = modified ? p.w : p.y;
+    }
+    const Real r6 = rinv2 * rinv2 * rinv2;
+    const Real r6B = B * r6;
+    const Real r12A = A * r6 * r6;
+    Real ff = (Real(12) * r12A - Real(6) * r6B) * rinv2;
+    switch_fast<Real, SPEC::lj>(a.lj_sw, r2, rinv, ff, r12A - r6B);
+    f += ff;
+  }
+  qq = modified ? qq * a.csf : qq;
+  if (TERMS & TERM_COUL) {
+    const Real en = qq * rinv;
+    Real ff = en * rinv2;
+    switch_fast<Real, SPEC::coul>(a.coul_sw, r2, rinv, ff, en);
+    f += ff;
+  }
+  if (TERMS & TERM_EWALD) {
+    const Real ar = a.alpha * (r2 * rinv);
+    const Real ee = qq * fast_exp(-ar * ar);
+    const Real en = SPEC::exact == 0 ? poly5_fast<Real>(ar) * ee * rinv : qq * erfc(ar) * rinv;
+    f += (en + a.a2pi * ee) * rinv2;
+  }
+  return f;
+}
+
 // FP64 energies (and, for the virial, the FP64 pair force) of one accepted
 // pair from the FP64 wrapped coordinates: the observables of output steps
 // in the mixed-precision path.
@@ -261,243 +330,268 @@ __device__ __forceinline__ void pair_energy64(const PairArgs<Real> &a, const dou
     f += (en + a.a2pi64 * ee) * rr2;
   }
   if (FORCE64) {
-    // addVirial(fij, d) with fij = d * f, half per visit
-    double hf = 0.5 * f;
-    V[0] += ex * ex * hf; V[1] += ex * ey * hf; V[2] += ex * ez * hf;
-    V[3] += ey * ey * hf; V[4] += ey * ez * hf; V[5] += ez * ez * hf;
+    // addVirial(fij, d) with fij = d * f (each pair is listed once)
+    V[0] += ex * ex * f; V[1] += ex * ey * f; V[2] += ex * ez * f;
+    V[3] += ey * ey * f; V[4] += ey * ez * f; V[5] += ez * ez * f;
   }
 }
 
-// One warp per sorted atom i over its full neighbour row.  Phase 1: the 32
-// lanes take 32 consecutive entries, form the distance, apply the cutoff
-// tests (with the exact FP64 re-test near a cutoff) and compact the accepted
-// pairs into a per-warp ring in shared memory.  Phase 2: whenever 32
-// accepted pairs are queued, every lane evaluates one of them, so the
-// expensive pair arithmetic runs with all lanes busy.  Each unordered pair
-// is visited from both ends; forces are written for i only (no atomics on
-// j), energies and virial are halved.
-constexpr int kQueue = 64;
-
-// Per-warp ring of accepted pairs: (dx, dy, dz, r2) and (j, type j, charge
-// j, flags | image << 4).
-template <typename Real> struct QueueVec;
-template <> struct QueueVec<float> { using T = float4; };
-template <> struct QueueVec<double> { using T = double4; };
-
-template <typename Real>
-struct PairQueue {
-  typename QueueVec<Real>::T d[kPairWarps][kQueue];
-  int4 m[kPairWarps][kQueue];
-  Real qj[kPairWarps][kQueue];
-};
-
-// Registers: the force-only FP32 variant (the inner MD steps) is held to 64
-// so four blocks fit per SM; energy/virial/record and FP64 variants get more.
-template <typename Real, int MODE>
+// Registers: the specialised force-only FP32 kernels (the inner MD steps)
+// are held to 48 so five blocks fit per SM, the generic force-only FP32
+// kernel to 64; energy/virial/record and FP64 variants get more.
+template <typename Real, int MODE, typename SPEC>
 struct PairOccupancy {
-  static constexpr int blocks = (MODE == PAIR_FORCE && sizeof(Real) == 4) ? 4 : 2;
+  static constexpr bool fast = MODE == PAIR_FORCE && sizeof(Real) == 4 && SPEC::lj >= 0 &&
+                               SPEC::exact >= 0;
+  static constexpr int blocks = fast ? 5 : ((MODE == PAIR_FORCE && sizeof(Real) == 4) ? 4 : 2);
 };
 
+// Sum of (x, y, z) over the 8 lanes that share lane >> 3, transposed: on
+// return lane l holds component (l & 3) of its group's sum (x, y, z, 0).
+// Four shuffles instead of nine.
+template <typename Real>
+__device__ __forceinline__ Real group8_sum3(Real x, Real y, Real z, int lane) {
+  const bool b0 = lane & 1, b1 = lane & 2;
+  // xor 1: even lanes keep (x, z), odd lanes keep (y, 0)
+  const Real k0 = b0 ? y : x, s0 = b0 ? x : y;
+  const Real k1 = b0 ? Real(0) : z, s1 = b0 ? z : Real(0);
+  const Real r0 = k0 + __shfl_xor_sync(0xffffffffu, s0, 1);
+  const Real r1 = k1 + __shfl_xor_sync(0xffffffffu, s1, 1);
+  // xor 2: lanes with bit 1 clear keep r0, the others r1
+  Real v = (b1 ? r1 : r0) + __shfl_xor_sync(0xffffffffu, b1 ? r0 : r1, 2);
+  v += __shfl_xor_sync(0xffffffffu, v, 4);
+  return v;
+}
+
+__device__ __forceinline__ long long fixed_force(float v) {
+  return __float2ll_rn(v * 4294967296.0f);  // exact scaling by 2^32
+}
+__device__ __forceinline__ long long fixed_force(double v) { return to_fixed(v, kForceScale); }
+
+// One warp per (8-atom i cluster, contiguous share of its tile row).  Lane
+// l holds pair (i atom l & 7, j atom l >> 3) of every 8 x 4 tile, so a
+// tile's 32 pairs are evaluated at once with no compaction.  The list holds
+// each unordered pair once, so the pair force goes to both atoms: i's
+// share accumulates in the lane over the warp's tiles, j's share is summed
+// over the 8 lanes of the same j atom and added with one fixed-point
+// atomic per component.  Energies and virial count every pair once.
+// Pairs are accepted by the cutoff tests of the reference (with the exact
+// FP64 re-test near a cutoff); the tile mask carries the list's exclusion
+// and modified (scaled 1-4) status.
 template <typename Real, int TERMS, int MODE, typename SPEC>
-__global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE>::blocks)
+__global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPEC>::blocks)
     k_pairs(PairArgs<Real> a) {
   constexpr bool MIXED = sizeof(Real) == 4;
   constexpr bool ENERGY = MODE != PAIR_FORCE;
   constexpr bool VIRIAL = MODE == PAIR_VIRIAL;
   constexpr bool RECORD = MODE == PAIR_RECORD;
+  // force-only kernels of a specialised configuration (launched only when
+  // every term shares one cutoff and the box holds twice the cutoff): every
+  // accepted pair takes every term, evaluated without branches
+  constexpr bool FAST = MIXED && MODE == PAIR_FORCE && SPEC::lj >= 0 && SPEC::exact >= 0;
   constexpr unsigned kAll = 0xffffffffu;
-  __shared__ PairQueue<Real> Q;
-  const int w = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const unsigned lt_mask = (1u << lane) - 1u;
+  const int gw = blockIdx.x * kPairWarps + (threadIdx.x >> 5);
+  const int ci = gw / a.splits, sp = gw - ci * a.splits;
+  if (ci >= a.nclusters) return;  // whole warps exit together
+  const int cnt = a.tile_count[ci];
+  const int t0 = (int)((long long)cnt * sp / a.splits);
+  const int t1 = (int)((long long)cnt * (sp + 1) / a.splits);
+  if (t1 <= t0) return;
+  const int il = lane & 7, jl = lane >> 3;
+  const int islot = 8 * ci + il;
+  const int oi = a.sorted[islot];
+  const double4 wi = a.xw[islot];  // energy modes and the FP64 kernel only
+  Real xi_h[3], xi_l[3];
+  Real qi;
+  int ti;
+  if (MIXED) {
+    const float4 h = a.xhi[islot], l = a.xlo[islot];
+    xi_h[0] = h.x; xi_h[1] = h.y; xi_h[2] = h.z; qi = h.w;
+    xi_l[0] = l.x; xi_l[1] = l.y; xi_l[2] = l.z; ti = __float_as_int(l.w);
+  } else {
+    xi_h[0] = wi.x; xi_h[1] = wi.y; xi_h[2] = wi.z; qi = wi.w;
+    xi_l[0] = xi_l[1] = xi_l[2] = Real(0);
+    ti = oi >= 0 ? a.type[oi] : 0;
+  }
+  const Real *ljrow = MIXED ? reinterpret_cast<const Real *>(a.lj32 + ti * a.ntypes)
+                            : reinterpret_cast<const Real *>(a.lj64 + ti * a.ntypes);
+  // i as seen from the tile's image of j (d = xj - (xi - s L))
+  int cur = kZeroShift;
+  Real xs_h[3] = {xi_h[0], xi_h[1], xi_h[2]};
+  Real xs_l[3] = {xi_l[0], xi_l[1], xi_l[2]};
+  Real fx = 0, fy = 0, fz = 0;
   Real vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
   double Elj = 0, Ec = 0;
   double V64[6] = {0, 0, 0, 0, 0, 0};
   int npairs = 0;
-  // Warps stride over the sorted atoms (the grid may be smaller than one
-  // warp per atom, which leaves room on every SM for the work of the other
-  // stream); no block-wide barrier below.
-  for (int ii = blockIdx.x * kPairWarps + w; ii < a.n; ii += gridDim.x * kPairWarps) {
-    const int cnt = a.nbr_count[ii];
-    const uint32_t *row = a.nbr + (size_t)ii * a.cap;
-    uint32_t e_next = lane < cnt ? __ldg(row + lane) : 0u;
-    const int oi = a.sorted[ii];
-    const double4 wi = a.xw[ii];
-    Real xi_h[3], xi_l[3], qi;
-    int ti;
-    if (MIXED) {
-      float4 h = a.xhi[ii], l = a.xlo[ii];
-      xi_h[0] = h.x; xi_h[1] = h.y; xi_h[2] = h.z; qi = h.w;
-      xi_l[0] = l.x; xi_l[1] = l.y; xi_l[2] = l.z; ti = __float_as_int(l.w);
-    } else {
-      xi_h[0] = wi.x; xi_h[1] = wi.y; xi_h[2] = wi.z; qi = wi.w;
-      xi_l[0] = xi_l[1] = xi_l[2] = Real(0);
-      ti = a.type[oi];
+  constexpr int kAllTerms = ((TERMS & TERM_LJ) ? kQLJ : 0) | ((TERMS & TERM_COUL) ? kQCoul : 0) |
+                            ((TERMS & TERM_EWALD) ? kQEwald : 0);
+  const uint4 *row = a.tiles + (size_t)ci * a.cap;
+  uint4 tnext = __ldg(row + t0);
+  for (int t = t0; t < t1; t++) {
+    const uint4 tile = tnext;
+    if (t + 1 < t1) tnext = __ldg(row + t + 1);
+    const int hj = (int)(tile.x & kJMask);
+    const int sh = (int)((tile.x >> kShiftBits) & kShiftMask);
+    if (sh != cur) {  // warp-uniform; tiles are grouped by image
+      const int sx = (sh & 3) - 1, sy = ((sh >> 2) & 3) - 1, sz = ((sh >> 4) & 3) - 1;
+      // reloaded rather than held in registers through the loop
+      const double4 w = a.xw[islot];
+      const double xs64[3] = {w.x - sx * a.box.e[0], w.y - sy * a.box.e[1],
+                              w.z - sz * a.box.e[2]};
+      for (int c = 0; c < 3; c++) {
+        if (MIXED) {
+          const float h = (float)xs64[c];
+          xs_h[c] = h;
+          xs_l[c] = (float)(xs64[c] - (double)h);
+        } else {
+          xs_h[c] = xs64[c];
+        }
+      }
+      cur = sh;
     }
-    const Real *ljrow = MIXED ? reinterpret_cast<const Real *>(a.lj32 + ti * a.ntypes)
-                              : reinterpret_cast<const Real *>(a.lj64 + ti * a.ntypes);
-    // i as seen from the current entry's image of j (d = xj - (xi - s L))
-    int cur = kZeroShift;
-    Real xs_h[3] = {xi_h[0], xi_h[1], xi_h[2]};
-    Real xs_l[3] = {xi_l[0], xi_l[1], xi_l[2]};
-    Real fx = 0, fy = 0, fz = 0;
-    int head = 0, queued = 0;
-
-    auto process = [&](int p) {
-      const auto d = Q.d[w][p];
-      const int4 m = Q.m[w][p];
-      const int flags = m.w & 15;
+    const int jslot = 4 * hj + jl;
+    const bool live = (tile.y >> lane) & 1u;
+    Real dx, dy, dz, qj;
+    int tj = 0;
+    if (MIXED) {
+      const float4 h = a.xhi[jslot], l = a.xlo[jslot];
+      dx = (h.x - xs_h[0]) + (l.x - xs_l[0]);
+      dy = (h.y - xs_h[1]) + (l.y - xs_l[1]);
+      dz = (h.z - xs_h[2]) + (l.z - xs_l[2]);
+      qj = h.w;
+      tj = __float_as_int(l.w);
+    } else {
+      const double4 wj = a.xw[jslot];
+      dx = wj.x - xs_h[0];
+      dy = wj.y - xs_h[1];
+      dz = wj.z - xs_h[2];
+      qj = wj.w;
+    }
+    const Real r2 = dx * dx + dy * dy + dz * dz;
+    if constexpr (FAST) {
+      bool act = live && r2 <= a.max_lo;
+      const bool band = live && !act && r2 <= a.max_hi;
+      if (__any_sync(kAll, band)) {
+        if (band)
+          act = exact_r2(a, oi, a.sorted[jslot], (double)dx, (double)dy, (double)dz) <=
+                a.max_cut2;
+      }
+      const unsigned actm = __ballot_sync(kAll, act);
+      npairs += act;
+      if (!actm) continue;
+      const bool modified = (tile.z >> lane) & 1u;
+      Real f = pair_force_fast<Real, TERMS, SPEC>(a, ljrow, act ? r2 : Real(1), qi * qj, tj,
+                                                  modified);
+      f = act ? f : Real(0);
+      const Real jx = dx * f, jy = dy * f, jz = dz * f;
+      fx -= jx;
+      fy -= jy;
+      fz -= jz;
+      const Real js = group8_sum3<Real>(jx, jy, jz, lane);
+      if (il < 3 && ((actm >> (8 * jl)) & 0xFFu))
+        red_add(&a.force[il * a.n + a.sorted[jslot]], fixed_force(js));
+      continue;
+    }
+    int flags = 0;
+    bool band = false;
+    if (live && a.same_cut) {  // every term shares one cutoff
+      if (r2 <= a.max_lo) flags = kAllTerms;
+      else band = r2 <= a.max_hi;
+    } else if (live) {
+      if (TERMS & TERM_LJ) {
+        if (r2 <= a.lj_lo) flags |= kQLJ;
+        else band |= r2 <= a.lj_hi;
+      }
+      if (TERMS & TERM_COUL) {
+        if (r2 <= a.coul_lo) flags |= kQCoul;
+        else band |= r2 <= a.coul_hi;
+      }
+      if (TERMS & TERM_EWALD) {
+        if (r2 <= a.ew_lo) flags |= kQEwald;
+        else band |= r2 <= a.ew_hi;
+      }
+    }
+    // pairs within a rounding band of a cutoff take the reference's exact
+    // FP64 test (rare: a real branch)
+    if (__any_sync(kAll, band)) {
+      if (band) {
+        const double r2x = exact_r2(a, oi, a.sorted[jslot], (double)dx, (double)dy, (double)dz);
+        if ((TERMS & TERM_LJ) && r2 > a.lj_lo && r2x <= a.lj_cut2) flags |= kQLJ;
+        if ((TERMS & TERM_COUL) && r2 > a.coul_lo && r2x <= a.coul_cut2) flags |= kQCoul;
+        if ((TERMS & TERM_EWALD) && r2 > a.ew_lo && r2x <= a.ew_cut2) flags |= kQEwald;
+      }
+    }
+    // boxes below twice the cutoff: cutoff terms take the minimal image only
+    // (Ewald real space sums every image, NonbondedFullEwaldSystemForce.h:790)
+    if ((TERMS & (TERM_LJ | TERM_COUL)) && a.minimal_image && (flags & (kQLJ | kQCoul)) &&
+        !(fabs(dx) <= a.half_edge[0] && fabs(dy) <= a.half_edge[1] &&
+          fabs(dz) <= a.half_edge[2]))
+      flags &= ~(kQLJ | kQCoul);
+    Real jx = 0, jy = 0, jz = 0;
+    if (flags) {
+      if ((tile.z >> lane) & 1u) flags |= kQModified;
+      if (!MIXED) tj = a.type[a.sorted[jslot]];
       Real en_lj = 0, en_c = 0;
-      const Real f = pair_force<Real, TERMS, SPEC>(a, ljrow, d.w, qi * Q.qj[w][p], m.y, flags,
-                                             en_lj, en_c);
-      fx -= d.x * f;
-      fy -= d.y * f;
-      fz -= d.z * f;
+      const Real f = pair_force<Real, TERMS, SPEC>(a, ljrow, r2, qi * qj, tj, flags, en_lj, en_c);
+      jx = dx * f;
+      jy = dy * f;
+      jz = dz * f;
+      fx -= jx;
+      fy -= jy;
+      fz -= jz;
       npairs++;
       if (ENERGY) {
         if (MIXED) {
-          pair_energy64<Real, TERMS, VIRIAL>(a, wi, a.xw[m.x], m.w >> 4, ti, m.y, flags, Elj,
-                                             Ec, V64);
+          pair_energy64<Real, TERMS, VIRIAL>(a, wi, a.xw[jslot], sh, ti, tj, flags, Elj, Ec,
+                                             V64);
         } else {
           Elj += (double)en_lj;
           Ec += (double)en_c;
         }
       }
       if (VIRIAL && !MIXED) {
-        // addVirial(fij, d) with fij = d * f, half per visit
-        Real hf = Real(0.5) * f;
-        vxx += d.x * d.x * hf; vxy += d.x * d.y * hf; vxz += d.x * d.z * hf;
-        vyy += d.y * d.y * hf; vyz += d.y * d.z * hf; vzz += d.z * d.z * hf;
+        // addVirial(fij, d) with fij = d * f
+        vxx += dx * jx; vxy += dx * jy; vxz += dx * jz;
+        vyy += dy * jy; vyz += dy * jz; vzz += dz * jz;
       }
       if (RECORD) {
-        int oj = a.sorted[m.x];
-        if (oi < oj) {
+        const int oj = a.sorted[jslot];
+        if (oi != oj) {
           long long slot = atomicAdd((unsigned long long *)a.paircount, 1ull);
-          if (slot < a.pairbuf_cap) a.pairbuf[slot] = ((long long)oi << 32) | (unsigned)oj;
+          if (slot < a.pairbuf_cap)
+            a.pairbuf[slot] = ((long long)min(oi, oj) << 32) | (unsigned)max(oi, oj);
         }
-      }
-    };
-
-    for (int k0 = 0; k0 < cnt; k0 += 32) {
-      const int k = k0 + lane;
-      const bool have = k < cnt;
-      const uint32_t e = e_next;
-      // the next round's entry is fetched while this round computes
-      e_next = (k + 32 < cnt) ? __ldg(row + k + 32) : 0u;
-      const int j = (int)(e & kJMask);
-      const int sh = (int)((e >> kShiftBits) & kShiftMask);
-      // image changes are rare (atoms near a face of the box): a real branch
-      if (__any_sync(kAll, have && sh != cur)) {
-        if (have && sh != cur) {
-          const int sx = (sh & 3) - 1, sy = ((sh >> 2) & 3) - 1, sz = ((sh >> 4) & 3) - 1;
-          const double xs64[3] = {wi.x - sx * a.box.e[0], wi.y - sy * a.box.e[1],
-                                  wi.z - sz * a.box.e[2]};
-          for (int c = 0; c < 3; c++) {
-            if (MIXED) {
-              float h = (float)xs64[c];
-              xs_h[c] = h;
-              xs_l[c] = (float)(xs64[c] - (double)h);
-            } else {
-              xs_h[c] = xs64[c];
-            }
-          }
-          cur = sh;
-        }
-      }
-      Real dx, dy, dz, qj;
-      int tj = 0;
-      if (MIXED) {
-        const float4 h = a.xhi[j], l = a.xlo[j];
-        dx = (h.x - xs_h[0]) + (l.x - xs_l[0]);
-        dy = (h.y - xs_h[1]) + (l.y - xs_l[1]);
-        dz = (h.z - xs_h[2]) + (l.z - xs_l[2]);
-        qj = h.w;
-        tj = __float_as_int(l.w);
-      } else {
-        const double4 wj = a.xw[j];
-        dx = wj.x - xs_h[0];
-        dy = wj.y - xs_h[1];
-        dz = wj.z - xs_h[2];
-        qj = wj.w;
-      }
-      const Real r2 = dx * dx + dy * dy + dz * dz;
-      constexpr int kAllTerms = ((TERMS & TERM_LJ) ? kQLJ : 0) | ((TERMS & TERM_COUL) ? kQCoul : 0) |
-                                ((TERMS & TERM_EWALD) ? kQEwald : 0);
-      int flags = 0;
-      bool band = false;
-      if (have && a.same_cut) {  // every term shares one cutoff
-        if (r2 <= a.max_lo) flags = kAllTerms;
-        else band = r2 <= a.max_hi;
-      } else if (have) {
-        if (TERMS & TERM_LJ) {
-          if (r2 <= a.lj_lo) flags |= kQLJ;
-          else band |= r2 <= a.lj_hi;
-        }
-        if (TERMS & TERM_COUL) {
-          if (r2 <= a.coul_lo) flags |= kQCoul;
-          else band |= r2 <= a.coul_hi;
-        }
-        if (TERMS & TERM_EWALD) {
-          if (r2 <= a.ew_lo) flags |= kQEwald;
-          else band |= r2 <= a.ew_hi;
-        }
-      }
-      // pairs within a rounding band of a cutoff take the reference's exact
-      // FP64 test (rare: a real branch)
-      if (__any_sync(kAll, band)) {
-        if (band) {
-          const double r2x = exact_r2(a, oi, a.sorted[j], (double)dx, (double)dy, (double)dz);
-          if ((TERMS & TERM_LJ) && r2 > a.lj_lo && r2x <= a.lj_cut2) flags |= kQLJ;
-          if ((TERMS & TERM_COUL) && r2 > a.coul_lo && r2x <= a.coul_cut2) flags |= kQCoul;
-          if ((TERMS & TERM_EWALD) && r2 > a.ew_lo && r2x <= a.ew_cut2) flags |= kQEwald;
-        }
-      }
-      // boxes below twice the cutoff: cutoff terms take the minimal image only
-      // (Ewald real space sums every image, NonbondedFullEwaldSystemForce.h:790)
-      if ((TERMS & (TERM_LJ | TERM_COUL)) && a.minimal_image && (flags & (kQLJ | kQCoul)) &&
-          !(fabs(dx) <= a.half_edge[0] && fabs(dy) <= a.half_edge[1] &&
-            fabs(dz) <= a.half_edge[2]))
-        flags &= ~(kQLJ | kQCoul);
-      const bool pass = flags != 0;
-      const unsigned mk = __ballot_sync(kAll, pass);
-      if (pass) {
-        if (!MIXED) tj = a.type[a.sorted[j]];
-        if (e & kModifiedBit) flags |= kQModified;
-        const int p = (head + queued + __popc(mk & lt_mask)) & (kQueue - 1);
-        typename QueueVec<Real>::T d;
-        d.x = dx; d.y = dy; d.z = dz; d.w = r2;
-        Q.d[w][p] = d;
-        Q.m[w][p] = make_int4(j, tj, 0, flags | (sh << 4));
-        Q.qj[w][p] = qj;
-      }
-      queued += __popc(mk);
-      if (queued >= 32) {
-        __syncwarp();
-        process((head + lane) & (kQueue - 1));
-        head += 32;
-        queued -= 32;
-        __syncwarp();
       }
     }
-    if (queued > 0) {
-      __syncwarp();
-      if (lane < queued) process((head + lane) & (kQueue - 1));
+    // j's share: summed over its 8 lanes, one atomic per component
+    const unsigned act = __ballot_sync(kAll, flags != 0);
+    const Real js = group8_sum3<Real>(jx, jy, jz, lane);
+    if (il < 3 && ((act >> (8 * jl)) & 0xFFu)) {
+      const int oj = a.sorted[jslot];
+      red_add(&a.force[il * a.n + oj], fixed_force(js));
     }
-    __syncwarp();  // the ring is refilled by the next atom
-    double Fx = warp_sum((double)fx), Fy = warp_sum((double)fy), Fz = warp_sum((double)fz);
-    if (lane == 0) {
-      red_add(&a.force[oi], to_fixed(Fx, kForceScale));
-      red_add(&a.force[a.n + oi], to_fixed(Fy, kForceScale));
-      red_add(&a.force[2 * a.n + oi], to_fixed(Fz, kForceScale));
-    }
+  }
+  // i's share: summed over the 4 j lanes of each i atom
+#pragma unroll
+  for (int o = 8; o < 32; o <<= 1) {
+    fx += __shfl_xor_sync(kAll, fx, o);
+    fy += __shfl_xor_sync(kAll, fy, o);
+    fz += __shfl_xor_sync(kAll, fz, o);
+  }
+  if (jl == 0 && oi >= 0) {
+    red_add(&a.force[oi], fixed_force(fx));
+    red_add(&a.force[a.n + oi], fixed_force(fy));
+    red_add(&a.force[2 * a.n + oi], fixed_force(fz));
   }
   if (ENERGY || a.count_pairs) {
     int np = warp_sum(npairs);
     if (lane == 0) red_add(&a.acc[ACC_PAIRS], (long long)np);
   }
   if (ENERGY) {
-    double dlj = warp_sum(Elj) * 0.5;
-    double dc = warp_sum(Ec) * 0.5;
+    double dlj = warp_sum(Elj);
+    double dc = warp_sum(Ec);
     double V[6] = {0, 0, 0, 0, 0, 0};
     if (VIRIAL) {
       if (MIXED) {

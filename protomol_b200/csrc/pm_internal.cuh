@@ -47,25 +47,26 @@ enum { ACC_COULOMB = 0, ACC_LJ, ACC_BOND, ACC_ANGLE, ACC_DIHEDRAL,
 enum { ST_LIST_OVERFLOW = 1, ST_NONFINITE = 2, ST_CELL_OVERFLOW = 4,
        ST_BAD_BOX = 8 };
 
-// Neighbour-entry layout: bits 0..23 sorted j index, 24..29 periodic image
-// of j as three 2-bit fields (sx+1, sy+1, sz+1), bit 30 "modified (scaled
-// 1-4) pair".  Fully excluded minimal-image pairs never enter the list.
+// Tile layout (uint4): x = j cluster (bits 0..23) | periodic image of the
+// j cluster as three 2-bit fields (sx+1, sy+1, sz+1) at bits 24..29;
+// y = interaction mask, z = modified (scaled 1-4) mask, bit l for lane l =
+// (i atom l & 7, j atom l >> 3).  Fully excluded minimal-image pairs are
+// cleared from the interaction mask when the list is built.
 constexpr uint32_t kJMask = 0xFFFFFFu;
 constexpr int kShiftBits = 24;
 constexpr uint32_t kShiftMask = 0x3Fu;
-constexpr uint32_t kModifiedBit = 1u << 30;
 constexpr int kZeroShift = 1 | (1 << 2) | (1 << 4);
 __host__ __device__ constexpr int shift_code(int sx, int sy, int sz) {
   return (sx + 1) | ((sy + 1) << 2) | ((sz + 1) << 4);
 }
 constexpr int kMaxAtoms = 1 << 24;
 
-// Fine sub-cells per coarse cell and axis (Morton-ordered inside a coarse
-// cell), so that 32 consecutive sorted atoms are spatially compact.
-constexpr int kFine = 4;
-constexpr int kFine3 = kFine * kFine * kFine;
+// Sort grid of the cluster-pair list: xy column width (about the edge of a
+// cube holding 8 atoms of condensed matter) and z-bin height.
+constexpr double kColumnWidth = 4.4;
+constexpr double kZBin = 0.5;
 
-// Warps per block of the warp-per-atom pair kernel and list build.
+// Warps per block of the tile kernel and of the list build.
 constexpr int kPairWarps = 8;
 constexpr int kBuildWarps = 8;
 // Inner MD steps captured per CUDA graph in pmgpu_run.
@@ -111,34 +112,48 @@ struct PairTerms {
   int minimal_image;        // cutoff terms see only the minimal image
 };
 
-// Device arrays of one neighbour-list structure (one per distinct
-// (cutoff, skin) in a system).
+// Device arrays of one cluster-pair list (one per distinct (cutoff, skin)
+// in a system).  Atoms are counting-sorted into ncx x ncy columns of the xy
+// plane and sorted by z inside a column; every column's atoms are
+// contiguous and padded to a whole number of 8-atom clusters (padding
+// slots hold no atom).  A per-column index of z bins gives the slot range
+// of a z window.  The list holds, per 8-atom i cluster, tiles against
+// 4-atom j clusters: each unordered pair within the reach appears in
+// exactly one tile (see k_build_tiles).
+constexpr int kColCap = 4096;  // atoms per column the in-block sort holds
+
 struct NeighborList {
   double cutoff = 0, skin = 0, reach = 0;
-  int ncx = 0, ncy = 0, ncz = 0;     // coarse cells
-  double cs[3] = {0, 0, 0};          // coarse cell size vector
-  double vac_origin[3] = {0, 0, 0};  // vacuum grid minimum
-  int nkeys = 0;
-  int cap = 0;                       // entries per atom
+  int ncx = 0, ncy = 0, nzb = 0, ncol = 0;
+  double lo[3] = {0, 0, 0};          // grid corner in the wrapped (xw) frame
+  double cs[3] = {0, 0, 0};          // column widths (x, y), z-bin height
+  int nkeys = 0;                     // ncol * nzb
+  int ns_max = 0;                    // slots incl. padding (multiple of 8)
+  int nclusters = 0;                 // ns_max / 8
+  int cap = 0;                       // tiles per i cluster
   int built = 0;
   long long builds = 0;
   // device
-  int *d_key = nullptr;         // n
-  int *d_key_count = nullptr;   // nkeys
-  int *d_key_start = nullptr;   // nkeys + 1
-  int *d_key_cursor = nullptr;  // nkeys
-  int *d_sorted = nullptr;      // n: original index of sorted slot
-  double *d_offset = nullptr;   // 3n: x_build - x_wrapped (original order)
-  double *d_xbuild = nullptr;   // 3n
-  float4 *d_xhi = nullptr;      // n (x,y,z,q)
-  float4 *d_xlo = nullptr;      // n (x,y,z, type bits)
-  double4 *d_xw = nullptr;      // n FP64 wrapped position + q
-  int *d_mol_s = nullptr;       // n molecule of each sorted slot
-  uint32_t *d_nbr = nullptr;    // n rows of cap entries (row per sorted atom)
-  int *d_nbr_count = nullptr;   // n
+  int *d_key = nullptr;          // n: column of each atom
+  unsigned *d_zkey = nullptr;    // n: z above the grid corner (FP32 bits, >= 0)
+  int *d_unsorted = nullptr;     // n: atoms grouped by column, any order
+  int *d_col_count = nullptr;    // ncol
+  int *d_col_u = nullptr;        // ncol: first entry of each column in d_unsorted
+  int *d_col_cursor = nullptr;   // ncol
+  int *d_col_base = nullptr;     // ncol + 1: first slot of each column (padded)
+  int *d_key_start = nullptr;    // nkeys + 1: first slot of each (column, z bin)
+  int *d_sorted = nullptr;       // ns_max: atom of each slot, -1 for padding
+  double *d_offset = nullptr;    // 3n: x_build - x_wrapped (original order)
+  double *d_xbuild = nullptr;    // 3n
+  float4 *d_xhi = nullptr;       // ns_max (x,y,z,q)
+  float4 *d_xlo = nullptr;       // ns_max (x,y,z residue, type bits)
+  double4 *d_xw = nullptr;       // ns_max FP64 wrapped position + q
+  int *d_mol_s = nullptr;        // ns_max molecule of each slot (-1 padding)
+  float4 *d_bb = nullptr;        // 2 per 4-atom cluster: lower, upper corner
+  uint4 *d_tiles = nullptr;      // nclusters rows of cap tiles
+  int *d_tile_count = nullptr;   // nclusters
   unsigned int *d_maxdisp = nullptr;  // float bits of max displacement^2
-  int *d_rebuild = nullptr;     // rebuild flag
-  void *d_scan_tmp = nullptr;
+  int *d_rebuild = nullptr;      // rebuild flag, build count
 };
 
 struct System;

@@ -24,6 +24,7 @@ constexpr double kGridScale = 4294967296.0;  // 2^32 per (scaled) charge
 struct PmeArgs {
   Box box;
   int n;
+  int nt;  // atom slots: n, or the pair list's padded spatial order (-1 = empty)
   int K[3];
   int order;
   double inv_L[3];
@@ -87,8 +88,9 @@ k_pme_spread(PmeArgs a, const double *__restrict__ pos, const double *__restrict
              const int *__restrict__ order_map, long long *__restrict__ grid) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = gt / L, kx = gt & (L - 1);
-  if (t >= a.n || kx >= P) return;
-  int i = order_map ? order_map[t] : t;
+  if (t >= a.nt || kx >= P) return;
+  const int i = order_map ? order_map[t] : t;
+  if (i < 0) return;
   double wx, wy, wz;
   box_minpos(a.box, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wx, wy, wz);
   int iu[3];
@@ -189,11 +191,10 @@ k_pme_gather(PmeArgs a, const double *__restrict__ pos, const double *__restrict
              long long *__restrict__ force) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = gt / L, kx = gt & (L - 1);
-  const bool valid = t < a.n;
+  int i = t < a.nt ? (order_map ? order_map[t] : t) : -1;
+  const bool valid = i >= 0;
   float sx = 0.f, sy = 0.f, sz = 0.f;
-  int i = 0;
   if (valid) {
-    i = order_map ? order_map[t] : t;
     double wx, wy, wz;
     box_minpos(a.box, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wx, wy, wz);
     int iu[3];
@@ -408,7 +409,7 @@ template <int P>
 static void launch_spread_gather(const PmeArgs &a, System *s, Force *f, const int *order_map,
                                  int gather) {
   constexpr int L = P <= 4 ? 4 : 8;
-  const int nb = (int)(((long long)a.n * L + 127) / 128);
+  const int nb = (int)(((long long)a.nt * L + 127) / 128);
   if (!gather)
     k_pme_spread<P, L><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
                                                   f->d_grid_fixed);
@@ -448,9 +449,12 @@ int pme_reciprocal(System *s, Force *f, int em) {
   // Spread in the spatial order of the pair list when there is one, so
   // neighbouring threads hit neighbouring grid lines.
   const int *order_map = nullptr;
+  a.nt = n;
   if (f->list_index >= 0 && f->list_index < (int)s->lists.size() &&
-      s->lists[f->list_index].built)
+      s->lists[f->list_index].built) {
     order_map = s->lists[f->list_index].d_sorted;
+    a.nt = s->lists[f->list_index].ns_max;
+  }
   // the plans run on whichever stream this evaluation uses
   if (cufftSetStream(f->plan_r2c, s->stream) != CUFFT_SUCCESS ||
       cufftSetStream(f->plan_c2r, s->stream) != CUFFT_SUCCESS)
