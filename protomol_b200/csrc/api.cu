@@ -200,6 +200,7 @@ static int system_free(System *s) {
   if (s->side) cudaStreamSynchronize(s->side);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->ev_fork2) cudaEventDestroy(s->ev_fork2);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->stream) cudaStreamDestroy(s->stream);
   return PMGPU_OK;
@@ -302,30 +303,20 @@ static int evaluate_forces(System *s, int only, int mode) {
     if (f.kind == FK_CUTOFF || (f.kind == FK_PME && (f.ewald_flags & PMGPU_EWALD_REAL)))
       add_pair_terms(groups, f.list_index, f.terms);
   }
-  // neighbour lists are prepared once per evaluation
-  for (auto &f : s->forces) {
-    if (only >= 0 ? f.id != only : !f.enabled) continue;
-    if (f.list_index >= 0 && !prepared[f.list_index]) {
-      prof_begin(s, PMGPU_PHASE_LIST);
-      int r = nb_prepare(s, &s->lists[f.list_index], 0);
-      prof_end(s);
-      PM_CHECK(r);
-      s->kernels += 7;  // check, bin, scan, scatter, sort, gather, build
-      prepared[f.list_index] = 1;
-    }
-  }
-  // The other terms (PME, corrections, bonded, GB, all-pairs) only read the
-  // positions and add into the fixed-point forces and energies, so they run
-  // on the system's second stream beside the pair kernels and join before
-  // the evaluation ends (not while profiling, which times phases in order).
-  // That stream has the higher priority and is enqueued first, so its short
-  // dependent kernels are not queued behind the pair kernel's blocks.
+  // Terms other than the pair kernels (bonded, GB, all-pairs, PME,
+  // corrections) only read the positions and add into the fixed-point
+  // forces and energies, so they run on the system's second stream beside
+  // the list work and the pair kernels, and join before the evaluation ends
+  // (not while profiling, which times phases in order).  The terms that do
+  // not read the list start at once; PME, which spreads in the list's slot
+  // order, starts once the (conditional) sort is done.  The second stream
+  // has the higher priority, so its short dependent kernels are not queued
+  // behind the pair kernel's blocks.
   const bool fork = s->side && !s->prof.enabled;
   const cudaStream_t main_stream = s->stream;
   if (fork) {
     PM_CUDA(cudaEventRecord(s->ev_fork, main_stream));
     PM_CUDA(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
-    s->stream = s->side;
   }
   struct Join {  // back on the main stream, joined, on every exit path
     System *s;
@@ -338,64 +329,99 @@ static int evaluate_forces(System *s, int only, int mode) {
       cudaStreamWaitEvent(main_stream, s->ev_join, 0);
     }
   } join{s, main_stream, fork};
+  auto run_terms = [&](bool list_terms) -> int {
+    if (fork) s->stream = s->side;
+    for (auto &f : s->forces) {
+      if (only >= 0 ? f.id != only : !f.enabled) continue;
+      if ((f.kind == FK_PME) != list_terms) continue;
+      int r = PMGPU_OK;
+      switch (f.kind) {
+        case FK_PME:
+          if (f.ewald_flags & PMGPU_EWALD_RECIPROCAL) {
+            prof_begin(s, PMGPU_PHASE_PME);
+            r = pme_reciprocal(s, &f, em);
+            prof_end(s);
+            PM_CHECK(r);
+            s->kernels += 4;  // spread, fixed->float, convolve, gather (+ cuFFT)
+          }
+          if (f.ewald_flags & PMGPU_EWALD_CORRECTION) {
+            prof_begin(s, PMGPU_PHASE_CORRECTION);
+            r = ewald_correction(s, &f, em);
+            prof_end(s);
+            s->kernels += s->n_excl > 0;
+          }
+          break;
+        case FK_GB:
+          prof_begin(s, PMGPU_PHASE_GB);
+          r = gb_forces(s, &f);
+          prof_end(s);
+          s->kernels += 5;
+          break;
+        case FK_BONDED:
+          prof_begin(s, PMGPU_PHASE_BONDED);
+          r = bonded_forces(s, &f, em);
+          prof_end(s);
+          s->kernels += (f.bonds && s->n_bonds > 0) + (f.angles && s->n_angles > 0);
+          break;
+        case FK_TORSION:
+          prof_begin(s, PMGPU_PHASE_BONDED);
+          r = torsion_forces(s, &f, em);
+          prof_end(s);
+          s->kernels +=
+              (f.dihedrals && s->n_dihedrals > 0) + (f.impropers && s->n_impropers > 0);
+          break;
+        case FK_SIMPLEFULL:
+          // all enabled simple-full terms share one all-pairs pass
+          if (sf_done) break;
+          sf_done = 1;
+          prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
+          r = nb_simplefull(s, only >= 0 ? f.sf_lj : sf_lj, only >= 0 ? f.sf_coul : sf_coul,
+                            em);
+          prof_end(s);
+          s->kernels += 1;
+          break;
+        default:
+          break;
+      }
+      PM_CHECK(r);
+    }
+    s->stream = main_stream;
+    return PMGPU_OK;
+  };
+  PM_CHECK(run_terms(false));
+  // neighbour lists are prepared once per evaluation: the rebuild decision,
+  // the (conditional) sort and the per-step gather here, the (conditional)
+  // tile build after PME has been forked
   for (auto &f : s->forces) {
     if (only >= 0 ? f.id != only : !f.enabled) continue;
-    int r = PMGPU_OK;
-    switch (f.kind) {
-      case FK_PME:
-        if (f.ewald_flags & PMGPU_EWALD_RECIPROCAL) {
-          prof_begin(s, PMGPU_PHASE_PME);
-          r = pme_reciprocal(s, &f, em);
-          prof_end(s);
-          PM_CHECK(r);
-          s->kernels += 4;  // spread, fixed->float, convolve, gather (+ cuFFT)
-        }
-        if (f.ewald_flags & PMGPU_EWALD_CORRECTION) {
-          prof_begin(s, PMGPU_PHASE_CORRECTION);
-          r = ewald_correction(s, &f, em);
-          prof_end(s);
-          s->kernels += s->n_excl > 0;
-        }
-        break;
-      case FK_GB:
-        prof_begin(s, PMGPU_PHASE_GB);
-        r = gb_forces(s, &f);
-        prof_end(s);
-        s->kernels += 5;
-        break;
-      case FK_BONDED:
-        prof_begin(s, PMGPU_PHASE_BONDED);
-        r = bonded_forces(s, &f, em);
-        prof_end(s);
-        s->kernels += (f.bonds && s->n_bonds > 0) + (f.angles && s->n_angles > 0);
-        break;
-      case FK_TORSION:
-        prof_begin(s, PMGPU_PHASE_BONDED);
-        r = torsion_forces(s, &f, em);
-        prof_end(s);
-        s->kernels += (f.dihedrals && s->n_dihedrals > 0) + (f.impropers && s->n_impropers > 0);
-        break;
-      case FK_SIMPLEFULL:
-        // all enabled simple-full terms share one all-pairs pass
-        if (sf_done) break;
-        sf_done = 1;
-        prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
-        r = nb_simplefull(s, only >= 0 ? f.sf_lj : sf_lj, only >= 0 ? f.sf_coul : sf_coul, em);
-        prof_end(s);
-        s->kernels += 1;
-        break;
-      default:
-        break;
+    if (f.list_index >= 0 && !prepared[f.list_index]) {
+      prof_begin(s, PMGPU_PHASE_LIST);
+      int r = nb_prepare(s, &s->lists[f.list_index], 0);
+      prof_end(s);
+      PM_CHECK(r);
+      s->kernels += 6;  // check, bin, scan, scatter, sort, gather
+      prepared[f.list_index] = 1;
     }
-    PM_CHECK(r);
   }
-  s->stream = main_stream;
+  if (fork) {
+    PM_CUDA(cudaEventRecord(s->ev_fork2, main_stream));
+    PM_CUDA(cudaStreamWaitEvent(s->side, s->ev_fork2, 0));
+  }
+  PM_CHECK(run_terms(true));
+  for (size_t k = 0; k < prepared.size(); k++) {
+    if (!prepared[k]) continue;
+    prof_begin(s, PMGPU_PHASE_LIST);
+    int r = nb_build(s, &s->lists[k]);
+    prof_end(s);
+    PM_CHECK(r);
+    s->kernels += 2;  // cluster boxes, tiles
+  }
   for (auto &g : groups) {
     prof_begin(s, PMGPU_PHASE_PAIRS);
     int r = nb_pair_forces(s, &s->lists[g.list], g.terms, mode);
     prof_end(s);
     PM_CHECK(r);
-    s->kernels += 1;
+    s->kernels += 2;  // tiles, slot forces
   }
   return PMGPU_OK;
 }
@@ -549,6 +575,7 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   PM_CUDA(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, prio_high));
   PM_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
   PM_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+  PM_CUDA(cudaEventCreateWithFlags(&s->ev_fork2, cudaEventDisableTiming));
   size_t nn = std::max(1, n);
   PM_CHECK(upload(s.get(), &s->d_charge, t->charge, n));
   PM_CHECK(upload(s.get(), &s->d_mass, t->mass, n));
@@ -974,12 +1001,13 @@ int pmgpu_force_evaluate(pmgpu_system *h, int id, const double *pos, double *for
 // evaluation at the new positions.
 static int one_step(System *s, const pmgpu_integrator *it, int phase, int mode) {
   prof_begin(s, PMGPU_PHASE_INTEGRATE);
-  int ri = integrate_kick_drift(s, it, phase);
+  // the update launch also starts the evaluation (clears the accumulators)
+  int ri = integrate_kick_drift(s, it, phase, 1);
   prof_end(s);
   PM_CHECK(ri);
   // update (+ step counter for the Langevin noise)
   s->kernels += (s->n > 0) + (it->kind == PMGPU_INT_LANGEVIN_LEAPFROG);
-  PM_CHECK(begin_eval(s));
+  if (s->n == 0) PM_CHECK(begin_eval(s));
   return evaluate_forces(s, -1, mode);
 }
 
@@ -1011,7 +1039,8 @@ static int run_graph(System *s, const pmgpu_integrator *it, long g, int *used) {
     const long long per_launch = s->kernels - k0;
     s->kernels = k0;
     if (r != PMGPU_OK || ec != cudaSuccess || !graph ||
-        cudaGraphInstantiate(&sg.exec, graph, 0) != cudaSuccess) {
+        cudaGraphInstantiate(&sg.exec, graph, cudaGraphInstantiateFlagUseNodePriority) !=
+            cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
       cudaGetLastError();
       sg.exec = nullptr;
@@ -1211,9 +1240,9 @@ int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
     const double ns = n + 7 * ncol + 8, ncl = ns / 8;
     const double dens = V > 0 ? std::max(n / V, 0.12) : 0.15;
     const double r = reach + 5.0;
-    const double cap = 4.18879 * r * r * r * dens / 8.0 * 1.4 + 64;
-    b += ns * (16 + 16 + 32 + 4 + 4 + 8) + n * (4 + 4 + 4 + 24 + 24) + nkeys * 4 + ncol * 16 +
-         ncl * (16 * cap + 4);
+    const double cap = 4.18879 * r * r * r * dens / 8.0 / kRowParts * 1.6 + 64;
+    b += ns * (16 + 16 + 32 + 4 + 4 + 8 + 24) + n * (4 + 4 + 4 + 24 + 24) + nkeys * 4 + ncol * 16 +
+         ncl * kRowParts * (16 * cap + 4);
   }
   if (grid) {
     double G = (double)grid[0] * grid[1] * grid[2];
@@ -1278,13 +1307,13 @@ int pmgpu_force_stats(pmgpu_system *h, int id, pmgpu_stats *out) {
     PM_CUDA(cudaStreamSynchronize(s->stream));
     out->list_builds = rb[1];
     // list entries: tiles (8 x 4 atom pairs each) over all i clusters
-    std::vector<int> cnt(std::max(1, nl.nclusters));
-    if (nl.nclusters) {
-      PM_CUDA(cudaMemcpyAsync(cnt.data(), nl.d_tile_count, sizeof(int) * nl.nclusters,
+    std::vector<int> cnt(std::max(1, nl.nrows));
+    if (nl.nrows) {
+      PM_CUDA(cudaMemcpyAsync(cnt.data(), nl.d_tile_count, sizeof(int) * nl.nrows,
                               cudaMemcpyDeviceToHost, s->stream));
       PM_CUDA(cudaStreamSynchronize(s->stream));
       long long tot = 0;
-      for (int k = 0; k < nl.nclusters; k++) tot += cnt[k];
+      for (int k = 0; k < nl.nrows; k++) tot += cnt[k];
       out->list_entries = tot;
     }
   }
@@ -1320,6 +1349,7 @@ int pmgpu_debug_pair_set(pmgpu_system *h, int id, int *pairs, long long cap,
   PM_CHECK(zero_forces(s));
   PM_CHECK(begin_eval(s));
   PM_CHECK(nb_prepare(s, &s->lists[f.list_index], 0));
+  PM_CHECK(nb_build(s, &s->lists[f.list_index]));
   PM_CHECK(nb_pair_forces(s, &s->lists[f.list_index], f.terms, PAIR_RECORD));
   long long total = 0;
   PM_CUDA(cudaMemcpyAsync(&total, s->d_paircount, sizeof(long long), cudaMemcpyDeviceToHost,

@@ -329,6 +329,7 @@ struct UpdateArgs {
   const unsigned long long *step_ptr;
   int kstep_off[2];
   int khalf[2];
+  long long *acc_zero;  // energy accumulators cleared by this launch (or null)
 };
 
 // Advances the device step counter (after the drift of a step).
@@ -345,6 +346,7 @@ __global__ void k_update(UpdateArgs a, const double *__restrict__ mass,
                          double *__restrict__ pos, double *__restrict__ vel,
                          long long *__restrict__ force, int *__restrict__ status) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a.acc_zero && i < ACC_COUNT) a.acc_zero[i] = 0;
   if (i >= a.n) return;
   double F[3];
   for (int c = 0; c < 3; c++) F[c] = (double)force[c * a.n + i] * (1.0 / kForceScale);
@@ -378,7 +380,7 @@ __global__ void k_update(UpdateArgs a, const double *__restrict__ mass,
 // drift), 2 = leapfrog last (half kick), 3 = Langevin half kick + drift,
 // 4 = Langevin two half kicks (end of step s, start of step s+1) + drift,
 // 5 = Langevin closing half kick.
-int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase) {
+int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int zero_acc) {
   UpdateArgs a;
   a.n = s->n;
   a.h = it->timestep_fs * kInvTimeFactor;
@@ -387,6 +389,7 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase) {
   // StandardIntegrator::run gives every step two half kicks; the noise of
   // kick (step, half) is Philox(seed; atom, step, half).
   a.step_ptr = s->d_step;
+  a.acc_zero = zero_acc ? s->d_acc : nullptr;
   a.kstep_off[0] = 0; a.khalf[0] = 0;
   a.kstep_off[1] = 0; a.khalf[1] = 0;
   a.vdt = a.fdt = a.ndt = a.fc = 0;

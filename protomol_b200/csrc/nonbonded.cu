@@ -241,56 +241,75 @@ k_sort_cols(const int *__restrict__ rebuild, int nzb, float inv_z,
 template <bool MIXED>
 __global__ void k_gather(int ns, const double *__restrict__ pos,
                          const double *__restrict__ offset,
-                         const double *__restrict__ xbuild,
                          const int *__restrict__ sorted,
                          const double *__restrict__ charge,
                          const int *__restrict__ type, const int *__restrict__ mol,
                          float4 *__restrict__ xhi, float4 *__restrict__ xlo,
-                         double4 *__restrict__ xw, int *__restrict__ mol_s,
-                         unsigned int *__restrict__ maxdisp) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  float d2 = 0.f;
-  if (s < ns) {
-    const int i = sorted[s];
-    if (i < 0) {
-      const double far = 1.0e5 + 16.0 * s;
-      xw[s] = make_double4(far, 1.0e5, 1.0e5, 0.0);
-      xhi[s] = make_float4((float)far, 1.0e5f, 1.0e5f, 0.f);
-      if (MIXED) xlo[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
-      mol_s[s] = -1;
-    } else {
-      double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-      double wx = x - offset[3 * i], wy = y - offset[3 * i + 1], wz = z - offset[3 * i + 2];
-      double q = charge[i];
-      xw[s] = make_double4(wx, wy, wz, q);
-      float hx = (float)wx, hy = (float)wy, hz = (float)wz;
-      xhi[s] = make_float4(hx, hy, hz, (float)q);
-      if (MIXED)
-        xlo[s] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
-                             (float)(wz - (double)hz), __int_as_float(type[i]));
-      mol_s[s] = mol[i];
-      double dx = x - xbuild[3 * i], dy = y - xbuild[3 * i + 1], dz = z - xbuild[3 * i + 2];
-      d2 = (float)(dx * dx + dy * dy + dz * dz);
-      if (!(d2 == d2)) d2 = 3.0e38f;  // NaN forces a rebuild / status check
-    }
+                         double4 *__restrict__ xw, int *__restrict__ mol_s) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const int i = sorted[s];
+  if (i < 0) {
+    const double far = 1.0e5 + 16.0 * s;
+    xw[s] = make_double4(far, 1.0e5, 1.0e5, 0.0);
+    xhi[s] = make_float4((float)far, 1.0e5f, 1.0e5f, 0.f);
+    if (MIXED) xlo[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+    mol_s[s] = -1;
+    return;
   }
-  float m = d2;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(maxdisp, __float_as_uint(m));
+  const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+  const double wx = x - offset[3 * i], wy = y - offset[3 * i + 1], wz = z - offset[3 * i + 2];
+  const double q = charge[i];
+  xw[s] = make_double4(wx, wy, wz, q);
+  const float hx = (float)wx, hy = (float)wy, hz = (float)wz;
+  xhi[s] = make_float4(hx, hy, hz, (float)q);
+  if (MIXED)
+    xlo[s] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
+                         (float)(wz - (double)hz), __int_as_float(type[i]));
+  mol_s[s] = mol[i];
 }
 
-// Decide whether this step rebuilds the list: first build, forced, or an
-// atom moved more than half the skin since the last build.
-// rebuild[0] is the flag, rebuild[1] counts builds.
-__global__ void k_check_rebuild(unsigned int *maxdisp, int *rebuild, float half_skin2,
-                                int force) {
-  float m = __uint_as_float(*maxdisp);
-  int r = force || (m > half_skin2);
-  rebuild[0] = r;
-  if (r) {
-    *maxdisp = 0u;
-    rebuild[1] += 1;
+// Decides whether this evaluation rebuilds the list: first build, forced,
+// or an atom of the current positions lies more than half the skin from
+// its position at the last build (so no pair can have come from beyond the
+// reach to within the cutoff).  Every block reduces its atoms' largest
+// displacement; the last block to finish takes the decision.
+// rebuild[0] is the flag, rebuild[1] counts builds; ticket[0] orders the
+// blocks, ticket[1] holds the running maximum (FP32 bits).
+constexpr int kCheckThreads = 256;
+__global__ void __launch_bounds__(kCheckThreads)
+k_check_rebuild(int n, const double *__restrict__ pos, const double *__restrict__ xbuild,
+                unsigned *__restrict__ ticket, int *__restrict__ rebuild, float half_skin2,
+                int force) {
+  __shared__ float wmax[kCheckThreads / 32];
+  __shared__ bool last;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float d2 = 0.f;
+  if (i < n && !force) {
+    const double dx = pos[3 * i] - xbuild[3 * i], dy = pos[3 * i + 1] - xbuild[3 * i + 1],
+                 dz = pos[3 * i + 2] - xbuild[3 * i + 2];
+    d2 = (float)(dx * dx + dy * dy + dz * dz);
+    if (!(d2 == d2)) d2 = 3.0e38f;  // NaN: rebuild (the binning flags it)
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = wmax[0];
+    for (int w = 1; w < kCheckThreads / 32; w++) m = fmaxf(m, wmax[w]);
+    if (m > 0.f) atomicMax(&ticket[1], __float_as_uint(m));
+    __threadfence();
+    last = atomicAdd(&ticket[0], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    const float m = __uint_as_float(atomicExch(&ticket[1], 0u));
+    const int r = force || m > half_skin2;
+    rebuild[0] = r;
+    if (r) rebuild[1] += 1;
+    ticket[0] = 0u;
   }
 }
 
@@ -320,7 +339,7 @@ __global__ void k_bbox(const int *__restrict__ rebuild, int nhalf,
 
 // ---------------------------------------------------------- list build
 struct TileBuildArgs {
-  int nclusters;
+  int nclusters;     // 8-atom i clusters (kRowParts tile rows each)
   int periodic;
   int ncx, ncy, nzb;
   float lo[3];       // grid corner in the wrapped frame
@@ -347,32 +366,41 @@ __device__ __forceinline__ int floor_div(int a, int b) {
   return a >= 0 ? a / b : -((-a + b - 1) / b);
 }
 
-// One warp per 8-atom i cluster.  Candidate 4-atom j clusters come from the
-// columns (and periodic images) whose box lies within the reach of the i
-// cluster's box, taking the z slice within the reach; a candidate is kept
-// if its box (in that image) lies within the reach.  Each unordered pair
-// is listed once: j clusters of a later i cluster are taken in every
-// image, those of the same i cluster in the zero image (pairs with the i
-// atom before the j atom) and in one half of the other images.  The 32
-// lanes then test the tile's 8 x 4 atom pairs at once: pairs beyond the
-// reach or with padding are masked off, and ExclusionTable::check
-// (topology/ExclusionTable.h:116-130; consulted for same-molecule
-// minimal-image pairs as in OneAtomPairTwo.h:47-53) clears fully excluded
-// pairs and marks modified ones.  Tiles are appended in a fixed order
-// (column image, z slice, cluster index), so the list is deterministic.
-__global__ void __launch_bounds__(kBuildWarps * 32)
+// One warp per (8-atom i cluster, row part).  The search window of the
+// i cluster is the set of (column, periodic image, z slice) ranges whose
+// box lies within the culling radius of the i cluster's box; the 32 lanes
+// form 32 of those ranges at a time, and the non-empty ones are dealt
+// round-robin over the kRowParts warps of the cluster.  In a range, a
+// 4-atom j cluster is a candidate if its box (in that image) lies within
+// the radius.  Each unordered pair is listed once: j clusters of a later i
+// cluster are taken in every image, those of the same i cluster in the
+// zero image (pairs with the i atom before the j atom) and in one half of
+// the other images.  Candidates are tested four at a time: lane
+// (i atom l & 7, candidate l >> 3) tests its i atom against the
+// candidate's 4 j atoms, pairs beyond the reach or with padding are masked
+// off, and ExclusionTable::check (topology/ExclusionTable.h:116-130;
+// consulted for same-molecule minimal-image pairs as in
+// OneAtomPairTwo.h:47-53) clears fully excluded pairs and marks modified
+// ones.  Tiles are appended in a fixed order (range, cluster index), so
+// the list is deterministic.
+__global__ void __launch_bounds__(kBuildWarps * 32, 3)
 k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__restrict__ sorted,
               const int *__restrict__ start, const float4 *__restrict__ xhi,
               const int *__restrict__ mol_s, const float4 *__restrict__ bb,
               uint4 *__restrict__ tiles, int *__restrict__ tile_count,
               int *__restrict__ status) {
   if (!*rebuild) return;
-  const int lane = threadIdx.x & 31;
-  const int ci = blockIdx.x * kBuildWarps + (threadIdx.x >> 5);
+  constexpr unsigned kAll = 0xffffffffu;
+  // this warp's staging of candidate j clusters (up to 32 of them)
+  __shared__ float4 st_x[kBuildWarps][128];
+  __shared__ int4 st_o[kBuildWarps][32], st_m[kBuildWarps][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int rw = blockIdx.x * kBuildWarps + wib;
+  const int ci = rw / kRowParts, part = rw - ci * kRowParts;
   if (ci >= a.nclusters) return;  // whole warps exit together
   const float4 l0 = bb[4 * ci], h0 = bb[4 * ci + 1], l1 = bb[4 * ci + 2], h1 = bb[4 * ci + 3];
   if (l0.w + l1.w == 0.f) {
-    if (lane == 0) tile_count[ci] = 0;
+    if (lane == 0) tile_count[rw] = 0;
     return;
   }
   float ilo[3] = {fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z)};
@@ -388,37 +416,38 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
   }
   if (!sane) {
     if (lane == 0) {
-      tile_count[ci] = 0;
+      tile_count[rw] = 0;
       atomicOr(status, ST_NONFINITE);
     }
     return;
   }
-  const int islot = 8 * ci + (lane & 7);
-  const int jl = lane >> 3;
+  const int il = lane & 7, cq = lane >> 3;
+  const int islot = 8 * ci + il;
   const int oi = sorted[islot];
+  const bool ilive = oi >= 0;
   const float4 pi = xhi[islot];
   const int mi = mol_s[islot];
   const float R = a.cull, R2 = a.cull * a.cull;
-  uint4 *row = tiles + (size_t)ci * a.cap;
+  uint4 *row = tiles + (size_t)rw * a.cap;
   int count = 0;
 
-  // the j clusters of slots [s0, s1) seen under image (sx, sy, sz)
-  auto scan = [&](int s0, int s1, int sx, int sy, int sz) {
-    if (s1 <= s0) return;
-    const int code = shift_code(sx, sy, sz);
+  // the j clusters of slots [s0, s1) seen under image code
+  auto scan = [&](int s0, int s1, int code) {
+    const int sx = (code & 3) - 1, sy = ((code >> 2) & 3) - 1, sz = ((code >> 4) & 3) - 1;
+    const bool zero = code == kZeroShift;
     const float S[3] = {sx * a.L[0], sy * a.L[1], sz * a.L[2]};
     const int hb = s0 >> 2, he = (s1 - 1) >> 2;
-    for (int h0 = hb; h0 <= he; h0 += 32) {
-      const int h = h0 + lane;
+    for (int hb0 = hb; hb0 <= he; hb0 += 32) {
+      const int h = hb0 + lane;
       bool cand = false;
       if (h <= he) {
         const int parent = h >> 1;
         cand = parent > ci || (parent == ci && code >= kZeroShift);
         if (cand) {
           const float4 jl4 = bb[2 * h], jh4 = bb[2 * h + 1];
+          float g2 = 0.f;
           const float jlo[3] = {jl4.x + S[0], jl4.y + S[1], jl4.z + S[2]};
           const float jhi[3] = {jh4.x + S[0], jh4.y + S[1], jh4.z + S[2]};
-          float g2 = 0.f;
 #pragma unroll
           for (int c = 0; c < 3; c++) {
             const float g = fmaxf(fmaxf(jlo[c] - ihi[c], ilo[c] - jhi[c]), 0.f);
@@ -427,49 +456,96 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
           cand = jl4.w > 0.f && g2 <= R2;
         }
       }
-      unsigned cm = __ballot_sync(0xffffffffu, cand);
-      // the 8 x 4 atom pairs of a candidate tile (ci, hj) in this image
-      auto test = [&](int hj, int jslot, int oj, float4 pj, int mj) {
-        const float dx = pj.x + S[0] - pi.x, dy = pj.y + S[1] - pi.y, dz = pj.z + S[2] - pi.z;
-        bool pass = oi >= 0 && oj >= 0 && dx * dx + dy * dy + dz * dz < a.reach2;
-        if ((hj >> 1) == ci && code == kZeroShift) pass = pass && islot < jslot;
-        bool mod = false;
-        if (pass && mj == mi) {
-          const bool minimal = !a.periodic || (fabsf(dx) <= a.H2[0] &&
-                                               fabsf(dy) <= a.H2[1] && fabsf(dz) <= a.H2[2]);
-          if (minimal) {
-            const int cls = excl_class_of(a.excl_start, a.excl_partner, a.excl_class, oi, oj);
-            if (cls == PMGPU_EXCL_FULL) pass = false;
-            else if (cls == PMGPU_EXCL_MODIFIED) mod = true;
+      unsigned cm = __ballot_sync(kAll, cand);
+      if (!cm) continue;
+      // every candidate's lane stages its 4 atoms for the tests below
+      if (cand) {
+        const float4 *xs = xhi + 4 * h;
+        st_x[wib][4 * lane] = xs[0];
+        st_x[wib][4 * lane + 1] = xs[1];
+        st_x[wib][4 * lane + 2] = xs[2];
+        st_x[wib][4 * lane + 3] = xs[3];
+        st_o[wib][lane] = *reinterpret_cast<const int4 *>(sorted + 4 * h);
+        st_m[wib][lane] = *reinterpret_cast<const int4 *>(mol_s + 4 * h);
+      }
+      __syncwarp();
+      while (cm) {
+        // the next (up to) four candidates, in ascending order
+        int bq[4];
+        int ng = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          bq[q] = cm ? __ffs(cm) - 1 : 0;
+          if (cm) {
+            cm &= cm - 1;
+            ng = q + 1;
           }
         }
-        const unsigned im = __ballot_sync(0xffffffffu, pass);
-        const unsigned mm = __ballot_sync(0xffffffffu, mod);
-        if (im) {
-          if (lane == 0 && count < a.cap)
-            row[count] = make_uint4((uint32_t)hj | ((uint32_t)code << kShiftBits), im, mm, 0u);
-          count++;
+        const int myb = cq == 0 ? bq[0] : (cq == 1 ? bq[1] : (cq == 2 ? bq[2] : bq[3]));
+        const bool cval = cq < ng;
+        const int hj = hb0 + myb;
+        const bool diag = zero && (hj >> 1) == ci;
+        const int4 o4 = st_o[wib][myb], m4 = st_m[wib][myb];
+        const int oj[4] = {o4.x, o4.y, o4.z, o4.w};
+        const int mj[4] = {m4.x, m4.y, m4.z, m4.w};
+        bool pass[4], same = false;
+        float dd[4][3];
+#pragma unroll
+        for (int jl = 0; jl < 4; jl++) {
+          const float4 pj = st_x[wib][4 * myb + jl];
+          dd[jl][0] = pj.x + S[0] - pi.x;
+          dd[jl][1] = pj.y + S[1] - pi.y;
+          dd[jl][2] = pj.z + S[2] - pi.z;
+          const float r2 = dd[jl][0] * dd[jl][0] + dd[jl][1] * dd[jl][1] + dd[jl][2] * dd[jl][2];
+          pass[jl] = cval && ilive && oj[jl] >= 0 && r2 < a.reach2 &&
+                     (!diag || islot < 4 * hj + jl);
+          same = same || (pass[jl] && mj[jl] == mi);
         }
-      };
-      // two candidates per round: both tiles' loads are in flight together
-      while (cm) {
-        const int bA = __ffs(cm) - 1;
-        cm &= cm - 1;
-        const int bB = cm ? __ffs(cm) - 1 : bA;
-        const bool two = cm != 0;
-        if (two) cm &= cm - 1;
-        const int hA = h0 + bA, hB = h0 + bB;
-        const int jA = 4 * hA + jl, jB = 4 * hB + jl;
-        const int oA = sorted[jA], oB = sorted[jB];
-        const float4 pA = xhi[jA], pB = xhi[jB];
-        const int mA = mol_s[jA], mB = mol_s[jB];
-        test(hA, jA, oA, pA, mA);
-        if (two) test(hB, jB, oB, pB, mB);
+        unsigned mb[4] = {0u, 0u, 0u, 0u};
+        // same-molecule pairs (few tiles): ExclusionTable lookup
+        if (__any_sync(kAll, same)) {
+#pragma unroll
+          for (int jl = 0; jl < 4; jl++) {
+            bool mod = false;
+            if (pass[jl] && mj[jl] == mi) {
+              const bool minimal = !a.periodic || (fabsf(dd[jl][0]) <= a.H2[0] &&
+                                                   fabsf(dd[jl][1]) <= a.H2[1] &&
+                                                   fabsf(dd[jl][2]) <= a.H2[2]);
+              if (minimal) {
+                const int cls =
+                    excl_class_of(a.excl_start, a.excl_partner, a.excl_class, oi, oj[jl]);
+                if (cls == PMGPU_EXCL_FULL) pass[jl] = false;
+                else if (cls == PMGPU_EXCL_MODIFIED) mod = true;
+              }
+            }
+            mb[jl] = __ballot_sync(kAll, mod);
+          }
+        }
+        unsigned pb[4];
+#pragma unroll
+        for (int jl = 0; jl < 4; jl++) pb[jl] = __ballot_sync(kAll, pass[jl]);
+        // lane q < 4 assembles candidate q's masks (bit il + 8 jl)
+        const int q = lane & 3, sh = 8 * q;
+        const unsigned im = ((pb[0] >> sh) & 0xFFu) | (((pb[1] >> sh) & 0xFFu) << 8) |
+                            (((pb[2] >> sh) & 0xFFu) << 16) | (((pb[3] >> sh) & 0xFFu) << 24);
+        const unsigned mm = ((mb[0] >> sh) & 0xFFu) | (((mb[1] >> sh) & 0xFFu) << 8) |
+                            (((mb[2] >> sh) & 0xFFu) << 16) | (((mb[3] >> sh) & 0xFFu) << 24);
+        const bool wr = lane < ng && im != 0u;
+        const unsigned wm = __ballot_sync(kAll, wr);
+        if (wr) {
+          const int idx = count + __popc(wm & ((1u << lane) - 1u));
+          const int bsel = q == 0 ? bq[0] : (q == 1 ? bq[1] : (q == 2 ? bq[2] : bq[3]));
+          if (idx < a.cap)
+            row[idx] = make_uint4((uint32_t)(hb0 + bsel) | ((uint32_t)code << kShiftBits), im,
+                                  mm, 0u);
+        }
+        count += __popc(wm);
       }
+      __syncwarp();  // the next batch overwrites the staging
     }
   };
-  auto slots = [&](int col, int b0, int b1) {  // z bins b0..b1 of a column
-    return make_int2(start[col * a.nzb + b0], start[col * a.nzb + b1 + 1]);
+  auto slots = [&](int col, int z0, int z1) {  // z bins z0..z1 of a column
+    return make_int2(start[col * a.nzb + z0], start[col * a.nzb + z1 + 1]);
   };
 
   const int ux0 = (int)floorf((ilo[0] - R - a.lo[0]) / a.cs[0]);
@@ -478,37 +554,56 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
   const int uy1 = (int)floorf((ihi[1] + R - a.lo[1]) / a.cs[1]);
   const int b0 = (int)floorf((ilo[2] - R - a.lo[2]) / a.cs[2]);
   const int b1 = (int)floorf((ihi[2] + R - a.lo[2]) / a.cs[2]);
-  if (!a.periodic) {
-    // vacuum: atoms outside the grid sit in its edge columns and bins;
-    // clamping the window the same way keeps every atom within the reach
-    for (int cx = clampi(ux0, 0, a.ncx - 1); cx <= clampi(ux1, 0, a.ncx - 1); cx++)
-      for (int cy = clampi(uy0, 0, a.ncy - 1); cy <= clampi(uy1, 0, a.ncy - 1); cy++) {
-        const int2 r = slots(cx * a.ncy + cy, clampi(b0, 0, a.nzb - 1),
-                             clampi(b1, 0, a.nzb - 1));
-        scan(r.x, r.y, 0, 0, 0);
-      }
-  } else {
-    // the box edge exceeds the culling radius, so the window spans images
-    // -1, 0, 1 only
-    for (int ux = ux0; ux <= ux1; ux++) {
-      const int sx = floor_div(ux, a.ncx), cx = ux - sx * a.ncx;
-      const float clx = a.lo[0] + ux * a.cs[0];
-      const float gx = fmaxf(fmaxf(clx - ihi[0], ilo[0] - (clx + a.cs[0])), 0.f);
-      for (int uy = uy0; uy <= uy1; uy++) {
+  // periodic: the box edge exceeds the culling radius, so the window spans
+  // images -1, 0, 1 only; vacuum: atoms outside the grid sit in its edge
+  // columns and bins, and clamping the window the same way keeps every
+  // atom within the reach
+  const int vx0 = a.periodic ? ux0 : clampi(ux0, 0, a.ncx - 1);
+  const int vy0 = a.periodic ? uy0 : clampi(uy0, 0, a.ncy - 1);
+  const int nux = (a.periodic ? ux1 : clampi(ux1, 0, a.ncx - 1)) - vx0 + 1;
+  const int nuy = (a.periodic ? uy1 : clampi(uy1, 0, a.ncy - 1)) - vy0 + 1;
+  const int nsz = a.periodic ? 3 : 1;
+  const int total = nux * nuy * nsz;
+  const int half0 = 8 * ci;  // j clusters of earlier i clusters are never taken
+  int deal = 0;
+  for (int k0 = 0; k0 < total; k0 += 32) {
+    const int k = k0 + lane;
+    int rs = 0, re = 0, code = kZeroShift;
+    if (k < total) {
+      const int iz = k % nsz, t = k / nsz;
+      const int iy = t % nuy, ix = t / nuy;
+      if (a.periodic) {
+        const int ux = vx0 + ix, uy = vy0 + iy, sz = iz - 1;
+        const int sx = floor_div(ux, a.ncx), cx = ux - sx * a.ncx;
         const int sy = floor_div(uy, a.ncy), cy = uy - sy * a.ncy;
-        const float cly = a.lo[1] + uy * a.cs[1];
+        const float clx = a.lo[0] + ux * a.cs[0], cly = a.lo[1] + uy * a.cs[1];
+        const float gx = fmaxf(fmaxf(clx - ihi[0], ilo[0] - (clx + a.cs[0])), 0.f);
         const float gy = fmaxf(fmaxf(cly - ihi[1], ilo[1] - (cly + a.cs[1])), 0.f);
-        if (gx * gx + gy * gy > R2) continue;
-        const int col = cx * a.ncy + cy;
-        // z bins of the window in images sz = -1, 0, 1 (bin b of image sz
-        // lies at unwrapped bin b + sz * nzb)
-        for (int sz = -1; sz <= 1; sz++) {
-          const int lo = max(b0 - sz * a.nzb, 0), hi = min(b1 - sz * a.nzb, a.nzb - 1);
-          if (lo > hi) continue;
-          const int2 r = slots(col, lo, hi);
-          scan(r.x, r.y, sx, sy, sz);
+        // z bins of the window in image sz (bin z of image sz lies at
+        // unwrapped bin z + sz * nzb)
+        const int zlo = max(b0 - sz * a.nzb, 0), zhi = min(b1 - sz * a.nzb, a.nzb - 1);
+        if (gx * gx + gy * gy <= R2 && zlo <= zhi) {
+          const int2 r = slots(cx * a.ncy + cy, zlo, zhi);
+          rs = r.x;
+          re = r.y;
+          code = shift_code(sx, sy, sz);
         }
+      } else {
+        const int2 r = slots((vx0 + ix) * a.ncy + (vy0 + iy), clampi(b0, 0, a.nzb - 1),
+                             clampi(b1, 0, a.nzb - 1));
+        rs = r.x;
+        re = r.y;
       }
+      rs = max(rs, half0);
+    }
+    unsigned live = __ballot_sync(kAll, re > rs);
+    while (live) {
+      const int b = __ffs(live) - 1;
+      live &= live - 1;
+      if (deal++ % kRowParts != part) continue;
+      const int s0 = __shfl_sync(kAll, rs, b), s1 = __shfl_sync(kAll, re, b);
+      const int cd = __shfl_sync(kAll, code, b);
+      scan(s0, s1, cd);
     }
   }
   if (lane == 0) {
@@ -516,7 +611,7 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
       atomicOr(status, ST_LIST_OVERFLOW);
       count = a.cap;
     }
-    tile_count[ci] = count;
+    tile_count[rw] = count;
   }
 }
 
@@ -577,6 +672,7 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   // slots: every column padded to whole 8-atom clusters
   nl->ns_max = ((n + 7 * nl->ncol) + 7) & ~7;
   nl->nclusters = nl->ns_max / 8;
+  nl->nrows = nl->nclusters * kRowParts;
   // capacity: j clusters within (reach + cluster extent) of an i cluster at
   // the mean density (condensed matter bounds the local density even in
   // sparse boxes), half of them by the one-tile-per-pair rule, with
@@ -584,7 +680,7 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   const double dens = b.periodic ? std::max(n / b.V, 0.12) : 0.15;
   const double r = nl->reach + 5.0;
   const double expect = 4.18879 * r * r * r * dens / 4.0 / 2.0;
-  int cap = (int)(expect * 1.4 + 32);
+  int cap = (int)(expect / kRowParts * 1.6 + 32);
   cap = std::min(cap, std::max(32, nl->ns_max / 4 * 27));
   cap = (cap + 31) & ~31;
   if (nl->cap > cap) cap = nl->cap;
@@ -608,12 +704,14 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   PM_CHECK(dev_alloc(s, &nl->d_xw, sizeof(double4) * ns));
   PM_CHECK(dev_alloc(s, &nl->d_mol_s, sizeof(int) * ns));
   PM_CHECK(dev_alloc(s, &nl->d_bb, sizeof(float4) * 2 * (ns / 4)));
-  PM_CHECK(dev_alloc(s, &nl->d_tiles, sizeof(uint4) * (size_t)cap * nl->nclusters));
-  PM_CHECK(dev_alloc(s, &nl->d_tile_count, sizeof(int) * std::max(1, nl->nclusters)));
-  PM_CUDA(cudaMemsetAsync(nl->d_tile_count, 0, sizeof(int) * std::max(1, nl->nclusters),
+  PM_CHECK(dev_alloc(s, &nl->d_fslot, sizeof(long long) * 3 * ns));
+  PM_CUDA(cudaMemsetAsync(nl->d_fslot, 0, sizeof(long long) * 3 * ns, s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_tiles, sizeof(uint4) * (size_t)cap * nl->nrows));
+  PM_CHECK(dev_alloc(s, &nl->d_tile_count, sizeof(int) * std::max(1, nl->nrows)));
+  PM_CUDA(cudaMemsetAsync(nl->d_tile_count, 0, sizeof(int) * std::max(1, nl->nrows),
                           s->stream));
-  PM_CHECK(dev_alloc(s, &nl->d_maxdisp, sizeof(unsigned int)));
-  PM_CUDA(cudaMemsetAsync(nl->d_maxdisp, 0, sizeof(unsigned int), s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_maxdisp, 2 * sizeof(unsigned int)));
+  PM_CUDA(cudaMemsetAsync(nl->d_maxdisp, 0, 2 * sizeof(unsigned int), s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_rebuild, 2 * sizeof(int)));
   PM_CUDA(cudaMemsetAsync(nl->d_rebuild, 0, 2 * sizeof(int), s->stream));
   nl->built = 0;
@@ -624,7 +722,8 @@ int nb_list_free(System *s, NeighborList *nl) {
   void *ptrs[] = {nl->d_key, nl->d_zkey, nl->d_unsorted, nl->d_col_count, nl->d_col_u,
                   nl->d_col_cursor, nl->d_col_base, nl->d_key_start, nl->d_sorted,
                   nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
-                  nl->d_bb, nl->d_tiles, nl->d_tile_count, nl->d_maxdisp, nl->d_rebuild};
+                  nl->d_bb, nl->d_fslot, nl->d_tiles, nl->d_tile_count, nl->d_maxdisp,
+                  nl->d_rebuild};
   for (void *p : ptrs) dev_free(s, p);
   nl->d_key = nl->d_unsorted = nl->d_col_count = nl->d_col_u = nl->d_col_cursor = nullptr;
   nl->d_col_base = nl->d_key_start = nl->d_sorted = nl->d_mol_s = nl->d_tile_count = nullptr;
@@ -634,6 +733,7 @@ int nb_list_free(System *s, NeighborList *nl) {
   nl->d_xhi = nl->d_xlo = nl->d_bb = nullptr;
   nl->d_xw = nullptr;
   nl->d_tiles = nullptr;
+  nl->d_fslot = nullptr;
   nl->d_maxdisp = nullptr;
   return PMGPU_OK;
 }
@@ -648,8 +748,9 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
   const int nb = (n + T - 1) / T, nbs = (nl->ns_max + T - 1) / T;
   const int first = !nl->built;
   const float hs = (float)(0.5 * nl->skin);
-  k_check_rebuild<<<1, 1, 0, st>>>(nl->d_maxdisp, nl->d_rebuild, hs * hs,
-                                   (force_rebuild || first) ? 1 : 0);
+  k_check_rebuild<<<nb, kCheckThreads, 0, st>>>(n, s->d_pos, nl->d_xbuild, nl->d_maxdisp,
+                                               nl->d_rebuild, hs * hs,
+                                               (force_rebuild || first) ? 1 : 0);
   ListGrid g;
   g.box = s->box;
   g.n = n;
@@ -670,15 +771,23 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
       nl->d_rebuild, nl->nzb, (float)(1.0 / nl->cs[2]), nl->d_col_count, nl->d_col_u,
       nl->d_col_base, nl->d_unsorted, nl->d_zkey, nl->d_sorted, nl->d_key_start, s->d_status);
   if (s->precision == PMGPU_PREC_MIXED)
-    k_gather<true><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_xbuild,
-                                      nl->d_sorted, s->d_charge, s->d_type, s->d_mol,
-                                      nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
-                                      nl->d_maxdisp);
+    k_gather<true><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted,
+                                      s->d_charge, s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo,
+                                      nl->d_xw, nl->d_mol_s);
   else
-    k_gather<false><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_xbuild,
-                                       nl->d_sorted, s->d_charge, s->d_type, s->d_mol,
-                                       nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
-                                       nl->d_maxdisp);
+    k_gather<false><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted,
+                                       s->d_charge, s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo,
+                                       nl->d_xw, nl->d_mol_s);
+  PM_CUDA(cudaGetLastError());
+  nl->built = 1;  // the slot order exists from here on
+  return PMGPU_OK;
+}
+
+// The (conditional) tile build of a prepared list: cluster boxes and tiles.
+int nb_build(System *s, NeighborList *nl) {
+  if (s->n == 0) return PMGPU_OK;
+  cudaStream_t st = s->stream;
+  const int T = 256;
   const int nhalf = nl->ns_max / 4;
   k_bbox<<<(nhalf + T - 1) / T, T, 0, st>>>(nl->d_rebuild, nhalf, nl->d_sorted, nl->d_xhi,
                                            nl->d_bb);
@@ -701,11 +810,10 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
   ba.excl_start = s->d_excl_start;
   ba.excl_partner = s->d_excl_partner;
   ba.excl_class = s->d_excl_class;
-  k_build_tiles<<<(nl->nclusters + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, st>>>(
+  k_build_tiles<<<(nl->nrows + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, st>>>(
       ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s, nl->d_bb,
       nl->d_tiles, nl->d_tile_count, s->d_status);
   PM_CUDA(cudaGetLastError());
-  nl->built = 1;
   return PMGPU_OK;
 }
 
@@ -772,7 +880,8 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   a.type = s->d_type;
   a.lj32 = s->d_lj32;
   a.lj64 = s->d_lj64;
-  a.force = s->d_force;
+  a.fslot = nl->d_fslot;
+  a.ns = nl->ns_max;
   a.acc = s->d_acc;
   a.pairbuf = s->d_pairbuf;
   a.pairbuf_cap = s->pairbuf_cap;
@@ -788,9 +897,9 @@ static int spec_kind(const SwitchParams &sw) {
   return -2;
 }
 
-// Warps per i cluster row of the tile kernel: about four waves of the
+// Warps per i cluster of the tile kernel: about four waves of the
 // force-only kernel's resident warps (five blocks of kPairWarps per SM),
-// at most 8 per row, so blocks that finish early are refilled and the
+// at most 8 per cluster, so blocks that finish early are refilled and the
 // tail stays short.  The split depends only on the system, so every launch
 // of a system sums its forces in the same order.
 static int pair_splits(int nclusters) {
@@ -868,11 +977,16 @@ int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode) {
   if (s->precision == PMGPU_PREC_MIXED) {
     PairArgs<float> a;
     fill_pair_args<float>(a, s, nl, t);
-    return launch_pairs<float>(a, s->stream, mode, t);
+    PM_CHECK(launch_pairs<float>(a, s->stream, mode, t));
+  } else {
+    PairArgs<double> a;
+    fill_pair_args<double>(a, s, nl, t);
+    PM_CHECK(launch_pairs<double>(a, s->stream, mode, t));
   }
-  PairArgs<double> a;
-  fill_pair_args<double>(a, s, nl, t);
-  return launch_pairs<double>(a, s->stream, mode, t);
+  k_slot_forces<<<(nl->ns_max + 255) / 256, 256, 0, s->stream>>>(nl->ns_max, s->n, nl->d_sorted,
+                                                                nl->d_fslot, s->d_force);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
 }
 
 // ProtoMol cell assignment with a given cellsize on the resident positions

@@ -43,9 +43,9 @@ struct PairArgs {
   int exact_erf;
   Real csf;  // coulomb scaling factor
   double csf64;
-  int cap;              // tiles per i cluster row
-  int nclusters;        // 8-atom i clusters
-  int splits;           // warps per i cluster row
+  int cap;              // tiles per row
+  int nclusters;        // 8-atom i clusters (kRowParts tile rows each)
+  int splits;           // warps per i cluster
   const int *sorted;
   const double *pos;     // raw positions (exact re-test)
   const int *excl_start, *excl_partner, *excl_class;
@@ -56,7 +56,9 @@ struct PairArgs {
   const int *type;
   const float4 *lj32;
   const double4 *lj64;
-  long long *force;      // 3 planes
+  long long *fslot;      // 3 planes of ns: forces by list slot (added to the
+                         // atoms' forces by k_slot_forces)
+  int ns;                // slots (plane stride of fslot)
   long long *acc;
   long long *pairbuf;
   long long pairbuf_cap;
@@ -368,7 +370,7 @@ __device__ __forceinline__ long long fixed_force(float v) {
 }
 __device__ __forceinline__ long long fixed_force(double v) { return to_fixed(v, kForceScale); }
 
-// One warp per (8-atom i cluster, contiguous share of its tile row).  Lane
+// One warp per (8-atom i cluster, contiguous share of its tiles).  Lane
 // l holds pair (i atom l & 7, j atom l >> 3) of every 8 x 4 tile, so a
 // tile's 32 pairs are evaluated at once with no compaction.  The list holds
 // each unordered pair once, so the pair force goes to both atoms: i's
@@ -394,7 +396,11 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
   const int gw = blockIdx.x * kPairWarps + (threadIdx.x >> 5);
   const int ci = gw / a.splits, sp = gw - ci * a.splits;
   if (ci >= a.nclusters) return;  // whole warps exit together
-  const int cnt = a.tile_count[ci];
+  // the cluster's tiles are its kRowParts rows read one after the other;
+  // this warp takes tiles [t0, t1) of that sequence
+  static_assert(kRowParts == 4, "one int4 of row counts per cluster");
+  const int4 c4 = *reinterpret_cast<const int4 *>(a.tile_count + kRowParts * ci);
+  const int cnt = c4.x + c4.y + c4.z + c4.w;
   const int t0 = (int)((long long)cnt * sp / a.splits);
   const int t1 = (int)((long long)cnt * (sp + 1) / a.splits);
   if (t1 <= t0) return;
@@ -427,11 +433,24 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
   int npairs = 0;
   constexpr int kAllTerms = ((TERMS & TERM_LJ) ? kQLJ : 0) | ((TERMS & TERM_COUL) ? kQCoul : 0) |
                             ((TERMS & TERM_EWALD) ? kQEwald : 0);
-  const uint4 *row = a.tiles + (size_t)ci * a.cap;
-  uint4 tnext = __ldg(row + t0);
+  // position of tile t0: row part p, index k in it
+  int p = 0, k = t0, rowlen = c4.x;
+  while (k >= rowlen) {
+    k -= rowlen;
+    p++;
+    rowlen = p == 1 ? c4.y : (p == 2 ? c4.z : c4.w);
+  }
+  const uint4 *row = a.tiles + (size_t)(kRowParts * ci + p) * a.cap;
   for (int t = t0; t < t1; t++) {
-    const uint4 tile = tnext;
-    if (t + 1 < t1) tnext = __ldg(row + t + 1);
+    const uint4 tile = __ldg(row + k);
+    if (++k == rowlen && t + 1 < t1) {  // next non-empty row part (rare)
+      do {
+        k = 0;
+        p++;
+        rowlen = __ldg(a.tile_count + kRowParts * ci + p);
+      } while (rowlen == 0);
+      row = a.tiles + (size_t)(kRowParts * ci + p) * a.cap;
+    }
     const int hj = (int)(tile.x & kJMask);
     const int sh = (int)((tile.x >> kShiftBits) & kShiftMask);
     if (sh != cur) {  // warp-uniform; tiles are grouped by image
@@ -491,7 +510,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
       fz -= jz;
       const Real js = group8_sum3<Real>(jx, jy, jz, lane);
       if (il < 3 && ((actm >> (8 * jl)) & 0xFFu))
-        red_add(&a.force[il * a.n + a.sorted[jslot]], fixed_force(js));
+        red_add(&a.fslot[il * a.ns + jslot], fixed_force(js));
       continue;
     }
     int flags = 0;
@@ -568,10 +587,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
     // j's share: summed over its 8 lanes, one atomic per component
     const unsigned act = __ballot_sync(kAll, flags != 0);
     const Real js = group8_sum3<Real>(jx, jy, jz, lane);
-    if (il < 3 && ((act >> (8 * jl)) & 0xFFu)) {
-      const int oj = a.sorted[jslot];
-      red_add(&a.force[il * a.n + oj], fixed_force(js));
-    }
+    if (il < 3 && ((act >> (8 * jl)) & 0xFFu))
+      red_add(&a.fslot[il * a.ns + jslot], fixed_force(js));
   }
   // i's share: summed over the 4 j lanes of each i atom
 #pragma unroll
@@ -581,9 +598,9 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
     fz += __shfl_xor_sync(kAll, fz, o);
   }
   if (jl == 0 && oi >= 0) {
-    red_add(&a.force[oi], fixed_force(fx));
-    red_add(&a.force[a.n + oi], fixed_force(fy));
-    red_add(&a.force[2 * a.n + oi], fixed_force(fz));
+    red_add(&a.fslot[islot], fixed_force(fx));
+    red_add(&a.fslot[a.ns + islot], fixed_force(fy));
+    red_add(&a.fslot[2 * a.ns + islot], fixed_force(fz));
   }
   if (ENERGY || a.count_pairs) {
     int np = warp_sum(npairs);
@@ -611,6 +628,24 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
         for (int q = 0; q < 9; q++)
           red_add(&a.acc[ACC_VIRIAL + q], to_fixed(V[map[q]], kEnergyScale));
       }
+    }
+  }
+}
+
+// Adds the forces accumulated by list slot into the atoms' forces and
+// clears the slot buffer for the next launch.
+__global__ void k_slot_forces(int ns, int n, const int *__restrict__ sorted,
+                              long long *__restrict__ fslot, long long *__restrict__ force) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const int i = sorted[s];
+  if (i < 0) return;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const long long v = fslot[(size_t)c * ns + s];
+    if (v) {
+      red_add(&force[(size_t)c * n + i], v);
+      fslot[(size_t)c * ns + s] = 0;
     }
   }
 }

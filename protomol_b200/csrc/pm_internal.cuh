@@ -121,6 +121,9 @@ struct PairTerms {
 // 4-atom j clusters: each unordered pair within the reach appears in
 // exactly one tile (see k_build_tiles).
 constexpr int kColCap = 4096;  // atoms per column the in-block sort holds
+// Every i cluster's tiles are split over kRowParts rows (the columns of its
+// search window dealt round-robin), each built and consumed by its own warp.
+constexpr int kRowParts = 4;
 
 struct NeighborList {
   double cutoff = 0, skin = 0, reach = 0;
@@ -130,7 +133,8 @@ struct NeighborList {
   int nkeys = 0;                     // ncol * nzb
   int ns_max = 0;                    // slots incl. padding (multiple of 8)
   int nclusters = 0;                 // ns_max / 8
-  int cap = 0;                       // tiles per i cluster
+  int nrows = 0;                     // nclusters * kRowParts tile rows
+  int cap = 0;                       // tiles per row
   int built = 0;
   long long builds = 0;
   // device
@@ -150,9 +154,10 @@ struct NeighborList {
   double4 *d_xw = nullptr;       // ns_max FP64 wrapped position + q
   int *d_mol_s = nullptr;        // ns_max molecule of each slot (-1 padding)
   float4 *d_bb = nullptr;        // 2 per 4-atom cluster: lower, upper corner
-  uint4 *d_tiles = nullptr;      // nclusters rows of cap tiles
-  int *d_tile_count = nullptr;   // nclusters
-  unsigned int *d_maxdisp = nullptr;  // float bits of max displacement^2
+  long long *d_fslot = nullptr;  // 3 planes of ns_max: pair forces by slot (fixed point)
+  uint4 *d_tiles = nullptr;      // nrows rows of cap tiles (row r: cluster r / kRowParts)
+  int *d_tile_count = nullptr;   // nrows
+  unsigned int *d_maxdisp = nullptr;  // rebuild check: block ticket, max displacement^2 bits
   int *d_rebuild = nullptr;      // rebuild flag, build count
 };
 
@@ -219,7 +224,7 @@ struct System {
   Box box{};
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;     // second stream for the non-pair terms
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr;
   // host copies of static topology
   std::vector<double> h_charge, h_mass;
   std::vector<int> h_type, h_mol;
@@ -310,7 +315,11 @@ void switch_setup(const pmgpu_switch *in, SwitchParams *o);
 int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin,
                  double cellsize_for_debug);
 int nb_list_free(System *s, NeighborList *nl);
+// Per evaluation: nb_prepare (rebuild decision, conditional sort, gather of
+// the slot coordinates), then nb_build (conditional cluster boxes and tile
+// build), then nb_pair_forces.
 int nb_prepare(System *s, NeighborList *nl, int force_rebuild);
+int nb_build(System *s, NeighborList *nl);
 int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode);
 int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
 int nb_simplefull(System *s, int lj, int coul, int em);
@@ -329,7 +338,9 @@ int gb_forces(System *s, Force *f);
 int bonded_forces(System *s, Force *f, int em);
 int torsion_forces(System *s, Force *f, int em);
 int zero_forces(System *s);
-int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase);
+// zero_acc: the update launch also clears the energy accumulators (the
+// start of a force evaluation)
+int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int zero_acc = 0);
 int set_device_step(System *s);
 int forces_to_host(System *s, double *out, int add);
 

@@ -125,10 +125,16 @@ k_pme_spread(PmeArgs a, const double *__restrict__ pos, const double *__restrict
   }
 }
 
-__global__ void k_pme_fixed_to_float(int total, const long long *__restrict__ g,
+// Converts the fixed-point charge grid to FP32 and clears it for the next
+// spread (the grid is zero at allocation and after every conversion, so no
+// separate clearing pass is needed).
+__global__ void k_pme_fixed_to_float(int total, long long *__restrict__ g,
                                      float *__restrict__ out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < total) out[i] = (float)((double)g[i] * (1.0 / kGridScale));
+  if (i < total) {
+    out[i] = (float)((double)g[i] * (1.0 / kGridScale));
+    g[i] = 0;
+  }
 }
 
 // Multiply by the influence function (precomputed for the box:
@@ -346,6 +352,7 @@ int pme_init(System *s, Force *f) {
   size_t ncplx = (size_t)K0 * K1 * (K2 / 2 + 1);
   PM_CHECK(dev_alloc(s, &f->d_grid, sizeof(float) * nreal));
   PM_CHECK(dev_alloc(s, &f->d_grid_fixed, sizeof(long long) * nreal));
+  PM_CUDA(cudaMemsetAsync(f->d_grid_fixed, 0, sizeof(long long) * nreal, s->stream));
   PM_CHECK(dev_alloc(s, &f->d_cgrid, sizeof(float2) * ncplx));
   {
     // influence function of the box (fixed for the life of the system)
@@ -459,7 +466,6 @@ int pme_reciprocal(System *s, Force *f, int em) {
   if (cufftSetStream(f->plan_r2c, s->stream) != CUFFT_SUCCESS ||
       cufftSetStream(f->plan_c2r, s->stream) != CUFFT_SUCCESS)
     return fail(PMGPU_ERR_CUDA, "cufftSetStream failed");
-  PM_CUDA(cudaMemsetAsync(f->d_grid_fixed, 0, sizeof(long long) * nreal, s->stream));
   spread_gather(a, s, f, order_map, 0);
   k_pme_fixed_to_float<<<(int)((nreal + 255) / 256), 256, 0, s->stream>>>(
       (int)nreal, f->d_grid_fixed, f->d_grid);
