@@ -362,9 +362,6 @@ __device__ __forceinline__ int excl_class_of(const int *start, const int *partne
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-__device__ __forceinline__ int floor_div(int a, int b) {
-  return a >= 0 ? a / b : -((-a + b - 1) / b);
-}
 
 // One warp per (8-atom i cluster, row part).  The search window of the
 // i cluster is the set of (column, periodic image, z slice) ranges whose
@@ -394,6 +391,7 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
   // this warp's staging of candidate j clusters (up to 32 of them)
   __shared__ float4 st_x[kBuildWarps][128];
   __shared__ int4 st_o[kBuildWarps][32], st_m[kBuildWarps][32];
+  __shared__ int st_h[kBuildWarps][32], st_c[kBuildWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int rw = blockIdx.x * kBuildWarps + wib;
   const int ci = rw / kRowParts, part = rw - ci * kRowParts;
@@ -431,121 +429,69 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
   uint4 *row = tiles + (size_t)rw * a.cap;
   int count = 0;
 
-  // the j clusters of slots [s0, s1) seen under image code
-  auto scan = [&](int s0, int s1, int code) {
+  // the candidate test of up to four staged j clusters (lane (il, cq)
+  // tests its i atom against the 4 atoms of staged candidate bq[cq])
+  auto test4 = [&](const int (&bq)[4], int ng) {
+    const int myb = cq == 0 ? bq[0] : (cq == 1 ? bq[1] : (cq == 2 ? bq[2] : bq[3]));
+    const bool cval = cq < ng;
+    const int hj = st_h[wib][myb], code = st_c[wib][myb];
     const int sx = (code & 3) - 1, sy = ((code >> 2) & 3) - 1, sz = ((code >> 4) & 3) - 1;
-    const bool zero = code == kZeroShift;
     const float S[3] = {sx * a.L[0], sy * a.L[1], sz * a.L[2]};
-    const int hb = s0 >> 2, he = (s1 - 1) >> 2;
-    for (int hb0 = hb; hb0 <= he; hb0 += 32) {
-      const int h = hb0 + lane;
-      bool cand = false;
-      if (h <= he) {
-        const int parent = h >> 1;
-        cand = parent > ci || (parent == ci && code >= kZeroShift);
-        if (cand) {
-          const float4 jl4 = bb[2 * h], jh4 = bb[2 * h + 1];
-          float g2 = 0.f;
-          const float jlo[3] = {jl4.x + S[0], jl4.y + S[1], jl4.z + S[2]};
-          const float jhi[3] = {jh4.x + S[0], jh4.y + S[1], jh4.z + S[2]};
+    const bool diag = code == kZeroShift && (hj >> 1) == ci;
+    const int4 o4 = st_o[wib][myb], m4 = st_m[wib][myb];
+    const int oj[4] = {o4.x, o4.y, o4.z, o4.w};
+    const int mj[4] = {m4.x, m4.y, m4.z, m4.w};
+    bool pass[4], same = false;
+    float dd[4][3];
 #pragma unroll
-          for (int c = 0; c < 3; c++) {
-            const float g = fmaxf(fmaxf(jlo[c] - ihi[c], ilo[c] - jhi[c]), 0.f);
-            g2 += g * g;
-          }
-          cand = jl4.w > 0.f && g2 <= R2;
-        }
-      }
-      unsigned cm = __ballot_sync(kAll, cand);
-      if (!cm) continue;
-      // every candidate's lane stages its 4 atoms for the tests below
-      if (cand) {
-        const float4 *xs = xhi + 4 * h;
-        st_x[wib][4 * lane] = xs[0];
-        st_x[wib][4 * lane + 1] = xs[1];
-        st_x[wib][4 * lane + 2] = xs[2];
-        st_x[wib][4 * lane + 3] = xs[3];
-        st_o[wib][lane] = *reinterpret_cast<const int4 *>(sorted + 4 * h);
-        st_m[wib][lane] = *reinterpret_cast<const int4 *>(mol_s + 4 * h);
-      }
-      __syncwarp();
-      while (cm) {
-        // the next (up to) four candidates, in ascending order
-        int bq[4];
-        int ng = 0;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          bq[q] = cm ? __ffs(cm) - 1 : 0;
-          if (cm) {
-            cm &= cm - 1;
-            ng = q + 1;
-          }
-        }
-        const int myb = cq == 0 ? bq[0] : (cq == 1 ? bq[1] : (cq == 2 ? bq[2] : bq[3]));
-        const bool cval = cq < ng;
-        const int hj = hb0 + myb;
-        const bool diag = zero && (hj >> 1) == ci;
-        const int4 o4 = st_o[wib][myb], m4 = st_m[wib][myb];
-        const int oj[4] = {o4.x, o4.y, o4.z, o4.w};
-        const int mj[4] = {m4.x, m4.y, m4.z, m4.w};
-        bool pass[4], same = false;
-        float dd[4][3];
-#pragma unroll
-        for (int jl = 0; jl < 4; jl++) {
-          const float4 pj = st_x[wib][4 * myb + jl];
-          dd[jl][0] = pj.x + S[0] - pi.x;
-          dd[jl][1] = pj.y + S[1] - pi.y;
-          dd[jl][2] = pj.z + S[2] - pi.z;
-          const float r2 = dd[jl][0] * dd[jl][0] + dd[jl][1] * dd[jl][1] + dd[jl][2] * dd[jl][2];
-          pass[jl] = cval && ilive && oj[jl] >= 0 && r2 < a.reach2 &&
-                     (!diag || islot < 4 * hj + jl);
-          same = same || (pass[jl] && mj[jl] == mi);
-        }
-        unsigned mb[4] = {0u, 0u, 0u, 0u};
-        // same-molecule pairs (few tiles): ExclusionTable lookup
-        if (__any_sync(kAll, same)) {
-#pragma unroll
-          for (int jl = 0; jl < 4; jl++) {
-            bool mod = false;
-            if (pass[jl] && mj[jl] == mi) {
-              const bool minimal = !a.periodic || (fabsf(dd[jl][0]) <= a.H2[0] &&
-                                                   fabsf(dd[jl][1]) <= a.H2[1] &&
-                                                   fabsf(dd[jl][2]) <= a.H2[2]);
-              if (minimal) {
-                const int cls =
-                    excl_class_of(a.excl_start, a.excl_partner, a.excl_class, oi, oj[jl]);
-                if (cls == PMGPU_EXCL_FULL) pass[jl] = false;
-                else if (cls == PMGPU_EXCL_MODIFIED) mod = true;
-              }
-            }
-            mb[jl] = __ballot_sync(kAll, mod);
-          }
-        }
-        unsigned pb[4];
-#pragma unroll
-        for (int jl = 0; jl < 4; jl++) pb[jl] = __ballot_sync(kAll, pass[jl]);
-        // lane q < 4 assembles candidate q's masks (bit il + 8 jl)
-        const int q = lane & 3, sh = 8 * q;
-        const unsigned im = ((pb[0] >> sh) & 0xFFu) | (((pb[1] >> sh) & 0xFFu) << 8) |
-                            (((pb[2] >> sh) & 0xFFu) << 16) | (((pb[3] >> sh) & 0xFFu) << 24);
-        const unsigned mm = ((mb[0] >> sh) & 0xFFu) | (((mb[1] >> sh) & 0xFFu) << 8) |
-                            (((mb[2] >> sh) & 0xFFu) << 16) | (((mb[3] >> sh) & 0xFFu) << 24);
-        const bool wr = lane < ng && im != 0u;
-        const unsigned wm = __ballot_sync(kAll, wr);
-        if (wr) {
-          const int idx = count + __popc(wm & ((1u << lane) - 1u));
-          const int bsel = q == 0 ? bq[0] : (q == 1 ? bq[1] : (q == 2 ? bq[2] : bq[3]));
-          if (idx < a.cap)
-            row[idx] = make_uint4((uint32_t)(hb0 + bsel) | ((uint32_t)code << kShiftBits), im,
-                                  mm, 0u);
-        }
-        count += __popc(wm);
-      }
-      __syncwarp();  // the next batch overwrites the staging
+    for (int jl = 0; jl < 4; jl++) {
+      const float4 pj = st_x[wib][4 * myb + jl];
+      dd[jl][0] = pj.x + S[0] - pi.x;
+      dd[jl][1] = pj.y + S[1] - pi.y;
+      dd[jl][2] = pj.z + S[2] - pi.z;
+      const float r2 = dd[jl][0] * dd[jl][0] + dd[jl][1] * dd[jl][1] + dd[jl][2] * dd[jl][2];
+      pass[jl] = cval && ilive && oj[jl] >= 0 && r2 < a.reach2 && (!diag || islot < 4 * hj + jl);
+      same = same || (pass[jl] && mj[jl] == mi);
     }
-  };
-  auto slots = [&](int col, int z0, int z1) {  // z bins z0..z1 of a column
-    return make_int2(start[col * a.nzb + z0], start[col * a.nzb + z1 + 1]);
+    unsigned mb[4] = {0u, 0u, 0u, 0u};
+    // same-molecule pairs (few tiles): ExclusionTable lookup
+    if (__any_sync(kAll, same)) {
+#pragma unroll
+      for (int jl = 0; jl < 4; jl++) {
+        bool mod = false;
+        if (pass[jl] && mj[jl] == mi) {
+          const bool minimal = !a.periodic || (fabsf(dd[jl][0]) <= a.H2[0] &&
+                                               fabsf(dd[jl][1]) <= a.H2[1] &&
+                                               fabsf(dd[jl][2]) <= a.H2[2]);
+          if (minimal) {
+            const int cls = excl_class_of(a.excl_start, a.excl_partner, a.excl_class, oi, oj[jl]);
+            if (cls == PMGPU_EXCL_FULL) pass[jl] = false;
+            else if (cls == PMGPU_EXCL_MODIFIED) mod = true;
+          }
+        }
+        mb[jl] = __ballot_sync(kAll, mod);
+      }
+    }
+    unsigned pb[4];
+#pragma unroll
+    for (int jl = 0; jl < 4; jl++) pb[jl] = __ballot_sync(kAll, pass[jl]);
+    // lane q < 4 assembles candidate q's masks (bit il + 8 jl) and writes it
+    const int q = lane & 3, sh = 8 * q;
+    const unsigned im = ((pb[0] >> sh) & 0xFFu) | (((pb[1] >> sh) & 0xFFu) << 8) |
+                        (((pb[2] >> sh) & 0xFFu) << 16) | (((pb[3] >> sh) & 0xFFu) << 24);
+    const unsigned mm = ((mb[0] >> sh) & 0xFFu) | (((mb[1] >> sh) & 0xFFu) << 8) |
+                        (((mb[2] >> sh) & 0xFFu) << 16) | (((mb[3] >> sh) & 0xFFu) << 24);
+    const bool wr = lane < ng && im != 0u;
+    const unsigned wm = __ballot_sync(kAll, wr);
+    if (wr) {
+      const int idx = count + __popc(wm & ((1u << lane) - 1u));
+      const int bsel = q == 0 ? bq[0] : (q == 1 ? bq[1] : (q == 2 ? bq[2] : bq[3]));
+      if (idx < a.cap)
+        row[idx] = make_uint4((uint32_t)st_h[wib][bsel] |
+                                  ((uint32_t)st_c[wib][bsel] << kShiftBits),
+                              im, mm, 0u);
+    }
+    count += __popc(wm);
   };
 
   const int ux0 = (int)floorf((ilo[0] - R - a.lo[0]) / a.cs[0]);
@@ -562,48 +508,150 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
   const int vy0 = a.periodic ? uy0 : clampi(uy0, 0, a.ncy - 1);
   const int nux = (a.periodic ? ux1 : clampi(ux1, 0, a.ncx - 1)) - vx0 + 1;
   const int nuy = (a.periodic ? uy1 : clampi(uy1, 0, a.ncy - 1)) - vy0 + 1;
-  const int nsz = a.periodic ? 3 : 1;
-  const int total = nux * nuy * nsz;
+  const float inv_nuy = 1.0f / (float)nuy;
+  const int total = nux * nuy;
   const int half0 = 8 * ci;  // j clusters of earlier i clusters are never taken
   int deal = 0;
+  // Columns of the window, 32 at a time: lane k forms column k's z ranges
+  // in images sz = -1, 0, 1 (clipped to the half list) as half-cluster
+  // ranges [hs, hs + nh); the non-empty columns are dealt round-robin over
+  // the row parts, and this part's ranges are concatenated into one index
+  // space that the lanes scan 32 half clusters at a time.
   for (int k0 = 0; k0 < total; k0 += 32) {
     const int k = k0 + lane;
-    int rs = 0, re = 0, code = kZeroShift;
+    int hs[3] = {0, 0, 0}, nh[3] = {0, 0, 0}, sxy = 0;
     if (k < total) {
-      const int iz = k % nsz, t = k / nsz;
-      const int iy = t % nuy, ix = t / nuy;
+      int ix = (int)(((float)k + 0.5f) * inv_nuy);
+      ix = ix * nuy > k ? ix - 1 : (ix * nuy + nuy <= k ? ix + 1 : ix);
+      const int iy = k - ix * nuy;
+      int col, sx = 0, sy = 0;
+      bool near = true;
       if (a.periodic) {
-        const int ux = vx0 + ix, uy = vy0 + iy, sz = iz - 1;
-        const int sx = floor_div(ux, a.ncx), cx = ux - sx * a.ncx;
-        const int sy = floor_div(uy, a.ncy), cy = uy - sy * a.ncy;
+        const int ux = vx0 + ix, uy = vy0 + iy;
+        sx = ux < 0 ? -1 : (ux >= a.ncx ? 1 : 0);
+        sy = uy < 0 ? -1 : (uy >= a.ncy ? 1 : 0);
+        col = (ux - sx * a.ncx) * a.ncy + (uy - sy * a.ncy);
         const float clx = a.lo[0] + ux * a.cs[0], cly = a.lo[1] + uy * a.cs[1];
         const float gx = fmaxf(fmaxf(clx - ihi[0], ilo[0] - (clx + a.cs[0])), 0.f);
         const float gy = fmaxf(fmaxf(cly - ihi[1], ilo[1] - (cly + a.cs[1])), 0.f);
-        // z bins of the window in image sz (bin z of image sz lies at
-        // unwrapped bin z + sz * nzb)
-        const int zlo = max(b0 - sz * a.nzb, 0), zhi = min(b1 - sz * a.nzb, a.nzb - 1);
-        if (gx * gx + gy * gy <= R2 && zlo <= zhi) {
-          const int2 r = slots(cx * a.ncy + cy, zlo, zhi);
-          rs = r.x;
-          re = r.y;
-          code = shift_code(sx, sy, sz);
-        }
+        near = gx * gx + gy * gy <= R2;
       } else {
-        const int2 r = slots((vx0 + ix) * a.ncy + (vy0 + iy), clampi(b0, 0, a.nzb - 1),
-                             clampi(b1, 0, a.nzb - 1));
-        rs = r.x;
-        re = r.y;
+        col = (vx0 + ix) * a.ncy + (vy0 + iy);
       }
-      rs = max(rs, half0);
+      sxy = (sx + 1) | ((sy + 1) << 2);
+      if (near) {
+#pragma unroll
+        for (int z = 0; z < 3; z++) {
+          const int sz = z - 1;
+          if (!a.periodic && sz != 0) continue;
+          // z bins of the window in image sz (bin z of image sz lies at
+          // unwrapped bin z + sz * nzb); vacuum: clamped window
+          int zlo, zhi;
+          if (a.periodic) {
+            zlo = max(b0 - sz * a.nzb, 0);
+            zhi = min(b1 - sz * a.nzb, a.nzb - 1);
+          } else {
+            zlo = clampi(b0, 0, a.nzb - 1);
+            zhi = clampi(b1, 0, a.nzb - 1);
+          }
+          if (zlo > zhi) continue;
+          const int rs = max(start[col * a.nzb + zlo], half0);
+          const int re = start[col * a.nzb + zhi + 1];
+          if (re > rs) {
+            hs[z] = rs >> 2;
+            nh[z] = ((re - 1) >> 2) - hs[z] + 1;
+          }
+        }
+      }
     }
-    unsigned live = __ballot_sync(kAll, re > rs);
-    while (live) {
-      const int b = __ffs(live) - 1;
-      live &= live - 1;
-      if (deal++ % kRowParts != part) continue;
-      const int s0 = __shfl_sync(kAll, rs, b), s1 = __shfl_sync(kAll, re, b);
-      const int cd = __shfl_sync(kAll, code, b);
-      scan(s0, s1, cd);
+    const int ncol_h = nh[0] + nh[1] + nh[2];
+    const unsigned live = __ballot_sync(kAll, ncol_h > 0);
+    const int di = deal + __popc(live & ((1u << lane) - 1u));
+    deal += __popc(live);
+    const int mine_h = (ncol_h > 0 && di % kRowParts == part) ? ncol_h : 0;
+    // inclusive scan of this part's half-cluster counts over the lanes
+    int incl = mine_h;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kAll, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int off = incl - mine_h;
+    const int H = __shfl_sync(kAll, incl, 31);
+    for (int base = 0; base < H; base += 32) {
+      const int idx = base + lane;
+      // the column lane r holding index idx: the last lane with off <= idx
+      int r = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int v = __shfl_sync(kAll, off, r + step);
+        if (v <= idx) r += step;
+      }
+      const int loc = idx - __shfl_sync(kAll, off, r);
+      const int n0 = __shfl_sync(kAll, nh[0], r), n1 = __shfl_sync(kAll, nh[1], r);
+      const int h0s = __shfl_sync(kAll, hs[0], r), h1s = __shfl_sync(kAll, hs[1], r);
+      const int h2s = __shfl_sync(kAll, hs[2], r), cxy = __shfl_sync(kAll, sxy, r);
+      int h, z;
+      if (loc < n0) {
+        h = h0s + loc;
+        z = 0;
+      } else if (loc < n0 + n1) {
+        h = h1s + loc - n0;
+        z = 1;
+      } else {
+        h = h2s + loc - n0 - n1;
+        z = 2;
+      }
+      const int code = cxy | (z << 4);
+      bool cand = false;
+      if (idx < H) {
+        const int parent = h >> 1;
+        cand = parent > ci || (parent == ci && code >= kZeroShift);
+        if (cand) {
+          const float S[3] = {((code & 3) - 1) * a.L[0], (((code >> 2) & 3) - 1) * a.L[1],
+                              (z - 1) * a.L[2]};
+          const float4 jl4 = bb[2 * h], jh4 = bb[2 * h + 1];
+          float g2 = 0.f;
+          const float jlo[3] = {jl4.x + S[0], jl4.y + S[1], jl4.z + S[2]};
+          const float jhi[3] = {jh4.x + S[0], jh4.y + S[1], jh4.z + S[2]};
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            const float g = fmaxf(fmaxf(jlo[c] - ihi[c], ilo[c] - jhi[c]), 0.f);
+            g2 += g * g;
+          }
+          cand = jl4.w > 0.f && g2 <= R2;
+        }
+      }
+      unsigned cm = __ballot_sync(kAll, cand);
+      if (!cm) continue;
+      // every candidate's lane stages its 4 atoms, cluster and image
+      if (cand) {
+        const float4 *xs = xhi + 4 * h;
+        st_x[wib][4 * lane] = xs[0];
+        st_x[wib][4 * lane + 1] = xs[1];
+        st_x[wib][4 * lane + 2] = xs[2];
+        st_x[wib][4 * lane + 3] = xs[3];
+        st_o[wib][lane] = *reinterpret_cast<const int4 *>(sorted + 4 * h);
+        st_m[wib][lane] = *reinterpret_cast<const int4 *>(mol_s + 4 * h);
+        st_h[wib][lane] = h;
+        st_c[wib][lane] = code;
+      }
+      __syncwarp();
+      while (cm) {
+        // the next (up to) four candidates, in ascending order
+        int bq[4];
+        int ng = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          bq[q] = cm ? __ffs(cm) - 1 : 0;
+          if (cm) {
+            cm &= cm - 1;
+            ng = q + 1;
+          }
+        }
+        test4(bq, ng);
+      }
+      __syncwarp();  // the next batch overwrites the staging
     }
   }
   if (lane == 0) {

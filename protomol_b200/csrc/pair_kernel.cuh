@@ -433,27 +433,22 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
   int npairs = 0;
   constexpr int kAllTerms = ((TERMS & TERM_LJ) ? kQLJ : 0) | ((TERMS & TERM_COUL) ? kQCoul : 0) |
                             ((TERMS & TERM_EWALD) ? kQEwald : 0);
-  // position of tile t0: row part p, index k in it
-  int p = 0, k = t0, rowlen = c4.x;
-  while (k >= rowlen) {
-    k -= rowlen;
+  // tile t0 is index kb of row part p; the warp walks the parts in order
+  int p = 0, kb = t0, rowlen = c4.x;
+  while (kb >= rowlen) {
+    kb -= rowlen;
     p++;
     rowlen = p == 1 ? c4.y : (p == 2 ? c4.z : c4.w);
   }
-  const uint4 *row = a.tiles + (size_t)(kRowParts * ci + p) * a.cap;
-  for (int t = t0; t < t1; t++) {
+  for (int left = t1 - t0; left > 0;) {
+    const uint4 *row = a.tiles + (size_t)(kRowParts * ci + p) * a.cap;
+    const int ke = min(rowlen, kb + left);
+    left -= ke - kb;
+  for (int k = kb; k < ke; k++) {
     const uint4 tile = __ldg(row + k);
-    if (++k == rowlen && t + 1 < t1) {  // next non-empty row part (rare)
-      do {
-        k = 0;
-        p++;
-        rowlen = __ldg(a.tile_count + kRowParts * ci + p);
-      } while (rowlen == 0);
-      row = a.tiles + (size_t)(kRowParts * ci + p) * a.cap;
-    }
     const int hj = (int)(tile.x & kJMask);
     const int sh = (int)((tile.x >> kShiftBits) & kShiftMask);
-    if (sh != cur) {  // warp-uniform; tiles are grouped by image
+    if (__any_sync(kAll, sh != cur)) {  // tiles are grouped by image
       const int sx = (sh & 3) - 1, sy = ((sh >> 2) & 3) - 1, sz = ((sh >> 4) & 3) - 1;
       // reloaded rather than held in registers through the loop
       const double4 w = a.xw[islot];
@@ -509,8 +504,10 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
       fy -= jy;
       fz -= jz;
       const Real js = group8_sum3<Real>(jx, jy, jz, lane);
-      if (il < 3 && ((actm >> (8 * jl)) & 0xFFu))
-        red_add(&a.fslot[il * a.ns + jslot], fixed_force(js));
+      // address and value formed by every lane, one predicated atomic
+      long long *dst = a.fslot + il * a.ns + jslot;
+      const long long v = fixed_force(js);
+      if (il < 3 && ((actm >> (8 * jl)) & 0xFFu)) red_add(dst, v);
       continue;
     }
     int flags = 0;
@@ -587,8 +584,17 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
     // j's share: summed over its 8 lanes, one atomic per component
     const unsigned act = __ballot_sync(kAll, flags != 0);
     const Real js = group8_sum3<Real>(jx, jy, jz, lane);
-    if (il < 3 && ((act >> (8 * jl)) & 0xFFu))
-      red_add(&a.fslot[il * a.ns + jslot], fixed_force(js));
+    long long *dst = a.fslot + il * a.ns + jslot;
+    const long long v = fixed_force(js);
+    if (il < 3 && ((act >> (8 * jl)) & 0xFFu)) red_add(dst, v);
+  }
+    if (left > 0) {  // next non-empty row part
+      do {
+        p++;
+        rowlen = __ldg(a.tile_count + kRowParts * ci + p);
+      } while (rowlen == 0);
+      kb = 0;
+    }
   }
   // i's share: summed over the 4 j lanes of each i atom
 #pragma unroll
