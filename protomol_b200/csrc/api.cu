@@ -3,6 +3,8 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -200,7 +202,6 @@ static int system_free(System *s) {
   if (s->side) cudaStreamSynchronize(s->side);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
-  if (s->ev_fork2) cudaEventDestroy(s->ev_fork2);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->stream) cudaStreamDestroy(s->stream);
   return PMGPU_OK;
@@ -307,11 +308,10 @@ static int evaluate_forces(System *s, int only, int mode) {
   // corrections) only read the positions and add into the fixed-point
   // forces and energies, so they run on the system's second stream beside
   // the list work and the pair kernels, and join before the evaluation ends
-  // (not while profiling, which times phases in order).  The terms that do
-  // not read the list start at once; PME, which spreads in the list's slot
-  // order, starts once the (conditional) sort is done.  The second stream
-  // has the higher priority, so its short dependent kernels are not queued
-  // behind the pair kernel's blocks.
+  // (not while profiling, which times phases in order).  They start at
+  // once, while the list work of the step leaves most of the device idle.
+  // The second stream has the higher priority, so its short dependent
+  // kernels are not queued behind the pair kernel's blocks.
   const bool fork = s->side && !s->prof.enabled;
   const cudaStream_t main_stream = s->stream;
   if (fork) {
@@ -324,16 +324,18 @@ static int evaluate_forces(System *s, int only, int mode) {
     bool on;
     ~Join() {
       s->stream = main_stream;
+      // a rebuild decision taken by an update kernel holds for this
+      // evaluation only
+      for (auto &nl : s->lists) nl.decided = 0;
       if (!on) return;
       cudaEventRecord(s->ev_join, s->side);
       cudaStreamWaitEvent(main_stream, s->ev_join, 0);
     }
   } join{s, main_stream, fork};
-  auto run_terms = [&](bool list_terms) -> int {
+  {
     if (fork) s->stream = s->side;
     for (auto &f : s->forces) {
       if (only >= 0 ? f.id != only : !f.enabled) continue;
-      if ((f.kind == FK_PME) != list_terms) continue;
       int r = PMGPU_OK;
       switch (f.kind) {
         case FK_PME:
@@ -386,12 +388,10 @@ static int evaluate_forces(System *s, int only, int mode) {
       PM_CHECK(r);
     }
     s->stream = main_stream;
-    return PMGPU_OK;
-  };
-  PM_CHECK(run_terms(false));
+  }
   // neighbour lists are prepared once per evaluation: the rebuild decision,
-  // the (conditional) sort and the per-step gather here, the (conditional)
-  // tile build after PME has been forked
+  // the (conditional) sort and the per-step gather, then the (conditional)
+  // tile build
   for (auto &f : s->forces) {
     if (only >= 0 ? f.id != only : !f.enabled) continue;
     if (f.list_index >= 0 && !prepared[f.list_index]) {
@@ -403,11 +403,6 @@ static int evaluate_forces(System *s, int only, int mode) {
       prepared[f.list_index] = 1;
     }
   }
-  if (fork) {
-    PM_CUDA(cudaEventRecord(s->ev_fork2, main_stream));
-    PM_CUDA(cudaStreamWaitEvent(s->side, s->ev_fork2, 0));
-  }
-  PM_CHECK(run_terms(true));
   for (size_t k = 0; k < prepared.size(); k++) {
     if (!prepared[k]) continue;
     prof_begin(s, PMGPU_PHASE_LIST);
@@ -575,7 +570,6 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   PM_CUDA(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, prio_high));
   PM_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
   PM_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
-  PM_CUDA(cudaEventCreateWithFlags(&s->ev_fork2, cudaEventDisableTiming));
   size_t nn = std::max(1, n);
   PM_CHECK(upload(s.get(), &s->d_charge, t->charge, n));
   PM_CHECK(upload(s.get(), &s->d_mass, t->mass, n));
@@ -1002,7 +996,9 @@ int pmgpu_force_evaluate(pmgpu_system *h, int id, const double *pos, double *for
 static int one_step(System *s, const pmgpu_integrator *it, int phase, int mode) {
   prof_begin(s, PMGPU_PHASE_INTEGRATE);
   // the update launch also starts the evaluation (clears the accumulators)
-  int ri = integrate_kick_drift(s, it, phase, 1);
+  // with one pair list, the update also takes its rebuild decision
+  NeighborList *nl = s->lists.size() == 1 ? &s->lists[0] : nullptr;
+  int ri = integrate_kick_drift(s, it, phase, 1, nl);
   prof_end(s);
   PM_CHECK(ri);
   // update (+ step counter for the Langevin noise)
@@ -1038,9 +1034,16 @@ static int run_graph(System *s, const pmgpu_integrator *it, long g, int *used) {
     cudaError_t ec = cudaStreamEndCapture(s->stream, &graph);
     const long long per_launch = s->kernels - k0;
     s->kernels = k0;
-    if (r != PMGPU_OK || ec != cudaSuccess || !graph ||
-        cudaGraphInstantiate(&sg.exec, graph, cudaGraphInstantiateFlagUseNodePriority) !=
-            cudaSuccess) {
+    cudaError_t ei = cudaSuccess;
+    if (r == PMGPU_OK && ec == cudaSuccess && graph)
+      ei = cudaGraphInstantiate(&sg.exec, graph, cudaGraphInstantiateFlagUseNodePriority);
+    if (r != PMGPU_OK || ec != cudaSuccess || !graph || ei != cudaSuccess) {
+      // the reason is kept for pmgpu_last_error and, with PMGPU_DEBUG set,
+      // printed; the run continues with eager launches
+      if (std::getenv("PMGPU_DEBUG"))
+        std::fprintf(stderr, "pmgpu: step graph not used (%s; end capture: %s; instantiate: %s)\n",
+                     r != PMGPU_OK ? g_last_error.c_str() : "capture ok",
+                     cudaGetErrorString(ec), cudaGetErrorString(ei));
       if (graph) cudaGraphDestroy(graph);
       cudaGetLastError();
       sg.exec = nullptr;

@@ -330,6 +330,12 @@ struct UpdateArgs {
   int kstep_off[2];
   int khalf[2];
   long long *acc_zero;  // energy accumulators cleared by this launch (or null)
+  // the pair list's rebuild decision from the drifted positions (xbuild null:
+  // none); see rebuild_decide
+  const double *xbuild;
+  unsigned *ticket;
+  int *rebuild;
+  float half_skin2;
 };
 
 // Advances the device step counter (after the drift of a step).
@@ -342,45 +348,57 @@ int set_device_step(System *s) {
   return PMGPU_OK;
 }
 
-__global__ void k_update(UpdateArgs a, const double *__restrict__ mass,
-                         double *__restrict__ pos, double *__restrict__ vel,
-                         long long *__restrict__ force, int *__restrict__ status) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+constexpr int kUpdateThreads = 256;
+__global__ void __launch_bounds__(kUpdateThreads)
+k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos,
+         double *__restrict__ vel, long long *__restrict__ force, int *__restrict__ status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (a.acc_zero && i < ACC_COUNT) a.acc_zero[i] = 0;
-  if (i >= a.n) return;
-  double F[3];
-  for (int c = 0; c < 3; c++) F[c] = (double)force[c * a.n + i] * (1.0 / kForceScale);
-  double m = mass[i];
-  double v[3] = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
-  for (int k = 0; k < a.kicks; k++) {
-    if (a.langevin) {
-      double g[3];
-      gauss3(a.seed, *a.step_ptr + (long long)a.kstep_off[k], a.khalf[k], i, g);
-      double sq = sqrt(a.fc / m);
-      for (int c = 0; c < 3; c++)
-        v[c] = xadd(xadd(xmul(v[c], a.vdt), xmul(F[c], a.fdt) / m), xmul(xmul(g[c], sq), a.ndt));
-    } else {
-      // StandardIntegrator::doHalfKick / LeapfrogIntegrator::doKickdoDrift
-      for (int c = 0; c < 3; c++) v[c] = xadd(v[c], xmul(F[c], a.coef) / m);
+  float d2 = 0.f;
+  if (i < a.n) {
+    double F[3];
+    for (int c = 0; c < 3; c++) F[c] = (double)force[c * a.n + i] * (1.0 / kForceScale);
+    double m = mass[i];
+    double v[3] = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+    for (int k = 0; k < a.kicks; k++) {
+      if (a.langevin) {
+        double g[3];
+        gauss3(a.seed, *a.step_ptr + (long long)a.kstep_off[k], a.khalf[k], i, g);
+        double sq = sqrt(a.fc / m);
+        for (int c = 0; c < 3; c++)
+          v[c] = xadd(xadd(xmul(v[c], a.vdt), xmul(F[c], a.fdt) / m),
+                      xmul(xmul(g[c], sq), a.ndt));
+      } else {
+        // StandardIntegrator::doHalfKick / LeapfrogIntegrator::doKickdoDrift
+        for (int c = 0; c < 3; c++) v[c] = xadd(v[c], xmul(F[c], a.coef) / m);
+      }
     }
-  }
-  for (int c = 0; c < 3; c++) vel[3 * i + c] = v[c];
-  if (a.drift) {
-    for (int c = 0; c < 3; c++) {
-      double x = xadd(pos[3 * i + c], xmul(v[c], a.h));
-      pos[3 * i + c] = x;
-      if (!isfinite(x)) atomicOr(status, ST_NONFINITE);
+    for (int c = 0; c < 3; c++) vel[3 * i + c] = v[c];
+    if (a.drift) {
+      double dd = 0.0;
+      for (int c = 0; c < 3; c++) {
+        double x = xadd(pos[3 * i + c], xmul(v[c], a.h));
+        pos[3 * i + c] = x;
+        if (!isfinite(x)) atomicOr(status, ST_NONFINITE);
+        if (a.xbuild) {
+          const double e = x - a.xbuild[3 * i + c];
+          dd += e * e;
+        }
+      }
+      d2 = (float)dd;
     }
+    if (a.zero_force)
+      for (int c = 0; c < 3; c++) force[c * a.n + i] = 0;
   }
-  if (a.zero_force)
-    for (int c = 0; c < 3; c++) force[c * a.n + i] = 0;
+  if (a.xbuild) rebuild_decide<kUpdateThreads>(d2, a.ticket, a.rebuild, a.half_skin2, 0);
 }
 
 // phase: 0 = leapfrog first (half kick + drift), 1 = leapfrog middle (kick +
 // drift), 2 = leapfrog last (half kick), 3 = Langevin half kick + drift,
 // 4 = Langevin two half kicks (end of step s, start of step s+1) + drift,
 // 5 = Langevin closing half kick.
-int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int zero_acc) {
+int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int zero_acc,
+                         NeighborList *list) {
   UpdateArgs a;
   a.n = s->n;
   a.h = it->timestep_fs * kInvTimeFactor;
@@ -390,6 +408,10 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int z
   // kick (step, half) is Philox(seed; atom, step, half).
   a.step_ptr = s->d_step;
   a.acc_zero = zero_acc ? s->d_acc : nullptr;
+  a.xbuild = nullptr;
+  a.ticket = nullptr;
+  a.rebuild = nullptr;
+  a.half_skin2 = 0.f;
   a.kstep_off[0] = 0; a.khalf[0] = 0;
   a.kstep_off[1] = 0; a.khalf[1] = 0;
   a.vdt = a.fdt = a.ndt = a.fc = 0;
@@ -418,9 +440,17 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int z
       break;
     default: return fail(PMGPU_ERR_ARG, "bad integrator phase");
   }
+  if (list && list->built && a.drift && s->n) {
+    const float hs = (float)(0.5 * list->skin);
+    a.xbuild = list->d_xbuild;
+    a.ticket = list->d_maxdisp;
+    a.rebuild = list->d_rebuild;
+    a.half_skin2 = hs * hs;
+    list->decided = 1;
+  }
   if (s->n)
-    k_update<<<(s->n + 255) / 256, 256, 0, s->stream>>>(a, s->d_mass, s->d_pos, s->d_vel,
-                                                        s->d_force, s->d_status);
+    k_update<<<(s->n + kUpdateThreads - 1) / kUpdateThreads, kUpdateThreads, 0, s->stream>>>(
+        a, s->d_mass, s->d_pos, s->d_vel, s->d_force, s->d_status);
   // only the Langevin noise reads the device step counter (every run sets
   // it from the host counter first)
   if (a.drift && a.langevin) k_step_inc<<<1, 1, 0, s->stream>>>(s->d_step);

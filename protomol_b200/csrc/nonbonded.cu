@@ -269,48 +269,24 @@ __global__ void k_gather(int ns, const double *__restrict__ pos,
   mol_s[s] = mol[i];
 }
 
-// Decides whether this evaluation rebuilds the list: first build, forced,
-// or an atom of the current positions lies more than half the skin from
-// its position at the last build (so no pair can have come from beyond the
-// reach to within the cutoff).  Every block reduces its atoms' largest
-// displacement; the last block to finish takes the decision.
-// rebuild[0] is the flag, rebuild[1] counts builds; ticket[0] orders the
-// blocks, ticket[1] holds the running maximum (FP32 bits).
+// Decides whether this evaluation rebuilds the list (rebuild_decide) from
+// the current positions: first build, forced, or an atom lies more than
+// half the skin from its position at the last build (so no pair can have
+// come from beyond the reach to within the cutoff).  MD steps take the
+// decision in the update kernel instead (k_update).
 constexpr int kCheckThreads = 256;
 __global__ void __launch_bounds__(kCheckThreads)
 k_check_rebuild(int n, const double *__restrict__ pos, const double *__restrict__ xbuild,
                 unsigned *__restrict__ ticket, int *__restrict__ rebuild, float half_skin2,
                 int force) {
-  __shared__ float wmax[kCheckThreads / 32];
-  __shared__ bool last;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.f;
   if (i < n && !force) {
     const double dx = pos[3 * i] - xbuild[3 * i], dy = pos[3 * i + 1] - xbuild[3 * i + 1],
                  dz = pos[3 * i + 2] - xbuild[3 * i + 2];
     d2 = (float)(dx * dx + dy * dy + dz * dz);
-    if (!(d2 == d2)) d2 = 3.0e38f;  // NaN: rebuild (the binning flags it)
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
-  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float m = wmax[0];
-    for (int w = 1; w < kCheckThreads / 32; w++) m = fmaxf(m, wmax[w]);
-    if (m > 0.f) atomicMax(&ticket[1], __float_as_uint(m));
-    __threadfence();
-    last = atomicAdd(&ticket[0], 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    const float m = __uint_as_float(atomicExch(&ticket[1], 0u));
-    const int r = force || m > half_skin2;
-    rebuild[0] = r;
-    if (r) rebuild[1] += 1;
-    ticket[0] = 0u;
-  }
+  rebuild_decide<kCheckThreads>(d2, ticket, rebuild, half_skin2, force);
 }
 
 // Bounding box of every 4-atom cluster at the build (lower corner with the
@@ -796,9 +772,12 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
   const int nb = (n + T - 1) / T, nbs = (nl->ns_max + T - 1) / T;
   const int first = !nl->built;
   const float hs = (float)(0.5 * nl->skin);
-  k_check_rebuild<<<nb, kCheckThreads, 0, st>>>(n, s->d_pos, nl->d_xbuild, nl->d_maxdisp,
-                                               nl->d_rebuild, hs * hs,
-                                               (force_rebuild || first) ? 1 : 0);
+  // an MD step's update kernel has taken the decision already
+  if (!nl->decided || first || force_rebuild)
+    k_check_rebuild<<<nb, kCheckThreads, 0, st>>>(n, s->d_pos, nl->d_xbuild, nl->d_maxdisp,
+                                                 nl->d_rebuild, hs * hs,
+                                                 (force_rebuild || first) ? 1 : 0);
+  nl->decided = 0;
   ListGrid g;
   g.box = s->box;
   g.n = n;
@@ -808,16 +787,19 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
     g.lo[a] = nl->lo[a];
     g.inv[a] = 1.0 / nl->cs[a];
   }
-  k_bin<<<nb, T, 0, st>>>(g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_zkey, nl->d_col_count,
-                          nl->d_offset, nl->d_xbuild, s->d_status);
-  k_scan_cols<<<1, 1024, 0, st>>>(nl->d_rebuild, nl->d_col_count, nl->ncol, nl->d_col_u,
-                                  nl->d_col_cursor, nl->d_col_base, nl->d_key_start,
-                                  nl->nkeys, nl->d_sorted, nl->ns_max);
-  k_scatter<<<nb, T, 0, st>>>(nl->d_rebuild, n, nl->d_key, nl->d_col_u, nl->d_col_cursor,
-                              nl->d_unsorted);
-  k_sort_cols<<<nl->ncol, kSortThreads, 0, st>>>(
-      nl->d_rebuild, nl->nzb, (float)(1.0 / nl->cs[2]), nl->d_col_count, nl->d_col_u,
-      nl->d_col_base, nl->d_unsorted, nl->d_zkey, nl->d_sorted, nl->d_key_start, s->d_status);
+  {
+    cudaStream_t q = st;
+    k_bin<<<nb, T, 0, q>>>(g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_zkey, nl->d_col_count,
+                           nl->d_offset, nl->d_xbuild, s->d_status);
+    k_scan_cols<<<1, 1024, 0, q>>>(nl->d_rebuild, nl->d_col_count, nl->ncol, nl->d_col_u,
+                                   nl->d_col_cursor, nl->d_col_base, nl->d_key_start,
+                                   nl->nkeys, nl->d_sorted, nl->ns_max);
+    k_scatter<<<nb, T, 0, q>>>(nl->d_rebuild, n, nl->d_key, nl->d_col_u, nl->d_col_cursor,
+                               nl->d_unsorted);
+    k_sort_cols<<<nl->ncol, kSortThreads, 0, q>>>(
+        nl->d_rebuild, nl->nzb, (float)(1.0 / nl->cs[2]), nl->d_col_count, nl->d_col_u,
+        nl->d_col_base, nl->d_unsorted, nl->d_zkey, nl->d_sorted, nl->d_key_start, s->d_status);
+  }
   if (s->precision == PMGPU_PREC_MIXED)
     k_gather<true><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted,
                                       s->d_charge, s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo,
@@ -837,8 +819,6 @@ int nb_build(System *s, NeighborList *nl) {
   cudaStream_t st = s->stream;
   const int T = 256;
   const int nhalf = nl->ns_max / 4;
-  k_bbox<<<(nhalf + T - 1) / T, T, 0, st>>>(nl->d_rebuild, nhalf, nl->d_sorted, nl->d_xhi,
-                                           nl->d_bb);
   TileBuildArgs ba;
   ba.nclusters = nl->nclusters;
   ba.periodic = s->box.periodic;
@@ -858,9 +838,14 @@ int nb_build(System *s, NeighborList *nl) {
   ba.excl_start = s->d_excl_start;
   ba.excl_partner = s->d_excl_partner;
   ba.excl_class = s->d_excl_class;
-  k_build_tiles<<<(nl->nrows + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, st>>>(
-      ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s, nl->d_bb,
-      nl->d_tiles, nl->d_tile_count, s->d_status);
+  {
+    cudaStream_t q = st;
+    k_bbox<<<(nhalf + T - 1) / T, T, 0, q>>>(nl->d_rebuild, nhalf, nl->d_sorted, nl->d_xhi,
+                                            nl->d_bb);
+    k_build_tiles<<<(nl->nrows + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, q>>>(
+        ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s, nl->d_bb,
+        nl->d_tiles, nl->d_tile_count, s->d_status);
+  }
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
@@ -946,8 +931,7 @@ static int spec_kind(const SwitchParams &sw) {
 }
 
 // Warps per i cluster of the tile kernel: about four waves of the
-// force-only kernel's resident warps (five blocks of kPairWarps per SM),
-// at most 8 per cluster, so blocks that finish early are refilled and the
+// force-only kernel's resident warps (40 per SM), at most 8 per cluster, so blocks that finish early are refilled and the
 // tail stays short.  The split depends only on the system, so every launch
 // of a system sums its forces in the same order.
 static int pair_splits(int nclusters) {
@@ -959,7 +943,7 @@ static int pair_splits(int nclusters) {
         sms <= 0)
       sms = 148;
   }
-  const long long want = 4LL * sms * 5 * kPairWarps;
+  const long long want = 4LL * sms * 40;
   return (int)std::max(1LL, std::min(8LL, (want + nclusters / 2) / std::max(1, nclusters)));
 }
 

@@ -345,7 +345,8 @@ template <typename Real, int MODE, typename SPEC>
 struct PairOccupancy {
   static constexpr bool fast = MODE == PAIR_FORCE && sizeof(Real) == 4 && SPEC::lj >= 0 &&
                                SPEC::exact >= 0;
-  static constexpr int blocks = fast ? 5 : ((MODE == PAIR_FORCE && sizeof(Real) == 4) ? 4 : 2);
+  static constexpr int warps = fast ? 40 : ((MODE == PAIR_FORCE && sizeof(Real) == 4) ? 32 : 16);
+  static constexpr int blocks = warps / kPairWarps;
 };
 
 // Sum of (x, y, z) over the 8 lanes that share lane >> 3, transposed: on
@@ -393,9 +394,17 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
   constexpr bool FAST = MIXED && MODE == PAIR_FORCE && SPEC::lj >= 0 && SPEC::exact >= 0;
   constexpr unsigned kAll = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * kPairWarps + (threadIdx.x >> 5);
+  const int il = lane & 7, jl = lane >> 3;
+  double Elj = 0, Ec = 0;
+  double V64[6] = {0, 0, 0, 0, 0, 0};
+  Real vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+  int npairs = 0;
+  // work items (i cluster, share of its tiles); the warps of a smaller
+  // grid stride over them
+  const int nitems = a.nclusters * a.splits;
+  for (int gw = blockIdx.x * kPairWarps + (threadIdx.x >> 5); gw < nitems;
+       gw += gridDim.x * kPairWarps) {
   const int ci = gw / a.splits, sp = gw - ci * a.splits;
-  if (ci >= a.nclusters) return;  // whole warps exit together
   // the cluster's tiles are its kRowParts rows read one after the other;
   // this warp takes tiles [t0, t1) of that sequence
   static_assert(kRowParts == 4, "one int4 of row counts per cluster");
@@ -403,8 +412,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
   const int cnt = c4.x + c4.y + c4.z + c4.w;
   const int t0 = (int)((long long)cnt * sp / a.splits);
   const int t1 = (int)((long long)cnt * (sp + 1) / a.splits);
-  if (t1 <= t0) return;
-  const int il = lane & 7, jl = lane >> 3;
+  if (t1 <= t0) continue;
   const int islot = 8 * ci + il;
   const int oi = a.sorted[islot];
   const double4 wi = a.xw[islot];  // energy modes and the FP64 kernel only
@@ -427,10 +435,6 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
   Real xs_h[3] = {xi_h[0], xi_h[1], xi_h[2]};
   Real xs_l[3] = {xi_l[0], xi_l[1], xi_l[2]};
   Real fx = 0, fy = 0, fz = 0;
-  Real vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
-  double Elj = 0, Ec = 0;
-  double V64[6] = {0, 0, 0, 0, 0, 0};
-  int npairs = 0;
   constexpr int kAllTerms = ((TERMS & TERM_LJ) ? kQLJ : 0) | ((TERMS & TERM_COUL) ? kQCoul : 0) |
                             ((TERMS & TERM_EWALD) ? kQEwald : 0);
   // tile t0 is index kb of row part p; the warp walks the parts in order
@@ -608,6 +612,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
     red_add(&a.fslot[a.ns + islot], fixed_force(fy));
     red_add(&a.fslot[2 * a.ns + islot], fixed_force(fz));
   }
+  }  // work items
   if (ENERGY || a.count_pairs) {
     int np = warp_sum(npairs);
     if (lane == 0) red_add(&a.acc[ACC_PAIRS], (long long)np);

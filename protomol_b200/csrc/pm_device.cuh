@@ -215,6 +215,41 @@ __device__ __forceinline__ void red_add(long long *p, long long v) {
             static_cast<unsigned long long>(v));
 }
 
+// Pair-list rebuild decision, taken on the device by the last block of a
+// grid to finish: every thread passes the squared displacement of its atom
+// from its position at the last build (0 for no atom); the list is rebuilt
+// when it is forced or some atom moved more than half the skin.
+// rebuild[0] is the flag, rebuild[1] counts builds; ticket[0] orders the
+// blocks, ticket[1] holds the running maximum (FP32 bits).  Every thread of
+// the block must call it; blockDim.x is THREADS.
+template <int THREADS>
+__device__ __forceinline__ void rebuild_decide(float d2, unsigned *ticket, int *rebuild,
+                                               float half_skin2, int force) {
+  __shared__ float wmax[THREADS / 32];
+  __shared__ bool last;
+  if (!(d2 == d2)) d2 = 3.0e38f;  // NaN: rebuild (the binning flags it)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = wmax[0];
+    for (int w = 1; w < THREADS / 32; w++) m = fmaxf(m, wmax[w]);
+    if (m > 0.f) atomicMax(&ticket[1], __float_as_uint(m));
+    __threadfence();
+    last = atomicAdd(&ticket[0], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    const float m = __uint_as_float(atomicExch(&ticket[1], 0u));
+    const int r = force || m > half_skin2;
+    rebuild[0] = r;
+    if (r) rebuild[1] += 1;
+    ticket[0] = 0u;
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -136,6 +136,7 @@ struct NeighborList {
   int nrows = 0;                     // nclusters * kRowParts tile rows
   int cap = 0;                       // tiles per row
   int built = 0;
+  int decided = 0;                   // this evaluation's rebuild decision is taken
   long long builds = 0;
   // device
   int *d_key = nullptr;          // n: column of each atom
@@ -224,7 +225,7 @@ struct System {
   Box box{};
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;     // second stream for the non-pair terms
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // host copies of static topology
   std::vector<double> h_charge, h_mass;
   std::vector<int> h_type, h_mol;
@@ -339,8 +340,10 @@ int bonded_forces(System *s, Force *f, int em);
 int torsion_forces(System *s, Force *f, int em);
 int zero_forces(System *s);
 // zero_acc: the update launch also clears the energy accumulators (the
-// start of a force evaluation)
-int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int zero_acc = 0);
+// start of a force evaluation); list: the pair list whose rebuild decision
+// the update takes from the drifted positions (or null)
+int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int zero_acc = 0,
+                         NeighborList *list = nullptr);
 int set_device_step(System *s);
 int forces_to_host(System *s, double *out, int add);
 

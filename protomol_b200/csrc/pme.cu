@@ -24,7 +24,6 @@ constexpr double kGridScale = 4294967296.0;  // 2^32 per (scaled) charge
 struct PmeArgs {
   Box box;
   int n;
-  int nt;  // atom slots: n, or the pair list's padded spatial order (-1 = empty)
   int K[3];
   int order;
   double inv_L[3];
@@ -85,12 +84,11 @@ __device__ __forceinline__ void grid_coord(const PmeArgs &a, int axis, double w,
 template <int P, int L>
 __global__ void __launch_bounds__(128)
 k_pme_spread(PmeArgs a, const double *__restrict__ pos, const double *__restrict__ charge,
-             const int *__restrict__ order_map, long long *__restrict__ grid) {
+             long long *__restrict__ grid) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = gt / L, kx = gt & (L - 1);
-  if (t >= a.nt || kx >= P) return;
-  const int i = order_map ? order_map[t] : t;
-  if (i < 0) return;
+  if (t >= a.n || kx >= P) return;
+  const int i = t;
   double wx, wy, wz;
   box_minpos(a.box, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wx, wy, wz);
   int iu[3];
@@ -193,12 +191,12 @@ __global__ void k_pme_convolve(int K0, int K1, int K2, double L0, double L1, dou
 template <int P, int L>
 __global__ void __launch_bounds__(128)
 k_pme_gather(PmeArgs a, const double *__restrict__ pos, const double *__restrict__ charge,
-             const int *__restrict__ order_map, const float *__restrict__ phi,
+             const float *__restrict__ phi,
              long long *__restrict__ force) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = gt / L, kx = gt & (L - 1);
-  int i = t < a.nt ? (order_map ? order_map[t] : t) : -1;
-  const bool valid = i >= 0;
+  const int i = t;
+  const bool valid = t < a.n;
   float sx = 0.f, sy = 0.f, sz = 0.f;
   if (valid) {
     double wx, wy, wz;
@@ -413,28 +411,28 @@ int pme_free(System *s, Force *f) {
 }
 
 template <int P>
-static void launch_spread_gather(const PmeArgs &a, System *s, Force *f, const int *order_map,
+static void launch_spread_gather(const PmeArgs &a, System *s, Force *f,
                                  int gather) {
   constexpr int L = P <= 4 ? 4 : 8;
-  const int nb = (int)(((long long)a.nt * L + 127) / 128);
+  const int nb = (int)(((long long)a.n * L + 127) / 128);
   if (!gather)
-    k_pme_spread<P, L><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
+    k_pme_spread<P, L><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge,
                                                   f->d_grid_fixed);
   else
-    k_pme_gather<P, L><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge, order_map,
+    k_pme_gather<P, L><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge,
                                                   f->d_grid, s->d_force);
 }
 
-static void spread_gather(const PmeArgs &a, System *s, Force *f, const int *order_map,
+static void spread_gather(const PmeArgs &a, System *s, Force *f,
                           int gather) {
   switch (f->order) {
-    case 2: launch_spread_gather<2>(a, s, f, order_map, gather); break;
-    case 3: launch_spread_gather<3>(a, s, f, order_map, gather); break;
-    case 4: launch_spread_gather<4>(a, s, f, order_map, gather); break;
-    case 5: launch_spread_gather<5>(a, s, f, order_map, gather); break;
-    case 6: launch_spread_gather<6>(a, s, f, order_map, gather); break;
-    case 7: launch_spread_gather<7>(a, s, f, order_map, gather); break;
-    default: launch_spread_gather<8>(a, s, f, order_map, gather); break;
+    case 2: launch_spread_gather<2>(a, s, f, gather); break;
+    case 3: launch_spread_gather<3>(a, s, f, gather); break;
+    case 4: launch_spread_gather<4>(a, s, f, gather); break;
+    case 5: launch_spread_gather<5>(a, s, f, gather); break;
+    case 6: launch_spread_gather<6>(a, s, f, gather); break;
+    case 7: launch_spread_gather<7>(a, s, f, gather); break;
+    default: launch_spread_gather<8>(a, s, f, gather); break;
   }
 }
 
@@ -453,20 +451,13 @@ int pme_reciprocal(System *s, Force *f, int em) {
   int K0 = f->grid[0], K1 = f->grid[1], K2 = f->grid[2];
   size_t nreal = (size_t)K0 * K1 * K2;
   size_t ncplx = (size_t)K0 * K1 * (K2 / 2 + 1);
-  // Spread in the spatial order of the pair list when there is one, so
-  // neighbouring threads hit neighbouring grid lines.
-  const int *order_map = nullptr;
-  a.nt = n;
-  if (f->list_index >= 0 && f->list_index < (int)s->lists.size() &&
-      s->lists[f->list_index].built) {
-    order_map = s->lists[f->list_index].d_sorted;
-    a.nt = s->lists[f->list_index].ns_max;
-  }
-  // the plans run on whichever stream this evaluation uses
+  // Atoms are spread and gathered in their own order: PME does not wait for
+  // the pair list's sort, so it runs beside the list work of a step.  The
+  // plans run on whichever stream this evaluation uses.
   if (cufftSetStream(f->plan_r2c, s->stream) != CUFFT_SUCCESS ||
       cufftSetStream(f->plan_c2r, s->stream) != CUFFT_SUCCESS)
     return fail(PMGPU_ERR_CUDA, "cufftSetStream failed");
-  spread_gather(a, s, f, order_map, 0);
+  spread_gather(a, s, f, 0);
   k_pme_fixed_to_float<<<(int)((nreal + 255) / 256), 256, 0, s->stream>>>(
       (int)nreal, f->d_grid_fixed, f->d_grid);
   if (cufftExecR2C(f->plan_r2c, f->d_grid, (cufftComplex *)f->d_cgrid) != CUFFT_SUCCESS)
@@ -476,7 +467,7 @@ int pme_reciprocal(System *s, Force *f, int em) {
       f->d_cgrid, s->d_acc, em);
   if (cufftExecC2R(f->plan_c2r, (cufftComplex *)f->d_cgrid, f->d_grid) != CUFFT_SUCCESS)
     return fail(PMGPU_ERR_CUDA, "cufftExecC2R failed");
-  spread_gather(a, s, f, order_map, 1);
+  spread_gather(a, s, f, 1);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
