@@ -172,6 +172,15 @@ def load_traffic() -> float | None:
     return None
 
 
+# FP32 flops of one in-cutoff pair in the force-only tile kernel
+# (LJ C2 + Ewald real space, an FMA counts two): hi/lo difference 9, r^2 5,
+# rsqrt with one Newton step 5, 1/r^2 1, LJ 10, C2 switch 12, charge
+# product 1, Ewald real term (exp, poly5 erfc, 1/(1+p ar)) 24, total 1,
+# pair and i forces 6, share of the j-force reduction 4; plus 4 MUFU
+# (rsqrt, ex2, rcp and the exp argument scaling) not counted.
+PAIR_FLOPS = 78
+
+
 def algorithmic_bytes_per_step(n: int, grid: int) -> dict:
     """Unique bytes one MD step must move (counted once), by phase:
     pair pass N*(16 pos+q + 4 type + 24 force write + 24 force read);
@@ -419,9 +428,11 @@ def main():
     ap.add_argument("--impl", default="pmgpu", choices=["pmgpu", "reference"])
     ap.add_argument("--segment", type=int, default=SEGMENT)
     ap.add_argument("--mode", default="bench",
-                    choices=["bench", "profile", "served", "batched", "gb"],
+                    choices=["bench", "profile", "profile-build", "served", "batched", "gb"],
                     help="profile: warm-up segments, then --steps MD steps between "
-                         "cudaProfilerStart/Stop (for ncu); served: a mixed request stream "
+                         "cudaProfilerStart/Stop (for ncu); profile-build: the first force "
+                         "evaluation (it builds the pair list) between "
+                         "cudaProfilerStart/Stop; served: a mixed request stream "
                          "served plain (one slot) and with continuous batching; batched: "
                          "an ensemble of small boxes, one MD segment each")
     ap.add_argument("--requests", type=int, default=48,
@@ -490,6 +501,17 @@ def main():
     for line in gpu_force_lines():
         ff.make(line)
     integ = LeapfrogIntegrator(DT_FS)
+    if args.mode == "profile-build":
+        # one full pair-list build (sort and tiles) and force evaluation
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        gs.evaluate()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"mode": "profile-build", "atoms": gs.n,
+                          "list_builds": gs.forces[3].stats()["list_builds"]}))
+        gs.close()
+        return
     if args.mode == "profile":
         # steady state: warm-up segments, then --steps MD steps as one run()
         # (graphs on) between cudaProfilerStart/Stop, for
@@ -577,6 +599,8 @@ def main():
     pair_gbs = ab["pairs"] / pair_avg_s / 1e9
     step_s = t_ms / 1000.0 / md_steps / world
     traffic = load_traffic()
+    fp32_peak = ctx.fp32_peak()
+    pair_tflops = PAIR_FLOPS * pairs / pair_avg_s / 1e12
     forms = run_forms(args, ctx, world, rank, dist) if args.forms else None
     if rank == 0:
         line = {
@@ -601,7 +625,13 @@ def main():
                          "avg_launch_us": pair_avg_s * 1e6,
                          "step": {"algorithmic_bytes": ab["total"],
                                   "achieved_gbs": ab["total"] / step_s / 1e9,
-                                  "frac": ab["total"] / step_s / 1e9 / peaks["hbm_gbs"]}},
+                                  "frac": ab["total"] / step_s / 1e9 / peaks["hbm_gbs"]},
+                         # the pair kernel is bound by FP32 issue, not DRAM:
+                         # its algorithmic flops against the measured FMA peak
+                         "fp32": {"achieved": pair_tflops, "peak": fp32_peak,
+                                  "unit": "TFLOP/s", "frac": pair_tflops / max(fp32_peak, 1e-9),
+                                  "flops_per_pair": PAIR_FLOPS,
+                                  "peak_source": "measured (pmgpu_fp32_peak, FMA chains)"}},
             "e2e": {"value": e2e_ns_day, "unit": "ns/day",
                     "h2d_bytes_per_step": 2 * 3 * n * 8,
                     "d2h_bytes_per_step": 2 * 3 * n * 8 + 7 * 8},

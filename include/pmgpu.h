@@ -287,6 +287,11 @@ int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
                              const int grid[3], long long *bytes);
 
 /* ---- diagnostics ---------------------------------------------------- */
+/* Measured FP32 FMA throughput of the context's GPU in TFLOP/s (an FMA
+ * counts two flops): every SM runs independent FMA chains for about a
+ * millisecond.  The compute roofline of the pair kernel is quoted against
+ * it.  No counterpart in the reference. */
+int pmgpu_fp32_peak(pmgpu_context *ctx, double *tflops);
 typedef struct {
   long long pairs_in_cutoff;   /* pairs that passed the cutoff test */
   long long list_entries;      /* tiles in the pair list: (8-atom i cluster,

@@ -39,6 +39,7 @@ EXPORTED = [
     "pmgpu_debug_pair_set", "pmgpu_profile_enable", "pmgpu_profile_read",
     "pmgpu_kernel_count", "pmgpu_gb_forces_noalloc", "pmgpu_run_async", "pmgpu_run_query",
     "pmgpu_run_wait", "pmgpu_mem_info", "pmgpu_footprint_estimate", "pmgpu_force_torsion_add",
+    "pmgpu_fp32_peak",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -130,6 +131,7 @@ def load() -> C.CDLL:
     lib.pmgpu_run_query.argtypes = [vp, C.POINTER(i32)]
     lib.pmgpu_run_wait.argtypes = [vp]
     lib.pmgpu_mem_info.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.pmgpu_fp32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     lib.pmgpu_footprint_estimate.argtypes = [i32, vp, dbl, vp, C.POINTER(C.c_longlong)]
     lib.pmgpu_gb_forces_noalloc.argtypes = [i32, vp, vp, vp, vp, vp, vp, C.POINTER(dbl),
                                             dbl, dbl, i32, vp, vp, vp]

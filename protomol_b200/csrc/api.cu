@@ -489,6 +489,52 @@ static int with_overflow_retry(Fn fn) {
   return r;
 }
 
+// FP32 FMA throughput: every thread advances 8 independent FMA chains (no
+// dependence between them, so the pipes stay full); the result is stored
+// only under a condition that never holds, so nothing is optimised away.
+constexpr int kPeakChains = 8;
+__global__ void __launch_bounds__(256) k_fma_peak(int iters, float a, float b, float *sink) {
+  float v[kPeakChains];
+#pragma unroll
+  for (int c = 0; c < kPeakChains; c++) v[c] = (float)(threadIdx.x + c);
+  for (int k = 0; k < iters; k++) {
+#pragma unroll
+    for (int c = 0; c < kPeakChains; c++) v[c] = fmaf(v[c], a, b);
+  }
+  float t = 0.f;
+#pragma unroll
+  for (int c = 0; c < kPeakChains; c++) t += v[c];
+  if (t == -1.2345f) sink[0] = t;
+}
+
+static int fp32_peak(int device, double *tflops) {
+  PM_CUDA(cudaSetDevice(device));
+  int sms = 148;
+  PM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  float *sink = nullptr;
+  PM_CUDA(cudaMalloc(&sink, sizeof(float)));
+  cudaEvent_t e0, e1;
+  PM_CUDA(cudaEventCreate(&e0));
+  PM_CUDA(cudaEventCreate(&e1));
+  const int blocks = sms * 8, iters = 4096;
+  double best = 0.0;
+  for (int rep = 0; rep < 4; rep++) {  // the first launch warms up
+    PM_CUDA(cudaEventRecord(e0));
+    k_fma_peak<<<blocks, 256>>>(iters, 0.999f, 1e-3f, sink);
+    PM_CUDA(cudaEventRecord(e1));
+    PM_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const double flops = 2.0 * kPeakChains * (double)iters * blocks * 256;
+    if (rep > 0 && ms > 0.f) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  *tflops = best;
+  return PMGPU_OK;
+}
+
 static int begin_eval(System *s) {
   PM_CUDA(cudaMemsetAsync(s->d_acc, 0, sizeof(long long) * ACC_COUNT, s->stream));
   return PMGPU_OK;
@@ -1228,6 +1274,11 @@ int pmgpu_mem_info(pmgpu_context *ctx, long long *free_bytes, long long *total_b
 // the resident state, the sorted coordinates, the list at its initial
 // capacity and the PME grids (cuFFT work areas are estimated as one more
 // complex grid).
+int pmgpu_fp32_peak(pmgpu_context *ctx, double *tflops) {
+  if (!ctx || !tflops) return fail(PMGPU_ERR_ARG, "null argument");
+  return fp32_peak(ctx->device, tflops);
+}
+
 int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
                              const int grid[3], long long *bytes) {
   if (!box || !bytes || n_atoms < 0 || !(reach >= 0)) return fail(PMGPU_ERR_ARG, "bad argument");

@@ -219,11 +219,14 @@ template <typename Real, int KIND>
 __device__ __forceinline__ void switch_fast(const SwitchDev<Real> &sw, Real r2, Real rinv,
                                             Real &ff, Real en) {
   if (KIND == PMGPU_SW_C2) {
-    const Real c2 = sw.cutoff2 - r2;
-    const Real c4 = c2 * (sw.s2 + Real(2) * r2);
-    const bool on = r2 >= sw.switchon2, off = r2 > sw.cutoff2;
-    const Real val = off ? Real(0) : (on ? sw.s1 * (c2 * c4) : Real(1));
-    const Real der = (on && !off) ? sw.s3 * (c2 * c2 - c4) : Real(0);
+    // the polynomial is 1 with zero slope at the switch-on distance and 0
+    // with zero slope at the cutoff, so r^2 clamped into [rs^2, rc^2] gives
+    // every region's value and derivative (to rounding) without selects
+    const Real r2c = fmin(fmax(r2, sw.switchon2), sw.cutoff2);
+    const Real c2 = sw.cutoff2 - r2c;
+    const Real c4 = c2 * (sw.s2 + Real(2) * r2c);
+    const Real val = sw.s1 * (c2 * c4);
+    const Real der = sw.s3 * (c2 * c2 - c4);
     ff = ff * val - en * der;
   } else if (KIND == PMGPU_SW_C1) {
     const Real d = r2 * rinv;
@@ -237,7 +240,7 @@ __device__ __forceinline__ void switch_fast(const SwitchDev<Real> &sw, Real r2, 
 // Pair force of the force-only specialised kernels: every term inside its
 // (common) cutoff, no energies, no branches.  Same arithmetic as
 // pair_force.
-template <typename Real, int TERMS, typename SPEC>
+template <typename Real, int TERMS, typename SPEC, bool MOD>
 __device__ __forceinline__ Real pair_force_fast(const PairArgs<Real> &a, const Real *ljrow,
                                                 Real r2, Real qq, int tj, bool modified) {
   const Real rinv = rsqrt_nr(r2);
@@ -247,12 +250,12 @@ __device__ __forceinline__ Real pair_force_fast(const PairArgs<Real> &a, const R
     Real A, B;
     if (sizeof(Real) == 4) {
       const float4 p = __ldg(reinterpret_cast<const float4 *>(ljrow) + tj);
-      A = modified ? p.z : p.x;
-      B = modified ? p.w : p.y;
+      A = MOD && modified ? p.z : p.x;
+      B = MOD && modified ? p.w : p.y;
     } else {
       const double4 p = reinterpret_cast<const double4 *>(ljrow)[tj];
-      A = modified ? p.z : p.x;
-      B = modified ? p.w : p.y;
+      A = MOD && modified ? p.z : p.x;
+      B = MOD && modified ? p.w : p.y;
     }
     const Real r6 = rinv2 * rinv2 * rinv2;
     const Real r6B = B * r6;
@@ -261,7 +264,7 @@ __device__ __forceinline__ Real pair_force_fast(const PairArgs<Real> &a, const R
     switch_fast<Real, SPEC::lj>(a.lj_sw, r2, rinv, ff, r12A - r6B);
     f += ff;
   }
-  qq = modified ? qq * a.csf : qq;
+  if (MOD) qq = modified ? qq * a.csf : qq;
   if (TERMS & TERM_COUL) {
     const Real en = qq * rinv;
     Real ff = en * rinv2;
@@ -395,6 +398,9 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
   constexpr unsigned kAll = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int il = lane & 7, jl = lane >> 3;
+  const unsigned lanebit = 1u << lane;        // this lane's bit of a tile mask
+  const unsigned jbyte = 0xFFu << (8 * jl);   // the 8 lanes of this lane's j atom
+  const bool jcomp = il < 3;                  // lane adds j's force component il
   double Elj = 0, Ec = 0;
   double V64[6] = {0, 0, 0, 0, 0, 0};
   Real vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
@@ -470,7 +476,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
       cur = sh;
     }
     const int jslot = 4 * hj + jl;
-    const bool live = (tile.y >> lane) & 1u;
+    const bool live = (tile.y & lanebit) != 0u;
     Real dx, dy, dz, qj;
     int tj = 0;
     if (MIXED) {
@@ -497,11 +503,18 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
                 a.max_cut2;
       }
       const unsigned actm = __ballot_sync(kAll, act);
-      npairs += act;
+      if (a.count_pairs) npairs += act;
       if (!actm) continue;
-      const bool modified = (tile.z >> lane) & 1u;
-      Real f = pair_force_fast<Real, TERMS, SPEC>(a, ljrow, act ? r2 : Real(1), qi * qj, tj,
-                                                  modified);
+      const Real rr = act ? r2 : Real(1);
+      Real f;
+      // modified (scaled 1-4) pairs are rare: tiles without any take the
+      // path without their selects (the mask is the tile's, so the branch
+      // is uniform)
+      if (__any_sync(kAll, tile.z != 0u))
+        f = pair_force_fast<Real, TERMS, SPEC, true>(a, ljrow, rr, qi * qj, tj,
+                                                     (tile.z & lanebit) != 0u);
+      else
+        f = pair_force_fast<Real, TERMS, SPEC, false>(a, ljrow, rr, qi * qj, tj, false);
       f = act ? f : Real(0);
       const Real jx = dx * f, jy = dy * f, jz = dz * f;
       fx -= jx;
@@ -511,7 +524,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
       // address and value formed by every lane, one predicated atomic
       long long *dst = a.fslot + il * a.ns + jslot;
       const long long v = fixed_force(js);
-      if (il < 3 && ((actm >> (8 * jl)) & 0xFFu)) red_add(dst, v);
+      if (jcomp && (actm & jbyte)) red_add(dst, v);
       continue;
     }
     int flags = 0;

@@ -62,6 +62,12 @@ class Context:
         L.check(self.lib.pmgpu_mem_info(self.h, C.byref(f), C.byref(t)))
         return int(f.value), int(t.value)
 
+    def fp32_peak(self) -> float:
+        """Measured FP32 FMA throughput of the device, TFLOP/s."""
+        t = C.c_double()
+        L.check(self.lib.pmgpu_fp32_peak(self.h, C.byref(t)))
+        return float(t.value)
+
     def close(self):
         if self.h:
             self.lib.pmgpu_context_destroy(self.h)
