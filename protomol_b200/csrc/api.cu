@@ -339,18 +339,20 @@ static int evaluate_forces(System *s, int only, int mode) {
       int r = PMGPU_OK;
       switch (f.kind) {
         case FK_PME:
+          // the short correction first, so the PME chain ends the stream
+          if (f.ewald_flags & PMGPU_EWALD_CORRECTION) {
+            prof_begin(s, PMGPU_PHASE_CORRECTION);
+            r = ewald_correction(s, &f, em);
+            prof_end(s);
+            PM_CHECK(r);
+            s->kernels += s->n_excl > 0;
+          }
           if (f.ewald_flags & PMGPU_EWALD_RECIPROCAL) {
             prof_begin(s, PMGPU_PHASE_PME);
             r = pme_reciprocal(s, &f, em);
             prof_end(s);
             PM_CHECK(r);
             s->kernels += 4;  // spread, fixed->float, convolve, gather (+ cuFFT)
-          }
-          if (f.ewald_flags & PMGPU_EWALD_CORRECTION) {
-            prof_begin(s, PMGPU_PHASE_CORRECTION);
-            r = ewald_correction(s, &f, em);
-            prof_end(s);
-            s->kernels += s->n_excl > 0;
           }
           break;
         case FK_GB:
@@ -409,7 +411,7 @@ static int evaluate_forces(System *s, int only, int mode) {
     int r = nb_build(s, &s->lists[k]);
     prof_end(s);
     PM_CHECK(r);
-    s->kernels += 2;  // cluster boxes, tiles
+    s->kernels += 1;  // tiles
   }
   for (auto &g : groups) {
     prof_begin(s, PMGPU_PHASE_PAIRS);

@@ -245,28 +245,53 @@ __global__ void k_gather(int ns, const double *__restrict__ pos,
                          const double *__restrict__ charge,
                          const int *__restrict__ type, const int *__restrict__ mol,
                          float4 *__restrict__ xhi, float4 *__restrict__ xlo,
-                         double4 *__restrict__ xw, int *__restrict__ mol_s) {
+                         double4 *__restrict__ xw, int *__restrict__ mol_s,
+                         const int *__restrict__ rebuild, float4 *__restrict__ bb) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
-  const int i = sorted[s];
-  if (i < 0) {
+  const bool in = s < ns;
+  const int i = in ? sorted[s] : -1;
+  float hx = 0.f, hy = 0.f, hz = 0.f;
+  if (in && i < 0) {
     const double far = 1.0e5 + 16.0 * s;
     xw[s] = make_double4(far, 1.0e5, 1.0e5, 0.0);
     xhi[s] = make_float4((float)far, 1.0e5f, 1.0e5f, 0.f);
     if (MIXED) xlo[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
     mol_s[s] = -1;
-    return;
+  } else if (in) {
+    const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    const double wx = x - offset[3 * i], wy = y - offset[3 * i + 1], wz = z - offset[3 * i + 2];
+    const double q = charge[i];
+    xw[s] = make_double4(wx, wy, wz, q);
+    hx = (float)wx;
+    hy = (float)wy;
+    hz = (float)wz;
+    xhi[s] = make_float4(hx, hy, hz, (float)q);
+    if (MIXED)
+      xlo[s] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
+                           (float)(wz - (double)hz), __int_as_float(type[i]));
+    mol_s[s] = mol[i];
   }
-  const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-  const double wx = x - offset[3 * i], wy = y - offset[3 * i + 1], wz = z - offset[3 * i + 2];
-  const double q = charge[i];
-  xw[s] = make_double4(wx, wy, wz, q);
-  const float hx = (float)wx, hy = (float)wy, hz = (float)wz;
-  xhi[s] = make_float4(hx, hy, hz, (float)q);
-  if (MIXED)
-    xlo[s] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
-                         (float)(wz - (double)hz), __int_as_float(type[i]));
-  mol_s[s] = mol[i];
+  // on a rebuild: the box of every 4-atom cluster (4 consecutive lanes;
+  // lower corner with the number of atoms in .w, upper corner)
+  if (*rebuild) {
+    const bool atom = in && i >= 0;
+    float lo[3] = {atom ? hx : 3.0e38f, atom ? hy : 3.0e38f, atom ? hz : 3.0e38f};
+    float hi[3] = {atom ? hx : -3.0e38f, atom ? hy : -3.0e38f, atom ? hz : -3.0e38f};
+    int m = atom ? 1 : 0;
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        lo[c] = fminf(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+        hi[c] = fmaxf(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+      }
+      m += __shfl_xor_sync(0xffffffffu, m, o);
+    }
+    if (in && (s & 3) == 0) {
+      bb[2 * (s >> 2)] = make_float4(lo[0], lo[1], lo[2], (float)m);
+      bb[2 * (s >> 2) + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
+    }
+  }
 }
 
 // Decides whether this evaluation rebuilds the list (rebuild_decide) from
@@ -287,30 +312,6 @@ k_check_rebuild(int n, const double *__restrict__ pos, const double *__restrict_
     d2 = (float)(dx * dx + dy * dy + dz * dz);
   }
   rebuild_decide<kCheckThreads>(d2, ticket, rebuild, half_skin2, force);
-}
-
-// Bounding box of every 4-atom cluster at the build (lower corner with the
-// number of atoms in .w, upper corner).
-__global__ void k_bbox(const int *__restrict__ rebuild, int nhalf,
-                       const int *__restrict__ sorted, const float4 *__restrict__ xhi,
-                       float4 *__restrict__ bb) {
-  if (!*rebuild) return;
-  const int h = blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= nhalf) return;
-  float lo[3] = {3.0e38f, 3.0e38f, 3.0e38f}, hi[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
-  int m = 0;
-  for (int k = 0; k < 4; k++) {
-    if (sorted[4 * h + k] < 0) continue;
-    const float4 p = xhi[4 * h + k];
-    const float c[3] = {p.x, p.y, p.z};
-    for (int a = 0; a < 3; a++) {
-      lo[a] = fminf(lo[a], c[a]);
-      hi[a] = fmaxf(hi[a], c[a]);
-    }
-    m++;
-  }
-  bb[2 * h] = make_float4(lo[0], lo[1], lo[2], (float)m);
-  bb[2 * h + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
 }
 
 // ---------------------------------------------------------- list build
@@ -369,13 +370,14 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
   __shared__ int4 st_o[kBuildWarps][32], st_m[kBuildWarps][32];
   __shared__ int st_h[kBuildWarps][32], st_c[kBuildWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int rw = blockIdx.x * kBuildWarps + wib;
+  // the warps of the (resident) grid stride over the rows
+  for (int rw = blockIdx.x * kBuildWarps + wib; rw < a.nclusters * kRowParts;
+       rw += gridDim.x * kBuildWarps) {
   const int ci = rw / kRowParts, part = rw - ci * kRowParts;
-  if (ci >= a.nclusters) return;  // whole warps exit together
   const float4 l0 = bb[4 * ci], h0 = bb[4 * ci + 1], l1 = bb[4 * ci + 2], h1 = bb[4 * ci + 3];
   if (l0.w + l1.w == 0.f) {
     if (lane == 0) tile_count[rw] = 0;
-    return;
+    continue;
   }
   float ilo[3] = {fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z)};
   float ihi[3] = {fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z)};
@@ -393,7 +395,7 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
       tile_count[rw] = 0;
       atomicOr(status, ST_NONFINITE);
     }
-    return;
+    continue;
   }
   const int il = lane & 7, cq = lane >> 3;
   const int islot = 8 * ci + il;
@@ -637,6 +639,8 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
     }
     tile_count[rw] = count;
   }
+  __syncwarp();  // the next row reuses the staging
+  }  // rows
 }
 
 }  // namespace pmgpu
@@ -788,7 +792,7 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
     g.inv[a] = 1.0 / nl->cs[a];
   }
   {
-    cudaStream_t q = st;
+    cudaStream_t q = st;  // the rebuild-only sort
     k_bin<<<nb, T, 0, q>>>(g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_zkey, nl->d_col_count,
                            nl->d_offset, nl->d_xbuild, s->d_status);
     k_scan_cols<<<1, 1024, 0, q>>>(nl->d_rebuild, nl->d_col_count, nl->ncol, nl->d_col_u,
@@ -803,22 +807,21 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
   if (s->precision == PMGPU_PREC_MIXED)
     k_gather<true><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted,
                                       s->d_charge, s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo,
-                                      nl->d_xw, nl->d_mol_s);
+                                      nl->d_xw, nl->d_mol_s, nl->d_rebuild, nl->d_bb);
   else
     k_gather<false><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted,
                                        s->d_charge, s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo,
-                                       nl->d_xw, nl->d_mol_s);
+                                       nl->d_xw, nl->d_mol_s, nl->d_rebuild, nl->d_bb);
   PM_CUDA(cudaGetLastError());
   nl->built = 1;  // the slot order exists from here on
   return PMGPU_OK;
 }
 
-// The (conditional) tile build of a prepared list: cluster boxes and tiles.
+// The (conditional) tile build of a prepared list (the cluster boxes come
+// with the gather).
 int nb_build(System *s, NeighborList *nl) {
   if (s->n == 0) return PMGPU_OK;
   cudaStream_t st = s->stream;
-  const int T = 256;
-  const int nhalf = nl->ns_max / 4;
   TileBuildArgs ba;
   ba.nclusters = nl->nclusters;
   ba.periodic = s->box.periodic;
@@ -838,14 +841,16 @@ int nb_build(System *s, NeighborList *nl) {
   ba.excl_start = s->d_excl_start;
   ba.excl_partner = s->d_excl_partner;
   ba.excl_class = s->d_excl_class;
-  {
-    cudaStream_t q = st;
-    k_bbox<<<(nhalf + T - 1) / T, T, 0, q>>>(nl->d_rebuild, nhalf, nl->d_sorted, nl->d_xhi,
-                                            nl->d_bb);
-    k_build_tiles<<<(nl->nrows + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, q>>>(
-        ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s, nl->d_bb,
-        nl->d_tiles, nl->d_tile_count, s->d_status);
-  }
+  // a grid of resident blocks whose warps stride over the rows: cheap to
+  // launch on the steps that keep the list
+  static int sms = 0;
+  if (!sms && (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device) !=
+                   cudaSuccess || sms <= 0))
+    sms = 148;
+  const int nblk = std::max(1, std::min((nl->nrows + kBuildWarps - 1) / kBuildWarps, 3 * sms));
+  k_build_tiles<<<nblk, kBuildWarps * 32, 0, st>>>(
+      ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s, nl->d_bb,
+      nl->d_tiles, nl->d_tile_count, s->d_status);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
