@@ -258,7 +258,12 @@ def served_line(args, ctx, world: int, rank: int, dist=None) -> dict:
                     f"rc 9 A")
     else:
         return ensemble_line(args, ctx, world, rank, dist)
-    serve.execute(ctx, serve.Request(rid=-1, n_waters=300, seed=1, steps=20))  # warm-up
+    # warm-up: every request shape once (short), so lazily loaded FFT and
+    # kernel modules of every grid size are resident before either form is
+    # timed
+    for r in replicas.my_share(mk(), world, rank):
+        serve.execute(ctx, serve.Request(rid=-1, n_waters=r.n_waters, seed=r.seed,
+                                         kind=r.kind, steps=min(r.steps, 12)))
     out = {}
     for name, slots in (("plain", 1), ("served", args.slots)):
         reqs = replicas.my_share(mk(), world, rank)

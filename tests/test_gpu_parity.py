@@ -240,3 +240,41 @@ def test_torsions_vs_reference(ctx, name):
     assert F.rms_rel(f, F.forces(z, 0)) <= 1e-8
     assert _energy_ok(e[4], F.energies(z, 0)[4], rel=1e-10, floor=1e-8)
     gs.close()
+
+
+def test_list_follows_uploaded_positions(ctx):
+    """The pair list is rebuilt whenever the positions handed in lie more
+    than half the skin from those of the last build, so evaluations at
+    configurations handed in between calls (the whole box shifted by
+    1-1.5 A, which changes the periodic images of atoms near the faces, and
+    every molecule moved by 0.05-0.2 A) still match the oracle at each
+    configuration."""
+    z = F.load("c1_tip3p648")
+    topo = F.topology(z)
+    gs = GpuSystem(ctx, topo, "mixed")
+    ff = ForceFactory(gs, 8.0)
+    line = ("LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction C2 "
+            "-switchon 7 -cutoff 8 -switchingFunction C2 -switchon 7 -cutoff 8 -cutoff 8")
+    force = ff.make(line)
+    terms = [("LennardJones", oracle.Switch("C2", 8.0, 7.0)),
+             ("Coulomb", oracle.Switch("C2", 8.0, 7.0))]
+    rng = np.random.default_rng(5)
+    pos = topo.pos.copy()
+    mol = topo.molecule
+    for k in range(4):
+        if k:
+            shift = rng.normal(size=3)
+            pos += shift / np.linalg.norm(shift) * rng.uniform(1.0, 1.5)
+            for m in np.unique(mol):
+                v = rng.normal(size=3)
+                pos[mol == m] += v / np.linalg.norm(v) * rng.uniform(0.05, 0.2)
+        f = np.zeros_like(pos)
+        e = ScalarStructure()
+        force.evaluate(pos, f, e)
+        s = F.oracle_system(z)
+        s.pos = pos.copy()
+        fo, eo, _ = oracle.cutoff_force(s, 8.0, 8.0, terms)
+        err = F.rms_rel(f, fo)
+        assert err <= RMS_MIXED, (k, err)
+    assert force.stats()["list_builds"] >= 4
+    gs.close()
