@@ -833,10 +833,12 @@ static int add_force(System *s, Force &f, int *force_id) {
 }
 
 static double default_skin(const System *s, double cutoff) {
-  // A 1 A skin keeps list rebuilds to every ~10-20 steps for liquid water
-  // at 1 fs; small boxes get a smaller skin so cutoff + skin stays below
-  // the box edge.
-  double skin = 1.0;
+  // A 1.3 A skin: the list is rebuilt on about 18 of 100 steps for liquid
+  // (flexible) water at 1 fs, which balances the build against the pairs
+  // the skin adds to every step (1.0 and 1.6 A measured within 1 %, 0.7 A
+  // 4 % slower); small boxes get a smaller skin so cutoff + skin stays
+  // below the box edge.
+  double skin = 1.3;
   if (s->box.periodic) {
     double emin = std::min(s->box.e[0], std::min(s->box.e[1], s->box.e[2]));
     if (cutoff + skin >= emin) skin = std::max(0.0, 0.5 * (emin - cutoff));

@@ -28,7 +28,7 @@ from .engine import (Context, ForceFactory, GpuSystem, LangevinLeapfrogIntegrato
                      LeapfrogIntegrator, footprint_estimate)
 
 WATER_DENSITY = 0.0334  # waters per A^3
-RC, ALPHA, ORDER, LJ_SWITCHON, SPACING, SKIN = 9.0, 0.35, 4, 8.0, 1.0, 1.0
+RC, ALPHA, ORDER, LJ_SWITCHON, SPACING, SKIN = 9.0, 0.35, 4, 8.0, 1.0, 1.3
 
 
 def fft_size(n: int) -> int:
