@@ -174,12 +174,50 @@ static int upload(System *s, T **d, const T *h, size_t count) {
   return PMGPU_OK;
 }
 
+// ProtoMol fills its LJ table from per-type (epsilon, rmin/2) by the CHARMM
+// rule (topology/BuildTopology.cpp:662-672): r = s_i + s_j,
+// e = sqrt(e_i e_j), A = e r^12, B = 2 e r^6.  When every normal (A, B)
+// entry follows that rule to 1e-10 relative, *out receives the per-type
+// (sqrt(e), s) and the FP32 all-pairs kernel computes A and B instead of
+// reading the ntypes^2 table.  The 1-4 entries are always read from the
+// table.
+static bool lj_charmm_rule(const double *lj, int nt, std::vector<float2> *out) {
+  if (nt <= 0 || !lj) return false;
+  std::vector<double> se(nt), sh(nt);
+  for (int t = 0; t < nt; t++) {
+    const double A = lj[4 * ((size_t)t * nt + t)], B = lj[4 * ((size_t)t * nt + t) + 1];
+    if (A == 0 && B == 0) {
+      se[t] = 0;
+      sh[t] = 0;
+      continue;
+    }
+    if (!(A > 0 && B > 0)) return false;
+    // diagonal: (2 s)^6 = 2 A / B and e = B^2 / (4 A)
+    sh[t] = 0.5 * std::pow(2 * A / B, 1.0 / 6.0);
+    se[t] = std::sqrt(B * B / (4 * A));
+  }
+  auto close = [](double got, double want) {
+    return std::fabs(got - want) <= 1e-10 * std::max(std::fabs(want), 1e-300);
+  };
+  for (int t1 = 0; t1 < nt; t1++)
+    for (int t2 = 0; t2 < nt; t2++) {
+      const double *p = lj + 4 * ((size_t)t1 * nt + t2);
+      const double r = sh[t1] + sh[t2], e = se[t1] * se[t2];
+      const double r6 = r * r * r * r * r * r;
+      if (!close(p[0], e * r6 * r6) || !close(p[1], 2 * e * r6)) return false;
+    }
+  out->resize(nt);
+  for (int t = 0; t < nt; t++) (*out)[t] = make_float2((float)se[t], (float)sh[t]);
+  return true;
+}
+
 static int system_free(System *s) {
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (auto &f : s->forces) pme_free(s, &f);
   for (auto &nl : s->lists) nb_list_free(s, &nl);
-  void *ptrs[] = {s->d_charge, s->d_mass, s->d_type, s->d_mol, s->d_lj32, s->d_lj64,
+  void *ptrs[] = {s->d_charge, s->d_mass, s->d_type, s->d_mol, s->d_lj32, s->d_ljab,
+                  s->d_ljcomb, s->d_lj64,
                   s->d_excl_start, s->d_excl_partner, s->d_excl_class, s->d_excl_pairs,
                   s->d_excl_range,
                   s->d_bond_atoms, s->d_angle_atoms, s->d_bond_params, s->d_angle_params,
@@ -359,7 +397,7 @@ static int evaluate_forces(System *s, int only, int mode) {
           prof_begin(s, PMGPU_PHASE_GB);
           r = gb_forces(s, &f);
           prof_end(s);
-          s->kernels += 5;
+          s->kernels += s->precision == PMGPU_PREC_MIXED ? 4 : 5;
           break;
         case FK_BONDED:
           prof_begin(s, PMGPU_PHASE_BONDED);
@@ -376,11 +414,15 @@ static int evaluate_forces(System *s, int only, int mode) {
           break;
         case FK_SIMPLEFULL:
           // all enabled simple-full terms share one all-pairs pass
+          // on the main stream, beside the dependent chains of the second
+          // stream (GB's three passes, PME)
           if (sf_done) break;
           sf_done = 1;
           prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
+          if (fork) s->stream = main_stream;
           r = nb_simplefull(s, only >= 0 ? f.sf_lj : sf_lj, only >= 0 ? f.sf_coul : sf_coul,
                             em);
+          if (fork) s->stream = s->side;
           prof_end(s);
           s->kernels += 1;
           break;
@@ -632,6 +674,20 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
     lj64[k] = make_double4(p[0], p[1], p[2], p[3]);
   }
   PM_CHECK(upload(s.get(), &s->d_lj32, lj32.data(), nt2));
+  std::vector<float2> comb;
+  if (lj_charmm_rule(t->lj, t->n_types, &comb)) {
+    PM_CHECK(upload(s.get(), &s->d_ljcomb, comb.data(), comb.size()));
+  } else {
+    // A, B stored by column: a warp whose lanes hold consecutive types of
+    // one atom reads the entries of a partner type as one coalesced row
+    std::vector<float2> ljab(nt2);
+    const int nt = t->n_types;
+    for (int t1 = 0; t1 < nt; t1++)
+      for (int t2 = 0; t2 < nt; t2++)
+        ljab[(size_t)t2 * nt + t1] = make_float2(lj32[(size_t)t1 * nt + t2].x,
+                                                 lj32[(size_t)t1 * nt + t2].y);
+    PM_CHECK(upload(s.get(), &s->d_ljab, ljab.data(), nt2));
+  }
   PM_CHECK(upload(s.get(), &s->d_lj64, lj64.data(), nt2));
   // exclusion table as CSR over both atoms of each pair
   int ne = std::max(0, t->n_exclusions);

@@ -271,6 +271,309 @@ __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
   if ((threadIdx.x & 31) == 0) red_add(&a.acc[ACC_COULOMB], to_fixed(epair, kEnergyScale));
 }
 
+// ---------------------------------------------------------------------
+// FP32 forms of the three all-pairs passes.  One accumulating atom per
+// thread (kApAtoms per block) against a chunk of partner atoms staged
+// kApTile at a time as broadcast float4 records with hi/lo FP32
+// coordinates, so the pair loops take no FP64 operation or conversion.
+// Reciprocals come from the hardware estimate plus one Newton step and
+// every distance from one rsqrt; the self pair is masked rather than
+// skipped.  Sums are kept per partner tile in FP32 and carried in FP64.
+
+// burial term of the "i sees j" direction given dist and 1/dist
+__device__ __forceinline__ float gb_burial_term_f32(float dist, float idist, float oi,
+                                                   float ioi, float sjoj) {
+  float L, U;
+  if (oi >= dist + sjoj) {
+    L = 1.0f;
+    U = 1.0f;
+  } else {
+    const float a = fabsf(dist - sjoj);
+    L = oi > a ? oi : a;
+    U = dist + sjoj;
+  }
+  const float iL = rcp_nr(L), iU = rcp_nr(U);
+  const float C = (oi < sjoj - dist) ? 2.0f * (ioi - iL) : 0.0f;
+  const float iL2 = iL * iL, iU2 = iU * iU;
+  return (iL - iU) + (0.25f * dist) * (iU2 - iL2) + (0.5f * idist) * logf(L * iU) +
+         (0.25f * sjoj * sjoj * idist) * (iL2 - iU2) + C;
+}
+
+// dBT/dr of the "i sees j" direction (same terms as gb_dBT above)
+__device__ __forceinline__ float gb_dBT_f32(float dist, float idist, float oi, float sjoj) {
+  float L, U;
+  if (oi >= dist + sjoj) {
+    L = 1.0f;
+    U = 1.0f;
+  } else {
+    const float a = fabsf(dist - sjoj);
+    L = oi > a ? oi : a;
+    U = dist + sjoj;
+  }
+  const float iL = rcp_nr(L), iU = rcp_nr(U);
+  const float dL = (oi <= (dist - sjoj)) ? 1.0f : 0.0f;
+  const float dU = (oi < (dist + sjoj)) ? 1.0f : 0.0f;
+  const float iL2 = iL * iL, iU2 = iU * iU;
+  const float dC = (oi <= (sjoj - dist)) ? 2.0f * iL2 * dL : 0.0f;
+  const float Sjt = sjoj * idist;
+  const float s2d = sjoj * sjoj * idist;
+  return -0.5f * dL * iL2 + 0.5f * dU * iU2 + 0.125f * (iU2 - iL2) +
+         0.125f * dist * (2.0f * iL2 * iL * dL - 2.0f * iU2 * iU * dU) -
+         0.25f * (idist * idist) * logf(L * iU) +
+         (0.25f * U * idist * iL) * (iU * dL - (L * iU2) * dU) -
+         0.125f * (Sjt * Sjt) * (iL2 - iU2) + 0.25f * s2d * iU2 * iU * dU -
+         0.25f * s2d * iL2 * iL * dL + dC;
+}
+
+__device__ __forceinline__ void gb_stage_pos(const double *pos, int j, float4 &h, float4 &l) {
+  split_hilo(pos[3 * j], h.x, l.x);
+  split_hilo(pos[3 * j + 1], h.y, l.y);
+  split_hilo(pos[3 * j + 2], h.z, l.z);
+}
+
+__global__ void __launch_bounds__(kApAtoms) k_gb_burial_f32(GbArgs a, int jchunk) {
+  __shared__ float4 sh[kApTile], sl[kApTile];
+  __shared__ int sw[kApTile];
+  const int i = blockIdx.x * kApAtoms + threadIdx.x;
+  const bool valid = i < a.n;
+  const int ii = valid ? i : 0;
+  float xh, yh, zh, xl, yl, zl;
+  split_hilo(a.pos[3 * ii], xh, xl);
+  split_hilo(a.pos[3 * ii + 1], yh, yl);
+  split_hilo(a.pos[3 * ii + 2], zh, zl);
+  const float oi = (float)(a.vdwr[ii] - a.offset[ii]);
+  const float ioi = rcp_nr(oi);
+  const bool active = valid && !(a.water && a.water[ii]);
+  double acc = 0.0;
+  const int j0 = blockIdx.y * jchunk, j1 = min(a.n, j0 + jchunk);
+  for (int base = j0; base < j1; base += kApTile) {
+    if (threadIdx.x < kApTile) {
+      const int j = base + threadIdx.x;
+      if (j < j1) {
+        float4 h, l;
+        gb_stage_pos(a.pos, j, h, l);
+        h.w = (float)(a.vdwr[j] - a.offset[j]);
+        l.w = (float)a.scale[j];
+        sh[threadIdx.x] = h;
+        sl[threadIdx.x] = l;
+        sw[threadIdx.x] = a.water ? a.water[j] : 0;
+      }
+    }
+    __syncthreads();
+    const int lim = min(kApTile, j1 - base);
+    if (active) {
+      float part = 0;
+#pragma unroll 2
+      for (int k = 0; k < lim; k++) {
+        const float4 h = sh[k], l = sl[k];
+        const bool use = (base + k != i) && !sw[k];
+        const float dx = (h.x - xh) + (l.x - xl);
+        const float dy = (h.y - yh) + (l.y - yl);
+        const float dz = (h.z - zh) + (l.z - zl);
+        const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
+        const float idist = rsqrt_nr(r2);
+        const float t = gb_burial_term_f32(r2 * idist, idist, oi, ioi, l.w * h.w);
+        part += use ? t : 0.0f;
+      }
+      acc += (double)part;
+    }
+    __syncthreads();
+  }
+  if (active && acc != 0.0) red_add(&a.burial_fx[i], to_fixed(acc, kGbScale));
+}
+
+// Partial sums over each unordered pair once: a warp takes one 32 x 32
+// tile pair (I, J), I <= J, lane l holding atom 32 I + l against the J atoms
+// broadcast from the warp's shared-memory slice; partialTerm[i][j] adds to
+// i in the lane and partialTerm[j][i] to j through warp_tsum8.
+__global__ void __launch_bounds__(kHpWarps * 32)
+k_gb_partial_half(GbArgs a, int tiles, long long items) {
+  __shared__ float4 sh[kHpWarps][32], sl[kHpWarps][32];
+  __shared__ float sib[kHpWarps][32];
+  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  const long long nw = (long long)gridDim.x * kHpWarps;
+  for (long long w = (long long)blockIdx.x * kHpWarps + wb; w < items; w += nw) {
+    int I, J;
+    tile_pair_of(w, tiles, &I, &J);
+    const int i = I * 32 + lane;
+    const bool vi = i < a.n;
+    const int ii = vi ? i : 0;
+    float xh, yh, zh, xl, yl, zl;
+    split_hilo(a.pos[3 * ii], xh, xl);
+    split_hilo(a.pos[3 * ii + 1], yh, yl);
+    split_hilo(a.pos[3 * ii + 2], zh, zl);
+    const float qi = (float)a.charge[ii], bi = (float)a.born[ii];
+    const float q4bi = (float)(0.25 / a.born[ii]);
+    {
+      const int j = J * 32 + lane;
+      const int jj = j < a.n ? j : 0;
+      float4 h, l;
+      gb_stage_pos(a.pos, jj, h, l);
+      h.w = (float)a.charge[jj];
+      l.w = (float)a.born[jj];
+      sh[wb][lane] = h;
+      sl[wb][lane] = l;
+      sib[wb][lane] = (float)(1.0 / a.born[jj]);
+    }
+    __syncwarp();
+    float pi = 0;
+#pragma unroll 1
+    for (int g = 0; g < 4; g++) {
+      float gp[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int k = g * 8 + u;
+        const int j = J * 32 + k;
+        const float4 h = sh[wb][k], l = sl[wb][k];
+        const float ibj = sib[wb][k];
+        const bool use = vi && j < a.n && (I < J || k > lane);
+        const float dx = (h.x - xh) + (l.x - xl);
+        const float dy = (h.y - yh) + (l.y - yl);
+        const float dz = (h.z - zh) + (l.z - zl);
+        const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
+        const float bj = l.w, bb = bi * bj;
+        const float ex = __expf(-r2 * (q4bi * ibj));
+        const float ifil = rsqrt_nr(r2 + bb * ex);
+        const float p = 0.5f * qi * h.w * (ifil * ifil * ifil) * ex;
+        // aTerm of both directions (GBPartialSum.cpp:33)
+        pi += use ? p * (bj + r2 * q4bi) : 0.0f;
+        gp[u] = use ? p * (bi + 0.25f * r2 * ibj) : 0.0f;
+      }
+      const float sp = warp_tsum8(gp, lane);
+      const int jt = J * 32 + g * 8 + (lane >> 2);
+      if ((lane & 3) == 0 && jt < a.n) red_add(&a.partial_fx[jt], to_fixed((double)sp, kGbScale));
+    }
+    if (vi) red_add(&a.partial_fx[i], to_fixed((double)pi, kGbScale));
+    __syncwarp();
+  }
+}
+
+// Forces and pair energy over each unordered pair once (same tiling as
+// k_gb_partial_half); the pair force of GBForce::operator() is symmetric in
+// i and j, so j receives its opposite through warp_tsum8.  The partial sums
+// are read straight from their fixed-point accumulators.
+__global__ void __launch_bounds__(kHpWarps * 32)
+k_gb_force_half(GbArgs a, int tiles, long long items) {
+  __shared__ float4 sh[kHpWarps][32], sl[kHpWarps][32], sg[kHpWarps][32];
+  __shared__ float2 sk[kHpWarps][32];
+  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  const long long nw = (long long)gridDim.x * kHpWarps;
+  const double d = a.dielec;
+  double epair = 0.0;
+  for (long long w = (long long)blockIdx.x * kHpWarps + wb; w < items; w += nw) {
+    int I, J;
+    tile_pair_of(w, tiles, &I, &J);
+    const int i = I * 32 + lane;
+    const bool vi = i < a.n;
+    const int ii = vi ? i : 0;
+    float xh, yh, zh, xl, yl, zl;
+    split_hilo(a.pos[3 * ii], xh, xl);
+    split_hilo(a.pos[3 * ii + 1], yh, yl);
+    split_hilo(a.pos[3 * ii + 2], zh, zl);
+    const float bi = (float)a.born[ii], qi = (float)a.charge[ii];
+    const double oid = a.vdwr[ii] - a.offset[ii];
+    const float oi = (float)oid;
+    const float soi = (float)(a.scale[ii] * oid);
+    const float dfac_i = (float)a.psi[ii];
+    const float part_i = (float)((double)a.partial_fx[ii] * (1.0 / kGbScale));
+    const double ibi = 1.0 / a.born[ii];
+    const float q4bi = (float)(0.25 * ibi);
+    const float selfi = (float)(0.5 * a.charge[ii] * a.charge[ii] * ibi * ibi);
+    {
+      const int j = J * 32 + lane;
+      const int jj = j < a.n ? j : 0;
+      float4 h, l, g;
+      gb_stage_pos(a.pos, jj, h, l);
+      h.w = (float)a.charge[jj];
+      const double bj = a.born[jj];
+      l.w = (float)bj;
+      const double oj = a.vdwr[jj] - a.offset[jj];
+      g.x = (float)oj;
+      g.y = (float)(a.scale[jj] * oj);
+      g.z = (float)a.psi[jj];
+      g.w = (float)((double)a.partial_fx[jj] * (1.0 / kGbScale));
+      const double ibj = 1.0 / bj;
+      sh[wb][lane] = h;
+      sl[wb][lane] = l;
+      sg[wb][lane] = g;
+      sk[wb][lane] = make_float2((float)ibj, (float)(0.5 * a.charge[jj] * a.charge[jj] * ibj * ibj));
+    }
+    __syncwarp();
+    float fx = 0, fy = 0, fz = 0, ep = 0;
+#pragma unroll 1
+    for (int gq = 0; gq < 4; gq++) {
+      float gx[8], gy[8], gz[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int k = gq * 8 + u;
+        const int j = J * 32 + k;
+        const float4 h = sh[wb][k], l = sl[wb][k], g = sg[wb][k];
+        const float2 kj = sk[wb][k];
+        const bool use = vi && j < a.n && (I < J || k > lane);
+        const float dx = (h.x - xh) + (l.x - xl);
+        const float dy = (h.y - yh) + (l.y - yl);
+        const float dz = (h.z - zh) + (l.z - zl);
+        const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
+        const float idist = rsqrt_nr(r2);
+        const float dist = r2 * idist;
+        const float qj = h.w, bj = l.w, bb = bi * bj;
+        const float ex = __expf(-r2 * (q4bi * kj.x));
+        const float ifgb = rsqrt_nr(r2 + bb * ex);
+        const float qq = qi * qj;
+        const float dRi = dfac_i * gb_dBT_f32(dist, idist, oi, g.y);
+        const float dRj = g.z * gb_dBT_f32(dist, idist, g.x, soi);
+        const float pref = 0.5f * qq * (ifgb * ifgb * ifgb);
+        // partialTerm[i][j] and [j][i] (GBPartialSum.cpp:33-41)
+        const float ai = bj + r2 * q4bi;
+        const float aj = bi + 0.25f * r2 * kj.x;
+        const float ptij = pref * ex * ai, ptji = pref * ex * aj;
+        float f = -pref * ((2.0f * dist - 0.5f * ex * dist) + ex * dRi * ai + ex * dRj * aj);
+        f -= selfi * dRi;
+        f -= kj.y * dRj;
+        f -= (part_i - ptij) * dRi;
+        f -= (g.w - ptji) * dRj;
+        f *= idist;
+        f = use ? f : 0.0f;
+        ep += use ? -qq * ifgb : 0.0f;
+        fx -= dx * f; fy -= dy * f; fz -= dz * f;
+        gx[u] = dx * f; gy[u] = dy * f; gz[u] = dz * f;
+      }
+      const float sx = warp_tsum8(gx, lane), sy = warp_tsum8(gy, lane),
+                  sz = warp_tsum8(gz, lane);
+      const int jt = J * 32 + gq * 8 + (lane >> 2);
+      if ((lane & 3) == 0 && jt < a.n) {
+        red_add(&a.force[jt], to_fixed((double)sx * d, kForceScale));
+        red_add(&a.force[a.n + jt], to_fixed((double)sy * d, kForceScale));
+        red_add(&a.force[2 * a.n + jt], to_fixed((double)sz * d, kForceScale));
+      }
+    }
+    if (vi) {
+      red_add(&a.force[i], to_fixed((double)fx * d, kForceScale));
+      red_add(&a.force[a.n + i], to_fixed((double)fy * d, kForceScale));
+      red_add(&a.force[2 * a.n + i], to_fixed((double)fz * d, kForceScale));
+    }
+    epair += (double)ep;
+    __syncwarp();
+  }
+  epair = warp_sum(epair) * d;
+  if (lane == 0 && epair != 0.0) red_add(&a.acc[ACC_COULOMB], to_fixed(epair, kEnergyScale));
+}
+
+// The FP32 chain: burial sums, Born radii, partial sums, forces (the
+// partial sums stay in their fixed-point accumulators).
+static void gb_passes_f32(const GbArgs &a, cudaStream_t st) {
+  dim3 grid;
+  int jchunk;
+  allpairs_grid(a.n, &grid, &jchunk);
+  int tiles, blocks;
+  long long items;
+  halfpairs_grid(a.n, &tiles, &items, &blocks);
+  k_gb_burial_f32<<<grid, kApAtoms, 0, st>>>(a, jchunk);
+  k_gb_radii<<<(a.n + 127) / 128, 128, 0, st>>>(a);
+  k_gb_partial_half<<<blocks, kHpWarps * 32, 0, st>>>(a, tiles, items);
+  k_gb_force_half<<<blocks, kHpWarps * 32, 0, st>>>(a, tiles, items);
+}
+
 int gb_init(System *s) {
   int n = std::max(1, s->n);
   if (!s->d_gb_vdwr) return fail(PMGPU_ERR_ARG, "GB force needs gb_vdwr/gb_scale/gb_offset");
@@ -311,11 +614,7 @@ int gb_forces(System *s, Force *f) {
   gb_grid(n, &grid, &jchunk);
   cudaStream_t st = s->stream;
   if (s->precision == PMGPU_PREC_MIXED) {
-    k_gb_burial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
-    k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);
-    k_gb_partial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
-    k_gb_partial_fin<<<(n + 127) / 128, 128, 0, st>>>(a);
-    k_gb_force<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    gb_passes_f32(a, st);
   } else {
     k_gb_burial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
     k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);
@@ -475,11 +774,7 @@ extern "C" int pmgpu_gb_forces_noalloc(int n_atoms, const double *pos, const dou
   int jchunk;
   gb_grid(n, &grid, &jchunk);
   if (precision == PMGPU_PREC_MIXED) {
-    k_gb_burial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
-    k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);
-    k_gb_partial<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
-    k_gb_partial_fin<<<(n + 127) / 128, 128, 0, st>>>(a);
-    k_gb_force<float><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    gb_passes_f32(a, st);
   } else {
     k_gb_burial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
     k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);

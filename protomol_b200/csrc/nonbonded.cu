@@ -1200,6 +1200,182 @@ k_simplefull(int n, int jchunk, const double *__restrict__ pos,
   }
 }
 
+// The FP32 pass over each unordered pair once, as the reference visits
+// i < j (NonbondedSimpleFullSystemForce.h:125-150): a warp takes one 32 x 32
+// tile pair (I, J), I <= J, lane l holding atom 32 I + l; the J atoms sit
+// in the warp's shared-memory slice and are broadcast one at a time.  The
+// force on i accumulates in the lane, the opposite force on each j is
+// summed over the lanes by warp_tsum8 per eight j atoms; on the diagonal
+// tile only j > i counts.  Energies and virial (EM 1, 2) are not halved.
+template <bool LJ, bool COUL, bool COMB, int EM>
+__global__ void __launch_bounds__(kHpWarps * 32)
+k_simplefull_half(int n, int tiles, long long items, const double *__restrict__ pos,
+                  const double *__restrict__ charge, const int *__restrict__ type, int ntypes,
+                  const float2 *__restrict__ ljab, const float2 *__restrict__ ljcomb,
+                  const float4 *__restrict__ lj32, const int2 *__restrict__ ex_range,
+                  const int *__restrict__ ex_start, const int *__restrict__ ex_partner,
+                  const int *__restrict__ ex_class, float csf, long long *__restrict__ force,
+                  long long *__restrict__ acc) {
+  __shared__ float4 sh[kHpWarps][32], sl[kHpWarps][32];
+  __shared__ float2 sc[kHpWarps][COMB ? 32 : 1];
+  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  const long long nw = (long long)gridDim.x * kHpWarps;
+  double elj = 0, ec = 0;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (long long w = (long long)blockIdx.x * kHpWarps + wb; w < items; w += nw) {
+    int I, J;
+    tile_pair_of(w, tiles, &I, &J);
+    const int i = I * 32 + lane;
+    const bool vi = i < n;
+    const int ii = vi ? i : 0;
+    float xh, yh, zh, xl, yl, zl;
+    split_hilo(pos[3 * ii], xh, xl);
+    split_hilo(pos[3 * ii + 1], yh, yl);
+    split_hilo(pos[3 * ii + 2], zh, zl);
+    const float qi = (float)charge[ii];
+    const int ti = type[ii];
+    const float2 ci = COMB ? ljcomb[ti] : make_float2(0.f, 0.f);
+    const int2 er = ex_range[ii];
+    {
+      const int j = J * 32 + lane;
+      const int jj = j < n ? j : 0;
+      float4 h, l;
+      split_hilo(pos[3 * jj], h.x, l.x);
+      split_hilo(pos[3 * jj + 1], h.y, l.y);
+      split_hilo(pos[3 * jj + 2], h.z, l.z);
+      h.w = (float)charge[jj];
+      const int tj = type[jj];
+      l.w = __int_as_float(tj);
+      sh[wb][lane] = h;
+      sl[wb][lane] = l;
+      if (COMB) sc[wb][lane] = ljcomb[tj];
+    }
+    __syncwarp();
+    float fx = 0, fy = 0, fz = 0;
+#pragma unroll 1
+    for (int g = 0; g < 4; g++) {
+      float gx[8], gy[8], gz[8];
+      float2 tab[8];
+      if (LJ && !COMB) {
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+          tab[u] = __ldg(&ljab[__float_as_int(sl[wb][g * 8 + u].w) * ntypes + ti]);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int k = g * 8 + u;
+        const int j = J * 32 + k;
+        const float4 h = sh[wb][k], l = sl[wb][k];
+        const float dx = (h.x - xh) + (l.x - xl);
+        const float dy = (h.y - yh) + (l.y - yl);
+        const float dz = (h.z - zh) + (l.z - zl);
+        int excl = (vi && j < n && (I < J || k > lane)) ? PMGPU_EXCL_NONE : PMGPU_EXCL_FULL;
+        if (excl == PMGPU_EXCL_NONE && j >= er.x && j <= er.y)
+          excl = excl_class_of(ex_start, ex_partner, ex_class, i, j);
+        const bool use = excl != PMGPU_EXCL_FULL;
+        const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
+        const float rinv = rsqrt_nr(r2);
+        const float rr2 = rinv * rinv;
+        float f = 0;
+        if (LJ) {
+          float A, B;
+          if (COMB) {
+            const float2 cj = sc[wb][k];
+            const float rm = ci.y + cj.y, e = ci.x * cj.x;
+            const float rm2 = rm * rm, rm6 = rm2 * rm2 * rm2;
+            B = 2.0f * e * rm6;
+            A = e * rm6 * rm6;
+          } else {
+            A = tab[u].x;
+            B = tab[u].y;
+          }
+          if (excl == PMGPU_EXCL_MODIFIED) {
+            const float4 m = __ldg(&lj32[ti * ntypes + __float_as_int(l.w)]);
+            A = m.z;
+            B = m.w;
+          }
+          const float r6 = rr2 * rr2 * rr2;
+          const float r6B = B * r6, r12A = A * r6 * r6;
+          if (EM && use) elj += (double)(r12A - r6B);
+          f += (12.0f * r12A - 6.0f * r6B) * rr2;
+        }
+        if (COUL) {
+          float en = qi * h.w * rinv;
+          if (excl == PMGPU_EXCL_MODIFIED) en *= csf;
+          if (EM && use) ec += (double)en;
+          f += en * rr2;
+        }
+        f = use ? f : 0.0f;
+        fx -= dx * f; fy -= dy * f; fz -= dz * f;
+        gx[u] = dx * f; gy[u] = dy * f; gz[u] = dz * f;
+        if (EM == 2) {
+          const double df = (double)f;
+          v[0] += dx * dx * df; v[1] += dx * dy * df; v[2] += dx * dz * df;
+          v[3] += dy * dy * df; v[4] += dy * dz * df; v[5] += dz * dz * df;
+        }
+      }
+      const float sx = warp_tsum8(gx, lane), sy = warp_tsum8(gy, lane),
+                  sz = warp_tsum8(gz, lane);
+      const int jt = J * 32 + g * 8 + (lane >> 2);
+      if ((lane & 3) == 0 && jt < n) {
+        red_add(&force[jt], to_fixed((double)sx, kForceScale));
+        red_add(&force[n + jt], to_fixed((double)sy, kForceScale));
+        red_add(&force[2 * n + jt], to_fixed((double)sz, kForceScale));
+      }
+    }
+    if (vi) {
+      red_add(&force[i], to_fixed((double)fx, kForceScale));
+      red_add(&force[n + i], to_fixed((double)fy, kForceScale));
+      red_add(&force[2 * n + i], to_fixed((double)fz, kForceScale));
+    }
+    __syncwarp();
+  }
+  if (!EM) return;
+  elj = warp_sum(elj);
+  ec = warp_sum(ec);
+  if (EM == 2)
+    for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
+  if (lane == 0) {
+    if (LJ) red_add(&acc[ACC_LJ], to_fixed(elj, kEnergyScale));
+    if (COUL) red_add(&acc[ACC_COULOMB], to_fixed(ec, kEnergyScale));
+    if (EM == 2) {
+      const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+      for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
+    }
+  }
+}
+
+void allpairs_grid(int n, dim3 *grid, int *jchunk) {
+  static int sms[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int &m = sms[dev & 63];
+  if (m <= 0 && (cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+                 m <= 0))
+    m = 148;
+  const int iblocks = (n + kApAtoms - 1) / kApAtoms;
+  const int want = kApBlocksPerSm * m;
+  int chunks = std::max(1, std::min((want + iblocks - 1) / iblocks, (n + kApTile - 1) / kApTile));
+  *jchunk = (n + chunks - 1) / chunks;
+  chunks = (n + *jchunk - 1) / *jchunk;
+  *grid = dim3(iblocks, chunks);
+}
+
+void halfpairs_grid(int n, int *tiles, long long *items, int *blocks) {
+  static int sms[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int &m = sms[dev & 63];
+  if (m <= 0 && (cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+                 m <= 0))
+    m = 148;
+  const int t = (n + 31) / 32;
+  *tiles = t;
+  *items = (long long)t * (t + 1) / 2;
+  const long long warps = std::max(1LL, std::min(*items, (long long)kHpWarpsPerSm * m));
+  *blocks = (int)((warps + kHpWarps - 1) / kHpWarps);
+}
+
 // em: 0 forces only, 1 + energies, 2 + energies and virial.
 int nb_simplefull(System *s, int lj, int coul, int em) {
   const int n = s->n;
@@ -1217,10 +1393,36 @@ int nb_simplefull(System *s, int lj, int coul, int em) {
                                           csf, s->d_force, s->d_acc, em);
   };
   if (s->precision == PMGPU_PREC_MIXED) {
-    const float csf = (float)s->coulomb_scaling;
-    if (lj && coul) go(k_simplefull<float, true, true>, csf);
-    else if (lj) go(k_simplefull<float, true, false>, csf);
-    else go(k_simplefull<float, false, true>, csf);
+    int tiles, blocks;
+    long long items;
+    halfpairs_grid(n, &tiles, &items, &blocks);
+    auto go32 = [&](auto kern) {
+      kern<<<blocks, kHpWarps * 32, 0, s->stream>>>(
+          n, tiles, items, s->d_pos, s->d_charge, s->d_type, s->ntypes, s->d_ljab,
+          s->d_ljcomb, s->d_lj32, s->d_excl_range, s->d_excl_start, s->d_excl_partner,
+          s->d_excl_class, (float)s->coulomb_scaling, s->d_force, s->d_acc);
+    };
+    auto by_em = [&](auto k0, auto k1, auto k2) {
+      if (em == 0) go32(k0);
+      else if (em == 1) go32(k1);
+      else go32(k2);
+    };
+    const bool comb = s->d_ljcomb != nullptr;
+    if (lj && coul) {
+      if (comb) by_em(k_simplefull_half<true, true, true, 0>, k_simplefull_half<true, true, true, 1>,
+                      k_simplefull_half<true, true, true, 2>);
+      else by_em(k_simplefull_half<true, true, false, 0>, k_simplefull_half<true, true, false, 1>,
+                 k_simplefull_half<true, true, false, 2>);
+    } else if (lj) {
+      if (comb) by_em(k_simplefull_half<true, false, true, 0>,
+                      k_simplefull_half<true, false, true, 1>,
+                      k_simplefull_half<true, false, true, 2>);
+      else by_em(k_simplefull_half<true, false, false, 0>, k_simplefull_half<true, false, false, 1>,
+                 k_simplefull_half<true, false, false, 2>);
+    } else {
+      by_em(k_simplefull_half<false, true, false, 0>, k_simplefull_half<false, true, false, 1>,
+            k_simplefull_half<false, true, false, 2>);
+    }
   } else {
     const double csf = s->coulomb_scaling;
     if (lj && coul) go(k_simplefull<double, true, true>, csf);

@@ -88,13 +88,6 @@ __device__ __forceinline__ double exact_r2(const PairArgs<Real> &a, int oi, int 
 
 __device__ __forceinline__ float fast_exp(float x) { return __expf(x); }
 __device__ __forceinline__ double fast_exp(double x) { return exp(x); }
-// rsqrt with one Newton step: the bare MUFU estimate carries a small bias
-// that would otherwise show in the summed forces.
-__device__ __forceinline__ float rsqrt_nr(float x) {
-  float y = rsqrtf(x);
-  return y * (1.5f - 0.5f * x * y * y);
-}
-__device__ __forceinline__ double rsqrt_nr(double x) { return 1.0 / sqrt(x); }
 
 template <typename Real>
 __device__ __forceinline__ void apply_switch(const SwitchDev<Real> &sw,

@@ -118,6 +118,63 @@ static __constant__ double c_cn_dsw[5][7] = {
 __device__ __forceinline__ float pm_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double pm_sqrt(double x) { return sqrt(x); }
 
+// rsqrt with one Newton step: the bare MUFU estimate carries a small bias
+// that would otherwise show in the summed forces.
+__device__ __forceinline__ float rsqrt_nr(float x) {
+  float y = rsqrtf(x);
+  return y * (1.5f - 0.5f * x * y * y);
+}
+__device__ __forceinline__ double rsqrt_nr(double x) { return 1.0 / sqrt(x); }
+
+// 1/x from the hardware estimate refined by one Newton step,
+// y' = y + y (1 - x y); within about one ulp for normal positive x.
+__device__ __forceinline__ float rcp_nr(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return fmaf(y, fmaf(-x, y, 1.0f), y);
+}
+
+// Sums v[0..7] over the 32 lanes of a warp by a transposed butterfly
+// (9 shuffles): each exchange step hands half of the remaining slots to the
+// partner lane, so lane l ends with the total of slot (l >> 2) & 7, as do
+// the other three lanes of its quad.  The order of the additions is fixed.
+__device__ __forceinline__ float warp_tsum8(const float (&v)[8], int lane) {
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  float a[4], b[2];
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+    a[m] = (b4 ? v[m + 4] : v[m]) + __shfl_xor_sync(0xffffffffu, b4 ? v[m] : v[m + 4], 16);
+#pragma unroll
+  for (int m = 0; m < 2; m++)
+    b[m] = (b3 ? a[m + 2] : a[m]) + __shfl_xor_sync(0xffffffffu, b3 ? a[m] : a[m + 2], 8);
+  float c = (b2 ? b[1] : b[0]) + __shfl_xor_sync(0xffffffffu, b2 ? b[0] : b[1], 4);
+  c += __shfl_xor_sync(0xffffffffu, c, 2);
+  c += __shfl_xor_sync(0xffffffffu, c, 1);
+  return c;
+}
+
+// Work item w of the half all-pairs sweep: the tile pairs (I, J), I <= J,
+// of `tiles` 32-atom tiles, numbered row by row (row I holds J = I..tiles-1).
+__device__ __forceinline__ void tile_pair_of(long long w, int tiles, int *I, int *J) {
+  const double t2 = 2.0 * tiles + 1.0;
+  int r = (int)((t2 - sqrt(t2 * t2 - 8.0 * (double)w)) * 0.5);
+  r = max(0, min(r, tiles - 1));
+  auto start = [&](long long q) { return q * tiles - q * (q - 1) / 2; };
+  while (r > 0 && start(r) > w) r--;
+  while (r + 1 < tiles && start(r + 1) <= w) r++;
+  *I = r;
+  *J = r + (int)(w - start(r));
+}
+
+// An FP64 coordinate as an FP32 pair: hi = x rounded, lo = x - hi rounded,
+// so hi + lo carries 48 significant bits and a difference of two such
+// pairs, (hj - hi) + (lj - li), is as good as the FP64 difference rounded
+// to FP32.
+__device__ __forceinline__ void split_hilo(double x, float &hi, float &lo) {
+  hi = (float)x;
+  lo = (float)(x - (double)hi);
+}
+
 template <typename Real>
 __device__ __forceinline__ void switch_eval(const SwitchDev<Real> &w, Real r2,
                                             Real &val, Real &der) {

@@ -237,6 +237,8 @@ struct System {
   double *d_charge = nullptr, *d_mass = nullptr;
   int *d_type = nullptr, *d_mol = nullptr;
   float4 *d_lj32 = nullptr;     // ntypes^2: A, B, A14, B14 (FP32)
+  float2 *d_ljab = nullptr;     // ntypes^2 by column: [t2 * ntypes + t1] = A, B of (t1, t2)
+  float2 *d_ljcomb = nullptr;   // per type sqrt(epsilon), rmin/2 when the table follows the CHARMM rule
   double4 *d_lj64 = nullptr;    // ntypes^2 (FP64)
   int *d_excl_start = nullptr, *d_excl_partner = nullptr;  // CSR
   int *d_excl_class = nullptr;
@@ -324,6 +326,21 @@ int nb_build(System *s, NeighborList *nl);
 int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode);
 int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
 int nb_simplefull(System *s, int lj, int coul, int em);
+// Launch shape of the FP32 all-pairs passes (simple-full and GB): blocks
+// of kApAtoms accumulating atoms (one per thread) times chunks of partner
+// atoms, sized so every SM holds about kApBlocksPerSm blocks; partners are
+// staged kApTile at a time.
+constexpr int kApAtoms = 128;
+constexpr int kApTile = 32;
+constexpr int kApBlocksPerSm = 4;
+void allpairs_grid(int n, dim3 *grid, int *jchunk);
+// Launch shape of the FP32 half all-pairs passes (each unordered pair once,
+// forces to both atoms): one warp per 32 x 32 tile pair (I <= J), blocks of
+// kHpWarps warps striding over the tile pairs, at most kHpWarpsPerSm warps
+// per SM.
+constexpr int kHpWarps = 4;
+constexpr int kHpWarpsPerSm = 16;
+void halfpairs_grid(int n, int *tiles, long long *items, int *blocks);
 
 // pme.cu
 int pme_init(System *s, Force *f);

@@ -278,3 +278,46 @@ def test_list_follows_uploaded_positions(ctx):
         assert err <= RMS_MIXED, (k, err)
     assert force.stats()["list_builds"] >= 4
     gs.close()
+
+
+@pytest.mark.parametrize("table", ["charmm_rule", "nbfix"])
+def test_polymer_all_pairs_vs_oracle(ctx, table):
+    """GB, LJ and Coulomb all pairs of a 700-atom heteropolymer (one LJ type
+    per atom) in the mixed FP32 form against the FP64 oracle.  Its table
+    follows the CHARMM rule, so the LJ pass computes (A, B) from per-type
+    parameters; "nbfix" scales the (A, B) of one off-diagonal pair in every
+    seventh row, which the rule cannot express, so the pass reads the table."""
+    import oracle
+    from protomol_b200 import systems
+    sm = systems.gb_polymer(700, seed=5)
+    if table == "nbfix":
+        lj = sm.lj.copy()
+        nt = lj.shape[0]
+        for t in range(0, nt, 7):
+            u = (13 * t + 5) % nt
+            if u != t:
+                lj[t, u, :2] *= 1.25
+                lj[u, t, :2] = lj[t, u, :2]
+        sm.lj = lj
+    s = oracle.System(pos=sm.pos, charge=sm.charge, type=sm.type, molecule=sm.molecule,
+                      lj=sm.lj, excl=sm.exclusions, periodic=False, box=sm.box, mass=sm.mass,
+                      water=sm.water, gb_vdwr=sm.gb_vdwr, gb_scale=sm.gb_scale,
+                      gb_offset=sm.gb_offset, gb_obc=sm.gb_obc)
+    gs = GpuSystem(ctx, sm, "mixed")
+    ff = ForceFactory(gs)
+    rf, re, _ = oracle.gb_force(s, 1.0, 78.5)
+    f, e = _eval(ff.make("GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 "
+                         "-solventDielec 78.5"), sm)
+    assert F.rms_rel(f, rf) <= RMS_MIXED, F.rms_rel(f, rf)
+    assert _energy_ok(e[0], re)
+    for line, pot, slot, key in (("LennardJones -algorithm NonbondedSimpleFull", "LennardJones",
+                                  1, "lj"),
+                                 ("Coulomb -algorithm NonbondedSimpleFull", "Coulomb", 0,
+                                  "coulomb")):
+        rf, re, rv = oracle.simplefull_force(s, pot)
+        f, e = _eval(ff.make(line), sm)
+        assert F.rms_rel(f, rf) <= RMS_MIXED, (line, F.rms_rel(f, rf))
+        assert _energy_ok(e[slot], re[key]), (line, e[slot], re[key])
+        vir_err = np.abs(e[7:16] - rv.ravel()).max() / max(np.abs(rv).max(), 1)
+        assert vir_err <= 1e-5, (line, vir_err)
+    gs.close()
