@@ -226,7 +226,8 @@ static int system_free(System *s) {
                   s->d_gb_vdwr, s->d_gb_scale, s->d_gb_offset, s->d_water, s->d_gb_born,
                   s->d_gb_psi, s->d_gb_partial, s->d_gb_fixed, s->d_pos, s->d_vel,
                   s->d_force, s->d_acc, s->d_status, s->d_pairbuf, s->d_paircount,
-                  s->d_stage, s->d_snap, s->d_step};
+                  s->d_stage, s->d_snap, s->d_step, s->d_sf_tile,
+                  s->d_sf_bits};
   for (auto &g : s->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (void *p : ptrs) dev_free(s, p);
@@ -337,6 +338,17 @@ static int evaluate_forces(System *s, int only, int mode) {
       sf_lj |= f.sf_lj;
       sf_coul |= f.sf_coul;
     }
+  int bd_bonds = 0, bd_angles = 0, bd_dihedrals = 0, bd_impropers = 0, bd_done = 0;
+  for (auto &f : s->forces) {
+    if (only >= 0 ? f.id != only : !f.enabled) continue;
+    if (f.kind == FK_BONDED) {
+      bd_bonds |= f.bonds;
+      bd_angles |= f.angles;
+    } else if (f.kind == FK_TORSION) {
+      bd_dihedrals |= f.dihedrals;
+      bd_impropers |= f.impropers;
+    }
+  }
   for (auto &f : s->forces) {
     if (only >= 0 ? f.id != only : !f.enabled) continue;
     if (f.kind == FK_CUTOFF || (f.kind == FK_PME && (f.ewald_flags & PMGPU_EWALD_REAL)))
@@ -350,6 +362,18 @@ static int evaluate_forces(System *s, int only, int mode) {
   // once, while the list work of the step leaves most of the device idle.
   // The second stream has the higher priority, so its short dependent
   // kernels are not queued behind the pair kernel's blocks.
+  // the all-pairs passes read the FP32 pair records of the positions,
+  // written by this step's update kernel or here
+  bool need_rec = false;
+  for (auto &f : s->forces) {
+    if (only >= 0 ? f.id != only : !f.enabled) continue;
+    need_rec |= f.kind == FK_SIMPLEFULL || f.kind == FK_GB;
+  }
+  if (need_rec && s->precision == PMGPU_PREC_MIXED && !s->rec_fresh) {
+    PM_CHECK(nb_stage_pairs(s));
+    s->kernels += s->n > 0;
+  }
+  s->rec_fresh = 0;
   const bool fork = s->side && !s->prof.enabled;
   const cudaStream_t main_stream = s->stream;
   if (fork) {
@@ -371,9 +395,17 @@ static int evaluate_forces(System *s, int only, int mode) {
     }
   } join{s, main_stream, fork};
   {
-    if (fork) s->stream = s->side;
+    // GB's passes and the PME chain are long dependent chains and take the
+    // second stream; the all-pairs terms go beside them on the main stream,
+    // and so do the bonded terms when the main stream has no list work
+    const bool main_idle = s->lists.empty();
     for (auto &f : s->forces) {
       if (only >= 0 ? f.id != only : !f.enabled) continue;
+      if (fork)
+        s->stream = f.kind == FK_SIMPLEFULL ||
+                            (main_idle && f.kind != FK_GB && f.kind != FK_PME)
+                        ? main_stream
+                        : s->side;
       int r = PMGPU_OK;
       switch (f.kind) {
         case FK_PME:
@@ -400,29 +432,24 @@ static int evaluate_forces(System *s, int only, int mode) {
           s->kernels += s->precision == PMGPU_PREC_MIXED ? 4 : 5;
           break;
         case FK_BONDED:
+        case FK_TORSION: {
+          // the bonded terms of every selected force share one launch
+          if (bd_done) break;
+          bd_done = 1;
+          int launched = 0;
           prof_begin(s, PMGPU_PHASE_BONDED);
-          r = bonded_forces(s, &f, em);
+          r = bonded_all(s, bd_bonds, bd_angles, bd_dihedrals, bd_impropers, em, &launched);
           prof_end(s);
-          s->kernels += (f.bonds && s->n_bonds > 0) + (f.angles && s->n_angles > 0);
+          s->kernels += launched;
           break;
-        case FK_TORSION:
-          prof_begin(s, PMGPU_PHASE_BONDED);
-          r = torsion_forces(s, &f, em);
-          prof_end(s);
-          s->kernels +=
-              (f.dihedrals && s->n_dihedrals > 0) + (f.impropers && s->n_impropers > 0);
-          break;
+        }
         case FK_SIMPLEFULL:
           // all enabled simple-full terms share one all-pairs pass
-          // on the main stream, beside the dependent chains of the second
-          // stream (GB's three passes, PME)
           if (sf_done) break;
           sf_done = 1;
           prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
-          if (fork) s->stream = main_stream;
           r = nb_simplefull(s, only >= 0 ? f.sf_lj : sf_lj, only >= 0 ? f.sf_coul : sf_coul,
                             em);
-          if (fork) s->stream = s->side;
           prof_end(s);
           s->kernels += 1;
           break;
@@ -728,6 +755,7 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   }
   PM_CHECK(upload(s.get(), &s->d_excl_pairs, table.data(), 3 * (size_t)ne));
   s->n_excl = ne;
+  s->h_excl.assign(t->exclusions, t->exclusions + 3 * (size_t)ne);
   s->n_bonds = std::max(0, t->n_bonds);
   s->n_angles = std::max(0, t->n_angles);
   if (s->n_bonds && (!t->bond_atoms || !t->bond_params))
@@ -762,7 +790,7 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   PM_CHECK(upload(s.get(), &s->d_force, (const long long *)nullptr, 3 * nn));
   PM_CHECK(upload(s.get(), &s->d_acc, (const long long *)nullptr, ACC_COUNT));
   PM_CHECK(upload(s.get(), &s->d_status, (const int *)nullptr, 1));
-  PM_CHECK(upload(s.get(), &s->d_step, (const unsigned long long *)nullptr, 1));
+  PM_CHECK(upload(s.get(), &s->d_step, (const unsigned long long *)nullptr, 2));  // step, blocks done
   PM_CHECK(upload(s.get(), &s->d_stage, (const double *)nullptr, 3 * nn));
   PM_CUDA(cudaMallocHost(&s->h_acc, sizeof(long long) * ACC_COUNT));
   PM_CUDA(cudaMallocHost(&s->h_status, sizeof(int)));
@@ -968,6 +996,10 @@ int pmgpu_force_simplefull_add(pmgpu_system *h, int lj, int coulomb, int *force_
   if (s->box.periodic)
     return fail(PMGPU_ERR_UNSUPPORTED, "NonbondedSimpleFull is the vacuum all-pairs path");
   if (!lj && !coulomb) return fail(PMGPU_ERR_ARG, "need LennardJones and/or Coulomb");
+  if (s->precision == PMGPU_PREC_MIXED) {
+    PM_CUDA(cudaSetDevice(s->device));
+    PM_CHECK(nb_simplefull_init(s));
+  }
   Force f;
   f.kind = FK_SIMPLEFULL;
   f.sf_lj = lj ? 1 : 0;
@@ -1107,8 +1139,8 @@ static int one_step(System *s, const pmgpu_integrator *it, int phase, int mode) 
   int ri = integrate_kick_drift(s, it, phase, 1, nl);
   prof_end(s);
   PM_CHECK(ri);
-  // update (+ step counter for the Langevin noise)
-  s->kernels += (s->n > 0) + (it->kind == PMGPU_INT_LANGEVIN_LEAPFROG);
+  // the update (which also advances the step counter of the Langevin noise)
+  s->kernels += s->n > 0;
   if (s->n == 0) PM_CHECK(begin_eval(s));
   return evaluate_forces(s, -1, mode);
 }

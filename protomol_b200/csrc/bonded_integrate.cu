@@ -7,11 +7,12 @@
 namespace pmgpu {
 
 // BondSystemForce::calcBond (force/bonded/BondSystemForce.h:89-124).
-__global__ void k_bonds(Box box, int nb, const int *__restrict__ atoms,
-                        const double *__restrict__ prm, const double *__restrict__ pos,
-                        int n, long long *__restrict__ force, long long *__restrict__ acc,
-                        int em) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void bond_term(int b, const Box &box, int nb,
+                                          const int *__restrict__ atoms,
+                                          const double *__restrict__ prm,
+                                          const double *__restrict__ pos, int n,
+                                          long long *__restrict__ force,
+                                          long long *__restrict__ acc, int em) {
   double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
   if (b < nb) {
     int a1 = atoms[2 * b], a2 = atoms[2 * b + 1];
@@ -51,11 +52,12 @@ __global__ void k_bonds(Box box, int nb, const int *__restrict__ atoms,
 
 // AngleSystemForce::calcAngle (force/bonded/AngleSystemForce.h:86-171),
 // harmonic angle plus Urey-Bradley.
-__global__ void k_angles(Box box, int na, const int *__restrict__ atoms,
-                         const double *__restrict__ prm, const double *__restrict__ pos,
-                         int n, long long *__restrict__ force, long long *__restrict__ acc,
-                         int em) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void angle_term(int t, const Box &box, int na,
+                                           const int *__restrict__ atoms,
+                                           const double *__restrict__ prm,
+                                           const double *__restrict__ pos, int n,
+                                           long long *__restrict__ force,
+                                           long long *__restrict__ acc, int em) {
   double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
   if (t < na) {
     int a1 = atoms[3 * t], a2 = atoms[3 * t + 1], a3 = atoms[3 * t + 2];
@@ -129,11 +131,12 @@ __device__ __forceinline__ double ddot(const double *u, const double *v) {
 // and (2,3,4) planes; the gradient goes through d cos(phi) when
 // |sin phi| > 0.1 and through d sin(phi) otherwise.  params: k,
 // periodicity n, phase delta; n > 0 cosine form, n == 0 harmonic.
-__global__ void k_torsions(Box box, int nt, const int *__restrict__ atoms,
-                           const double *__restrict__ prm, const double *__restrict__ pos,
-                           int n, long long *__restrict__ force, long long *__restrict__ acc,
-                           int slot, int em) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void torsion_term(int t, const Box &box, int nt,
+                                             const int *__restrict__ atoms,
+                                             const double *__restrict__ prm,
+                                             const double *__restrict__ pos, int n,
+                                             long long *__restrict__ force,
+                                             long long *__restrict__ acc, int slot, int em) {
   double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
   if (t < nt) {
     const int a1 = atoms[4 * t], a2 = atoms[4 * t + 1], a3 = atoms[4 * t + 2],
@@ -233,30 +236,63 @@ __global__ void k_torsions(Box box, int nt, const int *__restrict__ atoms,
   }
 }
 
-int torsion_forces(System *s, Force *f, int em) {
-  if (f->dihedrals && s->n_dihedrals > 0)
-    k_torsions<<<(s->n_dihedrals + 127) / 128, 128, 0, s->stream>>>(
-        s->box, s->n_dihedrals, s->d_dihedral_atoms, s->d_dihedral_params, s->d_pos, s->n,
-        s->d_force, s->d_acc, ACC_DIHEDRAL, em);
-  if (f->impropers && s->n_impropers > 0)
-    k_torsions<<<(s->n_impropers + 127) / 128, 128, 0, s->stream>>>(
-        s->box, s->n_impropers, s->d_improper_atoms, s->d_improper_params, s->d_pos, s->n,
-        s->d_force, s->d_acc, ACC_IMPROPER, em);
-  PM_CUDA(cudaGetLastError());
-  return PMGPU_OK;
+// All bonded terms of an evaluation in one launch: whole 128-thread blocks
+// of bonds, then angles, dihedrals and impropers, so every warp holds one
+// kind of term (its energy reduction stays per warp).
+constexpr int kBondedThreads = 128;
+struct BondedLaunch {
+  int nb, na, nd, ni;          // terms of each kind in this launch (0: none)
+  int bb, ab, db;              // blocks of bonds, angles, dihedrals
+};
+
+__global__ void __launch_bounds__(kBondedThreads)
+k_bonded(BondedLaunch L, Box box, const int *__restrict__ bond_atoms,
+         const double *__restrict__ bond_prm, const int *__restrict__ angle_atoms,
+         const double *__restrict__ angle_prm, const int *__restrict__ dih_atoms,
+         const double *__restrict__ dih_prm, const int *__restrict__ imp_atoms,
+         const double *__restrict__ imp_prm, const double *__restrict__ pos, int n,
+         long long *__restrict__ force, long long *__restrict__ acc, int em) {
+  int blk = blockIdx.x;
+  if (blk < L.bb) {
+    bond_term(blk * kBondedThreads + threadIdx.x, box, L.nb, bond_atoms, bond_prm, pos, n,
+              force, acc, em);
+    return;
+  }
+  blk -= L.bb;
+  if (blk < L.ab) {
+    angle_term(blk * kBondedThreads + threadIdx.x, box, L.na, angle_atoms, angle_prm, pos, n,
+               force, acc, em);
+    return;
+  }
+  blk -= L.ab;
+  if (blk < L.db) {
+    torsion_term(blk * kBondedThreads + threadIdx.x, box, L.nd, dih_atoms, dih_prm, pos, n,
+                 force, acc, ACC_DIHEDRAL, em);
+    return;
+  }
+  blk -= L.db;
+  torsion_term(blk * kBondedThreads + threadIdx.x, box, L.ni, imp_atoms, imp_prm, pos, n, force,
+               acc, ACC_IMPROPER, em);
 }
 
-int bonded_forces(System *s, Force *f, int em) {
-  if (f->bonds && s->n_bonds > 0) {
-    k_bonds<<<(s->n_bonds + 127) / 128, 128, 0, s->stream>>>(
-        s->box, s->n_bonds, s->d_bond_atoms, s->d_bond_params, s->d_pos, s->n,
-        s->d_force, s->d_acc, em);
-  }
-  if (f->angles && s->n_angles > 0) {
-    k_angles<<<(s->n_angles + 127) / 128, 128, 0, s->stream>>>(
-        s->box, s->n_angles, s->d_angle_atoms, s->d_angle_params, s->d_pos, s->n,
-        s->d_force, s->d_acc, em);
-  }
+int bonded_all(System *s, int bonds, int angles, int dihedrals, int impropers, int em,
+               int *launched) {
+  BondedLaunch L;
+  L.nb = bonds ? s->n_bonds : 0;
+  L.na = angles ? s->n_angles : 0;
+  L.nd = dihedrals ? s->n_dihedrals : 0;
+  L.ni = impropers ? s->n_impropers : 0;
+  auto blocks = [](int k) { return (k + kBondedThreads - 1) / kBondedThreads; };
+  L.bb = blocks(L.nb);
+  L.ab = blocks(L.na);
+  L.db = blocks(L.nd);
+  const int total = L.bb + L.ab + L.db + blocks(L.ni);
+  *launched = total > 0;
+  if (!total) return PMGPU_OK;
+  k_bonded<<<total, kBondedThreads, 0, s->stream>>>(
+      L, s->box, s->d_bond_atoms, s->d_bond_params, s->d_angle_atoms, s->d_angle_params,
+      s->d_dihedral_atoms, s->d_dihedral_params, s->d_improper_atoms, s->d_improper_params,
+      s->d_pos, s->n, s->d_force, s->d_acc, em);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
@@ -324,9 +360,12 @@ struct UpdateArgs {
   // Langevin (LangevinLeapfrogIntegrator.cpp:44-71)
   double vdt, fdt, ndt, fc;
   uint64_t seed;
-  // (step, half) of each kick's noise: step = *step_ptr + kstep_off[k].  The
-  // step counter lives in device memory so captured graphs stay valid.
-  const unsigned long long *step_ptr;
+  // (step, half) of each kick's noise: step = step_ptr[0] + kstep_off[k].  The
+  // step counter lives in device memory so captured graphs stay valid; with
+  // step_inc the last block of the launch advances it (step_ptr[1] counts
+  // the blocks done).
+  unsigned long long *step_ptr;
+  int step_inc;
   int kstep_off[2];
   int khalf[2];
   long long *acc_zero;  // energy accumulators cleared by this launch (or null)
@@ -336,10 +375,12 @@ struct UpdateArgs {
   unsigned *ticket;
   int *rebuild;
   float half_skin2;
+  // the FP32 pair records of the drifted positions (null: none)
+  float4 *rec;
+  const double *charge;
+  const int *type;
 };
 
-// Advances the device step counter (after the drift of a step).
-__global__ void k_step_inc(unsigned long long *step) { *step += 1ull; }
 __global__ void k_step_set(unsigned long long *step, unsigned long long v) { *step = v; }
 
 int set_device_step(System *s) {
@@ -348,7 +389,7 @@ int set_device_step(System *s) {
   return PMGPU_OK;
 }
 
-constexpr int kUpdateThreads = 256;
+constexpr int kUpdateThreads = 64;  // small blocks: the update is latency-bound FP64 work
 __global__ void __launch_bounds__(kUpdateThreads)
 k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos,
          double *__restrict__ vel, long long *__restrict__ force, int *__restrict__ status) {
@@ -386,11 +427,28 @@ k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos
         }
       }
       d2 = (float)dd;
+      if (a.rec)
+        write_pair_record(a.rec, a.n, i, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2],
+                          a.charge[i], a.type[i]);
     }
     if (a.zero_force)
       for (int c = 0; c < 3; c++) force[c * a.n + i] = 0;
   }
   if (a.xbuild) rebuild_decide<kUpdateThreads>(d2, a.ticket, a.rebuild, a.half_skin2, 0);
+  if (a.step_inc) {
+    // every block has read the counter before it counts itself done
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      last = atomicAdd(&a.step_ptr[1], 1ull) == (unsigned long long)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+      a.step_ptr[1] = 0ull;
+      a.step_ptr[0] += 1ull;
+    }
+  }
 }
 
 // phase: 0 = leapfrog first (half kick + drift), 1 = leapfrog middle (kick +
@@ -407,6 +465,9 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int z
   // StandardIntegrator::run gives every step two half kicks; the noise of
   // kick (step, half) is Philox(seed; atom, step, half).
   a.step_ptr = s->d_step;
+  // only the Langevin noise reads the device step counter (every run sets
+  // it from the host counter first); it advances after the drift of a step
+  a.step_inc = a.langevin && s->n > 0;
   a.acc_zero = zero_acc ? s->d_acc : nullptr;
   a.xbuild = nullptr;
   a.ticket = nullptr;
@@ -440,6 +501,12 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int z
       break;
     default: return fail(PMGPU_ERR_ARG, "bad integrator phase");
   }
+  a.step_inc = a.step_inc && a.drift;
+  // the pair records of the all-pairs passes, from the drifted positions
+  a.rec = a.drift && s->d_rec && s->precision == PMGPU_PREC_MIXED ? s->d_rec : nullptr;
+  a.charge = s->d_charge;
+  a.type = s->d_type;
+  s->rec_fresh = a.rec != nullptr;
   if (list && list->built && a.drift && s->n) {
     const float hs = (float)(0.5 * list->skin);
     a.xbuild = list->d_xbuild;
@@ -451,9 +518,6 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int z
   if (s->n)
     k_update<<<(s->n + kUpdateThreads - 1) / kUpdateThreads, kUpdateThreads, 0, s->stream>>>(
         a, s->d_mass, s->d_pos, s->d_vel, s->d_force, s->d_status);
-  // only the Langevin noise reads the device step counter (every run sets
-  // it from the host counter first)
-  if (a.drift && a.langevin) k_step_inc<<<1, 1, 0, s->stream>>>(s->d_step);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }

@@ -40,6 +40,11 @@ struct GbArgs {
   double *born, *partial;
   double *psi;  // per atom dR/d(burial sum) factor of the force pass
   long long *force, *acc;
+  // FP32 passes: pair records (write_pair_record), static records
+  // (k_gb_static) and the per-evaluation radius records (born, 1 / born,
+  // dR/d(burial sum), q^2 / (2 born^2)) from k_gb_radii
+  const float4 *rec, *gst;
+  float4 *grad;
 };
 
 template <typename Real>
@@ -117,8 +122,14 @@ __global__ void k_gb_radii(GbArgs a) {
     // dR_i/d(burial sum) (GBForce.cpp:108-118 without the pair factor dBT):
     // R_i^2 rho~_i (1 - tanh^2) (alpha - 2 beta psi + 3 gamma psi^2) / rho_i
     double td = a.alpha - 2.0 * a.beta * psi + 3.0 * a.gamma * psi * psi;
-    a.psi[i] = born * born * oi * (1.0 - th * th) * td / ri;
+    const double dfac = born * born * oi * (1.0 - th * th) * td / ri;
+    a.psi[i] = dfac;
     a.born[i] = born;
+    if (a.grad) {
+      const double q = a.charge[i];
+      a.grad[i] = make_float4((float)born, (float)(1.0 / born), (float)dfac,
+                              (float)(0.5 * q * q / (born * born)));
+    }
     a.burial_fx[i] = 0;
     a.partial_fx[i] = 0;
     if (a.n > 1) {
@@ -272,17 +283,58 @@ __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
 }
 
 // ---------------------------------------------------------------------
-// FP32 forms of the three all-pairs passes.  One accumulating atom per
-// thread (kApAtoms per block) against a chunk of partner atoms staged
-// kApTile at a time as broadcast float4 records with hi/lo FP32
-// coordinates, so the pair loops take no FP64 operation or conversion.
-// Reciprocals come from the hardware estimate plus one Newton step and
-// every distance from one rsqrt; the self pair is masked rather than
-// skipped.  Sums are kept per partner tile in FP32 and carried in FP64.
+// FP32 forms of the three all-pairs passes, each over every unordered pair
+// once in 32 x 32 tile pairs (see k_gb_burial_half).  Atom records are
+// staged with hi/lo FP32 coordinates, so the pair loops take no FP64
+// operation or conversion; reciprocals come from the hardware estimate plus
+// one Newton step and every distance from one rsqrt; pairs outside the
+// half set are masked rather than skipped.
+
+// Far pairs.  When d - s >= o_i (s = S_j o_j), L = d - s and U = d + s,
+// dL = dU = 1 and dC = 0, and with t = s / d the closed forms reduce to odd
+// power series (their Taylor expansions in t, all terms of one sign):
+//   term  = (1/d)   sum_k 2k/(2k+1)        t^(2k+1)
+//   dBT   = -(1/d^2) sum_k 2k(k+1)/(2k+1)  t^(2k+1),   k = 1, 2, ...
+// For t <= 1/4 eight terms leave a relative truncation below 2e-9, and
+// unlike the closed forms, whose terms cancel to O(t^3) of their size, the
+// series keeps full FP32 precision.  It needs no reciprocal or logarithm.
+constexpr float kGbFarT = 0.25f;
+
+__device__ __forceinline__ bool gb_far(float dist, float oi, float sjoj) {
+  return dist - sjoj >= oi && sjoj <= kGbFarT * dist;
+}
+
+// sum_{k=1..8} 2k/(2k+1) u^(k-1)
+__device__ __forceinline__ float gb_series_term(float u) {
+  float p = 16.0f / 17.0f;
+  p = fmaf(p, u, 14.0f / 15.0f);
+  p = fmaf(p, u, 12.0f / 13.0f);
+  p = fmaf(p, u, 10.0f / 11.0f);
+  p = fmaf(p, u, 8.0f / 9.0f);
+  p = fmaf(p, u, 6.0f / 7.0f);
+  p = fmaf(p, u, 4.0f / 5.0f);
+  return fmaf(p, u, 2.0f / 3.0f);
+}
+
+// sum_{k=1..8} 2k(k+1)/(2k+1) u^(k-1)
+__device__ __forceinline__ float gb_series_dbt(float u) {
+  float p = 144.0f / 17.0f;
+  p = fmaf(p, u, 112.0f / 15.0f);
+  p = fmaf(p, u, 84.0f / 13.0f);
+  p = fmaf(p, u, 60.0f / 11.0f);
+  p = fmaf(p, u, 40.0f / 9.0f);
+  p = fmaf(p, u, 24.0f / 7.0f);
+  p = fmaf(p, u, 12.0f / 5.0f);
+  return fmaf(p, u, 4.0f / 3.0f);
+}
 
 // burial term of the "i sees j" direction given dist and 1/dist
 __device__ __forceinline__ float gb_burial_term_f32(float dist, float idist, float oi,
                                                    float ioi, float sjoj) {
+  if (gb_far(dist, oi, sjoj)) {
+    const float t = sjoj * idist, u = t * t;
+    return idist * (t * u) * gb_series_term(u);
+  }
   float L, U;
   if (oi >= dist + sjoj) {
     L = 1.0f;
@@ -301,6 +353,10 @@ __device__ __forceinline__ float gb_burial_term_f32(float dist, float idist, flo
 
 // dBT/dr of the "i sees j" direction (same terms as gb_dBT above)
 __device__ __forceinline__ float gb_dBT_f32(float dist, float idist, float oi, float sjoj) {
+  if (gb_far(dist, oi, sjoj)) {
+    const float t = sjoj * idist, u = t * t;
+    return -(idist * idist) * (t * u) * gb_series_dbt(u);
+  }
   float L, U;
   if (oi >= dist + sjoj) {
     L = 1.0f;
@@ -325,97 +381,100 @@ __device__ __forceinline__ float gb_dBT_f32(float dist, float idist, float oi, f
          0.25f * s2d * iL2 * iL * dL + dC;
 }
 
-__device__ __forceinline__ void gb_stage_pos(const double *pos, int j, float4 &h, float4 &l) {
-  split_hilo(pos[3 * j], h.x, l.x);
-  split_hilo(pos[3 * j + 1], h.y, l.y);
-  split_hilo(pos[3 * j + 2], h.z, l.z);
-}
-
-__global__ void __launch_bounds__(kApAtoms) k_gb_burial_f32(GbArgs a, int jchunk) {
-  __shared__ float4 sh[kApTile], sl[kApTile];
-  __shared__ int sw[kApTile];
-  const int i = blockIdx.x * kApAtoms + threadIdx.x;
-  const bool valid = i < a.n;
-  const int ii = valid ? i : 0;
-  float xh, yh, zh, xl, yl, zl;
-  split_hilo(a.pos[3 * ii], xh, xl);
-  split_hilo(a.pos[3 * ii + 1], yh, yl);
-  split_hilo(a.pos[3 * ii + 2], zh, zl);
-  const float oi = (float)(a.vdwr[ii] - a.offset[ii]);
-  const float ioi = rcp_nr(oi);
-  const bool active = valid && !(a.water && a.water[ii]);
-  double acc = 0.0;
-  const int j0 = blockIdx.y * jchunk, j1 = min(a.n, j0 + jchunk);
-  for (int base = j0; base < j1; base += kApTile) {
-    if (threadIdx.x < kApTile) {
-      const int j = base + threadIdx.x;
-      if (j < j1) {
-        float4 h, l;
-        gb_stage_pos(a.pos, j, h, l);
-        h.w = (float)(a.vdwr[j] - a.offset[j]);
-        l.w = (float)a.scale[j];
-        sh[threadIdx.x] = h;
-        sl[threadIdx.x] = l;
-        sw[threadIdx.x] = a.water ? a.water[j] : 0;
-      }
-    }
-    __syncthreads();
-    const int lim = min(kApTile, j1 - base);
-    if (active) {
-      float part = 0;
-#pragma unroll 2
-      for (int k = 0; k < lim; k++) {
-        const float4 h = sh[k], l = sl[k];
-        const bool use = (base + k != i) && !sw[k];
-        const float dx = (h.x - xh) + (l.x - xl);
-        const float dy = (h.y - yh) + (l.y - yl);
-        const float dz = (h.z - zh) + (l.z - zl);
-        const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
-        const float idist = rsqrt_nr(r2);
-        const float t = gb_burial_term_f32(r2 * idist, idist, oi, ioi, l.w * h.w);
-        part += use ? t : 0.0f;
-      }
-      acc += (double)part;
-    }
-    __syncthreads();
-  }
-  if (active && acc != 0.0) red_add(&a.burial_fx[i], to_fixed(acc, kGbScale));
-}
-
-// Partial sums over each unordered pair once: a warp takes one 32 x 32
-// tile pair (I, J), I <= J, lane l holding atom 32 I + l against the J atoms
-// broadcast from the warp's shared-memory slice; partialTerm[i][j] adds to
-// i in the lane and partialTerm[j][i] to j through warp_tsum8.
-__global__ void __launch_bounds__(kHpWarps * 32)
-k_gb_partial_half(GbArgs a, int tiles, long long items) {
-  __shared__ float4 sh[kHpWarps][32], sl[kHpWarps][32];
-  __shared__ float sib[kHpWarps][32];
+// Burial sums over each unordered pair once, both directions per pair: a
+// warp takes 32 x 32 tile pairs (I, J), I <= J, from its block's share; the "i
+// sees j" term adds to i in the lane, the "j sees i" term to j through
+// warp_tsum8.  Water atoms neither receive nor give burial.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+k_gb_burial_half(GbArgs a, int tiles, long long items) {
+  // per j: (x_hi, y_hi, z_hi, rho~) | (x_lo, y_lo, z_lo, S rho~) | (1 / rho~, water)
+  __shared__ float4 sh[WARPS][32], sl[WARPS][32];
+  __shared__ float2 sg[WARPS][32];
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
-  const long long nw = (long long)gridDim.x * kHpWarps;
-  for (long long w = (long long)blockIdx.x * kHpWarps + wb; w < items; w += nw) {
+  __shared__ int counter;
+  if (threadIdx.x == 0) counter = 0;
+  __syncthreads();
+  const BlockItems queue{&counter};
+  long long w;
+  for (w = queue.next(lane); w < items; w = queue.next(lane)) {
     int I, J;
     tile_pair_of(w, tiles, &I, &J);
     const int i = I * 32 + lane;
     const bool vi = i < a.n;
     const int ii = vi ? i : 0;
-    float xh, yh, zh, xl, yl, zl;
-    split_hilo(a.pos[3 * ii], xh, xl);
-    split_hilo(a.pos[3 * ii + 1], yh, yl);
-    split_hilo(a.pos[3 * ii + 2], zh, zl);
-    const float qi = (float)a.charge[ii], bi = (float)a.born[ii];
-    const float q4bi = (float)(0.25 / a.born[ii]);
+    const float4 hi = a.rec[ii], li = a.rec[a.n + ii], gi = a.gst[ii];
+    const bool ai = vi && gi.w == 0.0f;
     {
       const int j = J * 32 + lane;
       const int jj = j < a.n ? j : 0;
-      float4 h, l;
-      gb_stage_pos(a.pos, jj, h, l);
-      h.w = (float)a.charge[jj];
-      l.w = (float)a.born[jj];
-      sh[wb][lane] = h;
-      sl[wb][lane] = l;
-      sib[wb][lane] = (float)(1.0 / a.born[jj]);
+      const float4 g = a.gst[jj], h = a.rec[jj], l = a.rec[a.n + jj];
+      sh[wb][lane] = make_float4(h.x, h.y, h.z, g.x);
+      sl[wb][lane] = make_float4(l.x, l.y, l.z, g.y);
+      // past the end: unused, like water
+      sg[wb][lane] = make_float2(g.z, j < a.n ? g.w : 1.0f);
     }
     __syncwarp();
+    float bsum = 0;
+#pragma unroll 1
+    for (int g = 0; g < 4; g++) {
+      float gb[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int k = g * 8 + u;
+        const float4 h = sh[wb][k], l = sl[wb][k];
+        const float2 gj = sg[wb][k];
+        const bool use = ai && gj.y == 0.0f && (I < J || k > lane);
+        const float dx = (h.x - hi.x) + (l.x - li.x);
+        const float dy = (h.y - hi.y) + (l.y - li.y);
+        const float dz = (h.z - hi.z) + (l.z - li.z);
+        const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
+        const float idist = rsqrt_nr(r2);
+        const float dist = r2 * idist;
+        const float tij = gb_burial_term_f32(dist, idist, gi.x, gi.z, l.w);
+        const float tji = gb_burial_term_f32(dist, idist, h.w, gj.x, gi.y);
+        bsum += use ? tij : 0.0f;
+        gb[u] = use ? tji : 0.0f;
+      }
+      const float sb = warp_tsum8(gb, lane);
+      const int jt = J * 32 + g * 8 + (lane >> 2);
+      if ((lane & 3) == 0 && jt < a.n) red_add(&a.burial_fx[jt], to_fixed((double)sb, kGbScale));
+    }
+    if (ai) red_add(&a.burial_fx[i], to_fixed((double)bsum, kGbScale));
+    __syncwarp();
+  }
+}
+
+// Partial sums over each unordered pair once (same tiling):
+// partialTerm[i][j] adds to i in the lane and partialTerm[j][i] to j
+// through warp_tsum8.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+k_gb_partial_half(GbArgs a, int tiles, long long items) {
+  __shared__ float4 sh[WARPS][32], sl[WARPS][32], sr[WARPS][32];
+  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  __shared__ int counter;
+  if (threadIdx.x == 0) counter = 0;
+  __syncthreads();
+  const BlockItems queue{&counter};
+  long long w;
+  for (w = queue.next(lane); w < items; w = queue.next(lane)) {
+    int I, J;
+    tile_pair_of(w, tiles, &I, &J);
+    const int i = I * 32 + lane;
+    const bool vi = i < a.n;
+    const int ii = vi ? i : 0;
+    const float4 hi = a.rec[ii], li = a.rec[a.n + ii], ri = a.grad[ii];
+    const float q4bi = 0.25f * ri.y;
+    {
+      const int j = J * 32 + lane;
+      const int jj = j < a.n ? j : 0;
+      sh[wb][lane] = a.rec[jj];
+      sl[wb][lane] = a.rec[a.n + jj];
+      sr[wb][lane] = a.grad[jj];
+    }
+    __syncwarp();
+    const int jn = a.n - J * 32;
     float pi = 0;
 #pragma unroll 1
     for (int g = 0; g < 4; g++) {
@@ -423,21 +482,19 @@ k_gb_partial_half(GbArgs a, int tiles, long long items) {
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int k = g * 8 + u;
-        const int j = J * 32 + k;
-        const float4 h = sh[wb][k], l = sl[wb][k];
-        const float ibj = sib[wb][k];
-        const bool use = vi && j < a.n && (I < J || k > lane);
-        const float dx = (h.x - xh) + (l.x - xl);
-        const float dy = (h.y - yh) + (l.y - yl);
-        const float dz = (h.z - zh) + (l.z - zl);
+        const float4 h = sh[wb][k], l = sl[wb][k], rj = sr[wb][k];
+        const bool use = vi && k < jn && (I < J || k > lane);
+        const float dx = (h.x - hi.x) + (l.x - li.x);
+        const float dy = (h.y - hi.y) + (l.y - li.y);
+        const float dz = (h.z - hi.z) + (l.z - li.z);
         const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
-        const float bj = l.w, bb = bi * bj;
-        const float ex = __expf(-r2 * (q4bi * ibj));
+        const float bj = rj.x, bb = ri.x * bj;
+        const float ex = __expf(-r2 * (q4bi * rj.y));
         const float ifil = rsqrt_nr(r2 + bb * ex);
-        const float p = 0.5f * qi * h.w * (ifil * ifil * ifil) * ex;
+        const float p = 0.5f * hi.w * h.w * (ifil * ifil * ifil) * ex;
         // aTerm of both directions (GBPartialSum.cpp:33)
         pi += use ? p * (bj + r2 * q4bi) : 0.0f;
-        gp[u] = use ? p * (bi + 0.25f * r2 * ibj) : 0.0f;
+        gp[u] = use ? p * (ri.x + 0.25f * r2 * rj.y) : 0.0f;
       }
       const float sp = warp_tsum8(gp, lane);
       const int jt = J * 32 + g * 8 + (lane >> 2);
@@ -448,90 +505,76 @@ k_gb_partial_half(GbArgs a, int tiles, long long items) {
   }
 }
 
-// Forces and pair energy over each unordered pair once (same tiling as
-// k_gb_partial_half); the pair force of GBForce::operator() is symmetric in
-// i and j, so j receives its opposite through warp_tsum8.  The partial sums
-// are read straight from their fixed-point accumulators.
-__global__ void __launch_bounds__(kHpWarps * 32)
+// Forces and pair energy over each unordered pair once (same tiling); the
+// pair force of GBForce::operator() is symmetric in i and j, so j receives
+// its opposite through warp_tsum8.  The partial sums are read straight from
+// their fixed-point accumulators.  Work items are halves of tile pairs
+// (16 j atoms), so the warps of a block share this heaviest pass finely.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1)
 k_gb_force_half(GbArgs a, int tiles, long long items) {
-  __shared__ float4 sh[kHpWarps][32], sl[kHpWarps][32], sg[kHpWarps][32];
-  __shared__ float2 sk[kHpWarps][32];
+  __shared__ float4 sh[WARPS][32], sl[WARPS][32], sg[WARPS][32], sr[WARPS][32];
+  __shared__ float sp[WARPS][32];
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
-  const long long nw = (long long)gridDim.x * kHpWarps;
+  __shared__ int counter;
+  if (threadIdx.x == 0) counter = 0;
+  __syncthreads();
+  const BlockItems queue{&counter};
   const double d = a.dielec;
   double epair = 0.0;
-  for (long long w = (long long)blockIdx.x * kHpWarps + wb; w < items; w += nw) {
+  long long w;
+  for (w = queue.next(lane); w < items; w = queue.next(lane)) {
     int I, J;
-    tile_pair_of(w, tiles, &I, &J);
+    tile_pair_of(w >> 1, tiles, &I, &J);
+    const int g0 = 2 * (int)(w & 1);
     const int i = I * 32 + lane;
     const bool vi = i < a.n;
     const int ii = vi ? i : 0;
-    float xh, yh, zh, xl, yl, zl;
-    split_hilo(a.pos[3 * ii], xh, xl);
-    split_hilo(a.pos[3 * ii + 1], yh, yl);
-    split_hilo(a.pos[3 * ii + 2], zh, zl);
-    const float bi = (float)a.born[ii], qi = (float)a.charge[ii];
-    const double oid = a.vdwr[ii] - a.offset[ii];
-    const float oi = (float)oid;
-    const float soi = (float)(a.scale[ii] * oid);
-    const float dfac_i = (float)a.psi[ii];
+    const float4 hi = a.rec[ii], li = a.rec[a.n + ii], gi = a.gst[ii], ri = a.grad[ii];
     const float part_i = (float)((double)a.partial_fx[ii] * (1.0 / kGbScale));
-    const double ibi = 1.0 / a.born[ii];
-    const float q4bi = (float)(0.25 * ibi);
-    const float selfi = (float)(0.5 * a.charge[ii] * a.charge[ii] * ibi * ibi);
+    const float q4bi = 0.25f * ri.y;
     {
       const int j = J * 32 + lane;
       const int jj = j < a.n ? j : 0;
-      float4 h, l, g;
-      gb_stage_pos(a.pos, jj, h, l);
-      h.w = (float)a.charge[jj];
-      const double bj = a.born[jj];
-      l.w = (float)bj;
-      const double oj = a.vdwr[jj] - a.offset[jj];
-      g.x = (float)oj;
-      g.y = (float)(a.scale[jj] * oj);
-      g.z = (float)a.psi[jj];
-      g.w = (float)((double)a.partial_fx[jj] * (1.0 / kGbScale));
-      const double ibj = 1.0 / bj;
-      sh[wb][lane] = h;
-      sl[wb][lane] = l;
-      sg[wb][lane] = g;
-      sk[wb][lane] = make_float2((float)ibj, (float)(0.5 * a.charge[jj] * a.charge[jj] * ibj * ibj));
+      sh[wb][lane] = a.rec[jj];
+      sl[wb][lane] = a.rec[a.n + jj];
+      sg[wb][lane] = a.gst[jj];
+      sr[wb][lane] = a.grad[jj];
+      sp[wb][lane] = (float)((double)a.partial_fx[jj] * (1.0 / kGbScale));
     }
     __syncwarp();
+    const int jn = a.n - J * 32;
     float fx = 0, fy = 0, fz = 0, ep = 0;
 #pragma unroll 1
-    for (int gq = 0; gq < 4; gq++) {
+    for (int gq = g0; gq < g0 + 2; gq++) {
       float gx[8], gy[8], gz[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int k = gq * 8 + u;
-        const int j = J * 32 + k;
-        const float4 h = sh[wb][k], l = sl[wb][k], g = sg[wb][k];
-        const float2 kj = sk[wb][k];
-        const bool use = vi && j < a.n && (I < J || k > lane);
-        const float dx = (h.x - xh) + (l.x - xl);
-        const float dy = (h.y - yh) + (l.y - yl);
-        const float dz = (h.z - zh) + (l.z - zl);
+        const float4 h = sh[wb][k], l = sl[wb][k], gj = sg[wb][k], rj = sr[wb][k];
+        const bool use = vi && k < jn && (I < J || k > lane);
+        const float dx = (h.x - hi.x) + (l.x - li.x);
+        const float dy = (h.y - hi.y) + (l.y - li.y);
+        const float dz = (h.z - hi.z) + (l.z - li.z);
         const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
         const float idist = rsqrt_nr(r2);
         const float dist = r2 * idist;
-        const float qj = h.w, bj = l.w, bb = bi * bj;
-        const float ex = __expf(-r2 * (q4bi * kj.x));
+        const float bj = rj.x, bb = ri.x * bj;
+        const float ex = __expf(-r2 * (q4bi * rj.y));
         const float ifgb = rsqrt_nr(r2 + bb * ex);
-        const float qq = qi * qj;
-        const float dRi = dfac_i * gb_dBT_f32(dist, idist, oi, g.y);
-        const float dRj = g.z * gb_dBT_f32(dist, idist, g.x, soi);
+        const float qq = hi.w * h.w;
+        const float dRi = ri.z * gb_dBT_f32(dist, idist, gi.x, gj.y);
+        const float dRj = rj.z * gb_dBT_f32(dist, idist, gj.x, gi.y);
         const float pref = 0.5f * qq * (ifgb * ifgb * ifgb);
         // partialTerm[i][j] and [j][i] (GBPartialSum.cpp:33-41)
         const float ai = bj + r2 * q4bi;
-        const float aj = bi + 0.25f * r2 * kj.x;
+        const float aj = ri.x + 0.25f * r2 * rj.y;
         const float ptij = pref * ex * ai, ptji = pref * ex * aj;
         float f = -pref * ((2.0f * dist - 0.5f * ex * dist) + ex * dRi * ai + ex * dRj * aj);
-        f -= selfi * dRi;
-        f -= kj.y * dRj;
+        f -= ri.w * dRi;
+        f -= rj.w * dRj;
         f -= (part_i - ptij) * dRi;
-        f -= (g.w - ptji) * dRj;
+        f -= (sp[wb][k] - ptji) * dRj;
         f *= idist;
         f = use ? f : 0.0f;
         ep += use ? -qq * ifgb : 0.0f;
@@ -559,19 +602,32 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
   if (lane == 0 && epair != 0.0) red_add(&a.acc[ACC_COULOMB], to_fixed(epair, kEnergyScale));
 }
 
+// Static FP32 record of the GB passes: (rho~ = vdwr - offset, S rho~,
+// 1 / rho~, 1 for water else 0).
+__global__ void k_gb_static(int n, const double *__restrict__ vdwr,
+                            const double *__restrict__ scale, const double *__restrict__ offset,
+                            const int *__restrict__ water, float4 *__restrict__ gst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double o = vdwr[i] - offset[i];
+  gst[i] = make_float4((float)o, (float)(scale[i] * o), (float)(1.0 / o),
+                       water && water[i] ? 1.0f : 0.0f);
+}
+
 // The FP32 chain: burial sums, Born radii, partial sums, forces (the
-// partial sums stay in their fixed-point accumulators).
+// partial sums stay in their fixed-point accumulators).  a.rec holds the
+// atoms' pair records and a.gst the static GB records.
 static void gb_passes_f32(const GbArgs &a, cudaStream_t st) {
-  dim3 grid;
-  int jchunk;
-  allpairs_grid(a.n, &grid, &jchunk);
-  int tiles, blocks;
-  long long items;
-  halfpairs_grid(a.n, &tiles, &items, &blocks);
-  k_gb_burial_f32<<<grid, kApAtoms, 0, st>>>(a, jchunk);
+  // one block per SM (the register counts admit no second), so every SM
+  // holds the same number of warps and the queue balances the items
+  int tiles, blocks, blocks2;
+  long long items, items2;
+  halfpairs_grid(a.n, 1, &tiles, &items, &blocks);
+  halfpairs_grid(a.n, 2, &tiles, &items2, &blocks2);
+  k_gb_burial_half<32><<<blocks, 32 * 32, 0, st>>>(a, tiles, items);
   k_gb_radii<<<(a.n + 127) / 128, 128, 0, st>>>(a);
-  k_gb_partial_half<<<blocks, kHpWarps * 32, 0, st>>>(a, tiles, items);
-  k_gb_force_half<<<blocks, kHpWarps * 32, 0, st>>>(a, tiles, items);
+  k_gb_partial_half<16><<<blocks, 16 * 32, 0, st>>>(a, tiles, items);
+  k_gb_force_half<16><<<blocks2, 16 * 32, 0, st>>>(a, tiles, items2);
 }
 
 int gb_init(System *s) {
@@ -583,6 +639,15 @@ int gb_init(System *s) {
     PM_CHECK(dev_alloc(s, &s->d_gb_partial, sizeof(double) * n));
     PM_CHECK(dev_alloc(s, &s->d_gb_fixed, sizeof(long long) * 2 * n));
     PM_CUDA(cudaMemsetAsync(s->d_gb_fixed, 0, sizeof(long long) * 2 * n, s->stream));
+  }
+  if (s->precision == PMGPU_PREC_MIXED && !s->d_gb_gst) {
+    if (!s->d_rec) PM_CHECK(dev_alloc(s, &s->d_rec, sizeof(float4) * 2 * n));
+    PM_CHECK(dev_alloc(s, &s->d_gb_gst, sizeof(float4) * n));
+    PM_CHECK(dev_alloc(s, &s->d_gb_grad, sizeof(float4) * n));
+    if (s->n > 0)
+      k_gb_static<<<(s->n + 127) / 128, 128, 0, s->stream>>>(
+          s->n, s->d_gb_vdwr, s->d_gb_scale, s->d_gb_offset, s->d_water, s->d_gb_gst);
+    PM_CUDA(cudaGetLastError());
   }
   return PMGPU_OK;
 }
@@ -609,6 +674,9 @@ int gb_forces(System *s, Force *f) {
   a.partial = s->d_gb_partial;
   a.force = s->d_force;
   a.acc = s->d_acc;
+  a.rec = s->d_rec;
+  a.gst = s->d_gb_gst;
+  a.grad = s->d_gb_grad;
   dim3 grid;
   int jchunk;
   gb_grid(n, &grid, &jchunk);
@@ -651,8 +719,10 @@ constexpr int kGbStaticMaxAtoms = PMGPU_GB_STATIC_MAX_ATOMS;
 constexpr int kGbStaticAccWords = 32;
 static_assert(ACC_COUNT <= kGbStaticAccWords, "accumulator block too small");
 // per atom: born, psi, partial (double), burial and partial sums (int64),
-// three force planes (int64); then the energy/virial accumulator block
-constexpr size_t kGbStaticWords = 8 * (size_t)kGbStaticMaxAtoms + kGbStaticAccWords;
+// three force planes (int64); then the energy/virial accumulator block;
+// then the FP32 records: pair records (2 float4 per atom), static and radius
+// records (1 float4 each)
+constexpr size_t kGbStaticWords = 16 * (size_t)kGbStaticMaxAtoms + kGbStaticAccWords;
 constexpr int kGbStaticMaxDevices = 64;
 
 // In host code this name is only a stand-in for the symbol; the device
@@ -767,6 +837,12 @@ extern "C" int pmgpu_gb_forces_noalloc(int n_atoms, const double *pos, const dou
   a.partial_fx = scratch + 4 * (size_t)n;
   a.force = scratch + 5 * (size_t)n;
   a.acc = scratch + 8 * (size_t)n;
+  float4 *rec = reinterpret_cast<float4 *>(a.acc + kGbStaticAccWords);
+  float4 *gst = rec + 2 * (size_t)n;
+  float4 *grad = gst + n;
+  a.rec = rec;
+  a.gst = gst;
+  a.grad = grad;
   PM_CUDA(cudaMemsetAsync(a.burial_fx, 0, sizeof(long long) * (5 * (size_t)n + kGbStaticAccWords),
                           st));
 
@@ -774,6 +850,8 @@ extern "C" int pmgpu_gb_forces_noalloc(int n_atoms, const double *pos, const dou
   int jchunk;
   gb_grid(n, &grid, &jchunk);
   if (precision == PMGPU_PREC_MIXED) {
+    launch_stage_pairs(n, pos, charge, nullptr, rec, st);
+    k_gb_static<<<(n + 127) / 128, 128, 0, st>>>(n, gb_vdwr, gb_scale, gb_offset, water, gst);
     gb_passes_f32(a, st);
   } else {
     k_gb_burial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);

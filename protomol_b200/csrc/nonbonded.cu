@@ -1201,78 +1201,96 @@ k_simplefull(int n, int jchunk, const double *__restrict__ pos,
 }
 
 // The FP32 pass over each unordered pair once, as the reference visits
-// i < j (NonbondedSimpleFullSystemForce.h:125-150): a warp takes one 32 x 32
-// tile pair (I, J), I <= J, lane l holding atom 32 I + l; the J atoms sit
-// in the warp's shared-memory slice and are broadcast one at a time.  The
-// force on i accumulates in the lane, the opposite force on each j is
-// summed over the lanes by warp_tsum8 per eight j atoms; on the diagonal
-// tile only j > i counts.  Energies and virial (EM 1, 2) are not halved.
+// i < j (NonbondedSimpleFullSystemForce.h:125-150): a warp takes 32 x 32
+// tile pairs (I, J), I <= J, of its block's share (BlockItems), lane l
+// holding atom 32 I + l; the J atoms sit in the warp's shared-memory slice
+// and are broadcast one at a time.  The force on i accumulates in the lane, the opposite force on
+// each j is summed over the lanes by warp_tsum8 per eight j atoms.  Which
+// pairs of a tile are excluded or modified comes from the tile's masks
+// (sf_tile, sf_bits), read once per tile; on the diagonal tile only j > i
+// counts.  Energies and virial (EM 1, 2) are not halved.
+constexpr int kSfWarps = 16;
+
 template <bool LJ, bool COUL, bool COMB, int EM>
-__global__ void __launch_bounds__(kHpWarps * 32)
-k_simplefull_half(int n, int tiles, long long items, const double *__restrict__ pos,
-                  const double *__restrict__ charge, const int *__restrict__ type, int ntypes,
-                  const float2 *__restrict__ ljab, const float2 *__restrict__ ljcomb,
-                  const float4 *__restrict__ lj32, const int2 *__restrict__ ex_range,
-                  const int *__restrict__ ex_start, const int *__restrict__ ex_partner,
-                  const int *__restrict__ ex_class, float csf, long long *__restrict__ force,
-                  long long *__restrict__ acc) {
-  __shared__ float4 sh[kHpWarps][32], sl[kHpWarps][32];
-  __shared__ float2 sc[kHpWarps][COMB ? 32 : 1];
+__global__ void __launch_bounds__(kSfWarps * 32, 1)
+k_simplefull_half(int n, int tiles, long long items,
+                  const float4 *__restrict__ rec, int ntypes, const float2 *__restrict__ ljab,
+                  const float2 *__restrict__ ljcomb, const float4 *__restrict__ lj32,
+                  const int *__restrict__ sf_tile, const uint2 *__restrict__ sf_bits, float csf,
+                  long long *__restrict__ force, long long *__restrict__ acc) {
+  __shared__ float4 sh[kSfWarps][32], sl[kSfWarps][32];
+  __shared__ float2 sc[kSfWarps][COMB ? 32 : 1];
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
-  const long long nw = (long long)gridDim.x * kHpWarps;
   double elj = 0, ec = 0;
   double v[6] = {0, 0, 0, 0, 0, 0};
-  for (long long w = (long long)blockIdx.x * kHpWarps + wb; w < items; w += nw) {
+  __shared__ int counter;
+  if (threadIdx.x == 0) counter = 0;
+  __syncthreads();
+  const BlockItems queue{&counter};
+  long long w;
+  for (w = queue.next(lane); w < items; w = queue.next(lane)) {
     int I, J;
     tile_pair_of(w, tiles, &I, &J);
     const int i = I * 32 + lane;
     const bool vi = i < n;
     const int ii = vi ? i : 0;
-    float xh, yh, zh, xl, yl, zl;
-    split_hilo(pos[3 * ii], xh, xl);
-    split_hilo(pos[3 * ii + 1], yh, yl);
-    split_hilo(pos[3 * ii + 2], zh, zl);
-    const float qi = (float)charge[ii];
-    const int ti = type[ii];
+    const float4 hi = rec[ii], li = rec[n + ii];
+    const float xh = hi.x, yh = hi.y, zh = hi.z, xl = li.x, yl = li.y, zl = li.z;
+    const float qi = hi.w;
+    const int ti = __float_as_int(li.w);
     const float2 ci = COMB ? ljcomb[ti] : make_float2(0.f, 0.f);
-    const int2 er = ex_range[ii];
+    // skip: excluded pairs, partners past the end, j <= i on the diagonal
+    unsigned skip = 0u, mod = 0u;
+    const int q = sf_tile[w];
+    if (q >= 0) {
+      const uint2 b = sf_bits[32 * q + lane];
+      skip = b.x;
+      mod = b.y;
+    }
+    const int jn = n - J * 32;
+    if (jn < 32) skip |= ~0u << jn;
+    if (I == J) skip |= (2u << lane) - 1u;
+    if (!vi) skip = ~0u;
     {
       const int j = J * 32 + lane;
       const int jj = j < n ? j : 0;
-      float4 h, l;
-      split_hilo(pos[3 * jj], h.x, l.x);
-      split_hilo(pos[3 * jj + 1], h.y, l.y);
-      split_hilo(pos[3 * jj + 2], h.z, l.z);
-      h.w = (float)charge[jj];
-      const int tj = type[jj];
-      l.w = __int_as_float(tj);
-      sh[wb][lane] = h;
+      const float4 l = rec[n + jj];
+      sh[wb][lane] = rec[jj];
       sl[wb][lane] = l;
-      if (COMB) sc[wb][lane] = ljcomb[tj];
+      if (COMB) sc[wb][lane] = ljcomb[__float_as_int(l.w)];
     }
     __syncwarp();
     float fx = 0, fy = 0, fz = 0;
 #pragma unroll 1
     for (int g = 0; g < 4; g++) {
       float gx[8], gy[8], gz[8];
-      float2 tab[8];
+      float2 tab[8], m14[8];
       if (LJ && !COMB) {
 #pragma unroll
         for (int u = 0; u < 8; u++)
           tab[u] = __ldg(&ljab[__float_as_int(sl[wb][g * 8 + u].w) * ntypes + ti]);
       }
+      // the modified (1-4) parameters of this group, loaded together
+      const unsigned gmod = LJ ? (mod >> (8 * g)) & 0xffu : 0u;
+      if (gmod) {
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          m14[u] = make_float2(0.f, 0.f);
+          if ((gmod >> u) & 1u) {
+            const float4 m = __ldg(&lj32[ti * ntypes + __float_as_int(sl[wb][g * 8 + u].w)]);
+            m14[u] = make_float2(m.z, m.w);
+          }
+        }
+      }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int k = g * 8 + u;
-        const int j = J * 32 + k;
         const float4 h = sh[wb][k], l = sl[wb][k];
         const float dx = (h.x - xh) + (l.x - xl);
         const float dy = (h.y - yh) + (l.y - yl);
         const float dz = (h.z - zh) + (l.z - zl);
-        int excl = (vi && j < n && (I < J || k > lane)) ? PMGPU_EXCL_NONE : PMGPU_EXCL_FULL;
-        if (excl == PMGPU_EXCL_NONE && j >= er.x && j <= er.y)
-          excl = excl_class_of(ex_start, ex_partner, ex_class, i, j);
-        const bool use = excl != PMGPU_EXCL_FULL;
+        const bool use = !((skip >> k) & 1u);
+        const bool modified = (mod >> k) & 1u;
         const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
         const float rinv = rsqrt_nr(r2);
         const float rr2 = rinv * rinv;
@@ -1289,10 +1307,9 @@ k_simplefull_half(int n, int tiles, long long items, const double *__restrict__ 
             A = tab[u].x;
             B = tab[u].y;
           }
-          if (excl == PMGPU_EXCL_MODIFIED) {
-            const float4 m = __ldg(&lj32[ti * ntypes + __float_as_int(l.w)]);
-            A = m.z;
-            B = m.w;
+          if (gmod && modified) {
+            A = m14[u].x;
+            B = m14[u].y;
           }
           const float r6 = rr2 * rr2 * rr2;
           const float r6B = B * r6, r12A = A * r6 * r6;
@@ -1301,7 +1318,7 @@ k_simplefull_half(int n, int tiles, long long items, const double *__restrict__ 
         }
         if (COUL) {
           float en = qi * h.w * rinv;
-          if (excl == PMGPU_EXCL_MODIFIED) en *= csf;
+          if (modified) en *= csf;
           if (EM && use) ec += (double)en;
           f += en * rr2;
         }
@@ -1345,23 +1362,69 @@ k_simplefull_half(int n, int tiles, long long items, const double *__restrict__ 
   }
 }
 
-void allpairs_grid(int n, dim3 *grid, int *jchunk) {
-  static int sms[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  int &m = sms[dev & 63];
-  if (m <= 0 && (cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-                 m <= 0))
-    m = 148;
-  const int iblocks = (n + kApAtoms - 1) / kApAtoms;
-  const int want = kApBlocksPerSm * m;
-  int chunks = std::max(1, std::min((want + iblocks - 1) / iblocks, (n + kApTile - 1) / kApTile));
-  *jchunk = (n + chunks - 1) / chunks;
-  chunks = (n + *jchunk - 1) / *jchunk;
-  *grid = dim3(iblocks, chunks);
+__global__ void k_stage_pairs(int n, const double *__restrict__ pos,
+                              const double *__restrict__ charge, const int *__restrict__ type,
+                              float4 *__restrict__ rec) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  write_pair_record(rec, n, i, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], charge[i],
+                    type ? type[i] : 0);
 }
 
-void halfpairs_grid(int n, int *tiles, long long *items, int *blocks) {
+void launch_stage_pairs(int n, const double *pos, const double *charge, const int *type,
+                        float4 *rec, cudaStream_t st) {
+  if (n > 0) k_stage_pairs<<<(n + 255) / 256, 256, 0, st>>>(n, pos, charge, type, rec);
+}
+
+int nb_stage_pairs(System *s) {
+  if (!s->d_rec) return PMGPU_OK;
+  launch_stage_pairs(s->n, s->d_pos, s->d_charge, s->d_type, s->d_rec, s->stream);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+int nb_simplefull_init(System *s) {
+  if (!s->d_rec) PM_CHECK(dev_alloc(s, &s->d_rec, sizeof(float4) * 2 * std::max(1, s->n)));
+  if (s->d_sf_tile) return PMGPU_OK;
+  const int n = s->n, T = (n + 31) / 32;
+  const long long items = (long long)T * (T + 1) / 2;
+  std::vector<int> tile((size_t)std::max(1LL, items), -1);
+  std::vector<uint2> bits;
+  std::vector<unsigned> seen;
+  // tile pair numbers as tile_pair_of counts them, diagonal by diagonal
+  auto dstart = [&](long long d) { return d * T - d * (d - 1) / 2; };
+  const size_t ne = s->h_excl.size() / 3;
+  for (size_t e = 0; e < ne; e++) {
+    const int a = s->h_excl[3 * e], b = s->h_excl[3 * e + 1], c = s->h_excl[3 * e + 2];
+    if (a == b) continue;
+    const int lo = std::min(a, b), hi = std::max(a, b);
+    const long long w = dstart(hi / 32 - lo / 32) + lo / 32;
+    if (tile[w] < 0) {
+      tile[w] = (int)(bits.size() / 32);
+      bits.resize(bits.size() + 32, make_uint2(0u, 0u));
+      seen.resize(seen.size() + 32, 0u);
+    }
+    // the first entry of a pair decides its class, as a scan of the
+    // exclusion table in order would
+    const size_t idx = 32 * (size_t)tile[w] + (lo & 31);
+    const unsigned bit = 1u << (hi & 31);
+    if (seen[idx] & bit) continue;
+    seen[idx] |= bit;
+    if (c == PMGPU_EXCL_FULL) bits[idx].x |= bit;
+    else if (c == PMGPU_EXCL_MODIFIED) bits[idx].y |= bit;
+  }
+  if (bits.empty()) bits.assign(32, make_uint2(0u, 0u));
+  PM_CHECK(dev_alloc(s, &s->d_sf_tile, sizeof(int) * tile.size()));
+  PM_CHECK(dev_alloc(s, &s->d_sf_bits, sizeof(uint2) * bits.size()));
+  PM_CUDA(cudaMemcpyAsync(s->d_sf_tile, tile.data(), sizeof(int) * tile.size(),
+                          cudaMemcpyHostToDevice, s->stream));
+  PM_CUDA(cudaMemcpyAsync(s->d_sf_bits, bits.data(), sizeof(uint2) * bits.size(),
+                          cudaMemcpyHostToDevice, s->stream));
+  PM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMGPU_OK;
+}
+
+void halfpairs_grid(int n, int split, int *tiles, long long *items, int *blocks) {
   static int sms[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -1371,9 +1434,8 @@ void halfpairs_grid(int n, int *tiles, long long *items, int *blocks) {
     m = 148;
   const int t = (n + 31) / 32;
   *tiles = t;
-  *items = (long long)t * (t + 1) / 2;
-  const long long warps = std::max(1LL, std::min(*items, (long long)kHpWarpsPerSm * m));
-  *blocks = (int)((warps + kHpWarps - 1) / kHpWarps);
+  *items = (long long)t * (t + 1) / 2 * split;
+  *blocks = (int)std::max(1LL, std::min(*items, (long long)m));
 }
 
 // em: 0 forces only, 1 + energies, 2 + energies and virial.
@@ -1395,12 +1457,13 @@ int nb_simplefull(System *s, int lj, int coul, int em) {
   if (s->precision == PMGPU_PREC_MIXED) {
     int tiles, blocks;
     long long items;
-    halfpairs_grid(n, &tiles, &items, &blocks);
+    halfpairs_grid(n, 1, &tiles, &items, &blocks);
+    PM_CHECK(nb_simplefull_init(s));
     auto go32 = [&](auto kern) {
-      kern<<<blocks, kHpWarps * 32, 0, s->stream>>>(
-          n, tiles, items, s->d_pos, s->d_charge, s->d_type, s->ntypes, s->d_ljab,
-          s->d_ljcomb, s->d_lj32, s->d_excl_range, s->d_excl_start, s->d_excl_partner,
-          s->d_excl_class, (float)s->coulomb_scaling, s->d_force, s->d_acc);
+      kern<<<blocks, kSfWarps * 32, 0, s->stream>>>(
+          n, tiles, items, s->d_rec, s->ntypes, s->d_ljab,
+          s->d_ljcomb, s->d_lj32, s->d_sf_tile, s->d_sf_bits, (float)s->coulomb_scaling,
+          s->d_force, s->d_acc);
     };
     auto by_em = [&](auto k0, auto k1, auto k2) {
       if (em == 0) go32(k0);

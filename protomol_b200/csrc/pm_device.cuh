@@ -153,17 +153,35 @@ __device__ __forceinline__ float warp_tsum8(const float (&v)[8], int lane) {
   return c;
 }
 
+// The work items of a launch dealt to the blocks round-robin (block b
+// takes items b, b + G, b + 2G, ... of G blocks), so every SM gets the same
+// number of items and the same mix of cheap and dear ones; inside a block
+// the warps take the items of its share from a shared-memory counter, so
+// they stay busy to the end of it.  `counter` is a __shared__ int the block
+// sets to zero (then synchronises) before the first next().
+struct BlockItems {
+  int *counter;
+  __device__ __forceinline__ long long next(int lane) const {
+    int k = 0;
+    if (lane == 0) k = atomicAdd(counter, 1);
+    return blockIdx.x + (long long)gridDim.x * __shfl_sync(0xffffffffu, k, 0);
+  }
+};
+
 // Work item w of the half all-pairs sweep: the tile pairs (I, J), I <= J,
-// of `tiles` 32-atom tiles, numbered row by row (row I holds J = I..tiles-1).
+// of `tiles` 32-atom tiles, numbered diagonal by diagonal: d = J - I = 0
+// holds I = 0..tiles-1, d = 1 holds I = 0..tiles-2, and so on, so that
+// w = d tiles - d (d - 1) / 2 + I.  Pairs of nearby tiles, which in a chain
+// molecule hold the near (dearer) atom pairs, are spread over the numbers.
 __device__ __forceinline__ void tile_pair_of(long long w, int tiles, int *I, int *J) {
   const double t2 = 2.0 * tiles + 1.0;
-  int r = (int)((t2 - sqrt(t2 * t2 - 8.0 * (double)w)) * 0.5);
-  r = max(0, min(r, tiles - 1));
+  int d = (int)((t2 - sqrt(t2 * t2 - 8.0 * (double)w)) * 0.5);
+  d = max(0, min(d, tiles - 1));
   auto start = [&](long long q) { return q * tiles - q * (q - 1) / 2; };
-  while (r > 0 && start(r) > w) r--;
-  while (r + 1 < tiles && start(r + 1) <= w) r++;
-  *I = r;
-  *J = r + (int)(w - start(r));
+  while (d > 0 && start(d) > w) d--;
+  while (d + 1 < tiles && start(d + 1) <= w) d++;
+  *I = (int)(w - start(d));
+  *J = *I + d;
 }
 
 // An FP64 coordinate as an FP32 pair: hi = x rounded, lo = x - hi rounded,
@@ -173,6 +191,20 @@ __device__ __forceinline__ void tile_pair_of(long long w, int tiles, int *I, int
 __device__ __forceinline__ void split_hilo(double x, float &hi, float &lo) {
   hi = (float)x;
   lo = (float)(x - (double)hi);
+}
+
+// The FP32 record of atom i read by the all-pairs passes: rec[i] =
+// (x_hi, y_hi, z_hi, charge), rec[n + i] = (x_lo, y_lo, z_lo, type bits).
+__device__ __forceinline__ void write_pair_record(float4 *rec, int n, int i, double x,
+                                                  double y, double z, double q, int type) {
+  float4 h, l;
+  split_hilo(x, h.x, l.x);
+  split_hilo(y, h.y, l.y);
+  split_hilo(z, h.z, l.z);
+  h.w = (float)q;
+  l.w = __int_as_float(type);
+  rec[i] = h;
+  rec[n + i] = l;
 }
 
 template <typename Real>

@@ -231,7 +231,7 @@ struct System {
   std::vector<int> h_type, h_mol;
   int ntypes = 0;
   std::vector<double> h_lj;
-  std::vector<int> h_excl;
+  std::vector<int> h_excl;  // exclusions as given: a, b, class per entry
   double coulomb_scaling = 1.0;
   // device topology
   double *d_charge = nullptr, *d_mass = nullptr;
@@ -263,6 +263,17 @@ struct System {
   long long *d_force = nullptr;  // 3 planes of n, fixed point
   long long *d_acc = nullptr;    // ACC_COUNT fixed point accumulators
   int *d_status = nullptr;
+  // simple-full tile masks: per tile pair (I <= J) of 32-atom tiles the
+  // index of its masks or -1; per (masks, lane) the bits of excluded (x)
+  // and modified (y) partners k of that lane's atom
+  int *d_sf_tile = nullptr;
+  uint2 *d_sf_bits = nullptr;
+  // FP32 pair records of the all-pairs passes (2n, write_pair_record);
+  // rec_fresh: this evaluation's update kernel wrote them
+  float4 *d_rec = nullptr;
+  int rec_fresh = 0;
+  // GB FP32 records: static (k_gb_static) and per evaluation (k_gb_radii)
+  float4 *d_gb_gst = nullptr, *d_gb_grad = nullptr;
   long long *h_acc = nullptr;    // pinned mirror
   int *h_status = nullptr;       // pinned mirror
   // forces and lists
@@ -326,21 +337,18 @@ int nb_build(System *s, NeighborList *nl);
 int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode);
 int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
 int nb_simplefull(System *s, int lj, int coul, int em);
-// Launch shape of the FP32 all-pairs passes (simple-full and GB): blocks
-// of kApAtoms accumulating atoms (one per thread) times chunks of partner
-// atoms, sized so every SM holds about kApBlocksPerSm blocks; partners are
-// staged kApTile at a time.
-constexpr int kApAtoms = 128;
-constexpr int kApTile = 32;
-constexpr int kApBlocksPerSm = 4;
-void allpairs_grid(int n, dim3 *grid, int *jchunk);
+// the exclusion tile masks of the FP32 simple-full pass (once per system)
+int nb_simplefull_init(System *s);
 // Launch shape of the FP32 half all-pairs passes (each unordered pair once,
-// forces to both atoms): one warp per 32 x 32 tile pair (I <= J), blocks of
-// kHpWarps warps striding over the tile pairs, at most kHpWarpsPerSm warps
-// per SM.
-constexpr int kHpWarps = 4;
-constexpr int kHpWarpsPerSm = 16;
-void halfpairs_grid(int n, int *tiles, long long *items, int *blocks);
+// forces to both atoms): work items of 32 i atoms x 32 / split j atoms (a
+// share of a 32 x 32 tile pair I <= J) in equal shares per block
+// (BlockItems); one block per SM (the kernels' register counts admit no
+// second).
+void halfpairs_grid(int n, int split, int *tiles, long long *items, int *blocks);
+// the atoms' FP32 pair records (write_pair_record) from the FP64 positions
+int nb_stage_pairs(System *s);
+void launch_stage_pairs(int n, const double *pos, const double *charge, const int *type,
+                        float4 *rec, cudaStream_t st);
 
 // pme.cu
 int pme_init(System *s, Force *f);
@@ -353,8 +361,10 @@ int gb_init(System *s);
 int gb_forces(System *s, Force *f);
 
 // bonded_integrate.cu
-int bonded_forces(System *s, Force *f, int em);
-int torsion_forces(System *s, Force *f, int em);
+// bonds, angles, dihedrals and impropers (each flag: include that kind) in
+// one launch; *launched = 1 when there was any term
+int bonded_all(System *s, int bonds, int angles, int dihedrals, int impropers, int em,
+               int *launched);
 int zero_forces(System *s);
 // zero_acc: the update launch also clears the energy accumulators (the
 // start of a force evaluation); list: the pair list whose rebuild decision
