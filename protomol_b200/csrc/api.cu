@@ -240,8 +240,11 @@ static int system_free(System *s) {
   s->prof.pool.clear();
   if (s->side) cudaStreamSynchronize(s->side);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->side2) cudaStreamSynchronize(s->side2);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->ev_join2) cudaEventDestroy(s->ev_join2);
   if (s->side) cudaStreamDestroy(s->side);
+  if (s->side2) cudaStreamDestroy(s->side2);
   if (s->stream) cudaStreamDestroy(s->stream);
   return PMGPU_OK;
 }
@@ -361,7 +364,9 @@ static int evaluate_forces(System *s, int only, int mode) {
   // (not while profiling, which times phases in order).  They start at
   // once, while the list work of the step leaves most of the device idle.
   // The second stream has the higher priority, so its short dependent
-  // kernels are not queued behind the pair kernel's blocks.
+  // kernels are not queued behind the pair kernel's blocks.  The PME chain
+  // is the longest of them, so the other short terms (bonded, Ewald
+  // correction) take a third stream and PME starts at once.
   // the all-pairs passes read the FP32 pair records of the positions,
   // written by this step's update kernel or here
   bool need_rec = false;
@@ -379,6 +384,7 @@ static int evaluate_forces(System *s, int only, int mode) {
   if (fork) {
     PM_CUDA(cudaEventRecord(s->ev_fork, main_stream));
     PM_CUDA(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
+    PM_CUDA(cudaStreamWaitEvent(s->side2, s->ev_fork, 0));
   }
   struct Join {  // back on the main stream, joined, on every exit path
     System *s;
@@ -392,30 +398,34 @@ static int evaluate_forces(System *s, int only, int mode) {
       if (!on) return;
       cudaEventRecord(s->ev_join, s->side);
       cudaStreamWaitEvent(main_stream, s->ev_join, 0);
+      cudaEventRecord(s->ev_join2, s->side2);
+      cudaStreamWaitEvent(main_stream, s->ev_join2, 0);
     }
   } join{s, main_stream, fork};
   {
     // GB's passes and the PME chain are long dependent chains and take the
     // second stream; the all-pairs terms go beside them on the main stream,
-    // and so do the bonded terms when the main stream has no list work
+    // and so do the bonded terms when the main stream has no list work;
+    // otherwise the bonded terms and the Ewald correction take the third
     const bool main_idle = s->lists.empty();
+    const cudaStream_t short_stream = main_idle ? main_stream : s->side2;
     for (auto &f : s->forces) {
       if (only >= 0 ? f.id != only : !f.enabled) continue;
       if (fork)
-        s->stream = f.kind == FK_SIMPLEFULL ||
-                            (main_idle && f.kind != FK_GB && f.kind != FK_PME)
-                        ? main_stream
-                        : s->side;
+        s->stream = f.kind == FK_SIMPLEFULL ? main_stream
+                    : f.kind == FK_GB || f.kind == FK_PME ? s->side
+                                                           : short_stream;
       int r = PMGPU_OK;
       switch (f.kind) {
         case FK_PME:
-          // the short correction first, so the PME chain ends the stream
           if (f.ewald_flags & PMGPU_EWALD_CORRECTION) {
+            if (fork) s->stream = short_stream;
             prof_begin(s, PMGPU_PHASE_CORRECTION);
             r = ewald_correction(s, &f, em);
             prof_end(s);
             PM_CHECK(r);
             s->kernels += s->n_excl > 0;
+            if (fork) s->stream = s->side;
           }
           if (f.ewald_flags & PMGPU_EWALD_RECIPROCAL) {
             prof_begin(s, PMGPU_PHASE_PME);
@@ -685,8 +695,10 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   int prio_low = 0, prio_high = 0;
   PM_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
   PM_CUDA(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, prio_high));
+  PM_CUDA(cudaStreamCreateWithPriority(&s->side2, cudaStreamNonBlocking, prio_high));
   PM_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
   PM_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+  PM_CUDA(cudaEventCreateWithFlags(&s->ev_join2, cudaEventDisableTiming));
   size_t nn = std::max(1, n);
   PM_CHECK(upload(s.get(), &s->d_charge, t->charge, n));
   PM_CHECK(upload(s.get(), &s->d_mass, t->mass, n));

@@ -393,6 +393,7 @@ constexpr int kUpdateThreads = 64;  // small blocks: the update is latency-bound
 __global__ void __launch_bounds__(kUpdateThreads)
 k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos,
          double *__restrict__ vel, long long *__restrict__ force, int *__restrict__ status) {
+  pdl_trigger();  // the list kernels after it may launch; they wait for this grid
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (a.acc_zero && i < ACC_COUNT) a.acc_zero[i] = 0;
   float d2 = 0.f;

@@ -65,6 +65,8 @@ __global__ void k_bin(ListGrid g, const double *__restrict__ pos,
                       unsigned *__restrict__ zkey, int *__restrict__ col_count,
                       double *__restrict__ offset, double *__restrict__ xbuild,
                       int *__restrict__ status) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
   if (!*rebuild) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.n) return;
@@ -139,6 +141,8 @@ __global__ void __launch_bounds__(1024)
 k_scan_cols(const int *__restrict__ rebuild, const int *__restrict__ col_count, int ncol,
             int *__restrict__ col_u, int *__restrict__ cursor, int *__restrict__ col_base,
             int *__restrict__ key_start, int nkeys, int *__restrict__ sorted, int ns_max) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
   if (!*rebuild) return;
   __shared__ int warp_tot[32];
   __shared__ int carry;
@@ -162,6 +166,8 @@ k_scan_cols(const int *__restrict__ rebuild, const int *__restrict__ col_count, 
 __global__ void k_scatter(const int *__restrict__ rebuild, int n,
                           const int *__restrict__ key, const int *__restrict__ col_u,
                           int *__restrict__ cursor, int *__restrict__ unsorted) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
   if (!*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -180,6 +186,8 @@ k_sort_cols(const int *__restrict__ rebuild, int nzb, float inv_z,
             const int *__restrict__ col_base, const int *__restrict__ unsorted,
             const unsigned *__restrict__ zkey, int *__restrict__ sorted,
             int *__restrict__ key_start, int *__restrict__ status) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
   if (!*rebuild) return;
   __shared__ unsigned long long keys[kColCap];
   const int col = blockIdx.x;
@@ -247,6 +255,8 @@ __global__ void k_gather(int ns, const double *__restrict__ pos,
                          float4 *__restrict__ xhi, float4 *__restrict__ xlo,
                          double4 *__restrict__ xw, int *__restrict__ mol_s,
                          const int *__restrict__ rebuild, float4 *__restrict__ bb) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const bool in = s < ns;
   const int i = in ? sorted[s] : -1;
@@ -304,6 +314,8 @@ __global__ void __launch_bounds__(kCheckThreads)
 k_check_rebuild(int n, const double *__restrict__ pos, const double *__restrict__ xbuild,
                 unsigned *__restrict__ ticket, int *__restrict__ rebuild, float half_skin2,
                 int force) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.f;
   if (i < n && !force) {
@@ -363,6 +375,7 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
               const int *__restrict__ mol_s, const float4 *__restrict__ bb,
               uint4 *__restrict__ tiles, int *__restrict__ tile_count,
               int *__restrict__ status) {
+  pdl_wait();  // the predecessor's writes are visible from here on
   if (!*rebuild) return;
   constexpr unsigned kAll = 0xffffffffu;
   // this warp's staging of candidate j clusters (up to 32 of them)
@@ -778,9 +791,8 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
   const float hs = (float)(0.5 * nl->skin);
   // an MD step's update kernel has taken the decision already
   if (!nl->decided || first || force_rebuild)
-    k_check_rebuild<<<nb, kCheckThreads, 0, st>>>(n, s->d_pos, nl->d_xbuild, nl->d_maxdisp,
-                                                 nl->d_rebuild, hs * hs,
-                                                 (force_rebuild || first) ? 1 : 0);
+    PM_CUDA(launch_pdl(k_check_rebuild, nb, kCheckThreads, 0, st, n, s->d_pos, nl->d_xbuild,
+                       nl->d_maxdisp, nl->d_rebuild, hs * hs, (force_rebuild || first) ? 1 : 0));
   nl->decided = 0;
   ListGrid g;
   g.box = s->box;
@@ -793,25 +805,25 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
   }
   {
     cudaStream_t q = st;  // the rebuild-only sort
-    k_bin<<<nb, T, 0, q>>>(g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_zkey, nl->d_col_count,
-                           nl->d_offset, nl->d_xbuild, s->d_status);
-    k_scan_cols<<<1, 1024, 0, q>>>(nl->d_rebuild, nl->d_col_count, nl->ncol, nl->d_col_u,
-                                   nl->d_col_cursor, nl->d_col_base, nl->d_key_start,
-                                   nl->nkeys, nl->d_sorted, nl->ns_max);
-    k_scatter<<<nb, T, 0, q>>>(nl->d_rebuild, n, nl->d_key, nl->d_col_u, nl->d_col_cursor,
-                               nl->d_unsorted);
-    k_sort_cols<<<nl->ncol, kSortThreads, 0, q>>>(
-        nl->d_rebuild, nl->nzb, (float)(1.0 / nl->cs[2]), nl->d_col_count, nl->d_col_u,
-        nl->d_col_base, nl->d_unsorted, nl->d_zkey, nl->d_sorted, nl->d_key_start, s->d_status);
+    // each kernel of the chain launches as a programmatic dependent of the
+    // one before, so on the steps that keep the list their early exits
+    // overlap their launches
+    PM_CUDA(launch_pdl(k_bin, nb, T, 0, q, g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_zkey,
+                       nl->d_col_count, nl->d_offset, nl->d_xbuild, s->d_status));
+    PM_CUDA(launch_pdl(k_scan_cols, 1, 1024, 0, q, nl->d_rebuild, nl->d_col_count, nl->ncol,
+                       nl->d_col_u, nl->d_col_cursor, nl->d_col_base, nl->d_key_start,
+                       nl->nkeys, nl->d_sorted, nl->ns_max));
+    PM_CUDA(launch_pdl(k_scatter, nb, T, 0, q, nl->d_rebuild, n, nl->d_key, nl->d_col_u,
+                       nl->d_col_cursor, nl->d_unsorted));
+    PM_CUDA(launch_pdl(k_sort_cols, nl->ncol, kSortThreads, 0, q, nl->d_rebuild, nl->nzb,
+                       (float)(1.0 / nl->cs[2]), nl->d_col_count, nl->d_col_u, nl->d_col_base,
+                       nl->d_unsorted, nl->d_zkey, nl->d_sorted, nl->d_key_start,
+                       s->d_status));
   }
-  if (s->precision == PMGPU_PREC_MIXED)
-    k_gather<true><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted,
-                                      s->d_charge, s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo,
-                                      nl->d_xw, nl->d_mol_s, nl->d_rebuild, nl->d_bb);
-  else
-    k_gather<false><<<nbs, T, 0, st>>>(nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted,
-                                       s->d_charge, s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo,
-                                       nl->d_xw, nl->d_mol_s, nl->d_rebuild, nl->d_bb);
+  PM_CUDA(launch_pdl(s->precision == PMGPU_PREC_MIXED ? k_gather<true> : k_gather<false>, nbs,
+                     T, 0, st, nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted, s->d_charge,
+                     s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
+                     nl->d_rebuild, nl->d_bb));
   PM_CUDA(cudaGetLastError());
   nl->built = 1;  // the slot order exists from here on
   return PMGPU_OK;
@@ -848,9 +860,9 @@ int nb_build(System *s, NeighborList *nl) {
                    cudaSuccess || sms <= 0))
     sms = 148;
   const int nblk = std::max(1, std::min((nl->nrows + kBuildWarps - 1) / kBuildWarps, 3 * sms));
-  k_build_tiles<<<nblk, kBuildWarps * 32, 0, st>>>(
-      ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s, nl->d_bb,
-      nl->d_tiles, nl->d_tile_count, s->d_status);
+  PM_CUDA(launch_pdl(k_build_tiles, nblk, kBuildWarps * 32, 0, st, ba, nl->d_rebuild,
+                     nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s, nl->d_bb,
+                     nl->d_tiles, nl->d_tile_count, s->d_status));
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
@@ -1020,8 +1032,8 @@ int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode) {
     fill_pair_args<double>(a, s, nl, t);
     PM_CHECK(launch_pairs<double>(a, s->stream, mode, t));
   }
-  k_slot_forces<<<(nl->ns_max + 255) / 256, 256, 0, s->stream>>>(nl->ns_max, s->n, nl->d_sorted,
-                                                                nl->d_fslot, s->d_force);
+  PM_CUDA(launch_pdl(k_slot_forces, (nl->ns_max + 255) / 256, 256, 0, s->stream, nl->ns_max,
+                     s->n, nl->d_sorted, nl->d_fslot, s->d_force));
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }

@@ -653,6 +653,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
 // clears the slot buffer for the next launch.
 __global__ void k_slot_forces(int ns, int n, const int *__restrict__ sorted,
                               long long *__restrict__ fslot, long long *__restrict__ force) {
+  pdl_wait();  // the predecessor's writes are visible from here on
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   const int i = sorted[s];

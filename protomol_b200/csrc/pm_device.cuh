@@ -115,6 +115,16 @@ static __constant__ double c_cn_dsw[5][7] = {
     {0, 0, 0, 0, 0, 0, 0},
     {12012., -72072., 180180., -240240., 180180., -72072., 12012.0}};
 
+// Programmatic dependent launch.  A kernel started with launch_pdl may begin
+// while its predecessor in the stream still runs: pdl_wait() blocks until
+// that grid has completed and its memory is visible, so it is the first
+// statement of every such kernel.  pdl_trigger() lets the successor's
+// launch begin once every block of this grid has triggered or exited, so
+// the successor's blocks never hold resources a block of this grid still
+// needs.  Both are no-ops for ordinary launches.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 __device__ __forceinline__ float pm_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double pm_sqrt(double x) { return sqrt(x); }
 

@@ -225,7 +225,8 @@ struct System {
   Box box{};
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;     // second stream for the non-pair terms
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t side2 = nullptr;    // third stream: short terms beside the PME chain
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
   // host copies of static topology
   std::vector<double> h_charge, h_mass;
   std::vector<int> h_type, h_mol;
@@ -314,6 +315,24 @@ struct System {
 // Device buffers are stream-ordered (cudaMallocAsync / cudaFreeAsync on the
 // system's stream): creating and destroying a system never synchronises the
 // whole device, so systems served side by side do not stall one another.
+// Launches kern on st as a programmatic dependent of the stream's previous
+// kernel (see pdl_wait in pm_device.cuh); kern must call pdl_wait() first.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, Args... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 int dev_alloc(System *s, void **p, size_t bytes);
 template <typename T>
 inline int dev_alloc(System *s, T **p, size_t bytes) {
