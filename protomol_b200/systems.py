@@ -188,7 +188,8 @@ def gb_polymer(n_atoms: int, seed: int, temperature: float = 300.0) -> Molecular
     pos = np.zeros((n_atoms, 3))
     b = 1.53
     theta = math.radians(109.5)
-    pos[1] = [b, 0, 0]
+    if n_atoms > 1:
+        pos[1] = [b, 0, 0]
     if n_atoms > 2:
         pos[2] = pos[1] + b * np.array([-math.cos(theta), math.sin(theta), 0.0])
     for i in range(3, n_atoms):

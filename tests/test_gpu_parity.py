@@ -321,3 +321,40 @@ def test_polymer_all_pairs_vs_oracle(ctx, table):
         vir_err = np.abs(e[7:16] - rv.ravel()).max() / max(np.abs(rv).max(), 1)
         assert vir_err <= 1e-5, (line, vir_err)
     gs.close()
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 31, 33, 65])
+def test_all_pairs_small_and_ragged_sizes(ctx, n):
+    """The half-pair tile sweeps at sizes below one tile, at a tile and a
+    bit, and with a ragged last tile: GB, LJ and Coulomb of a short polymer
+    (its exclusions fall on the diagonal and first off-diagonal tiles)
+    against the FP64 oracle."""
+    import oracle
+    from protomol_b200 import systems
+    sm = systems.gb_polymer(n, seed=7)
+    s = oracle.System(pos=sm.pos, charge=sm.charge, type=sm.type, molecule=sm.molecule,
+                      lj=sm.lj, excl=sm.exclusions, periodic=False, box=sm.box, mass=sm.mass,
+                      water=sm.water, gb_vdwr=sm.gb_vdwr, gb_scale=sm.gb_scale,
+                      gb_offset=sm.gb_offset, gb_obc=sm.gb_obc)
+    gs = GpuSystem(ctx, sm, "mixed")
+    ff = ForceFactory(gs)
+    rf, re, _ = oracle.gb_force(s, 1.0, 78.5)
+    f, e = _eval(ff.make("GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 "
+                         "-solventDielec 78.5"), sm)
+    if n > 1:
+        assert F.rms_rel(f, rf) <= RMS_MIXED, F.rms_rel(f, rf)
+    else:
+        assert np.abs(f).max() == 0.0
+    assert _energy_ok(e[0], re)
+    for line, pot, slot, key in (("LennardJones -algorithm NonbondedSimpleFull", "LennardJones",
+                                  1, "lj"),
+                                 ("Coulomb -algorithm NonbondedSimpleFull", "Coulomb", 0,
+                                  "coulomb")):
+        rf, re, _ = oracle.simplefull_force(s, pot)
+        f, e = _eval(ff.make(line), sm)
+        if np.abs(rf).max() > 0:
+            assert F.rms_rel(f, rf) <= RMS_MIXED, (line, F.rms_rel(f, rf))
+        else:
+            assert np.abs(f).max() == 0.0, line
+        assert _energy_ok(e[slot], re[key]), (line, e[slot], re[key])
+    gs.close()
