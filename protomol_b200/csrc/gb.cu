@@ -382,8 +382,10 @@ __device__ __forceinline__ float gb_dBT_f32(float dist, float idist, float oi, f
 }
 
 // Burial sums over each unordered pair once, both directions per pair: a
-// warp takes 32 x 32 tile pairs (I, J), I <= J, from its block's share; the "i
-// sees j" term adds to i in the lane, the "j sees i" term to j through
+// warp takes halves (16 j atoms) of 32 x 32 tile pairs (I, J), I <= J, from
+// its block's share (near tile pairs, which take the closed form, cost
+// several times more than far ones, so the finer items spread them); the
+// "i sees j" term adds to i in the lane, the "j sees i" term to j through
 // warp_tsum8.  Water atoms neither receive nor give burial.
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 1)
@@ -399,7 +401,8 @@ k_gb_burial_half(GbArgs a, int tiles, long long items) {
   long long w;
   for (w = queue.next(lane); w < items; w = queue.next(lane)) {
     int I, J;
-    tile_pair_of(w, tiles, &I, &J);
+    tile_pair_of(w >> 1, tiles, &I, &J);
+    const int g0 = 2 * (int)(w & 1);
     const int i = I * 32 + lane;
     const bool vi = i < a.n;
     const int ii = vi ? i : 0;
@@ -417,7 +420,7 @@ k_gb_burial_half(GbArgs a, int tiles, long long items) {
     __syncwarp();
     float bsum = 0;
 #pragma unroll 1
-    for (int g = 0; g < 4; g++) {
+    for (int g = g0; g < g0 + 2; g++) {
       float gb[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) {
@@ -624,7 +627,7 @@ static void gb_passes_f32(const GbArgs &a, cudaStream_t st) {
   long long items, items2;
   halfpairs_grid(a.n, 1, &tiles, &items, &blocks);
   halfpairs_grid(a.n, 2, &tiles, &items2, &blocks2);
-  k_gb_burial_half<32><<<blocks, 32 * 32, 0, st>>>(a, tiles, items);
+  k_gb_burial_half<32><<<blocks2, 32 * 32, 0, st>>>(a, tiles, items2);
   k_gb_radii<<<(a.n + 127) / 128, 128, 0, st>>>(a);
   k_gb_partial_half<16><<<blocks, 16 * 32, 0, st>>>(a, tiles, items);
   k_gb_force_half<16><<<blocks2, 16 * 32, 0, st>>>(a, tiles, items2);
