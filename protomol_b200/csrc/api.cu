@@ -226,7 +226,8 @@ static int system_free(System *s) {
                   s->d_gb_vdwr, s->d_gb_scale, s->d_gb_offset, s->d_water, s->d_gb_born,
                   s->d_gb_psi, s->d_gb_partial, s->d_gb_fixed, s->d_pos, s->d_vel,
                   s->d_force, s->d_acc, s->d_status, s->d_pairbuf, s->d_paircount,
-                  s->d_stage, s->d_snap, s->d_step, s->d_sf_tile,
+                  s->d_stage, s->d_snap, s->d_step, s->d_sf_tile, s->d_gb_gst, s->d_gb_grad,
+                  s->d_rec,
                   s->d_sf_bits};
   for (auto &g : s->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);

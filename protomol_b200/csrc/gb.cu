@@ -628,7 +628,8 @@ static void gb_passes_f32(const GbArgs &a, cudaStream_t st) {
   halfpairs_grid(a.n, 1, &tiles, &items, &blocks);
   halfpairs_grid(a.n, 2, &tiles, &items2, &blocks2);
   k_gb_burial_half<32><<<blocks2, 32 * 32, 0, st>>>(a, tiles, items2);
-  k_gb_radii<<<(a.n + 127) / 128, 128, 0, st>>>(a);
+  // one-warp blocks: they fit beside a resident simple-full block
+  k_gb_radii<<<(a.n + 31) / 32, 32, 0, st>>>(a);
   k_gb_partial_half<16><<<blocks, 16 * 32, 0, st>>>(a, tiles, items);
   k_gb_force_half<16><<<blocks2, 16 * 32, 0, st>>>(a, tiles, items2);
 }
