@@ -111,31 +111,28 @@ __global__ void k_gb_radii(GbArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double self = 0.0;
   if (i < a.n) {
+    // the reciprocals of the static radii do not wait for the burial sum
+    const double ri = a.vdwr[i];
+    const double oi = ri - a.offset[i];
+    const double iri = 1 / ri, ioi = 1 / oi;
+    const double q = a.charge[i];
     double burial = (double)a.burial_fx[i] * (1.0 / kGbScale);
-    double ri = a.vdwr[i];
-    double oi = ri - a.offset[i];
     double psi = 0.5 * burial * oi;
     double tp = a.alpha * psi - a.beta * psi * psi + a.gamma * psi * psi * psi;
     double th = tanh(tp);
-    double inv = (1 / oi) - (1 / ri) * th;
+    double inv = ioi - iri * th;  // 1 / R_i
     double born = 1 / inv;
     // dR_i/d(burial sum) (GBForce.cpp:108-118 without the pair factor dBT):
     // R_i^2 rho~_i (1 - tanh^2) (alpha - 2 beta psi + 3 gamma psi^2) / rho_i
     double td = a.alpha - 2.0 * a.beta * psi + 3.0 * a.gamma * psi * psi;
-    const double dfac = born * born * oi * (1.0 - th * th) * td / ri;
+    const double dfac = born * born * oi * (1.0 - th * th) * td * iri;
     a.psi[i] = dfac;
     a.born[i] = born;
-    if (a.grad) {
-      const double q = a.charge[i];
-      a.grad[i] = make_float4((float)born, (float)(1.0 / born), (float)dfac,
-                              (float)(0.5 * q * q / (born * born)));
-    }
+    if (a.grad)
+      a.grad[i] = make_float4((float)born, (float)inv, (float)dfac, (float)(0.5 * q * q * inv * inv));
     a.burial_fx[i] = 0;
     a.partial_fx[i] = 0;
-    if (a.n > 1) {
-      double q = a.charge[i];
-      self = -0.5 * (q * q) * (1 / born) * a.dielec;
-    }
+    if (a.n > 1) self = -0.5 * (q * q) * inv * a.dielec;
   }
   self = warp_sum(self);
   if ((threadIdx.x & 31) == 0) red_add(&a.acc[ACC_COULOMB], to_fixed(self, kEnergyScale));
