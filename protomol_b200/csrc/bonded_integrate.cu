@@ -391,13 +391,14 @@ k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos
          double *__restrict__ vel, long long *__restrict__ force, int *__restrict__ status) {
   pdl_trigger();  // the list kernels after it may launch; they wait for this grid
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a.acc_zero && i < ACC_COUNT) a.acc_zero[i] = 0;
+  const bool valid = i < a.n;
   float d2 = 0.f;
-  if (i < a.n) {
+  double v[3] = {0, 0, 0}, x[3] = {0, 0, 0};
+  if (valid) {
     double F[3];
     for (int c = 0; c < 3; c++) F[c] = (double)force[c * a.n + i] * (1.0 / kForceScale);
     double m = mass[i];
-    double v[3] = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+    for (int c = 0; c < 3; c++) v[c] = vel[3 * i + c];
     for (int k = 0; k < a.kicks; k++) {
       if (a.langevin) {
         double g[3];
@@ -411,26 +412,20 @@ k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos
         for (int c = 0; c < 3; c++) v[c] = xadd(v[c], xmul(F[c], a.coef) / m);
       }
     }
-    for (int c = 0; c < 3; c++) vel[3 * i + c] = v[c];
     if (a.drift) {
       double dd = 0.0;
       for (int c = 0; c < 3; c++) {
-        double x = xadd(pos[3 * i + c], xmul(v[c], a.h));
-        pos[3 * i + c] = x;
-        if (!isfinite(x)) atomicOr(status, ST_NONFINITE);
+        x[c] = xadd(pos[3 * i + c], xmul(v[c], a.h));
         if (a.xbuild) {
-          const double e = x - a.xbuild[3 * i + c];
+          const double e = x[c] - a.xbuild[3 * i + c];
           dd += e * e;
         }
       }
       d2 = (float)dd;
-      if (a.rec)
-        write_pair_record(a.rec, a.n, i, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2],
-                          a.charge[i], a.type[i]);
     }
-    if (a.zero_force)
-      for (int c = 0; c < 3; c++) force[c * a.n + i] = 0;
   }
+  // The grid-wide decisions come before this thread's stores, so the fences
+  // they take wait for no stores of the update.
   if (a.xbuild) rebuild_decide<kUpdateThreads>(d2, a.ticket, a.rebuild, a.half_skin2, 0);
   if (a.step_inc) {
     // every block has read the counter before it counts itself done
@@ -446,6 +441,18 @@ k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos
       a.step_ptr[0] += 1ull;
     }
   }
+  if (a.acc_zero && i < ACC_COUNT) a.acc_zero[i] = 0;
+  if (!valid) return;
+  for (int c = 0; c < 3; c++) vel[3 * i + c] = v[c];
+  if (a.drift) {
+    for (int c = 0; c < 3; c++) {
+      pos[3 * i + c] = x[c];
+      if (!isfinite(x[c])) atomicOr(status, ST_NONFINITE);
+    }
+    if (a.rec) write_pair_record(a.rec, a.n, i, x[0], x[1], x[2], a.charge[i], a.type[i]);
+  }
+  if (a.zero_force)
+    for (int c = 0; c < 3; c++) force[c * a.n + i] = 0;
 }
 
 // phase: 0 = leapfrog first (half kick + drift), 1 = leapfrog middle (kick +
