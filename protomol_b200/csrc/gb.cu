@@ -513,8 +513,10 @@ k_gb_partial_half(GbArgs a, int tiles, long long items) {
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 1)
 k_gb_force_half(GbArgs a, int tiles, long long items) {
-  __shared__ float4 sh[WARPS][32], sl[WARPS][32], sg[WARPS][32], sr[WARPS][32];
-  __shared__ float sp[WARPS][32];
+  // per j: (x_hi, y_hi, z_hi, q) | (x_lo, y_lo, z_lo, R) |
+  // (1 / R, dR/dI, q^2 / 2R^2, partial sum) | (rho~, S rho~)
+  __shared__ float4 sh[WARPS][32], sl[WARPS][32], sr[WARPS][32];
+  __shared__ float2 sg[WARPS][32];
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
   __shared__ int counter;
   if (threadIdx.x == 0) counter = 0;
@@ -536,11 +538,12 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
     {
       const int j = J * 32 + lane;
       const int jj = j < a.n ? j : 0;
+      const float4 l = a.rec[a.n + jj], g = a.gst[jj], r = a.grad[jj];
       sh[wb][lane] = a.rec[jj];
-      sl[wb][lane] = a.rec[a.n + jj];
-      sg[wb][lane] = a.gst[jj];
-      sr[wb][lane] = a.grad[jj];
-      sp[wb][lane] = (float)((double)a.partial_fx[jj] * (1.0 / kGbScale));
+      sl[wb][lane] = make_float4(l.x, l.y, l.z, r.x);
+      sr[wb][lane] = make_float4(r.y, r.z, r.w,
+                                 (float)((double)a.partial_fx[jj] * (1.0 / kGbScale)));
+      sg[wb][lane] = make_float2(g.x, g.y);
     }
     __syncwarp();
     const int jn = a.n - J * 32;
@@ -551,7 +554,8 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int k = gq * 8 + u;
-        const float4 h = sh[wb][k], l = sl[wb][k], gj = sg[wb][k], rj = sr[wb][k];
+        const float4 h = sh[wb][k], l = sl[wb][k], rj = sr[wb][k];
+        const float2 gj = sg[wb][k];
         const bool use = vi && k < jn && (I < J || k > lane);
         const float dx = (h.x - hi.x) + (l.x - li.x);
         const float dy = (h.y - hi.y) + (l.y - li.y);
@@ -559,22 +563,22 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
         const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
         const float idist = rsqrt_nr(r2);
         const float dist = r2 * idist;
-        const float bj = rj.x, bb = ri.x * bj;
-        const float ex = __expf(-r2 * (q4bi * rj.y));
+        const float bj = l.w, bb = ri.x * bj;
+        const float ex = __expf(-r2 * (q4bi * rj.x));
         const float ifgb = rsqrt_nr(r2 + bb * ex);
         const float qq = hi.w * h.w;
         const float dRi = ri.z * gb_dBT_f32(dist, idist, gi.x, gj.y);
-        const float dRj = rj.z * gb_dBT_f32(dist, idist, gj.x, gi.y);
+        const float dRj = rj.y * gb_dBT_f32(dist, idist, gj.x, gi.y);
         const float pref = 0.5f * qq * (ifgb * ifgb * ifgb);
         // partialTerm[i][j] and [j][i] (GBPartialSum.cpp:33-41)
         const float ai = bj + r2 * q4bi;
-        const float aj = ri.x + 0.25f * r2 * rj.y;
+        const float aj = ri.x + 0.25f * r2 * rj.x;
         const float ptij = pref * ex * ai, ptji = pref * ex * aj;
         float f = -pref * ((2.0f * dist - 0.5f * ex * dist) + ex * dRi * ai + ex * dRj * aj);
         f -= ri.w * dRi;
-        f -= rj.w * dRj;
+        f -= rj.z * dRj;
         f -= (part_i - ptij) * dRi;
-        f -= (sp[wb][k] - ptji) * dRj;
+        f -= (rj.w - ptji) * dRj;
         f *= idist;
         f = use ? f : 0.0f;
         ep += use ? -qq * ifgb : 0.0f;
