@@ -507,16 +507,23 @@ k_gb_partial_half(GbArgs a, int tiles, long long items) {
 
 // Forces and pair energy over each unordered pair once (same tiling); the
 // pair force of GBForce::operator() is symmetric in i and j, so j receives
-// its opposite through warp_tsum8.  The partial sums are read straight from
-// their fixed-point accumulators.  Work items are halves of tile pairs
+// its opposite through warp_tsum8.  Work items are halves of tile pairs
 // (16 j atoms), so the warps of a block share this heaviest pass finely.
+//
+// GBForce::operator() (GBForce.cpp:70-124) forms the pair force as
+//   -pref (2 d - ex d / 2 + ex dR_i a_ij + ex dR_j a_ji) / d
+//   - [q_i^2 / 2R_i^2 + (P_i - pt_ij)] dR_i / d - [same for j] dR_j / d
+// with pt_ij = pref ex a_ij the pair's own term of the partial sum P_i.
+// The pt_ij terms cancel exactly, leaving
+//   -pref (2 - ex / 2) - (D_i dBT_ij + D_j dBT_ji) / d,
+//   D_i = (q_i^2 / 2R_i^2 + P_i) dR_i/dI_i,
+// a per-atom factor formed once per item; the FP64 pass keeps the
+// reference's grouping.
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 1)
 k_gb_force_half(GbArgs a, int tiles, long long items) {
-  // per j: (x_hi, y_hi, z_hi, q) | (x_lo, y_lo, z_lo, R) |
-  // (1 / R, dR/dI, q^2 / 2R^2, partial sum) | (rho~, S rho~)
+  // per j: (x_hi, y_hi, z_hi, q) | (x_lo, y_lo, z_lo, R) | (1 / R, D, rho~, S rho~)
   __shared__ float4 sh[WARPS][32], sl[WARPS][32], sr[WARPS][32];
-  __shared__ float2 sg[WARPS][32];
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
   __shared__ int counter;
   if (threadIdx.x == 0) counter = 0;
@@ -533,17 +540,17 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
     const bool vi = i < a.n;
     const int ii = vi ? i : 0;
     const float4 hi = a.rec[ii], li = a.rec[a.n + ii], gi = a.gst[ii], ri = a.grad[ii];
-    const float part_i = (float)((double)a.partial_fx[ii] * (1.0 / kGbScale));
+    const float Di =
+        (float)(((double)ri.w + (double)a.partial_fx[ii] * (1.0 / kGbScale)) * (double)ri.z);
     const float q4bi = 0.25f * ri.y;
     {
       const int j = J * 32 + lane;
       const int jj = j < a.n ? j : 0;
       const float4 l = a.rec[a.n + jj], g = a.gst[jj], r = a.grad[jj];
+      const double Dj = ((double)r.w + (double)a.partial_fx[jj] * (1.0 / kGbScale)) * (double)r.z;
       sh[wb][lane] = a.rec[jj];
       sl[wb][lane] = make_float4(l.x, l.y, l.z, r.x);
-      sr[wb][lane] = make_float4(r.y, r.z, r.w,
-                                 (float)((double)a.partial_fx[jj] * (1.0 / kGbScale)));
-      sg[wb][lane] = make_float2(g.x, g.y);
+      sr[wb][lane] = make_float4(r.y, (float)Dj, g.x, g.y);
     }
     __syncwarp();
     const int jn = a.n - J * 32;
@@ -555,7 +562,6 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
       for (int u = 0; u < 8; u++) {
         const int k = gq * 8 + u;
         const float4 h = sh[wb][k], l = sl[wb][k], rj = sr[wb][k];
-        const float2 gj = sg[wb][k];
         const bool use = vi && k < jn && (I < J || k > lane);
         const float dx = (h.x - hi.x) + (l.x - li.x);
         const float dy = (h.y - hi.y) + (l.y - li.y);
@@ -563,23 +569,13 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
         const float r2 = use ? dx * dx + dy * dy + dz * dz : 1.0f;
         const float idist = rsqrt_nr(r2);
         const float dist = r2 * idist;
-        const float bj = l.w, bb = ri.x * bj;
         const float ex = __expf(-r2 * (q4bi * rj.x));
-        const float ifgb = rsqrt_nr(r2 + bb * ex);
+        const float ifgb = rsqrt_nr(r2 + ri.x * l.w * ex);
         const float qq = hi.w * h.w;
-        const float dRi = ri.z * gb_dBT_f32(dist, idist, gi.x, gj.y);
-        const float dRj = rj.y * gb_dBT_f32(dist, idist, gj.x, gi.y);
         const float pref = 0.5f * qq * (ifgb * ifgb * ifgb);
-        // partialTerm[i][j] and [j][i] (GBPartialSum.cpp:33-41)
-        const float ai = bj + r2 * q4bi;
-        const float aj = ri.x + 0.25f * r2 * rj.x;
-        const float ptij = pref * ex * ai, ptji = pref * ex * aj;
-        float f = -pref * ((2.0f * dist - 0.5f * ex * dist) + ex * dRi * ai + ex * dRj * aj);
-        f -= ri.w * dRi;
-        f -= rj.z * dRj;
-        f -= (part_i - ptij) * dRi;
-        f -= (rj.w - ptji) * dRj;
-        f *= idist;
+        const float bti = gb_dBT_f32(dist, idist, gi.x, rj.w);
+        const float btj = gb_dBT_f32(dist, idist, rj.z, gi.y);
+        float f = -pref * (2.0f - 0.5f * ex) - idist * (Di * bti + rj.y * btj);
         f = use ? f : 0.0f;
         ep += use ? -qq * ifgb : 0.0f;
         fx -= dx * f; fy -= dy * f; fz -= dz * f;
