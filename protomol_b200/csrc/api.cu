@@ -696,7 +696,7 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
   int prio_low = 0, prio_high = 0;
   PM_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
   PM_CUDA(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, prio_high));
-  PM_CUDA(cudaStreamCreateWithPriority(&s->side2, cudaStreamNonBlocking, prio_high));
+  PM_CUDA(cudaStreamCreateWithPriority(&s->side2, cudaStreamNonBlocking, prio_low));
   PM_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
   PM_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
   PM_CUDA(cudaEventCreateWithFlags(&s->ev_join2, cudaEventDisableTiming));
