@@ -358,3 +358,46 @@ def test_all_pairs_small_and_ragged_sizes(ctx, n):
             assert np.abs(f).max() == 0.0, line
         assert _energy_ok(e[slot], re[key]), (line, e[slot], re[key])
     gs.close()
+
+
+def test_polymer_leapfrog_force_only_steps_vs_oracle(ctx):
+    """Ten leapfrog steps of a 300-atom polymer under GB + LJ + Coulomb all
+    pairs: the inner MD steps take the force-only kernels (no energies),
+    which the single evaluations above never run; the trajectory is
+    integrated on the host with the FP64 oracle's forces beside it
+    (LeapfrogIntegrator.cpp:33-104: half kick, drift, forces, half kick)."""
+    import oracle
+    from protomol_b200 import systems
+    sm = systems.gb_polymer(300, seed=21)
+    lines = ["GBBornRadii -algorithm NonbondedSimpleFull",
+             "GBPartialSum -algorithm NonbondedSimpleFull",
+             "GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.5",
+             "LennardJones -algorithm NonbondedSimpleFull",
+             "Coulomb -algorithm NonbondedSimpleFull"]
+    gs = GpuSystem(ctx, sm, "mixed")
+    ff = ForceFactory(gs)
+    for line in lines:
+        ff.make(line)
+    steps, dt = 10, 1.0
+    LeapfrogIntegrator(dt).run(gs, steps)
+    x_gpu, v_gpu = gs.positions(), gs.velocities()
+    gs.close()
+
+    def forces(pos):
+        s = oracle.System(pos=pos, charge=sm.charge, type=sm.type, molecule=sm.molecule,
+                          lj=sm.lj, excl=sm.exclusions, periodic=False, box=sm.box,
+                          mass=sm.mass, water=sm.water, gb_vdwr=sm.gb_vdwr,
+                          gb_scale=sm.gb_scale, gb_offset=sm.gb_offset, gb_obc=sm.gb_obc)
+        return (oracle.gb_force(s, 1.0, 78.5)[0] + oracle.simplefull_force(s, "LennardJones")[0]
+                + oracle.simplefull_force(s, "Coulomb")[0])
+
+    h = dt * oracle.INV_TIMEFACTOR
+    x, v = sm.pos.copy(), sm.vel.copy()
+    f = forces(x)
+    for _ in range(steps):
+        v = oracle.kick(sm.mass, f, 0.5 * h, v)
+        x = oracle.drift(v, h, x)
+        f = forces(x)
+        v = oracle.kick(sm.mass, f, 0.5 * h, v)
+    assert np.abs(x_gpu - x).max() <= 1e-6, np.abs(x_gpu - x).max()
+    assert np.abs(v_gpu - v).max() / np.abs(v).max() <= 1e-5
