@@ -1279,7 +1279,10 @@ static int run_enqueue(System *s, const pmgpu_integrator *it, long n_steps) {
     k++;
   }
   prof_begin(s, PMGPU_PHASE_INTEGRATE);
-  int ri = integrate_kick_drift(s, it, lang ? 5 : 2);
+  // the closing half kick also takes the slot forces a force-only
+  // evaluation may have left (a run of zero steps)
+  int ri = integrate_kick_drift(s, it, lang ? 5 : 2, 0,
+                                s->lists.size() == 1 ? &s->lists[0] : nullptr);
   prof_end(s);
   PM_CHECK(ri);
   s->kernels += s->n > 0;

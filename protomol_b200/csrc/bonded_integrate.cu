@@ -375,6 +375,11 @@ struct UpdateArgs {
   float4 *rec;
   const double *charge;
   const int *type;
+  // the pair list's slot-ordered force buffer left by a force-only step
+  // (null: none): added into the forces here and cleared
+  long long *fslot;
+  const int *slot_of;
+  int ns;
 };
 
 __global__ void k_step_set(unsigned long long *step, unsigned long long v) { *step = v; }
@@ -394,9 +399,17 @@ k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos
   const bool valid = i < a.n;
   float d2 = 0.f;
   double v[3] = {0, 0, 0}, x[3] = {0, 0, 0};
+  long long Fx[3] = {0, 0, 0};
+  int slot = -1;
   if (valid) {
+    for (int c = 0; c < 3; c++) Fx[c] = force[c * a.n + i];
+    if (a.fslot) {
+      slot = a.slot_of[i];
+      if (slot >= 0)
+        for (int c = 0; c < 3; c++) Fx[c] += a.fslot[(size_t)c * a.ns + slot];
+    }
     double F[3];
-    for (int c = 0; c < 3; c++) F[c] = (double)force[c * a.n + i] * (1.0 / kForceScale);
+    for (int c = 0; c < 3; c++) F[c] = (double)Fx[c] * (1.0 / kForceScale);
     double m = mass[i];
     for (int c = 0; c < 3; c++) v[c] = vel[3 * i + c];
     for (int k = 0; k < a.kicks; k++) {
@@ -451,8 +464,12 @@ k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos
     }
     if (a.rec) write_pair_record(a.rec, a.n, i, x[0], x[1], x[2], a.charge[i], a.type[i]);
   }
+  if (slot >= 0)
+    for (int c = 0; c < 3; c++) a.fslot[(size_t)c * a.ns + slot] = 0;
   if (a.zero_force)
     for (int c = 0; c < 3; c++) force[c * a.n + i] = 0;
+  else if (a.fslot)
+    for (int c = 0; c < 3; c++) force[c * a.n + i] = Fx[c];
 }
 
 // phase: 0 = leapfrog first (half kick + drift), 1 = leapfrog middle (kick +
@@ -511,6 +528,14 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int z
   a.charge = s->d_charge;
   a.type = s->d_type;
   s->rec_fresh = a.rec != nullptr;
+  a.fslot = nullptr;
+  a.slot_of = nullptr;
+  a.ns = 0;
+  if (list && list->built && s->n) {
+    a.fslot = list->d_fslot;
+    a.slot_of = list->d_slot_of;
+    a.ns = list->ns_max;
+  }
   if (list && list->built && a.drift && s->n) {
     const float hs = (float)(0.5 * list->skin);
     a.xbuild = list->d_xbuild;

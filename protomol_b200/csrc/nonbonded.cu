@@ -185,7 +185,8 @@ k_sort_cols(const int *__restrict__ rebuild, int nzb, float inv_z,
             int *__restrict__ col_count, const int *__restrict__ col_u,
             const int *__restrict__ col_base, const int *__restrict__ unsorted,
             const unsigned *__restrict__ zkey, int *__restrict__ sorted,
-            int *__restrict__ key_start, int *__restrict__ status) {
+            int *__restrict__ slot_of, int *__restrict__ key_start,
+            int *__restrict__ status) {
   pdl_wait();  // the predecessor's writes are visible from here on
   pdl_trigger();
   if (!*rebuild) return;
@@ -231,8 +232,11 @@ k_sort_cols(const int *__restrict__ rebuild, int nzb, float inv_z,
     return b < 0 ? 0 : (b >= nzb ? nzb - 1 : b);
   };
   int *ks = key_start + (size_t)col * nzb;
-  for (int k = threadIdx.x; k < pend - base; k += kSortThreads)
-    sorted[base + k] = k < m ? (int)(keys[k] & 0xffffffffu) : -1;
+  for (int k = threadIdx.x; k < pend - base; k += kSortThreads) {
+    const int atom = k < m ? (int)(keys[k] & 0xffffffffu) : -1;
+    sorted[base + k] = atom;
+    if (atom >= 0) slot_of[atom] = base + k;
+  }
   for (int k = threadIdx.x; k < m; k += kSortThreads) {
     const int b = bin_of(k), prev = k ? bin_of(k - 1) : -1;
     for (int q = prev + 1; q <= b; q++) ks[q] = base + k;
@@ -737,6 +741,7 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   PM_CHECK(dev_alloc(s, &nl->d_col_base, sizeof(int) * (nl->ncol + 1)));
   PM_CHECK(dev_alloc(s, &nl->d_key_start, sizeof(int) * (nl->nkeys + 1)));
   PM_CHECK(dev_alloc(s, &nl->d_sorted, sizeof(int) * ns));
+  PM_CHECK(dev_alloc(s, &nl->d_slot_of, sizeof(int) * std::max(1, s->n)));
   PM_CUDA(cudaMemsetAsync(nl->d_sorted, 0xff, sizeof(int) * ns, s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_offset, sizeof(double) * 3 * nn));
   PM_CHECK(dev_alloc(s, &nl->d_xbuild, sizeof(double) * 3 * nn));
@@ -763,7 +768,8 @@ int nb_list_free(System *s, NeighborList *nl) {
   void *ptrs[] = {nl->d_key, nl->d_zkey, nl->d_unsorted, nl->d_col_count, nl->d_col_u,
                   nl->d_col_cursor, nl->d_col_base, nl->d_key_start, nl->d_sorted,
                   nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
-                  nl->d_bb, nl->d_fslot, nl->d_tiles, nl->d_tile_count, nl->d_maxdisp,
+                  nl->d_bb, nl->d_fslot, nl->d_slot_of, nl->d_tiles, nl->d_tile_count,
+                  nl->d_maxdisp,
                   nl->d_rebuild};
   for (void *p : ptrs) dev_free(s, p);
   nl->d_key = nl->d_unsorted = nl->d_col_count = nl->d_col_u = nl->d_col_cursor = nullptr;
@@ -775,6 +781,7 @@ int nb_list_free(System *s, NeighborList *nl) {
   nl->d_xw = nullptr;
   nl->d_tiles = nullptr;
   nl->d_fslot = nullptr;
+  nl->d_slot_of = nullptr;
   nl->d_maxdisp = nullptr;
   return PMGPU_OK;
 }
@@ -817,7 +824,8 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
                        nl->d_col_cursor, nl->d_unsorted));
     PM_CUDA(launch_pdl(k_sort_cols, nl->ncol, kSortThreads, 0, q, nl->d_rebuild, nl->nzb,
                        (float)(1.0 / nl->cs[2]), nl->d_col_count, nl->d_col_u, nl->d_col_base,
-                       nl->d_unsorted, nl->d_zkey, nl->d_sorted, nl->d_key_start,
+                       nl->d_unsorted, nl->d_zkey, nl->d_sorted, nl->d_slot_of,
+                       nl->d_key_start,
                        s->d_status));
   }
   PM_CUDA(launch_pdl(s->precision == PMGPU_PREC_MIXED ? k_gather<true> : k_gather<false>, nbs,
@@ -1032,6 +1040,9 @@ int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode) {
     fill_pair_args<double>(a, s, nl, t);
     PM_CHECK(launch_pairs<double>(a, s->stream, mode, t));
   }
+  // In the force-only steps of an MD run with one list the next update
+  // kernel adds the slot buffer into the forces itself (and clears it)
+  if (mode == PAIR_FORCE && s->lists.size() == 1) return PMGPU_OK;
   PM_CUDA(launch_pdl(k_slot_forces, (nl->ns_max + 255) / 256, 256, 0, s->stream, nl->ns_max,
                      s->n, nl->d_sorted, nl->d_fslot, s->d_force));
   PM_CUDA(cudaGetLastError());

@@ -156,6 +156,7 @@ struct NeighborList {
   int *d_mol_s = nullptr;        // ns_max molecule of each slot (-1 padding)
   float4 *d_bb = nullptr;        // 2 per 4-atom cluster: lower, upper corner
   long long *d_fslot = nullptr;  // 3 planes of ns_max: pair forces by slot (fixed point)
+  int *d_slot_of = nullptr;  // atom -> slot of the current order (rebuild steps write it)
   uint4 *d_tiles = nullptr;      // nrows rows of cap tiles (row r: cluster r / kRowParts)
   int *d_tile_count = nullptr;   // nrows
   unsigned int *d_maxdisp = nullptr;  // rebuild check: block ticket, max displacement^2 bits
