@@ -164,7 +164,10 @@ int pmgpu_system_get_forces(pmgpu_system *sys, double *forces);
  * evaluation. */
 int pmgpu_system_get_energies(pmgpu_system *sys, double *energies,
                               double *virial);
-/* The CUDA stream (a cudaStream_t) every kernel of this system runs on. */
+/* The CUDA stream (a cudaStream_t) that orders all of this system's work:
+ * each evaluation forks its concurrent terms from it onto two internal
+ * streams and joins them back before it ends, so work a caller enqueues on
+ * this stream after a call sees that call's results. */
 void *pmgpu_system_stream(pmgpu_system *sys);
 /* Device pointers of the resident state: positions and velocities as
  * double[3n] (Vector3DBlock layout), forces as int64 fixed point
