@@ -202,6 +202,51 @@ def algorithmic_bytes_per_step(n: int, grid: int) -> dict:
     return parts
 
 
+def restatement_baseline(gs, sysm, samples) -> dict:
+    """The builder's FP64 CPU restatement of the same step's forces (the
+    oracle's cutoff LJ, FullEwald real and correction terms and SPME
+    reciprocal at the benched grid, order and alpha, plus bonds and angles),
+    timed on one host core, at positions the benched run reached; at each
+    sample the GPU's force-only forces (the MD step's kernels) and its FP64
+    energies are compared with it.  Runs after the timed region."""
+    import oracle
+    from oracle import spme
+    s0 = oracle.System(pos=sysm.pos, charge=sysm.charge, type=sysm.type,
+                       molecule=sysm.molecule, lj=sysm.lj, excl=sysm.exclusions,
+                       periodic=True, box=sysm.box, mass=sysm.mass)
+    sw = oracle.Switch("C2", RC, LJ_SWITCHON)
+    errs, e_errs, cpu_s = [], [], []
+    for x in samples:
+        gs.set_positions(x)
+        fg = gs.evaluate_forces()
+        eg, _ = gs.evaluate()
+        s = s0.with_positions(x)
+        t0 = time.perf_counter()
+        f, e, _ = oracle.cutoff_force(s, RC, RC, [("LennardJones", sw)])
+        ew = oracle.ewald_params(s, ALPHA, math.exp(-(ALPHA * RC) ** 2))
+        ew.rc = RC
+        fr, er, _ = oracle.ewald_real(s, ew, RC)
+        fk, ek = spme.reciprocal(s.pos, s.charge, s.box, ALPHA, ORDER, GRID)
+        fc, ec, _ = oracle.ewald_correction(s, ew)
+        es, eq = oracle.ewald_self(s, ew)
+        fb, eb, _ = oracle.bonded_force(s, sysm.bonds, sysm.bond_params, sysm.angles,
+                                        sysm.angle_params)
+        cpu_s.append(time.perf_counter() - t0)
+        fo = f + fr + fk + fc + fb
+        eo = np.array([er + ek + ec + es + eq, e["lj"], eb["bond"], eb["angle"]])
+        errs.append(float(np.sqrt(((fg - fo) ** 2).sum() / (fo ** 2).sum())))
+        e_errs.append(float(abs(eg[:4].sum() - eo.sum()) / abs(eo.sum())))
+    dt = statistics.median(cpu_s)
+    return {"force_rms_rel_err": max(errs), "energy_rel_err": max(e_errs),
+            "per_sample_force_rms_rel_err": errs, "per_sample_energy_rel_err": e_errs,
+            "restatement": {"value": DT_FS * 1e-6 * 86400.0 / dt, "unit": "ns/day", "cores": 1,
+                            "kind": "port", "s_per_md_step": dt,
+                            "sample": f"{len(samples)} force evaluations of the 23,550-atom box "
+                                      "by the builder's FP64 CPU restatement (cutoff LJ C2, "
+                                      "Ewald real + SPME order 4 on 64^3 + correction, bonds, "
+                                      "angles), 1 core"}}
+
+
 def ensemble_line(args, ctx, world: int, rank: int, dist=None) -> dict:
     """The batched ensemble: --requests resident TIP3P boxes (100-1,000 waters
     log-uniform, split over the ranks), each advanced in 50-step leapfrog
@@ -553,7 +598,12 @@ def main():
     k0 = gs.kernel_count()
     builds0 = gs.forces[3].stats()["list_builds"]
     total_ms = 0.0
-    for _ in range(args.steps):
+    # positions at the end of some timed segments (copied after the segment's
+    # end event), where the accuracy against the FP64 restatement is checked
+    # once the timing is over
+    keep = sorted({0, 1, args.steps - 1} & set(range(args.steps)))
+    samples = []
+    for k in range(args.steps):
         with torch.cuda.stream(stream):
             flush.add_(1.0)
             a = torch.cuda.Event(enable_timing=True)
@@ -564,6 +614,8 @@ def main():
             b.record(stream)
         b.synchronize()
         total_ms += a.elapsed_time(b)
+        if k in keep:
+            samples.append(gs.positions())
     torch.cuda.synchronize()
     launches = gs.kernel_count() - k0
     builds = gs.forces[3].stats()["list_builds"] - builds0
@@ -646,6 +698,18 @@ def main():
             line["clocks"] = clk
         if forms:
             line["forms"] = forms
+        acc = None
+        if world == 1:
+            try:
+                acc = restatement_baseline(gs, sysm, samples)
+                line["accuracy"] = {k: acc[k] for k in acc if k != "restatement"}
+                line["accuracy"]["target"] = {"force_rms_rel_err": 1e-5, "energy_rel_err": 1e-6}
+                line["accuracy"]["ok"] = (acc["force_rms_rel_err"] <= 1e-5 and
+                                          acc["energy_rel_err"] <= 1e-6)
+                line["accuracy"]["at"] = (f"end of timed segments {keep} ({args.segment} MD "
+                                          f"steps each) against the FP64 restatement")
+            except Exception as ex:  # reported, never fatal
+                line["accuracy"] = {"error": str(ex)[:200]}
         if world == 1 and os.path.exists(REF_BIN):
             try:
                 r = run_reference(2)
@@ -656,7 +720,13 @@ def main():
                                                   "Rc 9 A) + LJ C2 8->9 A + bonds/angles, 1 core"}
             except Exception as ex:  # reported, never fatal
                 line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+        if acc is not None:
+            line.setdefault("cpu_baseline", {})["restatement"] = acc["restatement"]
         print(json.dumps(line), flush=True)
+        if isinstance(line.get("accuracy"), dict) and line["accuracy"].get("ok") is False:
+            print("accuracy outside the stated tolerance", file=sys.stderr)
+            gs.close()
+            sys.exit(1)
     gs.close()
     if dist:
         dist.barrier()

@@ -202,6 +202,14 @@ int pmgpu_force_pme_add(pmgpu_system *sys, double alpha, double rc,
  * force/GB/GB{BornRadii,PartialSum,Force}.cpp. */
 int pmgpu_force_gb_add(pmgpu_system *sys, double solute_dielec,
                        double solvent_dielec, int *force_id);
+/* GBACEForce (force/GB/GBACEForce.cpp:17-209): the ACE nonpolar solvation
+ * term on the OBC Born radii, vacuum, all pairs; its energy goes to
+ * PMGPU_E_COULOMB as in the reference.  solvation_param is -solvationparam
+ * [kcal/mol/A^2] (reference default 2.26 / 418.4), water_sphere_radius is
+ * -watersphereradius [A] (default 1.4).  Evaluated with a GB force, both
+ * share one Born-radius computation. */
+int pmgpu_force_gbace_add(pmgpu_system *sys, double solvation_param,
+                          double water_sphere_radius, int *force_id);
 /* GB forces (the same three passes as pmgpu_force_gb_add) for callers that
  * must not allocate device memory: a host that has given all of HBM to its
  * own pool, a plugin that may only use the buffers it is handed, or a loop
@@ -219,7 +227,9 @@ int pmgpu_force_gb_add(pmgpu_system *sys, double solute_dielec,
  * so n_atoms above PMGPU_GB_STATIC_MAX_ATOMS is rejected with
  * PMGPU_ERR_ARG.  The first call on each device (with that device current)
  * looks up the array's device address; make that first call before any
- * stream capture.  All calls on a device share the array and it keeps the
+ * stream capture.  The address is kept for the life of the process, so a
+ * host that calls cudaDeviceReset (which ends the context that address
+ * belongs to) must not call this entry point afterwards.  All calls on a device share the array and it keeps the
  * previous call's contents (the call clears what must start at zero): two
  * calls whose work overlaps on the GPU race and both results are wrong, so
  * issue them on one stream or otherwise serialise them. */
@@ -241,13 +251,19 @@ int pmgpu_force_torsion_add(pmgpu_system *sys, int dihedrals, int impropers,
 int pmgpu_force_set_enabled(pmgpu_system *sys, int force_id, int enabled);
 
 /* Evaluate all enabled forces at the resident positions.  energies (may be
- * NULL) gets PMGPU_E_COUNT values, virial (may be NULL) 9. */
+ * NULL) gets PMGPU_E_COUNT values, virial (may be NULL) 9.  With both NULL
+ * the evaluation is force-only: it runs the kernels of an inner MD step
+ * (including the specialised force-only pair kernels), computes no
+ * energies, and pmgpu_system_get_energies then reports zeros; the forces
+ * (pmgpu_system_get_forces) are complete. */
 int pmgpu_evaluate(pmgpu_system *sys, double *energies, double *virial);
 
 /* ProtoMol SystemForce::evaluate semantics for one force term: uploads
  * positions (3n doubles), evaluates that term only, ADDS its forces into
  * forces (3n doubles) and its energies into energies (ScalarStructure
- * slots, PMGPU_E_COUNT) and, if virial != NULL, its virial (9). */
+ * slots, PMGPU_E_COUNT) and, if virial != NULL, its virial (9).  With
+ * energies and virial both NULL the term is evaluated force-only, as in
+ * pmgpu_evaluate. */
 int pmgpu_force_evaluate(pmgpu_system *sys, int force_id, const double *pos,
                          double *forces, double *energies, double *virial);
 
@@ -302,7 +318,18 @@ typedef struct {
   long long clusters;          /* 8-atom i-clusters */
   long long list_builds;       /* pair-list builds so far */
   int cells[3];                /* sort-grid dims of the cutoff path */
+  int pair_kernel;             /* form of the last pair-kernel launch of the
+                                  force's list: PMGPU_PAIRK_* */
 } pmgpu_stats;
+/* Pair-kernel forms: the generic kernel (any terms and switches, energies,
+ * virial) and the specialised force-only FP32 kernels of the inner MD steps
+ * (every term with one cutoff, box edges at least twice the cutoff). */
+enum {
+  PMGPU_PAIRK_GENERIC = 0,
+  PMGPU_PAIRK_LJC2_EWALD = 1,   /* LJ with C2 switching + Ewald real space */
+  PMGPU_PAIRK_LJC2_COULC2 = 2,  /* LJ C2 + Coulomb C2 */
+  PMGPU_PAIRK_LJC2_COULC1 = 3   /* LJ C2 + Coulomb C1 */
+};
 /* Counts from the last evaluation of force_id (pairs_in_cutoff requires
  * the force to have been evaluated with counting on; see
  * pmgpu_set_count_pairs). */

@@ -286,6 +286,48 @@ def gb_force(sysm: System, solute_dielec: float = 1.0, solvent_dielec: float = 8
     return f, e.value, born
 
 
+def bonded_force(sysm: System, bonds=None, bond_params=None, angles=None, angle_params=None):
+    """Harmonic bonds and Urey-Bradley angles -> (forces (n,3), {"bond": E,
+    "angle": E}, virial (3,3))."""
+    cs = sysm.c()
+    f = np.zeros((sysm.n, 3))
+    out, vt = {}, np.zeros(9)
+    for key, atoms, prm, fn, w in (("bond", bonds, bond_params, lib().orc_bond_force, 2),
+                                   ("angle", angles, angle_params, lib().orc_angle_force, 3)):
+        if atoms is None or len(atoms) == 0:
+            out[key] = 0.0
+            continue
+        a = np.ascontiguousarray(atoms, dtype=np.int32).reshape(-1)
+        p = np.ascontiguousarray(prm, dtype=np.float64).reshape(-1)
+        e = C.c_double(0)
+        v = np.zeros(9)
+        assert fn(C.byref(cs), len(a) // w, _ptr(a), _ptr(p), _ptr(f), C.byref(e), _ptr(v)) == 0
+        out[key] = e.value
+        vt += v
+    return f, out, vt.reshape(3, 3)
+
+
+ACE_SIGMA = 2.26 / 418.4  # GBACEForce -solvationparam default (GBACEForce.cpp:226)
+ACE_RHO = 1.4             # -watersphereradius default (GBACEForce.cpp:229)
+
+
+def gbace_force(sysm: System, sigma: float = ACE_SIGMA, rho_s: float = ACE_RHO):
+    """GBACEForce on the GBBornRadii radii -> (forces (n,3), energy)."""
+    cs = sysm.c()
+    vd = np.ascontiguousarray(sysm.gb_vdwr, np.float64)
+    sc = np.ascontiguousarray(sysm.gb_scale, np.float64)
+    of = np.ascontiguousarray(sysm.gb_offset, np.float64)
+    wa = np.ascontiguousarray(sysm.water if sysm.water is not None else np.zeros(sysm.n),
+                              np.int32)
+    g = _GB(vd.ctypes.data, sc.ctypes.data, of.ctypes.data, wa.ctypes.data,
+            sysm.gb_obc[0], sysm.gb_obc[1], sysm.gb_obc[2], 1.0, 80.0)
+    f = np.zeros((sysm.n, 3))
+    e = C.c_double(0)
+    assert lib().orc_gbace_force(C.byref(cs), C.byref(g), C.c_double(sigma), C.c_double(rho_s),
+                                 _ptr(f), C.byref(e)) == 0
+    return f, e.value
+
+
 def kick(mass, forces, h, vel):
     vel = np.ascontiguousarray(vel, np.float64).copy()
     lib().orc_kick(len(mass), _ptr(np.ascontiguousarray(mass, np.float64)),

@@ -972,18 +972,10 @@ void orc_ewald_self(const orc_system *s, const orc_ewald *e, double *self,
 
 /* ------------------------------------------------------------------ */
 /* GB, OBC.  Pairs i < j in the SimpleFull order, vacuum differences. */
-int orc_gb_force(const orc_system *s, const orc_gb *g, double *born,
-                 double *forces, double *energy) {
+/* Burial sums, psi and Born radii (GBBornRadii pair op and postProcess). */
+static void gb_burial_born(const orc_system *s, const orc_gb *g, double *burial, double *psi,
+                           double *born) {
   int n = s->n, i, j;
-  double *burial = (double *)calloc(n, sizeof(double));
-  double *psi = (double *)calloc(n, sizeof(double));
-  double *partial = (double *)calloc(n, sizeof(double));
-  double *ptm = (double *)calloc((size_t)n * n, sizeof(double)); /* partialTerm[i][j] */
-  int *selfcount = (int *)calloc(n, sizeof(int));
-  double *selfE = (double *)calloc(n, sizeof(double));
-  const double dielec = (1 / g->solute_dielec) - (1 / g->solvent_dielec);
-  double en = 0.0;
-  if (!burial || !psi || !partial || !ptm || !selfcount || !selfE) return -1;
   /* GBBornRadii pair op (GBBornRadii.cpp:15-128) */
   for (i = 0; i < n; i++)
     for (j = i + 1; j < n; j++) {
@@ -1030,6 +1022,21 @@ int orc_gb_force(const orc_system *s, const orc_gb *g, double *born,
     inv = (1 / oi) - (1 / ri) * tanh(tp);
     born[i] = 1 / inv;
   }
+}
+
+int orc_gb_force(const orc_system *s, const orc_gb *g, double *born,
+                 double *forces, double *energy) {
+  int n = s->n, i, j;
+  double *burial = (double *)calloc(n, sizeof(double));
+  double *psi = (double *)calloc(n, sizeof(double));
+  double *partial = (double *)calloc(n, sizeof(double));
+  double *ptm = (double *)calloc((size_t)n * n, sizeof(double)); /* partialTerm[i][j] */
+  int *selfcount = (int *)calloc(n, sizeof(int));
+  double *selfE = (double *)calloc(n, sizeof(double));
+  const double dielec = (1 / g->solute_dielec) - (1 / g->solvent_dielec);
+  double en = 0.0;
+  if (!burial || !psi || !partial || !ptm || !selfcount || !selfE) return -1;
+  gb_burial_born(s, g, burial, psi, born);
   /* GBPartialSum (GBPartialSum.cpp:11-42) */
   for (i = 0; i < n; i++)
     for (j = i + 1; j < n; j++) {
@@ -1146,6 +1153,126 @@ int orc_gb_force(const orc_system *s, const orc_gb *g, double *born,
   return 0;
 }
 
+/* ProtoMol's integer power, MathUtilities.cpp:114-134 (square and
+ * multiply, so results round as the reference's do). */
+static double pm_power(double x, int n) {
+  double z = 1.0, y = x;
+  int m = n;
+  if (n == 0) return 1.0;
+  if (n < 0) return 1.0 / pm_power(x, -n);
+  while (m > 0) {
+    if (m & 1) z *= y;
+    y *= y;
+    m >>= 1;
+  }
+  return z;
+}
+
+/* GBACEForce (force/GB/GBACEForce.cpp:17-209): the ACE nonpolar term on the
+ * Born radii of GBBornRadii.  Energy: per atom 4 pi sigma (r_i + rho_s)^2
+ * (r_i / R_i)^6, set once for every atom that takes part in a pair
+ * (ACEPotentialCount, summed in postProcess :161-171); pair force
+ * c1 (c_i R_i^-7 dR_i/dr + c_j R_j^-7 dR_j/dr) / d with c1 = 24 pi sigma and
+ * c_i = (r_i + rho_s)^2 r_i^6, dR/dr as in GBForce.  "pi" is the
+ * reference's own constant 3.14169 (GBACEForce.cpp:6).  Every unordered pair
+ * once (NonbondedSimpleFull, OneAtomPairNoExclusion: exclusions ignored). */
+#define ACE_PI 3.14169
+int orc_gbace_force(const orc_system *s, const orc_gb *g, double sigma, double rho_s,
+                    double *forces, double *energy) {
+  int n = s->n, i, j;
+  double *burial = (double *)calloc(n > 0 ? n : 1, sizeof(double));
+  double *psi = (double *)calloc(n > 0 ? n : 1, sizeof(double));
+  double *born = (double *)calloc(n > 0 ? n : 1, sizeof(double));
+  double *ace = (double *)calloc(n > 0 ? n : 1, sizeof(double));
+  int *acecount = (int *)calloc(n > 0 ? n : 1, sizeof(int));
+  double en = 0.0;
+  if (!burial || !psi || !born || !ace || !acecount) return -1;
+  gb_burial_born(s, g, burial, psi, born);
+  for (i = 0; i < n; i++)
+    for (j = i + 1; j < n; j++) {
+      double d[3], r2, dist, ri, rj, oi, oj, Si, Sj, psi_i, psi_j, tpi, tpj, bi, bj, c1, ci,
+          cj, L, U, Lj, Uj, dL, dU, dC, dLj, dUj, dCj, th_i, th_j, tdi, tdj, Sit, Sjt, dBTi,
+          dRi, dBTj, dRj, force;
+      int t;
+      for (t = 0; t < 3; t++) d[t] = s->pos[3 * j + t] - s->pos[3 * i + t];
+      r2 = norm2(d);
+      dist = sqrt(r2);
+      ri = g->vdwr[i]; rj = g->vdwr[j];
+      oi = ri - g->offset[i]; oj = rj - g->offset[j];
+      Si = g->scale[i]; Sj = g->scale[j];
+      psi_i = psi[i]; psi_j = psi[j];
+      tpi = g->alpha_obc * psi_i - g->beta_obc * psi_i * psi_i +
+            g->gamma_obc * psi_i * psi_i * psi_i;
+      tpj = g->alpha_obc * psi_j - g->beta_obc * psi_j * psi_j +
+            g->gamma_obc * psi_j * psi_j * psi_j;
+      bi = born[i]; bj = born[j];
+      if (!acecount[i]) {
+        ace[i] = 4 * ACE_PI * sigma * (ri + rho_s) * (ri + rho_s) * pm_power(ri / bi, 6);
+        acecount[i] = 1;
+      }
+      if (!acecount[j]) {
+        ace[j] = 4 * ACE_PI * sigma * (rj + rho_s) * (rj + rho_s) * pm_power(rj / bj, 6);
+        acecount[j] = 1;
+      }
+      c1 = 24 * ACE_PI * sigma;
+      ci = (ri + rho_s) * (ri + rho_s) * pow(ri, 6);
+      cj = (rj + rho_s) * (rj + rho_s) * pow(rj, 6);
+      if (oi >= dist + Sj * oj) {
+        L = 1; U = 1;
+      } else {
+        L = (oi > fabs(dist - Sj * oj)) ? oi : fabs(dist - Sj * oj);
+        U = dist + Sj * oj;
+      }
+      if (oj >= dist + Si * oi) {
+        Lj = 1; Uj = 1;
+      } else {
+        Lj = (oj > fabs(dist - Si * oi)) ? oj : fabs(dist - Si * oi);
+        Uj = dist + Si * oi;
+      }
+      dL = (oi <= (dist - Sj * oj)) ? 1 : 0;
+      dU = (oi < (dist + Sj * oj)) ? 1 : 0;
+      dC = (oi <= (Sj * oj - dist)) ? 2 * (1 / L) * (1 / L) * dL : 0;
+      dLj = (oj <= (dist - Si * oi)) ? 1 : 0;
+      dUj = (oj < (dist + Si * oi)) ? 1 : 0;
+      dCj = (oj <= (Si * oi - dist)) ? 2 * (1 / Lj) * (1 / Lj) * dLj : 0;
+      th_i = tanh(tpi);
+      th_j = tanh(tpj);
+      tdi = (g->alpha_obc - 2 * g->beta_obc * psi_i + 3 * g->gamma_obc * psi_i * psi_i);
+      tdj = (g->alpha_obc - 2 * g->beta_obc * psi_j + 3 * g->gamma_obc * psi_j * psi_j);
+      Sit = (Si * oi) / dist;
+      Sjt = (Sj * oj) / dist;
+      dBTi = -0.5 * dL * (1 / (L * L)) + 0.5 * dU * (1 / (U * U)) +
+             0.125 * ((1 / (U * U)) - (1 / (L * L))) +
+             0.125 * dist * ((2 / (L * L * L)) * dL - (2 / (U * U * U)) * dU) -
+             0.25 * (1 / (dist * dist)) * log(L / U) +
+             (U / (4 * dist * L)) * ((1 / U) * dL - (L / (U * U)) * dU) -
+             0.125 * pm_power(Sjt, 2) * ((1 / (L * L)) - (1 / (U * U))) +
+             0.25 * ((Sj * Sj * oj * oj) / (dist * U * U * U)) * dU -
+             0.25 * ((Sj * Sj * oj * oj) / (dist * L * L * L)) * dL + dC;
+      dRi = pm_power(bi, 2) * oi * (1 - th_i * th_i) * tdi * (1 / ri) * dBTi;
+      dBTj = -0.5 * dLj * (1 / (Lj * Lj)) + 0.5 * dUj * (1 / (Uj * Uj)) +
+             0.125 * ((1 / (Uj * Uj)) - (1 / (Lj * Lj))) +
+             0.125 * dist * ((2 / (Lj * Lj * Lj)) * dLj - (2 / (Uj * Uj * Uj)) * dUj) -
+             0.25 * (1 / (dist * dist)) * log(Lj / Uj) +
+             (Uj / (4 * dist * Lj)) * ((1 / Uj) * dLj - (Lj / (Uj * Uj)) * dUj) -
+             0.125 * pm_power(Sit, 2) * ((1 / (Lj * Lj)) - (1 / (Uj * Uj))) +
+             0.25 * ((Si * Si * oi * oi) / (dist * Uj * Uj * Uj)) * dUj -
+             0.25 * ((Si * Si * oi * oi) / (dist * Lj * Lj * Lj)) * dLj + dCj;
+      dRj = pm_power(bj, 2) * oj * (1 - th_j * th_j) * tdj * (1 / rj) * dBTj;
+      force = 0;
+      force += c1 * (ci * (1 / pm_power(bi, 7)) * dRi * (1 / dist) +
+                     cj * (1 / pm_power(bj, 7)) * dRj * (1 / dist));
+      for (t = 0; t < 3; t++) {
+        forces[3 * i + t] -= d[t] * force;
+        forces[3 * j + t] += d[t] * force;
+      }
+    }
+  for (i = 0; i < n; i++) en += ace[i];
+  *energy = en;
+  free(burial); free(psi); free(born); free(ace); free(acecount);
+  return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* ---------------------------------------------------------- torsions */
 static void cross_to(const double *u, const double *v, double *o) {
@@ -1248,6 +1375,91 @@ int orc_torsion_force(const orc_system *s, int nt, const int *atoms,
     for (int i = 0; i < 3; i++)
       for (int j = i; j < 3; j++) {
         const double w = f1[i] * r12[j] + f2[i] * r23[j] + f3[i] * r34[j];
+        v[3 * i + j] += w;
+        if (j != i) v[3 * j + i] += w;
+      }
+  }
+  *energy = e;
+  if (virial)
+    for (c = 0; c < 9; c++) virial[c] = v[c];
+  return 0;
+}
+
+/* ------------------------------------------------------- bonds, angles */
+/* BondSystemForce::calcBond (force/bonded/BondSystemForce.h:89-124):
+ * harmonic k (r - r0)^2 along the minimal difference r12 = x1 - x2 seen
+ * from atom 2; the force on atom 1 is r12 (-dV/dr / r), atom 2 gets its
+ * negative, the virial is addVirial(f1, r12). */
+int orc_bond_force(const orc_system *s, int nb, const int *atoms, const double *params,
+                   double *forces, double *energy, double *virial) {
+  pbc_t p;
+  int b, c;
+  double e = 0.0, v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  pbc_set(s, &p);
+  for (b = 0; b < nb; b++) {
+    const int a1 = atoms[2 * b], a2 = atoms[2 * b + 1];
+    const double k = params[2 * b], r0 = params[2 * b + 1];
+    double r12[3], r2, f1[3];
+    pbc_mindiff(&p, s->pos + 3 * a2, s->pos + 3 * a1, r12, &r2);
+    const double r = sqrt(norm2(r12));
+    const double dpdr = 2.0 * k * (r - r0);
+    for (c = 0; c < 3; c++) {
+      f1[c] = r12[c] * (-dpdr / r);
+      forces[3 * a1 + c] += f1[c];
+      forces[3 * a2 + c] -= f1[c];
+    }
+    e += k * (r - r0) * (r - r0);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) v[3 * i + j] += f1[i] * r12[j];
+  }
+  *energy = e;
+  if (virial)
+    for (c = 0; c < 9; c++) virial[c] = v[c];
+  return 0;
+}
+
+/* AngleSystemForce::calcAngle (force/bonded/AngleSystemForce.h:86-171):
+ * harmonic in theta = atan2(|r12 x r32|, r12 . r32) plus the Urey-Bradley
+ * spring between atoms 1 and 3; d theta / d x1 = (u12 cos - u32) /
+ * (sin d12) and likewise for atom 3, atom 2 takes minus their sum.
+ * params: k_theta, theta0, k_ub, r_ub. */
+int orc_angle_force(const orc_system *s, int na, const int *atoms, const double *params,
+                    double *forces, double *energy, double *virial) {
+  pbc_t p;
+  int t, c;
+  double e = 0.0, v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  pbc_set(s, &p);
+  for (t = 0; t < na; t++) {
+    const int a1 = atoms[3 * t], a2 = atoms[3 * t + 1], a3 = atoms[3 * t + 2];
+    const double kt = params[4 * t], t0 = params[4 * t + 1], kub = params[4 * t + 2],
+                 rub = params[4 * t + 3];
+    double r12[3], r32[3], r13[3], r2, cr[3], f1[3], f3[3];
+    pbc_mindiff(&p, s->pos + 3 * a2, s->pos + 3 * a1, r12, &r2);
+    pbc_mindiff(&p, s->pos + 3 * a2, s->pos + 3 * a3, r32, &r2);
+    pbc_mindiff(&p, s->pos + 3 * a3, s->pos + 3 * a1, r13, &r2);
+    const double d12 = sqrt(norm2(r12)), d32 = sqrt(norm2(r32)), d13 = sqrt(norm2(r13));
+    cross3(r12, r32, cr);
+    const double theta = atan2(sqrt(norm2(cr)), dot3(r12, r32));
+    const double st = sin(theta), ct = cos(theta);
+    const double dpdt = 2.0 * kt * (theta - t0);
+    const double ub = 2.0 * kub * (d13 - rub);
+    for (c = 0; c < 3; c++) {
+      const double u12 = r12[c] / d12, u32 = r32[c] / d32, u13 = r13[c] / d13;
+      const double dt1 = (u12 * ct - u32) / (st * d12);
+      const double dt3 = (u32 * ct - u12) / (st * d32);
+      const double ub1 = u13 * ub;
+      f1[c] = -dt1 * dpdt - ub1;
+      f3[c] = -dt3 * dpdt - (-ub1);
+    }
+    for (c = 0; c < 3; c++) {
+      forces[3 * a1 + c] += f1[c];
+      forces[3 * a2 + c] += -f1[c] - f3[c];
+      forces[3 * a3 + c] += f3[c];
+    }
+    e += kt * (theta - t0) * (theta - t0) + kub * (d13 - rub) * (d13 - rub);
+    for (int i = 0; i < 3; i++)
+      for (int j = i; j < 3; j++) {
+        const double w = f1[i] * r12[j] + f3[i] * r32[j];
         v[3 * i + j] += w;
         if (j != i) v[3 * j + i] += w;
       }

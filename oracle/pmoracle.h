@@ -116,6 +116,10 @@ typedef struct {
   double alpha_obc, beta_obc, gamma_obc;
   double solute_dielec, solvent_dielec;
 } orc_gb;
+/* GBACEForce (ACE nonpolar term on the GBBornRadii radii): forces ADDED,
+ * energy set. */
+int orc_gbace_force(const orc_system *s, const orc_gb *g, double sigma, double rho_s,
+                    double *forces, double *energy);
 int orc_gb_force(const orc_system *s, const orc_gb *g, double *born,
                  double *forces, double *energy);
 
@@ -129,6 +133,12 @@ int orc_gb_force(const orc_system *s, const orc_gb *g, double *born,
  * term (k, periodicity n, phase delta [rad]); n > 0 is the cosine form
  * k (1 + cos(n phi + delta)), n == 0 the harmonic k (phi - delta)^2.
  * Forces are added; energy and virial (may be NULL) are set. */
+/* Harmonic bonds (2 atoms; k, r0) and angles with Urey-Bradley (3 atoms;
+ * k_theta, theta0 [rad], k_ub, r_ub): forces ADDED, energy and virial set. */
+int orc_bond_force(const orc_system *s, int nb, const int *atoms, const double *params,
+                   double *forces, double *energy, double *virial);
+int orc_angle_force(const orc_system *s, int na, const int *atoms, const double *params,
+                    double *forces, double *energy, double *virial);
 int orc_torsion_force(const orc_system *s, int nt, const int *atoms,
                       const double *params, double *forces, double *energy,
                       double *virial);

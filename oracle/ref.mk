@@ -3,7 +3,7 @@
 # undefined, which ProtoMolApp.cpp supports).  Test infrastructure only:
 # every output goes to oracle/_ref/, which git ignores.
 #
-#   make -f oracle/ref.mk -j8 REF=/root/reference
+#   make -f oracle/ref.mk -j8 REF=<ProtoMol checkout>
 #
 # Outputs
 #   oracle/_ref/libProtoMol.a      every library TU except base/Lapack.cpp
@@ -16,12 +16,13 @@
 #                                  library: evaluates named forces on a
 #                                  given configuration and dumps FP64
 #                                  forces / energies / virial
-#   oracle/_ref/protomol_gpu       the stock executable plus the GPU force
-#                                  module (protomol_b200/protomol_module),
-#                                  linked to protomol_b200/libpmgpu.so: the
-#                                  drop-in as a ProtoMol maintainer builds it
+#
+# The drop-in itself (the stock driver plus the GPU module) is built by
+# protomol_b200/protomol_module/Makefile against this library build.
 
-REF     ?= /root/reference
+ifndef REF
+$(error REF must name the ProtoMol source checkout)
+endif
 OUT     ?= oracle/_ref
 CXX     ?= g++
 CXXFLAGS_REF ?= -std=c++98 -O2 -w -fno-strict-aliasing
@@ -33,7 +34,7 @@ SRCS := $(shell cd $(REF) && find protomol -name '*.cpp' \
 OBJS := $(patsubst %.cpp,$(OUT)/obj/%.o,$(SRCS))
 EXACT_OBJ := $(OUT)/obj_exact/NonbondedFullElectrostaticForceModule.o
 
-all: $(OUT)/protomol $(OUT)/protomol_exacterf $(OUT)/pm_forcedump $(OUT)/protomol_gpu
+all: $(OUT)/protomol $(OUT)/protomol_exacterf $(OUT)/pm_forcedump
 
 $(OUT)/obj/%.o: $(REF)/%.cpp
 	@mkdir -p $(dir $@)
@@ -76,14 +77,3 @@ $(OUT)/pm_forcedump: $(OUT)/obj/app/ref_forcedump.o $(OUT)/obj/app/modules.o $(O
 	$(CXX) -o $@ $^
 
 .PHONY: all
-
-MOD := protomol_b200/protomol_module
-$(OUT)/obj/gpu/%.o: $(MOD)/%.cpp $(MOD)/PmgpuForceModule.h include/pmgpu.h
-	@mkdir -p $(dir $@)
-	$(CXX) $(CXXFLAGS_REF) $(INC) -Iinclude -c $< -o $@
-
-$(OUT)/protomol_gpu: $(OUT)/obj/gpu/main_gpu.o $(OUT)/obj/gpu/PmgpuForceModule.o \
-                     $(OUT)/obj/app/modules.o $(OUT)/libProtoMol.a protomol_b200/libpmgpu.so
-	$(CXX) -o $@ $(OUT)/obj/gpu/main_gpu.o $(OUT)/obj/gpu/PmgpuForceModule.o \
-	  $(OUT)/obj/app/modules.o $(OUT)/libProtoMol.a -Lprotomol_b200 -lpmgpu \
-	  -Wl,-rpath,'$$ORIGIN/../../protomol_b200'

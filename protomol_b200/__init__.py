@@ -8,7 +8,7 @@ system generators used by the benchmark.
 """
 from .engine import (  # noqa: F401
     ANGLE, BOND, COULOMB, LENNARDJONES, VIRIALXX, BondedSystemForce, Context, ForceFactory,
-    GBForce, GpuSystem, LangevinLeapfrogIntegrator, LeapfrogIntegrator,
+    GBACEForce, GBForce, GpuSystem, LangevinLeapfrogIntegrator, LeapfrogIntegrator,
     NonbondedCutoffSystemForce, NonbondedSimpleFullSystemForce, PMEwaldSystemForce,
     ScalarStructure, SystemForce, TorsionSystemForce)
 from ._lib import PmgpuError, load  # noqa: F401

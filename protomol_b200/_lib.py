@@ -39,7 +39,7 @@ EXPORTED = [
     "pmgpu_debug_pair_set", "pmgpu_profile_enable", "pmgpu_profile_read",
     "pmgpu_kernel_count", "pmgpu_gb_forces_noalloc", "pmgpu_run_async", "pmgpu_run_query",
     "pmgpu_run_wait", "pmgpu_mem_info", "pmgpu_footprint_estimate", "pmgpu_force_torsion_add",
-    "pmgpu_fp32_peak",
+    "pmgpu_fp32_peak", "pmgpu_force_gbace_add",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -79,7 +79,7 @@ class Integrator(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("pairs_in_cutoff", C.c_longlong), ("list_entries", C.c_longlong),
                 ("clusters", C.c_longlong), ("list_builds", C.c_longlong),
-                ("cells", C.c_int * 3)]
+                ("cells", C.c_int * 3), ("pair_kernel", C.c_int)]
 
 
 _lib = None
@@ -114,6 +114,7 @@ def load() -> C.CDLL:
     lib.pmgpu_force_simplefull_add.argtypes = [vp, i32, i32, C.POINTER(i32)]
     lib.pmgpu_force_pme_add.argtypes = [vp, dbl, dbl, i32, vp, i32, i32, dbl, C.POINTER(i32)]
     lib.pmgpu_force_gb_add.argtypes = [vp, dbl, dbl, C.POINTER(i32)]
+    lib.pmgpu_force_gbace_add.argtypes = [vp, dbl, dbl, C.POINTER(i32)]
     lib.pmgpu_force_bonded_add.argtypes = [vp, i32, i32, C.POINTER(i32)]
     lib.pmgpu_force_torsion_add.argtypes = [vp, i32, i32, C.POINTER(i32)]
     lib.pmgpu_force_set_enabled.argtypes = [vp, i32, i32]

@@ -224,7 +224,7 @@ static int system_free(System *s) {
                   s->d_dihedral_atoms, s->d_dihedral_params, s->d_improper_atoms,
                   s->d_improper_params,
                   s->d_gb_vdwr, s->d_gb_scale, s->d_gb_offset, s->d_water, s->d_gb_born,
-                  s->d_gb_psi, s->d_gb_partial, s->d_gb_fixed, s->d_pos, s->d_vel,
+                  s->d_gb_psi, s->d_gb_partial, s->d_gb_fixed, s->d_gb_ace, s->d_pos, s->d_vel,
                   s->d_force, s->d_acc, s->d_status, s->d_pairbuf, s->d_paircount,
                   s->d_stage, s->d_snap, s->d_step, s->d_sf_tile, s->d_gb_gst, s->d_gb_grad,
                   s->d_rec,
@@ -328,8 +328,9 @@ static int add_pair_terms(std::vector<Launch> &groups, int list, const PairTerms
 
 // Evaluates the enabled forces (or only force `only`) at the resident
 // positions, accumulating into the (already zeroed) force planes and
-// energy accumulators.
-static int evaluate_forces(System *s, int only, int mode) {
+// energy accumulators.  fold = 0 (the force-only steps of an MD run) lets
+// the pair forces stay in the list's slot buffer for the next update kernel.
+static int evaluate_forces(System *s, int only, int mode, int fold = 1) {
   const int want_virial = mode == PAIR_VIRIAL;
   // energy mode of the non-pair terms: 0 forces only (inner MD steps),
   // 1 + energies, 2 + energies and virial
@@ -373,7 +374,7 @@ static int evaluate_forces(System *s, int only, int mode) {
   bool need_rec = false;
   for (auto &f : s->forces) {
     if (only >= 0 ? f.id != only : !f.enabled) continue;
-    need_rec |= f.kind == FK_SIMPLEFULL || f.kind == FK_GB;
+    need_rec |= f.kind == FK_SIMPLEFULL || f.kind == FK_GB || f.kind == FK_GBACE;
   }
   if (need_rec && s->precision == PMGPU_PREC_MIXED && !s->rec_fresh) {
     PM_CHECK(nb_stage_pairs(s));
@@ -414,7 +415,7 @@ static int evaluate_forces(System *s, int only, int mode) {
       if (only >= 0 ? f.id != only : !f.enabled) continue;
       if (fork)
         s->stream = f.kind == FK_SIMPLEFULL ? main_stream
-                    : f.kind == FK_GB || f.kind == FK_PME ? s->side
+                    : f.kind == FK_GB || f.kind == FK_GBACE || f.kind == FK_PME ? s->side
                                                            : short_stream;
       int r = PMGPU_OK;
       switch (f.kind) {
@@ -437,11 +438,22 @@ static int evaluate_forces(System *s, int only, int mode) {
           }
           break;
         case FK_GB:
+        case FK_GBACE: {
+          // GBForce and GBACEForce of one evaluation share one chain of
+          // passes (the Born radii once), launched at the first of them
+          const Force *gb = nullptr, *ace = nullptr;
+          for (auto &g : s->forces) {
+            if (only >= 0 ? g.id != only : !g.enabled) continue;
+            if (g.kind == FK_GB && !gb) gb = &g;
+            if (g.kind == FK_GBACE && !ace) ace = &g;
+          }
+          if (&f != (gb ? gb : ace)) break;
           prof_begin(s, PMGPU_PHASE_GB);
-          r = gb_forces(s, &f);
+          r = gb_forces(s, gb, ace);
           prof_end(s);
-          s->kernels += s->precision == PMGPU_PREC_MIXED ? 4 : 5;
+          s->kernels += (s->precision == PMGPU_PREC_MIXED ? 3 : 4) + (gb ? 1 : 0);
           break;
+        }
         case FK_BONDED:
         case FK_TORSION: {
           // the bonded terms of every selected force share one launch
@@ -495,7 +507,7 @@ static int evaluate_forces(System *s, int only, int mode) {
   }
   for (auto &g : groups) {
     prof_begin(s, PMGPU_PHASE_PAIRS);
-    int r = nb_pair_forces(s, &s->lists[g.list], g.terms, mode);
+    int r = nb_pair_forces(s, &s->lists[g.list], g.terms, mode, fold);
     prof_end(s);
     PM_CHECK(r);
     s->kernels += 2;  // tiles, slot forces
@@ -519,7 +531,10 @@ static void constant_terms(System *s, int only, double *energies, double *virial
   }
 }
 
-static int read_results(System *s, int only, double *energies, double *virial, int add) {
+// energies_valid = 0: a force-only evaluation, whose energies and virial
+// were not computed (recorded as zeros).
+static int read_results(System *s, int only, double *energies, double *virial, int add,
+                        int energies_valid = 1) {
   PM_CUDA(cudaMemcpyAsync(s->h_acc, s->d_acc, sizeof(long long) * ACC_COUNT,
                           cudaMemcpyDeviceToHost, s->stream));
   PM_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost,
@@ -548,7 +563,11 @@ static int read_results(System *s, int only, double *energies, double *virial, i
   double e[PMGPU_E_COUNT], v[9];
   for (int k = 0; k < PMGPU_E_COUNT; k++) e[k] = (double)s->h_acc[k] / kEnergyScale;
   for (int k = 0; k < 9; k++) v[k] = (double)s->h_acc[ACC_VIRIAL + k] / kEnergyScale;
-  constant_terms(s, only, e, v);
+  if (energies_valid) constant_terms(s, only, e, v);
+  else
+    for (int k = 0; k < PMGPU_E_COUNT; k++) e[k] = 0.0;
+  if (!energies_valid)
+    for (int k = 0; k < 9; k++) v[k] = 0.0;
   s->last_pairs = s->h_acc[ACC_PAIRS];
   for (int k = 0; k < PMGPU_E_COUNT; k++) s->last_energy[k] = e[k];
   for (int k = 0; k < 9; k++) s->last_virial[k] = v[k];
@@ -1079,6 +1098,23 @@ int pmgpu_force_gb_add(pmgpu_system *h, double solute, double solvent, int *forc
   return add_force(s, f, force_id);
 }
 
+int pmgpu_force_gbace_add(pmgpu_system *h, double solvation_param,
+                          double water_sphere_radius, int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CHECK(run_finish(s));
+  PM_CUDA(cudaSetDevice(s->device));
+  if (s->box.periodic) return fail(PMGPU_ERR_UNSUPPORTED, "GBACE is the vacuum all-pairs path");
+  if (!std::isfinite(solvation_param) || !std::isfinite(water_sphere_radius))
+    return fail(PMGPU_ERR_ARG, "GBACE parameters must be finite");
+  PM_CHECK(gb_init(s));
+  Force f;
+  f.kind = FK_GBACE;
+  f.ace_sigma = solvation_param;
+  f.ace_rho = water_sphere_radius;
+  return add_force(s, f, force_id);
+}
+
 int pmgpu_force_bonded_add(pmgpu_system *h, int bonds, int angles, int *force_id) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   Force f;
@@ -1113,11 +1149,14 @@ int pmgpu_evaluate(pmgpu_system *h, double *energies, double *virial) {
   System *s = sysp(h);
   PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
+  // no energies and no virial wanted: the force-only kernels of the inner
+  // MD steps (the pair kernel's specialised form), forces only
+  const int mode = virial ? PAIR_VIRIAL : (energies ? PAIR_ENERGY : PAIR_FORCE);
   int r = with_overflow_retry([&]() {
     PM_CHECK(zero_forces(s));
     PM_CHECK(begin_eval(s));
-    PM_CHECK(evaluate_forces(s, -1, virial ? PAIR_VIRIAL : PAIR_ENERGY));
-    return read_results(s, -1, energies, virial, 0);
+    PM_CHECK(evaluate_forces(s, -1, mode));
+    return read_results(s, -1, energies, virial, 0, mode != PAIR_FORCE);
   });
   s->forces_valid = (r == PMGPU_OK);
   return r;
@@ -1132,11 +1171,12 @@ int pmgpu_force_evaluate(pmgpu_system *h, int id, const double *pos, double *for
   if (id < 0 || id >= (int)s->forces.size()) return fail(PMGPU_ERR_ARG, "no such force");
   if (pos) PM_CHECK(copy_in(s, s->d_pos, pos));
   s->forces_valid = 0;
+  const int mode = virial ? PAIR_VIRIAL : (energies ? PAIR_ENERGY : PAIR_FORCE);
   PM_CHECK(with_overflow_retry([&]() {
     PM_CHECK(zero_forces(s));
     PM_CHECK(begin_eval(s));
-    PM_CHECK(evaluate_forces(s, id, virial ? PAIR_VIRIAL : PAIR_ENERGY));
-    return read_results(s, id, energies, virial, 1);
+    PM_CHECK(evaluate_forces(s, id, mode));
+    return read_results(s, id, energies, virial, 1, mode != PAIR_FORCE);
   }));
   if (forces) PM_CHECK(forces_to_host(s, forces, 1));
   return PMGPU_OK;
@@ -1155,7 +1195,7 @@ static int one_step(System *s, const pmgpu_integrator *it, int phase, int mode) 
   // the update (which also advances the step counter of the Langevin noise)
   s->kernels += s->n > 0;
   if (s->n == 0) PM_CHECK(begin_eval(s));
-  return evaluate_forces(s, -1, mode);
+  return evaluate_forces(s, -1, mode, mode != PAIR_FORCE);
 }
 
 static bool same_integrator(const pmgpu_integrator &a, const pmgpu_integrator &b) {
@@ -1240,6 +1280,8 @@ static int run_snapshot(System *s, int restore) {
   long long *snap_f = reinterpret_cast<long long *>(snap_vel + n3);
   const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
   if (!restore) {
+    // the snapshot holds complete forces (no pair forces left in a slot buffer)
+    PM_CHECK(fold_pending_slots(s));
     PM_CUDA(cudaMemcpyAsync(snap_pos, s->d_pos, n3 * sizeof(double), k, s->stream));
     PM_CUDA(cudaMemcpyAsync(snap_vel, s->d_vel, n3 * sizeof(double), k, s->stream));
     PM_CUDA(cudaMemcpyAsync(snap_f, s->d_force, n3 * sizeof(long long), k, s->stream));
@@ -1257,7 +1299,7 @@ static int run_enqueue(System *s, const pmgpu_integrator *it, long n_steps) {
   if (!s->forces_valid) {
     PM_CHECK(zero_forces(s));
     PM_CHECK(begin_eval(s));
-    PM_CHECK(evaluate_forces(s, -1, PAIR_FORCE));
+    PM_CHECK(evaluate_forces(s, -1, PAIR_FORCE, 0));
   }
   for (long k = 0; k < n_steps;) {
     // Inner steps (not the first, not the last) replay a captured graph
@@ -1464,6 +1506,7 @@ int pmgpu_force_stats(pmgpu_system *h, int id, pmgpu_stats *out) {
     out->cells[1] = nl.ncy;
     out->cells[2] = nl.nzb;
     out->clusters = nl.nclusters;
+    out->pair_kernel = nl.last_form;
     int rb[2] = {0, 0};
     PM_CUDA(cudaMemcpyAsync(rb, nl.d_rebuild, sizeof(rb), cudaMemcpyDeviceToHost, s->stream));
     PM_CUDA(cudaStreamSynchronize(s->stream));
@@ -1512,7 +1555,7 @@ int pmgpu_debug_pair_set(pmgpu_system *h, int id, int *pairs, long long cap,
   PM_CHECK(begin_eval(s));
   PM_CHECK(nb_prepare(s, &s->lists[f.list_index], 0));
   PM_CHECK(nb_build(s, &s->lists[f.list_index]));
-  PM_CHECK(nb_pair_forces(s, &s->lists[f.list_index], f.terms, PAIR_RECORD));
+  PM_CHECK(nb_pair_forces(s, &s->lists[f.list_index], f.terms, PAIR_RECORD, 1));
   long long total = 0;
   PM_CUDA(cudaMemcpyAsync(&total, s->d_paircount, sizeof(long long), cudaMemcpyDeviceToHost,
                           s->stream));

@@ -298,6 +298,9 @@ int bonded_all(System *s, int bonds, int angles, int dihedrals, int impropers, i
 }
 
 int zero_forces(System *s) {
+  // a slot buffer still pending holds stale pair forces: fold (and clear) it
+  // before the forces are zeroed, so the next pair launch starts from zero
+  PM_CHECK(fold_pending_slots(s));
   PM_CUDA(cudaMemsetAsync(s->d_force, 0, sizeof(long long) * 3 * (size_t)s->n, s->stream));
   return PMGPU_OK;
 }
@@ -535,6 +538,7 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int z
     a.fslot = list->d_fslot;
     a.slot_of = list->d_slot_of;
     a.ns = list->ns_max;
+    list->slot_pending = 0;  // this launch adds the slot buffer and clears it
   }
   if (list && list->built && a.drift && s->n) {
     const float hs = (float)(0.5 * list->skin);
@@ -561,6 +565,8 @@ __global__ void k_forces_to_aos(int n, const long long *__restrict__ force,
 int forces_to_host(System *s, double *out, int add) {
   int n = s->n;
   if (n == 0) return PMGPU_OK;
+  // pair forces a force-only step left in a slot buffer belong to d_force
+  PM_CHECK(fold_pending_slots(s));
   double *d_tmp = nullptr;
   PM_CUDA(cudaMallocAsync(&d_tmp, sizeof(double) * 3 * n, s->stream));
   k_forces_to_aos<<<(n + 255) / 256, 256, 0, s->stream>>>(n, s->d_force, d_tmp);

@@ -45,7 +45,15 @@ struct GbArgs {
   // dR/d(burial sum), q^2 / (2 born^2)) from k_gb_radii
   const float4 *rec, *gst;
   float4 *grad;
+  // GBACEForce (null: off): per atom the factor A_i = c1 c_i R_i^-7 dR_i/dI
+  // of the ACE pair force, and its energy parameters
+  double *ace;
+  double ace_sigma, ace_rho;
+  int partial_pass;  // GBForce on: the partial sums are formed
 };
+
+// GBACEForce's pi (GBACEForce.cpp:6): the reference's constant, not M_PI.
+constexpr double kAcePi = 3.14169;
 
 template <typename Real>
 __device__ __forceinline__ Real gb_burial_term(Real dist, Real oi, Real oj, Real Sj) {
@@ -128,11 +136,20 @@ __global__ void k_gb_radii(GbArgs a) {
     const double dfac = born * born * oi * (1.0 - th * th) * td * iri;
     a.psi[i] = dfac;
     a.born[i] = born;
+    if (a.ace) {
+      // GBACEForce: c1 c_i R^-7 dR/dI (the pair force's per-atom factor,
+      // GBACEForce.cpp:164-205) and the atom's ACE energy
+      // 4 pi sigma (r + rho_s)^2 (r / R)^6 (:51-62)
+      const double rr = (ri + a.ace_rho) * (ri + a.ace_rho);
+      const double x = ri * inv, x2 = x * x, x6 = x2 * x2 * x2;
+      a.ace[i] = 24.0 * kAcePi * a.ace_sigma * rr * x6 * inv * dfac;
+      if (a.n > 1) self += 4.0 * kAcePi * a.ace_sigma * rr * x6;
+    }
     if (a.grad)
       a.grad[i] = make_float4((float)born, (float)inv, (float)dfac, (float)(0.5 * q * q * inv * inv));
     a.burial_fx[i] = 0;
     a.partial_fx[i] = 0;
-    if (a.n > 1) self = -0.5 * (q * q) * inv * a.dielec;
+    if (a.n > 1) self += -0.5 * (q * q) * inv * a.dielec;
   }
   self = warp_sum(self);
   if ((threadIdx.x & 31) == 0) red_add(&a.acc[ACC_COULOMB], to_fixed(self, kEnergyScale));
@@ -213,7 +230,7 @@ __device__ __forceinline__ Real gb_dBT(Real dist, Real oi, Real oj, Real Sj) {
 template <typename Real>
 __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
   __shared__ double sx[kGbTile], sy[kGbTile], sz[kGbTile], sb[kGbTile], sq[kGbTile];
-  __shared__ double so[kGbTile], ss[kGbTile], sp[kGbTile], spart[kGbTile];
+  __shared__ double so[kGbTile], ss[kGbTile], sp[kGbTile], spart[kGbTile], sa[kGbTile];
   int i = blockIdx.x * kGbTile + threadIdx.x;
   bool valid = i < a.n;
   int ii = valid ? i : 0;
@@ -222,6 +239,8 @@ __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
   Real oi = (Real)(a.vdwr[ii] - a.offset[ii]);
   Real Si = (Real)a.scale[ii], dfac_i = (Real)a.psi[ii];
   Real part_i = (Real)a.partial[ii];
+  const Real ace_i = a.ace ? (Real)a.ace[ii] : Real(0);
+  const Real d = (Real)a.dielec;
   Real fx = 0, fy = 0, fz = 0;
   double epair = 0.0;
   int j0 = blockIdx.y * jchunk, j1 = min(a.n, j0 + jchunk);
@@ -234,6 +253,7 @@ __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
       so[threadIdx.x] = a.vdwr[j] - a.offset[j];
       ss[threadIdx.x] = a.scale[j]; sp[threadIdx.x] = a.psi[j];
       spart[threadIdx.x] = a.partial[j];
+      sa[threadIdx.x] = a.ace ? a.ace[j] : 0.0;
     }
     __syncthreads();
     int lim = min(kGbTile, j1 - base);
@@ -250,8 +270,10 @@ __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
         Real ex = exp(-r2 / (Real(4) * bi * bj));
         Real fGB = pm_sqrt(r2 + bi * bj * ex);
         ep += -(qi * qj) / fGB;
-        Real dRi = dfac_i * gb_dBT<Real>(dist, oi, oj, Sj);
-        Real dRj = (Real)sp[k] * gb_dBT<Real>(dist, oj, oi, Si);
+        const Real bti = gb_dBT<Real>(dist, oi, oj, Sj);
+        const Real btj = gb_dBT<Real>(dist, oj, oi, Si);
+        Real dRi = dfac_i * bti;
+        Real dRj = (Real)sp[k] * btj;
         Real pref = qi * qj * (Real(1) / (fGB * fGB)) * Real(0.5) * (Real(1) / fGB);
         // partialTerm[i][j] and [j][i] (GBPartialSum.cpp:33-41)
         Real ptij = pref * ex * (bj + r2 / (Real(4) * bi));
@@ -263,19 +285,20 @@ __global__ void __launch_bounds__(kGbTile) k_gb_force(GbArgs a, int jchunk) {
         f -= Real(0.5) * qj * qj * dRj / (bj * bj) * idist;
         f -= (part_i - ptij) * (dRi * idist);
         f -= ((Real)spart[k] - ptji) * (dRj * idist);
+        // GBForce scaled by the dielectric factor, plus GBACEForce
+        f = f * d + (ace_i * bti + (Real)sa[k] * btj) * idist;
         fx -= dx * f; fy -= dy * f; fz -= dz * f;
       }
       epair += (double)ep;
     }
     __syncthreads();
   }
-  double d = a.dielec;
   if (valid) {
-    red_add(&a.force[i], to_fixed((double)fx * d, kForceScale));
-    red_add(&a.force[a.n + i], to_fixed((double)fy * d, kForceScale));
-    red_add(&a.force[2 * a.n + i], to_fixed((double)fz * d, kForceScale));
+    red_add(&a.force[i], to_fixed((double)fx, kForceScale));
+    red_add(&a.force[a.n + i], to_fixed((double)fy, kForceScale));
+    red_add(&a.force[2 * a.n + i], to_fixed((double)fz, kForceScale));
   }
-  epair = warp_sum(epair) * 0.5 * d;
+  epair = warp_sum(epair) * 0.5 * a.dielec;
   if ((threadIdx.x & 31) == 0) red_add(&a.acc[ACC_COULOMB], to_fixed(epair, kEnergyScale));
 }
 
@@ -540,14 +563,19 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
     const bool vi = i < a.n;
     const int ii = vi ? i : 0;
     const float4 hi = a.rec[ii], li = a.rec[a.n + ii], gi = a.gst[ii], ri = a.grad[ii];
-    const float Di =
-        (float)(((double)ri.w + (double)a.partial_fx[ii] * (1.0 / kGbScale)) * (double)ri.z);
+    // D_i scaled by the dielectric factor, less the ACE factor A_i
+    const float Di = (float)(d * ((double)ri.w + (double)a.partial_fx[ii] * (1.0 / kGbScale)) *
+                                 (double)ri.z -
+                             (a.ace ? a.ace[ii] : 0.0));
     const float q4bi = 0.25f * ri.y;
+    const float qd = (float)d;
     {
       const int j = J * 32 + lane;
       const int jj = j < a.n ? j : 0;
       const float4 l = a.rec[a.n + jj], g = a.gst[jj], r = a.grad[jj];
-      const double Dj = ((double)r.w + (double)a.partial_fx[jj] * (1.0 / kGbScale)) * (double)r.z;
+      const double Dj =
+          d * ((double)r.w + (double)a.partial_fx[jj] * (1.0 / kGbScale)) * (double)r.z -
+          (a.ace ? a.ace[jj] : 0.0);
       sh[wb][lane] = a.rec[jj];
       sl[wb][lane] = make_float4(l.x, l.y, l.z, r.x);
       sr[wb][lane] = make_float4(r.y, (float)Dj, g.x, g.y);
@@ -572,7 +600,7 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
         const float ex = __expf(-r2 * (q4bi * rj.x));
         const float ifgb = rsqrt_nr(r2 + ri.x * l.w * ex);
         const float qq = hi.w * h.w;
-        const float pref = 0.5f * qq * (ifgb * ifgb * ifgb);
+        const float pref = 0.5f * (qq * qd) * (ifgb * ifgb * ifgb);
         const float bti = gb_dBT_f32(dist, idist, gi.x, rj.w);
         const float btj = gb_dBT_f32(dist, idist, rj.z, gi.y);
         float f = -pref * (2.0f - 0.5f * ex) - idist * (Di * bti + rj.y * btj);
@@ -585,15 +613,15 @@ k_gb_force_half(GbArgs a, int tiles, long long items) {
                   sz = warp_tsum8(gz, lane);
       const int jt = J * 32 + gq * 8 + (lane >> 2);
       if ((lane & 3) == 0 && jt < a.n) {
-        red_add(&a.force[jt], to_fixed((double)sx * d, kForceScale));
-        red_add(&a.force[a.n + jt], to_fixed((double)sy * d, kForceScale));
-        red_add(&a.force[2 * a.n + jt], to_fixed((double)sz * d, kForceScale));
+        red_add(&a.force[jt], to_fixed((double)sx, kForceScale));
+        red_add(&a.force[a.n + jt], to_fixed((double)sy, kForceScale));
+        red_add(&a.force[2 * a.n + jt], to_fixed((double)sz, kForceScale));
       }
     }
     if (vi) {
-      red_add(&a.force[i], to_fixed((double)fx * d, kForceScale));
-      red_add(&a.force[a.n + i], to_fixed((double)fy * d, kForceScale));
-      red_add(&a.force[2 * a.n + i], to_fixed((double)fz * d, kForceScale));
+      red_add(&a.force[i], to_fixed((double)fx, kForceScale));
+      red_add(&a.force[a.n + i], to_fixed((double)fy, kForceScale));
+      red_add(&a.force[2 * a.n + i], to_fixed((double)fz, kForceScale));
     }
     epair += (double)ep;
     __syncwarp();
@@ -627,7 +655,7 @@ static void gb_passes_f32(const GbArgs &a, cudaStream_t st) {
   k_gb_burial_half<32><<<blocks2, 32 * 32, 0, st>>>(a, tiles, items2);
   // one-warp blocks: they fit beside a resident simple-full block
   k_gb_radii<<<(a.n + 31) / 32, 32, 0, st>>>(a);
-  k_gb_partial_half<16><<<blocks, 16 * 32, 0, st>>>(a, tiles, items);
+  if (a.partial_pass) k_gb_partial_half<16><<<blocks, 16 * 32, 0, st>>>(a, tiles, items);
   k_gb_force_half<16><<<blocks2, 16 * 32, 0, st>>>(a, tiles, items2);
 }
 
@@ -639,6 +667,7 @@ int gb_init(System *s) {
     PM_CHECK(dev_alloc(s, &s->d_gb_psi, sizeof(double) * n));
     PM_CHECK(dev_alloc(s, &s->d_gb_partial, sizeof(double) * n));
     PM_CHECK(dev_alloc(s, &s->d_gb_fixed, sizeof(long long) * 2 * n));
+    PM_CHECK(dev_alloc(s, &s->d_gb_ace, sizeof(double) * n));
     PM_CUDA(cudaMemsetAsync(s->d_gb_fixed, 0, sizeof(long long) * 2 * n, s->stream));
   }
   if (s->precision == PMGPU_PREC_MIXED && !s->d_gb_gst) {
@@ -653,9 +682,12 @@ int gb_init(System *s) {
   return PMGPU_OK;
 }
 
-int gb_forces(System *s, Force *f) {
+// gb: the GBForce term (null: none), ace: the GBACEForce term (null: none);
+// with both, one chain of passes serves both (the Born radii once, the ACE
+// pair force folded into the GB force pass).
+int gb_forces(System *s, const Force *gb, const Force *ace) {
   int n = s->n;
-  if (n == 0) return PMGPU_OK;
+  if (n == 0 || (!gb && !ace)) return PMGPU_OK;
   GbArgs a;
   a.n = n;
   a.pos = s->d_pos;
@@ -667,7 +699,11 @@ int gb_forces(System *s, Force *f) {
   a.alpha = s->gb_obc[0];
   a.beta = s->gb_obc[1];
   a.gamma = s->gb_obc[2];
-  a.dielec = (1 / f->solute) - (1 / f->solvent);
+  a.dielec = gb ? (1 / gb->solute) - (1 / gb->solvent) : 0.0;
+  a.partial_pass = gb != nullptr;
+  a.ace = ace ? s->d_gb_ace : nullptr;
+  a.ace_sigma = ace ? ace->ace_sigma : 0.0;
+  a.ace_rho = ace ? ace->ace_rho : 0.0;
   a.burial_fx = s->d_gb_fixed;
   a.partial_fx = s->d_gb_fixed + n;
   a.born = s->d_gb_born;
@@ -687,7 +723,7 @@ int gb_forces(System *s, Force *f) {
   } else {
     k_gb_burial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
     k_gb_radii<<<(n + 127) / 128, 128, 0, st>>>(a);
-    k_gb_partial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
+    if (a.partial_pass) k_gb_partial<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
     k_gb_partial_fin<<<(n + 127) / 128, 128, 0, st>>>(a);
     k_gb_force<double><<<grid, kGbTile, 0, st>>>(a, jchunk);
   }
@@ -734,7 +770,9 @@ std::mutex g_gb_scratch_mu;
 long long *g_gb_scratch_dev[kGbStaticMaxDevices] = {};
 
 // Device address of g_gb_scratch on the current device, looked up on the
-// first call made with that device current.
+// first call made with that device current and kept for the life of the
+// process (a cudaDeviceReset ends the context it belongs to; callers that
+// reset the device do not use this entry point afterwards).
 int gb_scratch_address(long long **out) {
   int dev = -1;
   PM_CUDA(cudaGetDevice(&dev));
@@ -831,6 +869,9 @@ extern "C" int pmgpu_gb_forces_noalloc(int n_atoms, const double *pos, const dou
   a.beta = obc[1];
   a.gamma = obc[2];
   a.dielec = (1 / solute_dielec) - (1 / solvent_dielec);
+  a.partial_pass = 1;
+  a.ace = nullptr;
+  a.ace_sigma = a.ace_rho = 0.0;
   a.born = reinterpret_cast<double *>(scratch);
   a.psi = reinterpret_cast<double *>(scratch + n);
   a.partial = reinterpret_cast<double *>(scratch + 2 * (size_t)n);

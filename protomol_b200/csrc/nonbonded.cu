@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 
 #include "pm_device.cuh"
 
@@ -985,41 +986,85 @@ static void launch_pairs_spec(PairArgs<Real> &a, cudaStream_t st, int mode) {
   }
 }
 
-template <typename Real, int TERMS, typename SPEC>
-static void launch_force_spec(PairArgs<Real> &a, cudaStream_t st) {
-  launch_pairs_spec<Real, TERMS, SPEC>(a, st, PAIR_FORCE);
+// Work items per i cluster of the j-lane force-only kernel: about three
+// waves of its resident warps (3 blocks of 8 warps per SM), at most 8 per
+// cluster.  Depends only on the system, so every launch of a system sums
+// its forces in the same order.
+static int jl_splits(int nclusters) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        sms <= 0)
+      sms = 148;
+  }
+  static int forced = -1;
+  if (forced < 0) {
+    const char *e = std::getenv("PMGPU_JL_SPLITS");
+    forced = e ? std::max(0, std::atoi(e)) : 0;
+  }
+  if (forced) return std::min(forced, 8);
+  const long long want = 3LL * sms * 3 * kJlWarps;
+  return (int)std::max(1LL, std::min(8LL, (want + nclusters / 2) / std::max(1, nclusters)));
 }
 
+// The specialised force-only FP32 kernels: j atoms on the lanes
+// (k_pairs_jl), the LJ table in shared memory when it is small.
+template <typename Real, int TERMS, typename SPEC>
+static void launch_force_spec(PairArgs<Real> &a, cudaStream_t st) {
+  if constexpr (sizeof(Real) == 4) {
+    a.splits = jl_splits(a.nclusters);
+    const long long items = (long long)a.nclusters * a.splits;
+    const int nb = (int)((items + kJlWarps - 1) / kJlWarps);
+    if (nb == 0) return;
+    if (a.ntypes <= kJlMaxTypes)
+      k_pairs_jl<TERMS, SPEC, true><<<nb, kJlWarps * 32, 0, st>>>(a);
+    else
+      k_pairs_jl<TERMS, SPEC, false><<<nb, kJlWarps * 32, 0, st>>>(a);
+  } else {
+    launch_pairs_spec<Real, TERMS, SPEC>(a, st, PAIR_FORCE);
+  }
+}
+
+// Returns the form launched: PMGPU_PAIRK_GENERIC or one of the specialised
+// force-only forms (PMGPU_PAIRK_*).
 template <typename Real, int TERMS>
-static void launch_pairs_t(PairArgs<Real> &a, cudaStream_t st, int mode, const PairTerms &t) {
+static int launch_pairs_t(PairArgs<Real> &a, cudaStream_t st, int mode, const PairTerms &t) {
   // specialised force-only FP32 kernels of the common configurations
   // (every term with one cutoff, box edges at least twice the cutoff)
   if (sizeof(Real) == 4 && mode == PAIR_FORCE && a.same_cut && !a.minimal_image) {
     const int lk = spec_kind(t.lj_sw), ck = spec_kind(t.coul_sw);
     if (TERMS == (TERM_LJ | TERM_EWALD) && !t.exact_erf && lk == PMGPU_SW_C2) {
       launch_force_spec<Real, TERM_LJ | TERM_EWALD, PairSpec<PMGPU_SW_C2, -1, 0>>(a, st);
-      return;
+      return PMGPU_PAIRK_LJC2_EWALD;
     }
     if (TERMS == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C2) {
       launch_force_spec<Real, TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C2, -1>>(a, st);
-      return;
+      return PMGPU_PAIRK_LJC2_COULC2;
     }
     if (TERMS == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C1) {
       launch_force_spec<Real, TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C1, -1>>(a, st);
-      return;
+      return PMGPU_PAIRK_LJC2_COULC1;
     }
   }
   launch_pairs_spec<Real, TERMS, GenericSpec>(a, st, mode);
+  return PMGPU_PAIRK_GENERIC;
 }
 
 template <typename Real>
-static int launch_pairs(PairArgs<Real> &a, cudaStream_t st, int mode, const PairTerms &t) {
+static int launch_pairs(PairArgs<Real> &a, cudaStream_t st, int mode, const PairTerms &t,
+                        int *form) {
   switch (a.mask) {
-    case TERM_LJ: launch_pairs_t<Real, TERM_LJ>(a, st, mode, t); break;
-    case TERM_COUL: launch_pairs_t<Real, TERM_COUL>(a, st, mode, t); break;
-    case TERM_LJ | TERM_COUL: launch_pairs_t<Real, TERM_LJ | TERM_COUL>(a, st, mode, t); break;
-    case TERM_EWALD: launch_pairs_t<Real, TERM_EWALD>(a, st, mode, t); break;
-    case TERM_LJ | TERM_EWALD: launch_pairs_t<Real, TERM_LJ | TERM_EWALD>(a, st, mode, t); break;
+    case TERM_LJ: *form = launch_pairs_t<Real, TERM_LJ>(a, st, mode, t); break;
+    case TERM_COUL: *form = launch_pairs_t<Real, TERM_COUL>(a, st, mode, t); break;
+    case TERM_LJ | TERM_COUL:
+      *form = launch_pairs_t<Real, TERM_LJ | TERM_COUL>(a, st, mode, t);
+      break;
+    case TERM_EWALD: *form = launch_pairs_t<Real, TERM_EWALD>(a, st, mode, t); break;
+    case TERM_LJ | TERM_EWALD:
+      *form = launch_pairs_t<Real, TERM_LJ | TERM_EWALD>(a, st, mode, t);
+      break;
     default:
       return fail(PMGPU_ERR_UNSUPPORTED, "unsupported pair-term combination");
   }
@@ -1029,23 +1074,38 @@ static int launch_pairs(PairArgs<Real> &a, cudaStream_t st, int mode, const Pair
 
 // mode: PAIR_FORCE (forces only), PAIR_ENERGY (+ FP64 energies),
 // PAIR_VIRIAL (+ virial), PAIR_RECORD (+ pair-set recording).
-int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode) {
+int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode, int fold) {
   if (s->n == 0) return PMGPU_OK;
   if (s->precision == PMGPU_PREC_MIXED) {
     PairArgs<float> a;
     fill_pair_args<float>(a, s, nl, t);
-    PM_CHECK(launch_pairs<float>(a, s->stream, mode, t));
+    PM_CHECK(launch_pairs<float>(a, s->stream, mode, t, &nl->last_form));
   } else {
     PairArgs<double> a;
     fill_pair_args<double>(a, s, nl, t);
-    PM_CHECK(launch_pairs<double>(a, s->stream, mode, t));
+    PM_CHECK(launch_pairs<double>(a, s->stream, mode, t, &nl->last_form));
   }
   // In the force-only steps of an MD run with one list the next update
   // kernel adds the slot buffer into the forces itself (and clears it)
-  if (mode == PAIR_FORCE && s->lists.size() == 1) return PMGPU_OK;
+  if (!fold && mode == PAIR_FORCE && s->lists.size() == 1) {
+    nl->slot_pending = 1;
+    return PMGPU_OK;
+  }
+  nl->slot_pending = 1;
+  return nb_fold_slots(s, nl);
+}
+
+int nb_fold_slots(System *s, NeighborList *nl) {
+  if (!nl->slot_pending || s->n == 0) return PMGPU_OK;
   PM_CUDA(launch_pdl(k_slot_forces, (nl->ns_max + 255) / 256, 256, 0, s->stream, nl->ns_max,
                      s->n, nl->d_sorted, nl->d_fslot, s->d_force));
   PM_CUDA(cudaGetLastError());
+  nl->slot_pending = 0;
+  return PMGPU_OK;
+}
+
+int fold_pending_slots(System *s) {
+  for (auto &nl : s->lists) PM_CHECK(nb_fold_slots(s, &nl));
   return PMGPU_OK;
 }
 

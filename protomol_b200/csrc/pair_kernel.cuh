@@ -232,24 +232,16 @@ __device__ __forceinline__ void switch_fast(const SwitchDev<Real> &sw, Real r2, 
 
 // Pair force of the force-only specialised kernels: every term inside its
 // (common) cutoff, no energies, no branches.  Same arithmetic as
-// pair_force.
-template <typename Real, int TERMS, typename SPEC, bool MOD>
-__device__ __forceinline__ Real pair_force_fast(const PairArgs<Real> &a, const Real *ljrow,
-                                                Real r2, Real qq, int tj, bool modified) {
+// pair_force.  p holds the pair's LJ table entry (A, B, A14, B14).
+template <typename Real, int TERMS, typename SPEC, bool MOD, typename P4>
+__device__ __forceinline__ Real pair_force_p(const PairArgs<Real> &a, const P4 &p, Real r2,
+                                             Real qq, bool modified) {
   const Real rinv = rsqrt_nr(r2);
   const Real rinv2 = rinv * rinv;
   Real f = 0;
   if (TERMS & TERM_LJ) {
-    Real A, B;
-    if (sizeof(Real) == 4) {
-      const float4 p = __ldg(reinterpret_cast<const float4 *>(ljrow) + tj);
-      A = MOD && modified ? p.z : p.x;
-      B = MOD && modified ? p.w : p.y;
-    } else {
-      const double4 p = reinterpret_cast<const double4 *>(ljrow)[tj];
-      A = MOD && modified ? p.z : p.x;
-      B = MOD && modified ? p.w : p.y;
-    }
+    const Real A = MOD && modified ? p.z : p.x;
+    const Real B = MOD && modified ? p.w : p.y;
     const Real r6 = rinv2 * rinv2 * rinv2;
     const Real r6B = B * r6;
     const Real r12A = A * r6 * r6;
@@ -271,6 +263,17 @@ __device__ __forceinline__ Real pair_force_fast(const PairArgs<Real> &a, const R
     f += (en + a.a2pi * ee) * rinv2;
   }
   return f;
+}
+
+template <typename Real, int TERMS, typename SPEC, bool MOD>
+__device__ __forceinline__ Real pair_force_fast(const PairArgs<Real> &a, const Real *ljrow,
+                                                Real r2, Real qq, int tj, bool modified) {
+  if (sizeof(Real) == 4) {
+    const float4 p = __ldg(reinterpret_cast<const float4 *>(ljrow) + tj);
+    return pair_force_p<Real, TERMS, SPEC, MOD>(a, p, r2, qq, modified);
+  }
+  const double4 p = reinterpret_cast<const double4 *>(ljrow)[tj];
+  return pair_force_p<Real, TERMS, SPEC, MOD>(a, p, r2, qq, modified);
 }
 
 // FP64 energies (and, for the virial, the FP64 pair force) of one accepted
@@ -646,6 +649,190 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
           red_add(&a.acc[ACC_VIRIAL + q], to_fixed(V[map[q]], kEnergyScale));
       }
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Force-only FP32 pair kernel of the inner MD steps, j atoms on the lanes.
+//
+// A warp takes the tiles of its work item (one 8-atom i cluster, a
+// contiguous share of its tiles) eight at a time: lane l holds j atom l & 3
+// of tile l >> 2 of the batch and evaluates its pairs with the cluster's 8
+// i atoms one after another, the i atoms broadcast from shared memory.  A
+// lane's j force is complete after those eight pairs and goes out with one
+// fixed-point atomic per component.  The i forces stay in registers (8
+// atoms x 3 components per lane) over all the tiles of the item and are
+// summed over the lanes once, at its end, by transposed butterflies
+// (warp_tsum8).  Against one pair per lane per tile (k_pairs) this leaves
+// out the per-tile image bookkeeping, the per-tile j-force reduction and the
+// tile-wide votes: the work per tile is the pair arithmetic and a few loads.
+//
+// Coordinates: FP32 vectors from the cluster's first atom, formed in FP64
+// from the wrapped FP64 positions with the j atom's periodic image added in
+// FP64, so each distance carries one FP32 rounding of vectors no longer
+// than the reach plus the cluster extent.  Pairs within the relative band
+// of the cutoff take the reference's exact FP64 test after the batch's
+// pairs (rare), so the accepted set is the reference's.
+constexpr int kJlWarps = 8;
+constexpr int kJlMaxTypes = 16;  // LJ tables staged in shared memory up to this many types
+
+// The eight pairs of one lane's j atom with the cluster's i atoms.
+template <int TERMS, typename SPEC, bool MOD, bool SMEM_LJ>
+__device__ __forceinline__ void jl_pairs8(const PairArgs<float> &a, const float4 *s_lj,
+                                          const float4 *xi, const int *ti, float rjx, float rjy,
+                                          float rjz, float qj, int tj, unsigned mi, unsigned mm,
+                                          float (&fi)[8][3], float &fjx, float &fjy, float &fjz,
+                                          unsigned &band, int &npairs) {
+#pragma unroll
+  for (int il = 0; il < 8; il++) {
+    const float4 x = xi[il];
+    const float dx = rjx - x.x, dy = rjy - x.y, dz = rjz - x.z;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const bool on = (mi >> il) & 1u;
+    const bool act = on && r2 <= a.max_lo;
+    band |= (on && !act && r2 <= a.max_hi) ? (1u << il) : 0u;
+    npairs += act;
+    const float rr = act ? r2 : 1.f;
+    const float4 p = SMEM_LJ ? s_lj[ti[il] + tj] : __ldg(a.lj32 + ti[il] + tj);
+    float f = pair_force_p<float, TERMS, SPEC, MOD>(a, p, rr, x.w * qj,
+                                                    MOD && ((mm >> il) & 1u));
+    f = act ? f : 0.f;
+    fjx = fmaf(dx, f, fjx);
+    fjy = fmaf(dy, f, fjy);
+    fjz = fmaf(dz, f, fjz);
+    fi[il][0] = fmaf(-dx, f, fi[il][0]);
+    fi[il][1] = fmaf(-dy, f, fi[il][1]);
+    fi[il][2] = fmaf(-dz, f, fi[il][2]);
+  }
+}
+
+template <int TERMS, typename SPEC, bool SMEM_LJ>
+__global__ void __launch_bounds__(kJlWarps * 32, 3) k_pairs_jl(PairArgs<float> a) {
+  constexpr unsigned kAll = 0xffffffffu;
+  __shared__ float4 s_lj[SMEM_LJ ? kJlMaxTypes * kJlMaxTypes : 1];
+  __shared__ float4 s_xi[kJlWarps][8];   // i atoms from the reference point, charge
+  __shared__ int s_ti[kJlWarps][8];      // i type * ntypes
+  __shared__ int s_oi[kJlWarps][8];      // i atom (-1: padding)
+  __shared__ double s_wc[kJlWarps][3];   // reference point (FP64)
+  if (SMEM_LJ) {
+    for (int k = threadIdx.x; k < a.ntypes * a.ntypes; k += blockDim.x) s_lj[k] = a.lj32[k];
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int tb = lane >> 2, jl = lane & 3;
+  int npairs = 0;
+  const int nitems = a.nclusters * a.splits;
+  for (int gw = blockIdx.x * kJlWarps + wib; gw < nitems; gw += gridDim.x * kJlWarps) {
+    const int ci = gw / a.splits, sp = gw - ci * a.splits;
+    static_assert(kRowParts == 4, "one int4 of row counts per cluster");
+    const int4 c4 = *reinterpret_cast<const int4 *>(a.tile_count + kRowParts * ci);
+    const int p1 = c4.x, p2 = p1 + c4.y, p3 = p2 + c4.z, cnt = p3 + c4.w;
+    const int t0 = (int)((long long)cnt * sp / a.splits);
+    const int t1 = (int)((long long)cnt * (sp + 1) / a.splits);
+    if (t1 <= t0) continue;
+    __syncwarp();  // the previous item's reads of this warp's staging are done
+    if (lane < 8) {
+      const int islot = 8 * ci + lane;
+      const double4 w0 = a.xw[8 * ci];  // a cluster with tiles has an atom in its first slot
+      const double4 wi = a.xw[islot];
+      const int oi = a.sorted[islot];
+      s_xi[wib][lane] = make_float4((float)(wi.x - w0.x), (float)(wi.y - w0.y),
+                                    (float)(wi.z - w0.z), (float)wi.w);
+      s_ti[wib][lane] = (oi >= 0 ? __float_as_int(__ldg(&a.xlo[islot].w)) : 0) * a.ntypes;
+      s_oi[wib][lane] = oi;
+      if (lane < 3) s_wc[wib][lane] = lane == 0 ? w0.x : (lane == 1 ? w0.y : w0.z);
+    }
+    __syncwarp();
+    const float4 *xi = s_xi[wib];
+    const int *ti = s_ti[wib];
+    float fi[8][3];
+#pragma unroll
+    for (int k = 0; k < 8; k++) fi[k][0] = fi[k][1] = fi[k][2] = 0.f;
+    for (int b0 = t0; b0 < t1; b0 += 8) {
+      const int idx = b0 + tb;
+      unsigned mi = 0u, mm = 0u;
+      int jslot = 0, tj = 0;
+      float rjx = 0.f, rjy = 0.f, rjz = 0.f, qj = 0.f;
+      if (idx < t1) {
+        // tile idx of the cluster's row parts read one after the other
+        const int p = (idx >= p1) + (idx >= p2) + (idx >= p3);
+        const int off = idx - (p == 0 ? 0 : (p == 1 ? p1 : (p == 2 ? p2 : p3)));
+        const uint4 tile = __ldg(a.tiles + (size_t)(kRowParts * ci + p) * a.cap + off);
+        const int hj = (int)(tile.x & kJMask);
+        const int sh = (int)((tile.x >> kShiftBits) & kShiftMask);
+        mi = (tile.y >> (8 * jl)) & 0xFFu;
+        mm = (tile.z >> (8 * jl)) & 0xFFu;
+        jslot = 4 * hj + jl;
+        const double4 wj = a.xw[jslot];
+        // the j atom in the tile's image (d = xj + s L - xi), from the
+        // reference point
+        rjx = (float)((wj.x + (double)((sh & 3) - 1) * a.box.e[0]) - s_wc[wib][0]);
+        rjy = (float)((wj.y + (double)(((sh >> 2) & 3) - 1) * a.box.e[1]) - s_wc[wib][1]);
+        rjz = (float)((wj.z + (double)(((sh >> 4) & 3) - 1) * a.box.e[2]) - s_wc[wib][2]);
+        qj = (float)wj.w;
+        tj = __float_as_int(__ldg(&a.xlo[jslot].w));
+      }
+      float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+      unsigned band = 0u;
+      // modified (scaled 1-4) pairs are rare: batches without any take the
+      // path without their selects
+      if (__any_sync(kAll, mm != 0u))
+        jl_pairs8<TERMS, SPEC, true, SMEM_LJ>(a, s_lj, xi, ti, rjx, rjy, rjz, qj, tj, mi, mm, fi,
+                                              fjx, fjy, fjz, band, npairs);
+      else
+        jl_pairs8<TERMS, SPEC, false, SMEM_LJ>(a, s_lj, xi, ti, rjx, rjy, rjz, qj, tj, mi, mm,
+                                               fi, fjx, fjy, fjz, band, npairs);
+      // pairs within the rounding band of the cutoff: the exact FP64 test
+      // (rare; their i forces go out as atomics, so this path keeps none of
+      // the register-held sums live)
+      if (__any_sync(kAll, band != 0u)) {
+        const int oj = band ? a.sorted[jslot] : -1;
+        while (band) {
+          const int il = __ffs(band) - 1;
+          band &= band - 1u;
+          const float4 x = xi[il];
+          const float dx = rjx - x.x, dy = rjy - x.y, dz = rjz - x.z;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          if (exact_r2(a, s_oi[wib][il], oj, (double)dx, (double)dy, (double)dz) > a.max_cut2)
+            continue;
+          const float4 p = SMEM_LJ ? s_lj[ti[il] + tj] : __ldg(a.lj32 + ti[il] + tj);
+          const float f = pair_force_p<float, TERMS, SPEC, true>(a, p, r2, x.w * qj,
+                                                                 (mm >> il) & 1u);
+          fjx = fmaf(dx, f, fjx);
+          fjy = fmaf(dy, f, fjy);
+          fjz = fmaf(dz, f, fjz);
+          long long *di = a.fslot + 8 * ci + il;
+          red_add(di, fixed_force(-dx * f));
+          red_add(di + a.ns, fixed_force(-dy * f));
+          red_add(di + 2 * (size_t)a.ns, fixed_force(-dz * f));
+          npairs++;
+        }
+      }
+      if (mi) {
+        long long *dst = a.fslot + jslot;
+        red_add(dst, fixed_force(fjx));
+        red_add(dst + a.ns, fixed_force(fjy));
+        red_add(dst + 2 * (size_t)a.ns, fixed_force(fjz));
+      }
+    }
+    // the i forces summed over the lanes: lane l ends with the totals of i
+    // atom (l >> 2) & 7 and writes component l & 3
+    float sum[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float v[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = fi[k][c];
+      sum[c] = warp_tsum8(v, lane);
+    }
+    const int il = (lane >> 2) & 7, comp = lane & 3;
+    if (comp < 3 && s_oi[wib][il] >= 0)
+      red_add(&a.fslot[(size_t)comp * a.ns + 8 * ci + il],
+              fixed_force(comp == 0 ? sum[0] : (comp == 1 ? sum[1] : sum[2])));
+  }
+  if (a.count_pairs) {
+    const int np = warp_sum(npairs);
+    if (lane == 0) red_add(&a.acc[ACC_PAIRS], (long long)np);
   }
 }
 

@@ -137,6 +137,10 @@ struct NeighborList {
   int cap = 0;                       // tiles per row
   int built = 0;
   int decided = 0;                   // this evaluation's rebuild decision is taken
+  // a force-only MD step left its pair forces in d_fslot for the next update
+  // kernel to add; until then d_force lacks them (nb_fold_slots adds them)
+  int slot_pending = 0;
+  int last_form = PMGPU_PAIRK_GENERIC;  // pair-kernel form of the last launch
   long long builds = 0;
   // device
   int *d_key = nullptr;          // n: column of each atom
@@ -191,6 +195,8 @@ struct Force {
   int sf_lj = 0, sf_coul = 0;
   // gb
   double solute = 1.0, solvent = 80.0;
+  // gbace (GBACEForce -solvationparam, -watersphereradius)
+  double ace_sigma = 0.0, ace_rho = 0.0;
   // bonded
   int bonds = 0, angles = 0;
   int dihedrals = 0, impropers = 0;
@@ -198,7 +204,7 @@ struct Force {
 };
 
 enum { FK_CUTOFF = 1, FK_PME = 2, FK_GB = 3, FK_BONDED = 4,
-       FK_SIMPLEFULL = 5, FK_TORSION = 6 };
+       FK_SIMPLEFULL = 5, FK_TORSION = 6, FK_GBACE = 7 };
 
 // Per-phase CUDA-event timing; events are recorded only when enabled and
 // summed at the next host synchronisation.
@@ -259,6 +265,7 @@ struct System {
   double gb_obc[3] = {1.0, 0.8, 4.85};
   double *d_gb_born = nullptr, *d_gb_psi = nullptr, *d_gb_partial = nullptr;
   long long *d_gb_fixed = nullptr;  // 2n: burial and partial-sum accumulators
+  double *d_gb_ace = nullptr;       // n: GBACE pair-force factor per atom
   // dynamic state
   double *d_pos = nullptr;   // 3n AoS
   double *d_vel = nullptr;   // 3n AoS
@@ -354,7 +361,13 @@ int nb_list_free(System *s, NeighborList *nl);
 // build), then nb_pair_forces.
 int nb_prepare(System *s, NeighborList *nl, int force_rebuild);
 int nb_build(System *s, NeighborList *nl);
-int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode);
+// fold: add the slot-ordered pair forces into the atom forces at once;
+// 0 (force-only MD steps with one list) leaves them for the next update
+// kernel and marks the list slot_pending
+int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode, int fold);
+// adds a pending slot buffer into the atom forces (no-op when none is pending)
+int nb_fold_slots(System *s, NeighborList *nl);
+int fold_pending_slots(System *s);
 int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
 int nb_simplefull(System *s, int lj, int coul, int em);
 // the exclusion tile masks of the FP32 simple-full pass (once per system)
@@ -378,7 +391,7 @@ int ewald_correction(System *s, Force *f, int em);
 
 // gb.cu
 int gb_init(System *s);
-int gb_forces(System *s, Force *f);
+int gb_forces(System *s, const Force *gb, const Force *ace);
 
 // bonded_integrate.cu
 // bonds, angles, dihedrals and impropers (each flag: include that kind) in

@@ -30,6 +30,10 @@ VIRIALXX = 7
 SCALAR_LAST = 36
 
 
+# forms of the pair kernel (PMGPU_PAIRK_*)
+PAIR_KERNELS = {0: "generic", 1: "lj_c2+ewald", 2: "lj_c2+coulomb_c2", 3: "lj_c2+coulomb_c1"}
+
+
 def ScalarStructure() -> np.ndarray:
     """A zeroed ScalarStructure-layout energy/virial array."""
     return np.zeros(SCALAR_LAST)
@@ -204,6 +208,13 @@ class GpuSystem:
         L.check(self.lib.pmgpu_evaluate(self.h, L.ptr(e), L.ptr(v)))
         return e, (v.reshape(3, 3) if v is not None else None)
 
+    def evaluate_forces(self) -> np.ndarray:
+        """Force-only evaluation of all enabled forces at the resident
+        positions (the kernels of an inner MD step, no energies); returns the
+        total force (n, 3)."""
+        L.check(self.lib.pmgpu_evaluate(self.h, None, None))
+        return self.forces_total()
+
     def energies(self):
         """(energies[7], virial[3,3]) of the last evaluation or run segment,
         without evaluating again."""
@@ -260,24 +271,26 @@ class SystemForce:
         self.id = fid
         system.forces.append(self)
 
-    def evaluate(self, positions, forces: np.ndarray, energies: np.ndarray,
+    def evaluate(self, positions, forces: np.ndarray, energies: np.ndarray | None,
                  virial: bool = False) -> None:
         """SystemForce::evaluate: uploads positions, evaluates this term,
-        ADDS into forces (n,3) and energies (ScalarStructure layout)."""
+        ADDS into forces (n,3) and energies (ScalarStructure layout).  With
+        energies None (and no virial) the term is evaluated force-only."""
         s = self.system
         pos = s._vec(positions)
         f = np.ascontiguousarray(forces, dtype=np.float64)
         if f.size != 3 * s.n:
             raise ValueError("forces must hold 3n values")
-        e = np.zeros(L.E_COUNT)
+        e = np.zeros(L.E_COUNT) if (energies is not None or virial) else None
         v = np.zeros(9) if virial else None
         L.check(s.lib.pmgpu_force_evaluate(s.h, self.id, L.ptr(pos), L.ptr(f), L.ptr(e),
                                            L.ptr(v)))
         if f is not forces:
             forces[...] = f.reshape(forces.shape)
-        energies[:L.E_COUNT] += e
-        if virial:
-            energies[VIRIALXX:VIRIALXX + 9] += v
+        if energies is not None:
+            energies[:L.E_COUNT] += e
+            if virial:
+                energies[VIRIALXX:VIRIALXX + 9] += v
 
     def set_enabled(self, on: bool) -> None:
         L.check(self.system.lib.pmgpu_force_set_enabled(self.system.h, self.id, 1 if on else 0))
@@ -286,7 +299,8 @@ class SystemForce:
         st = L.Stats()
         L.check(self.system.lib.pmgpu_force_stats(self.system.h, self.id, C.byref(st)))
         return dict(pairs_in_cutoff=st.pairs_in_cutoff, list_entries=st.list_entries,
-                    list_builds=st.list_builds, cells=tuple(st.cells))
+                    list_builds=st.list_builds, cells=tuple(st.cells),
+                    pair_kernel=PAIR_KERNELS.get(st.pair_kernel, st.pair_kernel))
 
     def pair_set(self, cap: int = 1 << 24) -> np.ndarray:
         """The unordered pair set (i < j) this force evaluates at the
@@ -358,6 +372,20 @@ class GBForce(SystemForce):
         fid = C.c_int()
         L.check(system.lib.pmgpu_force_gb_add(system.h, float(solute_dielec),
                                               float(solvent_dielec), C.byref(fid)))
+        super().__init__(system, fid.value)
+
+
+class GBACEForce(SystemForce):
+    """``GBACEForce`` (force/GB/GBACEForce.cpp): the ACE nonpolar term on the
+    OBC Born radii, vacuum all pairs; with a GBForce in the same evaluation
+    both share one Born-radius computation."""
+    keyword = "GBACEForce"
+
+    def __init__(self, system: GpuSystem, solvation_param: float = 2.26 / 418.4,
+                 water_sphere_radius: float = 1.4):
+        fid = C.c_int()
+        L.check(system.lib.pmgpu_force_gbace_add(system.h, float(solvation_param),
+                                                 float(water_sphere_radius), C.byref(fid)))
         super().__init__(system, fid.value)
 
 
@@ -469,6 +497,9 @@ class ForceFactory:
         if algn == "nonbondedsimplefull":
             if "gbforce" in names:
                 return GBForce(s, p.get("solutedielec", 1.0), p.get("solventdielec", 80.0))
+            if "gbaceforce" in names:
+                return GBACEForce(s, p.get("solvationparam", 2.26 / 418.4),
+                                  p.get("watersphereradius", 1.4))
             if "gbbornradii" in names or "gbpartialsum" in names:
                 return _NoOpForce(s, names[0])
             return NonbondedSimpleFullSystemForce(s, "lennardjones" in names, "coulomb" in names)

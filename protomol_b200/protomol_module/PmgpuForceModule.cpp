@@ -1,34 +1,62 @@
-// ProtoMol module that puts the libpmgpu forces behind ProtoMol's own
-// force-module API, so a .conf selects them with the usual grammar:
+// ProtoMol module that puts libpmgpu behind ProtoMol's own force and
+// integrator factories, so a .conf selects the device path with the
+// reference grammar, the algorithm name carrying a GPU suffix:
 //
-//   force LennardJones Coulomb -algorithm NonbondedCutoffGPU -cutoff 8
-//         -ljswitch C2 -ljswitchon 7 -coulombswitch C2 -coulombswitchon 7
-//   force LennardJones -algorithm NonbondedCutoffGPU -cutoff 9 -ljswitch C2 -ljswitchon 8
+//   force LennardJones Coulomb -algorithm NonbondedCutoffGPU
+//         -switchingFunction C2 -switchon 7 -cutoff 8
+//         -switchingFunction C1 -cutoff 8 -cutoff 8
 //   force Coulomb -algorithm PMEwaldGPU -alpha 0.35 -cutoff 9 -order 4 -gridsize 64
+//   force GBBornRadii -algorithm NonbondedSimpleFullGPU
+//   force GBPartialSum -algorithm NonbondedSimpleFullGPU
+//   force GBForce -algorithm NonbondedSimpleFullGPU -soluteDielec 1 -solventDielec 78.5
+//   force LennardJones -algorithm NonbondedSimpleFullGPU
 //   force Dihedral -algorithm TorsionGPU
+//   Integrator { level 0 LeapfrogGPU { timestep 1 force ... } }
+//   Integrator { level 0 LangevinLeapfrogGPU { timestep 1 temperature 300
+//                gamma 5 seed 1234 force ... } }
 //
-// Each force is a SystemForce (force/system/SystemForce.h:16-85) whose
-// evaluate() adds its forces into the caller's Vector3DBlock and its
-// energies (and virial when requested) into the ScalarStructure, exactly
-// the contract of the CPU forces it replaces.  All GPU forces of one
-// topology share one pmgpu system, built on first use from the topology
-// ProtoMol made (atoms, LJ table, exclusion table, periodic box, torsions).
-// Registration follows module/BondedForcesModule.cpp: a Module whose
-// registerForces() hands exemplars to app->forceFactory.
+// Forces.  Each GPU force is a SystemForce (force/system/SystemForce.h:16-85)
+// whose evaluate() adds its forces into the caller's Vector3DBlock and its
+// energies (and virial when asked) into the ScalarStructure, the contract of
+// the CPU forces it replaces; driven by a CPU integrator, positions go to
+// the device and forces come back every evaluation.  The cutoff forces are
+// registered per switching-function combination with the parameter lists of
+// their CPU counterparts (OneAtomPair(Two)::getParameters, then the
+// algorithm -cutoff, force/nonbonded/NonbondedCutoffForce.h:85-91), so the
+// factory (factory/ForceFactory.cpp:21-242) reads the same lines.
+//
+// Integrators.  LeapfrogGPU and LangevinLeapfrogGPU are STSIntegrators
+// whose run(n) (integrator/leapfrog/LeapfrogIntegrator.cpp:89-104 and
+// StandardIntegrator.cpp:27-37 with LangevinLeapfrogIntegrator's half
+// kicks) runs all n steps on the device: positions, velocities and forces
+// stay resident, and only at the end of run(n) (ProtoMolApp::step hands
+// run() the steps up to the next output, ProtoMolApp.cpp:486-498) are
+// positions, velocities, forces and energies written back to the app for
+// the outputs and checkpoints.  Every force of their force group must have
+// a device form: the GPU forces above, and the CPU Bond, Angle, Dihedral and
+// Improper forces, which they map to the device's bonded terms.
+//
+// All GPU forces and integrators of one topology share one pmgpu system,
+// built on first use from the topology ProtoMol made.  Registration follows
+// module/BondedForcesModule.cpp and module/LeapfrogModule.cpp:18-24.
 #include "PmgpuForceModule.h"
 
 #include <protomol/ProtoMolApp.h>
 #include <protomol/base/Exception.h>
+#include <protomol/base/PMConstants.h>
 #include <protomol/base/StringUtilities.h>
 #include <protomol/config/Parameter.h>
 #include <protomol/config/Value.h>
+#include <protomol/force/ForceGroup.h>
 #include <protomol/force/system/SystemForce.h>
+#include <protomol/integrator/STSIntegrator.h>
 #include <protomol/topology/GenericTopology.h>
 #include <protomol/topology/PeriodicBoundaryConditions.h>
 #include <protomol/topology/SemiGenericTopology.h>
 #include <protomol/type/ScalarStructure.h>
 #include <protomol/type/Vector3DBlock.h>
 
+#include <cstring>
 #include <map>
 #include <string>
 #include <vector>
@@ -55,14 +83,20 @@ Shared &shared() {
   return s;
 }
 
+// The pmgpu topology of a ProtoMol topology: atoms (scaled charges and
+// masses), the LJ table, the exclusion table (the class check() returns for
+// the pair forces, the class the table holds for the Ewald correction),
+// bonds, angles, torsions (one term per multiplicity), GB atom parameters
+// and OBC constants, and the periodic box.
 pmgpu_system *systemFor(const GenericTopology *topo) {
   Shared &sh = shared();
   map<const GenericTopology *, pmgpu_system *>::iterator it = sh.systems.find(topo);
   if (it != sh.systems.end()) return it->second;
   if (!sh.ctx) check(pmgpu_context_create(0, &sh.ctx), "pmgpu context");
   const int n = (int)topo->atoms.size();
-  vector<double> q(n), m(n);
+  vector<double> q(n), m(n), vdwr(n), scale(n), offset(n);
   vector<int> type(n), mol(n), water(n);
+  bool gb = n > 0;
   for (int i = 0; i < n; i++) {
     const Atom &a = topo->atoms[i];
     q[i] = a.scaledCharge;
@@ -70,6 +104,13 @@ pmgpu_system *systemFor(const GenericTopology *topo) {
     type[i] = a.type;
     mol[i] = a.molecule;
     water[i] = topo->molecules[a.molecule].water ? 1 : 0;
+    if (a.myGBSA_T) {
+      vdwr[i] = a.myGBSA_T->vanDerWaalRadius;
+      scale[i] = a.myGBSA_T->scalingFactor;
+      offset[i] = a.myGBSA_T->offsetRadius;
+    } else {
+      gb = false;
+    }
   }
   const int nt = (int)topo->lennardJonesParameters.size();
   vector<double> lj(4 * (size_t)nt * nt);
@@ -82,49 +123,85 @@ pmgpu_system *systemFor(const GenericTopology *topo) {
       d[2] = p.A14;
       d[3] = p.B14;
     }
-  // exclusions: the pair forces use ExclusionTable::check(), the Ewald
-  // correction iterates getTable()
   const vector<ExclusionPair> &ex = topo->exclusions.getTable();
-  vector<int> excl(3 * ex.size()), table_class(ex.size());
+  vector<int> excl(3 * ex.size() + 3), table_class(ex.size() + 1);
   for (size_t k = 0; k < ex.size(); k++) {
     excl[3 * k] = ex[k].a1;
     excl[3 * k + 1] = ex[k].a2;
     excl[3 * k + 2] = (int)topo->exclusions.check(ex[k].a1, ex[k].a2);
     table_class[k] = (int)ex[k].excl;
   }
-  vector<int> tors;
-  vector<double> tprm;
-  for (size_t k = 0; k < topo->dihedrals.size(); k++) {
-    const Torsion &t = topo->dihedrals[k];
-    for (int j = 0; j < t.multiplicity; j++) {
-      tors.push_back(t.atom1);
-      tors.push_back(t.atom2);
-      tors.push_back(t.atom3);
-      tors.push_back(t.atom4);
-      tprm.push_back(t.forceConstant[j]);
-      tprm.push_back((double)t.periodicity[j]);
-      tprm.push_back(t.phaseShift[j]);
+  vector<int> bonds, angles;
+  vector<double> bprm, aprm;
+  for (size_t k = 0; k < topo->bonds.size(); k++) {
+    const Bond &b = topo->bonds[k];
+    bonds.push_back(b.atom1);
+    bonds.push_back(b.atom2);
+    bprm.push_back(b.springConstant);
+    bprm.push_back(b.restLength);
+  }
+  for (size_t k = 0; k < topo->angles.size(); k++) {
+    const Angle &a = topo->angles[k];
+    angles.push_back(a.atom1);
+    angles.push_back(a.atom2);
+    angles.push_back(a.atom3);
+    aprm.push_back(a.forceConstant);
+    aprm.push_back(a.restAngle);
+    aprm.push_back(a.ureyBradleyConstant);
+    aprm.push_back(a.ureyBradleyRestLength);
+  }
+  vector<int> tors[2];
+  vector<double> tprm[2];
+  for (int kind = 0; kind < 2; kind++) {
+    const vector<Torsion> &list = kind == 0 ? topo->dihedrals : topo->impropers;
+    for (size_t k = 0; k < list.size(); k++) {
+      const Torsion &t = list[k];
+      for (int j = 0; j < t.multiplicity; j++) {
+        tors[kind].push_back(t.atom1);
+        tors[kind].push_back(t.atom2);
+        tors[kind].push_back(t.atom3);
+        tors[kind].push_back(t.atom4);
+        tprm[kind].push_back(t.forceConstant[j]);
+        tprm[kind].push_back((double)t.periodicity[j]);
+        tprm[kind].push_back(t.phaseShift[j]);
+      }
     }
   }
-  pmgpu_topology t = pmgpu_topology();
+  pmgpu_topology t;
+  memset(&t, 0, sizeof(t));
   t.n_atoms = n;
-  t.charge = &q[0];
-  t.mass = &m[0];
-  t.type = &type[0];
-  t.molecule = &mol[0];
+  t.charge = n ? &q[0] : 0;
+  t.mass = n ? &m[0] : 0;
+  t.type = n ? &type[0] : 0;
+  t.molecule = n ? &mol[0] : 0;
   t.n_types = nt;
   t.lj = lj.empty() ? 0 : &lj[0];
   t.n_exclusions = (int)ex.size();
-  t.exclusions = excl.empty() ? 0 : &excl[0];
-  t.exclusion_table_class = table_class.empty() ? 0 : &table_class[0];
+  t.exclusions = &excl[0];
+  t.exclusion_table_class = &table_class[0];
   t.coulomb_scaling = topo->coulombScalingFactor;
-  t.water = &water[0];
-  t.gb_obc[0] = 1.0;
-  t.gb_obc[1] = 0.8;
-  t.gb_obc[2] = 4.85;
-  t.n_dihedrals = (int)tors.size() / 4;
-  t.dihedral_atoms = tors.empty() ? 0 : &tors[0];
-  t.dihedral_params = tprm.empty() ? 0 : &tprm[0];
+  t.n_bonds = (int)topo->bonds.size();
+  t.bond_atoms = bonds.empty() ? 0 : &bonds[0];
+  t.bond_params = bprm.empty() ? 0 : &bprm[0];
+  t.n_angles = (int)topo->angles.size();
+  t.angle_atoms = angles.empty() ? 0 : &angles[0];
+  t.angle_params = aprm.empty() ? 0 : &aprm[0];
+  if (gb) {
+    t.gb_vdwr = &vdwr[0];
+    t.gb_scale = &scale[0];
+    t.gb_offset = &offset[0];
+  }
+  t.water = n ? &water[0] : 0;
+  // OBC constants as ProtoMolApp sets them for doGBSAObc (ProtoMolApp.cpp:285-299)
+  t.gb_obc[0] = topo->alphaObc;
+  t.gb_obc[1] = topo->betaObc;
+  t.gb_obc[2] = topo->gammaObc;
+  t.n_dihedrals = (int)tors[0].size() / 4;
+  t.dihedral_atoms = tors[0].empty() ? 0 : &tors[0][0];
+  t.dihedral_params = tprm[0].empty() ? 0 : &tprm[0][0];
+  t.n_impropers = (int)tors[1].size() / 4;
+  t.improper_atoms = tors[1].empty() ? 0 : &tors[1][0];
+  t.improper_params = tprm[1].empty() ? 0 : &tprm[1][0];
   const SemiGenericTopology<PeriodicBoundaryConditions> *pt =
       dynamic_cast<const SemiGenericTopology<PeriodicBoundaryConditions> *>(topo);
   if (pt) {
@@ -143,41 +220,44 @@ pmgpu_system *systemFor(const GenericTopology *topo) {
   return s;
 }
 
-int switchKind(const string &name) {
-  if (equalNocase(name, "C1")) return PMGPU_SW_C1;
-  if (equalNocase(name, "C2")) return PMGPU_SW_C2;
-  if (equalNocase(name, "Cutoff")) return PMGPU_SW_CUTOFF;
-  if (equalNocase(name, "Universal")) return PMGPU_SW_UNIVERSAL;
-  THROW("unknown switching function '" + name + "' (C1, C2, Cutoff)");
-  return PMGPU_SW_CUTOFF;
+// Adds the device's energies (ScalarStructure slots COULOMB .. OTHER) and
+// virial into ProtoMol's ScalarStructure.
+void addEnergies(ScalarStructure *energies, const double *e, const double *v) {
+  static const ScalarStructure::Index slot[PMGPU_E_COUNT] = {
+      ScalarStructure::COULOMB, ScalarStructure::LENNARDJONES, ScalarStructure::BOND,
+      ScalarStructure::ANGLE, ScalarStructure::DIHEDRAL, ScalarStructure::IMPROPER,
+      ScalarStructure::OTHER};
+  for (int k = 0; k < PMGPU_E_COUNT; k++) (*energies)[slot[k]] += e[k];
+  if (v)
+    for (int k = 0; k < 9; k++)
+      (*energies)[(ScalarStructure::Index)(ScalarStructure::VIRIALXX + k)] += v[k];
 }
 
 // Common part of the GPU system forces: the force id inside the shared
-// pmgpu system, made on first evaluation, and the ADD of forces, energies
-// and virial into ProtoMol's containers.
+// pmgpu system (attach() makes it once per system) and the ADD of forces,
+// energies and virial into ProtoMol's containers.
 class PmgpuSystemForce : public SystemForce {
  public:
   PmgpuSystemForce() : myId(-1), mySystem(0) {}
-  using SystemForce::evaluate;
-  virtual void evaluate(const GenericTopology *topo, const Vector3DBlock *positions,
-                        Vector3DBlock *forces, ScalarStructure *energies) {
-    pmgpu_system *s = systemFor(topo);
-    if (s != mySystem || myId < 0) {
+  // The force's id in s (-1: a pass that runs inside another force).
+  int attach(pmgpu_system *s, const GenericTopology *topo) {
+    if (s != mySystem) {
       mySystem = s;
       myId = addTo(s, topo);
     }
+    return myId;
+  }
+  using SystemForce::evaluate;
+  virtual void evaluate(const GenericTopology *topo, const Vector3DBlock *positions,
+                        Vector3DBlock *forces, ScalarStructure *energies) {
+    const int id = attach(systemFor(topo), topo);
+    if (id < 0) return;
     double e[PMGPU_E_COUNT] = {0, 0, 0, 0, 0, 0, 0};
     double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     const bool vir = energies->virial();
-    check(pmgpu_force_evaluate(s, myId, positions->c, forces->c, e, vir ? v : 0),
+    check(pmgpu_force_evaluate(mySystem, id, positions->c, forces->c, e, vir ? v : 0),
           getIdNoAlias());
-    (*energies)[ScalarStructure::COULOMB] += e[PMGPU_E_COULOMB];
-    (*energies)[ScalarStructure::LENNARDJONES] += e[PMGPU_E_LENNARDJONES];
-    (*energies)[ScalarStructure::DIHEDRAL] += e[PMGPU_E_DIHEDRAL];
-    (*energies)[ScalarStructure::IMPROPER] += e[PMGPU_E_IMPROPER];
-    if (vir)
-      for (int k = 0; k < 9; k++)
-        (*energies)[(ScalarStructure::Index)(ScalarStructure::VIRIALXX + k)] += v[k];
+    addEnergies(energies, e, vir ? v : 0);
   }
   virtual void parallelEvaluate(const GenericTopology *topo, const Vector3DBlock *positions,
                                 Vector3DBlock *forces, ScalarStructure *energies) {
@@ -193,48 +273,103 @@ class PmgpuSystemForce : public SystemForce {
   pmgpu_system *mySystem;
 };
 
-// NonbondedCutoff (module/NonbondedCutoffForceModule.cpp:40-201) on the GPU.
+// ---------------------------------------------------------------- switches
+// A switching function's kind and the parameters its CPU counterpart reads,
+// in its order (switch/C1SwitchingFunction.cpp:18-22,
+// C2SwitchingFunction.cpp:20-28, CnSwitchingFunction.cpp:64-79,
+// CutoffSwitchingFunction.h:47-51).
+enum { P_N = 0, P_SWITCHON, P_SWITCHOFF, P_CUTOFF };
+struct SwitchSpec {
+  const char *name;
+  int kind;
+  int nparams;
+  int params[4];
+};
+const SwitchSpec kC1 = {"C1", PMGPU_SW_C1, 1, {P_CUTOFF}};
+const SwitchSpec kC2 = {"C2", PMGPU_SW_C2, 2, {P_SWITCHON, P_CUTOFF}};
+const SwitchSpec kCn = {"Cn", PMGPU_SW_CN, 4, {P_N, P_SWITCHON, P_SWITCHOFF, P_CUTOFF}};
+const SwitchSpec kCutoff = {"Cutoff", PMGPU_SW_CUTOFF, 1, {P_CUTOFF}};
+
+void switchParameters(const SwitchSpec &sw, const pmgpu_switch &v, vector<Parameter> &p) {
+  for (int k = 0; k < sw.nparams; k++) switch (sw.params[k]) {
+      case P_N:
+        p.push_back(Parameter("-n", Value(v.order, ConstraintValueType::Positive())));
+        break;
+      case P_SWITCHON:
+        p.push_back(Parameter("-switchon", Value(v.switchon, ConstraintValueType::NotNegative())));
+        break;
+      case P_SWITCHOFF:
+        p.push_back(Parameter("-switchoff", Value(v.switchoff,
+                                                  ConstraintValueType::NotNegative()), 0.0));
+        break;
+      default:
+        p.push_back(Parameter("-cutoff", Value(v.cutoff, ConstraintValueType::Positive())));
+        break;
+    }
+}
+
+// Reads the switch's values from values[*at...], advancing *at.
+pmgpu_switch switchMake(const SwitchSpec &sw, const vector<Value> &values, size_t *at) {
+  pmgpu_switch s;
+  s.kind = sw.kind;
+  s.cutoff = s.switchon = s.switchoff = s.order = 0.0;
+  for (int k = 0; k < sw.nparams; k++) {
+    Real x = 0;
+    values[(*at)++].get(x);
+    switch (sw.params[k]) {
+      case P_N: s.order = x; break;
+      case P_SWITCHON: s.switchon = x; break;
+      case P_SWITCHOFF: s.switchoff = x; break;
+      default: s.cutoff = x; break;
+    }
+  }
+  return s;
+}
+
+// ---------------------------------------------------------------- forces
+// NonbondedCutoff (module/NonbondedCutoffForceModule.cpp:55-96) on the GPU:
+// LennardJones and/or Coulomb, one switching function each.
 class CutoffGpuForce : public PmgpuSystemForce {
  public:
-  CutoffGpuForce(const string &keyword, bool lj, bool coul)
-      : myKeyword(keyword), myLJ(lj), myCoul(coul), myCutoff(8.0), myLJSwitch("C2"),
-        myLJSwitchOn(0.0), myCoulSwitch("C2"), myCoulSwitchOn(0.0) {}
-  virtual string getKeyword() const { return myKeyword; }
-  virtual string getIdNoAlias() const { return myKeyword + " -algorithm NonbondedCutoffGPU"; }
+  CutoffGpuForce(bool lj, bool coul, const SwitchSpec &a, const SwitchSpec *b)
+      : myLJ(lj), myCoul(coul), mySwA(a), mySwB(b ? *b : a), myTwo(b != 0), myCutoff(8.0) {
+    memset(&myA, 0, sizeof(myA));
+    memset(&myB, 0, sizeof(myB));
+  }
+  virtual string getKeyword() const { return "NonbondedCutoffGPU"; }
+  virtual string getIdNoAlias() const {
+    string id = myTwo ? "LennardJones Coulomb" : (myLJ ? "LennardJones" : "Coulomb");
+    id += string(" -switchingFunction ") + mySwA.name;
+    if (myTwo) id += string(" -switchingFunction ") + mySwB.name;
+    return id + " -algorithm " + getKeyword();
+  }
   virtual void getParameters(vector<Parameter> &p) const {
-    p.push_back(Parameter("-cutoff", Value(myCutoff, ConstraintValueType::Positive()), 8.0));
-    p.push_back(Parameter("-ljswitch", Value(myLJSwitch), string("C2")));
-    p.push_back(Parameter("-ljswitchon", Value(myLJSwitchOn), 0.0));
-    p.push_back(Parameter("-coulombswitch", Value(myCoulSwitch), string("C2")));
-    p.push_back(Parameter("-coulombswitchon", Value(myCoulSwitchOn), 0.0));
+    switchParameters(mySwA, myA, p);
+    if (myTwo) switchParameters(mySwB, myB, p);
+    p.push_back(Parameter("-cutoff", Value(myCutoff, ConstraintValueType::Positive())));
   }
 
  private:
   virtual Force *doMake(const vector<Value> &values) const {
-    CutoffGpuForce *f = new CutoffGpuForce(myKeyword, myLJ, myCoul);
-    f->myCutoff = values[0];
-    f->myLJSwitch = values[1].getString();
-    f->myLJSwitchOn = values[2];
-    f->myCoulSwitch = values[3].getString();
-    f->myCoulSwitchOn = values[4];
+    CutoffGpuForce *f = new CutoffGpuForce(myLJ, myCoul, mySwA, myTwo ? &mySwB : 0);
+    size_t at = 0;
+    f->myA = switchMake(mySwA, values, &at);
+    if (myTwo) f->myB = switchMake(mySwB, values, &at);
+    values[at].get(f->myCutoff);
     return f;
   }
-  virtual int addTo(pmgpu_system *s, const GenericTopology *topo) const {
-    pmgpu_switch lj = {switchKind(myLJSwitch), myCutoff, myLJSwitchOn, 0.0, 0.0};
-    pmgpu_switch co = {switchKind(myCoulSwitch), myCutoff, myCoulSwitchOn, 0.0, 0.0};
+  virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
+    const pmgpu_switch *lj = myLJ ? &myA : 0;
+    const pmgpu_switch *co = myCoul ? (myTwo ? &myB : &myA) : 0;
     int id = -1;
-    check(pmgpu_force_cutoff_add(s, myLJ ? &lj : 0, myCoul ? &co : 0, myCutoff,
-                                 0.0, &id),
-          getIdNoAlias());
+    check(pmgpu_force_cutoff_add(s, lj, co, myCutoff, 0.0, &id), getIdNoAlias());
     return id;
   }
-  string myKeyword;
   bool myLJ, myCoul;
+  SwitchSpec mySwA, mySwB;
+  bool myTwo;
+  pmgpu_switch myA, myB;
   Real myCutoff;
-  string myLJSwitch;
-  Real myLJSwitchOn;
-  string myCoulSwitch;
-  Real myCoulSwitchOn;
 };
 
 // Ewald Coulomb (NonbondedFullEwaldSystemForce, -real -reciprocal
@@ -242,7 +377,7 @@ class CutoffGpuForce : public PmgpuSystemForce {
 class PmeGpuForce : public PmgpuSystemForce {
  public:
   PmeGpuForce() : myAlpha(0.35), myCutoff(9.0), myOrder(4), myGrid(64) {}
-  virtual string getKeyword() const { return "Coulomb"; }
+  virtual string getKeyword() const { return "PMEwaldGPU"; }
   virtual string getIdNoAlias() const { return "Coulomb -algorithm PMEwaldGPU"; }
   virtual void getParameters(vector<Parameter> &p) const {
     p.push_back(Parameter("-alpha", Value(myAlpha, ConstraintValueType::Positive()), 0.35));
@@ -260,11 +395,10 @@ class PmeGpuForce : public PmgpuSystemForce {
     f->myGrid = values[3];
     return f;
   }
-  virtual int addTo(pmgpu_system *s, const GenericTopology *topo) const {
+  virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
     const int grid[3] = {myGrid, myGrid, myGrid};
     int id = -1;
-    check(pmgpu_force_pme_add(s, myAlpha, myCutoff, myOrder, grid, PMGPU_EWALD_ALL, 0,
-                              0.0, &id),
+    check(pmgpu_force_pme_add(s, myAlpha, myCutoff, myOrder, grid, PMGPU_EWALD_ALL, 0, 0.0, &id),
           getIdNoAlias());
     return id;
   }
@@ -272,29 +406,263 @@ class PmeGpuForce : public PmgpuSystemForce {
   int myOrder, myGrid;
 };
 
-// Dihedral torsions (force/bonded/DihedralSystemForce.h) on the GPU.
+// NonbondedSimpleFull LennardJones / Coulomb (vacuum all pairs,
+// module/NonbondedSimpleFullForceModule.cpp) on the GPU; -blocksize is read
+// and ignored, as the device tiles its own way
+// (NonbondedSimpleFullSystemForce.h:93-99).
+class SimpleFullGpuForce : public PmgpuSystemForce {
+ public:
+  SimpleFullGpuForce(bool lj, bool coul) : myLJ(lj), myCoul(coul), myBlock(64) {}
+  virtual string getKeyword() const { return "NonbondedSimpleFullGPU"; }
+  virtual string getIdNoAlias() const {
+    return string(myLJ && myCoul ? "LennardJones Coulomb" : (myLJ ? "LennardJones" : "Coulomb")) +
+           " -algorithm " + getKeyword();
+  }
+  virtual void getParameters(vector<Parameter> &p) const {
+    p.push_back(Parameter("-blocksize", Value(myBlock, ConstraintValueType::Positive()), 64));
+  }
+
+ private:
+  virtual Force *doMake(const vector<Value> &values) const {
+    SimpleFullGpuForce *f = new SimpleFullGpuForce(myLJ, myCoul);
+    f->myBlock = values[0];
+    return f;
+  }
+  virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
+    int id = -1;
+    check(pmgpu_force_simplefull_add(s, myLJ ? 1 : 0, myCoul ? 1 : 0, &id), getIdNoAlias());
+    return id;
+  }
+  bool myLJ, myCoul;
+  int myBlock;
+};
+
+// The OBC GB chain (force/GB/GBBornRadii.cpp, GBPartialSum.cpp, GBForce.cpp,
+// GBACEForce.cpp) as NonbondedSimpleFull forces.  The device runs the
+// passes inside GBForce's (and GBACEForce's) evaluation, so GBBornRadii and
+// GBPartialSum only keep their places in the force list (they add no force
+// and no energy in the reference either); GBForce and GBACEForce add their
+// forces and energies (COULOMB).
+class GbGpuForce : public PmgpuSystemForce {
+ public:
+  explicit GbGpuForce(const string &keyword)
+      : myKeyword(keyword), mySolute(1.0), mySolvent(80.0), mySigma(2.26 / 418.4),
+        myRho(1.4), myBlock(64) {}
+  virtual string getKeyword() const { return "NonbondedSimpleFullGPU"; }
+  virtual string getIdNoAlias() const { return myKeyword + " -algorithm " + getKeyword(); }
+  virtual void getParameters(vector<Parameter> &p) const {
+    if (myKeyword == "GBForce") {
+      p.push_back(Parameter("-soluteDielec",
+                            Value(mySolute, ConstraintValueType::NoConstraints()), 1.0));
+      p.push_back(Parameter("-solventDielec",
+                            Value(mySolvent, ConstraintValueType::NoConstraints()), 80.0));
+    } else if (myKeyword == "GBACEForce") {
+      // GBACEForce::getParameters (force/GB/GBACEForce.cpp:224-230)
+      p.push_back(Parameter("-solvationparam",
+                            Value(mySigma, ConstraintValueType::NoConstraints()), 2.26 / 418.4));
+      p.push_back(Parameter("-watersphereradius",
+                            Value(myRho, ConstraintValueType::NoConstraints()), 1.4));
+    }
+    p.push_back(Parameter("-blocksize", Value(myBlock, ConstraintValueType::Positive()), 64));
+  }
+
+ private:
+  virtual Force *doMake(const vector<Value> &values) const {
+    GbGpuForce *f = new GbGpuForce(myKeyword);
+    size_t at = 0;
+    if (myKeyword == "GBForce") {
+      f->mySolute = values[at++];
+      f->mySolvent = values[at++];
+    } else if (myKeyword == "GBACEForce") {
+      f->mySigma = values[at++];
+      f->myRho = values[at++];
+    }
+    f->myBlock = values[at];
+    return f;
+  }
+  virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
+    int id = -1;
+    if (myKeyword == "GBForce")
+      check(pmgpu_force_gb_add(s, mySolute, mySolvent, &id), getIdNoAlias());
+    else if (myKeyword == "GBACEForce")
+      check(pmgpu_force_gbace_add(s, mySigma, myRho, &id), getIdNoAlias());
+    return id;
+  }
+  string myKeyword;
+  Real mySolute, mySolvent, mySigma, myRho;
+  int myBlock;
+};
+
+// Dihedral / Improper torsions (force/bonded/DihedralSystemForce.h,
+// ImproperSystemForce.h; MTorsionSystemForce) on the GPU.
 class TorsionGpuForce : public PmgpuSystemForce {
  public:
-  virtual string getKeyword() const { return "Dihedral"; }
-  virtual string getIdNoAlias() const { return "Dihedral -algorithm TorsionGPU"; }
+  explicit TorsionGpuForce(bool dihedral) : myDihedral(dihedral) {}
+  virtual string getKeyword() const { return "TorsionGPU"; }
+  virtual string getIdNoAlias() const {
+    return string(myDihedral ? "Dihedral" : "Improper") + " -algorithm TorsionGPU";
+  }
   virtual void getParameters(vector<Parameter> &) const {}
 
  private:
-  virtual Force *doMake(const vector<Value> &) const { return new TorsionGpuForce(); }
+  virtual Force *doMake(const vector<Value> &) const { return new TorsionGpuForce(myDihedral); }
   virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
     int id = -1;
-    check(pmgpu_force_torsion_add(s, 1, 0, &id), getIdNoAlias());
+    check(pmgpu_force_torsion_add(s, myDihedral ? 1 : 0, myDihedral ? 0 : 1, &id),
+          getIdNoAlias());
     return id;
   }
+  bool myDihedral;
+};
+
+// ------------------------------------------------------------ integrators
+// Leapfrog / LangevinLeapfrog with every step on the device.
+class DeviceIntegrator : public STSIntegrator {
+ public:
+  DeviceIntegrator(int kind, Real timestep, Real temperature, Real gamma, int seed,
+                   ForceGroup *fg)
+      : STSIntegrator(timestep, fg), myKind(kind), myTemperature(temperature),
+        myGamma(gamma), mySeed(seed), mySystem(0) {}
+
+  virtual void initialize(ProtoMolApp *app) {
+    STSIntegrator::initialize(app);
+    mySystem = systemFor(app->topology);
+    // every force of the group gets its device form; only those run
+    const vector<Force *> forces = myForcesToEvaluate->getForces();
+    vector<int> ids;
+    for (size_t k = 0; k < forces.size(); k++) {
+      PmgpuSystemForce *g = dynamic_cast<PmgpuSystemForce *>(forces[k]);
+      int id = -1;
+      if (g) {
+        id = g->attach(mySystem, app->topology);
+      } else {
+        const string kw = forces[k]->getKeyword();
+        if (equalNocase(kw, "Bond") || equalNocase(kw, "Angle"))
+          check(pmgpu_force_bonded_add(mySystem, equalNocase(kw, "Bond"), equalNocase(kw, "Angle"),
+                                       &id), kw);
+        else if (equalNocase(kw, "Dihedral") || equalNocase(kw, "Improper"))
+          check(pmgpu_force_torsion_add(mySystem, equalNocase(kw, "Dihedral"),
+                                        equalNocase(kw, "Improper"), &id), kw);
+        else
+          THROW(getIdNoAlias() + ": force '" + forces[k]->getId() +
+                "' has no device form (use a GPU algorithm)");
+      }
+      if (id >= 0) ids.push_back(id);
+    }
+    // forces attached to the system by other integrators stay off here
+    pmgpu_stats st;
+    for (int id = 0; pmgpu_force_stats(mySystem, id, &st) == PMGPU_OK; id++) {
+      bool mine = false;
+      for (size_t k = 0; k < ids.size(); k++) mine = mine || ids[k] == id;
+      check(pmgpu_force_set_enabled(mySystem, id, mine ? 1 : 0), getIdNoAlias());
+    }
+    myHostPos.clear();
+    myHostVel.clear();
+    // Integrator::initialize evaluates the initial forces (and energies)
+    upload();
+    double e[PMGPU_E_COUNT];
+    check(pmgpu_evaluate(mySystem, e, 0), getIdNoAlias());
+    download(e);
+  }
+
+  virtual long run(const long numTimesteps) {
+    if (numTimesteps < 1) return 0;
+    upload();
+    pmgpu_integrator it;
+    it.kind = myKind;
+    it.timestep_fs = getTimestep();
+    it.temperature = myTemperature;
+    it.gamma_ps = myGamma;
+    it.seed = (uint64_t)mySeed;
+    check(pmgpu_run(mySystem, &it, numTimesteps), getIdNoAlias());
+    double e[PMGPU_E_COUNT];
+    check(pmgpu_system_get_energies(mySystem, e, 0), getIdNoAlias());
+    download(e);
+    return numTimesteps;
+  }
+
+  virtual void getParameters(vector<Parameter> &parameters) const {
+    STSIntegrator::getParameters(parameters);
+    if (myKind == PMGPU_INT_LANGEVIN_LEAPFROG) {
+      // LangevinLeapfrogIntegrator::getParameters (integrator/base/
+      // LangevinLeapfrogIntegrator.cpp:74-85)
+      parameters.push_back(Parameter("temperature",
+                                     Value(myTemperature, ConstraintValueType::NotNegative())));
+      parameters.push_back(Parameter("gamma", Value(myGamma, ConstraintValueType::NotNegative())));
+      parameters.push_back(Parameter("seed", Value(mySeed, ConstraintValueType::NotNegative()),
+                                     1234));
+    }
+  }
+  virtual string getIdNoAlias() const {
+    return myKind == PMGPU_INT_LEAPFROG ? "LeapfrogGPU" : "LangevinLeapfrogGPU";
+  }
+
+ private:
+  virtual STSIntegrator *doMake(const vector<Value> &values, ForceGroup *fg) const {
+    if (myKind == PMGPU_INT_LEAPFROG) return new DeviceIntegrator(myKind, values[0], 0, 0, 0, fg);
+    return new DeviceIntegrator(myKind, values[0], values[1], values[2], values[3], fg);
+  }
+
+  // Positions and velocities go to the device only when the host changed
+  // them since the last download (a modifier, a restart, the first call).
+  void upload() {
+    const size_t n3 = 3 * app->positions.size();
+    const double *x = app->positions.c, *v = app->velocities.c;
+    if (myHostPos.size() != n3 || memcmp(&myHostPos[0], x, n3 * sizeof(double)) != 0)
+      check(pmgpu_system_set_positions(mySystem, x), getIdNoAlias());
+    if (myHostVel.size() != n3 || memcmp(&myHostVel[0], v, n3 * sizeof(double)) != 0)
+      check(pmgpu_system_set_velocities(mySystem, v), getIdNoAlias());
+  }
+  // The state at the end of a run() (or the initial evaluation) back in the
+  // app: positions, velocities, this integrator's forces and the energies.
+  void download(const double *e) {
+    const size_t n3 = 3 * app->positions.size();
+    check(pmgpu_system_get_positions(mySystem, app->positions.c), getIdNoAlias());
+    check(pmgpu_system_get_velocities(mySystem, app->velocities.c), getIdNoAlias());
+    check(pmgpu_system_get_forces(mySystem, myForces->c), getIdNoAlias());
+    myHostPos.assign(app->positions.c, app->positions.c + n3);
+    myHostVel.assign(app->velocities.c, app->velocities.c + n3);
+    app->energies.clear();
+    addEnergies(&app->energies, e, 0);
+  }
+
+  int myKind;
+  Real myTemperature, myGamma;
+  int mySeed;
+  pmgpu_system *mySystem;
+  vector<double> myHostPos, myHostVel;
 };
 
 }  // namespace
 
 void PmgpuForceModule::registerForces(ProtoMolApp *app) {
   ForceFactory &f = app->forceFactory;
-  f.registerExemplar(new CutoffGpuForce("LennardJones Coulomb", true, true));
-  f.registerExemplar(new CutoffGpuForce("LennardJones", true, false));
-  f.registerExemplar(new CutoffGpuForce("Coulomb", false, true));
+  // the switching-function combinations the reference registers for
+  // NonbondedCutoff (module/NonbondedCutoffForceModule.cpp:55-96), plus Cutoff
+  const SwitchSpec singles[] = {kC1, kC2, kCn, kCutoff};
+  for (int k = 0; k < 4; k++) {
+    f.registerExemplar(new CutoffGpuForce(true, false, singles[k], 0));
+    f.registerExemplar(new CutoffGpuForce(false, true, singles[k], 0));
+  }
+  const SwitchSpec pairs[][2] = {{kC2, kC1}, {kC2, kC2}, {kC2, kCn}, {kCn, kCn}, {kCn, kC2},
+                                 {kCutoff, kCutoff}, {kC2, kCutoff}};
+  for (int k = 0; k < 7; k++)
+    f.registerExemplar(new CutoffGpuForce(true, true, pairs[k][0], &pairs[k][1]));
   f.registerExemplar(new PmeGpuForce());
-  f.registerExemplar(new TorsionGpuForce());
+  f.registerExemplar(new SimpleFullGpuForce(true, false));
+  f.registerExemplar(new SimpleFullGpuForce(false, true));
+  f.registerExemplar(new SimpleFullGpuForce(true, true));
+  f.registerExemplar(new GbGpuForce("GBBornRadii"));
+  f.registerExemplar(new GbGpuForce("GBPartialSum"));
+  f.registerExemplar(new GbGpuForce("GBForce"));
+  f.registerExemplar(new GbGpuForce("GBACEForce"));
+  f.registerExemplar(new TorsionGpuForce(true));
+  f.registerExemplar(new TorsionGpuForce(false));
+}
+
+void PmgpuForceModule::init(ProtoMolApp *app) {
+  app->integratorFactory.registerExemplar(
+      new DeviceIntegrator(PMGPU_INT_LEAPFROG, 1.0, 0, 0, 0, 0));
+  app->integratorFactory.registerExemplar(
+      new DeviceIntegrator(PMGPU_INT_LANGEVIN_LEAPFROG, 1.0, 300.0, 5.0, 1234, 0));
 }

@@ -335,16 +335,19 @@ def write_protomol_inputs(sysm: MolecularSystem, directory: str, stem: str,
                           forces: list[str], integrator: str = "Leapfrog",
                           timestep: float = 0.5, numsteps: int = 0,
                           cellsize: float | None = None, extra: str = "",
-                          outputs: bool = True, integrator_params: str = "") -> str:
+                          outputs: bool = True, integrator_params: str = "",
+                          outputfreq: int | None = None) -> str:
     """Write PSF/PAR/XYZ inputs and a .conf evaluating the given force lines
-    with the given integrator; returns the conf path."""
+    with the given integrator; returns the conf path.  outputfreq defaults
+    to numsteps (one output at the end)."""
     os.makedirs(directory, exist_ok=True)
     names = [sysm.type_names[t] for t in sysm.type]
     write_psf(sysm, os.path.join(directory, stem + ".psf"))
     write_par(sysm, os.path.join(directory, stem + ".par"))
     write_xyz(sysm.pos, names, os.path.join(directory, stem + ".pos.xyz"))
     write_xyz(sysm.vel, names, os.path.join(directory, stem + ".vel.xyz"))
-    lines = [f"firststep 0", f"numsteps {numsteps}", f"outputfreq {max(1, numsteps)}",
+    ofreq = outputfreq if outputfreq else max(1, numsteps)
+    lines = [f"firststep 0", f"numsteps {numsteps}", f"outputfreq {ofreq}",
              "angularMomentum 0", "comMotion 0", "exclude scaled1-4", "seed 1234",
              f"posfile {stem}.pos.xyz", f"velfile {stem}.vel.xyz", f"psffile {stem}.psf",
              f"parfile {stem}.par", "temperature 300"]

@@ -8,7 +8,7 @@ line, as written by oracle/_ref/pm_forcedump.  Inputs are the reference's own
 test systems (its test/tests/*.conf data) and seeded synthetic systems from
 protomol_b200.systems written out as PSF/PAR/XYZ.
 
-    python tests/golden/make_golden.py            # needs the reference tree
+    PROTOMOL_REF=<ProtoMol checkout> python tests/golden/make_golden.py [part]
 """
 from __future__ import annotations
 
@@ -26,7 +26,13 @@ sys.path.insert(0, ROOT)
 from oracle import refdump  # noqa: E402
 from protomol_b200 import systems  # noqa: E402
 
-REF_TESTS = "/root/reference/test/tests"
+def _ref_tests() -> str:
+    """The reference's test inputs: $PROTOMOL_REF/test/tests, PROTOMOL_REF
+    being the ProtoMol checkout (required; no default)."""
+    ref = os.environ.get("PROTOMOL_REF")
+    if not ref:
+        raise SystemExit("set PROTOMOL_REF to the ProtoMol checkout")
+    return os.path.join(ref, "test", "tests")
 
 
 def save(name: str, d: dict, extra: dict | None = None) -> None:
@@ -55,8 +61,8 @@ def save(name: str, d: dict, extra: dict | None = None) -> None:
 def reference_conf(conf: str, forces: list[str], steps: int = 0) -> dict:
     tmp = tempfile.mkdtemp()
     try:
-        os.symlink(os.path.join(REF_TESTS, "data"), os.path.join(tmp, "data"))
-        shutil.copy(os.path.join(REF_TESTS, conf), tmp)
+        os.symlink(os.path.join(_ref_tests(), "data"), os.path.join(tmp, "data"))
+        shutil.copy(os.path.join(_ref_tests(), conf), tmp)
         os.makedirs(os.path.join(tmp, "output"))
         return refdump.run(conf, os.path.join(tmp, "dump.txt"), forces, steps=steps, cwd=tmp)
     finally:
@@ -95,6 +101,21 @@ def main(which: str = "all") -> None:
     if which == "torsions":
         torsions()
         return
+    if which == "gb":
+        gb = ["GBBornRadii -algorithm NonbondedSimpleFull",
+              "GBPartialSum -algorithm NonbondedSimpleFull",
+              "GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.3",
+              "LennardJones -algorithm NonbondedSimpleFull",
+              "Coulomb -algorithm NonbondedSimpleFull",
+              "GBACEForce -algorithm NonbondedSimpleFull"]
+        save("fip35_gb", reference_conf("www-fip35_FFAMBER_GB_LL.conf", gb))
+        save("alanylalanine_gb", reference_conf("alanylalanine_FFAMBER_GB_LL.conf", gb))
+        return
+    if which == "leapfrog100":
+        md = ["LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction C2 -switchon 7 "
+              "-cutoff 8 -switchingFunction C2 -switchon 7 -cutoff 8 -cutoff 8", "Bond", "Angle"]
+        leapfrog100(systems.tip3p_box(216, 18.6, seed=1, lattice=6), md)
+        return
     torsions()
     # 1. The reference's periodic water test (423 atoms, 28 A box).
     d = reference_conf("water_CHARMM_PERIODIC_L.conf", [
@@ -113,7 +134,8 @@ def main(which: str = "all") -> None:
           "GBPartialSum -algorithm NonbondedSimpleFull",
           "GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.3",
           "LennardJones -algorithm NonbondedSimpleFull",
-          "Coulomb -algorithm NonbondedSimpleFull"]
+          "Coulomb -algorithm NonbondedSimpleFull",
+          "GBACEForce -algorithm NonbondedSimpleFull"]
     save("fip35_gb", reference_conf("www-fip35_FFAMBER_GB_LL.conf", gb))
     save("alanylalanine_gb", reference_conf("alanylalanine_FFAMBER_GB_LL.conf", gb))
     # 3. Synthetic 648-atom TIP3P box (216 waters, 18.6 A): the small plain
@@ -143,6 +165,26 @@ def main(which: str = "all") -> None:
         save(f"c1_{tag}20", d0, {"positions_20": d1["positions"],
                                  "velocities_20": d1["velocities"],
                                  "timestep": np.array(dt), "md_forces": np.array(md)})
+    leapfrog100(c1, md)
+
+
+def leapfrog100(c1, md) -> None:
+    """The small plain configuration as specified: 100 leapfrog steps of
+    0.5 fs through the reference's own integrator, with the energies of
+    every MD force term at EVERY step (pm_forcedump --steps k for k = 1..100,
+    full precision) and the state at steps 25, 50, 75 and 100."""
+    d0 = synthetic(c1, "c1", md, 8.0, 0, md, "Leapfrog", 0.5, "")
+    per_step = np.zeros((101, 4))
+    extra = {"timestep": np.array(0.5), "md_forces": np.array(md)}
+    for k in range(0, 101):
+        d = d0 if k == 0 else synthetic(c1, "c1", md, 8.0, k, md, "Leapfrog", 0.5, "")
+        e = sum(f["energies"] for f in d["forces"])
+        per_step[k] = e[[0, 1, 2, 3]]  # COULOMB, LENNARDJONES, BOND, ANGLE
+        if k and k % 25 == 0:
+            extra[f"positions_{k}"] = d["positions"]
+            extra[f"velocities_{k}"] = d["velocities"]
+    extra["energies_per_step"] = per_step
+    save("c1_leapfrog100", d0, extra)
 
 
 if __name__ == "__main__":

@@ -401,3 +401,54 @@ def test_polymer_leapfrog_force_only_steps_vs_oracle(ctx):
         v = oracle.kick(sm.mass, f, 0.5 * h, v)
     assert np.abs(x_gpu - x).max() <= 1e-6, np.abs(x_gpu - x).max()
     assert np.abs(v_gpu - v).max() / np.abs(v).max() <= 1e-5
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", RMS_MIXED), ("double", RMS_DOUBLE)])
+@pytest.mark.parametrize("name", ["fip35_gb", "alanylalanine_gb"])
+def test_gbace_vs_reference(ctx, name, precision, tol):
+    """GBACEForce (ACE nonpolar term on the OBC Born radii) alone and
+    evaluated together with GBForce (one shared Born-radius chain) against
+    the reference's own forces and energies."""
+    z = F.load(name)
+    topo = F.topology(z)
+    k_ace = [k for k, d in enumerate(z["defs"]) if str(d).startswith("GBACEForce")][0]
+    gs = GpuSystem(ctx, topo, precision)
+    ff = ForceFactory(gs)
+    ace = ff.make("GBACEForce -algorithm NonbondedSimpleFull")
+    f, e = _eval(ace, topo)
+    ref = F.forces(z, k_ace)
+    assert F.rms_rel(f, ref) <= tol, F.rms_rel(f, ref)
+    assert _energy_ok(e[0], F.energies(z, k_ace)[0], floor=1e-6)
+    gb = ff.make("GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.3")
+    en, _ = gs.evaluate()
+    both = F.forces(z, 2) + ref
+    assert F.rms_rel(gs.forces_total(), both) <= tol
+    assert _energy_ok(en[0], F.energies(z, 2)[0] + F.energies(z, k_ace)[0])
+    fo = gs.evaluate_forces()  # the force-only form of the MD steps
+    assert F.rms_rel(fo, both) <= tol
+    gs.close()
+
+
+def test_gbace_polymer_vs_oracle(ctx):
+    """GBACE on a 700-atom heteropolymer (mixed precision) against the FP64
+    oracle, alone and beside GBForce."""
+    import oracle
+    from protomol_b200 import systems
+    sm = systems.gb_polymer(700, seed=9)
+    s = oracle.System(pos=sm.pos, charge=sm.charge, type=sm.type, molecule=sm.molecule,
+                      lj=sm.lj, excl=sm.exclusions, periodic=False, box=sm.box, mass=sm.mass,
+                      water=sm.water, gb_vdwr=sm.gb_vdwr, gb_scale=sm.gb_scale,
+                      gb_offset=sm.gb_offset, gb_obc=sm.gb_obc)
+    fa, ea = oracle.gbace_force(s)
+    fg, eg, _ = oracle.gb_force(s, 1.0, 78.5)
+    gs = GpuSystem(ctx, sm, "mixed")
+    ff = ForceFactory(gs)
+    ace = ff.make("GBACEForce -algorithm NonbondedSimpleFull")
+    f, e = _eval(ace, sm)
+    assert F.rms_rel(f, fa) <= RMS_MIXED, F.rms_rel(f, fa)
+    assert _energy_ok(e[0], ea, floor=1e-6)
+    ff.make("GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.5")
+    assert F.rms_rel(gs.evaluate_forces(), fa + fg) <= RMS_MIXED
+    en, _ = gs.evaluate()
+    assert _energy_ok(en[0], ea + eg)
+    gs.close()

@@ -137,3 +137,67 @@ def test_torsion_oracle_matches_reference(name):
     ref_f = F.forces(z, 0)
     assert np.abs(f - ref_f).max() <= 1e-10 * max(1.0, np.abs(ref_f).max())
     assert abs(e - F.energies(z, 0)[4]) <= 1e-10 * max(1.0, abs(e))
+
+
+@pytest.mark.parametrize("name", ["water423", "c1_tip3p648"])
+def test_bond_and_angle_oracle_match_reference(name):
+    """BondSystemForce / AngleSystemForce (with Urey-Bradley) restated in
+    the oracle against the reference's own forces, energies and virial."""
+    z = F.load(name)
+    s = F.oracle_system(z)
+    t = F.topology(z)
+    for kw, args, slot in (("Bond", (t.bonds, t.bond_params, None, None), 2),
+                           ("Angle", (None, None, t.angles, t.angle_params), 3)):
+        k = [i for i, d in enumerate(z["defs"]) if str(d) == kw][0]
+        f, e, v = oracle.bonded_force(s, *args)
+        ref_e = F.energies(z, k)
+        assert np.abs(f - F.forces(z, k)).max() <= 1e-12, kw
+        assert e[kw.lower()] == pytest.approx(ref_e[slot], rel=1e-13, abs=1e-12), kw
+        assert np.abs(v.reshape(-1) - ref_e[7:16]).max() <= 1e-10, kw
+
+
+def test_leapfrog100_oracle_trajectory_matches_reference():
+    """The small plain configuration (648-atom TIP3P box, LJ + Coulomb C2
+    7 -> 8 A, bonds, angles, leapfrog 0.5 fs) integrated on the host with the
+    oracle's forces (LeapfrogIntegrator.cpp:33-104: half kick, drift, forces,
+    half kick) reproduces the reference's own 100-step run: the energies of
+    every step and the state at steps 25, 50, 75 and 100."""
+    z = F.load("c1_leapfrog100")
+    t = F.topology(z)
+    s = F.oracle_system(z)
+    sw = oracle.Switch("C2", 8.0, 7.0)
+
+    def forces(x):
+        s2 = s.with_positions(x)
+        f, e, _ = oracle.cutoff_force(s2, 8.0, 8.0, [("LennardJones", sw), ("Coulomb", sw)])
+        fb, eb, _ = oracle.bonded_force(s2, t.bonds, t.bond_params, t.angles, t.angle_params)
+        return f + fb, np.array([e["coulomb"], e["lj"], eb["bond"], eb["angle"]])
+
+    h = float(z["timestep"]) * oracle.INV_TIMEFACTOR
+    x, v = t.pos.copy(), t.vel.copy()
+    f, e = forces(x)
+    ref = z["energies_per_step"]
+    assert np.abs(e - ref[0]).max() <= 1e-9
+    for k in range(1, 101):
+        v = oracle.kick(t.mass, f, 0.5 * h, v)
+        x = oracle.drift(v, h, x)
+        f, e = forces(x)
+        v = oracle.kick(t.mass, f, 0.5 * h, v)
+        assert np.abs(e - ref[k]).max() <= 1e-8 * max(1.0, np.abs(ref[k]).max()), k
+        if k % 25 == 0:
+            assert np.abs(x - z[f"positions_{k}"].reshape(-1, 3)).max() <= 1e-10, k
+            assert np.abs(v - z[f"velocities_{k}"].reshape(-1, 3)).max() <= 1e-9, k
+
+
+@pytest.mark.parametrize("name", ["fip35_gb", "alanylalanine_gb"])
+def test_gbace_oracle_matches_reference(name):
+    """GBACEForce (the ACE nonpolar term on the GB Born radii, default
+    -solvationparam and -watersphereradius) restated in the oracle against
+    the reference's own forces and energy on its GB test systems."""
+    z = F.load(name)
+    s = F.oracle_system(z)
+    k = [i for i, d in enumerate(z["defs"]) if str(d).startswith("GBACEForce")][0]
+    f, e = oracle.gbace_force(s)
+    ref_f = F.forces(z, k)
+    assert np.abs(f - ref_f).max() <= 1e-12 * max(1.0, np.abs(ref_f).max())
+    assert e == pytest.approx(F.energies(z, k)[0], rel=1e-13)

@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 SOLUTE, SOLVENT = 1.0, 78.3
 
 
-def _noalloc(lib, topo, pos, precision):
+def _noalloc(lib, topo, pos, precision, with_water=True):
     import torch
     dev = torch.device("cuda", 0)
     n = pos.shape[0]
@@ -24,14 +24,15 @@ def _noalloc(lib, topo, pos, precision):
          for k, v in (("pos", pos.reshape(-1)), ("charge", topo.charge),
                       ("vdwr", topo.gb_vdwr), ("scale", topo.gb_scale),
                       ("offset", topo.gb_offset))}
-    water = torch.as_tensor(topo.water.astype(np.int32), device=dev)
+    water = torch.as_tensor(topo.water.astype(np.int32), device=dev) if with_water else None
     forces = torch.full((3 * n,), np.nan, dtype=torch.float64, device=dev)
     energy = torch.full((1,), np.nan, dtype=torch.float64, device=dev)
     obc = (C.c_double * 3)(*topo.gb_obc)
     stream = torch.cuda.current_stream(dev)
     rc = lib.pmgpu_gb_forces_noalloc(
         n, t["pos"].data_ptr(), t["charge"].data_ptr(), t["vdwr"].data_ptr(),
-        t["scale"].data_ptr(), t["offset"].data_ptr(), water.data_ptr(), obc,
+        t["scale"].data_ptr(), t["offset"].data_ptr(),
+        water.data_ptr() if water is not None else None, obc,
         SOLUTE, SOLVENT, precision, forces.data_ptr(), energy.data_ptr(),
         stream.cuda_stream)
     L.check(rc)
@@ -62,6 +63,32 @@ def test_noalloc_matches_allocating_path(ctx, precision, name):
         f, e = _noalloc(lib, topo, pos, name)
         assert np.all(np.isfinite(f))
         assert F.rms_rel(f, f_ref) <= 1e-12, F.rms_rel(f, f_ref)
+        assert abs(e - e_ref) <= 1e-9 * max(1.0, abs(e_ref)), (e, e_ref)
+    gs.close()
+
+
+@pytest.mark.parametrize("precision,name", [("mixed", L.PREC_MIXED), ("double", L.PREC_DOUBLE)])
+@pytest.mark.parametrize("n", [1, 33, 65, L.GB_STATIC_MAX_ATOMS])
+def test_noalloc_small_ragged_and_limit_sizes(ctx, n, precision, name):
+    """Heteropolymers below one 32-atom tile, with a ragged last tile, and
+    at the static limit (where the carved scratch ends exactly at the end of
+    the array), with no water array (every atom solute), twice in a row."""
+    from protomol_b200 import systems
+    lib = L.load()
+    sm = systems.gb_polymer(n, seed=11)
+    sm.water = np.zeros(n, np.int32)
+    gs = GpuSystem(ctx, sm, precision)
+    gb = ForceFactory(gs).make(
+        f"GBForce -algorithm NonbondedSimpleFull -soluteDielec {SOLUTE} -solventDielec {SOLVENT}")
+    rng = np.random.default_rng(n)
+    for pos in (sm.pos, sm.pos + rng.normal(0.0, 0.05, sm.pos.shape)):
+        f_ref, e_ref = _allocating(gb, pos)
+        f, e = _noalloc(lib, sm, pos, name, with_water=False)
+        assert np.all(np.isfinite(f))
+        if np.abs(f_ref).max() > 0:
+            assert F.rms_rel(f, f_ref) <= 1e-12, F.rms_rel(f, f_ref)
+        else:
+            assert np.abs(f).max() == 0.0
         assert abs(e - e_ref) <= 1e-9 * max(1.0, abs(e_ref)), (e, e_ref)
     gs.close()
 
