@@ -129,16 +129,19 @@ class ClockSampler:
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "protomol")
 
 
-def run_reference(numsteps: int) -> dict:
+def run_reference_system(sysm, forces, numsteps: int, integrator: str = "Leapfrog",
+                         timestep: float = DT_FS, params: str = "", extra: str = "",
+                         cellsize: float = RC / 2) -> dict:
     """Runs ProtoMol's own CPU path (the reference built from its sources by
-    oracle/ref.mk) on the same system and returns its ns/day."""
+    oracle/ref.mk, one process, one core) on a system and returns its run
+    time (ProtoMol's own "run:" timer, set-up excluded) and ns/day."""
     from protomol_b200 import systems
-    sysm = build_system(SEED)
     tmp = tempfile.mkdtemp()
     try:
-        conf = systems.write_protomol_inputs(sysm, tmp, "bench", reference_force_lines(),
-                                             integrator="Leapfrog", timestep=DT_FS,
-                                             numsteps=numsteps, cellsize=RC / 2, outputs=False)
+        conf = systems.write_protomol_inputs(sysm, tmp, "bench", forces, integrator=integrator,
+                                             timestep=timestep, numsteps=numsteps,
+                                             cellsize=cellsize, outputs=False,
+                                             integrator_params=params, extra=extra)
         t0 = time.perf_counter()
         out = subprocess.run([REF_BIN, conf], cwd=tmp, capture_output=True, text=True)
         wall = time.perf_counter() - t0
@@ -146,10 +149,43 @@ def run_reference(numsteps: int) -> dict:
             raise RuntimeError(out.stdout[-2000:] + out.stderr[-2000:])
         m = re.search(r"run:\s*([0-9.eE+-]+)\[s\]", out.stdout + out.stderr)
         run_s = float(m.group(1)) if m else wall
-        return {"ns_per_day": numsteps * DT_FS * 1e-6 * 86400.0 / run_s, "run_s": run_s,
-                "wall_s": wall, "steps": numsteps}
+        return {"ns_per_day": numsteps * timestep * 1e-6 * 86400.0 / run_s, "run_s": run_s,
+                "wall_s": wall, "steps": numsteps, "s_per_step": run_s / numsteps}
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+def run_reference(numsteps: int) -> dict:
+    """The reference on the benched 23,550-atom box (FullEwald at the same
+    alpha and real-space cutoff: the reference has no PME)."""
+    return run_reference_system(build_system(SEED), reference_force_lines(), numsteps)
+
+
+def reference_water_lines() -> list[str]:
+    """The reference's force set for a TIP3P box of the batched / served
+    forms: LJ C2 8 -> 9 A, FullEwald at alpha 0.35 and Rc 9 A (images of
+    small boxes included by the reference's lattice sum), bonds, angles."""
+    acc = math.exp(-(ALPHA * RC) ** 2)
+    return ["Bond", "Angle",
+            f"LennardJones -algorithm NonbondedCutoff -switchingFunction C2 -switchon "
+            f"{LJ_SWITCHON} -cutoff {RC}",
+            f"Coulomb -algorithm FullEwald -real -reciprocal -correction -alpha {ALPHA} "
+            f"-accuracy {acc:.17g}"]
+
+
+def per_core_reference(boxes, steps: int = 2, cores: int | None = None) -> dict:
+    """One reference process per host core on distinct boxes at once (the
+    reference is single-threaded): each box's seconds per MD step."""
+    from concurrent.futures import ThreadPoolExecutor
+    cores = cores or os.cpu_count() or 1
+
+    def one(sysm):
+        r = run_reference_system(sysm, reference_water_lines(), steps,
+                                 cellsize=min(RC / 2, sysm.box[0] / 3))
+        return r["s_per_step"]
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        t = list(ex.map(one, boxes))
+    return {"s_per_step": t, "cores": cores}
 
 
 # --------------------------------------------------------------- GPU arm
@@ -273,6 +309,24 @@ def ensemble_line(args, ctx, world: int, rank: int, dist=None) -> dict:
                      "atom_steps_per_s": atoms * seg * args.steps / wall,
                      "segments_per_member": args.steps}
     ens.close()
+    cpu = None
+    if rank == 0 and world == 1 and os.path.exists(REF_BIN):
+        try:
+            # 16 boxes spread over the size range, one reference process per core
+            by_size = sorted(reqs, key=lambda r: r.n_waters)
+            sample = by_size[::max(1, len(by_size) // 16)][:16]
+            pc = per_core_reference([r.prepare().system for r in sample], steps=2)
+            mean_t = float(np.mean(pc["s_per_step"]))
+            t_ens = mean_t * len(reqs) / pc["cores"]  # every core busy with its share
+            cpu = {"value": len(reqs) * 1e-6 * 86400.0 / t_ens, "unit": "ns/day",
+                   "cores": pc["cores"], "kind": "reference",
+                   "sample": f"{len(sample)} of the {len(reqs)} boxes (spread over the size "
+                             f"range), 2 MD steps each through ProtoMol's own Leapfrog with "
+                             f"FullEwald (alpha 0.35, Rc 9 A) + LJ C2 + bonds/angles, one "
+                             f"process per host core; the ensemble step is the sample's mean "
+                             f"step time x {len(reqs)} boxes / {pc['cores']} cores"}
+        except Exception as ex:  # reported, never fatal
+            cpu = {"value": None, "error": str(ex)[:200]}
     workload = (f"batched ensemble: {args.requests} resident TIP3P boxes of 100-1,000 waters "
                 f"(log-uniform), 0.0334 waters/A^3, {seg}-step leapfrog segments (inner steps "
                 f"as CUDA graphs), PME order 4 spacing <= 1 A, rc 9 A, LJ C2 8->9 A")
@@ -282,7 +336,8 @@ def ensemble_line(args, ctx, world: int, rank: int, dist=None) -> dict:
             "scaling": "strong", "data": "synthetic",
             "config": {"workload": workload, "partition": f"boxes over {world} GPU(s)"},
             "batched": out["batched"], "plain": out["plain"],
-            "batched_over_plain": out["batched"]["ns_per_day"] / out["plain"]["ns_per_day"]}
+            "batched_over_plain": out["batched"]["ns_per_day"] / out["plain"]["ns_per_day"],
+            "cpu_baseline": cpu}
 
 
 def served_line(args, ctx, world: int, rank: int, dist=None) -> dict:
@@ -342,6 +397,25 @@ def gb_force_lines():
             "GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.5",
             "LennardJones -algorithm NonbondedSimpleFull",
             "Coulomb -algorithm NonbondedSimpleFull", "Bond", "Angle", "Dihedral"]
+
+
+def gb_reference_baseline(steps: int = 2) -> dict:
+    """The reference binary on the 2,000-atom polymer with its own GB
+    (doGBSAObc 2), LJ and Coulomb all pairs, bonds, angles, dihedrals and
+    LangevinLeapfrog, one core.  ProtoMol's PSF/PAR reader takes each
+    type's GB radius from its PAR Rmin/2 (topology/BuildTopology.cpp:608),
+    so the reference's polymer carries those radii; the work per step (the
+    O(N^2) passes) is the same as with the benched radii."""
+    from protomol_b200 import systems
+    sysm = systems.gb_polymer(GB_ATOMS, GB_SEED)
+    sysm.gb_vdwr = sysm.rmin2[sysm.type].copy()
+    r = run_reference_system(sysm, gb_force_lines(), steps, integrator="LangevinLeapfrog",
+                             params="temperature 300 gamma 5 seed 1234", extra="doGBSAObc 2",
+                             cellsize=5.0)
+    return {"value": r["ns_per_day"], "unit": "ns/day", "cores": 1, "kind": "reference",
+            "sample": f"{steps} LangevinLeapfrog steps of the 2,000-atom polymer through "
+                      f"ProtoMol's own GB + LJ + Coulomb all pairs + bonded forces, 1 core "
+                      f"(its GB radii are the PAR Rmin/2)"}
 
 
 def gb_cpu_baseline(sysm, evals: int = 3) -> dict:
@@ -426,7 +500,11 @@ def gb_line(args, ctx, world: int, rank: int, dist=None) -> dict:
             "gpu_launches": launches}
     if world == 1:
         try:
-            line["cpu_baseline"] = gb_cpu_baseline(sysm)
+            if os.path.exists(REF_BIN):
+                line["cpu_baseline"] = gb_reference_baseline()
+                line["cpu_baseline"]["restatement"] = gb_cpu_baseline(sysm)
+            else:
+                line["cpu_baseline"] = gb_cpu_baseline(sysm)
         except Exception as ex:  # reported, never fatal
             line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
     return line
@@ -456,7 +534,8 @@ def run_forms(args, ctx, world: int, rank: int, dist=None) -> dict:
         if mode == "batched":
             out[mode] = {"value": r["value"], "unit": "ns/day", "workload": r["config"]["workload"],
                          "plain_ns_per_day": r["plain"]["ns_per_day"],
-                         "batched_over_plain": r["batched_over_plain"]}
+                         "batched_over_plain": r["batched_over_plain"],
+                         "cpu_baseline": r.get("cpu_baseline")}
         elif mode == "served":
             sv = r["served"]
             out[mode] = {"value": r["value"], "unit": "ns/day", "workload": r["config"]["workload"],

@@ -153,7 +153,8 @@ int pmgpu_abi_version(void);
 int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *topo,
                         int precision, pmgpu_system **out);
 int pmgpu_system_destroy(pmgpu_system *sys);
-/* Host <-> device copies of Vector3DBlock-layout arrays (3n doubles). */
+/* Host <-> device copies of Vector3DBlock-layout arrays (3n doubles).
+ * Positions with a non-finite coordinate are refused with PMGPU_ERR_NAN. */
 int pmgpu_system_set_positions(pmgpu_system *sys, const double *pos);
 int pmgpu_system_get_positions(pmgpu_system *sys, double *pos);
 int pmgpu_system_set_velocities(pmgpu_system *sys, const double *vel);
@@ -364,6 +365,13 @@ int pmgpu_kernel_count(pmgpu_system *sys, long long *count);
  * on the resident positions: cell_xyz gets 3n ints, dims 3 ints. */
 int pmgpu_debug_cell_assign(pmgpu_system *sys, double cellsize,
                             int *cell_xyz, int *dims);
+/* Fixes the pair lists' capacity (tiles per list row) of the system's
+ * cutoff forces, for testing the growth path: a build that needs more
+ * flags the overflow internally, the capacity is grown to what the largest
+ * row needed and the evaluation or MD segment is repeated from its start,
+ * so results equal those of a list that never overflowed.  No counterpart
+ * in the reference (its cell lists have no capacity). */
+int pmgpu_debug_set_list_capacity(pmgpu_system *sys, int tiles_per_row);
 /* The unordered pair set (i < j, original indices) the cutoff force
  * force_id evaluated on its last evaluation: pairs gets 2 ints per pair,
  * up to cap pairs; *count gets the total. */

@@ -39,7 +39,7 @@ EXPORTED = [
     "pmgpu_debug_pair_set", "pmgpu_profile_enable", "pmgpu_profile_read",
     "pmgpu_kernel_count", "pmgpu_gb_forces_noalloc", "pmgpu_run_async", "pmgpu_run_query",
     "pmgpu_run_wait", "pmgpu_mem_info", "pmgpu_footprint_estimate", "pmgpu_force_torsion_add",
-    "pmgpu_fp32_peak", "pmgpu_force_gbace_add",
+    "pmgpu_fp32_peak", "pmgpu_force_gbace_add", "pmgpu_debug_set_list_capacity",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -125,6 +125,7 @@ def load() -> C.CDLL:
     lib.pmgpu_force_stats.argtypes = [vp, i32, C.POINTER(Stats)]
     lib.pmgpu_debug_cell_assign.argtypes = [vp, dbl, vp, vp]
     lib.pmgpu_debug_pair_set.argtypes = [vp, i32, vp, C.c_longlong, C.POINTER(C.c_longlong)]
+    lib.pmgpu_debug_set_list_capacity.argtypes = [vp, i32]
     lib.pmgpu_profile_enable.argtypes = [vp, i32]
     lib.pmgpu_profile_read.argtypes = [vp, vp, vp, i32]
     lib.pmgpu_kernel_count.argtypes = [vp, C.POINTER(C.c_longlong)]

@@ -545,16 +545,21 @@ static int read_results(System *s, int only, double *energies, double *virial, i
   if (st) {
     PM_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
     if (st & ST_LIST_OVERFLOW) {
-      // Grow every list (fresh build next time); this result is incomplete
-      // and no output is touched.
+      // Grow every list to at least its largest row's need (fresh build
+      // next time); this result is incomplete and no output is touched.
       for (auto &nl : s->lists) {
-        int cap = nl.cap * 2;
+        int rb[3] = {0, 0, 0};
+        PM_CUDA(cudaMemcpyAsync(rb, nl.d_rebuild, sizeof(rb), cudaMemcpyDeviceToHost, s->stream));
+        PM_CUDA(cudaStreamSynchronize(s->stream));
+        const int need = rb[2] + rb[2] / 4 + 32;
+        const int cap = (std::max(nl.cap * 2, need) + 31) & ~31;
         nb_list_free(s, &nl);
         nl.cap = cap;
+        nl.cap_set = 0;
         PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
         s->graph_version++;  // captured graphs hold the old list buffers
       }
-      return fail(PMGPU_ERR_OVERFLOW, "neighbour list capacity exceeded; capacity doubled");
+      return fail(PMGPU_ERR_OVERFLOW, "neighbour list capacity exceeded; capacity grown");
     }
     if (st & ST_NONFINITE) return fail(PMGPU_ERR_NAN, "non-finite position or force");
     if (st & ST_CELL_OVERFLOW)
@@ -677,6 +682,12 @@ int pmgpu_context_create(int device, pmgpu_context **out) {
 }
 
 int pmgpu_context_destroy(pmgpu_context *ctx) {
+  if (!ctx) return PMGPU_OK;
+  cudaSetDevice(ctx->device);
+  for (auto &p : ctx->fft_free) {
+    cufftDestroy(p.r2c);
+    cufftDestroy(p.c2r);
+  }
   delete ctx;
   return PMGPU_OK;
 }
@@ -865,6 +876,10 @@ static int copy_out(System *s, double *dst, const double *src) {
 int pmgpu_system_set_positions(pmgpu_system *h, const double *pos) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
+  if (pos)
+    for (size_t k = 0; k < 3 * (size_t)s->n; k++)
+      if (!std::isfinite(pos[k]))
+        return fail(PMGPU_ERR_NAN, "non-finite position of atom " + std::to_string(k / 3));
   PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   PM_CHECK(copy_in(s, s->d_pos, pos));
@@ -1532,6 +1547,23 @@ int pmgpu_debug_cell_assign(pmgpu_system *h, double cellsize, int *cell_xyz, int
   PM_CHECK(run_finish(s));
   PM_CUDA(cudaSetDevice(s->device));
   return nb_debug_cells(s, cellsize, cell_xyz, dims);
+}
+
+int pmgpu_debug_set_list_capacity(pmgpu_system *h, int tiles_per_row) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  if (tiles_per_row < 1) return fail(PMGPU_ERR_ARG, "tiles_per_row must be >= 1");
+  System *s = sysp(h);
+  PM_CHECK(run_finish(s));
+  PM_CUDA(cudaSetDevice(s->device));
+  for (auto &nl : s->lists) {
+    nb_list_free(s, &nl);
+    nl.cap = 0;
+    nl.cap_set = tiles_per_row;
+    PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
+  }
+  s->graph_version++;
+  s->forces_valid = 0;
+  return PMGPU_OK;
 }
 
 int pmgpu_debug_pair_set(pmgpu_system *h, int id, int *pairs, long long cap,

@@ -375,7 +375,7 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
 // ones.  Tiles are appended in a fixed order (range, cluster index), so
 // the list is deterministic.
 __global__ void __launch_bounds__(kBuildWarps * 32, 3)
-k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__restrict__ sorted,
+k_build_tiles(TileBuildArgs a, int *__restrict__ rebuild, const int *__restrict__ sorted,
               const int *__restrict__ start, const float4 *__restrict__ xhi,
               const int *__restrict__ mol_s, const float4 *__restrict__ bb,
               uint4 *__restrict__ tiles, int *__restrict__ tile_count,
@@ -652,7 +652,10 @@ k_build_tiles(TileBuildArgs a, const int *__restrict__ rebuild, const int *__res
   }
   if (lane == 0) {
     if (count > a.cap) {
+      // the row keeps its first cap tiles; the host grows the capacity to
+      // at least the largest row's need and repeats the work
       atomicOr(status, ST_LIST_OVERFLOW);
+      atomicMax(rebuild + 2, count);
       count = a.cap;
     }
     tile_count[rw] = count;
@@ -730,6 +733,7 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   cap = std::min(cap, std::max(32, nl->ns_max / 4 * 27));
   cap = (cap + 31) & ~31;
   if (nl->cap > cap) cap = nl->cap;
+  if (nl->cap_set > 0) cap = nl->cap_set;  // a capacity the caller fixed
   nl->cap = cap;
   const size_t nn = std::max(1, n), ns = std::max(8, nl->ns_max);
   PM_CHECK(dev_alloc(s, &nl->d_key, sizeof(int) * nn));
@@ -759,8 +763,8 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
                           s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_maxdisp, 2 * sizeof(unsigned int)));
   PM_CUDA(cudaMemsetAsync(nl->d_maxdisp, 0, 2 * sizeof(unsigned int), s->stream));
-  PM_CHECK(dev_alloc(s, &nl->d_rebuild, 2 * sizeof(int)));
-  PM_CUDA(cudaMemsetAsync(nl->d_rebuild, 0, 2 * sizeof(int), s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_rebuild, 3 * sizeof(int)));
+  PM_CUDA(cudaMemsetAsync(nl->d_rebuild, 0, 3 * sizeof(int), s->stream));
   nl->built = 0;
   return PMGPU_OK;
 }

@@ -5,6 +5,7 @@
 #include <cufft.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -135,6 +136,7 @@ struct NeighborList {
   int nclusters = 0;                 // ns_max / 8
   int nrows = 0;                     // nclusters * kRowParts tile rows
   int cap = 0;                       // tiles per row
+  int cap_set = 0;                   // tiles per row fixed by the caller (0: sized here)
   int built = 0;
   int decided = 0;                   // this evaluation's rebuild decision is taken
   // a force-only MD step left its pair forces in d_fslot for the next update
@@ -164,7 +166,7 @@ struct NeighborList {
   uint4 *d_tiles = nullptr;      // nrows rows of cap tiles (row r: cluster r / kRowParts)
   int *d_tile_count = nullptr;   // nrows
   unsigned int *d_maxdisp = nullptr;  // rebuild check: block ticket, max displacement^2 bits
-  int *d_rebuild = nullptr;      // rebuild flag, build count
+  int *d_rebuild = nullptr;      // rebuild flag, build count, largest row need after an overflow
 };
 
 struct System;
@@ -191,6 +193,7 @@ struct Force {
   float2 *d_cgrid = nullptr;          // complex grid (K1*K2*(K3/2+1))
   float *d_influence = nullptr;       // K1*K2*(K3/2+1) influence function
   void *d_fft_work = nullptr;         // cuFFT work area shared by both plans
+  size_t fft_work_bytes = 0;
   // simplefull
   int sf_lj = 0, sf_coul = 0;
   // gb
@@ -411,4 +414,13 @@ int forces_to_host(System *s, double *out, int add);
 
 struct pmgpu_context {
   int device = 0;
+  // cuFFT plan pairs (R2C, C2R) of systems that ended, kept for the next
+  // system of the same grid: plan creation costs more than a short request
+  struct FftPlans {
+    int dims[3];
+    cufftHandle r2c, c2r;
+    size_t work;  // work-area bytes the pair needs
+  };
+  std::mutex fft_mu;
+  std::vector<FftPlans> fft_free;
 };

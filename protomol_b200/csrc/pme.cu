@@ -381,15 +381,33 @@ int pme_init(System *s, Force *f) {
     PM_CUDA(cudaStreamSynchronize(s->stream));
   }
   // cuFFT plans without their own work area: one stream-ordered work area
-  // serves both (they run back to back on the system's stream)
+  // serves both (they run back to back on the system's stream).  A pair
+  // left by an ended system of the same grid is taken from the context
+  // first.
   size_t ws_r2c = 0, ws_c2r = 0;
-  if (cufftCreate(&f->plan_r2c) != CUFFT_SUCCESS || cufftCreate(&f->plan_c2r) != CUFFT_SUCCESS ||
-      cufftSetAutoAllocation(f->plan_r2c, 0) != CUFFT_SUCCESS ||
-      cufftSetAutoAllocation(f->plan_c2r, 0) != CUFFT_SUCCESS ||
-      cufftMakePlan3d(f->plan_r2c, K0, K1, K2, CUFFT_R2C, &ws_r2c) != CUFFT_SUCCESS ||
-      cufftMakePlan3d(f->plan_c2r, K0, K1, K2, CUFFT_C2R, &ws_c2r) != CUFFT_SUCCESS)
+  bool reused = false;
+  {
+    std::lock_guard<std::mutex> lock(s->ctx->fft_mu);
+    auto &pool = s->ctx->fft_free;
+    for (size_t k = 0; k < pool.size(); k++)
+      if (pool[k].dims[0] == K0 && pool[k].dims[1] == K1 && pool[k].dims[2] == K2) {
+        f->plan_r2c = pool[k].r2c;
+        f->plan_c2r = pool[k].c2r;
+        ws_r2c = ws_c2r = pool[k].work;
+        pool.erase(pool.begin() + k);
+        reused = true;
+        break;
+      }
+  }
+  if (!reused &&
+      (cufftCreate(&f->plan_r2c) != CUFFT_SUCCESS || cufftCreate(&f->plan_c2r) != CUFFT_SUCCESS ||
+       cufftSetAutoAllocation(f->plan_r2c, 0) != CUFFT_SUCCESS ||
+       cufftSetAutoAllocation(f->plan_c2r, 0) != CUFFT_SUCCESS ||
+       cufftMakePlan3d(f->plan_r2c, K0, K1, K2, CUFFT_R2C, &ws_r2c) != CUFFT_SUCCESS ||
+       cufftMakePlan3d(f->plan_c2r, K0, K1, K2, CUFFT_C2R, &ws_c2r) != CUFFT_SUCCESS))
     return fail(PMGPU_ERR_CUDA, "cuFFT plan creation failed");
-  PM_CHECK(dev_alloc(s, &f->d_fft_work, std::max(ws_r2c, ws_c2r)));
+  f->fft_work_bytes = std::max(ws_r2c, ws_c2r);
+  PM_CHECK(dev_alloc(s, &f->d_fft_work, f->fft_work_bytes));
   if (cufftSetWorkArea(f->plan_r2c, f->d_fft_work) != CUFFT_SUCCESS ||
       cufftSetWorkArea(f->plan_c2r, f->d_fft_work) != CUFFT_SUCCESS ||
       cufftSetStream(f->plan_r2c, s->stream) != CUFFT_SUCCESS ||
@@ -399,8 +417,16 @@ int pme_init(System *s, Force *f) {
 }
 
 int pme_free(System *s, Force *f) {
-  if (f->plan_r2c) cufftDestroy(f->plan_r2c);
-  if (f->plan_c2r) cufftDestroy(f->plan_c2r);
+  if (f->plan_r2c && f->plan_c2r && s->ctx) {
+    // back to the context for the next system of this grid (its next user
+    // sets the work area and the stream again)
+    std::lock_guard<std::mutex> lock(s->ctx->fft_mu);
+    s->ctx->fft_free.push_back(
+        {{f->grid[0], f->grid[1], f->grid[2]}, f->plan_r2c, f->plan_c2r, f->fft_work_bytes});
+  } else {
+    if (f->plan_r2c) cufftDestroy(f->plan_r2c);
+    if (f->plan_c2r) cufftDestroy(f->plan_c2r);
+  }
   f->plan_r2c = f->plan_c2r = 0;
   void *ptrs[] = {f->d_grid, f->d_grid_fixed, f->d_cgrid, f->d_influence, f->d_fft_work};
   for (void *p : ptrs) dev_free(s, p);

@@ -246,6 +246,10 @@ class GpuSystem:
         L.check(self.lib.pmgpu_kernel_count(self.h, C.byref(c)))
         return int(c.value)
 
+    def set_list_capacity(self, tiles_per_row: int) -> None:
+        """Fix the pair lists' capacity (testing the growth path)."""
+        L.check(self.lib.pmgpu_debug_set_list_capacity(self.h, int(tiles_per_row)))
+
     def cell_assign(self, cellsize: float):
         cells = np.zeros((self.n, 3), np.int32)
         dims = np.zeros(3, np.int32)
