@@ -340,49 +340,129 @@ def ensemble_line(args, ctx, world: int, rank: int, dist=None) -> dict:
             "cpu_baseline": cpu}
 
 
+def _oracle_water_forces(job):
+    """The FP64 restatement's forces and total potential energy of one TIP3P
+    box with the served force set (cutoff LJ C2, Ewald real + SPME + exclusion
+    correction + self terms, bonds, angles); run in a worker process."""
+    import oracle
+    from oracle import spme
+    (pos, charge, typ, mol, lj, excl, box, mass, bonds, bprm, angles, aprm, grid) = job
+    s = oracle.System(pos=pos, charge=charge, type=typ, molecule=mol, lj=lj, excl=excl,
+                      periodic=True, box=box, mass=mass)
+    t0 = time.perf_counter()
+    sw = oracle.Switch("C2", RC, LJ_SWITCHON)
+    f, e, _ = oracle.cutoff_force(s, RC, RC, [("LennardJones", sw)])
+    ew = oracle.ewald_params(s, ALPHA, math.exp(-(ALPHA * RC) ** 2))
+    ew.rc = RC
+    fr, er, _ = oracle.ewald_real(s, ew, RC)
+    fk, ek = spme.reciprocal(s.pos, s.charge, s.box, ALPHA, ORDER, grid)
+    fc, ec, _ = oracle.ewald_correction(s, ew)
+    es, eq = oracle.ewald_self(s, ew)
+    fb, eb, _ = oracle.bonded_force(s, bonds, bprm, angles, aprm)
+    return (f + fr + fk + fc + fb, er + ek + ec + es + eq + e["lj"] + eb["bond"] + eb["angle"],
+            time.perf_counter() - t0)
+
+
+def served_error_sample(ctx, reqs, every: int = 20) -> dict:
+    """The cpu_baseline leg of the served form: on every `every`-th request
+    (5 %) the forces the GPU path gives at the request's result (the
+    returned forces of an evaluation; a force-only evaluation at the final
+    positions of a segment) against the FP64 restatement, which is timed
+    there too (several worker processes, spawned)."""
+    import multiprocessing as mp
+    from protomol_b200 import serve
+    sample = [r for r in reqs if r.rid % every == 0 and r.error is None]
+    jobs, gpu = [], []
+    for r in sample:
+        m = r.system
+        if r.kind == "evaluate":
+            pos, fg = m.pos, r.forces
+        else:
+            gs = serve.build(ctx, r)
+            gs.set_positions(r.positions)
+            fg = gs.evaluate_forces()
+            gs.close()
+            pos = r.positions
+        gpu.append(fg)
+        jobs.append((pos, m.charge, m.type, m.molecule, m.lj, m.exclusions, m.box, m.mass,
+                     m.bonds, m.bond_params, m.angles, m.angle_params, r.grid))
+    cores = min(len(jobs), os.cpu_count() or 1) or 1
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_oracle_water_forces, jobs)
+    errs = [float(np.sqrt(((fg - fo) ** 2).sum() / (fo ** 2).sum()))
+            for fg, (fo, _, _) in zip(gpu, res)]
+    atom_s = sum(r.n_atoms for r in sample) / max(1e-9, sum(t for _, _, t in res))
+    return {"force_rms_rel_err_max": max(errs) if errs else None,
+            "force_rms_rel_err_median": float(np.median(errs)) if errs else None,
+            "sampled_requests": len(sample), "ok": bool(errs) and max(errs) <= 1e-5,
+            "restatement": {"value": atom_s, "unit": "atom force evaluations/s", "cores": 1,
+                            "kind": "port",
+                            "sample": f"{len(sample)} requests' force evaluations by the FP64 "
+                                      f"restatement, {cores} worker processes"}}
+
+
 def served_line(args, ctx, world: int, rank: int, dist=None) -> dict:
-    """Aggregate ns/day of the served (or batched) form beside the plain
-    form on the same requests: plain = one request at a time, served = up
-    to --slots requests in flight with continuous admission.  With N ranks
-    the stream is partitioned across the GPUs by estimated cost (replicas;
-    the only collectives are the max-over-ranks wall time and the gathered
+    """The served form beside the plain form on the same request stream:
+    plain = one request at a time (all queued, so always busy), served = up
+    to --slots requests in flight with continuous admission, the requests
+    arriving as a Poisson stream at twice the plain form's request rate
+    (saturating: the arrivals end halfway through the plain form's service
+    time), with latency measured from each arrival.  With N ranks the
+    stream is partitioned across the GPUs by estimated cost (replicas; the
+    only collectives are the max-over-ranks wall time and the gathered
     summaries)."""
     from protomol_b200 import replicas, serve
-    if args.mode == "served":
-        # 500-50,000 atoms log-uniform, 30 % single evaluations, 70 % Langevin
-        # segments; all requests queued at t = 0 (a saturating stream)
-        mk = lambda: serve.request_stream(args.requests, 7, steps=args.md_steps)
-        workload = (f"served stream: {args.requests} requests, TIP3P boxes of 500-50,000 atoms "
-                    f"(log-uniform), 30% energy+force evaluations, 70% {args.md_steps}-step "
-                    f"LangevinLeapfrog segments (1 fs, 5/ps, 300 K), PME order 4 spacing <= 1 A, "
-                    f"rc 9 A")
-    else:
+    if args.mode != "served":
         return ensemble_line(args, ctx, world, rank, dist)
-    # warm-up: every request shape once (short), so lazily loaded FFT and
-    # kernel modules of every grid size are resident before either form is
-    # timed
-    for r in replicas.my_share(mk(), world, rank):
+    # 500-50,000 atoms log-uniform, 30 % single evaluations, 70 % Langevin
+    # segments
+    mk = lambda rate: serve.request_stream(args.requests, 7, steps=args.md_steps,
+                                           rate_per_s=rate)
+    workload = (f"served stream: {args.requests} requests, TIP3P boxes of 500-50,000 atoms "
+                f"(log-uniform), 30% energy+force evaluations, 70% {args.md_steps}-step "
+                f"LangevinLeapfrog segments (1 fs, 5/ps, 300 K), PME order 4 spacing <= 1 A, "
+                f"rc 9 A, Poisson arrivals at twice the plain form's request rate")
+    # warm-up: one short request per grid size, so the lazily loaded FFT
+    # kernels of every size are resident before either form is timed
+    seen = set()
+    for r in replicas.my_share(mk(None), world, rank):
+        if r.grid in seen:
+            continue
+        seen.add(r.grid)
         serve.execute(ctx, serve.Request(rid=-1, n_waters=r.n_waters, seed=r.seed,
-                                         kind=r.kind, steps=min(r.steps, 12)))
+                                         kind="segment", steps=12))
     out = {}
+    rate = None
     for name, slots in (("plain", 1), ("served", args.slots)):
-        reqs = replicas.my_share(mk(), world, rank)
+        reqs = replicas.my_share(mk(rate), world, rank)
         if dist:
             dist.barrier()
-        st = serve.Server(ctx, slots=slots).run(reqs, realtime=False)
+        st = serve.Server(ctx, slots=slots).run(reqs, realtime=name == "served")
         wall = replicas.max_over_ranks(st["wall_s"], dist)
         parts = replicas.gather_summaries(st, dist)
         md_ns = sum(p["ns_per_day"] * p["wall_s"] / 86400.0 for p in parts)
         st.update({"ranks": len(parts), "wall_s": wall, "ns_per_day": md_ns * 86400.0 / wall,
                    "p99_latency_s": max(p["p99_latency_s"] for p in parts)})
         out[name] = st
-    return {"metric": "ns/day (" + args.mode + " form)", "impl": "pmgpu", "mode": args.mode,
+        if name == "plain":
+            rate = 2.0 * args.requests / wall
+            out["arrival_rate_per_s"] = rate
+    line = {"metric": "ns/day (served form)", "impl": "pmgpu", "mode": "served",
             "value": out["served"]["ns_per_day"], "unit": "ns/day", "n_gpus": world,
             "higher_is_better": True, "scaling": "strong", "data": "synthetic",
-            "config": {"workload": workload, "partition": f"requests over {world} GPU(s)"},
+            "config": {"workload": workload, "partition": f"requests over {world} GPU(s)",
+                       "arrival_rate_per_s": out["arrival_rate_per_s"]},
             "served": out["served"], "plain": out["plain"],
             "served_over_plain": out["served"]["ns_per_day"] / max(out["plain"]["ns_per_day"],
                                                                    1e-30)}
+    if rank == 0 and world == 1 and getattr(args, "error_sample", True):
+        try:
+            acc = served_error_sample(ctx, reqs)
+            line["accuracy"] = {k: acc[k] for k in acc if k != "restatement"}
+            line["cpu_baseline"] = acc["restatement"]
+        except Exception as ex:  # reported, never fatal
+            line["accuracy"] = {"error": str(ex)[:200]}
+    return line
 
 
 GB_ATOMS, GB_SEED, GB_SEGMENT = 2000, 3, 500
@@ -517,7 +597,7 @@ def run_forms(args, ctx, world: int, rank: int, dist=None) -> dict:
     Failures are reported in place, never fatal."""
     import copy
     legs = (("batched", dict(requests=256, steps=2, warmup=1)),
-            ("served", dict(requests=32, md_steps=1000, slots=32)),
+            ("served", dict(requests=60, md_steps=1000, slots=32)),
             ("gb", dict(steps=2, warmup=2, segment=GB_SEGMENT)))
     out = {}
     for mode, kw in legs:
@@ -541,7 +621,8 @@ def run_forms(args, ctx, world: int, rank: int, dist=None) -> dict:
             out[mode] = {"value": r["value"], "unit": "ns/day", "workload": r["config"]["workload"],
                          "plain_ns_per_day": r["plain"]["ns_per_day"],
                          "served_over_plain": r["served_over_plain"],
-                         "p50_latency_s": sv["p50_latency_s"], "p99_latency_s": sv["p99_latency_s"]}
+                         "p50_latency_s": sv["p50_latency_s"], "p99_latency_s": sv["p99_latency_s"],
+                         "accuracy": r.get("accuracy"), "cpu_baseline": r.get("cpu_baseline")}
         else:
             out[mode] = {"value": r["value"], "unit": "ns/day", "workload": r["config"]["workload"],
                          "us_per_md_step": r["us_per_md_step"], "e2e": r["e2e"]["value"],

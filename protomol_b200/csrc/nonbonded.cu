@@ -950,6 +950,7 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   a.pairbuf_cap = s->pairbuf_cap;
   a.paircount = s->d_paircount;
   a.count_pairs = s->count_pairs;
+  a.energy_only = 0;
 }
 
 // Compile-time switch kind of a term for the specialised force-only
@@ -1037,19 +1038,37 @@ template <typename Real, int TERMS>
 static int launch_pairs_t(PairArgs<Real> &a, cudaStream_t st, int mode, const PairTerms &t) {
   // specialised force-only FP32 kernels of the common configurations
   // (every term with one cutoff, box edges at least twice the cutoff)
-  if (sizeof(Real) == 4 && mode == PAIR_FORCE && a.same_cut && !a.minimal_image) {
+  if (sizeof(Real) == 4 && mode != PAIR_RECORD && a.same_cut && !a.minimal_image) {
     const int lk = spec_kind(t.lj_sw), ck = spec_kind(t.coul_sw);
-    if (TERMS == (TERM_LJ | TERM_EWALD) && !t.exact_erf && lk == PMGPU_SW_C2) {
-      launch_force_spec<Real, TERM_LJ | TERM_EWALD, PairSpec<PMGPU_SW_C2, -1, 0>>(a, st);
-      return PMGPU_PAIRK_LJC2_EWALD;
-    }
-    if (TERMS == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C2) {
-      launch_force_spec<Real, TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C2, -1>>(a, st);
-      return PMGPU_PAIRK_LJC2_COULC2;
-    }
-    if (TERMS == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C1) {
-      launch_force_spec<Real, TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C1, -1>>(a, st);
-      return PMGPU_PAIRK_LJC2_COULC1;
+    int form = PMGPU_PAIRK_GENERIC;
+    if (TERMS == (TERM_LJ | TERM_EWALD) && !t.exact_erf && lk == PMGPU_SW_C2)
+      form = PMGPU_PAIRK_LJC2_EWALD;
+    else if (TERMS == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C2)
+      form = PMGPU_PAIRK_LJC2_COULC2;
+    else if (TERMS == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C1)
+      form = PMGPU_PAIRK_LJC2_COULC1;
+    if (form != PMGPU_PAIRK_GENERIC) {
+      // The forces of every mode come from the specialised kernel, so an
+      // energy step's forces equal a force-only step's bit for bit (a run
+      // split into several calls, whose energy steps fall elsewhere, gives
+      // the same trajectory); energies and virial then come from the
+      // generic kernel in its energy-only form.
+      PairArgs<Real> fa = a;
+      if (mode != PAIR_FORCE) fa.count_pairs = 0;  // the energy pass counts
+      if (form == PMGPU_PAIRK_LJC2_EWALD)
+        launch_force_spec<Real, TERM_LJ | TERM_EWALD, PairSpec<PMGPU_SW_C2, -1, 0>>(fa, st);
+      else if (form == PMGPU_PAIRK_LJC2_COULC2)
+        launch_force_spec<Real, TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C2, -1>>(fa,
+                                                                                          st);
+      else
+        launch_force_spec<Real, TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C1, -1>>(fa,
+                                                                                          st);
+      if (mode != PAIR_FORCE) {
+        PairArgs<Real> ea = a;
+        ea.energy_only = 1;
+        launch_pairs_spec<Real, TERMS, GenericSpec>(ea, st, mode);
+      }
+      return form;
     }
   }
   launch_pairs_spec<Real, TERMS, GenericSpec>(a, st, mode);

@@ -64,6 +64,8 @@ struct PairArgs {
   long long pairbuf_cap;
   long long *paircount;
   int count_pairs;       // accumulate the accepted-pair count
+  int energy_only;       // energies (and virial) only: the forces come from the
+                         // force-only kernel launched beside
 };
 
 // Exact FP64 squared distance of the image in hand, formed the way the
@@ -599,7 +601,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
     const Real js = group8_sum3<Real>(jx, jy, jz, lane);
     long long *dst = a.fslot + il * a.ns + jslot;
     const long long v = fixed_force(js);
-    if (il < 3 && ((act >> (8 * jl)) & 0xFFu)) red_add(dst, v);
+    if (il < 3 && ((act >> (8 * jl)) & 0xFFu) && !a.energy_only) red_add(dst, v);
   }
     if (left > 0) {  // next non-empty row part
       do {
@@ -616,7 +618,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
     fy += __shfl_xor_sync(kAll, fy, o);
     fz += __shfl_xor_sync(kAll, fz, o);
   }
-  if (jl == 0 && oi >= 0) {
+  if (jl == 0 && oi >= 0 && !a.energy_only) {
     red_add(&a.fslot[islot], fixed_force(fx));
     red_add(&a.fslot[a.ns + islot], fixed_force(fy));
     red_add(&a.fslot[2 * a.ns + islot], fixed_force(fz));

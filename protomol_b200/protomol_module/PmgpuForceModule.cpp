@@ -575,6 +575,10 @@ class DeviceIntegrator : public STSIntegrator {
     it.gamma_ps = myGamma;
     it.seed = (uint64_t)mySeed;
     check(pmgpu_run(mySystem, &it, numTimesteps), getIdNoAlias());
+    // the simulated time the outputs report, advanced by the steps taken
+    // (as the reference's own device integrator does,
+    // integrator/openMM/OpenMMIntegrator.cpp:688)
+    app->topology->time += numTimesteps * getTimestep();
     double e[PMGPU_E_COUNT];
     check(pmgpu_system_get_energies(mySystem, e, 0), getIdNoAlias());
     download(e);

@@ -97,9 +97,46 @@ def torsions() -> None:
                                           cellsize=5.0), {"seed": np.array(3)})
 
 
+def langevin_temperature() -> None:
+    """The reference's LangevinLeapfrog thermostat on the 648-atom box with
+    its MD forces (1 fs, 5/ps, 300 K): the mean kinetic temperature of steps
+    1,000-3,000 (outputs every 20 steps), one run per random seed.  At 1 fs
+    the stiff O-H bonds of flexible TIP3P leave the kinetic temperature a
+    few per cent above the target in the reference's own integrator."""
+    import subprocess
+    c1 = systems.tip3p_box(216, 18.6, seed=1, lattice=6)
+    md = ["LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction C2 -switchon 7 "
+          "-cutoff 8 -switchingFunction C2 -switchon 7 -cutoff 8 -cutoff 8", "Bond", "Angle"]
+    means = []
+    seeds = [1234, 5, 6, 7]
+    for seed in seeds:
+        tmp = tempfile.mkdtemp()
+        try:
+            conf = systems.write_protomol_inputs(
+                c1, tmp, "w", md, integrator="LangevinLeapfrog", timestep=1.0, numsteps=3000,
+                cellsize=8.0, outputs=True, outputfreq=20,
+                integrator_params=f"temperature 300 gamma 5 seed {seed}")
+            text = open(conf).read().replace("seed 1234\n", f"seed {seed}\n", 1)
+            open(conf, "w").write(text)
+            subprocess.run([refdump.PROTOMOL, conf], cwd=tmp, check=True,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            rows = [[float(t[0])] + [float.fromhex(x) for x in t[1:]]
+                    for t in (ln.split() for ln in open(os.path.join(tmp, "w.out.energy"))) if t]
+            rows = np.array(rows)
+            means.append(rows[rows[:, 0] > 1000.0, 4].mean())  # Temperature column
+        finally:
+            shutil.rmtree(tmp)
+    np.savez_compressed(os.path.join(HERE, "c1_langevin_temperature.npz"),
+                        seeds=np.array(seeds), mean_temperature=np.array(means))
+    print("wrote c1_langevin_temperature", means)
+
+
 def main(which: str = "all") -> None:
     if which == "torsions":
         torsions()
+        return
+    if which == "langevin":
+        langevin_temperature()
         return
     if which == "gb":
         gb = ["GBBornRadii -algorithm NonbondedSimpleFull",
@@ -166,6 +203,7 @@ def main(which: str = "all") -> None:
                                  "velocities_20": d1["velocities"],
                                  "timestep": np.array(dt), "md_forces": np.array(md)})
     leapfrog100(c1, md)
+    langevin_temperature()
 
 
 def leapfrog100(c1, md) -> None:

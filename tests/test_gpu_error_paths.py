@@ -109,12 +109,16 @@ def test_langevin_noise_statistics_without_forces(ctx):
     gs.close()
 
 
-def test_langevin_thermostat_holds_300K(ctx):
+def test_langevin_thermostat_matches_reference(ctx):
     """The 648-atom TIP3P box with all its forces under LangevinLeapfrog
     (1 fs, 5/ps, 300 K): after 1,000 steps of equilibration the average
-    kinetic temperature over the next 2,000 steps is 300 K within 3 %
-    (single-sample fluctuations are sqrt(2 / 3N) = 3.2 %; the average over
-    100 samples spaced by 20 fs is far tighter)."""
+    kinetic temperature over the next 2,000 steps matches the reference's
+    own LangevinLeapfrog on the same system (tests/golden/
+    c1_langevin_temperature.npz, four seeds: 311-316 K; at 1 fs the stiff
+    O-H bonds of flexible water leave the kinetic temperature a few per cent
+    above the target in both).  The bound, 10 K, is about three times the
+    combined scatter of such 2,000-step means."""
+    ref = np.load(F.GOLDEN + "/c1_langevin_temperature.npz")["mean_temperature"]
     gs = _c1(ctx)
     mass = F.topology(F.load("c1_leapfrog100")).mass
     it = LangevinLeapfrogIntegrator(1.0, temperature=300.0, gamma=5.0, seed=77)
@@ -124,5 +128,6 @@ def test_langevin_thermostat_holds_300K(ctx):
         it.run(gs, 20)
         temps.append(_temperature(gs.velocities(), mass))
     t = float(np.mean(temps))
-    assert abs(t - 300.0) <= 9.0, t
+    assert abs(t - float(ref.mean())) <= 10.0, (t, ref)
+    assert t > 300.0  # the integrator's bias has the reference's sign
     gs.close()

@@ -417,6 +417,11 @@ def test_gbace_vs_reference(ctx, name, precision, tol):
     ace = ff.make("GBACEForce -algorithm NonbondedSimpleFull")
     f, e = _eval(ace, topo)
     ref = F.forces(z, k_ace)
+    # the ACE forces of the 32-atom dipeptide are ~1e-3 kcal/mol/A, where
+    # the int64 fixed-point sums (2^-32 per unit) leave ~1e-9 absolute:
+    # an RMS floor of 1e-9 kcal/mol/A below the relative tolerance
+    rms_ref = float(np.sqrt((ref ** 2).mean()))
+    tol = max(tol, 1e-9 / rms_ref)
     assert F.rms_rel(f, ref) <= tol, F.rms_rel(f, ref)
     assert _energy_ok(e[0], F.energies(z, k_ace)[0], floor=1e-6)
     gb = ff.make("GBForce -algorithm NonbondedSimpleFull -soluteDielec 1.0 -solventDielec 78.3")
