@@ -286,21 +286,27 @@ def restatement_baseline(gs, sysm, samples) -> dict:
 def ensemble_line(args, ctx, world: int, rank: int, dist=None) -> dict:
     """The batched ensemble: --requests resident TIP3P boxes (100-1,000 waters
     log-uniform, split over the ranks), each advanced in 50-step leapfrog
-    segments.  Set-up and the first segment (graph capture) are untimed;
-    then --steps segments are timed with all members in flight at once
-    (batched) and one member at a time (plain)."""
-    from protomol_b200 import replicas, serve
+    segments.  Set-up, the split autotuning and the first segment of each
+    form (graph capture) are untimed; then --steps segments are timed in
+    each form: batched (one launch per kernel over all members, each
+    segment one CUDA graph), streams (every member's own segment on its own
+    stream, all in flight) and plain (one member at a time)."""
+    from protomol_b200 import replicas, serve, tuner
     seg = 50
     reqs = replicas.my_share(serve.ensemble(args.requests, 9, steps=seg), world, rank,
                             cost=lambda r: float(r.n_atoms))
-    ens = serve.Ensemble(ctx, reqs)
-    for _ in range(max(1, args.warmup)):
-        ens.run(seg)
+    tn = tuner.SplitTuner(os.environ.get("PMGPU_TUNE_CACHE"), key="lj_c2+ewald")
+    ens = serve.Ensemble(ctx, reqs, tuner=tn)
     out = {}
-    for name, plain in (("plain", True), ("batched", False)):
+    info = None
+    for name in ("plain", "streams", "batched"):
+        for _ in range(max(1, args.warmup)):
+            ens.run(seg, mode=name)
         if dist:
             dist.barrier()
-        wall = sum(ens.run(seg, plain=plain) for _ in range(args.steps))
+        wall = sum(ens.run(seg, mode=name) for _ in range(args.steps))
+        if name == "batched":
+            info = ens.info()
         wall = replicas.max_over_ranks(wall, dist)
         members = args.requests
         md_ns = members * seg * args.steps * 1e-6  # 1 fs steps
@@ -308,6 +314,11 @@ def ensemble_line(args, ctx, world: int, rank: int, dist=None) -> dict:
         out[name] = {"wall_s": wall, "ns_per_day": md_ns * 86400.0 / wall,
                      "atom_steps_per_s": atoms * seg * args.steps / wall,
                      "segments_per_member": args.steps}
+    out["batched"]["kernels_per_md_step"] = info["kernels"] / max(1, info["steps"])
+    out["batched"]["graph_replays_per_segment"] = info["graph_replays"]
+    out["batched"]["fft_buckets"] = info["fft_buckets"]
+    out["batched"]["splits_by_bucket"] = {str(b): v for b, v in sorted(tn.table.items())}
+    out["batched"]["tuner_timed_launches"] = tn.timings
     ens.close()
     cpu = None
     if rank == 0 and world == 1 and os.path.exists(REF_BIN):
@@ -328,15 +339,17 @@ def ensemble_line(args, ctx, world: int, rank: int, dist=None) -> dict:
         except Exception as ex:  # reported, never fatal
             cpu = {"value": None, "error": str(ex)[:200]}
     workload = (f"batched ensemble: {args.requests} resident TIP3P boxes of 100-1,000 waters "
-                f"(log-uniform), 0.0334 waters/A^3, {seg}-step leapfrog segments (inner steps "
-                f"as CUDA graphs), PME order 4 spacing <= 1 A, rc 9 A, LJ C2 8->9 A")
+                f"(log-uniform), 0.0334 waters/A^3, {seg}-step leapfrog segments (each one "
+                f"CUDA graph of batched launches over all boxes), PME order 4 spacing <= 1 A, "
+                f"rc 9 A, LJ C2 8->9 A")
     return {"metric": "ns/day (batched form)", "impl": "pmgpu", "mode": "batched",
             "value": out["batched"]["ns_per_day"], "unit": "ns/day", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "strong", "data": "synthetic",
             "config": {"workload": workload, "partition": f"boxes over {world} GPU(s)"},
-            "batched": out["batched"], "plain": out["plain"],
+            "batched": out["batched"], "streams": out["streams"], "plain": out["plain"],
             "batched_over_plain": out["batched"]["ns_per_day"] / out["plain"]["ns_per_day"],
+            "batched_over_streams": out["batched"]["ns_per_day"] / out["streams"]["ns_per_day"],
             "cpu_baseline": cpu}
 
 
@@ -437,7 +450,9 @@ def served_line(args, ctx, world: int, rank: int, dist=None) -> dict:
         reqs = replicas.my_share(mk(rate), world, rank)
         if dist:
             dist.barrier()
-        st = serve.Server(ctx, slots=slots).run(reqs, realtime=name == "served")
+        server = serve.Server(ctx, slots=slots)
+        st = server.run(reqs, realtime=name == "served")
+        server.close()
         wall = replicas.max_over_ranks(st["wall_s"], dist)
         parts = replicas.gather_summaries(st, dist)
         md_ns = sum(p["ns_per_day"] * p["wall_s"] / 86400.0 for p in parts)
@@ -614,7 +629,9 @@ def run_forms(args, ctx, world: int, rank: int, dist=None) -> dict:
         if mode == "batched":
             out[mode] = {"value": r["value"], "unit": "ns/day", "workload": r["config"]["workload"],
                          "plain_ns_per_day": r["plain"]["ns_per_day"],
+                         "streams_ns_per_day": r["streams"]["ns_per_day"],
                          "batched_over_plain": r["batched_over_plain"],
+                         "kernels_per_md_step": r["batched"]["kernels_per_md_step"],
                          "cpu_baseline": r.get("cpu_baseline")}
         elif mode == "served":
             sv = r["served"]
@@ -834,7 +851,7 @@ def main():
             "us_per_md_step": 1e6 * step_s,
             "phase_ms_per_md_step_eager": {k: v[0] / args.segment for k, v in prof.items()
                                            if v[1]},
-            "roofline": {"bound": "hbm", "kernel": "k_pairs (fused LJ + Ewald real)",
+            "roofline": {"bound": "hbm", "kernel": "k_pairs_jl (force-only LJ C2 + Ewald real)",
                          "achieved": pair_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": pair_gbs / peaks["hbm_gbs"],
                          "traffic": traffic, "peak_source": peaks["src"],

@@ -154,11 +154,18 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *topo,
                         int precision, pmgpu_system **out);
 int pmgpu_system_destroy(pmgpu_system *sys);
 /* Host <-> device copies of Vector3DBlock-layout arrays (3n doubles).
- * Positions with a non-finite coordinate are refused with PMGPU_ERR_NAN. */
+ * Positions with a non-finite coordinate are refused with PMGPU_ERR_NAN.
+ * New positions are a new configuration: the next evaluation builds every
+ * pair list afresh, as for a new system. */
 int pmgpu_system_set_positions(pmgpu_system *sys, const double *pos);
 int pmgpu_system_get_positions(pmgpu_system *sys, double *pos);
 int pmgpu_system_set_velocities(pmgpu_system *sys, const double *vel);
 int pmgpu_system_get_velocities(pmgpu_system *sys, double *vel);
+/* The step counter that keys the Langevin noise (ProtoMol's current step;
+ * a new system starts at 0, every MD step adds one).  With positions,
+ * velocities and this counter set, a system continues exactly as a new
+ * system made from that state would. */
+int pmgpu_system_set_step(pmgpu_system *sys, long long step);
 /* Total force of the last evaluation (all enabled terms), 3n doubles. */
 int pmgpu_system_get_forces(pmgpu_system *sys, double *forces);
 /* Energies (PMGPU_E_COUNT) and atomic virial (9, may be NULL) of the last
@@ -306,6 +313,53 @@ int pmgpu_mem_info(pmgpu_context *ctx, long long *free_bytes, long long *total_b
 int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
                              const int grid[3], long long *bytes);
 
+/* ---- ensembles ------------------------------------------------------ */
+/* Many resident systems advanced together.  Every kernel of an MD step is
+ * one launch over all members (a device table of per-member arguments and
+ * first-block offsets; each block finds its member by binary search), the
+ * members whose PME grids have the same dimensions share one batched FFT
+ * plan pair, and the steps of a segment replay as captured CUDA graphs, so
+ * the launches per step do not grow with the member count.  A member's
+ * launches compute what its own single-system launches compute, in the
+ * same fixed-point sums: its trajectory is bitwise the same in any
+ * ensemble, alone or beside others, for the same pair-kernel splits.
+ *
+ * Members: periodic, PMGPU_PREC_MIXED, one context, one cutoff pair list
+ * (LennardJones and / or Coulomb or the Ewald real term), at most one PME
+ * force, bonded terms; the same force set on every member.  They stay
+ * owned by the caller, must outlive the ensemble and must not be used
+ * through the single-system calls while an ensemble call runs (every
+ * ensemble call is synchronous).  No counterpart in the reference, which
+ * runs one system per process. */
+typedef struct pmgpu_ensemble pmgpu_ensemble;
+int pmgpu_ensemble_create(pmgpu_system *const *members, int n, pmgpu_ensemble **out);
+/* Gives the members their own PME grids back and frees the ensemble. */
+int pmgpu_ensemble_destroy(pmgpu_ensemble *e);
+/* n_steps MD steps of integrator it on every member: for each member the
+ * steps pmgpu_run(member, it, n_steps) takes, its energies of the last
+ * step then read by pmgpu_system_get_energies.  A pair list that overflows
+ * grows and the segment runs again from its start on every member. */
+int pmgpu_ensemble_run(pmgpu_ensemble *e, const pmgpu_integrator *it, long n_steps);
+/* Pair-kernel splits (the warps each 8-atom i cluster's tiles are divided
+ * over in the force-only kernel): splits[k] for member k, 0 the
+ * single-system choice.  Changes rounding (not the pair set), so results
+ * are bitwise reproducible for a given table. */
+int pmgpu_ensemble_set_splits(pmgpu_ensemble *e, const int *splits);
+/* Device milliseconds of one force-only pair launch over all members with
+ * member k at splits[k] (0: its current choice), averaged over reps
+ * launches; the members' state is unchanged.  For autotuning. */
+int pmgpu_ensemble_time_pairs(pmgpu_ensemble *e, const int *splits, int reps, double *ms);
+typedef struct {
+  int members;
+  int fft_buckets;         /* distinct PME grids (one batched FFT pair each) */
+  long long kernels;       /* own kernel launches of the last run */
+  long long graph_replays; /* CUDA graph launches of the last run */
+  long long steps;         /* MD steps of the last run */
+} pmgpu_ensemble_info;
+int pmgpu_ensemble_get_info(pmgpu_ensemble *e, pmgpu_ensemble_info *out);
+/* Member k's i-cluster count and the splits its pair launch takes. */
+int pmgpu_ensemble_member(pmgpu_ensemble *e, int k, int *clusters, int *splits);
+
 /* ---- diagnostics ---------------------------------------------------- */
 /* Measured FP32 FMA throughput of the context's GPU in TFLOP/s (an FMA
  * counts two flops): every SM runs independent FMA chains for about a
@@ -321,6 +375,7 @@ typedef struct {
   int cells[3];                /* sort-grid dims of the cutoff path */
   int pair_kernel;             /* form of the last pair-kernel launch of the
                                   force's list: PMGPU_PAIRK_* */
+  int list_capacity;           /* tiles a list row holds (grows on overflow) */
 } pmgpu_stats;
 /* Pair-kernel forms: the generic kernel (any terms and switches, energies,
  * virial) and the specialised force-only FP32 kernels of the inner MD steps
@@ -372,6 +427,11 @@ int pmgpu_debug_cell_assign(pmgpu_system *sys, double cellsize,
  * so results equal those of a list that never overflowed.  No counterpart
  * in the reference (its cell lists have no capacity). */
 int pmgpu_debug_set_list_capacity(pmgpu_system *sys, int tiles_per_row);
+/* Limits the tiles a list row may hold in the next builds to tiles_per_row
+ * without touching the current list, positions or forces: the first later
+ * build (an MD step's rebuild) that needs more takes the growth path, which
+ * lifts the limit.  For testing that path inside MD segments. */
+int pmgpu_debug_limit_list_rows(pmgpu_system *sys, int tiles_per_row);
 /* The unordered pair set (i < j, original indices) the cutoff force
  * force_id evaluated on its last evaluation: pairs gets 2 ints per pair,
  * up to cap pairs; *count gets the total. */

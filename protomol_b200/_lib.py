@@ -40,8 +40,16 @@ EXPORTED = [
     "pmgpu_kernel_count", "pmgpu_gb_forces_noalloc", "pmgpu_run_async", "pmgpu_run_query",
     "pmgpu_run_wait", "pmgpu_mem_info", "pmgpu_footprint_estimate", "pmgpu_force_torsion_add",
     "pmgpu_fp32_peak", "pmgpu_force_gbace_add", "pmgpu_debug_set_list_capacity",
+    "pmgpu_ensemble_create", "pmgpu_ensemble_destroy", "pmgpu_ensemble_run",
+    "pmgpu_ensemble_set_splits", "pmgpu_ensemble_time_pairs", "pmgpu_ensemble_get_info",
+    "pmgpu_ensemble_member", "pmgpu_debug_limit_list_rows", "pmgpu_system_set_step",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
+
+
+class EnsembleInfo(C.Structure):
+    _fields_ = [("members", C.c_int), ("fft_buckets", C.c_int), ("kernels", C.c_longlong),
+                ("graph_replays", C.c_longlong), ("steps", C.c_longlong)]
 
 
 class PmgpuError(RuntimeError):
@@ -79,7 +87,7 @@ class Integrator(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("pairs_in_cutoff", C.c_longlong), ("list_entries", C.c_longlong),
                 ("clusters", C.c_longlong), ("list_builds", C.c_longlong),
-                ("cells", C.c_int * 3), ("pair_kernel", C.c_int)]
+                ("cells", C.c_int * 3), ("pair_kernel", C.c_int), ("list_capacity", C.c_int)]
 
 
 _lib = None
@@ -126,6 +134,8 @@ def load() -> C.CDLL:
     lib.pmgpu_debug_cell_assign.argtypes = [vp, dbl, vp, vp]
     lib.pmgpu_debug_pair_set.argtypes = [vp, i32, vp, C.c_longlong, C.POINTER(C.c_longlong)]
     lib.pmgpu_debug_set_list_capacity.argtypes = [vp, i32]
+    lib.pmgpu_debug_limit_list_rows.argtypes = [vp, i32]
+    lib.pmgpu_system_set_step.argtypes = [vp, C.c_longlong]
     lib.pmgpu_profile_enable.argtypes = [vp, i32]
     lib.pmgpu_profile_read.argtypes = [vp, vp, vp, i32]
     lib.pmgpu_kernel_count.argtypes = [vp, C.POINTER(C.c_longlong)]
@@ -137,6 +147,13 @@ def load() -> C.CDLL:
     lib.pmgpu_footprint_estimate.argtypes = [i32, vp, dbl, vp, C.POINTER(C.c_longlong)]
     lib.pmgpu_gb_forces_noalloc.argtypes = [i32, vp, vp, vp, vp, vp, vp, C.POINTER(dbl),
                                             dbl, dbl, i32, vp, vp, vp]
+    lib.pmgpu_ensemble_create.argtypes = [vp, i32, C.POINTER(vp)]
+    lib.pmgpu_ensemble_destroy.argtypes = [vp]
+    lib.pmgpu_ensemble_run.argtypes = [vp, C.POINTER(Integrator), C.c_long]
+    lib.pmgpu_ensemble_set_splits.argtypes = [vp, vp]
+    lib.pmgpu_ensemble_time_pairs.argtypes = [vp, vp, i32, C.POINTER(dbl)]
+    lib.pmgpu_ensemble_get_info.argtypes = [vp, C.POINTER(EnsembleInfo)]
+    lib.pmgpu_ensemble_member.argtypes = [vp, i32, C.POINTER(i32), C.POINTER(i32)]
     _lib = lib
     return lib
 

@@ -326,11 +326,24 @@ static int add_pair_terms(std::vector<Launch> &groups, int list, const PairTerms
   return 0;
 }
 
+// The pair-kernel groups of an evaluation of all enabled forces: the
+// (list, merged terms) of each pair-kernel launch.
+void pair_groups(System *s, std::vector<std::pair<int, PairTerms>> *out) {
+  std::vector<Launch> groups;
+  for (auto &f : s->forces) {
+    if (!f.enabled) continue;
+    if (f.kind == FK_CUTOFF || (f.kind == FK_PME && (f.ewald_flags & PMGPU_EWALD_REAL)))
+      add_pair_terms(groups, f.list_index, f.terms);
+  }
+  out->clear();
+  for (auto &g : groups) out->push_back({g.list, g.terms});
+}
+
 // Evaluates the enabled forces (or only force `only`) at the resident
 // positions, accumulating into the (already zeroed) force planes and
 // energy accumulators.  fold = 0 (the force-only steps of an MD run) lets
 // the pair forces stay in the list's slot buffer for the next update kernel.
-static int evaluate_forces(System *s, int only, int mode, int fold = 1) {
+int evaluate_forces(System *s, int only, int mode, int fold) {
   const int want_virial = mode == PAIR_VIRIAL;
   // energy mode of the non-pair terms: 0 forces only (inner MD steps),
   // 1 + energies, 2 + energies and virial
@@ -533,14 +546,19 @@ static void constant_terms(System *s, int only, double *energies, double *virial
 
 // energies_valid = 0: a force-only evaluation, whose energies and virial
 // were not computed (recorded as zeros).
-static int read_results(System *s, int only, double *energies, double *virial, int add,
-                        int energies_valid = 1) {
+int read_results(System *s, int only, double *energies, double *virial, int add,
+                 int energies_valid) {
   PM_CUDA(cudaMemcpyAsync(s->h_acc, s->d_acc, sizeof(long long) * ACC_COUNT,
                           cudaMemcpyDeviceToHost, s->stream));
   PM_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(int), cudaMemcpyDeviceToHost,
                           s->stream));
   PM_CUDA(cudaStreamSynchronize(s->stream));
   prof_collect(s);
+  return take_results(s, only, energies, virial, add, energies_valid);
+}
+
+int take_results(System *s, int only, double *energies, double *virial, int add,
+                 int energies_valid) {
   int st = *s->h_status;
   if (st) {
     PM_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
@@ -556,6 +574,7 @@ static int read_results(System *s, int only, double *energies, double *virial, i
         nb_list_free(s, &nl);
         nl.cap = cap;
         nl.cap_set = 0;
+        nl.limit = 0;
         PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
         s->graph_version++;  // captured graphs hold the old list buffers
       }
@@ -641,7 +660,7 @@ static int fp32_peak(int device, double *tflops) {
   return PMGPU_OK;
 }
 
-static int begin_eval(System *s) {
+int begin_eval(System *s) {
   PM_CUDA(cudaMemsetAsync(s->d_acc, 0, sizeof(long long) * ACC_COUNT, s->stream));
   return PMGPU_OK;
 }
@@ -884,6 +903,16 @@ int pmgpu_system_set_positions(pmgpu_system *h, const double *pos) {
   PM_CUDA(cudaSetDevice(s->device));
   PM_CHECK(copy_in(s, s->d_pos, pos));
   s->forces_valid = 0;
+  for (auto &nl : s->lists) nl.built = 0;  // a fresh build at the next evaluation
+  return PMGPU_OK;
+}
+
+int pmgpu_system_set_step(pmgpu_system *h, long long step) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  if (step < 0) return fail(PMGPU_ERR_ARG, "step must be >= 0");
+  System *s = sysp(h);
+  PM_CHECK(run_finish(s));
+  s->step = (uint64_t)step;  // the device counter is set at the next run
   return PMGPU_OK;
 }
 int pmgpu_system_get_positions(pmgpu_system *h, double *pos) {
@@ -1283,11 +1312,15 @@ static int check_integrator(const pmgpu_integrator *it) {
   return PMGPU_OK;
 }
 
+}  // extern "C"
+
+namespace pmgpu {
+
 // Snapshot of the state a segment starts from: a neighbour list that
 // overflows mid-segment is only seen at the end of the segment (no host
 // synchronisation per step), and the segment then runs again from here
 // with the grown capacity.
-static int run_snapshot(System *s, int restore) {
+int run_snapshot(System *s, int restore) {
   size_t n3 = 3 * (size_t)std::max(1, s->n);
   if (!s->d_snap) PM_CHECK(dev_alloc(s, &s->d_snap, n3 * (2 * sizeof(double) + sizeof(long long))));
   double *snap_pos = reinterpret_cast<double *>(s->d_snap);
@@ -1307,6 +1340,10 @@ static int run_snapshot(System *s, int restore) {
   }
   return PMGPU_OK;
 }
+
+}  // namespace pmgpu
+
+extern "C" {
 
 static int run_enqueue(System *s, const pmgpu_integrator *it, long n_steps) {
   const bool lang = it->kind == PMGPU_INT_LANGEVIN_LEAPFROG;
@@ -1461,7 +1498,7 @@ int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
     const double r = reach + 5.0;
     const double cap = 4.18879 * r * r * r * dens / 8.0 / kRowParts * 1.6 + 64;
     b += ns * (16 + 16 + 32 + 4 + 4 + 8 + 24) + n * (4 + 4 + 4 + 24 + 24) + nkeys * 4 + ncol * 16 +
-         ncl * kRowParts * (16 * cap + 4);
+         ncl * kRowParts * (12 * cap + 4);
   }
   if (grid) {
     double G = (double)grid[0] * grid[1] * grid[2];
@@ -1522,6 +1559,7 @@ int pmgpu_force_stats(pmgpu_system *h, int id, pmgpu_stats *out) {
     out->cells[2] = nl.nzb;
     out->clusters = nl.nclusters;
     out->pair_kernel = nl.last_form;
+    out->list_capacity = nl.cap;
     int rb[2] = {0, 0};
     PM_CUDA(cudaMemcpyAsync(rb, nl.d_rebuild, sizeof(rb), cudaMemcpyDeviceToHost, s->stream));
     PM_CUDA(cudaStreamSynchronize(s->stream));
@@ -1563,6 +1601,16 @@ int pmgpu_debug_set_list_capacity(pmgpu_system *h, int tiles_per_row) {
   }
   s->graph_version++;
   s->forces_valid = 0;
+  return PMGPU_OK;
+}
+
+int pmgpu_debug_limit_list_rows(pmgpu_system *h, int tiles_per_row) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  if (tiles_per_row < 1) return fail(PMGPU_ERR_ARG, "tiles_per_row must be >= 1");
+  System *s = sysp(h);
+  PM_CHECK(run_finish(s));
+  for (auto &nl : s->lists) nl.limit = tiles_per_row;
+  s->graph_version++;  // captured graphs hold the build's arguments
   return PMGPU_OK;
 }
 

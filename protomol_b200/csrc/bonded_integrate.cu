@@ -245,14 +245,39 @@ struct BondedLaunch {
   int bb, ab, db;              // blocks of bonds, angles, dihedrals
 };
 
-__global__ void __launch_bounds__(kBondedThreads)
-k_bonded(BondedLaunch L, Box box, const int *__restrict__ bond_atoms,
-         const double *__restrict__ bond_prm, const int *__restrict__ angle_atoms,
-         const double *__restrict__ angle_prm, const int *__restrict__ dih_atoms,
-         const double *__restrict__ dih_prm, const int *__restrict__ imp_atoms,
-         const double *__restrict__ imp_prm, const double *__restrict__ pos, int n,
-         long long *__restrict__ force, long long *__restrict__ acc, int em) {
-  int blk = blockIdx.x;
+struct BondedArgs {
+  BondedLaunch L;
+  Box box;
+  const int *bond_atoms;
+  const double *bond_prm;
+  const int *angle_atoms;
+  const double *angle_prm;
+  const int *dih_atoms;
+  const double *dih_prm;
+  const int *imp_atoms;
+  const double *imp_prm;
+  const double *pos;
+  int n;
+  long long *force, *acc;
+  int em;
+};
+
+__device__ __forceinline__ void bonded_body(const BondedArgs &A, Blk b) {
+  const BondedLaunch &L = A.L;
+  const Box &box = A.box;
+  const int n = A.n, em = A.em;
+  const double *__restrict__ pos = A.pos;
+  long long *__restrict__ force = A.force;
+  long long *__restrict__ acc = A.acc;
+  const int *__restrict__ bond_atoms = A.bond_atoms;
+  const double *__restrict__ bond_prm = A.bond_prm;
+  const int *__restrict__ angle_atoms = A.angle_atoms;
+  const double *__restrict__ angle_prm = A.angle_prm;
+  const int *__restrict__ dih_atoms = A.dih_atoms;
+  const double *__restrict__ dih_prm = A.dih_prm;
+  const int *__restrict__ imp_atoms = A.imp_atoms;
+  const double *__restrict__ imp_prm = A.imp_prm;
+  int blk = b.x;
   if (blk < L.bb) {
     bond_term(blk * kBondedThreads + threadIdx.x, box, L.nb, bond_atoms, bond_prm, pos, n,
               force, acc, em);
@@ -275,24 +300,54 @@ k_bonded(BondedLaunch L, Box box, const int *__restrict__ bond_atoms,
                acc, ACC_IMPROPER, em);
 }
 
-int bonded_all(System *s, int bonds, int angles, int dihedrals, int impropers, int em,
-               int *launched) {
-  BondedLaunch L;
+__global__ void __launch_bounds__(kBondedThreads) k_bonded(BondedArgs a) {
+  bonded_body(a, own_blk());
+}
+
+__global__ void __launch_bounds__(kBondedThreads)
+k_bonded_batch(const BondedArgs *__restrict__ tab, const int *__restrict__ first, int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  bonded_body(tab[m], batch_blk(first, m));
+}
+
+// The bonded terms' launch arguments of a system (blocks: its grid size).
+static BondedArgs bonded_args(System *s, int bonds, int angles, int dihedrals, int impropers,
+                              int em, int *blocks) {
+  BondedArgs a;
+  BondedLaunch &L = a.L;
   L.nb = bonds ? s->n_bonds : 0;
   L.na = angles ? s->n_angles : 0;
   L.nd = dihedrals ? s->n_dihedrals : 0;
   L.ni = impropers ? s->n_impropers : 0;
-  auto blocks = [](int k) { return (k + kBondedThreads - 1) / kBondedThreads; };
-  L.bb = blocks(L.nb);
-  L.ab = blocks(L.na);
-  L.db = blocks(L.nd);
-  const int total = L.bb + L.ab + L.db + blocks(L.ni);
+  auto nbk = [](int k) { return (k + kBondedThreads - 1) / kBondedThreads; };
+  L.bb = nbk(L.nb);
+  L.ab = nbk(L.na);
+  L.db = nbk(L.nd);
+  *blocks = L.bb + L.ab + L.db + nbk(L.ni);
+  a.box = s->box;
+  a.bond_atoms = s->d_bond_atoms;
+  a.bond_prm = s->d_bond_params;
+  a.angle_atoms = s->d_angle_atoms;
+  a.angle_prm = s->d_angle_params;
+  a.dih_atoms = s->d_dihedral_atoms;
+  a.dih_prm = s->d_dihedral_params;
+  a.imp_atoms = s->d_improper_atoms;
+  a.imp_prm = s->d_improper_params;
+  a.pos = s->d_pos;
+  a.n = s->n;
+  a.force = s->d_force;
+  a.acc = s->d_acc;
+  a.em = em;
+  return a;
+}
+
+int bonded_all(System *s, int bonds, int angles, int dihedrals, int impropers, int em,
+               int *launched) {
+  int total = 0;
+  const BondedArgs a = bonded_args(s, bonds, angles, dihedrals, impropers, em, &total);
   *launched = total > 0;
   if (!total) return PMGPU_OK;
-  k_bonded<<<total, kBondedThreads, 0, s->stream>>>(
-      L, s->box, s->d_bond_atoms, s->d_bond_params, s->d_angle_atoms, s->d_angle_params,
-      s->d_dihedral_atoms, s->d_dihedral_params, s->d_improper_atoms, s->d_improper_params,
-      s->d_pos, s->n, s->d_force, s->d_acc, em);
+  k_bonded<<<total, kBondedThreads, 0, s->stream>>>(a);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
@@ -383,6 +438,11 @@ struct UpdateArgs {
   long long *fslot;
   const int *slot_of;
   int ns;
+  // the system's state
+  const double *mass;
+  double *pos, *vel;
+  long long *force;
+  int *status;
 };
 
 __global__ void k_step_set(unsigned long long *step, unsigned long long v) { *step = v; }
@@ -394,11 +454,13 @@ int set_device_step(System *s) {
 }
 
 constexpr int kUpdateThreads = 64;  // small blocks: the update is latency-bound FP64 work
-__global__ void __launch_bounds__(kUpdateThreads)
-k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos,
-         double *__restrict__ vel, long long *__restrict__ force, int *__restrict__ status) {
-  pdl_trigger();  // the list kernels after it may launch; they wait for this grid
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void update_body(const UpdateArgs &a, Blk blk) {
+  const double *__restrict__ mass = a.mass;
+  double *__restrict__ pos = a.pos;
+  double *__restrict__ vel = a.vel;
+  long long *__restrict__ force = a.force;
+  int *__restrict__ status = a.status;
+  const int i = blk.x * blockDim.x + threadIdx.x;
   const bool valid = i < a.n;
   float d2 = 0.f;
   double v[3] = {0, 0, 0}, x[3] = {0, 0, 0};
@@ -442,14 +504,14 @@ k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos
   }
   // The grid-wide decisions come before this thread's stores, so the fences
   // they take wait for no stores of the update.
-  if (a.xbuild) rebuild_decide<kUpdateThreads>(d2, a.ticket, a.rebuild, a.half_skin2, 0);
+  if (a.xbuild) rebuild_decide<kUpdateThreads>(d2, a.ticket, a.rebuild, a.half_skin2, 0, blk.n);
   if (a.step_inc) {
     // every block has read the counter before it counts itself done
     __shared__ bool last;
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
-      last = atomicAdd(&a.step_ptr[1], 1ull) == (unsigned long long)gridDim.x - 1;
+      last = atomicAdd(&a.step_ptr[1], 1ull) == (unsigned long long)blk.n - 1;
     }
     __syncthreads();
     if (last && threadIdx.x == 0) {
@@ -475,13 +537,24 @@ k_update(UpdateArgs a, const double *__restrict__ mass, double *__restrict__ pos
     for (int c = 0; c < 3; c++) force[c * a.n + i] = Fx[c];
 }
 
+__global__ void __launch_bounds__(kUpdateThreads) k_update(UpdateArgs a) {
+  pdl_trigger();  // the list kernels after it may launch; they wait for this grid
+  update_body(a, own_blk());
+}
+
+__global__ void __launch_bounds__(kUpdateThreads)
+k_update_batch(const UpdateArgs *__restrict__ tab, const int *__restrict__ first, int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  update_body(tab[m], batch_blk(first, m));
+}
+
 // phase: 0 = leapfrog first (half kick + drift), 1 = leapfrog middle (kick +
 // drift), 2 = leapfrog last (half kick), 3 = Langevin half kick + drift,
 // 4 = Langevin two half kicks (end of step s, start of step s+1) + drift,
 // 5 = Langevin closing half kick.
-int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int zero_acc,
-                         NeighborList *list) {
-  UpdateArgs a;
+int update_args(System *s, const pmgpu_integrator *it, int phase, int zero_acc,
+                NeighborList *list, UpdateArgs *out) {
+  UpdateArgs &a = *out;
   a.n = s->n;
   a.h = it->timestep_fs * kInvTimeFactor;
   a.langevin = it->kind == PMGPU_INT_LANGEVIN_LEAPFROG;
@@ -548,9 +621,22 @@ int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int z
     a.half_skin2 = hs * hs;
     list->decided = 1;
   }
+  a.mass = s->d_mass;
+  a.pos = s->d_pos;
+  a.vel = s->d_vel;
+  a.force = s->d_force;
+  a.status = s->d_status;
+  return PMGPU_OK;
+}
+
+int update_blocks(const System *s) { return (s->n + kUpdateThreads - 1) / kUpdateThreads; }
+
+int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int zero_acc,
+                         NeighborList *list) {
+  UpdateArgs a;
+  PM_CHECK(update_args(s, it, phase, zero_acc, list, &a));
   if (s->n)
-    k_update<<<(s->n + kUpdateThreads - 1) / kUpdateThreads, kUpdateThreads, 0, s->stream>>>(
-        a, s->d_mass, s->d_pos, s->d_vel, s->d_force, s->d_status);
+    k_update<<<update_blocks(s), kUpdateThreads, 0, s->stream>>>(a);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
@@ -582,6 +668,77 @@ int forces_to_host(System *s, double *out, int add) {
     for (size_t k = 0; k < h.size(); k++) out[k] += h[k];
   else
     for (size_t k = 0; k < h.size(); k++) out[k] = h[k];
+  return PMGPU_OK;
+}
+
+// ---------------------------------------------------------------- batches
+// The update kernel (every phase of an integrator) and the bonded terms of
+// an ensemble's members as batched launches.
+struct BdBatch {
+  BatchTable<UpdateArgs> upd[6][2];  // [phase][clears the accumulators]
+  BatchTable<BondedArgs> bonded[2];  // [energies]
+  pmgpu_integrator key{};
+};
+
+BdBatch *bd_batch_new() { return new BdBatch(); }
+void bd_batch_free(BdBatch *b) {
+  if (!b) return;
+  for (auto &p : b->upd)
+    for (auto &t : p) t.release();
+  for (auto &t : b->bonded) t.release();
+  delete b;
+}
+
+// Update tables of integrator it for every phase (with and without the
+// accumulator clear) and the bonded tables.  Builds host-side flags as
+// integrate_kick_drift would, so a member's list state matches.
+int bd_batch_build(BdBatch *b, System *const *m, int n, const pmgpu_integrator *it,
+                   const int *bd_flags) {
+  b->key = *it;
+  const int first_phase = it->kind == PMGPU_INT_LANGEVIN_LEAPFROG ? 3 : 0;
+  for (int ph = 0; ph < 6; ph++)
+    for (int z = 0; z < 2; z++) {
+      BatchTable<UpdateArgs> &t = b->upd[ph][z];
+      t.clear();
+      if (ph < first_phase || ph >= first_phase + 3) continue;
+      for (int k = 0; k < n; k++) {
+        UpdateArgs a;
+        // update_args marks the list as decided and its slot buffer as taken;
+        // those flags are set again by every step of the batched run
+        PM_CHECK(update_args(m[k], it, ph, z, &m[k]->lists[0], &a));
+        t.add(a, update_blocks(m[k]));
+      }
+      PM_CUDA(t.upload());
+    }
+  for (int e = 0; e < 2; e++) {
+    BatchTable<BondedArgs> &t = b->bonded[e];
+    t.clear();
+    for (int k = 0; k < n; k++) {
+      int blocks = 0;
+      const int *f = bd_flags + 4 * k;
+      const BondedArgs a = bonded_args(m[k], f[0], f[1], f[2], f[3], e, &blocks);
+      t.add(a, blocks);
+    }
+    PM_CUDA(t.upload());
+  }
+  return PMGPU_OK;
+}
+
+int bd_batch_update(BdBatch *b, int phase, int zero_acc, cudaStream_t st, long long *launched) {
+  BatchTable<UpdateArgs> &t = b->upd[phase][zero_acc ? 1 : 0];
+  if (!t.members() || !t.total()) return PMGPU_OK;
+  *launched += 1;
+  k_update_batch<<<t.total(), kUpdateThreads, 0, st>>>(t.d, t.d_first, t.members());
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+int bd_batch_bonded(BdBatch *b, int em, cudaStream_t st, long long *launched) {
+  BatchTable<BondedArgs> &t = b->bonded[em ? 1 : 0];
+  if (!t.members() || !t.total()) return PMGPU_OK;
+  *launched += 1;
+  k_bonded_batch<<<t.total(), kBondedThreads, 0, st>>>(t.d, t.d_first, t.members());
+  PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
 

@@ -61,15 +61,27 @@ struct ListGrid {
   double inv[3];   // 1 / column width (x, y), 1 / z-bin height
 };
 
-__global__ void k_bin(ListGrid g, const double *__restrict__ pos,
-                      const int *__restrict__ rebuild, int *__restrict__ key,
-                      unsigned *__restrict__ zkey, int *__restrict__ col_count,
-                      double *__restrict__ offset, double *__restrict__ xbuild,
-                      int *__restrict__ status) {
-  pdl_wait();  // the predecessor's writes are visible from here on
-  pdl_trigger();
-  if (!*rebuild) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+struct BinArgs {
+  ListGrid g;
+  const double *pos;
+  const int *rebuild;
+  int *key;
+  unsigned *zkey;
+  int *col_count;
+  double *offset, *xbuild;
+  int *status;
+};
+__device__ __forceinline__ void bin_body(const BinArgs &A, Blk b) {
+  const ListGrid &g = A.g;
+  const double *__restrict__ pos = A.pos;
+  int *__restrict__ key = A.key;
+  unsigned *__restrict__ zkey = A.zkey;
+  int *__restrict__ col_count = A.col_count;
+  double *__restrict__ offset = A.offset;
+  double *__restrict__ xbuild = A.xbuild;
+  int *__restrict__ status = A.status;
+  if (!*A.rebuild) return;
+  const int i = b.x * blockDim.x + threadIdx.x;
   if (i >= g.n) return;
   const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
   double w[3];
@@ -95,6 +107,16 @@ __global__ void k_bin(ListGrid g, const double *__restrict__ pos,
   xbuild[3 * i] = x;
   xbuild[3 * i + 1] = y;
   xbuild[3 * i + 2] = z;
+}
+__global__ void k_bin(BinArgs a) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
+  bin_body(a, own_blk());
+}
+__global__ void k_bin_batch(const BinArgs *__restrict__ tab, const int *__restrict__ first,
+                            int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  bin_body(tab[m], batch_blk(first, m));
 }
 
 // Exclusive scan of value(k), k < count, by one block; write(k, prefix)
@@ -138,13 +160,24 @@ __device__ int block_scan(int count, V value, W write, int *warp_tot, int *carry
 // One block: column starts (unpadded, for the scatter) and padded column
 // bases (every column a whole number of 8-atom clusters); slots past the
 // padded total are marked empty.
-__global__ void __launch_bounds__(1024)
-k_scan_cols(const int *__restrict__ rebuild, const int *__restrict__ col_count, int ncol,
-            int *__restrict__ col_u, int *__restrict__ cursor, int *__restrict__ col_base,
-            int *__restrict__ key_start, int nkeys, int *__restrict__ sorted, int ns_max) {
-  pdl_wait();  // the predecessor's writes are visible from here on
-  pdl_trigger();
-  if (!*rebuild) return;
+struct ScanArgs {
+  const int *rebuild;
+  const int *col_count;
+  int ncol;
+  int *col_u, *cursor, *col_base, *key_start;
+  int nkeys;
+  int *sorted;
+  int ns_max;
+};
+__device__ __forceinline__ void scan_body(const ScanArgs &A) {
+  const int *__restrict__ col_count = A.col_count;
+  const int ncol = A.ncol, nkeys = A.nkeys, ns_max = A.ns_max;
+  int *__restrict__ col_u = A.col_u;
+  int *__restrict__ cursor = A.cursor;
+  int *__restrict__ col_base = A.col_base;
+  int *__restrict__ key_start = A.key_start;
+  int *__restrict__ sorted = A.sorted;
+  if (!*A.rebuild) return;
   __shared__ int warp_tot[32];
   __shared__ int carry;
   block_scan(
@@ -163,17 +196,38 @@ k_scan_cols(const int *__restrict__ rebuild, const int *__restrict__ col_count, 
   }
   for (int s = padded + threadIdx.x; s < ns_max; s += blockDim.x) sorted[s] = -1;
 }
-
-__global__ void k_scatter(const int *__restrict__ rebuild, int n,
-                          const int *__restrict__ key, const int *__restrict__ col_u,
-                          int *__restrict__ cursor, int *__restrict__ unsorted) {
+__global__ void __launch_bounds__(1024) k_scan_cols(ScanArgs a) {
   pdl_wait();  // the predecessor's writes are visible from here on
   pdl_trigger();
-  if (!*rebuild) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int c = key[i];
-  unsorted[col_u[c] + atomicAdd(&cursor[c], 1)] = i;
+  scan_body(a);
+}
+__global__ void __launch_bounds__(1024)
+k_scan_cols_batch(const ScanArgs *__restrict__ tab, const int *__restrict__ first, int nm) {
+  scan_body(tab[batch_member(first, nm, blockIdx.x)]);
+}
+
+struct ScatterArgs {
+  const int *rebuild;
+  int n;
+  const int *key, *col_u;
+  int *cursor, *unsorted;
+};
+__device__ __forceinline__ void scatter_body(const ScatterArgs &A, Blk b) {
+  if (!*A.rebuild) return;
+  int i = b.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const int c = A.key[i];
+  A.unsorted[A.col_u[c] + atomicAdd(&A.cursor[c], 1)] = i;
+}
+__global__ void k_scatter(ScatterArgs a) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
+  scatter_body(a, own_blk());
+}
+__global__ void k_scatter_batch(const ScatterArgs *__restrict__ tab, const int *__restrict__ first,
+                                int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  scatter_body(tab[m], batch_blk(first, m));
 }
 
 // One block per column: bitonic sort of (z, atom) in shared memory, the
@@ -181,18 +235,30 @@ __global__ void k_scatter(const int *__restrict__ rebuild, int n,
 // index (first slot of every bin).  A column above kColCap atoms flags
 // ST_CELL_OVERFLOW and is left empty.
 constexpr int kSortThreads = 256;
-__global__ void __launch_bounds__(kSortThreads)
-k_sort_cols(const int *__restrict__ rebuild, int nzb, float inv_z,
-            int *__restrict__ col_count, const int *__restrict__ col_u,
-            const int *__restrict__ col_base, const int *__restrict__ unsorted,
-            const unsigned *__restrict__ zkey, int *__restrict__ sorted,
-            int *__restrict__ slot_of, int *__restrict__ key_start,
-            int *__restrict__ status) {
-  pdl_wait();  // the predecessor's writes are visible from here on
-  pdl_trigger();
-  if (!*rebuild) return;
+struct SortArgs {
+  const int *rebuild;
+  int nzb;
+  float inv_z;
+  int *col_count;
+  const int *col_u, *col_base, *unsorted;
+  const unsigned *zkey;
+  int *sorted, *slot_of, *key_start, *status;
+};
+__device__ __forceinline__ void sort_body(const SortArgs &A, Blk b) {
+  const int nzb = A.nzb;
+  const float inv_z = A.inv_z;
+  int *__restrict__ col_count = A.col_count;
+  const int *__restrict__ col_u = A.col_u;
+  const int *__restrict__ col_base = A.col_base;
+  const int *__restrict__ unsorted = A.unsorted;
+  const unsigned *__restrict__ zkey = A.zkey;
+  int *__restrict__ sorted = A.sorted;
+  int *__restrict__ slot_of = A.slot_of;
+  int *__restrict__ key_start = A.key_start;
+  int *__restrict__ status = A.status;
+  if (!*A.rebuild) return;
   __shared__ unsigned long long keys[kColCap];
-  const int col = blockIdx.x;
+  const int col = b.x;
   int m = col_count[col];
   const int base = col_base[col], pend = col_base[col + 1];
   if (m > kColCap) {
@@ -247,22 +313,48 @@ k_sort_cols(const int *__restrict__ rebuild, int nzb, float inv_z,
   __syncthreads();
   if (threadIdx.x == 0) col_count[col] = 0;  // ready for the next build
 }
+__global__ void __launch_bounds__(kSortThreads) k_sort_cols(SortArgs a) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
+  sort_body(a, own_blk());
+}
+__global__ void __launch_bounds__(kSortThreads)
+k_sort_cols_batch(const SortArgs *__restrict__ tab, const int *__restrict__ first, int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  sort_body(tab[m], batch_blk(first, m));
+}
 
 // Per-step gather of the sorted coordinates: xw = x - offset keeps every
 // atom in the image it had at the last build, so tile images stay valid.
 // Padding slots get far-away positions and no charge; no tile pairs them.
+struct GatherArgs {
+  int ns;
+  const double *pos, *offset;
+  const int *sorted;
+  const double *charge;
+  const int *type, *mol;
+  float4 *xhi, *xlo;
+  double4 *xw;
+  int *mol_s;
+  const int *rebuild;
+  float4 *bb;
+};
 template <bool MIXED>
-__global__ void k_gather(int ns, const double *__restrict__ pos,
-                         const double *__restrict__ offset,
-                         const int *__restrict__ sorted,
-                         const double *__restrict__ charge,
-                         const int *__restrict__ type, const int *__restrict__ mol,
-                         float4 *__restrict__ xhi, float4 *__restrict__ xlo,
-                         double4 *__restrict__ xw, int *__restrict__ mol_s,
-                         const int *__restrict__ rebuild, float4 *__restrict__ bb) {
-  pdl_wait();  // the predecessor's writes are visible from here on
-  pdl_trigger();
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void gather_slots_body(const GatherArgs &A, Blk b) {
+  const int ns = A.ns;
+  const double *__restrict__ pos = A.pos;
+  const double *__restrict__ offset = A.offset;
+  const int *__restrict__ sorted = A.sorted;
+  const double *__restrict__ charge = A.charge;
+  const int *__restrict__ type = A.type;
+  const int *__restrict__ mol = A.mol;
+  float4 *__restrict__ xhi = A.xhi;
+  float4 *__restrict__ xlo = A.xlo;
+  double4 *__restrict__ xw = A.xw;
+  int *__restrict__ mol_s = A.mol_s;
+  const int *__restrict__ rebuild = A.rebuild;
+  float4 *__restrict__ bb = A.bb;
+  const int s = b.x * blockDim.x + threadIdx.x;
   const bool in = s < ns;
   const int i = in ? sorted[s] : -1;
   float hx = 0.f, hy = 0.f, hz = 0.f;
@@ -308,6 +400,18 @@ __global__ void k_gather(int ns, const double *__restrict__ pos,
     }
   }
 }
+template <bool MIXED>
+__global__ void k_gather(GatherArgs a) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  pdl_trigger();
+  gather_slots_body<MIXED>(a, own_blk());
+}
+template <bool MIXED>
+__global__ void k_gather_batch(const GatherArgs *__restrict__ tab, const int *__restrict__ first,
+                               int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  gather_slots_body<MIXED>(tab[m], batch_blk(first, m));
+}
 
 // Decides whether this evaluation rebuilds the list (rebuild_decide) from
 // the current positions: first build, forced, or an atom lies more than
@@ -328,7 +432,7 @@ k_check_rebuild(int n, const double *__restrict__ pos, const double *__restrict_
                  dz = pos[3 * i + 2] - xbuild[3 * i + 2];
     d2 = (float)(dx * dx + dy * dy + dz * dz);
   }
-  rebuild_decide<kCheckThreads>(d2, ticket, rebuild, half_skin2, force);
+  rebuild_decide<kCheckThreads>(d2, ticket, rebuild, half_skin2, force, (int)gridDim.x);
 }
 
 // ---------------------------------------------------------- list build
@@ -342,7 +446,8 @@ struct TileBuildArgs {
   float H2[3];       // half box edges (minimal-image test)
   float reach2;      // FP32 pair test radius^2 (reach plus a rounding margin)
   float cull;        // cluster / column culling radius (wider margin)
-  int cap;
+  int cap;           // tiles per row in the buffer (the row stride)
+  int limit;         // tiles a row may hold (cap, or a lower test limit)
   const int *excl_start, *excl_partner, *excl_class;
 };
 
@@ -374,13 +479,30 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
 // OneAtomPairTwo.h:47-53) clears fully excluded pairs and marks modified
 // ones.  Tiles are appended in a fixed order (range, cluster index), so
 // the list is deterministic.
-__global__ void __launch_bounds__(kBuildWarps * 32, 3)
-k_build_tiles(TileBuildArgs a, int *__restrict__ rebuild, const int *__restrict__ sorted,
-              const int *__restrict__ start, const float4 *__restrict__ xhi,
-              const int *__restrict__ mol_s, const float4 *__restrict__ bb,
-              uint4 *__restrict__ tiles, int *__restrict__ tile_count,
-              int *__restrict__ status) {
-  pdl_wait();  // the predecessor's writes are visible from here on
+struct BuildArgs {
+  TileBuildArgs a;
+  int *rebuild;
+  const int *sorted, *start;
+  const float4 *xhi;
+  const int *mol_s;
+  const float4 *bb;
+  uint2 *tiles;
+  unsigned *tmod;
+  int *tile_count;
+  int *status;
+};
+__device__ __forceinline__ void build_body(const BuildArgs &B, Blk blk) {
+  const TileBuildArgs &a = B.a;
+  int *__restrict__ rebuild = B.rebuild;
+  const int *__restrict__ sorted = B.sorted;
+  const int *__restrict__ start = B.start;
+  const float4 *__restrict__ xhi = B.xhi;
+  const int *__restrict__ mol_s = B.mol_s;
+  const float4 *__restrict__ bb = B.bb;
+  uint2 *__restrict__ tiles = B.tiles;
+  unsigned *__restrict__ tmod = B.tmod;
+  int *__restrict__ tile_count = B.tile_count;
+  int *__restrict__ status = B.status;
   if (!*rebuild) return;
   constexpr unsigned kAll = 0xffffffffu;
   // this warp's staging of candidate j clusters (up to 32 of them)
@@ -389,8 +511,8 @@ k_build_tiles(TileBuildArgs a, int *__restrict__ rebuild, const int *__restrict_
   __shared__ int st_h[kBuildWarps][32], st_c[kBuildWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   // the warps of the (resident) grid stride over the rows
-  for (int rw = blockIdx.x * kBuildWarps + wib; rw < a.nclusters * kRowParts;
-       rw += gridDim.x * kBuildWarps) {
+  for (int rw = blk.x * kBuildWarps + wib; rw < a.nclusters * kRowParts;
+       rw += blk.n * kBuildWarps) {
   const int ci = rw / kRowParts, part = rw - ci * kRowParts;
   const float4 l0 = bb[4 * ci], h0 = bb[4 * ci + 1], l1 = bb[4 * ci + 2], h1 = bb[4 * ci + 3];
   if (l0.w + l1.w == 0.f) {
@@ -422,7 +544,8 @@ k_build_tiles(TileBuildArgs a, int *__restrict__ rebuild, const int *__restrict_
   const float4 pi = xhi[islot];
   const int mi = mol_s[islot];
   const float R = a.cull, R2 = a.cull * a.cull;
-  uint4 *row = tiles + (size_t)rw * a.cap;
+  uint2 *row = tiles + (size_t)rw * a.cap;
+  unsigned *rowmod = tmod + (size_t)rw * a.cap;
   int count = 0;
 
   // the candidate test of up to four staged j clusters (lane (il, cq)
@@ -482,10 +605,13 @@ k_build_tiles(TileBuildArgs a, int *__restrict__ rebuild, const int *__restrict_
     if (wr) {
       const int idx = count + __popc(wm & ((1u << lane) - 1u));
       const int bsel = q == 0 ? bq[0] : (q == 1 ? bq[1] : (q == 2 ? bq[2] : bq[3]));
-      if (idx < a.cap)
-        row[idx] = make_uint4((uint32_t)st_h[wib][bsel] |
-                                  ((uint32_t)st_c[wib][bsel] << kShiftBits),
-                              im, mm, 0u);
+      if (idx < a.limit) {
+        row[idx] = make_uint2((uint32_t)st_h[wib][bsel] |
+                                  ((uint32_t)st_c[wib][bsel] << kShiftBits) |
+                                  (mm ? kModFlag : 0u),
+                              im);
+        if (mm) rowmod[idx] = mm;
+      }
     }
     count += __popc(wm);
   };
@@ -651,17 +777,26 @@ k_build_tiles(TileBuildArgs a, int *__restrict__ rebuild, const int *__restrict_
     }
   }
   if (lane == 0) {
-    if (count > a.cap) {
-      // the row keeps its first cap tiles; the host grows the capacity to
+    if (count > a.limit) {
+      // the row keeps its first limit tiles; the host grows the capacity to
       // at least the largest row's need and repeats the work
       atomicOr(status, ST_LIST_OVERFLOW);
       atomicMax(rebuild + 2, count);
-      count = a.cap;
+      count = a.limit;
     }
     tile_count[rw] = count;
   }
   __syncwarp();  // the next row reuses the staging
   }  // rows
+}
+__global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_tiles(BuildArgs a) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  build_body(a, own_blk());
+}
+__global__ void __launch_bounds__(kBuildWarps * 32, 3)
+k_build_tiles_batch(const BuildArgs *__restrict__ tab, const int *__restrict__ first, int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  build_body(tab[m], batch_blk(first, m));
 }
 
 }  // namespace pmgpu
@@ -757,7 +892,8 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   PM_CHECK(dev_alloc(s, &nl->d_bb, sizeof(float4) * 2 * (ns / 4)));
   PM_CHECK(dev_alloc(s, &nl->d_fslot, sizeof(long long) * 3 * ns));
   PM_CUDA(cudaMemsetAsync(nl->d_fslot, 0, sizeof(long long) * 3 * ns, s->stream));
-  PM_CHECK(dev_alloc(s, &nl->d_tiles, sizeof(uint4) * (size_t)cap * nl->nrows));
+  PM_CHECK(dev_alloc(s, &nl->d_tiles, sizeof(uint2) * (size_t)cap * nl->nrows));
+  PM_CHECK(dev_alloc(s, &nl->d_tmod, sizeof(unsigned) * (size_t)cap * nl->nrows));
   PM_CHECK(dev_alloc(s, &nl->d_tile_count, sizeof(int) * std::max(1, nl->nrows)));
   PM_CUDA(cudaMemsetAsync(nl->d_tile_count, 0, sizeof(int) * std::max(1, nl->nrows),
                           s->stream));
@@ -773,8 +909,8 @@ int nb_list_free(System *s, NeighborList *nl) {
   void *ptrs[] = {nl->d_key, nl->d_zkey, nl->d_unsorted, nl->d_col_count, nl->d_col_u,
                   nl->d_col_cursor, nl->d_col_base, nl->d_key_start, nl->d_sorted,
                   nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
-                  nl->d_bb, nl->d_fslot, nl->d_slot_of, nl->d_tiles, nl->d_tile_count,
-                  nl->d_maxdisp,
+                  nl->d_bb, nl->d_fslot, nl->d_slot_of, nl->d_tiles, nl->d_tmod,
+                  nl->d_tile_count, nl->d_maxdisp,
                   nl->d_rebuild};
   for (void *p : ptrs) dev_free(s, p);
   nl->d_key = nl->d_unsorted = nl->d_col_count = nl->d_col_u = nl->d_col_cursor = nullptr;
@@ -785,10 +921,69 @@ int nb_list_free(System *s, NeighborList *nl) {
   nl->d_xhi = nl->d_xlo = nl->d_bb = nullptr;
   nl->d_xw = nullptr;
   nl->d_tiles = nullptr;
+  nl->d_tmod = nullptr;
   nl->d_fslot = nullptr;
   nl->d_slot_of = nullptr;
   nl->d_maxdisp = nullptr;
   return PMGPU_OK;
+}
+
+// Launch arguments of a list's per-step kernels (the sort, the gather and
+// the tile build).
+struct ListArgs {
+  BinArgs bin;
+  ScanArgs scan;
+  ScatterArgs scatter;
+  SortArgs sort;
+  GatherArgs gather;
+  BuildArgs build;
+};
+
+static void list_args(System *s, NeighborList *nl, ListArgs *L) {
+  ListGrid g;
+  g.box = s->box;
+  g.n = s->n;
+  g.periodic = s->box.periodic;
+  g.ncx = nl->ncx; g.ncy = nl->ncy; g.nzb = nl->nzb;
+  for (int a = 0; a < 3; a++) {
+    g.lo[a] = nl->lo[a];
+    g.inv[a] = 1.0 / nl->cs[a];
+  }
+  L->bin = BinArgs{g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_zkey, nl->d_col_count,
+                   nl->d_offset, nl->d_xbuild, s->d_status};
+  L->scan = ScanArgs{nl->d_rebuild, nl->d_col_count, nl->ncol, nl->d_col_u, nl->d_col_cursor,
+                     nl->d_col_base, nl->d_key_start, nl->nkeys, nl->d_sorted, nl->ns_max};
+  L->scatter = ScatterArgs{nl->d_rebuild, s->n, nl->d_key, nl->d_col_u, nl->d_col_cursor,
+                           nl->d_unsorted};
+  L->sort = SortArgs{nl->d_rebuild, nl->nzb, (float)(1.0 / nl->cs[2]), nl->d_col_count,
+                     nl->d_col_u, nl->d_col_base, nl->d_unsorted, nl->d_zkey, nl->d_sorted,
+                     nl->d_slot_of, nl->d_key_start, s->d_status};
+  L->gather = GatherArgs{nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted, s->d_charge,
+                         s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
+                         nl->d_rebuild, nl->d_bb};
+  TileBuildArgs ba;
+  ba.nclusters = nl->nclusters;
+  ba.periodic = s->box.periodic;
+  ba.ncx = nl->ncx; ba.ncy = nl->ncy; ba.nzb = nl->nzb;
+  for (int c = 0; c < 3; c++) {
+    ba.lo[c] = (float)nl->lo[c];
+    ba.cs[c] = (float)nl->cs[c];
+    ba.L[c] = (float)s->box.e[c];
+    ba.H2[c] = (float)s->box.H2[c];
+  }
+  // FP32 pair test with a margin well above its rounding error; wider for
+  // the box culling
+  const double r1 = nl->reach + 0.01;
+  ba.reach2 = (float)(r1 * r1);
+  ba.cull = (float)(nl->reach + 0.05);
+  ba.cap = nl->cap;
+  ba.limit = nl->limit > 0 ? std::min(nl->limit, nl->cap) : nl->cap;
+  ba.excl_start = s->d_excl_start;
+  ba.excl_partner = s->d_excl_partner;
+  ba.excl_class = s->d_excl_class;
+  L->build = BuildArgs{ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi,
+                       nl->d_mol_s, nl->d_bb, nl->d_tiles, nl->d_tmod, nl->d_tile_count,
+                       s->d_status};
 }
 
 // Sort + (conditional) list build + per-step gather.  Never synchronises
@@ -806,37 +1001,20 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
     PM_CUDA(launch_pdl(k_check_rebuild, nb, kCheckThreads, 0, st, n, s->d_pos, nl->d_xbuild,
                        nl->d_maxdisp, nl->d_rebuild, hs * hs, (force_rebuild || first) ? 1 : 0));
   nl->decided = 0;
-  ListGrid g;
-  g.box = s->box;
-  g.n = n;
-  g.periodic = s->box.periodic;
-  g.ncx = nl->ncx; g.ncy = nl->ncy; g.nzb = nl->nzb;
-  for (int a = 0; a < 3; a++) {
-    g.lo[a] = nl->lo[a];
-    g.inv[a] = 1.0 / nl->cs[a];
-  }
   {
     cudaStream_t q = st;  // the rebuild-only sort
     // each kernel of the chain launches as a programmatic dependent of the
     // one before, so on the steps that keep the list their early exits
     // overlap their launches
-    PM_CUDA(launch_pdl(k_bin, nb, T, 0, q, g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_zkey,
-                       nl->d_col_count, nl->d_offset, nl->d_xbuild, s->d_status));
-    PM_CUDA(launch_pdl(k_scan_cols, 1, 1024, 0, q, nl->d_rebuild, nl->d_col_count, nl->ncol,
-                       nl->d_col_u, nl->d_col_cursor, nl->d_col_base, nl->d_key_start,
-                       nl->nkeys, nl->d_sorted, nl->ns_max));
-    PM_CUDA(launch_pdl(k_scatter, nb, T, 0, q, nl->d_rebuild, n, nl->d_key, nl->d_col_u,
-                       nl->d_col_cursor, nl->d_unsorted));
-    PM_CUDA(launch_pdl(k_sort_cols, nl->ncol, kSortThreads, 0, q, nl->d_rebuild, nl->nzb,
-                       (float)(1.0 / nl->cs[2]), nl->d_col_count, nl->d_col_u, nl->d_col_base,
-                       nl->d_unsorted, nl->d_zkey, nl->d_sorted, nl->d_slot_of,
-                       nl->d_key_start,
-                       s->d_status));
+    ListArgs la;
+    list_args(s, nl, &la);
+    PM_CUDA(launch_pdl(k_bin, nb, T, 0, q, la.bin));
+    PM_CUDA(launch_pdl(k_scan_cols, 1, 1024, 0, q, la.scan));
+    PM_CUDA(launch_pdl(k_scatter, nb, T, 0, q, la.scatter));
+    PM_CUDA(launch_pdl(k_sort_cols, nl->ncol, kSortThreads, 0, q, la.sort));
+    PM_CUDA(launch_pdl(s->precision == PMGPU_PREC_MIXED ? k_gather<true> : k_gather<false>, nbs,
+                       T, 0, st, la.gather));
   }
-  PM_CUDA(launch_pdl(s->precision == PMGPU_PREC_MIXED ? k_gather<true> : k_gather<false>, nbs,
-                     T, 0, st, nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted, s->d_charge,
-                     s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
-                     nl->d_rebuild, nl->d_bb));
   PM_CUDA(cudaGetLastError());
   nl->built = 1;  // the slot order exists from here on
   return PMGPU_OK;
@@ -847,25 +1025,8 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
 int nb_build(System *s, NeighborList *nl) {
   if (s->n == 0) return PMGPU_OK;
   cudaStream_t st = s->stream;
-  TileBuildArgs ba;
-  ba.nclusters = nl->nclusters;
-  ba.periodic = s->box.periodic;
-  ba.ncx = nl->ncx; ba.ncy = nl->ncy; ba.nzb = nl->nzb;
-  for (int c = 0; c < 3; c++) {
-    ba.lo[c] = (float)nl->lo[c];
-    ba.cs[c] = (float)nl->cs[c];
-    ba.L[c] = (float)s->box.e[c];
-    ba.H2[c] = (float)s->box.H2[c];
-  }
-  // FP32 pair test with a margin well above its rounding error; wider for
-  // the box culling
-  const double r1 = nl->reach + 0.01;
-  ba.reach2 = (float)(r1 * r1);
-  ba.cull = (float)(nl->reach + 0.05);
-  ba.cap = nl->cap;
-  ba.excl_start = s->d_excl_start;
-  ba.excl_partner = s->d_excl_partner;
-  ba.excl_class = s->d_excl_class;
+  ListArgs la;
+  list_args(s, nl, &la);
   // a grid of resident blocks whose warps stride over the rows: cheap to
   // launch on the steps that keep the list
   static int sms = 0;
@@ -873,9 +1034,7 @@ int nb_build(System *s, NeighborList *nl) {
                    cudaSuccess || sms <= 0))
     sms = 148;
   const int nblk = std::max(1, std::min((nl->nrows + kBuildWarps - 1) / kBuildWarps, 3 * sms));
-  PM_CUDA(launch_pdl(k_build_tiles, nblk, kBuildWarps * 32, 0, st, ba, nl->d_rebuild,
-                     nl->d_sorted, nl->d_key_start, nl->d_xhi, nl->d_mol_s, nl->d_bb,
-                     nl->d_tiles, nl->d_tile_count, s->d_status));
+  PM_CUDA(launch_pdl(k_build_tiles, nblk, kBuildWarps * 32, 0, st, la.build));
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }
@@ -936,6 +1095,7 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   a.excl_partner = s->d_excl_partner;
   a.excl_class = s->d_excl_class;
   a.tiles = nl->d_tiles;
+  a.tmod = nl->d_tmod;
   a.tile_count = nl->d_tile_count;
   a.xhi = nl->d_xhi;
   a.xlo = nl->d_xlo;
@@ -1009,7 +1169,7 @@ static int jl_splits(int nclusters) {
     const char *e = std::getenv("PMGPU_JL_SPLITS");
     forced = e ? std::max(0, std::atoi(e)) : 0;
   }
-  if (forced) return std::min(forced, 8);
+  if (forced) return std::min(forced, kJlMaxSplits);
   const long long want = 3LL * sms * 3 * kJlWarps;
   return (int)std::max(1LL, std::min(8LL, (want + nclusters / 2) / std::max(1, nclusters)));
 }
@@ -1120,8 +1280,8 @@ int nb_pair_forces(System *s, NeighborList *nl, const PairTerms &t, int mode, in
 
 int nb_fold_slots(System *s, NeighborList *nl) {
   if (!nl->slot_pending || s->n == 0) return PMGPU_OK;
-  PM_CUDA(launch_pdl(k_slot_forces, (nl->ns_max + 255) / 256, 256, 0, s->stream, nl->ns_max,
-                     s->n, nl->d_sorted, nl->d_fslot, s->d_force));
+  PM_CUDA(launch_pdl(k_slot_forces, (nl->ns_max + 255) / 256, 256, 0, s->stream,
+                     SlotArgs{nl->ns_max, s->n, nl->d_sorted, nl->d_fslot, s->d_force}));
   PM_CUDA(cudaGetLastError());
   nl->slot_pending = 0;
   return PMGPU_OK;
@@ -1130,6 +1290,271 @@ int nb_fold_slots(System *s, NeighborList *nl) {
 int fold_pending_slots(System *s) {
   for (auto &nl : s->lists) PM_CHECK(nb_fold_slots(s, &nl));
   return PMGPU_OK;
+}
+
+// ---------------------------------------------------------------- batches
+// The list and pair kernels of an ensemble's members as batched launches:
+// one launch per kernel over every member's part (each member with the
+// arguments and grid its own launch would have), so a member's results are
+// those of its own launches.
+struct NbBatch {
+  BatchTable<BinArgs> bin;
+  BatchTable<ScanArgs> scan;
+  BatchTable<ScatterArgs> scatter;
+  BatchTable<SortArgs> sort;
+  BatchTable<GatherArgs> gather;
+  BatchTable<BuildArgs> build;
+  int terms = 0;
+  int form = PMGPU_PAIRK_GENERIC;  // the specialised form of the jl members
+  int smem_lj = 1;
+  BatchTable<PairArgs<float>> jl;      // members with the specialised force-only form
+  BatchTable<PairArgs<float>> gforce;  // members without one (force-only, generic kernel)
+  BatchTable<PairArgs<float>> energy;  // every member on energy steps
+  BatchTable<SlotArgs> slots;
+  std::vector<int> has_form;           // per member: 1 if in jl
+  std::vector<PairArgs<float>> base;   // per member: its force-only pair arguments
+  BatchTable<PairArgs<float>> probe;   // a timing launch (nb_batch_time_jl)
+};
+
+NbBatch *nb_batch_new() { return new NbBatch(); }
+void nb_batch_free(NbBatch *b) {
+  if (!b) return;
+  b->bin.release(); b->scan.release(); b->scatter.release(); b->sort.release();
+  b->gather.release(); b->build.release(); b->jl.release(); b->gforce.release();
+  b->energy.release(); b->slots.release(); b->probe.release();
+  delete b;
+}
+
+// The specialised force-only form a member's pair launch takes
+// (launch_pairs_t), or PMGPU_PAIRK_GENERIC.
+static int special_form(const PairArgs<float> &a, const PairTerms &t) {
+  if (!a.same_cut || a.minimal_image) return PMGPU_PAIRK_GENERIC;
+  const int lk = spec_kind(t.lj_sw), ck = spec_kind(t.coul_sw);
+  if (t.mask == (TERM_LJ | TERM_EWALD) && !t.exact_erf && lk == PMGPU_SW_C2)
+    return PMGPU_PAIRK_LJC2_EWALD;
+  if (t.mask == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C2)
+    return PMGPU_PAIRK_LJC2_COULC2;
+  if (t.mask == (TERM_LJ | TERM_COUL) && lk == PMGPU_SW_C2 && ck == PMGPU_SW_C1)
+    return PMGPU_PAIRK_LJC2_COULC1;
+  return PMGPU_PAIRK_GENERIC;
+}
+
+// splits[k] > 0 sets member k's jl splits (the tiles of each i cluster
+// divided over that many warps), 0 or splits == NULL the single-system
+// choice.
+int nb_batch_build(NbBatch *b, System *const *m, int n, const PairTerms *terms,
+                   const int *splits) {
+  static int sms = 0;
+  if (!sms && (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m[0]->device) !=
+                   cudaSuccess || sms <= 0))
+    sms = 148;
+  b->bin.clear(); b->scan.clear(); b->scatter.clear(); b->sort.clear(); b->gather.clear();
+  b->build.clear(); b->jl.clear(); b->gforce.clear(); b->energy.clear(); b->slots.clear();
+  b->has_form.assign(n, 0);
+  b->base.assign(n, PairArgs<float>());
+  b->terms = terms[0].mask;
+  b->form = PMGPU_PAIRK_GENERIC;
+  b->smem_lj = 1;
+  for (int k = 0; k < n; k++) {
+    System *s = m[k];
+    NeighborList *nl = &s->lists[0];
+    if (s->precision != PMGPU_PREC_MIXED || terms[k].mask != b->terms)
+      return fail(PMGPU_ERR_UNSUPPORTED, "ensemble members need one precision and one force set");
+    ListArgs la;
+    list_args(s, nl, &la);
+    const int T = 256;
+    const int nb = (s->n + T - 1) / T, nbs = (nl->ns_max + T - 1) / T;
+    b->bin.add(la.bin, nb);
+    b->scan.add(la.scan, 1);
+    b->scatter.add(la.scatter, nb);
+    b->sort.add(la.sort, nl->ncol);
+    b->gather.add(la.gather, nbs);
+    b->build.add(la.build, std::max(1, std::min((nl->nrows + kBuildWarps - 1) / kBuildWarps,
+                                                3 * sms)));
+    PairArgs<float> a;
+    fill_pair_args<float>(a, s, nl, terms[k]);
+    a.count_pairs = 0;
+    const int form = special_form(a, terms[k]);
+    if (form != PMGPU_PAIRK_GENERIC) {
+      if (b->form != PMGPU_PAIRK_GENERIC && b->form != form)
+        return fail(PMGPU_ERR_UNSUPPORTED, "ensemble members need one pair-kernel form");
+      b->form = form;
+      b->smem_lj = b->smem_lj && a.ntypes <= kJlMaxTypes;
+      PairArgs<float> fa = a;
+      fa.splits = splits && splits[k] > 0 ? std::min(splits[k], kJlMaxSplits)
+                                          : jl_splits(fa.nclusters);
+      b->base[k] = fa;
+      b->jl.add(fa, (int)(((long long)fa.nclusters * fa.splits + kJlWarps - 1) / kJlWarps));
+      b->has_form[k] = 1;
+    } else {
+      b->gforce.add(a, (int)(((long long)a.nclusters * a.splits + kPairWarps - 1) / kPairWarps));
+    }
+    PairArgs<float> ea = a;
+    ea.energy_only = form != PMGPU_PAIRK_GENERIC;
+    b->energy.add(ea, (int)(((long long)a.nclusters * a.splits + kPairWarps - 1) / kPairWarps));
+    b->slots.add(SlotArgs{nl->ns_max, s->n, nl->d_sorted, nl->d_fslot, s->d_force},
+                 (nl->ns_max + 255) / 256);
+  }
+  BatchTable<PairArgs<float>> *pt[] = {&b->jl, &b->gforce, &b->energy};
+  PM_CUDA(b->bin.upload());
+  PM_CUDA(b->scan.upload());
+  PM_CUDA(b->scatter.upload());
+  PM_CUDA(b->sort.upload());
+  PM_CUDA(b->gather.upload());
+  PM_CUDA(b->build.upload());
+  for (auto *t : pt) PM_CUDA(t->upload());
+  PM_CUDA(b->slots.upload());
+  return PMGPU_OK;
+}
+
+// The (conditional) sort, the per-step gather and the (conditional) tile
+// build of every member (nb_prepare after an update's rebuild decision,
+// then nb_build).
+int nb_batch_list(NbBatch *b, cudaStream_t st, long long *launched) {
+  const int nm = b->bin.members();
+  if (!nm) return PMGPU_OK;
+  *launched += 4 + (b->bin.total() > 0) + (b->scatter.total() > 0);
+  if (b->bin.total()) k_bin_batch<<<b->bin.total(), 256, 0, st>>>(b->bin.d, b->bin.d_first, nm);
+  k_scan_cols_batch<<<b->scan.total(), 1024, 0, st>>>(b->scan.d, b->scan.d_first, nm);
+  if (b->scatter.total())
+    k_scatter_batch<<<b->scatter.total(), 256, 0, st>>>(b->scatter.d, b->scatter.d_first, nm);
+  k_sort_cols_batch<<<b->sort.total(), kSortThreads, 0, st>>>(b->sort.d, b->sort.d_first, nm);
+  k_gather_batch<true><<<b->gather.total(), 256, 0, st>>>(b->gather.d, b->gather.d_first, nm);
+  k_build_tiles_batch<<<b->build.total(), kBuildWarps * 32, 0, st>>>(b->build.d,
+                                                                      b->build.d_first, nm);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+template <int TERMS>
+static int launch_generic_batch(BatchTable<PairArgs<float>> &t, int mode, cudaStream_t st) {
+  if (!t.members() || !t.total()) return 0;
+  const int T = kPairWarps * 32;
+  if (mode == PAIR_FORCE)
+    k_pairs_batch<float, TERMS, PAIR_FORCE, GenericSpec><<<t.total(), T, 0, st>>>(t.d, t.d_first,
+                                                                                   t.members());
+  else
+    k_pairs_batch<float, TERMS, PAIR_ENERGY, GenericSpec><<<t.total(), T, 0, st>>>(
+        t.d, t.d_first, t.members());
+  return 1;
+}
+
+static int generic_batch(BatchTable<PairArgs<float>> &t, int terms, int mode, cudaStream_t st) {
+  switch (terms) {
+    case TERM_LJ: return launch_generic_batch<TERM_LJ>(t, mode, st);
+    case TERM_COUL: return launch_generic_batch<TERM_COUL>(t, mode, st);
+    case TERM_LJ | TERM_COUL: return launch_generic_batch<TERM_LJ | TERM_COUL>(t, mode, st);
+    case TERM_EWALD: return launch_generic_batch<TERM_EWALD>(t, mode, st);
+    default: return launch_generic_batch<TERM_LJ | TERM_EWALD>(t, mode, st);
+  }
+}
+
+template <int TERMS, typename SPEC>
+static void jl_batch(NbBatch *b, BatchTable<PairArgs<float>> &t, cudaStream_t st) {
+  if (b->smem_lj)
+    k_pairs_jl_batch<TERMS, SPEC, true><<<t.total(), kJlWarps * 32, 0, st>>>(t.d, t.d_first,
+                                                                            t.members());
+  else
+    k_pairs_jl_batch<TERMS, SPEC, false><<<t.total(), kJlWarps * 32, 0, st>>>(t.d, t.d_first,
+                                                                             t.members());
+}
+
+// The pair forces of every member: force-only (the inner MD steps; the
+// slot-ordered forces stay for the next update kernel) or with energies
+// (the last step; the slot forces are folded in), as nb_pair_forces does
+// for each member.
+static int jl_form(NbBatch *b, BatchTable<PairArgs<float>> &t, cudaStream_t st) {
+  if (!t.members() || !t.total()) return 0;
+  switch (b->form) {
+    case PMGPU_PAIRK_LJC2_EWALD:
+      jl_batch<TERM_LJ | TERM_EWALD, PairSpec<PMGPU_SW_C2, -1, 0>>(b, t, st);
+      break;
+    case PMGPU_PAIRK_LJC2_COULC2:
+      jl_batch<TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C2, -1>>(b, t, st);
+      break;
+    default:
+      jl_batch<TERM_LJ | TERM_COUL, PairSpec<PMGPU_SW_C2, PMGPU_SW_C1, -1>>(b, t, st);
+      break;
+  }
+  return 1;
+}
+
+int nb_batch_pairs(NbBatch *b, int mode, cudaStream_t st, long long *launched) {
+  *launched += jl_form(b, b->jl, st);
+  if (mode == PAIR_FORCE) {
+    *launched += generic_batch(b->gforce, b->terms, PAIR_FORCE, st);
+  } else {
+    *launched += generic_batch(b->energy, b->terms, PAIR_ENERGY, st);
+    if (b->slots.total()) {
+      k_slot_forces_batch<<<b->slots.total(), 256, 0, st>>>(b->slots.d, b->slots.d_first,
+                                                           b->slots.members());
+      *launched += 1;
+    }
+  }
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+// Device milliseconds of one force-only jl launch over every member with
+// the specialised form, member k with splits[k] warps per i cluster (0:
+// the single-system choice), averaged over reps launches after one warm-up
+// launch.  The launches add into the members' slot buffers, which are
+// cleared again, so the members' state is unchanged; the members' lists
+// must be built and their slot buffers empty.
+int nb_batch_time_jl(NbBatch *b, System *const *m, int n, const int *splits, int reps,
+                     cudaStream_t st, double *ms) {
+  *ms = 0.0;
+  b->probe.clear();
+  for (int k = 0; k < n && k < (int)b->has_form.size(); k++) {
+    if (!b->has_form[k]) continue;
+    PairArgs<float> a = b->base[k];
+    a.splits = splits[k] > 0 ? std::min(splits[k], kJlMaxSplits) : jl_splits(a.nclusters);
+    b->probe.add(a, (int)(((long long)a.nclusters * a.splits + kJlWarps - 1) / kJlWarps));
+  }
+  if (!b->probe.members()) return PMGPU_OK;
+  PM_CUDA(b->probe.upload());
+  cudaEvent_t e0, e1;
+  PM_CUDA(cudaEventCreate(&e0));
+  PM_CUDA(cudaEventCreate(&e1));
+  jl_form(b, b->probe, st);
+  cudaEventRecord(e0, st);
+  for (int r = 0; r < reps; r++) jl_form(b, b->probe, st);
+  cudaEventRecord(e1, st);
+  cudaError_t err = cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  PM_CUDA(err);
+  PM_CUDA(cudaGetLastError());
+  for (int k = 0; k < n && k < (int)b->has_form.size(); k++) {
+    if (!b->has_form[k]) continue;
+    NeighborList &nl = m[k]->lists[0];
+    PM_CUDA(cudaMemsetAsync(nl.d_fslot, 0, sizeof(long long) * 3 * (size_t)nl.ns_max, st));
+  }
+  PM_CUDA(cudaStreamSynchronize(st));
+  *ms = reps > 0 ? t / reps : 0.0;
+  return PMGPU_OK;
+}
+
+// The jl splits member k takes (its own choice when splits[k] is 0) and
+// its i-cluster count; -1 / 0 for a member without the specialised form.
+void nb_batch_member_info(NbBatch *b, int k, int *splits, int *clusters) {
+  const bool f = k >= 0 && k < (int)b->has_form.size() && b->has_form[k];
+  *splits = f ? b->base[k].splits : -1;
+  *clusters = f ? b->base[k].nclusters : 0;
+}
+
+// Host-side state of the members after a batched step's list and pair
+// work, as nb_prepare / nb_pair_forces leave it.
+void nb_batch_mark(NbBatch *b, System *const *m, int n, int mode) {
+  for (int k = 0; k < n; k++) {
+    NeighborList &nl = m[k]->lists[0];
+    nl.built = 1;
+    nl.decided = 0;
+    nl.slot_pending = mode == PAIR_FORCE;
+    nl.last_form = b->has_form[k] ? b->form : PMGPU_PAIRK_GENERIC;
+  }
 }
 
 // ProtoMol cell assignment with a given cellsize on the resident positions

@@ -49,7 +49,8 @@ struct PairArgs {
   const int *sorted;
   const double *pos;     // raw positions (exact re-test)
   const int *excl_start, *excl_partner, *excl_class;
-  const uint4 *tiles;
+  const uint2 *tiles;
+  const unsigned *tmod;  // modified masks of flagged tiles
   const int *tile_count;
   const float4 *xhi, *xlo;
   const double4 *xw;
@@ -383,8 +384,7 @@ __device__ __forceinline__ long long fixed_force(double v) { return to_fixed(v, 
 // FP64 re-test near a cutoff); the tile mask carries the list's exclusion
 // and modified (scaled 1-4) status.
 template <typename Real, int TERMS, int MODE, typename SPEC>
-__global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPEC>::blocks)
-    k_pairs(PairArgs<Real> a) {
+__device__ __forceinline__ void pairs_body(const PairArgs<Real> &a, Blk blk) {
   constexpr bool MIXED = sizeof(Real) == 4;
   constexpr bool ENERGY = MODE != PAIR_FORCE;
   constexpr bool VIRIAL = MODE == PAIR_VIRIAL;
@@ -406,8 +406,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
   // work items (i cluster, share of its tiles); the warps of a smaller
   // grid stride over them
   const int nitems = a.nclusters * a.splits;
-  for (int gw = blockIdx.x * kPairWarps + (threadIdx.x >> 5); gw < nitems;
-       gw += gridDim.x * kPairWarps) {
+  for (int gw = blk.x * kPairWarps + (threadIdx.x >> 5); gw < nitems;
+       gw += blk.n * kPairWarps) {
   const int ci = gw / a.splits, sp = gw - ci * a.splits;
   // the cluster's tiles are its kRowParts rows read one after the other;
   // this warp takes tiles [t0, t1) of that sequence
@@ -449,11 +449,14 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
     rowlen = p == 1 ? c4.y : (p == 2 ? c4.z : c4.w);
   }
   for (int left = t1 - t0; left > 0;) {
-    const uint4 *row = a.tiles + (size_t)(kRowParts * ci + p) * a.cap;
+    const size_t row0 = (size_t)(kRowParts * ci + p) * a.cap;
+    const uint2 *row = a.tiles + row0;
     const int ke = min(rowlen, kb + left);
     left -= ke - kb;
   for (int k = kb; k < ke; k++) {
-    const uint4 tile = __ldg(row + k);
+    const uint2 t2 = __ldg(row + k);
+    const uint3 tile = make_uint3(t2.x, t2.y,
+                                  (t2.x & kModFlag) ? __ldg(a.tmod + row0 + k) : 0u);
     const int hj = (int)(tile.x & kJMask);
     const int sh = (int)((tile.x >> kShiftBits) & kShiftMask);
     if (__any_sync(kAll, sh != cur)) {  // tiles are grouped by image
@@ -654,6 +657,33 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
   }
 }
 
+// The launch arguments of a batched launch's member, copied into shared
+// memory by the block (every thread reads them many times).
+template <typename A>
+__device__ __forceinline__ const A &batch_args_shared(const A *__restrict__ tab, int m,
+                                                      unsigned char *raw) {
+  static_assert(sizeof(A) % 4 == 0, "argument structs are whole words");
+  const int *src = reinterpret_cast<const int *>(tab + m);
+  int *dst = reinterpret_cast<int *>(raw);
+  for (int k = threadIdx.x; k < (int)(sizeof(A) / 4); k += blockDim.x) dst[k] = __ldg(src + k);
+  __syncthreads();
+  return *reinterpret_cast<const A *>(raw);
+}
+
+template <typename Real, int TERMS, int MODE, typename SPEC>
+__global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPEC>::blocks)
+    k_pairs(PairArgs<Real> a) {
+  pairs_body<Real, TERMS, MODE, SPEC>(a, own_blk());
+}
+
+template <typename Real, int TERMS, int MODE, typename SPEC>
+__global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPEC>::blocks)
+    k_pairs_batch(const PairArgs<Real> *__restrict__ tab, const int *__restrict__ first, int nm) {
+  __shared__ __align__(16) unsigned char raw[sizeof(PairArgs<Real>)];
+  const int m = batch_member(first, nm, blockIdx.x);
+  pairs_body<Real, TERMS, MODE, SPEC>(batch_args_shared(tab, m, raw), batch_blk(first, m));
+}
+
 // ---------------------------------------------------------------------------
 // Force-only FP32 pair kernel of the inner MD steps, j atoms on the lanes.
 //
@@ -677,8 +707,11 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
 // pairs (rare), so the accepted set is the reference's.
 constexpr int kJlWarps = 8;
 constexpr int kJlMaxTypes = 16;  // LJ tables staged in shared memory up to this many types
+constexpr int kJlMaxSplits = 16;  // warps one i cluster's tiles may be divided over
 
-// The eight pairs of one lane's j atom with the cluster's i atoms.
+// The eight pairs of one lane's j atom with the cluster's i atoms; mi
+// holds the pairs within max_hi (the queue's test), so a pair of mi beyond
+// max_lo is a band pair.
 template <int TERMS, typename SPEC, bool MOD, bool SMEM_LJ>
 __device__ __forceinline__ void jl_pairs8(const PairArgs<float> &a, const float4 *s_lj,
                                           const float4 *xi, const int *ti, float rjx, float rjy,
@@ -692,7 +725,7 @@ __device__ __forceinline__ void jl_pairs8(const PairArgs<float> &a, const float4
     const float r2 = dx * dx + dy * dy + dz * dz;
     const bool on = (mi >> il) & 1u;
     const bool act = on && r2 <= a.max_lo;
-    band |= (on && !act && r2 <= a.max_hi) ? (1u << il) : 0u;
+    band |= (on && !act) ? (1u << il) : 0u;
     npairs += act;
     const float rr = act ? r2 : 1.f;
     const float4 p = SMEM_LJ ? s_lj[ti[il] + tj] : __ldg(a.lj32 + ti[il] + tj);
@@ -708,23 +741,104 @@ __device__ __forceinline__ void jl_pairs8(const PairArgs<float> &a, const float4
   }
 }
 
+// Per-warp queue of j lanes that have at least one i atom in range: the
+// candidates of each batch of 8 tiles are tested (the eight FP32 distances,
+// cheap against the pair arithmetic) and only the active ones are queued;
+// the pair arithmetic runs on full warps of queued lanes.  About half of a
+// tile's j lanes have no i atom within the cutoff, so this halves the
+// pair evaluations.  The queue keeps the tile order, so the sums are a
+// function of the list alone.
+constexpr int kJlQueue = 64;
+struct JlQueue {
+  float x[kJlQueue], y[kJlQueue], z[kJlQueue], q[kJlQueue];
+  int t[kJlQueue];     // j type
+  int m[kJlQueue];     // i atoms in range (bits 0-7), modified pairs (bits 8-15)
+  int slot[kJlQueue];  // j slot
+};
+
+// The pair arithmetic of up to 32 queued j lanes (lane < cnt) against the
+// warp's i cluster.
 template <int TERMS, typename SPEC, bool SMEM_LJ>
-__global__ void __launch_bounds__(kJlWarps * 32, 3) k_pairs_jl(PairArgs<float> a) {
+__device__ __forceinline__ void jl_process(const PairArgs<float> &a, const float4 *s_lj,
+                                           const float4 *xi, const int *ti, const int *oi,
+                                           const JlQueue &qu, int cnt, int lane, int ci,
+                                           float (&fi)[8][3], int &npairs) {
+  constexpr unsigned kAll = 0xffffffffu;
+  unsigned mi = 0u, mm = 0u;
+  int jslot = 0, tj = 0;
+  float rjx = 0.f, rjy = 0.f, rjz = 0.f, qj = 0.f;
+  if (lane < cnt) {
+    rjx = qu.x[lane];
+    rjy = qu.y[lane];
+    rjz = qu.z[lane];
+    qj = qu.q[lane];
+    tj = qu.t[lane];
+    const int m = qu.m[lane];
+    mi = (unsigned)m & 0xFFu;
+    mm = ((unsigned)m >> 8) & 0xFFu;
+    jslot = qu.slot[lane];
+  }
+  float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+  unsigned band = 0u;
+  // modified (scaled 1-4) pairs are rare: batches without any take the
+  // path without their selects
+  if (__any_sync(kAll, mm != 0u))
+    jl_pairs8<TERMS, SPEC, true, SMEM_LJ>(a, s_lj, xi, ti, rjx, rjy, rjz, qj, tj, mi, mm, fi,
+                                          fjx, fjy, fjz, band, npairs);
+  else
+    jl_pairs8<TERMS, SPEC, false, SMEM_LJ>(a, s_lj, xi, ti, rjx, rjy, rjz, qj, tj, mi, mm, fi,
+                                           fjx, fjy, fjz, band, npairs);
+  // pairs within the rounding band of the cutoff: the exact FP64 test
+  // (rare; their i forces go out as atomics, so this path keeps none of
+  // the register-held sums live)
+  if (__any_sync(kAll, band != 0u)) {
+    const int oj = band ? a.sorted[jslot] : -1;
+    while (band) {
+      const int il = __ffs(band) - 1;
+      band &= band - 1u;
+      const float4 x = xi[il];
+      const float dx = rjx - x.x, dy = rjy - x.y, dz = rjz - x.z;
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      if (exact_r2(a, oi[il], oj, (double)dx, (double)dy, (double)dz) > a.max_cut2) continue;
+      const float4 p = SMEM_LJ ? s_lj[ti[il] + tj] : __ldg(a.lj32 + ti[il] + tj);
+      const float f = pair_force_p<float, TERMS, SPEC, true>(a, p, r2, x.w * qj, (mm >> il) & 1u);
+      fjx = fmaf(dx, f, fjx);
+      fjy = fmaf(dy, f, fjy);
+      fjz = fmaf(dz, f, fjz);
+      long long *di = a.fslot + 8 * ci + il;
+      red_add(di, fixed_force(-dx * f));
+      red_add(di + a.ns, fixed_force(-dy * f));
+      red_add(di + 2 * (size_t)a.ns, fixed_force(-dz * f));
+      npairs++;
+    }
+  }
+  if (mi) {
+    long long *dst = a.fslot + jslot;
+    red_add(dst, fixed_force(fjx));
+    red_add(dst + a.ns, fixed_force(fjy));
+    red_add(dst + 2 * (size_t)a.ns, fixed_force(fjz));
+  }
+}
+
+template <int TERMS, typename SPEC, bool SMEM_LJ>
+__device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk) {
   constexpr unsigned kAll = 0xffffffffu;
   __shared__ float4 s_lj[SMEM_LJ ? kJlMaxTypes * kJlMaxTypes : 1];
   __shared__ float4 s_xi[kJlWarps][8];   // i atoms from the reference point, charge
   __shared__ int s_ti[kJlWarps][8];      // i type * ntypes
   __shared__ int s_oi[kJlWarps][8];      // i atom (-1: padding)
   __shared__ double s_wc[kJlWarps][3];   // reference point (FP64)
+  __shared__ JlQueue s_q[kJlWarps];
   if (SMEM_LJ) {
     for (int k = threadIdx.x; k < a.ntypes * a.ntypes; k += blockDim.x) s_lj[k] = a.lj32[k];
     __syncthreads();
   }
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int tb = lane >> 2, jl = lane & 3;
+  JlQueue &qu = s_q[wib];
   int npairs = 0;
   const int nitems = a.nclusters * a.splits;
-  for (int gw = blockIdx.x * kJlWarps + wib; gw < nitems; gw += gridDim.x * kJlWarps) {
+  for (int gw = blk.x * kJlWarps + wib; gw < nitems; gw += blk.n * kJlWarps) {
     const int ci = gw / a.splits, sp = gw - ci * a.splits;
     static_assert(kRowParts == 4, "one int4 of row counts per cluster");
     const int4 c4 = *reinterpret_cast<const int4 *>(a.tile_count + kRowParts * ci);
@@ -750,72 +864,80 @@ __global__ void __launch_bounds__(kJlWarps * 32, 3) k_pairs_jl(PairArgs<float> a
     float fi[8][3];
 #pragma unroll
     for (int k = 0; k < 8; k++) fi[k][0] = fi[k][1] = fi[k][2] = 0.f;
+    int qn = 0;  // queued j lanes
     for (int b0 = t0; b0 < t1; b0 += 8) {
       const int idx = b0 + tb;
-      unsigned mi = 0u, mm = 0u;
-      int jslot = 0, tj = 0;
+      unsigned act = 0u;
+      int m = 0, jslot = 0, tj = 0;
       float rjx = 0.f, rjy = 0.f, rjz = 0.f, qj = 0.f;
       if (idx < t1) {
         // tile idx of the cluster's row parts read one after the other
         const int p = (idx >= p1) + (idx >= p2) + (idx >= p3);
         const int off = idx - (p == 0 ? 0 : (p == 1 ? p1 : (p == 2 ? p2 : p3)));
-        const uint4 tile = __ldg(a.tiles + (size_t)(kRowParts * ci + p) * a.cap + off);
+        const size_t ti0 = (size_t)(kRowParts * ci + p) * a.cap + off;
+        const uint2 tile = __ldg(a.tiles + ti0);
         const int hj = (int)(tile.x & kJMask);
         const int sh = (int)((tile.x >> kShiftBits) & kShiftMask);
-        mi = (tile.y >> (8 * jl)) & 0xFFu;
-        mm = (tile.z >> (8 * jl)) & 0xFFu;
+        const unsigned mi = (tile.y >> (8 * jl)) & 0xFFu;
+        const unsigned mm =
+            (tile.x & kModFlag) ? (__ldg(a.tmod + ti0) >> (8 * jl)) & 0xFFu : 0u;
         jslot = 4 * hj + jl;
-        const double4 wj = a.xw[jslot];
-        // the j atom in the tile's image (d = xj + s L - xi), from the
-        // reference point
-        rjx = (float)((wj.x + (double)((sh & 3) - 1) * a.box.e[0]) - s_wc[wib][0]);
-        rjy = (float)((wj.y + (double)(((sh >> 2) & 3) - 1) * a.box.e[1]) - s_wc[wib][1]);
-        rjz = (float)((wj.z + (double)(((sh >> 4) & 3) - 1) * a.box.e[2]) - s_wc[wib][2]);
-        qj = (float)wj.w;
-        tj = __float_as_int(__ldg(&a.xlo[jslot].w));
-      }
-      float fjx = 0.f, fjy = 0.f, fjz = 0.f;
-      unsigned band = 0u;
-      // modified (scaled 1-4) pairs are rare: batches without any take the
-      // path without their selects
-      if (__any_sync(kAll, mm != 0u))
-        jl_pairs8<TERMS, SPEC, true, SMEM_LJ>(a, s_lj, xi, ti, rjx, rjy, rjz, qj, tj, mi, mm, fi,
-                                              fjx, fjy, fjz, band, npairs);
-      else
-        jl_pairs8<TERMS, SPEC, false, SMEM_LJ>(a, s_lj, xi, ti, rjx, rjy, rjz, qj, tj, mi, mm,
-                                               fi, fjx, fjy, fjz, band, npairs);
-      // pairs within the rounding band of the cutoff: the exact FP64 test
-      // (rare; their i forces go out as atomics, so this path keeps none of
-      // the register-held sums live)
-      if (__any_sync(kAll, band != 0u)) {
-        const int oj = band ? a.sorted[jslot] : -1;
-        while (band) {
-          const int il = __ffs(band) - 1;
-          band &= band - 1u;
-          const float4 x = xi[il];
-          const float dx = rjx - x.x, dy = rjy - x.y, dz = rjz - x.z;
-          const float r2 = dx * dx + dy * dy + dz * dz;
-          if (exact_r2(a, s_oi[wib][il], oj, (double)dx, (double)dy, (double)dz) > a.max_cut2)
-            continue;
-          const float4 p = SMEM_LJ ? s_lj[ti[il] + tj] : __ldg(a.lj32 + ti[il] + tj);
-          const float f = pair_force_p<float, TERMS, SPEC, true>(a, p, r2, x.w * qj,
-                                                                 (mm >> il) & 1u);
-          fjx = fmaf(dx, f, fjx);
-          fjy = fmaf(dy, f, fjy);
-          fjz = fmaf(dz, f, fjz);
-          long long *di = a.fslot + 8 * ci + il;
-          red_add(di, fixed_force(-dx * f));
-          red_add(di + a.ns, fixed_force(-dy * f));
-          red_add(di + 2 * (size_t)a.ns, fixed_force(-dz * f));
-          npairs++;
+        if (mi) {
+          const double4 wj = a.xw[jslot];
+          // the j atom in the tile's image (d = xj + s L - xi), from the
+          // reference point; the image offsets are exact (-L, 0 or L)
+          const int sx = sh & 3, sy = (sh >> 2) & 3, sz = (sh >> 4) & 3;
+          const double ox = sx == 1 ? 0.0 : (sx == 0 ? -a.box.e[0] : a.box.e[0]);
+          const double oy = sy == 1 ? 0.0 : (sy == 0 ? -a.box.e[1] : a.box.e[1]);
+          const double oz = sz == 1 ? 0.0 : (sz == 0 ? -a.box.e[2] : a.box.e[2]);
+          rjx = (float)((wj.x + ox) - s_wc[wib][0]);
+          rjy = (float)((wj.y + oy) - s_wc[wib][1]);
+          rjz = (float)((wj.z + oz) - s_wc[wib][2]);
+          qj = (float)wj.w;
+          tj = __float_as_int(__ldg(&a.xlo[jslot].w));
+          // the i atoms in range of this j atom (the band pairs included)
+#pragma unroll
+          for (int il = 0; il < 8; il++) {
+            const float4 x = xi[il];
+            const float dx = rjx - x.x, dy = rjy - x.y, dz = rjz - x.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            act |= (((mi >> il) & 1u) && r2 <= a.max_hi) ? (1u << il) : 0u;
+          }
+          m = (int)(act | ((mm & act) << 8));
         }
       }
-      if (mi) {
-        long long *dst = a.fslot + jslot;
-        red_add(dst, fixed_force(fjx));
-        red_add(dst + a.ns, fixed_force(fjy));
-        red_add(dst + 2 * (size_t)a.ns, fixed_force(fjz));
+      const unsigned vote = __ballot_sync(kAll, act != 0u);
+      if (act) {
+        const int at = qn + __popc(vote & ((1u << lane) - 1u));
+        qu.x[at] = rjx;
+        qu.y[at] = rjy;
+        qu.z[at] = rjz;
+        qu.q[at] = qj;
+        qu.t[at] = tj;
+        qu.m[at] = m;
+        qu.slot[at] = jslot;
       }
+      qn += __popc(vote);
+      if (qn >= 32) {
+        __syncwarp();
+        jl_process<TERMS, SPEC, SMEM_LJ>(a, s_lj, xi, ti, s_oi[wib], qu, 32, lane, ci, fi, npairs);
+        __syncwarp();  // every lane has read its entry before the rest moves up
+        qn -= 32;
+        if (lane < qn) {
+          qu.x[lane] = qu.x[32 + lane];
+          qu.y[lane] = qu.y[32 + lane];
+          qu.z[lane] = qu.z[32 + lane];
+          qu.q[lane] = qu.q[32 + lane];
+          qu.t[lane] = qu.t[32 + lane];
+          qu.m[lane] = qu.m[32 + lane];
+          qu.slot[lane] = qu.slot[32 + lane];
+        }
+        __syncwarp();
+      }
+    }
+    if (qn > 0) {
+      __syncwarp();
+      jl_process<TERMS, SPEC, SMEM_LJ>(a, s_lj, xi, ti, s_oi[wib], qu, qn, lane, ci, fi, npairs);
     }
     // the i forces summed over the lanes: lane l ends with the totals of i
     // atom (l >> 2) & 7 and writes component l & 3
@@ -838,12 +960,33 @@ __global__ void __launch_bounds__(kJlWarps * 32, 3) k_pairs_jl(PairArgs<float> a
   }
 }
 
+template <int TERMS, typename SPEC, bool SMEM_LJ>
+__global__ void __launch_bounds__(kJlWarps * 32, 3) k_pairs_jl(PairArgs<float> a) {
+  pairs_jl_body<TERMS, SPEC, SMEM_LJ>(a, own_blk());
+}
+
+template <int TERMS, typename SPEC, bool SMEM_LJ>
+__global__ void __launch_bounds__(kJlWarps * 32, 3)
+    k_pairs_jl_batch(const PairArgs<float> *__restrict__ tab, const int *__restrict__ first,
+                     int nm) {
+  __shared__ __align__(16) unsigned char raw[sizeof(PairArgs<float>)];
+  const int m = batch_member(first, nm, blockIdx.x);
+  pairs_jl_body<TERMS, SPEC, SMEM_LJ>(batch_args_shared(tab, m, raw), batch_blk(first, m));
+}
+
 // Adds the forces accumulated by list slot into the atoms' forces and
 // clears the slot buffer for the next launch.
-__global__ void k_slot_forces(int ns, int n, const int *__restrict__ sorted,
-                              long long *__restrict__ fslot, long long *__restrict__ force) {
-  pdl_wait();  // the predecessor's writes are visible from here on
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+struct SlotArgs {
+  int ns, n;
+  const int *sorted;
+  long long *fslot, *force;
+};
+__device__ __forceinline__ void slot_forces_body(const SlotArgs &A, Blk b) {
+  const int ns = A.ns, n = A.n;
+  const int *__restrict__ sorted = A.sorted;
+  long long *__restrict__ fslot = A.fslot;
+  long long *__restrict__ force = A.force;
+  const int s = b.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   const int i = sorted[s];
   if (i < 0) return;
@@ -855,6 +998,15 @@ __global__ void k_slot_forces(int ns, int n, const int *__restrict__ sorted,
       fslot[(size_t)c * ns + s] = 0;
     }
   }
+}
+__global__ void k_slot_forces(SlotArgs a) {
+  pdl_wait();  // the predecessor's writes are visible from here on
+  slot_forces_body(a, own_blk());
+}
+__global__ void k_slot_forces_batch(const SlotArgs *__restrict__ tab, const int *__restrict__ first,
+                                    int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  slot_forces_body(tab[m], batch_blk(first, m));
 }
 
 }  // namespace pmgpu

@@ -320,10 +320,11 @@ __device__ __forceinline__ void red_add(long long *p, long long v) {
 // when it is forced or some atom moved more than half the skin.
 // rebuild[0] is the flag, rebuild[1] counts builds; ticket[0] orders the
 // blocks, ticket[1] holds the running maximum (FP32 bits).  Every thread of
-// the block must call it; blockDim.x is THREADS.
+// the block must call it; blockDim.x is THREADS and nblocks the number of
+// blocks of this system's launch.
 template <int THREADS>
 __device__ __forceinline__ void rebuild_decide(float d2, unsigned *ticket, int *rebuild,
-                                               float half_skin2, int force) {
+                                               float half_skin2, int force, int nblocks) {
   __shared__ float wmax[THREADS / 32];
   __shared__ bool last;
   if (!(d2 == d2)) d2 = 3.0e38f;  // NaN: rebuild (the binning flags it)
@@ -336,7 +337,7 @@ __device__ __forceinline__ void rebuild_decide(float d2, unsigned *ticket, int *
     for (int w = 1; w < THREADS / 32; w++) m = fmaxf(m, wmax[w]);
     if (m > 0.f) atomicMax(&ticket[1], __float_as_uint(m));
     __threadfence();
-    last = atomicAdd(&ticket[0], 1u) == gridDim.x - 1;
+    last = atomicAdd(&ticket[0], 1u) == (unsigned)nblocks - 1;
   }
   __syncthreads();
   if (last && threadIdx.x == 0) {
@@ -347,6 +348,32 @@ __device__ __forceinline__ void rebuild_decide(float d2, unsigned *ticket, int *
     if (r) rebuild[1] += 1;
     ticket[0] = 0u;
   }
+}
+
+// ------------------------------------------------------- batched launches
+// A kernel body runs either as its own launch (one system) or inside a
+// batched launch over the members of an ensemble, one after another in the
+// grid.  Blk is the block's index and the block count of its system's part.
+struct Blk {
+  int x, n;
+};
+__device__ __forceinline__ Blk own_blk() { return Blk{(int)blockIdx.x, (int)gridDim.x}; }
+
+// The member of a batched launch that block b belongs to: first[m] is the
+// first block of member m (first[nm] is the grid size), members with no
+// blocks are skipped.
+__device__ __forceinline__ int batch_member(const int *__restrict__ first, int nm, int b) {
+  int lo = 0, hi = nm;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(first + mid) <= b) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+__device__ __forceinline__ Blk batch_blk(const int *__restrict__ first, int m) {
+  const int f = __ldg(first + m);
+  return Blk{(int)blockIdx.x - f, __ldg(first + m + 1) - f};
 }
 
 template <typename T>

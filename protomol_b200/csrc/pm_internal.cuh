@@ -5,7 +5,9 @@
 #include <cufft.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -48,14 +50,18 @@ enum { ACC_COULOMB = 0, ACC_LJ, ACC_BOND, ACC_ANGLE, ACC_DIHEDRAL,
 enum { ST_LIST_OVERFLOW = 1, ST_NONFINITE = 2, ST_CELL_OVERFLOW = 4,
        ST_BAD_BOX = 8 };
 
-// Tile layout (uint4): x = j cluster (bits 0..23) | periodic image of the
-// j cluster as three 2-bit fields (sx+1, sy+1, sz+1) at bits 24..29;
-// y = interaction mask, z = modified (scaled 1-4) mask, bit l for lane l =
-// (i atom l & 7, j atom l >> 3).  Fully excluded minimal-image pairs are
-// cleared from the interaction mask when the list is built.
+// Tile layout (uint2, 8 bytes): x = j cluster (bits 0..23) | periodic image
+// of the j cluster as three 2-bit fields (sx+1, sy+1, sz+1) at bits 24..29
+// | kModFlag (bit 30) when the tile has modified (scaled 1-4) pairs;
+// y = interaction mask, bit l for lane l = (i atom l & 7, j atom l >> 3).
+// The modified mask of a flagged tile is in a parallel array (tmod) at the
+// tile's index; it is read only for flagged tiles.  Fully excluded
+// minimal-image pairs are cleared from the interaction mask when the list
+// is built.
 constexpr uint32_t kJMask = 0xFFFFFFu;
 constexpr int kShiftBits = 24;
 constexpr uint32_t kShiftMask = 0x3Fu;
+constexpr uint32_t kModFlag = 1u << 30;
 constexpr int kZeroShift = 1 | (1 << 2) | (1 << 4);
 __host__ __device__ constexpr int shift_code(int sx, int sy, int sz) {
   return (sx + 1) | ((sy + 1) << 2) | ((sz + 1) << 4);
@@ -142,6 +148,7 @@ struct NeighborList {
   // a force-only MD step left its pair forces in d_fslot for the next update
   // kernel to add; until then d_force lacks them (nb_fold_slots adds them)
   int slot_pending = 0;
+  int limit = 0;  // tiles a row may hold below cap (a test hook; 0: cap)
   int last_form = PMGPU_PAIRK_GENERIC;  // pair-kernel form of the last launch
   long long builds = 0;
   // device
@@ -163,7 +170,8 @@ struct NeighborList {
   float4 *d_bb = nullptr;        // 2 per 4-atom cluster: lower, upper corner
   long long *d_fslot = nullptr;  // 3 planes of ns_max: pair forces by slot (fixed point)
   int *d_slot_of = nullptr;  // atom -> slot of the current order (rebuild steps write it)
-  uint4 *d_tiles = nullptr;      // nrows rows of cap tiles (row r: cluster r / kRowParts)
+  uint2 *d_tiles = nullptr;      // nrows rows of cap tiles (row r: cluster r / kRowParts)
+  unsigned *d_tmod = nullptr;    // modified masks of the flagged tiles, same indexing
   int *d_tile_count = nullptr;   // nrows
   unsigned int *d_maxdisp = nullptr;  // rebuild check: block ticket, max displacement^2 bits
   int *d_rebuild = nullptr;      // rebuild flag, build count, largest row need after an overflow
@@ -351,9 +359,100 @@ inline int dev_alloc(System *s, T **p, size_t bytes) {
 }
 void dev_free(System *s, void *p);
 
+// ------------------------------------------------------- batched launches
+// One batched launch's arguments: the launch arguments of every member of an
+// ensemble and the first block of each member in the grid (first[n] is the
+// grid size), copied to the device once; a kernel's batched form finds its
+// member by the block index (batch_member in pm_device.cuh).
+template <typename A>
+struct BatchTable {
+  std::vector<A> h;
+  std::vector<int> first = std::vector<int>(1, 0);
+  A *d = nullptr;
+  int *d_first = nullptr;
+  size_t cap = 0;
+  void clear() {
+    h.clear();
+    first.assign(1, 0);
+  }
+  void add(const A &a, int blocks) {
+    h.push_back(a);
+    first.push_back(first.back() + blocks);
+  }
+  int total() const { return first.back(); }
+  int members() const { return (int)h.size(); }
+  // copies the host tables to the device (synchronously: the host vectors
+  // may change afterwards)
+  cudaError_t upload() {
+    if (h.size() > cap) {
+      release();
+      cap = h.size();
+      cudaError_t e = cudaMalloc(&d, sizeof(A) * std::max<size_t>(cap, 1));
+      if (e == cudaSuccess) e = cudaMalloc(&d_first, sizeof(int) * (cap + 1));
+      if (e != cudaSuccess) return e;
+    }
+    if (h.empty()) return cudaSuccess;
+    cudaError_t e = cudaMemcpy(d, h.data(), sizeof(A) * h.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(d_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice);
+  }
+  void release() {
+    if (d) cudaFree(d);
+    if (d_first) cudaFree(d_first);
+    d = nullptr;
+    d_first = nullptr;
+    cap = 0;
+  }
+};
+
 // ------------------------------------------------------------ host API of TUs
 void box_from_topology(const pmgpu_topology *t, Box *b);
 void switch_setup(const pmgpu_switch *in, SwitchParams *o);
+
+// api.cu (shared with the ensemble driver)
+// evaluates the enabled forces (only >= 0: that force) at the resident
+// positions into the zeroed forces and accumulators; fold = 0 leaves the
+// pair forces of a force-only MD step in the list's slot buffer
+int evaluate_forces(System *s, int only, int mode, int fold = 1);
+int begin_eval(System *s);
+// reads the accumulators and the status word after an evaluation or a
+// segment (overflow: the lists grow and PMGPU_ERR_OVERFLOW is returned)
+int read_results(System *s, int only, double *energies, double *virial, int add,
+                 int energies_valid = 1);
+// the same on accumulators and status already copied to h_acc / h_status
+int take_results(System *s, int only, double *energies, double *virial, int add,
+                 int energies_valid = 1);
+int run_snapshot(System *s, int restore);
+void pair_groups(System *s, std::vector<std::pair<int, PairTerms>> *out);
+
+// batched launches over an ensemble's members (nonbonded.cu, pme.cu,
+// bonded_integrate.cu)
+struct NbBatch;
+struct PmeBatch;
+struct BdBatch;
+NbBatch *nb_batch_new();
+void nb_batch_free(NbBatch *b);
+int nb_batch_build(NbBatch *b, System *const *m, int n, const PairTerms *terms,
+                   const int *splits);
+int nb_batch_time_jl(NbBatch *b, System *const *m, int n, const int *splits, int reps,
+                     cudaStream_t st, double *ms);
+void nb_batch_member_info(NbBatch *b, int k, int *splits, int *clusters);
+int nb_batch_list(NbBatch *b, cudaStream_t st, long long *launched);
+int nb_batch_pairs(NbBatch *b, int mode, cudaStream_t st, long long *launched);
+void nb_batch_mark(NbBatch *b, System *const *m, int n, int mode);
+PmeBatch *pme_batch_new();
+void pme_batch_free(PmeBatch *b);
+int pme_batch_build(PmeBatch *b, System *const *m, int n, Force *const *fs);
+int pme_batch_reciprocal(PmeBatch *b, int em, cudaStream_t st, long long *launched);
+int pme_batch_correction(PmeBatch *b, int em, cudaStream_t st, long long *launched);
+int pme_batch_buckets(const PmeBatch *b);
+BdBatch *bd_batch_new();
+void bd_batch_free(BdBatch *b);
+int bd_batch_build(BdBatch *b, System *const *m, int n, const pmgpu_integrator *it,
+                   const int *bd_flags);
+int bd_batch_update(BdBatch *b, int phase, int zero_acc, cudaStream_t st,
+                    long long *launched);
+int bd_batch_bonded(BdBatch *b, int em, cudaStream_t st, long long *launched);
 
 // nonbonded.cu
 int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin,
@@ -407,6 +506,10 @@ int zero_forces(System *s);
 // the update takes from the drifted positions (or null)
 int integrate_kick_drift(System *s, const pmgpu_integrator *it, int phase, int zero_acc = 0,
                          NeighborList *list = nullptr);
+struct UpdateArgs;
+int update_args(System *s, const pmgpu_integrator *it, int phase, int zero_acc,
+                NeighborList *list, UpdateArgs *out);
+int update_blocks(const System *s);
 int set_device_step(System *s);
 int forces_to_host(System *s, double *out, int add);
 

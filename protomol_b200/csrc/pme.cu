@@ -27,6 +27,10 @@ struct PmeArgs {
   int K[3];
   int order;
   double inv_L[3];
+  const double *pos, *charge;
+  long long *grid_fixed;  // spread target (int64 fixed point)
+  const float *phi;       // potential grid the gather reads
+  long long *force;
 };
 
 // B-spline weights M_p(fr + k), k = 0..p-1, and their derivatives with
@@ -82,10 +86,11 @@ __device__ __forceinline__ void grid_coord(const PmeArgs &a, int axis, double w,
 // Spread: L lanes per atom (L = order rounded up to a power of two); lane
 // kx < P adds the P^2 points of its x plane.
 template <int P, int L>
-__global__ void __launch_bounds__(128)
-k_pme_spread(PmeArgs a, const double *__restrict__ pos, const double *__restrict__ charge,
-             long long *__restrict__ grid) {
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void spread_body(const PmeArgs &a, Blk b) {
+  const double *__restrict__ pos = a.pos;
+  const double *__restrict__ charge = a.charge;
+  long long *__restrict__ grid = a.grid_fixed;
+  const int gt = b.x * blockDim.x + threadIdx.x;
   const int t = gt / L, kx = gt & (L - 1);
   if (t >= a.n || kx >= P) return;
   const int i = t;
@@ -123,28 +128,60 @@ k_pme_spread(PmeArgs a, const double *__restrict__ pos, const double *__restrict
   }
 }
 
+template <int P, int L>
+__global__ void __launch_bounds__(128) k_pme_spread(PmeArgs a) {
+  spread_body<P, L>(a, own_blk());
+}
+template <int P, int L>
+__global__ void __launch_bounds__(128)
+k_pme_spread_batch(const PmeArgs *__restrict__ tab, const int *__restrict__ first, int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  spread_body<P, L>(tab[m], batch_blk(first, m));
+}
+
 // Converts the fixed-point charge grid to FP32 and clears it for the next
 // spread (the grid is zero at allocation and after every conversion, so no
 // separate clearing pass is needed).
-__global__ void k_pme_fixed_to_float(int total, long long *__restrict__ g,
-                                     float *__restrict__ out) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < total) {
-    out[i] = (float)((double)g[i] * (1.0 / kGridScale));
-    g[i] = 0;
+struct GridConvArgs {
+  int total;
+  long long *g;
+  float *out;
+};
+__device__ __forceinline__ void fixed_to_float_body(const GridConvArgs &a, Blk b) {
+  int i = b.x * blockDim.x + threadIdx.x;
+  if (i < a.total) {
+    a.out[i] = (float)((double)a.g[i] * (1.0 / kGridScale));
+    a.g[i] = 0;
   }
+}
+__global__ void k_pme_fixed_to_float(GridConvArgs a) { fixed_to_float_body(a, own_blk()); }
+__global__ void k_pme_fixed_to_float_batch(const GridConvArgs *__restrict__ tab,
+                                           const int *__restrict__ first, int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  fixed_to_float_body(tab[m], batch_blk(first, m));
 }
 
 // Multiply by the influence function (precomputed for the box:
 // exp(-pi^2 m^2/alpha^2)/(pi V m^2) |b(m)|^2, zero at m = 0); with em >= 1
 // reduce the energy, with em == 2 also the virial.
 // m index convention: m in [0, K/2] -> m, (K/2, K) -> m - K.
-__global__ void k_pme_convolve(int K0, int K1, int K2, double L0, double L1, double L2,
-                               double alpha, const float *__restrict__ infl,
-                               float2 *__restrict__ c, long long *__restrict__ acc, int em) {
+struct ConvolveArgs {
+  int K0, K1, K2;
+  double L0, L1, L2, alpha;
+  const float *infl;
+  float2 *c;
+  long long *acc;
+  int em;
+};
+__device__ __forceinline__ void convolve_body(const ConvolveArgs &A, Blk b) {
+  const int K0 = A.K0, K1 = A.K1, K2 = A.K2, em = A.em;
+  const double L0 = A.L0, L1 = A.L1, L2 = A.L2, alpha = A.alpha;
+  const float *__restrict__ infl = A.infl;
+  float2 *__restrict__ c = A.c;
+  long long *__restrict__ acc = A.acc;
   const int Kh = K2 / 2 + 1;
   const int total = K0 * K1 * Kh;
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int idx = b.x * blockDim.x + threadIdx.x;
   double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
   if (idx < total) {
     const float g = infl[idx];
@@ -185,15 +222,22 @@ __global__ void k_pme_convolve(int K0, int K1, int K2, double L0, double L1, dou
     }
   }
 }
+__global__ void k_pme_convolve(ConvolveArgs a) { convolve_body(a, own_blk()); }
+__global__ void k_pme_convolve_batch(const ConvolveArgs *__restrict__ tab,
+                                     const int *__restrict__ first, int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  convolve_body(tab[m], batch_blk(first, m));
+}
 
 // Gather: L lanes per atom, lane kx < P sums its x plane; the partial
 // forces are reduced over the lanes with shuffles.
 template <int P, int L>
-__global__ void __launch_bounds__(128)
-k_pme_gather(PmeArgs a, const double *__restrict__ pos, const double *__restrict__ charge,
-             const float *__restrict__ phi,
-             long long *__restrict__ force) {
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void gather_body(const PmeArgs &a, Blk b) {
+  const double *__restrict__ pos = a.pos;
+  const double *__restrict__ charge = a.charge;
+  const float *__restrict__ phi = a.phi;
+  long long *__restrict__ force = a.force;
+  const int gt = b.x * blockDim.x + threadIdx.x;
   const int t = gt / L, kx = gt & (L - 1);
   const int i = t;
   const bool valid = t < a.n;
@@ -254,13 +298,38 @@ k_pme_gather(PmeArgs a, const double *__restrict__ pos, const double *__restrict
   }
 }
 
+template <int P, int L>
+__global__ void __launch_bounds__(128) k_pme_gather(PmeArgs a) {
+  gather_body<P, L>(a, own_blk());
+}
+template <int P, int L>
+__global__ void __launch_bounds__(128)
+k_pme_gather_batch(const PmeArgs *__restrict__ tab, const int *__restrict__ first, int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  gather_body<P, L>(tab[m], batch_blk(first, m));
+}
+
 // correctionTerm, NonbondedFullEwaldSystemForce.h:1092-1131, FP64.
-__global__ void k_ewald_correction(Box box, int nexcl, const int *__restrict__ ex,
-                                   const double *__restrict__ pos,
-                                   const double *__restrict__ charge, double alpha,
-                                   double csf, int n, long long *__restrict__ force,
-                                   long long *__restrict__ acc, int em) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
+struct CorrectionArgs {
+  Box box;
+  int nexcl;
+  const int *ex;
+  const double *pos, *charge;
+  double alpha, csf;
+  int n;
+  long long *force, *acc;
+  int em;
+};
+__device__ __forceinline__ void correction_body(const CorrectionArgs &A, Blk b) {
+  const Box &box = A.box;
+  const int nexcl = A.nexcl, n = A.n, em = A.em;
+  const double alpha = A.alpha, csf = A.csf;
+  const int *__restrict__ ex = A.ex;
+  const double *__restrict__ pos = A.pos;
+  const double *__restrict__ charge = A.charge;
+  long long *__restrict__ force = A.force;
+  long long *__restrict__ acc = A.acc;
+  int k = b.x * blockDim.x + threadIdx.x;
   double e = 0, v[6] = {0, 0, 0, 0, 0, 0};
   if (k < nexcl) {
     int a1 = ex[3 * k], a2 = ex[3 * k + 1], cl = ex[3 * k + 2];
@@ -299,6 +368,13 @@ __global__ void k_ewald_correction(Box box, int nexcl, const int *__restrict__ e
       for (int q = 0; q < 9; q++) red_add(&acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
     }
   }
+}
+
+__global__ void k_ewald_correction(CorrectionArgs a) { correction_body(a, own_blk()); }
+__global__ void k_ewald_correction_batch(const CorrectionArgs *__restrict__ tab,
+                                         const int *__restrict__ first, int nm) {
+  const int m = batch_member(first, nm, blockIdx.x);
+  correction_body(tab[m], batch_blk(first, m));
 }
 
 // ------------------------------------------------------------ host side
@@ -442,11 +518,9 @@ static void launch_spread_gather(const PmeArgs &a, System *s, Force *f,
   constexpr int L = P <= 4 ? 4 : 8;
   const int nb = (int)(((long long)a.n * L + 127) / 128);
   if (!gather)
-    k_pme_spread<P, L><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge,
-                                                  f->d_grid_fixed);
+    k_pme_spread<P, L><<<nb, 128, 0, s->stream>>>(a);
   else
-    k_pme_gather<P, L><<<nb, 128, 0, s->stream>>>(a, s->d_pos, s->d_charge,
-                                                  f->d_grid, s->d_force);
+    k_pme_gather<P, L><<<nb, 128, 0, s->stream>>>(a);
 }
 
 static void spread_gather(const PmeArgs &a, System *s, Force *f,
@@ -474,6 +548,11 @@ int pme_reciprocal(System *s, Force *f, int em) {
     a.inv_L[d] = 1.0 / s->box.e[d];
   }
   a.order = f->order;
+  a.pos = s->d_pos;
+  a.charge = s->d_charge;
+  a.grid_fixed = f->d_grid_fixed;
+  a.phi = f->d_grid;
+  a.force = s->d_force;
   int K0 = f->grid[0], K1 = f->grid[1], K2 = f->grid[2];
   size_t nreal = (size_t)K0 * K1 * K2;
   size_t ncplx = (size_t)K0 * K1 * (K2 / 2 + 1);
@@ -485,12 +564,12 @@ int pme_reciprocal(System *s, Force *f, int em) {
     return fail(PMGPU_ERR_CUDA, "cufftSetStream failed");
   spread_gather(a, s, f, 0);
   k_pme_fixed_to_float<<<(int)((nreal + 255) / 256), 256, 0, s->stream>>>(
-      (int)nreal, f->d_grid_fixed, f->d_grid);
+      GridConvArgs{(int)nreal, f->d_grid_fixed, f->d_grid});
   if (cufftExecR2C(f->plan_r2c, f->d_grid, (cufftComplex *)f->d_cgrid) != CUFFT_SUCCESS)
     return fail(PMGPU_ERR_CUDA, "cufftExecR2C failed");
   k_pme_convolve<<<(int)((ncplx + 255) / 256), 256, 0, s->stream>>>(
-      K0, K1, K2, s->box.e[0], s->box.e[1], s->box.e[2], f->alpha, f->d_influence,
-      f->d_cgrid, s->d_acc, em);
+      ConvolveArgs{K0, K1, K2, s->box.e[0], s->box.e[1], s->box.e[2], f->alpha, f->d_influence,
+                   f->d_cgrid, s->d_acc, em});
   if (cufftExecC2R(f->plan_c2r, (cufftComplex *)f->d_cgrid, f->d_grid) != CUFFT_SUCCESS)
     return fail(PMGPU_ERR_CUDA, "cufftExecC2R failed");
   spread_gather(a, s, f, 1);
@@ -501,8 +580,214 @@ int pme_reciprocal(System *s, Force *f, int em) {
 int ewald_correction(System *s, Force *f, int em) {
   if (s->n_excl == 0) return PMGPU_OK;
   k_ewald_correction<<<(s->n_excl + 127) / 128, 128, 0, s->stream>>>(
-      s->box, s->n_excl, s->d_excl_pairs, s->d_pos, s->d_charge, f->alpha,
-      s->coulomb_scaling, s->n, s->d_force, s->d_acc, em);
+      CorrectionArgs{s->box, s->n_excl, s->d_excl_pairs, s->d_pos, s->d_charge, f->alpha,
+                     s->coulomb_scaling, s->n, s->d_force, s->d_acc, em});
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+// ---------------------------------------------------------------- batches
+// The PME chain and the Ewald correction of an ensemble's members as
+// batched launches.  Members whose grids have the same dimensions form a
+// bucket: their real and complex grids are slices of one buffer, and one
+// batched cuFFT plan pair transforms the bucket at once.
+struct PmeBucket {
+  int K[3];
+  std::vector<int> members;
+  cufftHandle r2c = 0, c2r = 0;
+  float *grid = nullptr;
+  float2 *cgrid = nullptr;
+};
+struct PmeBatch {
+  int order = 4;
+  BatchTable<PmeArgs> atoms;  // spread and gather
+  BatchTable<GridConvArgs> conv;
+  BatchTable<ConvolveArgs> convolve[2];
+  BatchTable<CorrectionArgs> corr[2];
+  std::vector<PmeBucket> buckets;
+  std::vector<System *> sys;
+  std::vector<Force *> forces;
+};
+
+PmeBatch *pme_batch_new() { return new PmeBatch(); }
+
+// Gives every member its own grids again and frees the buckets.
+void pme_batch_free(PmeBatch *b) {
+  if (!b) return;
+  for (auto &bk : b->buckets) {
+    for (int k : bk.members) {
+      System *s = b->sys[k];
+      Force *f = b->forces[k];
+      const size_t nreal = (size_t)f->grid[0] * f->grid[1] * f->grid[2];
+      const size_t ncplx = (size_t)f->grid[0] * f->grid[1] * (f->grid[2] / 2 + 1);
+      f->d_grid = nullptr;
+      f->d_cgrid = nullptr;
+      dev_alloc(s, &f->d_grid, sizeof(float) * nreal);
+      dev_alloc(s, &f->d_cgrid, sizeof(float2) * ncplx);
+      s->graph_version++;  // graphs captured with the bucket's grids
+    }
+    if (bk.r2c) cufftDestroy(bk.r2c);
+    if (bk.c2r) cufftDestroy(bk.c2r);
+    if (bk.grid) cudaFree(bk.grid);
+    if (bk.cgrid) cudaFree(bk.cgrid);
+  }
+  b->atoms.release();
+  b->conv.release();
+  for (int e = 0; e < 2; e++) {
+    b->convolve[e].release();
+    b->corr[e].release();
+  }
+  delete b;
+}
+
+int pme_batch_build(PmeBatch *b, System *const *m, int n, Force *const *fs) {
+  b->sys.assign(m, m + n);
+  b->forces.assign(fs, fs + n);
+  b->order = fs[0]->order;
+  // buckets by grid dimensions
+  std::vector<int> bucket_of(n, -1);
+  for (int k = 0; k < n; k++) {
+    const Force *f = fs[k];
+    if (f->order != b->order || !(f->ewald_flags & PMGPU_EWALD_RECIPROCAL))
+      return fail(PMGPU_ERR_UNSUPPORTED, "ensemble members need one PME order");
+    int found = -1;
+    for (size_t q = 0; q < b->buckets.size(); q++)
+      if (b->buckets[q].K[0] == f->grid[0] && b->buckets[q].K[1] == f->grid[1] &&
+          b->buckets[q].K[2] == f->grid[2])
+        found = (int)q;
+    if (found < 0) {
+      b->buckets.push_back(PmeBucket());
+      found = (int)b->buckets.size() - 1;
+      for (int a = 0; a < 3; a++) b->buckets[found].K[a] = f->grid[a];
+    }
+    b->buckets[found].members.push_back(k);
+    bucket_of[k] = found;
+  }
+  for (auto &bk : b->buckets) {
+    const int B = (int)bk.members.size();
+    const size_t G = (size_t)bk.K[0] * bk.K[1] * bk.K[2];
+    const size_t Gc = (size_t)bk.K[0] * bk.K[1] * (bk.K[2] / 2 + 1);
+    PM_CUDA(cudaMalloc(&bk.grid, sizeof(float) * G * B));
+    PM_CUDA(cudaMalloc(&bk.cgrid, sizeof(float2) * Gc * B));
+    int dims[3] = {bk.K[0], bk.K[1], bk.K[2]};
+    if (cufftPlanMany(&bk.r2c, 3, dims, nullptr, 1, (int)G, nullptr, 1, (int)Gc, CUFFT_R2C, B) !=
+            CUFFT_SUCCESS ||
+        cufftPlanMany(&bk.c2r, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G, CUFFT_C2R, B) !=
+            CUFFT_SUCCESS)
+      return fail(PMGPU_ERR_CUDA, "batched cuFFT plan creation failed");
+    for (int q = 0; q < B; q++) {
+      System *s = m[bk.members[q]];
+      Force *f = fs[bk.members[q]];
+      PM_CUDA(cudaStreamSynchronize(s->stream));
+      dev_free(s, f->d_grid);
+      dev_free(s, f->d_cgrid);
+      f->d_grid = bk.grid + G * q;
+      f->d_cgrid = bk.cgrid + Gc * q;
+      s->graph_version++;  // graphs captured with the member's own grids
+    }
+  }
+  // argument tables in member order
+  b->atoms.clear();
+  b->conv.clear();
+  for (int e = 0; e < 2; e++) {
+    b->convolve[e].clear();
+    b->corr[e].clear();
+  }
+  int L = b->order <= 4 ? 4 : 8;
+  for (int k = 0; k < n; k++) {
+    System *s = m[k];
+    Force *f = fs[k];
+    PmeArgs a;
+    a.box = s->box;
+    a.n = s->n;
+    for (int d = 0; d < 3; d++) {
+      a.K[d] = f->grid[d];
+      a.inv_L[d] = 1.0 / s->box.e[d];
+    }
+    a.order = f->order;
+    a.pos = s->d_pos;
+    a.charge = s->d_charge;
+    a.grid_fixed = f->d_grid_fixed;
+    a.phi = f->d_grid;
+    a.force = s->d_force;
+    b->atoms.add(a, (int)(((long long)s->n * L + 127) / 128));
+    const size_t nreal = (size_t)f->grid[0] * f->grid[1] * f->grid[2];
+    const size_t ncplx = (size_t)f->grid[0] * f->grid[1] * (f->grid[2] / 2 + 1);
+    b->conv.add(GridConvArgs{(int)nreal, f->d_grid_fixed, f->d_grid}, (int)((nreal + 255) / 256));
+    for (int e = 0; e < 2; e++) {
+      b->convolve[e].add(ConvolveArgs{f->grid[0], f->grid[1], f->grid[2], s->box.e[0],
+                                      s->box.e[1], s->box.e[2], f->alpha, f->d_influence,
+                                      f->d_cgrid, s->d_acc, e},
+                         (int)((ncplx + 255) / 256));
+      b->corr[e].add(CorrectionArgs{s->box, s->n_excl, s->d_excl_pairs, s->d_pos, s->d_charge,
+                                    f->alpha, s->coulomb_scaling, s->n, s->d_force, s->d_acc, e},
+                     (s->n_excl + 127) / 128);
+    }
+  }
+  PM_CUDA(b->atoms.upload());
+  PM_CUDA(b->conv.upload());
+  for (int e = 0; e < 2; e++) {
+    PM_CUDA(b->convolve[e].upload());
+    PM_CUDA(b->corr[e].upload());
+  }
+  return PMGPU_OK;
+}
+
+template <int P>
+static void pme_batch_atoms(PmeBatch *b, int gather, cudaStream_t st) {
+  constexpr int L = P <= 4 ? 4 : 8;
+  BatchTable<PmeArgs> &t = b->atoms;
+  if (!t.total()) return;
+  if (!gather)
+    k_pme_spread_batch<P, L><<<t.total(), 128, 0, st>>>(t.d, t.d_first, t.members());
+  else
+    k_pme_gather_batch<P, L><<<t.total(), 128, 0, st>>>(t.d, t.d_first, t.members());
+}
+
+static void pme_batch_sg(PmeBatch *b, int gather, cudaStream_t st) {
+  switch (b->order) {
+    case 2: pme_batch_atoms<2>(b, gather, st); break;
+    case 3: pme_batch_atoms<3>(b, gather, st); break;
+    case 4: pme_batch_atoms<4>(b, gather, st); break;
+    case 5: pme_batch_atoms<5>(b, gather, st); break;
+    case 6: pme_batch_atoms<6>(b, gather, st); break;
+    case 7: pme_batch_atoms<7>(b, gather, st); break;
+    default: pme_batch_atoms<8>(b, gather, st); break;
+  }
+}
+
+// The reciprocal term of every member (pme_reciprocal of each), em as
+// there.
+int pme_batch_reciprocal(PmeBatch *b, int em, cudaStream_t st, long long *launched) {
+  const int nm = b->atoms.members();
+  if (!nm) return PMGPU_OK;
+  *launched += 4;  // spread, fixed->float, convolve, gather (+ cuFFT's)
+  pme_batch_sg(b, 0, st);
+  k_pme_fixed_to_float_batch<<<b->conv.total(), 256, 0, st>>>(b->conv.d, b->conv.d_first, nm);
+  for (auto &bk : b->buckets) {
+    if (cufftSetStream(bk.r2c, st) != CUFFT_SUCCESS ||
+        cufftExecR2C(bk.r2c, bk.grid, (cufftComplex *)bk.cgrid) != CUFFT_SUCCESS)
+      return fail(PMGPU_ERR_CUDA, "batched cufftExecR2C failed");
+  }
+  BatchTable<ConvolveArgs> &cv = b->convolve[em ? 1 : 0];
+  k_pme_convolve_batch<<<cv.total(), 256, 0, st>>>(cv.d, cv.d_first, nm);
+  for (auto &bk : b->buckets) {
+    if (cufftSetStream(bk.c2r, st) != CUFFT_SUCCESS ||
+        cufftExecC2R(bk.c2r, (cufftComplex *)bk.cgrid, bk.grid) != CUFFT_SUCCESS)
+      return fail(PMGPU_ERR_CUDA, "batched cufftExecC2R failed");
+  }
+  pme_batch_sg(b, 1, st);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+int pme_batch_buckets(const PmeBatch *b) { return (int)b->buckets.size(); }
+
+int pme_batch_correction(PmeBatch *b, int em, cudaStream_t st, long long *launched) {
+  BatchTable<CorrectionArgs> &t = b->corr[em ? 1 : 0];
+  if (!t.members() || !t.total()) return PMGPU_OK;
+  *launched += 1;
+  k_ewald_correction_batch<<<t.total(), 128, 0, st>>>(t.d, t.d_first, t.members());
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }

@@ -186,6 +186,11 @@ class GpuSystem:
         L.check(self.lib.pmgpu_system_get_positions(self.h, L.ptr(out)))
         return out
 
+    def set_step(self, step: int) -> None:
+        """The step counter that keys the Langevin noise (0 for a new
+        system)."""
+        L.check(self.lib.pmgpu_system_set_step(self.h, int(step)))
+
     def set_velocities(self, vel):
         a = self._vec(vel)
         L.check(self.lib.pmgpu_system_set_velocities(self.h, L.ptr(a)))
@@ -250,6 +255,11 @@ class GpuSystem:
         """Fix the pair lists' capacity (testing the growth path)."""
         L.check(self.lib.pmgpu_debug_set_list_capacity(self.h, int(tiles_per_row)))
 
+    def limit_list_rows(self, tiles_per_row: int) -> None:
+        """Limit the tiles a list row may hold in later builds, keeping the
+        current list and forces (testing the growth path inside segments)."""
+        L.check(self.lib.pmgpu_debug_limit_list_rows(self.h, int(tiles_per_row)))
+
     def cell_assign(self, cellsize: float):
         cells = np.zeros((self.n, 3), np.int32)
         dims = np.zeros(3, np.int32)
@@ -304,7 +314,8 @@ class SystemForce:
         L.check(self.system.lib.pmgpu_force_stats(self.system.h, self.id, C.byref(st)))
         return dict(pairs_in_cutoff=st.pairs_in_cutoff, list_entries=st.list_entries,
                     list_builds=st.list_builds, cells=tuple(st.cells),
-                    pair_kernel=PAIR_KERNELS.get(st.pair_kernel, st.pair_kernel))
+                    pair_kernel=PAIR_KERNELS.get(st.pair_kernel, st.pair_kernel),
+                    list_capacity=st.list_capacity)
 
     def pair_set(self, cap: int = 1 << 24) -> np.ndarray:
         """The unordered pair set (i < j) this force evaluates at the
@@ -558,3 +569,65 @@ class LeapfrogIntegrator(_Integrator):
 
 class LangevinLeapfrogIntegrator(_Integrator):
     kind = L.INT_LANGEVIN_LEAPFROG
+
+
+class SystemEnsemble:
+    """Resident systems advanced together (pmgpu_ensemble_*): every kernel
+    of an MD step is one launch over all members, members with the same PME
+    grid share one batched FFT, and segments replay as captured CUDA
+    graphs.  A member's trajectory is bitwise the one it follows in any
+    other ensemble with the same pair-kernel splits.  The members stay
+    owned by the caller and must outlive the ensemble."""
+
+    def __init__(self, members: list[GpuSystem]):
+        if not members:
+            raise ValueError("an ensemble needs members")
+        self.lib = members[0].lib
+        self.members = list(members)
+        arr = (C.c_void_p * len(members))(*[m.h for m in members])
+        h = C.c_void_p()
+        L.check(self.lib.pmgpu_ensemble_create(arr, len(members), C.byref(h)))
+        self.h = h
+
+    def run(self, integrator: "_Integrator", n_steps: int) -> None:
+        """integrator.run(member, n_steps) for every member at once."""
+        L.check(self.lib.pmgpu_ensemble_run(self.h, C.byref(integrator.p), int(n_steps)))
+
+    def set_splits(self, splits) -> None:
+        a = np.ascontiguousarray(splits, dtype=np.int32)
+        if a.shape != (len(self.members),):
+            raise ValueError("one splits value per member")
+        L.check(self.lib.pmgpu_ensemble_set_splits(self.h, L.ptr(a)))
+
+    def time_pairs(self, splits, reps: int = 10) -> float:
+        """Device ms of one force-only pair launch over all members with the
+        given per-member splits (0: the member's current choice)."""
+        a = np.ascontiguousarray(splits, dtype=np.int32)
+        ms = C.c_double()
+        L.check(self.lib.pmgpu_ensemble_time_pairs(self.h, L.ptr(a), int(reps), C.byref(ms)))
+        return float(ms.value)
+
+    def member(self, k: int) -> tuple[int, int]:
+        """(i clusters, splits in use) of member k; (0, -1) for a member
+        without the specialised force-only pair kernel."""
+        c, sp = C.c_int(), C.c_int()
+        L.check(self.lib.pmgpu_ensemble_member(self.h, int(k), C.byref(c), C.byref(sp)))
+        return int(c.value), int(sp.value)
+
+    def info(self) -> dict:
+        i = L.EnsembleInfo()
+        L.check(self.lib.pmgpu_ensemble_get_info(self.h, C.byref(i)))
+        return {"members": i.members, "fft_buckets": i.fft_buckets, "kernels": i.kernels,
+                "graph_replays": i.graph_replays, "steps": i.steps}
+
+    def close(self) -> None:
+        if self.h:
+            L.check(self.lib.pmgpu_ensemble_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

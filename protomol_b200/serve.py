@@ -25,6 +25,7 @@ import numpy as np
 
 from . import systems
 from .engine import (Context, ForceFactory, GpuSystem, LangevinLeapfrogIntegrator,
+                     SystemEnsemble,
                      LeapfrogIntegrator, footprint_estimate)
 
 WATER_DENSITY = 0.0334  # waters per A^3
@@ -111,9 +112,87 @@ def build(ctx: Context, req: Request, precision: str = "mixed") -> GpuSystem:
     return gs
 
 
-def execute(ctx: Context, req: Request, keep_positions: bool = True) -> Request:
-    """Runs one request to completion on the calling thread."""
-    gs = build(ctx, req)
+class ShellPool:
+    """Idle systems kept for reuse.  Requests on boxes of the same shape
+    (water count, hence edge, grid and topology) share a key; a request
+    whose key has an idle shell takes it instead of creating a system: its
+    positions, velocities and Langevin step counter are set, and the
+    shell's device buffers, pair list, cuFFT plans and captured step graphs
+    are reused.  A request's results are the same in a reused shell as in
+    a new system (every list is built afresh from the new positions).
+    Idle shells beyond cap_bytes (by their footprint estimates) are closed,
+    the least recently used first."""
+
+    def __init__(self, ctx: Context, cap_bytes: int):
+        self.ctx = ctx
+        self.cap = int(cap_bytes)
+        self.lock = threading.Lock()
+        self.idle: dict = {}  # key -> [GpuSystem]
+        self.lru: list = []   # (key, footprint) of idle shells, oldest first
+        self.held = 0
+        self.reused = 0
+        self.created = 0
+
+    @staticmethod
+    def key(req: Request):
+        return (req.n_waters, req.grid)
+
+    def acquire(self, req: Request) -> GpuSystem:
+        k = self.key(req)
+        gs = None
+        with self.lock:
+            if self.idle.get(k):
+                gs = self.idle[k].pop()
+                for q, (kk, fp) in enumerate(self.lru):
+                    if kk == k:
+                        self.held -= fp
+                        del self.lru[q]
+                        break
+                self.reused += 1
+            else:
+                self.created += 1
+        if gs is None:
+            return build(self.ctx, req)
+        sysm = req.prepare().system
+        gs.set_positions(sysm.pos)
+        gs.set_velocities(sysm.vel)
+        gs.set_step(0)
+        return gs
+
+    def release(self, req: Request, gs: GpuSystem) -> None:
+        k = self.key(req)
+        fp = req.footprint()
+        evict = []
+        with self.lock:
+            if fp > self.cap:
+                evict.append(gs)
+            else:
+                self.idle.setdefault(k, []).append(gs)
+                self.lru.append((k, fp))
+                self.held += fp
+                while self.held > self.cap and self.lru:
+                    kk, f = self.lru.pop(0)
+                    evict.append(self.idle[kk].pop(0))
+                    self.held -= f
+        for g in evict:
+            g.close()
+
+    def close(self) -> None:
+        with self.lock:
+            shells = [g for v in self.idle.values() for g in v]
+            self.idle.clear()
+            self.lru.clear()
+            self.held = 0
+        for g in shells:
+            g.close()
+
+
+def execute(ctx: Context, req: Request, keep_positions: bool = True,
+            pool: ShellPool | None = None) -> Request:
+    """Runs one request to completion on the calling thread (in a shell
+    from `pool` when one is given)."""
+    gs = pool.acquire(req) if pool is not None else build(ctx, req)
+    ok = False
     try:
         if req.kind == "evaluate":
             e, _ = gs.evaluate()
@@ -129,8 +208,12 @@ def execute(ctx: Context, req: Request, keep_positions: bool = True) -> Request:
             req.energies = gs.energies()[0]
             if keep_positions:
                 req.positions = gs.positions()
+        ok = True
     finally:
-        gs.close()
+        if pool is not None and ok:
+            pool.release(req, gs)
+        else:
+            gs.close()
     return req
 
 
@@ -139,13 +222,18 @@ class Server:
 
     slots: requests in flight at once (one worker thread each);
     mem_fraction: share of the device memory free at start-up that admitted
-    requests may hold (by their footprint estimates)."""
+    requests may hold (by their footprint estimates);
+    pool_fraction: share of it kept for idle shells (ShellPool; 0: every
+    request creates and frees its own system)."""
 
-    def __init__(self, ctx: Context, slots: int = 16, mem_fraction: float = 0.8):
+    def __init__(self, ctx: Context, slots: int = 16, mem_fraction: float = 0.8,
+                 pool_fraction: float = 0.2):
         self.ctx = ctx
         self.slots = slots
         free, _ = ctx.mem_info()
-        self.budget = int(free * mem_fraction)
+        total = int(free * mem_fraction)
+        self.pool = ShellPool(ctx, int(total * pool_fraction)) if pool_fraction > 0 else None
+        self.budget = total - (self.pool.cap if self.pool else 0)
         self.in_use = 0
         self.lock = threading.Condition()
         self.admit_q: queue.Queue = queue.Queue()
@@ -160,7 +248,7 @@ class Server:
             if req is None:
                 return
             try:
-                execute(self.ctx, req)
+                execute(self.ctx, req, pool=self.pool)
             except Exception as ex:  # reported per request, the loop goes on
                 req.error = str(ex)[:300]
             req.t_done = time.perf_counter() - self.t0
@@ -209,35 +297,73 @@ class Server:
         out = summarize(reqs, wall, self.slots, self.peak_in_flight)
         out["peak_footprint_bytes"] = self.peak_in_use
         out["budget_bytes"] = self.budget
+        if self.pool is not None:
+            out["shells_reused"] = self.pool.reused
+            out["shells_created"] = self.pool.created
         return out
+
+    def close(self) -> None:
+        if self.pool is not None:
+            self.pool.close()
 
 
 class Ensemble:
-    """The batched form: many resident boxes advanced together.  Every
-    member keeps its state on the device between segments; a segment is
-    enqueued on every member's stream (inner steps replay each member's
-    captured CUDA graph) before any is waited for, so the members' kernels
-    overlap on the device.  `plain` advances the members one at a time."""
+    """Many resident boxes advanced together, in three forms:
 
-    def __init__(self, ctx: Context, requests: list[Request]):
+    - "batched": one engine.SystemEnsemble; every kernel of a step is one
+      launch over all members (pair-kernel splits per size bucket from the
+      autotuner), each segment one captured CUDA graph;
+    - "streams": each member's own pmgpu_run segment enqueued on its own
+      stream before any is waited for, so the members' kernels overlap;
+    - "plain": the members one at a time.
+
+    Every member keeps its state on the device between segments."""
+
+    def __init__(self, ctx: Context, requests: list[Request], tuner=None):
         self.requests = requests
         self.members = [build(ctx, r.prepare()) for r in requests]
         self.integ = [LeapfrogIntegrator(r.timestep) if r.integrator == "leapfrog" else
                       LangevinLeapfrogIntegrator(r.timestep, r.temperature, r.gamma, seed=r.seed)
                       for r in requests]
+        self.batch = None
+        self.splits = None
+        self.tuner = tuner
 
-    def run(self, steps: int, plain: bool = False) -> float:
+    def _batched(self) -> SystemEnsemble:
+        if self.batch is None:
+            p0 = self.integ[0].p
+            for it in self.integ:
+                if (it.p.kind, it.p.timestep_fs, it.p.temperature, it.p.gamma_ps,
+                        it.p.seed) != (p0.kind, p0.timestep_fs, p0.temperature, p0.gamma_ps,
+                                       p0.seed):
+                    raise ValueError("the batched form runs one integrator for all members")
+            self.batch = SystemEnsemble(self.members)
+            if self.tuner is not None:
+                self.splits = self.tuner.apply(self.batch)
+        return self.batch
+
+    def run(self, steps: int, mode: str = "batched") -> float:
         """One segment of `steps` MD steps for every member; wall seconds."""
+        if mode == "batched":
+            ens = self._batched()
+            t0 = time.perf_counter()
+            ens.run(self.integ[0], steps)
+            return time.perf_counter() - t0
         t0 = time.perf_counter()
-        if plain:
+        if mode == "plain":
             for gs, it in zip(self.members, self.integ):
                 it.run(gs, steps)
-        else:
+        elif mode == "streams":
             for gs, it in zip(self.members, self.integ):
                 it.run_async(gs, steps)
             for gs, it in zip(self.members, self.integ):
                 it.wait(gs)
+        else:
+            raise ValueError(f"unknown ensemble form {mode!r}")
         return time.perf_counter() - t0
+
+    def info(self) -> dict | None:
+        return self.batch.info() if self.batch is not None else None
 
     def energies(self) -> list[np.ndarray]:
         return [gs.energies()[0] for gs in self.members]
@@ -246,6 +372,9 @@ class Ensemble:
         return [gs.positions() for gs in self.members]
 
     def close(self):
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None
         for gs in self.members:
             gs.close()
         self.members = []

@@ -37,6 +37,32 @@ def test_served_results_equal_alone(ctx):
             assert np.array_equal(a.positions, m.positions), a.rid
 
 
+def test_reused_shells_give_the_results_of_new_systems(ctx):
+    """Requests on boxes of one shape (different seeds) run one after the
+    other in shells from the pool: new positions, velocities and step
+    counter, every list built afresh; each result equals the request run
+    in a new system, bit for bit (Langevin noise included)."""
+    shapes = [(250, "segment", 30), (250, "evaluate", 0), (250, "segment", 30),
+              (400, "segment", 20), (400, "segment", 20), (250, "evaluate", 0)]
+
+    def reqs():
+        return [serve.Request(rid=k, n_waters=nw, seed=40 + k, kind=kind, steps=st)
+                for k, (nw, kind, st) in enumerate(shapes)]
+
+    alone = [serve.execute(ctx, r) for r in reqs()]
+    srv = serve.Server(ctx, slots=1)
+    pooled = reqs()
+    stats = srv.run(pooled, realtime=False)
+    srv.close()
+    assert stats["failed"] == 0 and stats["shells_reused"] >= 3, stats
+    for a, m in zip(alone, sorted(pooled, key=lambda r: r.rid)):
+        assert np.array_equal(a.energies, m.energies), a.rid
+        if a.kind == "evaluate":
+            assert np.array_equal(a.forces, m.forces), a.rid
+        else:
+            assert np.array_equal(a.positions, m.positions), a.rid
+
+
 def test_admission_respects_memory_budget(ctx):
     srv = serve.Server(ctx, slots=8)
     reqs = _mix()
