@@ -666,6 +666,9 @@ def main():
                     help="served/batched: requests (boxes) in the stream")
     ap.add_argument("--slots", type=int, default=32,
                     help="served/batched: requests in flight at once")
+    ap.add_argument("--no-baselines", dest="baselines", action="store_false",
+                    help="skip the accuracy check and the CPU baseline legs (for sweeps; "
+                         "the line then carries no accuracy)")
     ap.add_argument("--no-forms", dest="forms", action="store_false",
                     help="bench: skip the short batched / served / GB summaries")
     ap.add_argument("--md-steps", type=int, default=1000,
@@ -751,9 +754,11 @@ def main():
         integ.run(gs, args.steps)
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
-        b1 = gs.forces[3].stats()["list_builds"]
+        st = gs.forces[3].stats()
         print(json.dumps({"mode": "profile", "md_steps": args.steps, "atoms": gs.n,
-                          "list_builds": b1 - b0}))
+                          "list_builds": st["list_builds"] - b0,
+                          "list_entries": st["list_entries"], "clusters": st["clusters"],
+                          "list_capacity": st["list_capacity"]}))
         gs.close()
         return
     stream = torch.cuda.ExternalStream(gs.stream())
@@ -876,7 +881,7 @@ def main():
         if forms:
             line["forms"] = forms
         acc = None
-        if world == 1:
+        if world == 1 and args.baselines:
             try:
                 acc = restatement_baseline(gs, sysm, samples)
                 line["accuracy"] = {k: acc[k] for k in acc if k != "restatement"}
@@ -887,7 +892,7 @@ def main():
                                           f"steps each) against the FP64 restatement")
             except Exception as ex:  # reported, never fatal
                 line["accuracy"] = {"error": str(ex)[:200]}
-        if world == 1 and os.path.exists(REF_BIN):
+        if world == 1 and args.baselines and os.path.exists(REF_BIN):
             try:
                 r = run_reference(2)
                 line["cpu_baseline"] = {"value": r["ns_per_day"], "unit": "ns/day", "cores": 1,

@@ -233,11 +233,11 @@ int pmgpu_force_gbace_add(pmgpu_system *sys, double solvation_param,
  *
  * Scratch lives in one statically sized device array inside the library,
  * so n_atoms above PMGPU_GB_STATIC_MAX_ATOMS is rejected with
- * PMGPU_ERR_ARG.  The first call on each device (with that device current)
- * looks up the array's device address; make that first call before any
- * stream capture.  The address is kept for the life of the process, so a
- * host that calls cudaDeviceReset (which ends the context that address
- * belongs to) must not call this entry point afterwards.  All calls on a device share the array and it keeps the
+ * PMGPU_ERR_ARG.  Every call looks up the array's device address in the
+ * current context (no allocation; a context made after cudaDeviceReset gets
+ * its own array); make the first call on a device before any stream
+ * capture, since it may load the library's device code.  All calls on a
+ * device share the array and it keeps the
  * previous call's contents (the call clears what must start at zero): two
  * calls whose work overlaps on the GPU race and both results are wrong, so
  * issue them on one stream or otherwise serialise them. */

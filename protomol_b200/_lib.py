@@ -98,10 +98,12 @@ def load() -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+    # PMGPU_LIB: another build of the same library (for comparing builds)
+    path = os.environ.get("PMGPU_LIB", LIB_PATH)
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with __graft_entry__.build() "
                           "or `make -C protomol_b200/csrc`")
-    lib = C.CDLL(LIB_PATH)
+    lib = C.CDLL(path)
     vp, i32, dbl = C.c_void_p, C.c_int, C.c_double
     lib.pmgpu_last_error.restype = C.c_char_p
     lib.pmgpu_system_stream.restype = vp

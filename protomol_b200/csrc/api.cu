@@ -997,8 +997,12 @@ static double default_skin(const System *s, double cutoff) {
   // (flexible) water at 1 fs, which balances the build against the pairs
   // the skin adds to every step (1.0 and 1.6 A measured within 1 %, 0.7 A
   // 4 % slower); small boxes get a smaller skin so cutoff + skin stays
-  // below the box edge.
+  // below the box edge.  PMGPU_LIST_SKIN overrides the 1.3 A (a tuning
+  // knob: any skin gives the same pair set, only the work split between
+  // the list builds and the pair kernel changes).
   double skin = 1.3;
+  static const char *env = std::getenv("PMGPU_LIST_SKIN");
+  if (env && std::atof(env) >= 0.0) skin = std::atof(env);
   if (s->box.periodic) {
     double emin = std::min(s->box.e[0], std::min(s->box.e[1], s->box.e[2]));
     if (cutoff + skin >= emin) skin = std::max(0.0, 0.5 * (emin - cutoff));

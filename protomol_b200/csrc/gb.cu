@@ -760,34 +760,21 @@ static_assert(ACC_COUNT <= kGbStaticAccWords, "accumulator block too small");
 // then the FP32 records: pair records (2 float4 per atom), static and radius
 // records (1 float4 each)
 constexpr size_t kGbStaticWords = 16 * (size_t)kGbStaticMaxAtoms + kGbStaticAccWords;
-constexpr int kGbStaticMaxDevices = 64;
 
 // In host code this name is only a stand-in for the symbol; the device
-// address comes from cudaGetSymbolAddress, once per device.
+// address comes from cudaGetSymbolAddress.
 static __device__ __align__(256) long long g_gb_scratch[kGbStaticWords];
 
-std::mutex g_gb_scratch_mu;
-long long *g_gb_scratch_dev[kGbStaticMaxDevices] = {};
-
-// Device address of g_gb_scratch on the current device, looked up on the
-// first call made with that device current and kept for the life of the
-// process (a cudaDeviceReset ends the context it belongs to; callers that
-// reset the device do not use this entry point afterwards).
+// Device address of g_gb_scratch in the current context, looked up on every
+// call (a lookup, no allocation), so a context created after a
+// cudaDeviceReset gets its own copy's address.
 int gb_scratch_address(long long **out) {
-  int dev = -1;
-  PM_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kGbStaticMaxDevices)
-    return fail(PMGPU_ERR_UNSUPPORTED, "device ordinal beyond the static scratch table");
-  std::lock_guard<std::mutex> lock(g_gb_scratch_mu);
-  if (!g_gb_scratch_dev[dev]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_gb_scratch);
-    if (e != cudaSuccess || !p)
-      return fail(PMGPU_ERR_CUDA, std::string("cudaGetSymbolAddress(GB scratch): ") +
-                                      cudaGetErrorString(e));
-    g_gb_scratch_dev[dev] = static_cast<long long *>(p);
-  }
-  *out = g_gb_scratch_dev[dev];
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_gb_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(PMGPU_ERR_CUDA, std::string("cudaGetSymbolAddress(GB scratch): ") +
+                                    cudaGetErrorString(e));
+  *out = static_cast<long long *>(p);
   return PMGPU_OK;
 }
 

@@ -865,17 +865,23 @@ __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk)
 #pragma unroll
     for (int k = 0; k < 8; k++) fi[k][0] = fi[k][1] = fi[k][2] = 0.f;
     int qn = 0;  // queued j lanes
+    // tile idx of the cluster's row parts read one after the other; the
+    // record of the next batch is loaded one batch ahead
+    auto tile_index = [&](int idx) -> size_t {
+      const int p = (idx >= p1) + (idx >= p2) + (idx >= p3);
+      const int off = idx - (p == 0 ? 0 : (p == 1 ? p1 : (p == 2 ? p2 : p3)));
+      return (size_t)(kRowParts * ci + p) * a.cap + off;
+    };
+    uint2 next = t0 + tb < t1 ? __ldg(a.tiles + tile_index(t0 + tb)) : make_uint2(0u, 0u);
     for (int b0 = t0; b0 < t1; b0 += 8) {
       const int idx = b0 + tb;
+      const uint2 tile = next;
+      if (idx + 8 < t1) next = __ldg(a.tiles + tile_index(idx + 8));
       unsigned act = 0u;
       int m = 0, jslot = 0, tj = 0;
       float rjx = 0.f, rjy = 0.f, rjz = 0.f, qj = 0.f;
       if (idx < t1) {
-        // tile idx of the cluster's row parts read one after the other
-        const int p = (idx >= p1) + (idx >= p2) + (idx >= p3);
-        const int off = idx - (p == 0 ? 0 : (p == 1 ? p1 : (p == 2 ? p2 : p3)));
-        const size_t ti0 = (size_t)(kRowParts * ci + p) * a.cap + off;
-        const uint2 tile = __ldg(a.tiles + ti0);
+        const size_t ti0 = tile_index(idx);
         const int hj = (int)(tile.x & kJMask);
         const int sh = (int)((tile.x >> kShiftBits) & kShiftMask);
         const unsigned mi = (tile.y >> (8 * jl)) & 0xFFu;

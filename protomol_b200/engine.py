@@ -313,7 +313,7 @@ class SystemForce:
         st = L.Stats()
         L.check(self.system.lib.pmgpu_force_stats(self.system.h, self.id, C.byref(st)))
         return dict(pairs_in_cutoff=st.pairs_in_cutoff, list_entries=st.list_entries,
-                    list_builds=st.list_builds, cells=tuple(st.cells),
+                    clusters=st.clusters, list_builds=st.list_builds, cells=tuple(st.cells),
                     pair_kernel=PAIR_KERNELS.get(st.pair_kernel, st.pair_kernel),
                     list_capacity=st.list_capacity)
 

@@ -80,8 +80,9 @@ def test_cpu_integrator_with_gpu_cutoff_forces_reference_grammar():
         sysm, [f"LennardJones Coulomb -algorithm NonbondedCutoff {C2C2}", "Bond", "Angle"],
         [f"LennardJones Coulomb -algorithm NonbondedCutoffGPU {C2C2}", "Bond", "Angle"], 20)
     # FP32 pair arithmetic (RMS relative force error ~1e-6) over 20 steps of
-    # 0.5 fs: positions agree far below the 1e-3 A of thermal motion per step
-    assert np.abs(pc - pg).max() < 1e-6, np.abs(pc - pg).max()
+    # 0.5 fs: positions agree to ~1e-6 A, far below the 1e-3 A of thermal
+    # motion per step
+    assert np.abs(pc - pg).max() < 1e-5, np.abs(pc - pg).max()
     for c in (1, 3):  # E_potential, E_total of the last output line
         assert abs(ec[-1, c] - eg[-1, c]) <= 1e-5 * abs(ec[-1, c]), (c, ec[-1], eg[-1])
 
@@ -119,7 +120,7 @@ def test_cn_switching_through_the_module():
     pc, ec, pg, eg = _both(
         sysm, [f"LennardJones Coulomb -algorithm NonbondedCutoff {cn}", "Bond", "Angle"],
         [f"LennardJones Coulomb -algorithm NonbondedCutoffGPU {cn}", "Bond", "Angle"], 10)
-    assert np.abs(pc - pg).max() < 1e-6, np.abs(pc - pg).max()
+    assert np.abs(pc - pg).max() < 1e-5, np.abs(pc - pg).max()  # FP32 forces, as above
     for c in (1, 3):
         assert abs(ec[-1, c] - eg[-1, c]) <= 1e-5 * abs(ec[-1, c]), (c, ec[-1], eg[-1])
 
@@ -137,7 +138,7 @@ def test_cpu_integrator_with_gpu_pme_matches_full_ewald():
                f"-accuracy {acc:.17g}", "Bond", "Angle"],
         [f"Coulomb -algorithm PMEwaldGPU -alpha {alpha} -cutoff {rc:.17g} -order 8 "
          f"-gridsize 48", "Bond", "Angle"], 10)
-    assert np.abs(pc - pg).max() < 1e-6, np.abs(pc - pg).max()
+    assert np.abs(pc - pg).max() < 1e-5, np.abs(pc - pg).max()  # FP32 forces, as above
     for c in (1, 3):
         assert abs(ec[-1, c] - eg[-1, c]) <= 1e-4 * abs(ec[-1, c]), (c, ec[-1], eg[-1])
 
