@@ -314,6 +314,7 @@ static int add_pair_terms(std::vector<Launch> &groups, int list, const PairTerms
       g.terms.coul_cut2 = t.coul_cut2;
     }
     if (t.mask & TERM_EWALD) {
+      g.terms.ewtab = t.ewtab;
       g.terms.ewald_alpha = t.ewald_alpha;
       g.terms.ewald_rc2 = t.ewald_rc2;
       g.terms.exact_erf = t.exact_erf;
@@ -1112,6 +1113,10 @@ int pmgpu_force_pme_add(pmgpu_system *h, double alpha, double rc, int order,
     f.terms.ewald_alpha = alpha;
     f.terms.ewald_rc2 = rc * rc;
     f.terms.exact_erf = exact_erf ? 1 : 0;
+    if (!exact_erf) {
+      PM_CHECK(ewald_table_build(s, &f));
+      f.terms.ewtab = f.d_ewtab;
+    }
     int li = list_for(s, rc, default_skin(s, rc));
     if (li < 0) return -li;
     f.list_index = li;
@@ -1502,7 +1507,7 @@ int pmgpu_footprint_estimate(int n_atoms, const double box[3], double reach,
     const double r = reach + 5.0;
     const double cap = 4.18879 * r * r * r * dens / 8.0 / kRowParts * 1.6 + 64;
     b += ns * (16 + 16 + 32 + 4 + 4 + 8 + 24) + n * (4 + 4 + 4 + 24 + 24) + nkeys * 4 + ncol * 16 +
-         ncl * kRowParts * (12 * cap + 4);
+         ncl * kRowParts * (44 * cap + 8);
   }
   if (grid) {
     double G = (double)grid[0] * grid[1] * grid[2];

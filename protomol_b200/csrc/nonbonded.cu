@@ -489,6 +489,8 @@ struct BuildArgs {
   uint2 *tiles;
   unsigned *tmod;
   int *tile_count;
+  uint2 *jlanes;
+  int *jl_count;
   int *status;
 };
 __device__ __forceinline__ void build_body(const BuildArgs &B, Blk blk) {
@@ -502,6 +504,8 @@ __device__ __forceinline__ void build_body(const BuildArgs &B, Blk blk) {
   uint2 *__restrict__ tiles = B.tiles;
   unsigned *__restrict__ tmod = B.tmod;
   int *__restrict__ tile_count = B.tile_count;
+  uint2 *__restrict__ jlanes = B.jlanes;
+  int *__restrict__ jl_count = B.jl_count;
   int *__restrict__ status = B.status;
   if (!*rebuild) return;
   constexpr unsigned kAll = 0xffffffffu;
@@ -516,7 +520,7 @@ __device__ __forceinline__ void build_body(const BuildArgs &B, Blk blk) {
   const int ci = rw / kRowParts, part = rw - ci * kRowParts;
   const float4 l0 = bb[4 * ci], h0 = bb[4 * ci + 1], l1 = bb[4 * ci + 2], h1 = bb[4 * ci + 3];
   if (l0.w + l1.w == 0.f) {
-    if (lane == 0) tile_count[rw] = 0;
+    if (lane == 0) tile_count[rw] = jl_count[rw] = 0;
     continue;
   }
   float ilo[3] = {fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z)};
@@ -532,7 +536,7 @@ __device__ __forceinline__ void build_body(const BuildArgs &B, Blk blk) {
   }
   if (!sane) {
     if (lane == 0) {
-      tile_count[rw] = 0;
+      tile_count[rw] = jl_count[rw] = 0;
       atomicOr(status, ST_NONFINITE);
     }
     continue;
@@ -782,9 +786,45 @@ __device__ __forceinline__ void build_body(const BuildArgs &B, Blk blk) {
       // at least the largest row's need and repeats the work
       atomicOr(status, ST_LIST_OVERFLOW);
       atomicMax(rebuild + 2, count);
-      count = a.limit;
     }
-    tile_count[rw] = count;
+    tile_count[rw] = min(count, a.limit);
+  }
+  // the row's j-lane entries, in tile order, from the tiles just written
+  // (visible to the warp after the __syncwarp)
+  __syncwarp();
+  {
+    const int nt = min(count, a.limit);
+    uint2 *erow = jlanes + (size_t)rw * 4 * a.cap;
+    int ne = 0;
+    for (int k0 = 0; k0 < nt; k0 += 32) {
+      const int k = k0 + lane;
+      uint2 t = make_uint2(0u, 0u);
+      unsigned tz = 0u;
+      if (k < nt) {
+        t = row[k];
+        if (t.x & kModFlag) tz = rowmod[k];
+      }
+      int nb = 0;
+#pragma unroll
+      for (int q = 0; q < 4; q++) nb += ((t.y >> (8 * q)) & 0xFFu) != 0u;
+      int incl = nb;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(kAll, incl, o);
+        if (lane >= o) incl += v;
+      }
+      int at = ne + incl - nb;
+      const uint32_t hj = t.x & kJMask, sh = (t.x >> kShiftBits) & kShiftMask;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint32_t mb = (t.y >> (8 * q)) & 0xFFu;
+        if (mb)
+          erow[at++] = make_uint2((4u * hj + q) | (sh << kJSlotBits),
+                                  mb | (((tz >> (8 * q)) & 0xFFu) << 8));
+      }
+      ne += __shfl_sync(kAll, incl, 31);
+    }
+    if (lane == 0) jl_count[rw] = ne;
   }
   __syncwarp();  // the next row reuses the staging
   }  // rows
@@ -894,6 +934,9 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   PM_CUDA(cudaMemsetAsync(nl->d_fslot, 0, sizeof(long long) * 3 * ns, s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_tiles, sizeof(uint2) * (size_t)cap * nl->nrows));
   PM_CHECK(dev_alloc(s, &nl->d_tmod, sizeof(unsigned) * (size_t)cap * nl->nrows));
+  PM_CHECK(dev_alloc(s, &nl->d_jlanes, sizeof(uint2) * 4 * (size_t)cap * nl->nrows));
+  PM_CHECK(dev_alloc(s, &nl->d_jl_count, sizeof(int) * std::max(1, nl->nrows)));
+  PM_CUDA(cudaMemsetAsync(nl->d_jl_count, 0, sizeof(int) * std::max(1, nl->nrows), s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_tile_count, sizeof(int) * std::max(1, nl->nrows)));
   PM_CUDA(cudaMemsetAsync(nl->d_tile_count, 0, sizeof(int) * std::max(1, nl->nrows),
                           s->stream));
@@ -910,7 +953,7 @@ int nb_list_free(System *s, NeighborList *nl) {
                   nl->d_col_cursor, nl->d_col_base, nl->d_key_start, nl->d_sorted,
                   nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
                   nl->d_bb, nl->d_fslot, nl->d_slot_of, nl->d_tiles, nl->d_tmod,
-                  nl->d_tile_count, nl->d_maxdisp,
+                  nl->d_jlanes, nl->d_jl_count, nl->d_tile_count, nl->d_maxdisp,
                   nl->d_rebuild};
   for (void *p : ptrs) dev_free(s, p);
   nl->d_key = nl->d_unsorted = nl->d_col_count = nl->d_col_u = nl->d_col_cursor = nullptr;
@@ -922,6 +965,8 @@ int nb_list_free(System *s, NeighborList *nl) {
   nl->d_xw = nullptr;
   nl->d_tiles = nullptr;
   nl->d_tmod = nullptr;
+  nl->d_jlanes = nullptr;
+  nl->d_jl_count = nullptr;
   nl->d_fslot = nullptr;
   nl->d_slot_of = nullptr;
   nl->d_maxdisp = nullptr;
@@ -983,7 +1028,7 @@ static void list_args(System *s, NeighborList *nl, ListArgs *L) {
   ba.excl_class = s->d_excl_class;
   L->build = BuildArgs{ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi,
                        nl->d_mol_s, nl->d_bb, nl->d_tiles, nl->d_tmod, nl->d_tile_count,
-                       s->d_status};
+                       nl->d_jlanes, nl->d_jl_count, s->d_status};
 }
 
 // Sort + (conditional) list build + per-step gather.  Never synchronises
@@ -1041,6 +1086,61 @@ int nb_build(System *s, NeighborList *nl) {
 
 static int pair_splits(int nclusters);
 
+// The Ewald real-space force factor of one pair in FP64, the reference's
+// form with the A&S erfc (MathUtilities.cpp:39-49; Abramowitz & Stegun
+// 7.1.26): [erfc(a r)/r + 2a/sqrt(pi) exp(-a^2 r^2)] / r^2.
+static double ewald_factor(double alpha, double r2) {
+  const double r = std::sqrt(r2), x = alpha * r;
+  const double t = 1.0 / (1.0 + 0.3275911 * x);
+  const double poly =
+      t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 + t * (-1.453152027 +
+                                                                    t * 1.061405429))));
+  const double ex = std::exp(-x * x);
+  return (poly * ex / r + 2.0 * alpha / std::sqrt(M_PI) * ex) / r2;
+}
+
+// The cubic of each table interval through the factor at the four
+// Chebyshev nodes of the interval (near-minimax), as monomials in t.
+int ewald_table_build(System *s, Force *f) {
+  std::vector<float4> tab(kEwTabN);
+  const int sub = 1 << kEwTabSubBits;
+  double tn[4];
+  for (int k = 0; k < 4; k++) tn[k] = 0.5 + 0.5 * std::cos((2 * k + 1) * M_PI / 8.0);
+  for (int i = 0; i < kEwTabN; i++) {
+    const int e = kEwTabLoExp + i / sub, k = i % sub;
+    const double a = std::ldexp(1.0 + (double)k / sub, e);
+    const double b = std::ldexp(1.0 + (double)(k + 1) / sub, e);
+    // Vandermonde system V c = y for c0 + c1 t + c2 t^2 + c3 t^3
+    double V[4][5];
+    for (int r = 0; r < 4; r++) {
+      double tp = 1.0;
+      for (int c = 0; c < 4; c++, tp *= tn[r]) V[r][c] = tp;
+      V[r][4] = ewald_factor(f->alpha, a + tn[r] * (b - a));
+    }
+    for (int c = 0; c < 4; c++) {  // Gaussian elimination with partial pivoting
+      int pr = c;
+      for (int r = c + 1; r < 4; r++)
+        if (std::fabs(V[r][c]) > std::fabs(V[pr][c])) pr = r;
+      for (int q = 0; q < 5; q++) std::swap(V[c][q], V[pr][q]);
+      for (int r = 0; r < 4; r++) {
+        if (r == c) continue;
+        const double m = V[r][c] / V[c][c];
+        for (int q = c; q < 5; q++) V[r][q] -= m * V[c][q];
+      }
+    }
+    tab[i] = make_float4((float)(V[0][4] / V[0][0]), (float)(V[1][4] / V[1][1]),
+                         (float)(V[2][4] / V[2][2]), (float)(V[3][4] / V[3][3]));
+  }
+  if (f->d_ewtab) dev_free(s, f->d_ewtab);
+  f->d_ewtab = nullptr;
+  PM_CHECK(dev_alloc(s, &f->d_ewtab, sizeof(float4) * kEwTabN));
+  PM_CUDA(cudaMemcpyAsync(f->d_ewtab, tab.data(), sizeof(float4) * kEwTabN,
+                          cudaMemcpyHostToDevice, s->stream));
+  // the host vector goes out of scope: wait for the copy
+  PM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMGPU_OK;
+}
+
 template <typename Real>
 static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
                            const PairTerms &t) {
@@ -1094,8 +1194,15 @@ static void fill_pair_args(PairArgs<Real> &a, System *s, NeighborList *nl,
   a.excl_start = s->d_excl_start;
   a.excl_partner = s->d_excl_partner;
   a.excl_class = s->d_excl_class;
+  // the table covers r^2 below 2^(kEwTabLoExp + kEwTabOctaves)
+  a.ewtab = sizeof(Real) == 4 && (t.mask & TERM_EWALD) && !t.exact_erf &&
+                    a.max_hi < std::ldexp(1.0, kEwTabLoExp + kEwTabOctaves)
+                ? t.ewtab
+                : nullptr;
   a.tiles = nl->d_tiles;
   a.tmod = nl->d_tmod;
+  a.jlanes = nl->d_jlanes;
+  a.jl_count = nl->d_jl_count;
   a.tile_count = nl->d_tile_count;
   a.xhi = nl->d_xhi;
   a.xlo = nl->d_xlo;
@@ -1183,10 +1290,16 @@ static void launch_force_spec(PairArgs<Real> &a, cudaStream_t st) {
     const long long items = (long long)a.nclusters * a.splits;
     const int nb = (int)((items + kJlWarps - 1) / kJlWarps);
     if (nb == 0) return;
-    if (a.ntypes <= kJlMaxTypes)
-      k_pairs_jl<TERMS, SPEC, true><<<nb, kJlWarps * 32, 0, st>>>(a);
-    else
-      k_pairs_jl<TERMS, SPEC, false><<<nb, kJlWarps * 32, 0, st>>>(a);
+    // the Ewald force table for the LJ + Ewald real form when the list has one
+    constexpr bool kTab = TERMS == (TERM_LJ | TERM_EWALD) && SPEC::exact == 0;
+    const bool tab = kTab && a.ewtab != nullptr;
+    if (a.ntypes <= kJlMaxTypes) {
+      if (tab) k_pairs_jl<TERMS, SPEC, true, kTab><<<nb, kJlWarps * 32, 0, st>>>(a);
+      else k_pairs_jl<TERMS, SPEC, true, false><<<nb, kJlWarps * 32, 0, st>>>(a);
+    } else {
+      if (tab) k_pairs_jl<TERMS, SPEC, false, kTab><<<nb, kJlWarps * 32, 0, st>>>(a);
+      else k_pairs_jl<TERMS, SPEC, false, false><<<nb, kJlWarps * 32, 0, st>>>(a);
+    }
   } else {
     launch_pairs_spec<Real, TERMS, SPEC>(a, st, PAIR_FORCE);
   }
@@ -1307,6 +1420,7 @@ struct NbBatch {
   int terms = 0;
   int form = PMGPU_PAIRK_GENERIC;  // the specialised form of the jl members
   int smem_lj = 1;
+  int tab = 1;                         // every jl member has the Ewald force table
   BatchTable<PairArgs<float>> jl;      // members with the specialised force-only form
   BatchTable<PairArgs<float>> gforce;  // members without one (force-only, generic kernel)
   BatchTable<PairArgs<float>> energy;  // every member on energy steps
@@ -1355,6 +1469,7 @@ int nb_batch_build(NbBatch *b, System *const *m, int n, const PairTerms *terms,
   b->terms = terms[0].mask;
   b->form = PMGPU_PAIRK_GENERIC;
   b->smem_lj = 1;
+  b->tab = 1;
   for (int k = 0; k < n; k++) {
     System *s = m[k];
     NeighborList *nl = &s->lists[0];
@@ -1380,6 +1495,7 @@ int nb_batch_build(NbBatch *b, System *const *m, int n, const PairTerms *terms,
         return fail(PMGPU_ERR_UNSUPPORTED, "ensemble members need one pair-kernel form");
       b->form = form;
       b->smem_lj = b->smem_lj && a.ntypes <= kJlMaxTypes;
+      b->tab = b->tab && a.ewtab != nullptr;
       PairArgs<float> fa = a;
       fa.splits = splits && splits[k] > 0 ? std::min(splits[k], kJlMaxSplits)
                                           : jl_splits(fa.nclusters);
@@ -1451,12 +1567,15 @@ static int generic_batch(BatchTable<PairArgs<float>> &t, int terms, int mode, cu
 
 template <int TERMS, typename SPEC>
 static void jl_batch(NbBatch *b, BatchTable<PairArgs<float>> &t, cudaStream_t st) {
-  if (b->smem_lj)
-    k_pairs_jl_batch<TERMS, SPEC, true><<<t.total(), kJlWarps * 32, 0, st>>>(t.d, t.d_first,
-                                                                            t.members());
-  else
-    k_pairs_jl_batch<TERMS, SPEC, false><<<t.total(), kJlWarps * 32, 0, st>>>(t.d, t.d_first,
-                                                                             t.members());
+  constexpr bool kTab = TERMS == (TERM_LJ | TERM_EWALD) && SPEC::exact == 0;
+  const int g = t.total(), nm = t.members(), T = kJlWarps * 32;
+  if (kTab && b->tab) {
+    if (b->smem_lj) k_pairs_jl_batch<TERMS, SPEC, true, kTab><<<g, T, 0, st>>>(t.d, t.d_first, nm);
+    else k_pairs_jl_batch<TERMS, SPEC, false, kTab><<<g, T, 0, st>>>(t.d, t.d_first, nm);
+  } else {
+    if (b->smem_lj) k_pairs_jl_batch<TERMS, SPEC, true, false><<<g, T, 0, st>>>(t.d, t.d_first, nm);
+    else k_pairs_jl_batch<TERMS, SPEC, false, false><<<g, T, 0, st>>>(t.d, t.d_first, nm);
+  }
 }
 
 // The pair forces of every member: force-only (the inner MD steps; the

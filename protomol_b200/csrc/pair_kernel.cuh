@@ -51,6 +51,9 @@ struct PairArgs {
   const int *excl_start, *excl_partner, *excl_class;
   const uint2 *tiles;
   const unsigned *tmod;  // modified masks of flagged tiles
+  const uint2 *jlanes;   // j-lane entries (force-only kernel)
+  const float4 *ewtab;   // Ewald real-space force table (null: analytic)
+  const int *jl_count;   // entries per row
   const int *tile_count;
   const float4 *xhi, *xlo;
   const double4 *xw;
@@ -266,6 +269,32 @@ __device__ __forceinline__ Real pair_force_p(const PairArgs<Real> &a, const P4 &
     f += (en + a.a2pi * ee) * rinv2;
   }
   return f;
+}
+
+// pair_force_p of the LJ + Ewald real force-only kernel with the Ewald
+// factor read from the force table (kEwTabN cubics in shared memory): no
+// square root, exponential or erfc per pair.  r2 must lie in the table's
+// range [2^kEwTabLoExp, 2^(kEwTabLoExp + kEwTabOctaves)); others read the
+// nearest end interval (the callers keep them out of the accepted pairs).
+template <typename SPEC, bool MOD>
+__device__ __forceinline__ float pair_force_tab(const PairArgs<float> &a, const float4 &p,
+                                                float r2, float qq, bool modified,
+                                                const float4 *s_ew) {
+  const float rinv2 = __fdividef(1.f, r2);
+  const float A = MOD && modified ? p.z : p.x;
+  const float B = MOD && modified ? p.w : p.y;
+  const float r6 = rinv2 * rinv2 * rinv2;
+  const float r6B = B * r6;
+  const float r12A = A * r6 * r6;
+  float ff = (12.f * r12A - 6.f * r6B) * rinv2;
+  switch_fast<float, SPEC::lj>(a.lj_sw, r2, 0.f, ff, r12A - r6B);
+  if (MOD) qq = modified ? qq * a.csf : qq;
+  const unsigned bits = __float_as_uint(r2);
+  const int idx = min(max((int)(bits >> (23 - kEwTabSubBits)) - (int)kEwTabBase, 0), kEwTabN - 1);
+  const float t =
+      __uint_as_float(((bits << kEwTabSubBits) & 0x007FFFFFu) | 0x3F800000u) - 1.f;
+  const float4 c = s_ew[idx];
+  return fmaf(qq, fmaf(t, fmaf(t, fmaf(t, c.w, c.z), c.y), c.x), ff);
 }
 
 template <typename Real, int TERMS, typename SPEC, bool MOD>
@@ -708,12 +737,13 @@ __global__ void __launch_bounds__(kPairWarps * 32, PairOccupancy<Real, MODE, SPE
 constexpr int kJlWarps = 8;
 constexpr int kJlMaxTypes = 16;  // LJ tables staged in shared memory up to this many types
 constexpr int kJlMaxSplits = 16;  // warps one i cluster's tiles may be divided over
+constexpr float kEwTabMin = 1.0f / (1 << -kEwTabLoExp);  // the table's lowest r^2
 
-// The eight pairs of one lane's j atom with the cluster's i atoms; mi
-// holds the pairs within max_hi (the queue's test), so a pair of mi beyond
-// max_lo is a band pair.
-template <int TERMS, typename SPEC, bool MOD, bool SMEM_LJ>
+// The eight pairs of one lane's j atom with the cluster's i atoms (mi: the
+// pairs of the list's interaction mask).
+template <int TERMS, typename SPEC, bool MOD, bool SMEM_LJ, bool TAB>
 __device__ __forceinline__ void jl_pairs8(const PairArgs<float> &a, const float4 *s_lj,
+                                          const float4 *s_ew,
                                           const float4 *xi, const int *ti, float rjx, float rjy,
                                           float rjz, float qj, int tj, unsigned mi, unsigned mm,
                                           float (&fi)[8][3], float &fjx, float &fjy, float &fjz,
@@ -724,13 +754,17 @@ __device__ __forceinline__ void jl_pairs8(const PairArgs<float> &a, const float4
     const float dx = rjx - x.x, dy = rjy - x.y, dz = rjz - x.z;
     const float r2 = dx * dx + dy * dy + dz * dz;
     const bool on = (mi >> il) & 1u;
-    const bool act = on && r2 <= a.max_lo;
-    band |= (on && !act) ? (1u << il) : 0u;
+    // (table form: pairs closer than the table's range take the exact path)
+    const bool act = on && r2 <= a.max_lo && (!TAB || r2 >= kEwTabMin);
+    band |= (on && !act && r2 <= a.max_hi) ? (1u << il) : 0u;
     npairs += act;
     const float rr = act ? r2 : 1.f;
     const float4 p = SMEM_LJ ? s_lj[ti[il] + tj] : __ldg(a.lj32 + ti[il] + tj);
-    float f = pair_force_p<float, TERMS, SPEC, MOD>(a, p, rr, x.w * qj,
-                                                    MOD && ((mm >> il) & 1u));
+    float f;
+    if constexpr (TAB)
+      f = pair_force_tab<SPEC, MOD>(a, p, rr, x.w * qj, MOD && ((mm >> il) & 1u), s_ew);
+    else
+      f = pair_force_p<float, TERMS, SPEC, MOD>(a, p, rr, x.w * qj, MOD && ((mm >> il) & 1u));
     f = act ? f : 0.f;
     fjx = fmaf(dx, f, fjx);
     fjy = fmaf(dy, f, fjy);
@@ -741,107 +775,28 @@ __device__ __forceinline__ void jl_pairs8(const PairArgs<float> &a, const float4
   }
 }
 
-// Per-warp queue of j lanes that have at least one i atom in range: the
-// candidates of each batch of 8 tiles are tested (the eight FP32 distances,
-// cheap against the pair arithmetic) and only the active ones are queued;
-// the pair arithmetic runs on full warps of queued lanes.  About half of a
-// tile's j lanes have no i atom within the cutoff, so this halves the
-// pair evaluations.  The queue keeps the tile order, so the sums are a
-// function of the list alone.
-constexpr int kJlQueue = 64;
-struct JlQueue {
-  float x[kJlQueue], y[kJlQueue], z[kJlQueue], q[kJlQueue];
-  int t[kJlQueue];     // j type
-  int m[kJlQueue];     // i atoms in range (bits 0-7), modified pairs (bits 8-15)
-  int slot[kJlQueue];  // j slot
-};
-
-// The pair arithmetic of up to 32 queued j lanes (lane < cnt) against the
-// warp's i cluster.
-template <int TERMS, typename SPEC, bool SMEM_LJ>
-__device__ __forceinline__ void jl_process(const PairArgs<float> &a, const float4 *s_lj,
-                                           const float4 *xi, const int *ti, const int *oi,
-                                           const JlQueue &qu, int cnt, int lane, int ci,
-                                           float (&fi)[8][3], int &npairs) {
-  constexpr unsigned kAll = 0xffffffffu;
-  unsigned mi = 0u, mm = 0u;
-  int jslot = 0, tj = 0;
-  float rjx = 0.f, rjy = 0.f, rjz = 0.f, qj = 0.f;
-  if (lane < cnt) {
-    rjx = qu.x[lane];
-    rjy = qu.y[lane];
-    rjz = qu.z[lane];
-    qj = qu.q[lane];
-    tj = qu.t[lane];
-    const int m = qu.m[lane];
-    mi = (unsigned)m & 0xFFu;
-    mm = ((unsigned)m >> 8) & 0xFFu;
-    jslot = qu.slot[lane];
-  }
-  float fjx = 0.f, fjy = 0.f, fjz = 0.f;
-  unsigned band = 0u;
-  // modified (scaled 1-4) pairs are rare: batches without any take the
-  // path without their selects
-  if (__any_sync(kAll, mm != 0u))
-    jl_pairs8<TERMS, SPEC, true, SMEM_LJ>(a, s_lj, xi, ti, rjx, rjy, rjz, qj, tj, mi, mm, fi,
-                                          fjx, fjy, fjz, band, npairs);
-  else
-    jl_pairs8<TERMS, SPEC, false, SMEM_LJ>(a, s_lj, xi, ti, rjx, rjy, rjz, qj, tj, mi, mm, fi,
-                                           fjx, fjy, fjz, band, npairs);
-  // pairs within the rounding band of the cutoff: the exact FP64 test
-  // (rare; their i forces go out as atomics, so this path keeps none of
-  // the register-held sums live)
-  if (__any_sync(kAll, band != 0u)) {
-    const int oj = band ? a.sorted[jslot] : -1;
-    while (band) {
-      const int il = __ffs(band) - 1;
-      band &= band - 1u;
-      const float4 x = xi[il];
-      const float dx = rjx - x.x, dy = rjy - x.y, dz = rjz - x.z;
-      const float r2 = dx * dx + dy * dy + dz * dz;
-      if (exact_r2(a, oi[il], oj, (double)dx, (double)dy, (double)dz) > a.max_cut2) continue;
-      const float4 p = SMEM_LJ ? s_lj[ti[il] + tj] : __ldg(a.lj32 + ti[il] + tj);
-      const float f = pair_force_p<float, TERMS, SPEC, true>(a, p, r2, x.w * qj, (mm >> il) & 1u);
-      fjx = fmaf(dx, f, fjx);
-      fjy = fmaf(dy, f, fjy);
-      fjz = fmaf(dz, f, fjz);
-      long long *di = a.fslot + 8 * ci + il;
-      red_add(di, fixed_force(-dx * f));
-      red_add(di + a.ns, fixed_force(-dy * f));
-      red_add(di + 2 * (size_t)a.ns, fixed_force(-dz * f));
-      npairs++;
-    }
-  }
-  if (mi) {
-    long long *dst = a.fslot + jslot;
-    red_add(dst, fixed_force(fjx));
-    red_add(dst + a.ns, fixed_force(fjy));
-    red_add(dst + 2 * (size_t)a.ns, fixed_force(fjz));
-  }
-}
-
-template <int TERMS, typename SPEC, bool SMEM_LJ>
+template <int TERMS, typename SPEC, bool SMEM_LJ, bool TAB>
 __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk) {
   constexpr unsigned kAll = 0xffffffffu;
   __shared__ float4 s_lj[SMEM_LJ ? kJlMaxTypes * kJlMaxTypes : 1];
+  __shared__ float4 s_ew[TAB ? kEwTabN : 1];
   __shared__ float4 s_xi[kJlWarps][8];   // i atoms from the reference point, charge
   __shared__ int s_ti[kJlWarps][8];      // i type * ntypes
   __shared__ int s_oi[kJlWarps][8];      // i atom (-1: padding)
   __shared__ double s_wc[kJlWarps][3];   // reference point (FP64)
-  __shared__ JlQueue s_q[kJlWarps];
-  if (SMEM_LJ) {
+  if (SMEM_LJ)
     for (int k = threadIdx.x; k < a.ntypes * a.ntypes; k += blockDim.x) s_lj[k] = a.lj32[k];
-    __syncthreads();
-  }
+  if (TAB)
+    for (int k = threadIdx.x; k < kEwTabN; k += blockDim.x) s_ew[k] = __ldg(a.ewtab + k);
+  if (SMEM_LJ || TAB) __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int tb = lane >> 2, jl = lane & 3;
-  JlQueue &qu = s_q[wib];
   int npairs = 0;
   const int nitems = a.nclusters * a.splits;
+  const size_t rowcap = 4 * (size_t)a.cap;  // entries per row
   for (int gw = blk.x * kJlWarps + wib; gw < nitems; gw += blk.n * kJlWarps) {
     const int ci = gw / a.splits, sp = gw - ci * a.splits;
     static_assert(kRowParts == 4, "one int4 of row counts per cluster");
-    const int4 c4 = *reinterpret_cast<const int4 *>(a.tile_count + kRowParts * ci);
+    const int4 c4 = *reinterpret_cast<const int4 *>(a.jl_count + kRowParts * ci);
     const int p1 = c4.x, p2 = p1 + c4.y, p3 = p2 + c4.z, cnt = p3 + c4.w;
     const int t0 = (int)((long long)cnt * sp / a.splits);
     const int t1 = (int)((long long)cnt * (sp + 1) / a.splits);
@@ -849,7 +804,7 @@ __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk)
     __syncwarp();  // the previous item's reads of this warp's staging are done
     if (lane < 8) {
       const int islot = 8 * ci + lane;
-      const double4 w0 = a.xw[8 * ci];  // a cluster with tiles has an atom in its first slot
+      const double4 w0 = a.xw[8 * ci];  // a cluster with entries has an atom in its first slot
       const double4 wi = a.xw[islot];
       const int oi = a.sorted[islot];
       s_xi[wib][lane] = make_float4((float)(wi.x - w0.x), (float)(wi.y - w0.y),
@@ -864,86 +819,77 @@ __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk)
     float fi[8][3];
 #pragma unroll
     for (int k = 0; k < 8; k++) fi[k][0] = fi[k][1] = fi[k][2] = 0.f;
-    int qn = 0;  // queued j lanes
-    // tile idx of the cluster's row parts read one after the other; the
-    // record of the next batch is loaded one batch ahead
-    auto tile_index = [&](int idx) -> size_t {
-      const int p = (idx >= p1) + (idx >= p2) + (idx >= p3);
-      const int off = idx - (p == 0 ? 0 : (p == 1 ? p1 : (p == 2 ? p2 : p3)));
-      return (size_t)(kRowParts * ci + p) * a.cap + off;
-    };
-    uint2 next = t0 + tb < t1 ? __ldg(a.tiles + tile_index(t0 + tb)) : make_uint2(0u, 0u);
-    for (int b0 = t0; b0 < t1; b0 += 8) {
-      const int idx = b0 + tb;
-      const uint2 tile = next;
-      if (idx + 8 < t1) next = __ldg(a.tiles + tile_index(idx + 8));
-      unsigned act = 0u;
-      int m = 0, jslot = 0, tj = 0;
+    for (int b0 = t0; b0 < t1; b0 += 32) {
+      const int idx = b0 + lane;
+      unsigned mi = 0u, mm = 0u;
+      int jslot = 0, tj = 0;
       float rjx = 0.f, rjy = 0.f, rjz = 0.f, qj = 0.f;
       if (idx < t1) {
-        const size_t ti0 = tile_index(idx);
-        const int hj = (int)(tile.x & kJMask);
-        const int sh = (int)((tile.x >> kShiftBits) & kShiftMask);
-        const unsigned mi = (tile.y >> (8 * jl)) & 0xFFu;
-        const unsigned mm =
-            (tile.x & kModFlag) ? (__ldg(a.tmod + ti0) >> (8 * jl)) & 0xFFu : 0u;
-        jslot = 4 * hj + jl;
-        if (mi) {
-          const double4 wj = a.xw[jslot];
-          // the j atom in the tile's image (d = xj + s L - xi), from the
-          // reference point; the image offsets are exact (-L, 0 or L)
-          const int sx = sh & 3, sy = (sh >> 2) & 3, sz = (sh >> 4) & 3;
-          const double ox = sx == 1 ? 0.0 : (sx == 0 ? -a.box.e[0] : a.box.e[0]);
-          const double oy = sy == 1 ? 0.0 : (sy == 0 ? -a.box.e[1] : a.box.e[1]);
-          const double oz = sz == 1 ? 0.0 : (sz == 0 ? -a.box.e[2] : a.box.e[2]);
-          rjx = (float)((wj.x + ox) - s_wc[wib][0]);
-          rjy = (float)((wj.y + oy) - s_wc[wib][1]);
-          rjz = (float)((wj.z + oz) - s_wc[wib][2]);
-          qj = (float)wj.w;
-          tj = __float_as_int(__ldg(&a.xlo[jslot].w));
-          // the i atoms in range of this j atom (the band pairs included)
-#pragma unroll
-          for (int il = 0; il < 8; il++) {
-            const float4 x = xi[il];
-            const float dx = rjx - x.x, dy = rjy - x.y, dz = rjz - x.z;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            act |= (((mi >> il) & 1u) && r2 <= a.max_hi) ? (1u << il) : 0u;
-          }
-          m = (int)(act | ((mm & act) << 8));
+        // entry idx of the cluster's row parts read one after the other
+        const int p = (idx >= p1) + (idx >= p2) + (idx >= p3);
+        const int off = idx - (p == 0 ? 0 : (p == 1 ? p1 : (p == 2 ? p2 : p3)));
+        const uint2 e = __ldg(a.jlanes + (size_t)(kRowParts * ci + p) * rowcap + off);
+        jslot = (int)(e.x & kJSlotMask);
+        const int sh = (int)(e.x >> kJSlotBits);
+        mi = e.y & 0xFFu;
+        mm = (e.y >> 8) & 0xFFu;
+        const double4 wj = a.xw[jslot];
+        // the j atom in the entry's image (d = xj + s L - xi), from the
+        // reference point; the image offsets are exact (-L, 0 or L)
+        const int sx = sh & 3, sy = (sh >> 2) & 3, sz = (sh >> 4) & 3;
+        const double ox = sx == 1 ? 0.0 : (sx == 0 ? -a.box.e[0] : a.box.e[0]);
+        const double oy = sy == 1 ? 0.0 : (sy == 0 ? -a.box.e[1] : a.box.e[1]);
+        const double oz = sz == 1 ? 0.0 : (sz == 0 ? -a.box.e[2] : a.box.e[2]);
+        rjx = (float)((wj.x + ox) - s_wc[wib][0]);
+        rjy = (float)((wj.y + oy) - s_wc[wib][1]);
+        rjz = (float)((wj.z + oz) - s_wc[wib][2]);
+        qj = (float)wj.w;
+        tj = __float_as_int(__ldg(&a.xlo[jslot].w));
+      }
+      float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+      unsigned band = 0u;
+      // modified (scaled 1-4) pairs are rare: batches without any take the
+      // path without their selects
+      if (__any_sync(kAll, mm != 0u))
+        jl_pairs8<TERMS, SPEC, true, SMEM_LJ, TAB>(a, s_lj, s_ew, xi, ti, rjx, rjy, rjz, qj, tj,
+                                                   mi, mm, fi,
+                                              fjx, fjy, fjz, band, npairs);
+      else
+        jl_pairs8<TERMS, SPEC, false, SMEM_LJ, TAB>(a, s_lj, s_ew, xi, ti, rjx, rjy, rjz, qj, tj,
+                                                    mi, mm,
+                                               fi, fjx, fjy, fjz, band, npairs);
+      // pairs within the rounding band of the cutoff: the exact FP64 test
+      // (rare; their i forces go out as atomics, so this path keeps none of
+      // the register-held sums live)
+      if (__any_sync(kAll, band != 0u)) {
+        const int oj = band ? a.sorted[jslot] : -1;
+        while (band) {
+          const int il = __ffs(band) - 1;
+          band &= band - 1u;
+          const float4 x = xi[il];
+          const float dx = rjx - x.x, dy = rjy - x.y, dz = rjz - x.z;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          if (exact_r2(a, s_oi[wib][il], oj, (double)dx, (double)dy, (double)dz) > a.max_cut2)
+            continue;
+          const float4 p = SMEM_LJ ? s_lj[ti[il] + tj] : __ldg(a.lj32 + ti[il] + tj);
+          const float f = pair_force_p<float, TERMS, SPEC, true>(a, p, r2, x.w * qj,
+                                                                 (mm >> il) & 1u);
+          fjx = fmaf(dx, f, fjx);
+          fjy = fmaf(dy, f, fjy);
+          fjz = fmaf(dz, f, fjz);
+          long long *di = a.fslot + 8 * ci + il;
+          red_add(di, fixed_force(-dx * f));
+          red_add(di + a.ns, fixed_force(-dy * f));
+          red_add(di + 2 * (size_t)a.ns, fixed_force(-dz * f));
+          npairs++;
         }
       }
-      const unsigned vote = __ballot_sync(kAll, act != 0u);
-      if (act) {
-        const int at = qn + __popc(vote & ((1u << lane) - 1u));
-        qu.x[at] = rjx;
-        qu.y[at] = rjy;
-        qu.z[at] = rjz;
-        qu.q[at] = qj;
-        qu.t[at] = tj;
-        qu.m[at] = m;
-        qu.slot[at] = jslot;
+      if (mi) {
+        long long *dst = a.fslot + jslot;
+        red_add(dst, fixed_force(fjx));
+        red_add(dst + a.ns, fixed_force(fjy));
+        red_add(dst + 2 * (size_t)a.ns, fixed_force(fjz));
       }
-      qn += __popc(vote);
-      if (qn >= 32) {
-        __syncwarp();
-        jl_process<TERMS, SPEC, SMEM_LJ>(a, s_lj, xi, ti, s_oi[wib], qu, 32, lane, ci, fi, npairs);
-        __syncwarp();  // every lane has read its entry before the rest moves up
-        qn -= 32;
-        if (lane < qn) {
-          qu.x[lane] = qu.x[32 + lane];
-          qu.y[lane] = qu.y[32 + lane];
-          qu.z[lane] = qu.z[32 + lane];
-          qu.q[lane] = qu.q[32 + lane];
-          qu.t[lane] = qu.t[32 + lane];
-          qu.m[lane] = qu.m[32 + lane];
-          qu.slot[lane] = qu.slot[32 + lane];
-        }
-        __syncwarp();
-      }
-    }
-    if (qn > 0) {
-      __syncwarp();
-      jl_process<TERMS, SPEC, SMEM_LJ>(a, s_lj, xi, ti, s_oi[wib], qu, qn, lane, ci, fi, npairs);
     }
     // the i forces summed over the lanes: lane l ends with the totals of i
     // atom (l >> 2) & 7 and writes component l & 3
@@ -966,18 +912,19 @@ __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk)
   }
 }
 
-template <int TERMS, typename SPEC, bool SMEM_LJ>
+template <int TERMS, typename SPEC, bool SMEM_LJ, bool TAB>
 __global__ void __launch_bounds__(kJlWarps * 32, 3) k_pairs_jl(PairArgs<float> a) {
-  pairs_jl_body<TERMS, SPEC, SMEM_LJ>(a, own_blk());
+  pairs_jl_body<TERMS, SPEC, SMEM_LJ, TAB>(a, own_blk());
 }
 
-template <int TERMS, typename SPEC, bool SMEM_LJ>
+template <int TERMS, typename SPEC, bool SMEM_LJ, bool TAB>
 __global__ void __launch_bounds__(kJlWarps * 32, 3)
     k_pairs_jl_batch(const PairArgs<float> *__restrict__ tab, const int *__restrict__ first,
                      int nm) {
   __shared__ __align__(16) unsigned char raw[sizeof(PairArgs<float>)];
   const int m = batch_member(first, nm, blockIdx.x);
-  pairs_jl_body<TERMS, SPEC, SMEM_LJ>(batch_args_shared(tab, m, raw), batch_blk(first, m));
+  pairs_jl_body<TERMS, SPEC, SMEM_LJ, TAB>(batch_args_shared(tab, m, raw),
+                                           batch_blk(first, m));
 }
 
 // Adds the forces accumulated by list slot into the atoms' forces and

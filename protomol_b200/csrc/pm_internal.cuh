@@ -62,6 +62,13 @@ constexpr uint32_t kJMask = 0xFFFFFFu;
 constexpr int kShiftBits = 24;
 constexpr uint32_t kShiftMask = 0x3Fu;
 constexpr uint32_t kModFlag = 1u << 30;
+// j-lane entries (uint2, the force-only kernel's list): for each tile and
+// each of its j atoms with at least one pair in the interaction mask,
+// x = j slot (bits 0..25) | the tile's image code << 26, y = that j atom's
+// byte of the interaction mask | its byte of the modified mask << 8.
+// A row holds up to 4 entries per tile of capacity.
+constexpr int kJSlotBits = 26;
+constexpr uint32_t kJSlotMask = (1u << kJSlotBits) - 1u;
 constexpr int kZeroShift = 1 | (1 << 2) | (1 << 4);
 __host__ __device__ constexpr int shift_code(int sx, int sy, int sz) {
   return (sx + 1) | ((sy + 1) << 2) | ((sz + 1) << 4);
@@ -117,7 +124,23 @@ struct PairTerms {
   int exact_erf;
   double coulomb_scaling;
   int minimal_image;        // cutoff terms see only the minimal image
+  const float4 *ewtab = nullptr;  // Ewald real-space force table (see below)
 };
+
+// Ewald real-space force table of the FP32 force-only kernel: the pair
+// force factor G(r^2) = [erfc(a r)/r + 2a/sqrt(pi) exp(-a^2 r^2)] / r^2 (the
+// A&S erfc the reference uses, NonbondedFullEwaldSystemForce.h:753-858,
+// MathUtilities.cpp:39-49) as cubics in t over intervals of r^2 that split
+// each octave [2^e, 2^(e+1)) into 2^kEwTabSubBits equal parts, for
+// e = kEwTabLoExp .. kEwTabLoExp + kEwTabOctaves - 1.  The interval index
+// and t are bit fields of the FP32 r^2 (exponent and top mantissa bits; the
+// rest of the mantissa).  Interpolation error below 1e-8 relative (FP32
+// evaluation about 1e-7, as the analytic FP32 form).
+constexpr int kEwTabLoExp = -4;      // r^2 from 1/16 A^2
+constexpr int kEwTabOctaves = 11;    // to 128 A^2
+constexpr int kEwTabSubBits = 7;
+constexpr int kEwTabN = kEwTabOctaves << kEwTabSubBits;
+constexpr unsigned kEwTabBase = (unsigned)(127 + kEwTabLoExp) << kEwTabSubBits;
 
 // Device arrays of one cluster-pair list (one per distinct (cutoff, skin)
 // in a system).  Atoms are counting-sorted into ncx x ncy columns of the xy
@@ -172,6 +195,8 @@ struct NeighborList {
   int *d_slot_of = nullptr;  // atom -> slot of the current order (rebuild steps write it)
   uint2 *d_tiles = nullptr;      // nrows rows of cap tiles (row r: cluster r / kRowParts)
   unsigned *d_tmod = nullptr;    // modified masks of the flagged tiles, same indexing
+  uint2 *d_jlanes = nullptr;     // nrows rows of 4 cap j-lane entries
+  int *d_jl_count = nullptr;     // entries per row
   int *d_tile_count = nullptr;   // nrows
   unsigned int *d_maxdisp = nullptr;  // rebuild check: block ticket, max displacement^2 bits
   int *d_rebuild = nullptr;      // rebuild flag, build count, largest row need after an overflow
@@ -200,6 +225,7 @@ struct Force {
   long long *d_grid_fixed = nullptr;  // fixed-point spread target
   float2 *d_cgrid = nullptr;          // complex grid (K1*K2*(K3/2+1))
   float *d_influence = nullptr;       // K1*K2*(K3/2+1) influence function
+  float4 *d_ewtab = nullptr;          // real-space force table (kEwTabN cubics)
   void *d_fft_work = nullptr;         // cuFFT work area shared by both plans
   size_t fft_work_bytes = 0;
   // simplefull
@@ -488,6 +514,8 @@ void launch_stage_pairs(int n, const double *pos, const double *charge, const in
 // pme.cu
 int pme_init(System *s, Force *f);
 int pme_free(System *s, Force *f);
+// builds f->d_ewtab for f->alpha (nonbonded.cu)
+int ewald_table_build(System *s, Force *f);
 int pme_reciprocal(System *s, Force *f, int em);
 int ewald_correction(System *s, Force *f, int em);
 

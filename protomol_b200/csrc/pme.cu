@@ -504,10 +504,13 @@ int pme_free(System *s, Force *f) {
     if (f->plan_c2r) cufftDestroy(f->plan_c2r);
   }
   f->plan_r2c = f->plan_c2r = 0;
-  void *ptrs[] = {f->d_grid, f->d_grid_fixed, f->d_cgrid, f->d_influence, f->d_fft_work};
+  void *ptrs[] = {f->d_grid, f->d_grid_fixed, f->d_cgrid, f->d_influence, f->d_fft_work,
+                  f->d_ewtab};
   for (void *p : ptrs) dev_free(s, p);
   f->d_grid = nullptr; f->d_grid_fixed = nullptr; f->d_cgrid = nullptr;
   f->d_influence = nullptr;
+  f->d_ewtab = nullptr;
+  f->terms.ewtab = nullptr;
   f->d_fft_work = nullptr;
   return PMGPU_OK;
 }
