@@ -593,17 +593,23 @@ __device__ __forceinline__ void pairs_body(const PairArgs<Real> &a, Blk blk) {
           fabs(dz) <= a.half_edge[2]))
       flags &= ~(kQLJ | kQCoul);
     Real jx = 0, jy = 0, jz = 0;
+    // an energy-only pass (the forces of the step come from the force-only
+    // kernel) skips the FP32 force and the j-force sums
+    const bool forces = !(MIXED && ENERGY && a.energy_only);
     if (flags) {
       if ((tile.z >> lane) & 1u) flags |= kQModified;
       if (!MIXED) tj = a.type[a.sorted[jslot]];
       Real en_lj = 0, en_c = 0;
-      const Real f = pair_force<Real, TERMS, SPEC>(a, ljrow, r2, qi * qj, tj, flags, en_lj, en_c);
-      jx = dx * f;
-      jy = dy * f;
-      jz = dz * f;
-      fx -= jx;
-      fy -= jy;
-      fz -= jz;
+      if (forces) {
+        const Real f =
+            pair_force<Real, TERMS, SPEC>(a, ljrow, r2, qi * qj, tj, flags, en_lj, en_c);
+        jx = dx * f;
+        jy = dy * f;
+        jz = dz * f;
+        fx -= jx;
+        fy -= jy;
+        fz -= jz;
+      }
       npairs++;
       if (ENERGY) {
         if (MIXED) {
@@ -629,11 +635,13 @@ __device__ __forceinline__ void pairs_body(const PairArgs<Real> &a, Blk blk) {
       }
     }
     // j's share: summed over its 8 lanes, one atomic per component
-    const unsigned act = __ballot_sync(kAll, flags != 0);
-    const Real js = group8_sum3<Real>(jx, jy, jz, lane);
-    long long *dst = a.fslot + il * a.ns + jslot;
-    const long long v = fixed_force(js);
-    if (il < 3 && ((act >> (8 * jl)) & 0xFFu) && !a.energy_only) red_add(dst, v);
+    if (forces) {
+      const unsigned act = __ballot_sync(kAll, flags != 0);
+      const Real js = group8_sum3<Real>(jx, jy, jz, lane);
+      long long *dst = a.fslot + il * a.ns + jslot;
+      const long long v = fixed_force(js);
+      if (il < 3 && ((act >> (8 * jl)) & 0xFFu)) red_add(dst, v);
+    }
   }
     if (left > 0) {  // next non-empty row part
       do {
@@ -775,6 +783,29 @@ __device__ __forceinline__ void jl_pairs8(const PairArgs<float> &a, const float4
   }
 }
 
+// The j atoms' records of one warp step, staged by cp.async: the FP64
+// wrapped position and charge, and the type.
+struct JlStage {
+  double4 w[32];
+  int t[32];
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 template <int TERMS, typename SPEC, bool SMEM_LJ, bool TAB>
 __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk) {
   constexpr unsigned kAll = 0xffffffffu;
@@ -784,6 +815,7 @@ __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk)
   __shared__ int s_ti[kJlWarps][8];      // i type * ntypes
   __shared__ int s_oi[kJlWarps][8];      // i atom (-1: padding)
   __shared__ double s_wc[kJlWarps][3];   // reference point (FP64)
+  __shared__ JlStage s_js[kJlWarps][2];  // j-atom records of two warp steps
   if (SMEM_LJ)
     for (int k = threadIdx.x; k < a.ntypes * a.ntypes; k += blockDim.x) s_lj[k] = a.lj32[k];
   if (TAB)
@@ -819,23 +851,45 @@ __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk)
     float fi[8][3];
 #pragma unroll
     for (int k = 0; k < 8; k++) fi[k][0] = fi[k][1] = fi[k][2] = 0.f;
-    for (int b0 = t0; b0 < t1; b0 += 32) {
-      const int idx = b0 + lane;
-      unsigned mi = 0u, mm = 0u;
-      int jslot = 0, tj = 0;
+    // Software pipeline over the warp steps (32 entries each): the entries
+    // of step k + 2 are loaded into registers and the j atoms' records of
+    // step k + 1 are copied into this lane's shared-memory slot (cp.async)
+    // while step k computes, so the dependent loads (entry, then the j
+    // atom's record) are in flight during a whole step.  A lane reads only
+    // the slot it copied itself.
+    auto entry_at = [&](int idx) -> uint2 {
+      if (idx >= t1) return make_uint2(0u, 0u);  // mask 0: no entry
+      const int p = (idx >= p1) + (idx >= p2) + (idx >= p3);
+      const int off = idx - (p == 0 ? 0 : (p == 1 ? p1 : (p == 2 ? p2 : p3)));
+      return __ldg(a.jlanes + (size_t)(kRowParts * ci + p) * rowcap + off);
+    };
+    auto stage = [&](uint2 e, int buf) {
+      if (e.y & 0xFFu) {
+        const int js = (int)(e.x & kJSlotMask);
+        JlStage &g = s_js[wib][buf];
+        cp_async16(&g.w[lane], &a.xw[js]);
+        cp_async16(reinterpret_cast<char *>(&g.w[lane]) + 16,
+                   reinterpret_cast<const char *>(&a.xw[js]) + 16);
+        cp_async4(&g.t[lane], &a.xlo[js].w);
+      }
+      cp_async_commit();
+    };
+    uint2 ecur = entry_at(t0 + lane), enext = entry_at(t0 + 32 + lane);
+    stage(ecur, 0);
+    for (int b0 = t0, k = 0; b0 < t1; b0 += 32, k++) {
+      stage(enext, (k + 1) & 1);
+      const uint2 enext2 = entry_at(b0 + 64 + lane);
+      cp_async_wait<1>();  // this step's copies have landed
+      unsigned mi = ecur.y & 0xFFu, mm = (ecur.y >> 8) & 0xFFu;
+      const int jslot = (int)(ecur.x & kJSlotMask);
+      int tj = 0;
       float rjx = 0.f, rjy = 0.f, rjz = 0.f, qj = 0.f;
-      if (idx < t1) {
-        // entry idx of the cluster's row parts read one after the other
-        const int p = (idx >= p1) + (idx >= p2) + (idx >= p3);
-        const int off = idx - (p == 0 ? 0 : (p == 1 ? p1 : (p == 2 ? p2 : p3)));
-        const uint2 e = __ldg(a.jlanes + (size_t)(kRowParts * ci + p) * rowcap + off);
-        jslot = (int)(e.x & kJSlotMask);
-        const int sh = (int)(e.x >> kJSlotBits);
-        mi = e.y & 0xFFu;
-        mm = (e.y >> 8) & 0xFFu;
-        const double4 wj = a.xw[jslot];
+      if (mi) {
+        const JlStage &g = s_js[wib][k & 1];
+        const double4 wj = g.w[lane];
         // the j atom in the entry's image (d = xj + s L - xi), from the
         // reference point; the image offsets are exact (-L, 0 or L)
+        const int sh = (int)(ecur.x >> kJSlotBits);
         const int sx = sh & 3, sy = (sh >> 2) & 3, sz = (sh >> 4) & 3;
         const double ox = sx == 1 ? 0.0 : (sx == 0 ? -a.box.e[0] : a.box.e[0]);
         const double oy = sy == 1 ? 0.0 : (sy == 0 ? -a.box.e[1] : a.box.e[1]);
@@ -844,8 +898,10 @@ __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk)
         rjy = (float)((wj.y + oy) - s_wc[wib][1]);
         rjz = (float)((wj.z + oz) - s_wc[wib][2]);
         qj = (float)wj.w;
-        tj = __float_as_int(__ldg(&a.xlo[jslot].w));
+        tj = g.t[lane];
       }
+      ecur = enext;
+      enext = enext2;
       float fjx = 0.f, fjy = 0.f, fjz = 0.f;
       unsigned band = 0u;
       // modified (scaled 1-4) pairs are rare: batches without any take the
@@ -891,6 +947,7 @@ __device__ __forceinline__ void pairs_jl_body(const PairArgs<float> &a, Blk blk)
         red_add(dst + 2 * (size_t)a.ns, fixed_force(fjz));
       }
     }
+    cp_async_wait<0>();  // no copy of this item is left in flight
     // the i forces summed over the lanes: lane l ends with the totals of i
     // atom (l >> 2) & 7 and writes component l & 3
     float sum[3];
