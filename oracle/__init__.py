@@ -25,7 +25,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 
 EXCL_NONE, EXCL_MODIFIED, EXCL_FULL = 0, 1, 2
-SW_UNIVERSAL, SW_CUTOFF, SW_C1, SW_C2, SW_CN = 0, 1, 2, 3, 4
+SW_UNIVERSAL, SW_CUTOFF, SW_C1, SW_C2, SW_CN, SW_CMPCNCN = 0, 1, 2, 3, 4, 5
+SW_COMPLEMENT = 16  # flag on C1 / C2 / Cn: ComplementSwitchingFunction of it
 POT_COULOMB, POT_LJ = 0, 1
 INV_TIMEFACTOR = 0.02045482828087295  # base/PMConstants.cpp:54
 SQRTCOULOMBCONSTANT = 18.2226123264  # base/PMConstants.cpp:67
@@ -81,7 +82,9 @@ def lib():
 
 @dataclass
 class Switch:
-    """A ProtoMol switching function: kind in {Universal, Cutoff, C1, C2, Cn}."""
+    """A ProtoMol switching function: kind in {Universal, Cutoff, C1, C2, Cn,
+    CmpCnCn, ComplementC1, ComplementC2, ComplementCn}.  CmpCnCn takes
+    switchon < switchoff < cutoff and the order."""
     kind: str = "Cutoff"
     cutoff: float = 0.0
     switchon: float = 0.0
@@ -89,8 +92,14 @@ class Switch:
     order: float = 0.0
 
     def c(self) -> _Switch:
+        name = self.kind.lower()
+        comp = name.startswith("complement")
+        if comp:
+            name = name[len("complement"):]
         k = {"universal": SW_UNIVERSAL, "cutoff": SW_CUTOFF, "c1": SW_C1, "c2": SW_C2,
-             "cn": SW_CN}[self.kind.lower()]
+             "cn": SW_CN, "cmpcncn": SW_CMPCNCN, "complimentcncn": SW_CMPCNCN}[name]
+        if comp:
+            k |= SW_COMPLEMENT
         return _Switch(k, self.cutoff, self.switchon, self.switchoff, self.order)
 
 
@@ -207,6 +216,37 @@ def simplefull_force(sysm: System, potential: str, sw: Switch | None = None):
     e = np.zeros(2)
     v = np.zeros(9)
     rc = lib().orc_simplefull_force(C.byref(cs), pot, C.byref(s), _ptr(f), _ptr(e), _ptr(v))
+    assert rc == 0
+    return f, {"coulomb": e[0], "lj": e[1]}, v.reshape(3, 3)
+
+
+def simplefull_force_n(sysm: System, terms):
+    """NonbondedSimpleFull with OneAtomPair or OneAtomPairTwo: terms is a
+    list of (potential 'LennardJones'|'Coulomb', Switch); vacuum, or the
+    minimal image of a periodic box."""
+    cs = sysm.c()
+    pots = np.array([POT_LJ if p.lower().startswith("lennard") else POT_COULOMB
+                     for p, _ in terms], np.int32)
+    sws = (_Switch * len(terms))(*[s.c() for _, s in terms])
+    f = np.zeros((sysm.n, 3))
+    e = np.zeros(2)
+    v = np.zeros(9)
+    rc = lib().orc_simplefull_force_n(C.byref(cs), len(terms), _ptr(pots), sws, _ptr(f),
+                                      _ptr(e), _ptr(v))
+    assert rc == 0
+    return f, {"coulomb": e[0], "lj": e[1]}, v.reshape(3, 3)
+
+
+def full_force(sysm: System, potential: str, sw: Switch, alg_cutoff: float):
+    """NonbondedFull (lattice sum) with OneAtomPairFull of one potential."""
+    cs = sysm.c()
+    pot = POT_LJ if potential.lower().startswith("lennard") else POT_COULOMB
+    s = sw.c()
+    f = np.zeros((sysm.n, 3))
+    e = np.zeros(2)
+    v = np.zeros(9)
+    rc = lib().orc_full_force(C.byref(cs), pot, C.byref(s), C.c_double(alg_cutoff), _ptr(f),
+                              _ptr(e), _ptr(v))
     assert rc == 0
     return f, {"coulomb": e[0], "lj": e[1]}, v.reshape(3, 3)
 

@@ -408,6 +408,9 @@ typedef struct {
   double s1, s2, s3;                     /* C2SwitchingFunction.cpp:12-19 */
   int ordInt, ordIdx;                    /* CnSwitchingFunction.cpp:41-60 */
   double irange[8];
+  double compoff, compoff2, itrange[8];  /* CmpCnCnSwitchingFunction.cpp:11-25 */
+  int complement;                        /* ComplementSwitchingFunction.h */
+  double rough2;                         /* cutoffSquared() of the rough test */
 } sw_t;
 
 static const double CN_SW[5][7] = {     /* CnSwitchingFunction.cpp:9-15 */
@@ -427,8 +430,8 @@ static void sw_init(const orc_switch *in, sw_t *o) {
   int i;
   double rc = in->cutoff, rs = in->switchon;
   memset(o, 0, sizeof(*o));
-  o->kind = in->kind;
-  switch (in->kind) {
+  o->kind = in->kind & ~ORC_SW_COMPLEMENT;
+  switch (o->kind) {
     case ORC_SW_UNIVERSAL:
       o->cutoff = 1e300;
       o->cutoff2 = 1e300; /* Constant::MAXREAL */
@@ -467,10 +470,46 @@ static void sw_init(const orc_switch *in, sw_t *o) {
         o->irange[i] = o->irange[i - 1] / (rs - rc);
       break;
     }
+    case ORC_SW_CMPCNCN: { /* CmpCnCnSwitchingFunction.cpp:11-25 */
+      double so = in->switchoff, ord = in->order;
+      o->cutoff = rc;
+      o->cutoff2 = rc * rc;
+      o->switchon2 = rs * rs;
+      o->compoff = so;
+      o->compoff2 = so * so;
+      if (ord == 5.0) ord = 2.0; /* the order is remapped before its index */
+      o->ordInt = (int)ord;
+      o->ordIdx = o->ordInt - 2;
+      o->irange[0] = 1.0 / pow(rs - so, o->ordInt + 1);
+      o->itrange[0] = 1.0 / pow(so - rc, o->ordInt + 1);
+      for (i = 1; i < o->ordInt + 1; i++) {
+        o->irange[i] = o->irange[i - 1] / (rs - so);
+        o->itrange[i] = o->itrange[i - 1] / (so - rc);
+      }
+      break;
+    }
+  }
+  o->rough2 = o->cutoff2;
+  if (in->kind & ORC_SW_COMPLEMENT) {
+    /* ComplementSwitchingFunction: no rough test, cutoff MAXREAL; the
+     * original function keeps its own constants */
+    o->complement = 1;
+    o->rough2 = 1e300;
   }
 }
 
+static void sw_eval_base(const sw_t *w, double r2, double *val, double *der);
+/* ComplementSwitchingFunction::operator() (ComplementSwitchingFunction.h:42-46):
+ * 1 - value, -derivative of the original function. */
 static void sw_eval(const sw_t *w, double r2, double *val, double *der) {
+  sw_eval_base(w, r2, val, der);
+  if (w->complement) {
+    *val = 1.0 - *val;
+    *der = -*der;
+  }
+}
+
+static void sw_eval_base(const sw_t *w, double r2, double *val, double *der) {
   switch (w->kind) {
     case ORC_SW_UNIVERSAL: /* UniversalSwitchingFunction.h:45-48 */
       *val = 1.0;
@@ -523,6 +562,39 @@ static void sw_eval(const sw_t *w, double r2, double *val, double *der) {
         *der += CN_DSW[w->ordIdx][i] * c[i] * w->irange[i];
       }
       *der /= sq;
+      return;
+    }
+    case ORC_SW_CMPCNCN: { /* CmpCnCnSwitchingFunction.h:45-95 */
+      double c[9], sd, sq;
+      int i;
+      *der = 0.0;
+      if (r2 > w->cutoff2)
+        *val = 0.0;
+      else if (r2 > w->compoff2) {
+        sq = sqrt(r2);
+        sd = sq - w->cutoff;
+        c[0] = pow(sd, w->ordInt);
+        for (i = 1; i < w->ordInt + 2; i++) c[i] = c[i - 1] * sd;
+        *val = *der = 0.0;
+        for (i = 0; i < w->ordInt + 1; i++) {
+          *val += CN_SW[w->ordIdx][i] * c[i + 1] * w->itrange[i];
+          *der += CN_DSW[w->ordIdx][i] * c[i] * w->itrange[i];
+        }
+        *der /= sq;
+      } else if (r2 >= w->switchon2) {
+        sq = sqrt(r2);
+        sd = sq - w->compoff;
+        c[0] = pow(sd, w->ordInt);
+        for (i = 1; i < w->ordInt + 2; i++) c[i] = c[i - 1] * sd;
+        *val = *der = 0.0;
+        for (i = 0; i < w->ordInt + 1; i++) {
+          *val += CN_SW[w->ordIdx][i] * c[i + 1] * w->irange[i];
+          *der -= CN_DSW[w->ordIdx][i] * c[i] * w->irange[i];
+        }
+        *val = 1.0 - *val;
+        *der /= sq;
+      } else
+        *val = 0.0;
       return;
     }
   }
@@ -623,9 +695,12 @@ static void cutoff_visit(void *vctx, int i, int j) {
   add_virial(c->virial, fij, d);
 }
 
-static double sw_cut2(const sw_t *w) { return w->cutoff2; }
+static double sw_cut2(const sw_t *w) { return w->rough2; }
 static int sw_modifies(int kind) {
-  return kind == ORC_SW_C1 || kind == ORC_SW_C2 || kind == ORC_SW_CN;
+  /* MODIFY = 1: C1, C2, Cn, CmpCnCn and every Complement (switch/ headers) */
+  if (kind & ORC_SW_COMPLEMENT) return 1;
+  return kind == ORC_SW_C1 || kind == ORC_SW_C2 || kind == ORC_SW_CN ||
+         kind == ORC_SW_CMPCNCN;
 }
 
 long orc_cutoff_pairs(const orc_system *s, double cellsize, double alg_cutoff,
@@ -679,20 +754,34 @@ int orc_cutoff_force(const orc_system *s, double cellsize, double alg_cutoff,
 int orc_simplefull_force(const orc_system *s, int potential,
                          const orc_switch *sw, double *forces,
                          double *energies, double *virial) {
+  return orc_simplefull_force_n(s, 1, &potential, sw, forces, energies, virial);
+}
+
+/* OneAtomPair / OneAtomPairTwo over every pair i < j in blocks of 64
+ * (NonbondedSimpleFullSystemForce.h:125-150); the rough test is against
+ * the larger switch cutoff (OneAtomPairTwo.h:40-44), minimal image in a
+ * periodic box. */
+int orc_simplefull_force_n(const orc_system *s, int nterms, const int *potentials,
+                           const orc_switch *sw, double *forces, double *energies,
+                           double *virial) {
   pbc_t p;
   cutoff_ctx c;
-  int bi, bj, i, j;
+  int bi, bj, i, j, t;
   const int bs = 64;
+  if (nterms < 1 || nterms > 2) return -1;
   memset(&c, 0, sizeof(c));
   pbc_set(s, &p);
   c.s = s;
   c.p = &p;
   excl_build(s, &c.ex);
-  c.nterms = 1;
-  c.pot[0] = potential;
-  sw_init(sw, &c.sw[0]);
-  c.cut2 = sw_cut2(&c.sw[0]);
-  c.modify = sw_modifies(sw->kind);
+  c.nterms = nterms;
+  c.cut2 = 0.0;
+  for (t = 0; t < nterms; t++) {
+    c.pot[t] = potentials[t];
+    sw_init(&sw[t], &c.sw[t]);
+    if (sw_cut2(&c.sw[t]) > c.cut2) c.cut2 = sw_cut2(&c.sw[t]);
+    if (sw_modifies(sw[t].kind)) c.modify = 1;
+  }
   c.forces = forces;
   c.energies = energies;
   c.virial = virial;
@@ -972,6 +1061,90 @@ void orc_ewald_self(const orc_system *s, const orc_ewald *e, double *self,
 
 /* ------------------------------------------------------------------ */
 /* GB, OBC.  Pairs i < j in the SimpleFull order, vacuum differences. */
+/* ------------------------------------------------------------------ */
+/* Lattice sum: NonbondedFullSystemForce::doEvaluate (force/nonbonded/
+ * NonbondedFullSystemForce.h:38-62) with OneAtomPairFull::doOneAtomPair
+ * (force/OneAtomPairFull.h:35-135). */
+static void full_pot(const orc_system *s, int pot, int i, int j, int excl, double r2,
+                     const sw_t *w, int modify, double *e, double *f) {
+  double rr2 = 1.0 / r2, sv, sd;
+  if (pot == ORC_POT_LJ)
+    lj_eval(s, i, j, excl, rr2, e, f);
+  else
+    coul_eval(s, i, j, excl, rr2, e, f);
+  if (modify) {
+    sw_eval(w, r2, &sv, &sd);
+    *f = *f * sv - *e * sd;
+    *e = *e * sv;
+  }
+}
+
+int orc_full_force(const orc_system *s, int potential, const orc_switch *sw,
+                   double alg_cutoff, double *forces, double *energies, double *virial) {
+  pbc_t p;
+  sw_t w;
+  excl_t ex;
+  double *lat;
+  int nlat, modify, bi, bj, i, j, k, t;
+  const int bs = 64; /* defaultBlockSize */
+  double *esum = energies + (potential == ORC_POT_LJ ? 1 : 0);
+  pbc_set(s, &p);
+  if (!p.periodic) return -1;
+  sw_init(sw, &w);
+  modify = sw_modifies(sw->kind);
+  excl_build(s, &ex);
+  nlat = build_lattice(&p, alg_cutoff, &lat); /* lat[0] is the zero vector */
+  for (bi = 0; bi < s->n; bi += bs)
+    for (bj = bi; bj < s->n; bj += bs)
+      for (i = bi; i < bi + bs && i < s->n; i++)
+        for (j = (bj <= i ? i : bj); j < bj + bs && j < s->n; j++) {
+          const int same = i == j;
+          double dmin[3], r2, e, f, fij[3];
+          if (same && nlat == 1) continue;
+          pbc_mindiff(&p, s->pos + 3 * i, s->pos + 3 * j, dmin, &r2);
+          if (!same) {
+            int excl;
+            r2 = norm2(dmin);
+            if (r2 > w.rough2) continue; /* roughTest fails: no image either */
+            excl = excl_check(&ex, i, j);
+            if (excl != ORC_EXCL_FULL) {
+              full_pot(s, potential, i, j, excl, r2, &w, modify, &e, &f);
+              *esum += e;
+              for (t = 0; t < 3; t++) fij[t] = -dmin[t] * f;
+              for (t = 0; t < 3; t++) {
+                forces[3 * i + t] += fij[t];
+                forces[3 * j + t] -= fij[t];
+              }
+              for (t = 0; t < 3; t++) dmin[t] = -dmin[t];
+              add_virial(virial, fij, dmin);
+              for (t = 0; t < 3; t++) dmin[t] = -dmin[t];
+            }
+          }
+          for (k = 1; k < nlat; k++) {
+            double d[3];
+            for (t = 0; t < 3; t++) d[t] = dmin[t] + lat[3 * k + t];
+            r2 = norm2(d);
+            if (r2 > w.rough2) continue;
+            full_pot(s, potential, i, j, ORC_EXCL_NONE, r2, &w, modify, &e, &f);
+            if (same)
+              e /= 2;
+            else {
+              for (t = 0; t < 3; t++) fij[t] = -d[t] * f;
+              for (t = 0; t < 3; t++) {
+                forces[3 * i + t] += fij[t];
+                forces[3 * j + t] -= fij[t];
+              }
+              for (t = 0; t < 3; t++) d[t] = -d[t];
+              add_virial(virial, fij, d);
+            }
+            *esum += e;
+          }
+        }
+  free(lat);
+  excl_free(&ex);
+  return 0;
+}
+
 /* Burial sums, psi and Born radii (GBBornRadii pair op and postProcess). */
 static void gb_burial_born(const orc_system *s, const orc_gb *g, double *burial, double *psi,
                            double *born) {

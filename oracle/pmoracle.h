@@ -19,7 +19,10 @@ enum { ORC_EXCL_NONE = 0, ORC_EXCL_MODIFIED = 1, ORC_EXCL_FULL = 2 };
 
 /* Switching functions (the switch/ directory). */
 enum { ORC_SW_UNIVERSAL = 0, ORC_SW_CUTOFF = 1, ORC_SW_C1 = 2, ORC_SW_C2 = 3,
-       ORC_SW_CN = 4 };
+       ORC_SW_CN = 4, ORC_SW_CMPCNCN = 5 };
+/* Flag OR'd into a C1, C2 or Cn kind: ComplementSwitchingFunction of it
+ * (switch/ComplementSwitchingFunction.h:14-74). */
+enum { ORC_SW_COMPLEMENT = 16 };
 /* Potentials. */
 enum { ORC_POT_COULOMB = 0, ORC_POT_LJ = 1 };
 
@@ -27,7 +30,8 @@ typedef struct {
   int kind;
   double cutoff;    /* -cutoff */
   double switchon;  /* -switchon (C2, Cn) */
-  double switchoff; /* -switchoff (Cn; 0 = use cutoff) */
+  double switchoff; /* -switchoff (Cn: 0 = use cutoff; CmpCnCn: the middle
+                       distance, switchon < switchoff < cutoff) */
   double order;     /* -n (Cn) */
 } orc_switch;
 
@@ -77,6 +81,21 @@ int orc_cutoff_force(const orc_system *s, double cellsize, double alg_cutoff,
 int orc_simplefull_force(const orc_system *s, int potential,
                          const orc_switch *sw, double *forces,
                          double *energies, double *virial);
+
+/* NonbondedSimpleFullSystemForce with OneAtomPair (nterms = 1) or
+ * OneAtomPairTwo (nterms = 2), vacuum or periodic (minimal image). */
+int orc_simplefull_force_n(const orc_system *s, int nterms, const int *potentials,
+                           const orc_switch *sw, double *forces, double *energies,
+                           double *virial);
+
+/* NonbondedFullSystemForce (lattice sum, force/nonbonded/
+ * NonbondedFullSystemForce.h:38-62) with OneAtomPairFull
+ * (force/OneAtomPairFull.h:35-135): every pair i <= j in blocks of 64, the
+ * minimal image with the pair's exclusion class and every lattice image
+ * (|L| <= 2 alg_cutoff) with none; an atom's own images add half their
+ * energy and no force.  Periodic boxes only. */
+int orc_full_force(const orc_system *s, int potential, const orc_switch *sw,
+                   double alg_cutoff, double *forces, double *energies, double *virial);
 
 /* NonbondedFullEwaldSystemForce parameters, derived exactly as in
  * force/nonbonded/NonbondedFullEwaldSystemForce.h:598-620. */

@@ -75,7 +75,8 @@ def rms_rel(a: np.ndarray, b: np.ndarray) -> float:
 
 
 def parse_cutoff_def(d: str):
-    """(potentials, switch dicts, algorithm cutoff) of a NonbondedCutoff line."""
+    """(potentials, switch dicts, algorithm cutoff) of a NonbondedCutoff,
+    NonbondedFull or NonbondedSimpleFull line."""
     toks = d.split()
     pots = [t for t in toks if t in ("LennardJones", "Coulomb")]
     sws, i, alg = [], 0, None
@@ -83,7 +84,7 @@ def parse_cutoff_def(d: str):
         if toks[i] == "-switchingFunction":
             sw = {"kind": toks[i + 1]}
             i += 2
-            while i < len(toks) and toks[i] in ("-cutoff", "-switchon", "-n") and \
+            while i < len(toks) and toks[i] in ("-cutoff", "-switchon", "-switchoff", "-n") and \
                     toks[i][1:] not in sw:
                 sw[toks[i][1:]] = float(toks[i + 1])
                 i += 2

@@ -131,7 +131,54 @@ def langevin_temperature() -> None:
     print("wrote c1_langevin_temperature", means)
 
 
+def switch_variants() -> None:
+    """The remaining switching functions and the lattice sum through the
+    reference's own factory.  A 300-atom TIP3P box of 14.4 A (below twice
+    the 8 A cutoff, so lattice images beyond the minimal one contribute):
+    CmpCnCn on the cutoff path, NonbondedFull (lattice sum) with C1, C2, Cn
+    and CmpCnCn, and the all-pairs path in a periodic box (minimal image)
+    with C2, Cn and the Complement of C1, C2 and Cn.  The reference's
+    vacuum GB protein (www-fip35): the all-pairs path with Complement
+    switches."""
+    small = systems.tip3p_box(100, 14.4, seed=5, lattice=5)
+    d = synthetic(small, "small", [
+        "Coulomb -algorithm NonbondedCutoff -switchingFunction ComplimentCnCn -switchon 2 "
+        "-switchoff 4 -cutoff 6.5 -n 2 -cutoff 6.5",
+        "LennardJones Coulomb -algorithm NonbondedCutoff -switchingFunction ComplimentCnCn "
+        "-switchon 2 -switchoff 5 -cutoff 7 -n 3 -switchingFunction ComplimentCnCn "
+        "-switchon 1 -switchoff 4 -cutoff 7 -n 4 -cutoff 7",
+        "Coulomb -algorithm NonbondedFull -switchingFunction C1 -cutoff 8 -cutoff 8",
+        "LennardJones -algorithm NonbondedFull -switchingFunction C2 -switchon 6 -cutoff 8 "
+        "-cutoff 8",
+        "Coulomb -algorithm NonbondedFull -switchingFunction Cn -n 3 -switchon 5 -cutoff 8 "
+        "-cutoff 8",
+        "LennardJones -algorithm NonbondedFull -switchingFunction ComplimentCnCn -switchon 2 "
+        "-switchoff 5 -cutoff 8 -n 2 -cutoff 8",
+        "LennardJones Coulomb -algorithm NonbondedSimpleFull -switchingFunction ComplementC2 "
+        "-switchon 5 -cutoff 6 -switchingFunction ComplementC1 -cutoff 6",
+        "Coulomb -algorithm NonbondedSimpleFull -switchingFunction ComplementCn -n 2 "
+        "-switchon 4 -cutoff 6",
+        "LennardJones -algorithm NonbondedSimpleFull -switchingFunction C2 -switchon 4 "
+        "-cutoff 6",
+        "LennardJones Coulomb -algorithm NonbondedSimpleFull -switchingFunction Cn -n 3 "
+        "-switchon 4 -cutoff 6 -switchingFunction Cn -n 2 -switchon 3 -cutoff 6",
+        "Bond"], cellsize=6.5)
+    save("small_tip3p300_switches", d, {"seed": np.array(5)})
+    d = reference_conf("www-fip35_FFAMBER_GB_LL.conf", [
+        "Coulomb -algorithm NonbondedSimpleFull -switchingFunction ComplementC1 -cutoff 8",
+        "LennardJones -algorithm NonbondedSimpleFull -switchingFunction ComplementCn -n 4 "
+        "-switchon 6 -cutoff 9",
+        "LennardJones Coulomb -algorithm NonbondedSimpleFull -switchingFunction ComplementC2 "
+        "-switchon 7 -cutoff 9 -switchingFunction ComplementC1 -cutoff 9",
+        "LennardJones Coulomb -algorithm NonbondedSimpleFull -switchingFunction C2 "
+        "-switchon 7 -cutoff 9 -switchingFunction C1 -cutoff 9"])
+    save("fip35_switches", d)
+
+
 def main(which: str = "all") -> None:
+    if which == "switches":
+        switch_variants()
+        return
     if which == "torsions":
         torsions()
         return

@@ -201,3 +201,44 @@ def test_gbace_oracle_matches_reference(name):
     ref_f = F.forces(z, k)
     assert np.abs(f - ref_f).max() <= 1e-12 * max(1.0, np.abs(ref_f).max())
     assert e == pytest.approx(F.energies(z, k)[0], rel=1e-13)
+
+
+def _switch_terms(d):
+    pots, sws, alg = F.parse_cutoff_def(d)
+    terms = [(p, oracle.Switch(sws[j]["kind"], sws[j].get("cutoff", 0.0),
+                               sws[j].get("switchon", 0.0), sws[j].get("switchoff", 0.0),
+                               sws[j].get("n", 0.0)))
+             for j, p in enumerate(pots)]
+    return terms, alg
+
+
+@pytest.mark.parametrize("name", ["small_tip3p300_switches", "fip35_switches"])
+def test_switch_variants_and_lattice_sum_match_reference(name):
+    """CmpCnCn (cutoff path), the Complement switches and C1/C2/Cn on the
+    all-pairs path (vacuum and periodic minimal image), and the NonbondedFull
+    lattice sum in a box below twice the cutoff, against the reference's
+    own forces, energies and virial."""
+    z = F.load(name)
+    s = F.oracle_system(z)
+    kinds = set()
+    for k, d in enumerate(z["defs"]):
+        d = str(d)
+        if "-algorithm" not in d:
+            continue
+        terms, alg = _switch_terms(d)
+        if "NonbondedCutoff" in d:
+            f, e, v = oracle.cutoff_force(s, 6.5, alg, terms)
+        elif "NonbondedFull " in d:
+            assert len(terms) == 1
+            f, e, v = oracle.full_force(s, terms[0][0], terms[0][1], alg)
+        else:
+            f, e, v = oracle.simplefull_force_n(s, terms)
+        ref_f, ref_e = F.forces(z, k), F.energies(z, k)
+        scale = max(1.0, np.abs(ref_f).max())
+        assert np.abs(f - ref_f).max() < 1e-11 * scale, d
+        assert e["coulomb"] == pytest.approx(ref_e[0], rel=1e-12, abs=1e-9), d
+        assert e["lj"] == pytest.approx(ref_e[1], rel=1e-12, abs=1e-9), d
+        assert np.abs(v.reshape(-1) - ref_e[7:16]).max() < 1e-8 * max(1.0, np.abs(ref_e[7:16]).max()), d
+        kinds.add(d.split("-algorithm")[1].split()[0])
+    assert kinds >= ({"NonbondedSimpleFull"} if name == "fip35_switches" else
+                     {"NonbondedCutoff", "NonbondedFull", "NonbondedSimpleFull"})
