@@ -208,13 +208,14 @@ def load_traffic() -> float | None:
     return None
 
 
-# FP32 flops of one in-cutoff pair in the force-only tile kernel
-# (LJ C2 + Ewald real space, an FMA counts two): hi/lo difference 9, r^2 5,
-# rsqrt with one Newton step 5, 1/r^2 1, LJ 10, C2 switch 12, charge
-# product 1, Ewald real term (exp, poly5 erfc, 1/(1+p ar)) 24, total 1,
-# pair and i forces 6, share of the j-force reduction 4; plus 4 MUFU
-# (rsqrt, ex2, rcp and the exp argument scaling) not counted.
-PAIR_FLOPS = 78
+# FP32 flops of one in-cutoff pair in the force-only pair kernel
+# (k_pairs_jl: LJ C2 + Ewald real space from the r^2 table, an FMA counts
+# two), from its source: difference 3, r^2 5, charge product 1, 1/r^2 1,
+# r^-6 2, B r^-6 1, A r^-12 2, LJ force over r^2 4, C2 switch (clamp 2,
+# polynomial 10, applied 3) 15, Ewald cubic in t with its coordinate 8
+# plus the charge 1, pair forces on i and j 12; the selects of the pair
+# and cutoff masks not counted.
+PAIR_FLOPS = 55
 
 
 def algorithmic_bytes_per_step(n: int, grid: int) -> dict:

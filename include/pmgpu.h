@@ -53,13 +53,19 @@ enum {
 /* ExclusionClass, topology/ExclusionTable.h:19-23 */
 enum { PMGPU_EXCL_NONE = 0, PMGPU_EXCL_MODIFIED = 1, PMGPU_EXCL_FULL = 2 };
 
-/* Switching functions, switch/{Universal,Cutoff,C1,C2,Cn}SwitchingFunction */
+/* Switching functions, switch/{Universal,Cutoff,C1,C2,Cn,CmpCnCn}
+ * SwitchingFunction.  PMGPU_SW_COMPLEMENT OR'd into C1, C2 or Cn is the
+ * ComplementSwitchingFunction of that function
+ * (switch/ComplementSwitchingFunction.h:14-74: 1 - S, no cutoff), which
+ * ProtoMol registers on the all-pairs path only. */
 enum {
   PMGPU_SW_UNIVERSAL = 0,
   PMGPU_SW_CUTOFF = 1,
   PMGPU_SW_C1 = 2,
   PMGPU_SW_C2 = 3,
-  PMGPU_SW_CN = 4
+  PMGPU_SW_CN = 4,
+  PMGPU_SW_CMPCNCN = 5,
+  PMGPU_SW_COMPLEMENT = 16
 };
 
 /* Energy slots written by pmgpu_evaluate / pmgpu_force_evaluate: the first
@@ -134,8 +140,9 @@ typedef struct {
   int kind;         /* PMGPU_SW_* */
   double cutoff;    /* -cutoff */
   double switchon;  /* -switchon (C2, Cn) */
-  double switchoff; /* -switchoff (Cn; 0 means "use cutoff") */
-  double order;     /* -n (Cn) */
+  double switchoff; /* -switchoff (Cn: 0 means "use cutoff"; CmpCnCn: the
+                       middle distance, switchon < switchoff <= cutoff) */
+  double order;     /* -n (Cn, CmpCnCn) */
 } pmgpu_switch;
 
 typedef struct pmgpu_context pmgpu_context;
@@ -192,6 +199,26 @@ int pmgpu_system_device_state(pmgpu_system *sys, double **pos, double **vel,
 int pmgpu_force_cutoff_add(pmgpu_system *sys, const pmgpu_switch *lj_sw,
                            const pmgpu_switch *coul_sw, double alg_cutoff,
                            double cellsize, int *force_id);
+/* NonbondedFull (lattice sum) LennardJones and/or Coulomb
+ * (force/nonbonded/NonbondedFullSystemForce.h:38-62 with
+ * force/OneAtomPairFull.h:35-135; module/NonbondedFullForceModule.cpp:39-46):
+ * every periodic image of every pair within the switch cutoff, the
+ * minimal image with the pair's exclusion class and the others with none.
+ * Switches C1, C2, Cn or CmpCnCn; alg_cutoff (the algorithm's -cutoff,
+ * which bounds the lattice) at least the switch cutoffs; periodic boxes
+ * with edges longer than the cutoff (PMGPU_ERR_UNSUPPORTED otherwise: an
+ * atom's own images then lie within the cutoff). */
+int pmgpu_force_full_add(pmgpu_system *sys, const pmgpu_switch *lj_sw,
+                         const pmgpu_switch *coul_sw, double alg_cutoff, double cellsize,
+                         int *force_id);
+/* NonbondedSimpleFull with switching functions: LennardJones and/or
+ * Coulomb over every pair i < j (OneAtomPair / OneAtomPairTwo,
+ * module/NonbondedSimpleFullForceModule.cpp:55-199), vacuum or the
+ * minimal image of a periodic box, switches Universal, C1, C2, Cn or the
+ * Complement of C1, C2, Cn.  NULL switch: the term is absent.  The pair
+ * arithmetic is FP64 in both precisions. */
+int pmgpu_force_simplefull_switched_add(pmgpu_system *sys, const pmgpu_switch *lj_sw,
+                                        const pmgpu_switch *coul_sw, int *force_id);
 /* NonbondedSimpleFull LennardJones and/or Coulomb (vacuum all pairs with
  * exclusions, module/NonbondedSimpleFullForceModule.cpp). */
 int pmgpu_force_simplefull_add(pmgpu_system *sys, int lj, int coulomb,

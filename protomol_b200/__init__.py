@@ -9,6 +9,7 @@ system generators used by the benchmark.
 from .engine import (  # noqa: F401
     ANGLE, BOND, COULOMB, LENNARDJONES, VIRIALXX, BondedSystemForce, Context, ForceFactory,
     GBACEForce, GBForce, GpuSystem, LangevinLeapfrogIntegrator, LeapfrogIntegrator,
-    NonbondedCutoffSystemForce, NonbondedSimpleFullSystemForce, PMEwaldSystemForce,
+    NonbondedCutoffSystemForce, NonbondedFullSystemForce, NonbondedSimpleFullSwitchedForce,
+    NonbondedSimpleFullSystemForce, PMEwaldSystemForce,
     ScalarStructure, SystemForce, TorsionSystemForce)
 from ._lib import PmgpuError, load  # noqa: F401

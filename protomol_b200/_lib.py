@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(HERE, "libpmgpu.so")
 # status codes (pmgpu.h)
 OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_OVERFLOW, ERR_NAN, ERR_UNSUPPORTED, ERR_STATE = range(8)
 EXCL_NONE, EXCL_MODIFIED, EXCL_FULL = 0, 1, 2
-SW_UNIVERSAL, SW_CUTOFF, SW_C1, SW_C2, SW_CN = range(5)
+SW_UNIVERSAL, SW_CUTOFF, SW_C1, SW_C2, SW_CN, SW_CMPCNCN = range(6)
+SW_COMPLEMENT = 16  # flag on C1 / C2 / Cn
 E_COULOMB, E_LENNARDJONES, E_BOND, E_ANGLE, E_DIHEDRAL, E_IMPROPER, E_OTHER = range(7)
 E_COUNT = 7
 PREC_MIXED, PREC_DOUBLE = 0, 1
@@ -43,6 +44,7 @@ EXPORTED = [
     "pmgpu_ensemble_create", "pmgpu_ensemble_destroy", "pmgpu_ensemble_run",
     "pmgpu_ensemble_set_splits", "pmgpu_ensemble_time_pairs", "pmgpu_ensemble_get_info",
     "pmgpu_ensemble_member", "pmgpu_debug_limit_list_rows", "pmgpu_system_set_step",
+    "pmgpu_force_full_add", "pmgpu_force_simplefull_switched_add",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -122,6 +124,10 @@ def load() -> C.CDLL:
     lib.pmgpu_force_cutoff_add.argtypes = [vp, C.POINTER(Switch), C.POINTER(Switch), dbl, dbl,
                                            C.POINTER(i32)]
     lib.pmgpu_force_simplefull_add.argtypes = [vp, i32, i32, C.POINTER(i32)]
+    lib.pmgpu_force_full_add.argtypes = [vp, C.POINTER(Switch), C.POINTER(Switch), dbl, dbl,
+                                         C.POINTER(i32)]
+    lib.pmgpu_force_simplefull_switched_add.argtypes = [vp, C.POINTER(Switch), C.POINTER(Switch),
+                                                        C.POINTER(i32)]
     lib.pmgpu_force_pme_add.argtypes = [vp, dbl, dbl, i32, vp, i32, i32, dbl, C.POINTER(i32)]
     lib.pmgpu_force_gb_add.argtypes = [vp, dbl, dbl, C.POINTER(i32)]
     lib.pmgpu_force_gbace_add.argtypes = [vp, dbl, dbl, C.POINTER(i32)]

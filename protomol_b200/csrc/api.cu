@@ -70,12 +70,14 @@ void box_from_topology(const pmgpu_topology *t, Box *b) {
 
 // Switching-function constants exactly as the ProtoMol constructors form
 // them (C1SwitchingFunction.cpp:12-17, C2SwitchingFunction.cpp:12-19,
-// CnSwitchingFunction.cpp:41-60).
+// CnSwitchingFunction.cpp:41-60, CmpCnCnSwitchingFunction.cpp:11-25); a
+// complement keeps its function's constants and drops the rough test
+// (ComplementSwitchingFunction.h:35-41).
 void switch_setup(const pmgpu_switch *in, SwitchParams *o) {
   std::memset(o, 0, sizeof(*o));
-  o->kind = in->kind;
+  o->kind = in->kind & ~PMGPU_SW_COMPLEMENT;
   double rc = in->cutoff, rs = in->switchon;
-  switch (in->kind) {
+  switch (o->kind) {
     case PMGPU_SW_UNIVERSAL:
       o->cutoff = 1e300;
       o->cutoff2 = 1e300;
@@ -117,12 +119,40 @@ void switch_setup(const pmgpu_switch *in, SwitchParams *o) {
         o->irange[i] = o->irange[i - 1] / (rs - rc);
       break;
     }
+    case PMGPU_SW_CMPCNCN: {
+      o->modify = 1;
+      const double so = in->switchoff;
+      double ord = in->order;
+      if (ord == 5.0) ord = 2.0;  // remapped before the table index is taken
+      o->cutoff = rc;
+      o->cutoff2 = rc * rc;
+      o->switchon2 = rs * rs;
+      o->compoff = so;
+      o->compoff2 = so * so;
+      o->ord_int = (int)ord;
+      o->ord_idx = o->ord_int - 2;
+      o->irange[0] = 1.0 / std::pow(rs - so, o->ord_int + 1);
+      o->itrange[0] = 1.0 / std::pow(so - rc, o->ord_int + 1);
+      for (int i = 1; i < o->ord_int + 1 && i < 8; i++) {
+        o->irange[i] = o->irange[i - 1] / (rs - so);
+        o->itrange[i] = o->itrange[i - 1] / (so - rc);
+      }
+      break;
+    }
+  }
+  o->rough2 = o->cutoff2;
+  if (in->kind & PMGPU_SW_COMPLEMENT) {
+    o->modify = 1;
+    o->complement = 1;
+    o->rough2 = 1e300;  // Constant::MAXREAL
   }
 }
 
 static int validate_switch(const pmgpu_switch *sw, const char *what) {
   if (!sw) return PMGPU_OK;
   std::string w(what);
+  if (sw->kind & PMGPU_SW_COMPLEMENT)
+    return fail(PMGPU_ERR_ARG, w + ": a Complement switch belongs to the all-pairs path");
   switch (sw->kind) {
     case PMGPU_SW_CUTOFF:
     case PMGPU_SW_C1:
@@ -139,6 +169,14 @@ static int validate_switch(const pmgpu_switch *sw, const char *what) {
           (sw->switchoff > 0 && sw->switchoff != sw->cutoff) || sw->order < 2 ||
           sw->order > 6)
         return fail(PMGPU_ERR_ARG, w + ": Cn needs 0 <= switchon < cutoff, order 2..6");
+      return PMGPU_OK;
+    case PMGPU_SW_CMPCNCN:
+      // CmpCnCnSwitchingFunction::make (CmpCnCnSwitchingFunction.cpp:47-63)
+      if (!(sw->switchon >= 0 && sw->cutoff > 0 && sw->switchoff > 0 &&
+            sw->switchon < sw->switchoff && sw->switchoff <= sw->cutoff) ||
+          sw->order < 2 || sw->order > 6)
+        return fail(PMGPU_ERR_ARG, w + ": CmpCnCn needs 0 <= switchon < switchoff <= cutoff, "
+                                       "order 2..6");
       return PMGPU_OK;
     case PMGPU_SW_UNIVERSAL:
       return fail(PMGPU_ERR_ARG, w + ": a cutoff force needs a cutoff switching function");
@@ -305,6 +343,11 @@ struct Launch {
 static int add_pair_terms(std::vector<Launch> &groups, int list, const PairTerms &t) {
   for (auto &g : groups) {
     if (g.list != list || (g.terms.mask & t.mask)) continue;
+    // a lattice sum's cutoff terms (every image) and NonbondedCutoff's
+    // (minimal image only) take separate launches
+    const bool g_lc = g.terms.mask & (TERM_LJ | TERM_COUL);
+    const bool t_lc = t.mask & (TERM_LJ | TERM_COUL);
+    if (g_lc && t_lc && g.terms.minimal_image != t.minimal_image) continue;
     if (t.mask & TERM_LJ) {
       g.terms.lj_sw = t.lj_sw;
       g.terms.lj_cut2 = t.lj_cut2;
@@ -320,7 +363,7 @@ static int add_pair_terms(std::vector<Launch> &groups, int list, const PairTerms
       g.terms.exact_erf = t.exact_erf;
     }
     g.terms.mask |= t.mask;
-    g.terms.minimal_image |= t.minimal_image;
+    if (t_lc) g.terms.minimal_image = t.minimal_image;  // the rule applies to LJ / Coulomb only
     return 0;
   }
   groups.push_back({list, t});
@@ -480,6 +523,13 @@ int evaluate_forces(System *s, int only, int mode, int fold) {
           s->kernels += launched;
           break;
         }
+        case FK_SIMPLEFULL_SW:
+          prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
+          r = nb_simplefull_sw(s, (f.terms.mask & TERM_LJ) ? &f.terms.lj_sw : nullptr,
+                               (f.terms.mask & TERM_COUL) ? &f.terms.coul_sw : nullptr, em);
+          prof_end(s);
+          s->kernels += 1;
+          break;
         case FK_SIMPLEFULL:
           // all enabled simple-full terms share one all-pairs pass
           if (sf_done) break;
@@ -1011,9 +1061,11 @@ static double default_skin(const System *s, double cutoff) {
   return skin;
 }
 
-int pmgpu_force_cutoff_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
-                           const pmgpu_switch *coul_sw, double alg_cutoff,
-                           double cellsize, int *force_id) {
+// The cutoff terms of NonbondedCutoff (all_images 0) and of the
+// NonbondedFull lattice sum (all_images 1) over the cluster-pair list.
+static int cutoff_terms_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
+                            const pmgpu_switch *coul_sw, double alg_cutoff, double cellsize,
+                            int all_images, int *force_id) {
   if (!h) return fail(PMGPU_ERR_ARG, "null system");
   System *s = sysp(h);
   PM_CHECK(run_finish(s));
@@ -1022,6 +1074,21 @@ int pmgpu_force_cutoff_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
   PM_CHECK(validate_switch(lj_sw, "LennardJones"));
   PM_CHECK(validate_switch(coul_sw, "Coulomb"));
   if (!(alg_cutoff > 0)) return fail(PMGPU_ERR_ARG, "algorithm cutoff must be > 0");
+  if (all_images) {
+    if (!s->box.periodic) return fail(PMGPU_ERR_UNSUPPORTED, "NonbondedFull needs a periodic box");
+    for (const pmgpu_switch *w : {lj_sw, coul_sw}) {
+      if (!w) continue;
+      if (w->kind == PMGPU_SW_CUTOFF)
+        return fail(PMGPU_ERR_ARG, "NonbondedFull takes C1, C2, Cn or CmpCnCn switching");
+      const double wc = (w->kind == PMGPU_SW_CN && w->switchoff > 0) ? w->switchoff : w->cutoff;
+      // the lattice holds the vectors up to twice the algorithm cutoff
+      // (PeriodicBoundaryConditions.cpp:80-104), which reaches every image
+      // inside the switch cutoff only when that is no longer
+      if (wc > alg_cutoff)
+        return fail(PMGPU_ERR_UNSUPPORTED,
+                    "NonbondedFull: switch cutoff beyond the algorithm cutoff");
+    }
+  }
   Force f;
   f.kind = FK_CUTOFF;
   f.alg_cutoff = alg_cutoff;
@@ -1061,13 +1128,26 @@ int pmgpu_force_cutoff_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
       return fail(PMGPU_ERR_UNSUPPORTED, "cutoff forces need box edges longer than the cutoff");
     // Below twice the cutoff a pair can be inside it under two images; the
     // reference's minimalDifference (PeriodicBoundaryConditions.h:72-110)
-    // keeps only the minimal one, and so does the pair kernel.
-    f.terms.minimal_image = 2 * rc > emin;
+    // keeps only the minimal one, and so does the pair kernel.  The
+    // lattice sum takes every image (OneAtomPairFull.h:91-132).
+    f.terms.minimal_image = all_images ? 0 : 2 * rc > emin;
   }
   int li = list_for(s, rc, default_skin(s, rc));
   if (li < 0) return -li;
   f.list_index = li;
   return add_force(s, f, force_id);
+}
+
+int pmgpu_force_cutoff_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
+                           const pmgpu_switch *coul_sw, double alg_cutoff,
+                           double cellsize, int *force_id) {
+  return cutoff_terms_add(h, lj_sw, coul_sw, alg_cutoff, cellsize, 0, force_id);
+}
+
+int pmgpu_force_full_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
+                         const pmgpu_switch *coul_sw, double alg_cutoff, double cellsize,
+                         int *force_id) {
+  return cutoff_terms_add(h, lj_sw, coul_sw, alg_cutoff, cellsize, 1, force_id);
 }
 
 int pmgpu_force_simplefull_add(pmgpu_system *h, int lj, int coulomb, int *force_id) {
@@ -1085,6 +1165,47 @@ int pmgpu_force_simplefull_add(pmgpu_system *h, int lj, int coulomb, int *force_
   f.kind = FK_SIMPLEFULL;
   f.sf_lj = lj ? 1 : 0;
   f.sf_coul = coulomb ? 1 : 0;
+  return add_force(s, f, force_id);
+}
+
+int pmgpu_force_simplefull_switched_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
+                                        const pmgpu_switch *coul_sw, int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CHECK(run_finish(s));
+  PM_CUDA(cudaSetDevice(s->device));
+  if (!lj_sw && !coul_sw) return fail(PMGPU_ERR_ARG, "need LennardJones and/or Coulomb");
+  for (const pmgpu_switch *w : {lj_sw, coul_sw}) {
+    if (!w) continue;
+    const int base = w->kind & ~PMGPU_SW_COMPLEMENT;
+    if (w->kind & PMGPU_SW_COMPLEMENT) {
+      if (base != PMGPU_SW_C1 && base != PMGPU_SW_C2 && base != PMGPU_SW_CN)
+        return fail(PMGPU_ERR_ARG, "Complement applies to C1, C2 or Cn");
+      pmgpu_switch b = *w;
+      b.kind = base;
+      PM_CHECK(validate_switch(&b, "Complement switch"));
+    } else if (base != PMGPU_SW_UNIVERSAL) {
+      PM_CHECK(validate_switch(w, "NonbondedSimpleFull switch"));
+    }
+  }
+  Force f;
+  f.kind = FK_SIMPLEFULL_SW;
+  // OneAtomPairTwo switches both terms when either switch modifies
+  // (OneAtomPairTwo.h:66-76); a single term by its own MODIFY
+  int modify = 0;
+  if (lj_sw) {
+    switch_setup(lj_sw, &f.terms.lj_sw);
+    f.terms.mask |= TERM_LJ;
+    modify |= f.terms.lj_sw.modify;
+  }
+  if (coul_sw) {
+    switch_setup(coul_sw, &f.terms.coul_sw);
+    f.terms.mask |= TERM_COUL;
+    modify |= f.terms.coul_sw.modify;
+  }
+  f.terms.lj_sw.modify = modify;
+  f.terms.coul_sw.modify = modify;
+  f.terms.coulomb_scaling = s->coulomb_scaling;
   return add_force(s, f, force_id);
 }
 

@@ -1850,6 +1850,132 @@ k_simplefull(int n, int jchunk, const double *__restrict__ pos,
   }
 }
 
+// NonbondedSimpleFull with switching functions: OneAtomPair /
+// OneAtomPairTwo (force/OneAtomPair.h:47-107, force/OneAtomPairTwo.h:30-100)
+// over every pair, vacuum or the minimal image of a periodic box, the
+// Complement switches included.  FP64 pair arithmetic in both precisions.
+// Same decomposition as k_simplefull: every i sees every j != i and keeps
+// only its own force; energies and virial are halved at the end.
+struct SfSwArgs {
+  int n, jchunk;
+  const double *pos, *charge;
+  const int *type, *mol;
+  int ntypes;
+  const double4 *lj64;
+  const int2 *ex_range;
+  const int *ex_start, *ex_partner, *ex_class;
+  double csf;
+  Box box;
+  SwitchDev<double> lj_sw, coul_sw;
+  int lj, coul, modify;
+  double rough2;  // the larger rough-test cutoff^2
+  long long *force, *acc;
+  int em;  // 0 forces, 1 + energies, 2 + virial
+};
+
+__global__ void __launch_bounds__(kSfTile) k_simplefull_sw(SfSwArgs a) {
+  __shared__ double sx[kSfTile], sy[kSfTile], sz[kSfTile], sq[kSfTile];
+  __shared__ int st[kSfTile], sm[kSfTile];
+  const int i = blockIdx.x * kSfTile + threadIdx.x;
+  const bool valid = i < a.n;
+  const int ii = valid ? i : 0;
+  const double xi = a.pos[3 * ii], yi = a.pos[3 * ii + 1], zi = a.pos[3 * ii + 2];
+  const double qi = a.charge[ii];
+  const int ti = a.type[ii], mi = a.mol[ii];
+  const int2 er = a.ex_range[ii];
+  double fx = 0, fy = 0, fz = 0, elj = 0, ec = 0;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  const int j0 = blockIdx.y * a.jchunk, j1 = min(a.n, j0 + a.jchunk);
+  for (int base = j0; base < j1; base += kSfTile) {
+    const int j = base + threadIdx.x;
+    if (j < j1) {
+      sx[threadIdx.x] = a.pos[3 * j];
+      sy[threadIdx.x] = a.pos[3 * j + 1];
+      sz[threadIdx.x] = a.pos[3 * j + 2];
+      sq[threadIdx.x] = a.charge[j];
+      st[threadIdx.x] = a.type[j];
+      sm[threadIdx.x] = a.mol[j];
+    }
+    __syncthreads();
+    const int lim = min(kSfTile, j1 - base);
+    if (valid) {
+      for (int k = 0; k < lim; k++) {
+        const int jj = base + k;
+        if (jj == i) continue;
+        double dx, dy, dz;
+        // minimalDifference(x_i, x_j): d = x_j - x_i
+        const double r2 = box_mindiff(a.box, xi, yi, zi, sx[k], sy[k], sz[k], dx, dy, dz);
+        if (r2 > a.rough2) continue;
+        // the exclusion table only for atoms of one molecule
+        int excl = PMGPU_EXCL_NONE;
+        if (sm[k] == mi && jj >= er.x && jj <= er.y) {
+          excl = excl_class_of(a.ex_start, a.ex_partner, a.ex_class, i, jj);
+          if (excl == PMGPU_EXCL_FULL) continue;
+        }
+        const double rr2 = 1.0 / r2;
+        double f = 0;
+        if (a.lj) {
+          const double4 p = a.lj64[ti * a.ntypes + st[k]];
+          const double A = excl == PMGPU_EXCL_MODIFIED ? p.z : p.x;
+          const double B = excl == PMGPU_EXCL_MODIFIED ? p.w : p.y;
+          const double r6 = rr2 * rr2 * rr2;
+          const double r6B = B * r6, r12A = A * r6 * r6;
+          double e = r12A - r6B, ff = 12.0 * r12A * rr2 - 6.0 * r6B * rr2;
+          if (a.modify) {
+            double sv, sd;
+            switch_eval<double>(a.lj_sw, r2, sv, sd);
+            ff = ff * sv - e * sd;
+            e = e * sv;
+          }
+          elj += e;
+          f += ff;
+        }
+        if (a.coul) {
+          double e = qi * sq[k] * sqrt(rr2);
+          if (excl == PMGPU_EXCL_MODIFIED) e *= a.csf;
+          double ff = e * rr2;
+          if (a.modify) {
+            double sv, sd;
+            switch_eval<double>(a.coul_sw, r2, sv, sd);
+            ff = ff * sv - e * sd;
+            e = e * sv;
+          }
+          ec += e;
+          f += ff;
+        }
+        fx -= dx * f;
+        fy -= dy * f;
+        fz -= dz * f;
+        if (a.em == 2) {
+          const double hf = 0.5 * f;
+          v[0] += dx * dx * hf; v[1] += dx * dy * hf; v[2] += dx * dz * hf;
+          v[3] += dy * dy * hf; v[4] += dy * dz * hf; v[5] += dz * dz * hf;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (valid) {
+    red_add(&a.force[i], to_fixed(fx, kForceScale));
+    red_add(&a.force[a.n + i], to_fixed(fy, kForceScale));
+    red_add(&a.force[2 * a.n + i], to_fixed(fz, kForceScale));
+  }
+  if (!a.em) return;
+  elj = warp_sum(elj) * 0.5;
+  ec = warp_sum(ec) * 0.5;
+  if (a.em == 2)
+    for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
+  if ((threadIdx.x & 31) == 0) {
+    if (a.lj) red_add(&a.acc[ACC_LJ], to_fixed(elj, kEnergyScale));
+    if (a.coul) red_add(&a.acc[ACC_COULOMB], to_fixed(ec, kEnergyScale));
+    if (a.em == 2) {
+      const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+      for (int q = 0; q < 9; q++)
+        red_add(&a.acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
+    }
+  }
+}
+
 // The FP32 pass over each unordered pair once, as the reference visits
 // i < j (NonbondedSimpleFullSystemForce.h:125-150): a warp takes 32 x 32
 // tile pairs (I, J), I <= J, of its block's share (BlockItems), lane l
@@ -2086,6 +2212,46 @@ void halfpairs_grid(int n, int split, int *tiles, long long *items, int *blocks)
   *tiles = t;
   *items = (long long)t * (t + 1) / 2 * split;
   *blocks = (int)std::max(1LL, std::min(*items, (long long)m));
+}
+
+// The switched all-pairs form (k_simplefull_sw); lj_sw / coul_sw NULL for
+// an absent term.  em as nb_simplefull.
+int nb_simplefull_sw(System *s, const SwitchParams *lj_sw, const SwitchParams *coul_sw,
+                     int em) {
+  const int n = s->n;
+  if (n == 0 || !(lj_sw || coul_sw)) return PMGPU_OK;
+  const int iblocks = (n + kSfTile - 1) / kSfTile;
+  int chunks = std::max(1, std::min((296 + iblocks - 1) / iblocks, iblocks));
+  const int jchunk = ((n + chunks - 1) / chunks + kSfTile - 1) / kSfTile * kSfTile;
+  chunks = (n + jchunk - 1) / jchunk;
+  SfSwArgs a;
+  a.n = n;
+  a.jchunk = jchunk;
+  a.pos = s->d_pos;
+  a.charge = s->d_charge;
+  a.type = s->d_type;
+  a.mol = s->d_mol;
+  a.ntypes = s->ntypes;
+  a.lj64 = s->d_lj64;
+  a.ex_range = s->d_excl_range;
+  a.ex_start = s->d_excl_start;
+  a.ex_partner = s->d_excl_partner;
+  a.ex_class = s->d_excl_class;
+  a.csf = s->coulomb_scaling;
+  a.box = s->box;
+  SwitchParams none{};
+  a.lj_sw = make_switch_dev<double>(lj_sw ? *lj_sw : none);
+  a.coul_sw = make_switch_dev<double>(coul_sw ? *coul_sw : none);
+  a.lj = lj_sw != nullptr;
+  a.coul = coul_sw != nullptr;
+  a.modify = (lj_sw && lj_sw->modify) || (coul_sw && coul_sw->modify);
+  a.rough2 = std::max(lj_sw ? lj_sw->rough2 : 0.0, coul_sw ? coul_sw->rough2 : 0.0);
+  a.force = s->d_force;
+  a.acc = s->d_acc;
+  a.em = em;
+  k_simplefull_sw<<<dim3(iblocks, chunks), kSfTile, 0, s->stream>>>(a);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
 }
 
 // em: 0 forces only, 1 + energies, 2 + energies and virial.

@@ -100,7 +100,8 @@ __device__ __forceinline__ void apply_switch(const SwitchDev<Real> &sw,
                                              const SwitchDev<double> &sw64, Real r2,
                                              Real &ff, Real &en) {
   Real sv, sd;
-  if (sizeof(Real) == 4 && sw.kind == PMGPU_SW_CN) {
+  // the Cn and CmpCnCn polynomials cancel in FP32: evaluated in FP64
+  if (sizeof(Real) == 4 && (sw.kind == PMGPU_SW_CN || sw.kind == PMGPU_SW_CMPCNCN)) {
     double v64, d64;
     switch_eval<double>(sw64, (double)r2, v64, d64);
     sv = (Real)v64;

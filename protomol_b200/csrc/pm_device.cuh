@@ -75,8 +75,10 @@ __device__ __forceinline__ void box_minpos(const Box &b, double x, double y,
 // ------------------------------------------------------------ switching
 // Value and derivative-over-distance of ProtoMol's switching functions
 // (switch/C1SwitchingFunction.h:41-50, C2SwitchingFunction.h:42-52,
-// CnSwitchingFunction.cpp:149-175, CutoffSwitchingFunction.h:41-44,
-// UniversalSwitchingFunction.h:45-48), in the precision Real.
+// CnSwitchingFunction.cpp:149-175, CmpCnCnSwitchingFunction.h:45-95,
+// CutoffSwitchingFunction.h:41-44, UniversalSwitchingFunction.h:45-48,
+// and the complement 1 - S of ComplementSwitchingFunction.h:42-46), in
+// the precision Real.
 template <typename Real>
 struct SwitchDev {
   int kind;
@@ -85,6 +87,9 @@ struct SwitchDev {
   Real s1, s2, s3;
   int ord_int, ord_idx;
   Real irange[8];
+  Real compoff, compoff2;
+  Real itrange[8];
+  int complement;
 };
 
 template <typename Real>
@@ -98,6 +103,10 @@ __host__ inline SwitchDev<Real> make_switch_dev(const SwitchParams &p) {
   d.s1 = (Real)p.s1; d.s2 = (Real)p.s2; d.s3 = (Real)p.s3;
   d.ord_int = p.ord_int; d.ord_idx = p.ord_idx;
   for (int i = 0; i < 8; i++) d.irange[i] = (Real)p.irange[i];
+  d.compoff = (Real)p.compoff;
+  d.compoff2 = (Real)p.compoff2;
+  for (int i = 0; i < 8; i++) d.itrange[i] = (Real)p.itrange[i];
+  d.complement = p.complement;
   return d;
 }
 
@@ -218,8 +227,21 @@ __device__ __forceinline__ void write_pair_record(float4 *rec, int n, int i, dou
 }
 
 template <typename Real>
+__device__ __forceinline__ void switch_eval_base(const SwitchDev<Real> &w, Real r2,
+                                                 Real &val, Real &der);
+template <typename Real>
 __device__ __forceinline__ void switch_eval(const SwitchDev<Real> &w, Real r2,
                                             Real &val, Real &der) {
+  switch_eval_base<Real>(w, r2, val, der);
+  if (w.complement) {
+    val = Real(1) - val;
+    der = -der;
+  }
+}
+
+template <typename Real>
+__device__ __forceinline__ void switch_eval_base(const SwitchDev<Real> &w, Real r2,
+                                                 Real &val, Real &der) {
   switch (w.kind) {
     case PMGPU_SW_C2:
       der = Real(0);
@@ -245,16 +267,24 @@ __device__ __forceinline__ void switch_eval(const SwitchDev<Real> &w, Real r2,
       der = -w.c1a / d + d * w.c1c;
       return;
     }
-    case PMGPU_SW_CN: {
+    case PMGPU_SW_CN:
+    case PMGPU_SW_CMPCNCN: {
+      // Cn: one polynomial from the switch-on distance to the cutoff.
+      // CmpCnCn (CmpCnCnSwitchingFunction.h:45-95): 0 below switchon, a
+      // rising polynomial (1 - p) up to switchoff, a falling one (p) to the
+      // cutoff; each is the Cn loop with its own offset and range table.
+      const bool cmp = w.kind == PMGPU_SW_CMPCNCN;
       der = Real(0);
       val = Real(0);
       if (r2 > w.cutoff2) return;
       if (r2 < w.switchon2) {
-        val = Real(1);
+        val = cmp ? Real(0) : Real(1);
         return;
       }
+      const bool rising = cmp && r2 <= w.compoff2;
+      const bool falling = cmp && !rising;
       Real sq = pm_sqrt(r2);
-      Real sd = sq - w.cutoff;
+      Real sd = sq - (rising ? w.compoff : w.cutoff);
       Real c;  // c[0] = sd^ordInt
       if (sizeof(Real) == 8) {
         c = (Real)pow((double)sd, (double)w.ord_int);
@@ -264,9 +294,14 @@ __device__ __forceinline__ void switch_eval(const SwitchDev<Real> &w, Real r2,
       }
       for (int i = 0; i < w.ord_int + 1; i++) {
         Real cn = c * sd;                            // c[i+1]
-        val += (Real)c_cn_sw[w.ord_idx][i] * cn * w.irange[i];
-        der += (Real)c_cn_dsw[w.ord_idx][i] * c * w.irange[i];
+        const Real rg = falling ? w.itrange[i] : w.irange[i];
+        val += (Real)c_cn_sw[w.ord_idx][i] * cn * rg;
+        der += (Real)c_cn_dsw[w.ord_idx][i] * c * rg;
         c = cn;
+      }
+      if (rising) {
+        val = Real(1) - val;
+        der = -der;
       }
       der /= sq;
       return;

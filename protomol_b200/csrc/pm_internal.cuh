@@ -106,8 +106,12 @@ struct SwitchParams {
   double cutoff, cutoff2, switchon2;
   double c1a, c1b, c1c;          // C1: 1.5/rc, 0.5/rc^3, 1.5/rc^3
   double s1, s2, s3;             // C2: 1/(rc2-rs2)^3, rc2-3rs2, 4/(rc2-rs2)^3
-  int ord_int, ord_idx;          // Cn
+  int ord_int, ord_idx;          // Cn, CmpCnCn
   double irange[8];
+  double compoff, compoff2;      // CmpCnCn: the middle distance (-switchoff)
+  double itrange[8];             // CmpCnCn: 1/(switchoff - cutoff)^(k)
+  int complement;                // ComplementSwitchingFunction of the kind
+  double rough2;                 // rough-test cutoff^2 (MAXREAL for a complement)
 };
 
 // Pair-term selection for the fused pair kernel.
@@ -241,7 +245,8 @@ struct Force {
 };
 
 enum { FK_CUTOFF = 1, FK_PME = 2, FK_GB = 3, FK_BONDED = 4,
-       FK_SIMPLEFULL = 5, FK_TORSION = 6, FK_GBACE = 7 };
+       FK_SIMPLEFULL = 5, FK_TORSION = 6, FK_GBACE = 7,
+       FK_SIMPLEFULL_SW = 8 /* switched all pairs: terms.mask, lj_sw, coul_sw */ };
 
 // Per-phase CUDA-event timing; events are recorded only when enabled and
 // summed at the next host synchronisation.
@@ -498,6 +503,8 @@ int nb_fold_slots(System *s, NeighborList *nl);
 int fold_pending_slots(System *s);
 int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
 int nb_simplefull(System *s, int lj, int coul, int em);
+int nb_simplefull_sw(System *s, const SwitchParams *lj_sw, const SwitchParams *coul_sw,
+                     int em);
 // the exclusion tile masks of the FP32 simple-full pass (once per system)
 int nb_simplefull_init(System *s);
 // Launch shape of the FP32 half all-pairs passes (each unordered pair once,

@@ -271,8 +271,17 @@ class GpuSystem:
 # ------------------------------------------------------------------ forces
 def _switch(kind: str, cutoff: float, switchon: float = 0.0, switchoff: float = 0.0,
             order: float = 0.0) -> L.Switch:
+    """A switching function by its ProtoMol name: Universal, Cutoff, C1, C2,
+    Cn, CmpCnCn (ProtoMol's id "ComplimentCnCn"), or ComplementC1 /
+    ComplementC2 / ComplementCn."""
+    name = kind.lower()
+    comp = name.startswith("complement")
+    if comp:
+        name = name[len("complement"):]
     k = {"universal": L.SW_UNIVERSAL, "cutoff": L.SW_CUTOFF, "c1": L.SW_C1, "c2": L.SW_C2,
-         "cn": L.SW_CN}[kind.lower()]
+         "cn": L.SW_CN, "cmpcncn": L.SW_CMPCNCN, "complimentcncn": L.SW_CMPCNCN}[name]
+    if comp:
+        k |= L.SW_COMPLEMENT
     return L.Switch(k, float(cutoff), float(switchon), float(switchoff), float(order))
 
 
@@ -341,6 +350,35 @@ class NonbondedCutoffSystemForce(SystemForce):
         L.check(system.lib.pmgpu_force_cutoff_add(
             system.h, C.byref(lj) if lj else None, C.byref(coulomb) if coulomb else None,
             float(cutoff), float(cellsize), C.byref(fid)))
+        super().__init__(system, fid.value)
+
+
+class NonbondedFullSystemForce(SystemForce):
+    """``LennardJones|Coulomb -algorithm NonbondedFull``: the lattice sum
+    (force/nonbonded/NonbondedFullSystemForce.h, OneAtomPairFull) over the
+    cluster-pair list, every periodic image within the switch cutoff."""
+    keyword = "NonbondedFull"
+
+    def __init__(self, system: GpuSystem, lj: L.Switch | None, coulomb: L.Switch | None,
+                 cutoff: float, cellsize: float = 0.0):
+        fid = C.c_int()
+        L.check(system.lib.pmgpu_force_full_add(
+            system.h, C.byref(lj) if lj else None, C.byref(coulomb) if coulomb else None,
+            float(cutoff), float(cellsize), C.byref(fid)))
+        super().__init__(system, fid.value)
+
+
+class NonbondedSimpleFullSwitchedForce(SystemForce):
+    """``LennardJones|Coulomb -algorithm NonbondedSimpleFull
+    -switchingFunction ...``: every pair with switching functions
+    (Complement ones included), vacuum or the periodic minimal image."""
+    keyword = "NonbondedSimpleFull"
+
+    def __init__(self, system: GpuSystem, lj: L.Switch | None, coulomb: L.Switch | None):
+        fid = C.c_int()
+        L.check(system.lib.pmgpu_force_simplefull_switched_add(
+            system.h, C.byref(lj) if lj else None, C.byref(coulomb) if coulomb else None,
+            C.byref(fid)))
         super().__init__(system, fid.value)
 
 
@@ -485,9 +523,7 @@ class ForceFactory:
             return BondedSystemForce(s, "bond" in names, "angle" in names)
         if names and all(n in ("dihedral", "improper") for n in names):
             return TorsionSystemForce(s, "dihedral" in names, "improper" in names)
-        if algn == "nonbondedcutoff":
-            if not switches:
-                raise ValueError("NonbondedCutoff needs -switchingFunction")
+        def term_switches():
             sws = []
             for k, name in enumerate(names):
                 sw = switches[k] if k < len(switches) else switches[-1]
@@ -496,8 +532,16 @@ class ForceFactory:
                                           sw.get("n", 0.0))))
             lj = next((w for n, w in sws if n == "lennardjones"), None)
             co = next((w for n, w in sws if n == "coulomb"), None)
+            return sws, lj, co
+
+        if algn in ("nonbondedcutoff", "nonbondedfull"):
+            if not switches:
+                raise ValueError(f"{alg} needs -switchingFunction")
+            sws, lj, co = term_switches()
             alg_cut = p.get("cutoff", max(w.cutoff for _, w in sws))
-            return NonbondedCutoffSystemForce(s, lj, co, alg_cut, p.get("cellsize", self.cellsize))
+            cls = NonbondedCutoffSystemForce if algn == "nonbondedcutoff" else \
+                NonbondedFullSystemForce
+            return cls(s, lj, co, alg_cut, p.get("cellsize", self.cellsize))
         if algn in ("pmewald", "fullewald"):
             any_term = any(k in p for k in ("real", "reciprocal", "correction"))
             alpha = p["alpha"]
@@ -517,6 +561,15 @@ class ForceFactory:
                                   p.get("watersphereradius", 1.4))
             if "gbbornradii" in names or "gbpartialsum" in names:
                 return _NoOpForce(s, names[0])
+            if s.periodic or (switches and any(sw["kind"].lower() != "universal"
+                                               for sw in switches)):
+                if switches:
+                    _, lj, co = term_switches()
+                else:
+                    uni = _switch("Universal", 0.0)
+                    lj = uni if "lennardjones" in names else None
+                    co = uni if "coulomb" in names else None
+                return NonbondedSimpleFullSwitchedForce(s, lj, co)
             return NonbondedSimpleFullSystemForce(s, "lennardjones" in names, "coulomb" in names)
         raise ValueError(f"no GPU force for: {line}")
 
