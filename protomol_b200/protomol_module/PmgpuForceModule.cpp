@@ -289,6 +289,16 @@ const SwitchSpec kC1 = {"C1", PMGPU_SW_C1, 1, {P_CUTOFF}};
 const SwitchSpec kC2 = {"C2", PMGPU_SW_C2, 2, {P_SWITCHON, P_CUTOFF}};
 const SwitchSpec kCn = {"Cn", PMGPU_SW_CN, 4, {P_N, P_SWITCHON, P_SWITCHOFF, P_CUTOFF}};
 const SwitchSpec kCutoff = {"Cutoff", PMGPU_SW_CUTOFF, 1, {P_CUTOFF}};
+// CmpCnCnSwitchingFunction.cpp:27-45 (its id is spelled "ComplimentCnCn")
+const SwitchSpec kCmpCnCn = {"ComplimentCnCn", PMGPU_SW_CMPCNCN, 4,
+                             {P_SWITCHON, P_SWITCHOFF, P_CUTOFF, P_N}};
+// ComplementSwitchingFunction.h:48-60: "Complement" + the function's id and
+// its parameters
+const SwitchSpec kCompC1 = {"ComplementC1", PMGPU_SW_C1 | PMGPU_SW_COMPLEMENT, 1, {P_CUTOFF}};
+const SwitchSpec kCompC2 = {"ComplementC2", PMGPU_SW_C2 | PMGPU_SW_COMPLEMENT, 2,
+                            {P_SWITCHON, P_CUTOFF}};
+const SwitchSpec kCompCn = {"ComplementCn", PMGPU_SW_CN | PMGPU_SW_COMPLEMENT, 4,
+                            {P_N, P_SWITCHON, P_SWITCHOFF, P_CUTOFF}};
 
 void switchParameters(const SwitchSpec &sw, const pmgpu_switch &v, vector<Parameter> &p) {
   for (int k = 0; k < sw.nparams; k++) switch (sw.params[k]) {
@@ -328,15 +338,18 @@ pmgpu_switch switchMake(const SwitchSpec &sw, const vector<Value> &values, size_
 
 // ---------------------------------------------------------------- forces
 // NonbondedCutoff (module/NonbondedCutoffForceModule.cpp:55-96) on the GPU:
-// LennardJones and/or Coulomb, one switching function each.
+// LennardJones and/or Coulomb, one switching function each; with full set,
+// the NonbondedFull lattice sum (module/NonbondedFullForceModule.cpp:39-46,
+// force/nonbonded/NonbondedFullSystemForce.h, which adds -blocksize).
 class CutoffGpuForce : public PmgpuSystemForce {
  public:
-  CutoffGpuForce(bool lj, bool coul, const SwitchSpec &a, const SwitchSpec *b)
-      : myLJ(lj), myCoul(coul), mySwA(a), mySwB(b ? *b : a), myTwo(b != 0), myCutoff(8.0) {
+  CutoffGpuForce(bool lj, bool coul, const SwitchSpec &a, const SwitchSpec *b, bool full = false)
+      : myLJ(lj), myCoul(coul), mySwA(a), mySwB(b ? *b : a), myTwo(b != 0), myFull(full),
+        myCutoff(8.0), myBlock(64) {
     memset(&myA, 0, sizeof(myA));
     memset(&myB, 0, sizeof(myB));
   }
-  virtual string getKeyword() const { return "NonbondedCutoffGPU"; }
+  virtual string getKeyword() const { return myFull ? "NonbondedFullGPU" : "NonbondedCutoffGPU"; }
   virtual string getIdNoAlias() const {
     string id = myTwo ? "LennardJones Coulomb" : (myLJ ? "LennardJones" : "Coulomb");
     id += string(" -switchingFunction ") + mySwA.name;
@@ -347,29 +360,36 @@ class CutoffGpuForce : public PmgpuSystemForce {
     switchParameters(mySwA, myA, p);
     if (myTwo) switchParameters(mySwB, myB, p);
     p.push_back(Parameter("-cutoff", Value(myCutoff, ConstraintValueType::Positive())));
+    if (myFull)
+      p.push_back(Parameter("-blocksize", Value(myBlock, ConstraintValueType::Positive()), 64));
   }
 
  private:
   virtual Force *doMake(const vector<Value> &values) const {
-    CutoffGpuForce *f = new CutoffGpuForce(myLJ, myCoul, mySwA, myTwo ? &mySwB : 0);
+    CutoffGpuForce *f = new CutoffGpuForce(myLJ, myCoul, mySwA, myTwo ? &mySwB : 0, myFull);
     size_t at = 0;
     f->myA = switchMake(mySwA, values, &at);
     if (myTwo) f->myB = switchMake(mySwB, values, &at);
-    values[at].get(f->myCutoff);
+    values[at++].get(f->myCutoff);
+    if (myFull) values[at].get(f->myBlock);  // read and ignored: the device tiles its own way
     return f;
   }
   virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
     const pmgpu_switch *lj = myLJ ? &myA : 0;
     const pmgpu_switch *co = myCoul ? (myTwo ? &myB : &myA) : 0;
     int id = -1;
-    check(pmgpu_force_cutoff_add(s, lj, co, myCutoff, 0.0, &id), getIdNoAlias());
+    if (myFull)
+      check(pmgpu_force_full_add(s, lj, co, myCutoff, 0.0, &id), getIdNoAlias());
+    else
+      check(pmgpu_force_cutoff_add(s, lj, co, myCutoff, 0.0, &id), getIdNoAlias());
     return id;
   }
   bool myLJ, myCoul;
   SwitchSpec mySwA, mySwB;
-  bool myTwo;
+  bool myTwo, myFull;
   pmgpu_switch myA, myB;
   Real myCutoff;
+  int myBlock;
 };
 
 // Ewald Coulomb (NonbondedFullEwaldSystemForce, -real -reciprocal
@@ -430,10 +450,66 @@ class SimpleFullGpuForce : public PmgpuSystemForce {
   }
   virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
     int id = -1;
-    check(pmgpu_force_simplefull_add(s, myLJ ? 1 : 0, myCoul ? 1 : 0, &id), getIdNoAlias());
+    const int rc = pmgpu_force_simplefull_add(s, myLJ ? 1 : 0, myCoul ? 1 : 0, &id);
+    if (rc == PMGPU_ERR_UNSUPPORTED) {
+      // a periodic box: every pair's minimal image, Universal switching
+      pmgpu_switch u;
+      memset(&u, 0, sizeof(u));
+      u.kind = PMGPU_SW_UNIVERSAL;
+      check(pmgpu_force_simplefull_switched_add(s, myLJ ? &u : 0, myCoul ? &u : 0, &id),
+            getIdNoAlias());
+      return id;
+    }
+    check(rc, getIdNoAlias());
     return id;
   }
   bool myLJ, myCoul;
+  int myBlock;
+};
+
+// NonbondedSimpleFull with switching functions (module/
+// NonbondedSimpleFullForceModule.cpp:55-199: C1, C2, Cn and the Complement
+// of C1, C2 and Cn, one or two terms), vacuum or periodic.
+class SimpleFullSwGpuForce : public PmgpuSystemForce {
+ public:
+  SimpleFullSwGpuForce(bool lj, bool coul, const SwitchSpec &a, const SwitchSpec *b)
+      : myLJ(lj), myCoul(coul), mySwA(a), mySwB(b ? *b : a), myTwo(b != 0), myBlock(64) {
+    memset(&myA, 0, sizeof(myA));
+    memset(&myB, 0, sizeof(myB));
+  }
+  virtual string getKeyword() const { return "NonbondedSimpleFullGPU"; }
+  virtual string getIdNoAlias() const {
+    string id = myTwo ? "LennardJones Coulomb" : (myLJ ? "LennardJones" : "Coulomb");
+    id += string(" -switchingFunction ") + mySwA.name;
+    if (myTwo) id += string(" -switchingFunction ") + mySwB.name;
+    return id + " -algorithm " + getKeyword();
+  }
+  virtual void getParameters(vector<Parameter> &p) const {
+    switchParameters(mySwA, myA, p);
+    if (myTwo) switchParameters(mySwB, myB, p);
+    p.push_back(Parameter("-blocksize", Value(myBlock, ConstraintValueType::Positive()), 64));
+  }
+
+ private:
+  virtual Force *doMake(const vector<Value> &values) const {
+    SimpleFullSwGpuForce *f = new SimpleFullSwGpuForce(myLJ, myCoul, mySwA, myTwo ? &mySwB : 0);
+    size_t at = 0;
+    f->myA = switchMake(mySwA, values, &at);
+    if (myTwo) f->myB = switchMake(mySwB, values, &at);
+    values[at].get(f->myBlock);
+    return f;
+  }
+  virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
+    const pmgpu_switch *lj = myLJ ? &myA : 0;
+    const pmgpu_switch *co = myCoul ? (myTwo ? &myB : &myA) : 0;
+    int id = -1;
+    check(pmgpu_force_simplefull_switched_add(s, lj, co, &id), getIdNoAlias());
+    return id;
+  }
+  bool myLJ, myCoul;
+  SwitchSpec mySwA, mySwB;
+  bool myTwo;
+  pmgpu_switch myA, myB;
   int myBlock;
 };
 
@@ -643,15 +719,31 @@ void PmgpuForceModule::registerForces(ProtoMolApp *app) {
   ForceFactory &f = app->forceFactory;
   // the switching-function combinations the reference registers for
   // NonbondedCutoff (module/NonbondedCutoffForceModule.cpp:55-96), plus Cutoff
-  const SwitchSpec singles[] = {kC1, kC2, kCn, kCutoff};
-  for (int k = 0; k < 4; k++) {
+  const SwitchSpec singles[] = {kC1, kC2, kCn, kCutoff, kCmpCnCn};
+  for (int k = 0; k < 5; k++) {
     f.registerExemplar(new CutoffGpuForce(true, false, singles[k], 0));
     f.registerExemplar(new CutoffGpuForce(false, true, singles[k], 0));
   }
   const SwitchSpec pairs[][2] = {{kC2, kC1}, {kC2, kC2}, {kC2, kCn}, {kCn, kCn}, {kCn, kC2},
-                                 {kCutoff, kCutoff}, {kC2, kCutoff}};
-  for (int k = 0; k < 7; k++)
+                                 {kCutoff, kCutoff}, {kC2, kCutoff}, {kCmpCnCn, kCmpCnCn}};
+  for (int k = 0; k < 8; k++)
     f.registerExemplar(new CutoffGpuForce(true, true, pairs[k][0], &pairs[k][1]));
+  // NonbondedFull: one term, C1, C2, Cn or CmpCnCn
+  // (module/NonbondedFullForceModule.cpp:39-46)
+  const SwitchSpec fulls[] = {kC1, kC2, kCn, kCmpCnCn};
+  for (int k = 0; k < 4; k++) {
+    f.registerExemplar(new CutoffGpuForce(true, false, fulls[k], 0, true));
+    f.registerExemplar(new CutoffGpuForce(false, true, fulls[k], 0, true));
+  }
+  // NonbondedSimpleFull with switching functions
+  const SwitchSpec sf_coul[] = {kC1, kC2, kCompC1, kCompC2, kCompCn};
+  for (int k = 0; k < 5; k++) f.registerExemplar(new SimpleFullSwGpuForce(false, true, sf_coul[k], 0));
+  const SwitchSpec sf_lj[] = {kC2, kCn, kCompC1, kCompC2, kCompCn};
+  for (int k = 0; k < 5; k++) f.registerExemplar(new SimpleFullSwGpuForce(true, false, sf_lj[k], 0));
+  const SwitchSpec sf_pairs[][2] = {{kCompC2, kCompC1}, {kCompCn, kCompC1}, {kC2, kC1},
+                                    {kC2, kC2}, {kCn, kCn}};
+  for (int k = 0; k < 5; k++)
+    f.registerExemplar(new SimpleFullSwGpuForce(true, true, sf_pairs[k][0], &sf_pairs[k][1]));
   f.registerExemplar(new PmeGpuForce());
   f.registerExemplar(new SimpleFullGpuForce(true, false));
   f.registerExemplar(new SimpleFullGpuForce(false, true));

@@ -143,6 +143,33 @@ def test_cpu_integrator_with_gpu_pme_matches_full_ewald():
         assert abs(ec[-1, c] - eg[-1, c]) <= 1e-4 * abs(ec[-1, c]), (c, ec[-1], eg[-1])
 
 
+@needs_bins
+def test_lattice_sum_cmpcncn_and_complement_through_the_module():
+    """The remaining algorithm and switches through ProtoMol's factory: the
+    NonbondedFull lattice sum (C1 Coulomb, C2 LJ) in a 14.4 A box below
+    twice its 8 A cutoff, CmpCnCn on NonbondedCutoff and the Complement
+    switches on the periodic all-pairs form, under the stock Leapfrog
+    against the stock binary with the CPU forces."""
+    sysm = systems.tip3p_box(100, 14.4, seed=5, lattice=5)
+    lines = [
+        "Coulomb -algorithm {full} -switchingFunction C1 -cutoff 8 -cutoff 8",
+        "LennardJones -algorithm {full} -switchingFunction C2 -switchon 6 -cutoff 8 -cutoff 8",
+        "LennardJones Coulomb -algorithm {cut} -switchingFunction ComplimentCnCn -switchon 2 "
+        "-switchoff 5 -cutoff 6.5 -n 3 -switchingFunction ComplimentCnCn -switchon 1 "
+        "-switchoff 4 -cutoff 6.5 -n 2 -cutoff 6.5",
+        "LennardJones Coulomb -algorithm {sf} -switchingFunction ComplementC2 -switchon 5 "
+        "-cutoff 6 -switchingFunction ComplementC1 -cutoff 6",
+        "Bond", "Angle"]
+    cpu = [ln.format(full="NonbondedFull", cut="NonbondedCutoff", sf="NonbondedSimpleFull")
+           for ln in lines]
+    gpu = [ln.format(full="NonbondedFullGPU", cut="NonbondedCutoffGPU",
+                     sf="NonbondedSimpleFullGPU") for ln in lines]
+    pc, ec, pg, eg = _both(sysm, cpu, gpu, 10, cellsize=6.5)
+    assert np.abs(pc - pg).max() < 1e-5, np.abs(pc - pg).max()  # FP32 forces, as above
+    for c in (1, 3):
+        assert abs(ec[-1, c] - eg[-1, c]) <= 1e-5 * abs(ec[-1, c]), (c, ec[-1], eg[-1])
+
+
 def _gb_polymer(n, seed):
     """A GB heteropolymer as ProtoMol's PSF/PAR path builds it: the reader
     takes each type's GB radius from its PAR Rmin/2 (topology/
