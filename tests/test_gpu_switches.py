@@ -32,6 +32,16 @@ def _energy_ok(got, want, rel=E_REL, floor=1e-4):
     return abs(got - want) <= max(rel * abs(want), floor)
 
 
+# forces are summed in 64-bit fixed point, 2^-32 kcal/mol/A per unit: for
+# terms whose forces are small (the far-pair Complement terms, ~1e-2) a few
+# units of that resolution exceed 1e-8 relative
+FIXED_QUANTUM = 2.0 ** -32
+
+
+def _forces_ok(f, ref, tol):
+    return F.rms_rel(f, ref) <= tol or np.abs(f - ref).max() <= 4 * FIXED_QUANTUM
+
+
 @pytest.mark.parametrize("name", ["small_tip3p300_switches", "fip35_switches"])
 @pytest.mark.parametrize("precision,tol", [("mixed", 1e-5), ("double", 1e-8)])
 def test_switch_variants_and_lattice_sum_vs_reference(ctx, name, precision, tol):
@@ -49,7 +59,7 @@ def test_switch_variants_and_lattice_sum_vs_reference(ctx, name, precision, tol)
         f = np.zeros_like(topo.pos)
         e = ScalarStructure()
         force.evaluate(topo.pos, f, e, virial=True)
-        assert F.rms_rel(f, ref_f) <= tol, (d, F.rms_rel(f, ref_f))
+        assert _forces_ok(f, ref_f, tol), (d, F.rms_rel(f, ref_f), np.abs(f - ref_f).max())
         assert _energy_ok(e[0], ref_e[0], rel=min(E_REL, tol)), (d, e[0], ref_e[0])
         assert _energy_ok(e[1], ref_e[1], rel=min(E_REL, tol)), (d, e[1], ref_e[1])
         vir = np.asarray(e[7:16])
@@ -58,7 +68,7 @@ def test_switch_variants_and_lattice_sum_vs_reference(ctx, name, precision, tol)
         # the force-only evaluation (the kernels of an inner MD step)
         f2 = np.zeros_like(topo.pos)
         force.evaluate(topo.pos, f2, None)
-        assert F.rms_rel(f2, ref_f) <= tol, (d, "force-only", F.rms_rel(f2, ref_f))
+        assert _forces_ok(f2, ref_f, tol), (d, "force-only", F.rms_rel(f2, ref_f))
         force.set_enabled(False)
         seen += 1
     assert seen == (4 if name == "fip35_switches" else 10)
