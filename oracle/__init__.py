@@ -27,7 +27,7 @@ LIB = os.path.join(HERE, "liboracle.so")
 EXCL_NONE, EXCL_MODIFIED, EXCL_FULL = 0, 1, 2
 SW_UNIVERSAL, SW_CUTOFF, SW_C1, SW_C2, SW_CN, SW_CMPCNCN = 0, 1, 2, 3, 4, 5
 SW_COMPLEMENT = 16  # flag on C1 / C2 / Cn: ComplementSwitchingFunction of it
-POT_COULOMB, POT_LJ = 0, 1
+POT_COULOMB, POT_LJ, POT_SCPISM = 0, 1, 2
 INV_TIMEFACTOR = 0.02045482828087295  # base/PMConstants.cpp:54
 SQRTCOULOMBCONSTANT = 18.2226123264  # base/PMConstants.cpp:67
 BOLTZMANN = 0.001987191  # base/PMConstants.cpp:70
@@ -125,6 +125,10 @@ class System:
     # class per exclusion-table entry as getTable() holds it (None: same as
     # excl[:, 2]); the Ewald correction term iterates the table
     excl_table_class: np.ndarray | None = None
+    # SCPISM per-atom data (keys as pm_forcedump writes them: scp_sqrtalpha,
+    # scp_alpha, scp_zeta, scp_eta, scp_c, scp_g, scp_hbond, scp_residue,
+    # scp_name); None: no SCPISM parameters
+    scpism: dict | None = None
 
     @property
     def n(self) -> int:
@@ -349,6 +353,63 @@ def bonded_force(sysm: System, bonds=None, bond_params=None, angles=None, angle_
 
 ACE_SIGMA = 2.26 / 418.4  # GBACEForce -solvationparam default (GBACEForce.cpp:226)
 ACE_RHO = 1.4             # -watersphereradius default (GBACEForce.cpp:229)
+
+
+class _Scpism(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("sqrtalpha", "alpha", "zeta", "eta", "c", "g", "hbond",
+                                           "residue", "name", "water")]
+
+
+def _scpism(sysm: System):
+    d = sysm.scpism
+    keep = {k: np.ascontiguousarray(d["scp_" + k], dtype=np.float64)
+            for k in ("sqrtalpha", "alpha", "zeta", "eta", "c", "g")}
+    keep.update({k: np.ascontiguousarray(d["scp_" + k], dtype=np.int32)
+                 for k in ("hbond", "residue", "name")})
+    keep["water"] = np.ascontiguousarray(sysm.water if sysm.water is not None
+                                         else np.zeros(sysm.n), dtype=np.int32)
+    p = _Scpism(**{k: v.ctypes.data for k, v in keep.items()})
+    return p, keep
+
+
+def _pot(name: str) -> int:
+    n = name.lower()
+    if n.startswith("lennard"):
+        return POT_LJ
+    return POT_SCPISM if n == "coulombscpism" else POT_COULOMB
+
+
+def scpism_pair_force(sysm: System, terms, D: float = 80.0):
+    """LennardJones and/or CoulombSCPISM over every pair within the switch
+    cutoffs: terms is a list of (potential, Switch)."""
+    cs = sysm.c()
+    p, keep = _scpism(sysm)
+    pots = np.array([_pot(t) for t, _ in terms], np.int32)
+    sws = (_Switch * len(terms))(*[w.c() for _, w in terms])
+    f = np.zeros((sysm.n, 3))
+    e = np.zeros(2)
+    v = np.zeros(9)
+    rc = lib().orc_scpism_pair_force(C.byref(cs), C.byref(p), C.c_double(D), len(terms),
+                                     _ptr(pots), sws, _ptr(f), _ptr(e), _ptr(v))
+    assert rc == 0
+    return f, {"coulomb": e[0], "lj": e[1]}, v.reshape(3, 3)
+
+
+def born_force(sysm: System, radii_switch: int = 3, radii_cutoff: float = 5.0,
+               self_switch: int = 3, self_cutoff: float = 5.0, D: float = 80.0):
+    """BornRadii then BornSelf: (forces, self energy, Born radii)."""
+    cs = sysm.c()
+    p, keep = _scpism(sysm)
+    f = np.zeros((sysm.n, 3))
+    e = np.zeros(2)
+    v = np.zeros(9)
+    born = np.zeros(sysm.n)
+    rc = lib().orc_born_force(C.byref(cs), C.byref(p), int(radii_switch),
+                              C.c_double(radii_cutoff), int(self_switch),
+                              C.c_double(self_cutoff), C.c_double(D), _ptr(born), _ptr(f),
+                              _ptr(e), _ptr(v))
+    assert rc == 0
+    return f, float(e[0]), born
 
 
 def gbace_force(sysm: System, sigma: float = ACE_SIGMA, rho_s: float = ACE_RHO):

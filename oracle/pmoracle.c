@@ -623,9 +623,36 @@ static void coul_eval(const orc_system *s, int i, int j, int excl, double rr2,
   *f = *e * rr2;
 }
 
+/* CoulombSCPISMForce::operator() (force/coulomb/CoulombSCPISMForce.h:
+ * 33-71): the Coulomb energy over a distance-dependent dielectric; no
+ * contribution when either atom's molecule is water. */
+static void scpism_eval(const orc_system *s, const orc_scpism *p, double D, int i, int j,
+                        int excl, double rr2, double *e, double *f) {
+  double rDist, Dist, alpha_ij, Dp1, rDp1, Dm1, k, rEXP, DiElec, rDiElec, drDiElec;
+  *e = 0.0;
+  *f = 0.0;
+  if (p->water[i] || p->water[j]) return;
+  rDist = sqrt(rr2);
+  Dist = 1.0 / rDist;
+  alpha_ij = p->sqrtalpha[i] * p->sqrtalpha[j];
+  Dp1 = D + 1.0;
+  rDp1 = 1.0 / Dp1;
+  Dm1 = D - 1.0;
+  k = Dm1 * 0.5;
+  rEXP = k * exp(-alpha_ij * Dist);
+  DiElec = Dp1 / (1.0 + rEXP) - 1.0;
+  rDiElec = 1.0 / DiElec;
+  *e = s->charge[i] * s->charge[j] * rDist * rDiElec *
+       (excl == ORC_EXCL_MODIFIED ? s->coulomb_scaling : 1);
+  drDiElec = alpha_ij * rDp1 * (1.0 + DiElec) * (D - DiElec);
+  *f = (rDiElec * drDiElec + rDist) * *e * rDist;
+}
+
 typedef struct {
   const orc_system *s;
   const pbc_t *p;
+  const orc_scpism *scp;
+  double scp_D;
   excl_t ex;
   int nterms;
   int pot[2];
@@ -672,6 +699,8 @@ static void cutoff_visit(void *vctx, int i, int j) {
     double e, f, sv = 1.0, sd = 0.0;
     if (c->pot[t] == ORC_POT_LJ)
       lj_eval(s, i, j, excl, rr2, &e, &f);
+    else if (c->pot[t] == ORC_POT_SCPISM)
+      scpism_eval(s, c->scp, c->scp_D, i, j, excl, rr2, &e, &f);
     else
       coul_eval(s, i, j, excl, rr2, &e, &f);
     /* MODIFY is set for C1/C2/Cn only (enums in the switch/ headers); OneAtomPairTwo
@@ -761,9 +790,26 @@ int orc_simplefull_force(const orc_system *s, int potential,
  * (NonbondedSimpleFullSystemForce.h:125-150); the rough test is against
  * the larger switch cutoff (OneAtomPairTwo.h:40-44), minimal image in a
  * periodic box. */
+static int allpairs_force(const orc_system *s, const orc_scpism *scp, double D, int nterms,
+                          const int *potentials, const orc_switch *sw, double *forces,
+                          double *energies, double *virial);
+
 int orc_simplefull_force_n(const orc_system *s, int nterms, const int *potentials,
                            const orc_switch *sw, double *forces, double *energies,
                            double *virial) {
+  return allpairs_force(s, NULL, 0.0, nterms, potentials, sw, forces, energies, virial);
+}
+
+int orc_scpism_pair_force(const orc_system *s, const orc_scpism *p, double D, int nterms,
+                          const int *potentials, const orc_switch *sw, double *forces,
+                          double *energies, double *virial) {
+  if (!p) return -1;
+  return allpairs_force(s, p, D, nterms, potentials, sw, forces, energies, virial);
+}
+
+static int allpairs_force(const orc_system *s, const orc_scpism *scp, double D, int nterms,
+                          const int *potentials, const orc_switch *sw, double *forces,
+                          double *energies, double *virial) {
   pbc_t p;
   cutoff_ctx c;
   int bi, bj, i, j, t;
@@ -773,6 +819,8 @@ int orc_simplefull_force_n(const orc_system *s, int nterms, const int *potential
   pbc_set(s, &p);
   c.s = s;
   c.p = &p;
+  c.scp = scp;
+  c.scp_D = D;
   excl_build(s, &c.ex);
   c.nterms = nterms;
   c.cut2 = 0.0;
@@ -1141,6 +1189,125 @@ int orc_full_force(const orc_system *s, int potential, const orc_switch *sw,
           }
         }
   free(lat);
+  excl_free(&ex);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* SCPISM Born radii and self force (force/born/BornRadii.h:33-77,
+ * force/born/BornSelfForce.h:31-118, force/born/BornSwitch.h). */
+static double born_sw(int sw, double r) { /* BornSwitch::switchValue */
+  double f;
+  if (r >= 5.0) return 0.0;
+  if (sw == 3) {
+    f = (1 - .0016 * r * r * r * r);
+    return f * f * f * f;
+  } else if (sw == 1) {
+    f = (1 - .04 * r * r);
+    return f * f;
+  } else if (sw == 2) {
+    f = (1 - 0.008 * r * r * r);
+    return f * f * f;
+  }
+  return 1.0;
+}
+static double born_swd(int sw, double r) { /* BornSwitch::switchDerivative */
+  double f;
+  if (r >= 5.0) return 0.0;
+  if (sw == 3) {
+    f = (1 - .0016 * r * r * r * r);
+    return -16 * .0016 * r * r * r * f * f * f;
+  } else if (sw == 1) {
+    return -0.16 * (1 - 0.04 * r * r) * r;
+  } else if (sw == 2) {
+    return -9 * .008 * r * r * (1 - .008 * r * r * r) * (1 - .008 * r * r * r);
+  }
+  return 0.0;
+}
+/* The polar hydrogen term of atom a against atom b: g_a' g_b when a is a
+ * polar H (1), b an acceptor (2) in another residue, with g_a' = -0.378
+ * for an HN against an O (BornRadii.h:45-58). */
+static int born_polar(const orc_scpism *p, int a, int b, double *gg) {
+  double ga;
+  if (!(p->hbond[a] == 1 && p->hbond[b] == 2 && p->residue[a] != p->residue[b])) return 0;
+  ga = (p->name[a] == 1 && p->name[b] == 2) ? -0.378 : p->g[a];
+  *gg = ga * p->g[b];
+  return 1;
+}
+
+int orc_born_force(const orc_system *s, const orc_scpism *p, int radii_bornswitch,
+                   double radii_cutoff, int self_bornswitch, double self_cutoff, double D,
+                   double *born_out, double *forces, double *energies, double *virial) {
+  pbc_t pb;
+  excl_t ex;
+  int i, j, t;
+  const int n = s->n;
+  const double E = 0.80; /* the polar H+ constant (BornRadii.h:51) */
+  const double K = (D - 1.0) / 2;
+  double *R = (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+  double *Ds = (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+  int *used = (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int));
+  double self_total = 0.0;
+  if (!p) return -1;
+  pbc_set(s, &pb);
+  excl_build(s, &ex);
+  /* BornRadii: preForce (radius = zeta), then every pair op in cutoff */
+  for (i = 0; i < n; i++) R[i] = p->zeta[i];
+  for (i = 0; i < n; i++)
+    for (j = i + 1; j < n; j++) {
+      double d[3], r2, dist, f, gg;
+      int excl;
+      pbc_mindiff(&pb, s->pos + 3 * i, s->pos + 3 * j, d, &r2);
+      if (r2 > radii_cutoff * radii_cutoff) continue;
+      excl = s->molecule[i] == s->molecule[j] ? excl_check(&ex, i, j) : ORC_EXCL_NONE;
+      if (excl == ORC_EXCL_FULL) continue;
+      if (p->water[i] || p->water[j]) continue;
+      dist = sqrt(r2);
+      f = born_sw(radii_bornswitch, dist);
+      R[i] += p->eta[i] * f * exp(-p->c[i] * dist);
+      if (born_polar(p, i, j, &gg)) R[i] += gg * f * exp(-E * dist);
+      R[j] += p->eta[j] * f * exp(-p->c[j] * dist);
+      if (born_polar(p, j, i, &gg)) R[j] += gg * f * exp(-E * dist);
+    }
+  if (born_out)
+    for (i = 0; i < n; i++) born_out[i] = R[i];
+  /* BornSelf: the solvation factor D_s of each atom, computed once */
+  for (i = 0; i < n; i++) Ds[i] = (1.0 + D) / (1 + K * exp(-p->alpha[i] * R[i])) - 1.0;
+  for (i = 0; i < n; i++)
+    for (j = i + 1; j < n; j++) {
+      double d[3], r2, dist, rDist, f, fp, gg, force = 0.0, fij[3];
+      int excl, side;
+      pbc_mindiff(&pb, s->pos + 3 * i, s->pos + 3 * j, d, &r2);
+      if (r2 > self_cutoff * self_cutoff) continue;
+      excl = s->molecule[i] == s->molecule[j] ? excl_check(&ex, i, j) : ORC_EXCL_NONE;
+      if (excl == ORC_EXCL_FULL) continue;
+      dist = sqrt(r2);
+      rDist = 1.0 / dist;
+      f = born_sw(self_bornswitch, dist);
+      fp = born_swd(self_bornswitch, dist);
+      for (side = 0; side < 2; side++) {
+        const int a = side ? j : i, b = side ? i : j;
+        double dRs = p->eta[a] * (fp - f * p->c[a]) * exp(-p->c[a] * dist);
+        double rR = 1.0 / R[a], rDs = 1.0 / Ds[a];
+        double dDs = p->alpha[a] * (1.0 / (1.0 + D)) * (1 + Ds[a]) * (D - Ds[a]);
+        double q = s->charge[a];
+        if (born_polar(p, a, b, &gg)) dRs += gg * (fp - f * E) * exp(-E * dist);
+        force += (-0.5 * q * q * rR * rR * (1.0 - rDs - R[a] * rDs * rDs * dDs) * dRs) * rDist;
+      }
+      used[i] = used[j] = 1;
+      for (t = 0; t < 3; t++) fij[t] = d[t] * force;
+      for (t = 0; t < 3; t++) {
+        forces[3 * i + t] -= fij[t];
+        forces[3 * j + t] += fij[t];
+      }
+      add_virial(virial, fij, d);
+    }
+  for (i = 0; i < n; i++)
+    if (used[i]) self_total += 0.5 * s->charge[i] * s->charge[i] / R[i] * (1.0 / Ds[i] - 1);
+  energies[0] += self_total;
+  free(R);
+  free(Ds);
+  free(used);
   excl_free(&ex);
   return 0;
 }

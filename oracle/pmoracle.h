@@ -23,8 +23,18 @@ enum { ORC_SW_UNIVERSAL = 0, ORC_SW_CUTOFF = 1, ORC_SW_C1 = 2, ORC_SW_C2 = 3,
 /* Flag OR'd into a C1, C2 or Cn kind: ComplementSwitchingFunction of it
  * (switch/ComplementSwitchingFunction.h:14-74). */
 enum { ORC_SW_COMPLEMENT = 16 };
-/* Potentials. */
-enum { ORC_POT_COULOMB = 0, ORC_POT_LJ = 1 };
+/* Potentials (CoulombSCPISM: force/coulomb/CoulombSCPISMForce.h). */
+enum { ORC_POT_COULOMB = 0, ORC_POT_LJ = 1, ORC_POT_SCPISM = 2 };
+
+/* SCPISM per-atom data as ProtoMol's topology builder forms it
+ * (topology/BuildTopology.cpp:757-818): the atom's type's alpha, C_i, g_i
+ * and H-bond class (0 none, 1 polar H, 2 acceptor; topology/AtomType.h:10),
+ * the atom's sqrt(alpha), zeta and eta, its residue number, whether its
+ * name is HN (1) or O (2), and whether its molecule is water. */
+typedef struct {
+  const double *sqrtalpha, *alpha, *zeta, *eta, *c, *g;
+  const int *hbond, *residue, *name, *water;
+} orc_scpism;
 
 typedef struct {
   int kind;
@@ -87,6 +97,24 @@ int orc_simplefull_force(const orc_system *s, int potential,
 int orc_simplefull_force_n(const orc_system *s, int nterms, const int *potentials,
                            const orc_switch *sw, double *forces, double *energies,
                            double *virial);
+
+/* LennardJones and/or CoulombSCPISM (-D dielectric) over every pair within
+ * the larger switch cutoff, OneAtomPair / OneAtomPairTwo
+ * (force/coulomb/CoulombSCPISMForce.h), vacuum or the periodic minimal
+ * image: the pair set of NonbondedCutoff and of NonbondedSimpleFull with a
+ * cutoff switch alike. */
+int orc_scpism_pair_force(const orc_system *s, const orc_scpism *p, double D, int nterms,
+                          const int *potentials, const orc_switch *sw, double *forces,
+                          double *energies, double *virial);
+
+/* BornRadii then BornSelf (force/born/BornRadii.h, force/born/
+ * BornSelfForce.h) over the pairs within each force's cutoff switch
+ * (OneAtomPair with the Cutoff switch): the Born radii (written to
+ * born_out if not NULL), the BornSelf pair forces and the self energies of
+ * the atoms that took part in a pair (energies[0], COULOMB). */
+int orc_born_force(const orc_system *s, const orc_scpism *p, int radii_bornswitch,
+                   double radii_cutoff, int self_bornswitch, double self_cutoff, double D,
+                   double *born_out, double *forces, double *energies, double *virial);
 
 /* NonbondedFullSystemForce (lattice sum, force/nonbonded/
  * NonbondedFullSystemForce.h:38-62) with OneAtomPairFull

@@ -116,6 +116,36 @@ int main(int argc, char *argv[]) {
       obc[0] = topo->alphaObc; obc[1] = topo->betaObc; obc[2] = topo->gammaObc;
       putv(f, "gb_obc", obc);
     }
+    if (topo->doSCPISM) {
+      // SCPISM data as the topology builder forms it (topology/
+      // BuildTopology.cpp:757-818): per atom its type's alpha, C_i, g_i and
+      // H-bond class, its own sqrt(alpha), zeta and eta, its residue and
+      // whether its name is HN (1) or O (2) (force/born/BornRadii.h:56-58)
+      vector<double> sa(n), al(n), ze(n), et(n), ci(n), gi(n);
+      vector<long> hb(n), res(n), nm(n);
+      for (unsigned i = 0; i < n; i++) {
+        const Atom &at = topo->atoms[i];
+        const SCPISMAtomTypeParameters *t = topo->atomTypes[at.type].mySCPISM_T;
+        sa[i] = at.mySCPISM_A->sqrtalphaSCPISM;
+        al[i] = t->alpha;
+        ze[i] = at.mySCPISM_A->zeta;
+        et[i] = at.mySCPISM_A->eta;
+        ci[i] = t->C_i;
+        gi[i] = t->g_i;
+        hb[i] = (long)t->isHbonded;
+        res[i] = at.residue_seq;
+        nm[i] = at.name == "HN" ? 1 : (at.name == "O" ? 2 : 0);
+      }
+      putv(f, "scp_sqrtalpha", sa);
+      putv(f, "scp_alpha", al);
+      putv(f, "scp_zeta", ze);
+      putv(f, "scp_eta", et);
+      putv(f, "scp_c", ci);
+      putv(f, "scp_g", gi);
+      puti(f, "scp_hbond", hb);
+      puti(f, "scp_residue", res);
+      puti(f, "scp_name", nm);
+    }
     // Type names, used only by tests that re-derive GB scaling factors.
     fprintf(f, "typenames %lu", (unsigned long)topo->atomTypes.size());
     for (size_t t = 0; t < topo->atomTypes.size(); t++)

@@ -46,7 +46,8 @@ def parse(path: str) -> dict:
                 out["forces"].append(cur)
                 continue
             if key in ("type", "molecule", "water", "exclusions", "exclusions_check", "bonds",
-                       "angles", "dihedrals", "impropers"):
+                       "angles", "dihedrals", "impropers", "scp_hbond", "scp_residue",
+                       "scp_name"):
                 arr = np.array([int(v) for v in vals], dtype=np.int64)
             else:
                 arr = np.array([float(v) for v in vals], dtype=np.float64)
@@ -81,6 +82,8 @@ def to_system(d: dict) -> System:
         water=d["water"].astype(np.int32),
         excl_table_class=table_class,
     )
+    if "scp_alpha" in d:
+        s.scpism = {k: d[k].copy() for k in d if k.startswith("scp_")}
     if "gb_vdwr" in d:
         s.gb_vdwr = d["gb_vdwr"].copy()
         s.gb_scale = d["gb_scale"].copy()

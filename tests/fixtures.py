@@ -45,6 +45,8 @@ def topology(z: dict) -> SimpleNamespace:
         t.gb_scale = z["gb_scale"].copy()
         t.gb_offset = z["gb_offset"].copy()
         t.gb_obc = tuple(z["gb_obc"])
+    if "scp_alpha" in z:
+        t.scpism = {k: z[k].copy() for k in z if k.startswith("scp_")}
     return t
 
 
@@ -58,6 +60,8 @@ def oracle_system(z: dict):
     if hasattr(t, "gb_vdwr"):
         s.gb_vdwr, s.gb_scale, s.gb_offset, s.gb_obc = (t.gb_vdwr, t.gb_scale, t.gb_offset,
                                                          t.gb_obc)
+    if hasattr(t, "scpism"):
+        s.scpism = t.scpism
     return s
 
 
@@ -78,7 +82,7 @@ def parse_cutoff_def(d: str):
     """(potentials, switch dicts, algorithm cutoff) of a NonbondedCutoff,
     NonbondedFull or NonbondedSimpleFull line."""
     toks = d.split()
-    pots = [t for t in toks if t in ("LennardJones", "Coulomb")]
+    pots = [t for t in toks if t in ("LennardJones", "Coulomb", "CoulombSCPISM")]
     sws, i, alg = [], 0, None
     while i < len(toks):
         if toks[i] == "-switchingFunction":

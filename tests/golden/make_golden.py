@@ -38,6 +38,8 @@ def _ref_tests() -> str:
 def save(name: str, d: dict, extra: dict | None = None) -> None:
     out = {}
     for k in ("natoms", "charge", "mass", "type", "molecule", "water", "lj", "ntypes",
+              "scp_sqrtalpha", "scp_alpha", "scp_zeta", "scp_eta", "scp_c", "scp_g",
+              "scp_hbond", "scp_residue", "scp_name",
               "exclusions", "exclusions_check", "coulomb_scaling", "periodic", "box",
               "positions", "velocities", "bonds", "bond_params", "angles", "angle_params",
               "dihedrals", "dihedral_params", "impropers", "improper_params",
@@ -175,7 +177,36 @@ def switch_variants() -> None:
     save("fip35_switches", d)
 
 
+def scpism() -> None:
+    """The reference's implicit-solvent (SCPISM) systems: its own force
+    lines (LennardJones + CoulombSCPISM with Cn switching on NonbondedCutoff,
+    BornRadii and BornSelf) and CoulombSCPISM with other switches and -D on
+    the cutoff and all-pairs algorithms."""
+    forces = [
+        "LennardJones CoulombSCPISM -algorithm NonbondedCutoff -switchingFunction Cn -n 4 "
+        "-switchon 8.0 -cutoff 20.0 -switchingFunction Cn -n 4 -switchon 8.0 -cutoff 20.0 "
+        "-cutoff 20.0",
+        "BornRadii -algorithm NonbondedCutoff -switchingFunction Cutoff -bornswitch 3 "
+        "-cutoff 5 -cutoff 5",
+        "BornSelf -algorithm NonbondedCutoff -switchingFunction Cutoff -bornswitch 3 "
+        "-cutoff 5 -cutoff 5",
+        "CoulombSCPISM -algorithm NonbondedCutoff -switchingFunction C2 -switchon 0 "
+        "-cutoff 12 -cutoff 12 -D 60",
+        "CoulombSCPISM -algorithm NonbondedSimpleFull -switchingFunction C1 -cutoff 15",
+        "LennardJones CoulombSCPISM -algorithm NonbondedSimpleFull -switchingFunction C2 "
+        "-switchon 6 -cutoff 14 -switchingFunction C1 -cutoff 14",
+        "BornRadii -algorithm NonbondedCutoff -switchingFunction Cutoff -bornswitch 1 "
+        "-cutoff 4 -cutoff 4",
+        "BornSelf -algorithm NonbondedCutoff -switchingFunction Cutoff -bornswitch 2 "
+        "-cutoff 4.5 -cutoff 4.5 -D 60"]
+    save("alanine_scpism", reference_conf("alanine_CHARMM_IMPLICIT_LL.conf", forces))
+    save("wwdomain_scpism", reference_conf("wwdomain_CHARMM_IMPLICIT_LL.conf", forces))
+
+
 def main(which: str = "all") -> None:
+    if which == "scpism":
+        scpism()
+        return
     if which == "switches":
         switch_variants()
         return

@@ -242,3 +242,40 @@ def test_switch_variants_and_lattice_sum_match_reference(name):
         kinds.add(d.split("-algorithm")[1].split()[0])
     assert kinds >= ({"NonbondedSimpleFull"} if name == "fip35_switches" else
                      {"NonbondedCutoff", "NonbondedFull", "NonbondedSimpleFull"})
+
+
+def _param(line, key, default):
+    toks = line.split()
+    return float(toks[toks.index(key) + 1]) if key in toks else default
+
+
+@pytest.mark.parametrize("name", ["alanine_scpism", "wwdomain_scpism"])
+def test_scpism_oracle_matches_reference(name):
+    """SCPISM on the reference's implicit-solvent systems: LennardJones +
+    CoulombSCPISM (Cn on NonbondedCutoff; C1, C2 on the cutoff and
+    all-pairs algorithms; -D), and the BornRadii + BornSelf chain (Born
+    switches 3, 1 and 2), against the reference's own forces and energies."""
+    z = F.load(name)
+    s = F.oracle_system(z)
+    seen = 0
+    for k, d in enumerate(z["defs"]):
+        d = str(d)
+        if d.startswith("BornRadii"):
+            continue
+        if d.startswith("BornSelf"):
+            rd = str(z["defs"][k - 1])  # its BornRadii line
+            f, e, _ = oracle.born_force(s, int(_param(rd, "-bornswitch", 3)),
+                                        _param(rd, "-cutoff", 5.0),
+                                        int(_param(d, "-bornswitch", 3)),
+                                        _param(d, "-cutoff", 5.0), _param(d, "-D", 80.0))
+            e_c, e_lj = e, 0.0
+        else:
+            terms, _ = _switch_terms(d)
+            f, e, _ = oracle.scpism_pair_force(s, terms, _param(d, "-D", 80.0))
+            e_c, e_lj = e["coulomb"], e["lj"]
+        ref_f, ref_e = F.forces(z, k), F.energies(z, k)
+        assert np.abs(f - ref_f).max() < 1e-11 * max(1.0, np.abs(ref_f).max()), d
+        assert e_c == pytest.approx(ref_e[0], rel=1e-12, abs=1e-9), d
+        assert e_lj == pytest.approx(ref_e[1], rel=1e-12, abs=1e-9), d
+        seen += 1
+    assert seen == 6
