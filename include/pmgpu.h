@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define PMGPU_ABI_VERSION 1
+#define PMGPU_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------- */
 enum {
@@ -134,6 +134,17 @@ typedef struct {
   int n_impropers;
   const int *improper_atoms;
   const double *improper_params;
+  /* SCPISM implicit-solvent data as ProtoMol's topology builder forms it
+   * (topology/BuildTopology.cpp:757-818, topology/Atom.h:10-29,
+   * topology/AtomType.h:10-21), n each: the atom's sqrt(alpha), its type's
+   * alpha, the atom's zeta and eta, its type's C_i and g_i, its type's
+   * H-bond class (0 none, 1 polar hydrogen, 2 acceptor), its residue
+   * number, and its name class (1 "HN", 2 "O", 0 other; BornRadii.h:56).
+   * NULL scpism_alpha: no SCPISM parameters (the SCPISM forces are then
+   * refused).  The water flags above mark atoms the SCPISM pair terms skip. */
+  const double *scpism_sqrtalpha, *scpism_alpha, *scpism_zeta, *scpism_eta;
+  const double *scpism_c, *scpism_g;
+  const int *scpism_hbond, *scpism_residue, *scpism_name;
 } pmgpu_topology;
 
 typedef struct {
@@ -219,6 +230,24 @@ int pmgpu_force_full_add(pmgpu_system *sys, const pmgpu_switch *lj_sw,
  * arithmetic is FP64 in both precisions. */
 int pmgpu_force_simplefull_switched_add(pmgpu_system *sys, const pmgpu_switch *lj_sw,
                                         const pmgpu_switch *coul_sw, int *force_id);
+/* LennardJones and/or CoulombSCPISM (force/coulomb/CoulombSCPISMForce.h,
+ * -D the bulk dielectric) on NonbondedCutoff or NonbondedSimpleFull
+ * (module/NonbondedCutoffForceModule.cpp:91-107, 145-160;
+ * module/NonbondedSimpleFullForceModule.cpp:104-116): every pair within the
+ * larger switch cutoff, vacuum or the periodic minimal image, which is the
+ * pair set of both algorithms; FP64 pair arithmetic.  coul_sw is the
+ * CoulombSCPISM term's switch (required), lj_sw NULL for no LJ term. */
+int pmgpu_force_scpism_add(pmgpu_system *sys, const pmgpu_switch *lj_sw,
+                           const pmgpu_switch *coul_sw, double dielectric, int *force_id);
+/* BornRadii followed by BornSelf (force/born/BornRadii.h:33-77,
+ * force/born/BornSelfForce.h:31-118, module/NonbondedCutoffForceModule.cpp:
+ * 145-148): the SCPISM Born radii over the pairs within radii_cutoff (Born
+ * switch radii_bornswitch), then the BornSelf pair forces over the pairs
+ * within self_cutoff and the self energy of every atom in such a pair
+ * (COULOMB).  FP64. */
+int pmgpu_force_born_add(pmgpu_system *sys, int radii_bornswitch, double radii_cutoff,
+                         int self_bornswitch, double self_cutoff, double dielectric,
+                         int *force_id);
 /* NonbondedSimpleFull LennardJones and/or Coulomb (vacuum all pairs with
  * exclusions, module/NonbondedSimpleFullForceModule.cpp). */
 int pmgpu_force_simplefull_add(pmgpu_system *sys, int lj, int coulomb,

@@ -10,6 +10,6 @@ from .engine import (  # noqa: F401
     ANGLE, BOND, COULOMB, LENNARDJONES, VIRIALXX, BondedSystemForce, Context, ForceFactory,
     GBACEForce, GBForce, GpuSystem, LangevinLeapfrogIntegrator, LeapfrogIntegrator,
     NonbondedCutoffSystemForce, NonbondedFullSystemForce, NonbondedSimpleFullSwitchedForce,
-    NonbondedSimpleFullSystemForce, PMEwaldSystemForce,
+    NonbondedSimpleFullSystemForce, PMEwaldSystemForce, ScpismSystemForce, BornSystemForce,
     ScalarStructure, SystemForce, TorsionSystemForce)
 from ._lib import PmgpuError, load  # noqa: F401

@@ -44,7 +44,8 @@ EXPORTED = [
     "pmgpu_ensemble_create", "pmgpu_ensemble_destroy", "pmgpu_ensemble_run",
     "pmgpu_ensemble_set_splits", "pmgpu_ensemble_time_pairs", "pmgpu_ensemble_get_info",
     "pmgpu_ensemble_member", "pmgpu_debug_limit_list_rows", "pmgpu_system_set_step",
-    "pmgpu_force_full_add", "pmgpu_force_simplefull_switched_add",
+    "pmgpu_force_full_add", "pmgpu_force_simplefull_switched_add", "pmgpu_force_scpism_add",
+    "pmgpu_force_born_add",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -73,6 +74,10 @@ class Topology(C.Structure):
         ("water", C.c_void_p), ("gb_obc", C.c_double * 3),
         ("n_dihedrals", C.c_int), ("dihedral_atoms", C.c_void_p), ("dihedral_params", C.c_void_p),
         ("n_impropers", C.c_int), ("improper_atoms", C.c_void_p), ("improper_params", C.c_void_p),
+        ("scpism_sqrtalpha", C.c_void_p), ("scpism_alpha", C.c_void_p),
+        ("scpism_zeta", C.c_void_p), ("scpism_eta", C.c_void_p), ("scpism_c", C.c_void_p),
+        ("scpism_g", C.c_void_p), ("scpism_hbond", C.c_void_p),
+        ("scpism_residue", C.c_void_p), ("scpism_name", C.c_void_p),
     ]
 
 
@@ -128,6 +133,9 @@ def load() -> C.CDLL:
                                          C.POINTER(i32)]
     lib.pmgpu_force_simplefull_switched_add.argtypes = [vp, C.POINTER(Switch), C.POINTER(Switch),
                                                         C.POINTER(i32)]
+    lib.pmgpu_force_scpism_add.argtypes = [vp, C.POINTER(Switch), C.POINTER(Switch), dbl,
+                                           C.POINTER(i32)]
+    lib.pmgpu_force_born_add.argtypes = [vp, i32, dbl, i32, dbl, dbl, C.POINTER(i32)]
     lib.pmgpu_force_pme_add.argtypes = [vp, dbl, dbl, i32, vp, i32, i32, dbl, C.POINTER(i32)]
     lib.pmgpu_force_gb_add.argtypes = [vp, dbl, dbl, C.POINTER(i32)]
     lib.pmgpu_force_gbace_add.argtypes = [vp, dbl, dbl, C.POINTER(i32)]

@@ -265,7 +265,7 @@ static int system_free(System *s) {
                   s->d_gb_psi, s->d_gb_partial, s->d_gb_fixed, s->d_gb_ace, s->d_pos, s->d_vel,
                   s->d_force, s->d_acc, s->d_status, s->d_pairbuf, s->d_paircount,
                   s->d_stage, s->d_snap, s->d_step, s->d_sf_tile, s->d_gb_gst, s->d_gb_grad,
-                  s->d_rec,
+                  s->d_rec, s->d_scp, s->d_scp_i, s->d_born_q,
                   s->d_sf_bits};
   for (auto &g : s->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -523,6 +523,19 @@ int evaluate_forces(System *s, int only, int mode, int fold) {
           s->kernels += launched;
           break;
         }
+        case FK_SCPISM:
+          prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
+          r = nb_simplefull_sw(s, (f.terms.mask & TERM_LJ) ? &f.terms.lj_sw : nullptr,
+                               &f.terms.coul_sw, em, 1, f.scp_D);
+          prof_end(s);
+          s->kernels += 1;
+          break;
+        case FK_BORN:
+          prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
+          r = nb_born(s, f, em);
+          prof_end(s);
+          s->kernels += 2;
+          break;
         case FK_SIMPLEFULL_SW:
           prof_begin(s, PMGPU_PHASE_SIMPLEFULL);
           r = nb_simplefull_sw(s, (f.terms.mask & TERM_LJ) ? &f.terms.lj_sw : nullptr,
@@ -898,6 +911,23 @@ int pmgpu_system_create(pmgpu_context *ctx, const pmgpu_topology *t, int precisi
     for (int k = 0; k < 3; k++) s->gb_obc[k] = t->gb_obc[k];
   }
   if (t->water) PM_CHECK(upload(s.get(), &s->d_water, t->water, n));
+  if (t->scpism_alpha) {
+    const double *pd[6] = {t->scpism_sqrtalpha, t->scpism_alpha, t->scpism_zeta,
+                           t->scpism_eta, t->scpism_c, t->scpism_g};
+    const int *pi[3] = {t->scpism_hbond, t->scpism_residue, t->scpism_name};
+    for (const double *p : pd)
+      if (!p) return fail(PMGPU_ERR_ARG, "SCPISM data given in part");
+    for (const int *p : pi)
+      if (!p) return fail(PMGPU_ERR_ARG, "SCPISM data given in part");
+    std::vector<double> hd(6 * (size_t)nn);
+    std::vector<int> hi(3 * (size_t)nn);
+    for (int k = 0; k < 6; k++) std::copy(pd[k], pd[k] + n, hd.begin() + (size_t)k * nn);
+    for (int k = 0; k < 3; k++) std::copy(pi[k], pi[k] + n, hi.begin() + (size_t)k * nn);
+    PM_CHECK(upload(s.get(), &s->d_scp, hd.data(), hd.size()));
+    PM_CHECK(upload(s.get(), &s->d_scp_i, hi.data(), hi.size()));
+    PM_CHECK(upload(s.get(), &s->d_born_q, (const double *)nullptr, 2 * (size_t)nn));
+    PM_CUDA(cudaStreamSynchronize(s->stream));  // the packed host arrays end here
+  }
   PM_CHECK(upload(s.get(), &s->d_pos, (const double *)nullptr, 3 * nn));
   PM_CHECK(upload(s.get(), &s->d_vel, (const double *)nullptr, 3 * nn));
   PM_CHECK(upload(s.get(), &s->d_force, (const long long *)nullptr, 3 * nn));
@@ -1206,6 +1236,63 @@ int pmgpu_force_simplefull_switched_add(pmgpu_system *h, const pmgpu_switch *lj_
   f.terms.lj_sw.modify = modify;
   f.terms.coul_sw.modify = modify;
   f.terms.coulomb_scaling = s->coulomb_scaling;
+  return add_force(s, f, force_id);
+}
+
+int pmgpu_force_scpism_add(pmgpu_system *h, const pmgpu_switch *lj_sw,
+                           const pmgpu_switch *coul_sw, double dielectric, int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CHECK(run_finish(s));
+  PM_CUDA(cudaSetDevice(s->device));
+  if (!s->d_scp) return fail(PMGPU_ERR_ARG, "CoulombSCPISM requires SCPISM parameters");
+  if (!coul_sw) return fail(PMGPU_ERR_ARG, "CoulombSCPISM needs its switching function");
+  if (!(dielectric >= 0)) return fail(PMGPU_ERR_ARG, "-D must be >= 0");
+  for (const pmgpu_switch *w : {lj_sw, coul_sw}) {
+    if (!w) continue;
+    if (w->kind & PMGPU_SW_COMPLEMENT)
+      return fail(PMGPU_ERR_ARG, "CoulombSCPISM takes C1, C2, Cn or CmpCnCn switching");
+    if (w->kind != PMGPU_SW_UNIVERSAL) PM_CHECK(validate_switch(w, "SCPISM switch"));
+  }
+  Force f;
+  f.kind = FK_SCPISM;
+  // OneAtomPairTwo switches both terms when either switch modifies
+  // (OneAtomPairTwo.h:66-76); one term by its own MODIFY
+  int modify = 0;
+  if (lj_sw) {
+    switch_setup(lj_sw, &f.terms.lj_sw);
+    f.terms.mask |= TERM_LJ;
+    modify |= f.terms.lj_sw.modify;
+  }
+  switch_setup(coul_sw, &f.terms.coul_sw);
+  f.terms.mask |= TERM_COUL;
+  modify |= f.terms.coul_sw.modify;
+  f.terms.lj_sw.modify = modify;
+  f.terms.coul_sw.modify = modify;
+  f.terms.coulomb_scaling = s->coulomb_scaling;
+  f.scp_D = dielectric;
+  return add_force(s, f, force_id);
+}
+
+int pmgpu_force_born_add(pmgpu_system *h, int radii_bornswitch, double radii_cutoff,
+                         int self_bornswitch, double self_cutoff, double dielectric,
+                         int *force_id) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  System *s = sysp(h);
+  PM_CHECK(run_finish(s));
+  PM_CUDA(cudaSetDevice(s->device));
+  if (!s->d_scp) return fail(PMGPU_ERR_ARG, "BornRadii / BornSelf require SCPISM parameters");
+  if (radii_bornswitch < 0 || self_bornswitch < 0)
+    return fail(PMGPU_ERR_ARG, "-bornswitch must be >= 0");
+  if (!(radii_cutoff > 0) || !(self_cutoff > 0)) return fail(PMGPU_ERR_ARG, "cutoff must be > 0");
+  if (!(dielectric >= 0)) return fail(PMGPU_ERR_ARG, "-D must be >= 0");
+  Force f;
+  f.kind = FK_BORN;
+  f.born_rsw = radii_bornswitch;
+  f.born_ssw = self_bornswitch;
+  f.born_rcut = radii_cutoff;
+  f.born_scut = self_cutoff;
+  f.scp_D = dielectric;
   return add_force(s, f, force_id);
 }
 

@@ -1871,7 +1871,29 @@ struct SfSwArgs {
   double rough2;  // the larger rough-test cutoff^2
   long long *force, *acc;
   int em;  // 0 forces, 1 + energies, 2 + virial
+  // the Coulomb term as CoulombSCPISM (scpism 1): bulk dielectric, each
+  // atom's sqrt(alpha) and water flag (null: no water)
+  int scpism;
+  double D;
+  const double *sqrtalpha;
+  const int *water;
 };
+
+// CoulombSCPISMForce::operator() (force/coulomb/CoulombSCPISMForce.h:33-71)
+// for the pair (i, j) at 1/r^2 = rr2: the Coulomb energy over the
+// distance-dependent dielectric and its force over r.
+__device__ __forceinline__ void scpism_pair(double qq, double sai, double saj, double D,
+                                            double rr2, double &e, double &f) {
+  const double rDist = sqrt(rr2);
+  const double Dist = 1.0 / rDist;
+  const double alpha_ij = sai * saj;
+  const double Dp1 = D + 1.0, rDp1 = 1.0 / Dp1, k = (D - 1.0) * 0.5;
+  const double DiElec = Dp1 / (1.0 + k * exp(-alpha_ij * Dist)) - 1.0;
+  const double rDiElec = 1.0 / DiElec;
+  e = qq * rDist * rDiElec;
+  const double drDiElec = alpha_ij * rDp1 * (1.0 + DiElec) * (D - DiElec);
+  f = (rDiElec * drDiElec + rDist) * e * rDist;
+}
 
 __global__ void __launch_bounds__(kSfTile) k_simplefull_sw(SfSwArgs a) {
   __shared__ double sx[kSfTile], sy[kSfTile], sz[kSfTile], sq[kSfTile];
@@ -1931,9 +1953,22 @@ __global__ void __launch_bounds__(kSfTile) k_simplefull_sw(SfSwArgs a) {
           f += ff;
         }
         if (a.coul) {
-          double e = qi * sq[k] * sqrt(rr2);
-          if (excl == PMGPU_EXCL_MODIFIED) e *= a.csf;
-          double ff = e * rr2;
+          double e, ff;
+          if (a.scpism) {
+            if (a.water && (a.water[i] || a.water[jj])) {
+              e = ff = 0.0;  // no contribution from water (CoulombSCPISMForce.h:38-40)
+            } else {
+              scpism_pair(qi * sq[k], a.sqrtalpha[i], a.sqrtalpha[jj], a.D, rr2, e, ff);
+              if (excl == PMGPU_EXCL_MODIFIED) {
+                e *= a.csf;
+                ff *= a.csf;
+              }
+            }
+          } else {
+            e = qi * sq[k] * sqrt(rr2);
+            if (excl == PMGPU_EXCL_MODIFIED) e *= a.csf;
+            ff = e * rr2;
+          }
           if (a.modify) {
             double sv, sd;
             switch_eval<double>(a.coul_sw, r2, sv, sd);
@@ -2217,7 +2252,7 @@ void halfpairs_grid(int n, int split, int *tiles, long long *items, int *blocks)
 // The switched all-pairs form (k_simplefull_sw); lj_sw / coul_sw NULL for
 // an absent term.  em as nb_simplefull.
 int nb_simplefull_sw(System *s, const SwitchParams *lj_sw, const SwitchParams *coul_sw,
-                     int em) {
+                     int em, int scpism, double dielectric) {
   const int n = s->n;
   if (n == 0 || !(lj_sw || coul_sw)) return PMGPU_OK;
   const int iblocks = (n + kSfTile - 1) / kSfTile;
@@ -2249,7 +2284,208 @@ int nb_simplefull_sw(System *s, const SwitchParams *lj_sw, const SwitchParams *c
   a.force = s->d_force;
   a.acc = s->d_acc;
   a.em = em;
+  a.scpism = scpism;
+  a.D = dielectric;
+  a.sqrtalpha = s->d_scp;  // plane 0 of the SCPISM data
+  a.water = s->d_water;
   k_simplefull_sw<<<dim3(iblocks, chunks), kSfTile, 0, s->stream>>>(a);
+  PM_CUDA(cudaGetLastError());
+  return PMGPU_OK;
+}
+
+// ------------------------------------------------ SCPISM Born radii/self
+// BornRadii and BornSelf (force/born/BornRadii.h:33-77, force/born/
+// BornSelfForce.h:31-118) as two all-pairs passes in FP64, one thread per
+// atom visiting every other atom: the first forms each atom's Born radius
+// and from it the atom's BornSelf factor and self energy, the second the
+// pair forces (each atom keeps its own; energies and virial halved where a
+// pair is seen twice).  Pairs are those the reference's OneAtomPair with
+// the Cutoff switch evaluates: within the force's cutoff and not fully
+// excluded (the exclusion table only for atoms of one molecule).
+struct BornArgs {
+  int n;
+  const double *pos, *charge;
+  const int *mol, *water;
+  const double *scp;   // [6][n] sqrt(alpha), alpha, zeta, eta, C_i, g_i
+  const int *scp_i;    // [3][n] H-bond class, residue, name class
+  const int2 *ex_range;
+  const int *ex_start, *ex_partner, *ex_class;
+  Box box;
+  int rsw, ssw;
+  double rcut2, scut2, D;
+  double *born_q;      // [2][n] BornSelf factor, self energy
+  long long *force, *acc;
+  int em;
+};
+
+// BornSwitch::switchValue / switchDerivative (force/born/BornSwitch.h:33-68).
+__device__ __forceinline__ double born_switch(int sw, double r) {
+  if (r >= 5.0) return 0.0;
+  if (sw == 3) {
+    const double f = 1 - .0016 * r * r * r * r;
+    return f * f * f * f;
+  }
+  if (sw == 1) {
+    const double f = 1 - .04 * r * r;
+    return f * f;
+  }
+  if (sw == 2) {
+    const double f = 1 - 0.008 * r * r * r;
+    return f * f * f;
+  }
+  return 1.0;
+}
+__device__ __forceinline__ double born_switch_d(int sw, double r) {
+  if (r >= 5.0) return 0.0;
+  if (sw == 3) {
+    const double f = 1 - .0016 * r * r * r * r;
+    return -16 * .0016 * r * r * r * f * f * f;
+  }
+  if (sw == 1) return -0.16 * (1 - 0.04 * r * r) * r;
+  if (sw == 2) return -9 * .008 * r * r * (1 - .008 * r * r * r) * (1 - .008 * r * r * r);
+  return 0.0;
+}
+
+// The polar-hydrogen factor g_p' g_q of atom p against atom q: p a polar
+// H, q an acceptor in another residue; g_p' = -0.378 for an HN against an
+// O (BornRadii.h:45-58).
+__device__ __forceinline__ bool born_polar(const BornArgs &a, int p, int q, double &gg) {
+  const int n = a.n;
+  if (!(a.scp_i[p] == 1 && a.scp_i[q] == 2 && a.scp_i[n + p] != a.scp_i[n + q])) return false;
+  const double gp = (a.scp_i[2 * n + p] == 1 && a.scp_i[2 * n + q] == 2) ? -0.378
+                                                                           : a.scp[5 * n + p];
+  gg = gp * a.scp[5 * n + q];
+  return true;
+}
+
+__device__ __forceinline__ int born_excl(const BornArgs &a, int i, int j, int2 er) {
+  if (a.mol[i] != a.mol[j] || j < er.x || j > er.y) return PMGPU_EXCL_NONE;
+  return excl_class_of(a.ex_start, a.ex_partner, a.ex_class, i, j);
+}
+
+constexpr int kBornThreads = 128;
+constexpr double kBornPolarE = 0.80;  // the polar H+ exponent (BornRadii.h:51)
+
+__global__ void __launch_bounds__(kBornThreads) k_born_radii(BornArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const int n = a.n;
+  const double xi = a.pos[3 * i], yi = a.pos[3 * i + 1], zi = a.pos[3 * i + 2];
+  const double eta = a.scp[3 * n + i], C = a.scp[4 * n + i];
+  const int2 er = a.ex_range[i];
+  const bool wi = a.water && a.water[i];
+  double R = a.scp[2 * n + i];  // preForce: the radius starts at zeta
+  for (int j = 0; j < n; j++) {
+    if (j == i) continue;
+    double dx, dy, dz;
+    const double r2 = box_mindiff(a.box, xi, yi, zi, a.pos[3 * j], a.pos[3 * j + 1],
+                                  a.pos[3 * j + 2], dx, dy, dz);
+    if (r2 > a.rcut2) continue;
+    if (born_excl(a, i, j, er) == PMGPU_EXCL_FULL) continue;
+    if (wi || (a.water && a.water[j])) continue;
+    const double dist = sqrt(r2);
+    const double f = born_switch(a.rsw, dist);
+    R += eta * f * exp(-C * dist);
+    double gg;
+    if (born_polar(a, i, j, gg)) R += gg * f * exp(-kBornPolarE * dist);
+  }
+  // BornSelfForce.h:76-88: the solvation factor, its derivative, the
+  // atom's force factor and self energy
+  const double D = a.D, K = (D - 1.0) / 2, alpha = a.scp[n + i], q = a.charge[i];
+  const double Ds = (1.0 + D) / (1 + K * exp(-alpha * R)) - 1.0;
+  const double rDs = 1.0 / Ds, rR = 1.0 / R;
+  const double dDs = alpha * (1.0 / (1.0 + D)) * (1 + Ds) * (D - Ds);
+  a.born_q[i] = -0.5 * q * q * rR * rR * (1.0 - rDs - R * rDs * rDs * dDs);
+  a.born_q[n + i] = 0.5 * q * q * rR * (rDs - 1);
+}
+
+__global__ void __launch_bounds__(kBornThreads) k_born_self(BornArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < a.n;
+  const int n = a.n;
+  double fx = 0, fy = 0, fz = 0, e = 0;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  if (valid) {
+    const double xi = a.pos[3 * i], yi = a.pos[3 * i + 1], zi = a.pos[3 * i + 2];
+    const double eta = a.scp[3 * n + i], C = a.scp[4 * n + i], Qi = a.born_q[i];
+    const int2 er = a.ex_range[i];
+    bool used = false;
+    for (int j = 0; j < n; j++) {
+      if (j == i) continue;
+      double dx, dy, dz;
+      const double r2 = box_mindiff(a.box, xi, yi, zi, a.pos[3 * j], a.pos[3 * j + 1],
+                                    a.pos[3 * j + 2], dx, dy, dz);
+      if (r2 > a.scut2) continue;
+      if (born_excl(a, i, j, er) == PMGPU_EXCL_FULL) continue;
+      const double dist = sqrt(r2), rDist = 1.0 / dist;
+      const double f = born_switch(a.ssw, dist), fp = born_switch_d(a.ssw, dist);
+      double gg;
+      double dRij = eta * (fp - f * C) * exp(-C * dist);
+      if (born_polar(a, i, j, gg)) dRij += gg * (fp - f * kBornPolarE) * exp(-kBornPolarE * dist);
+      const double etaj = a.scp[3 * n + j], Cj = a.scp[4 * n + j];
+      double dRji = etaj * (fp - f * Cj) * exp(-Cj * dist);
+      if (born_polar(a, j, i, gg)) dRji += gg * (fp - f * kBornPolarE) * exp(-kBornPolarE * dist);
+      const double force = (Qi * dRij + a.born_q[j] * dRji) * rDist;
+      // fij = d force on the pair, F_i -= fij (d = x_j - x_i)
+      fx -= dx * force;
+      fy -= dy * force;
+      fz -= dz * force;
+      used = true;
+      if (a.em == 2) {
+        const double hf = 0.5 * force;
+        v[0] += dx * dx * hf; v[1] += dx * dy * hf; v[2] += dx * dz * hf;
+        v[3] += dy * dy * hf; v[4] += dy * dz * hf; v[5] += dz * dz * hf;
+      }
+    }
+    // the self energy of every atom that took part in a pair
+    // (BornSelfForce.h:108-117, postProcess :128-135)
+    if (used) e = a.born_q[n + i];
+    red_add(&a.force[i], to_fixed(fx, kForceScale));
+    red_add(&a.force[n + i], to_fixed(fy, kForceScale));
+    red_add(&a.force[2 * n + i], to_fixed(fz, kForceScale));
+  }
+  if (!a.em) return;
+  e = warp_sum(e);
+  if (a.em == 2)
+    for (int q = 0; q < 6; q++) v[q] = warp_sum(v[q]);
+  if ((threadIdx.x & 31) == 0) {
+    red_add(&a.acc[ACC_COULOMB], to_fixed(e, kEnergyScale));
+    if (a.em == 2) {
+      const int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+      for (int q = 0; q < 9; q++)
+        red_add(&a.acc[ACC_VIRIAL + q], to_fixed(v[map[q]], kEnergyScale));
+    }
+  }
+}
+
+int nb_born(System *s, const Force &f, int em) {
+  const int n = s->n;
+  if (n == 0) return PMGPU_OK;
+  BornArgs a;
+  a.n = n;
+  a.pos = s->d_pos;
+  a.charge = s->d_charge;
+  a.mol = s->d_mol;
+  a.water = s->d_water;
+  a.scp = s->d_scp;
+  a.scp_i = s->d_scp_i;
+  a.ex_range = s->d_excl_range;
+  a.ex_start = s->d_excl_start;
+  a.ex_partner = s->d_excl_partner;
+  a.ex_class = s->d_excl_class;
+  a.box = s->box;
+  a.rsw = f.born_rsw;
+  a.ssw = f.born_ssw;
+  a.rcut2 = f.born_rcut * f.born_rcut;
+  a.scut2 = f.born_scut * f.born_scut;
+  a.D = f.scp_D;
+  a.born_q = s->d_born_q;
+  a.force = s->d_force;
+  a.acc = s->d_acc;
+  a.em = em;
+  const int nb = (n + kBornThreads - 1) / kBornThreads;
+  k_born_radii<<<nb, kBornThreads, 0, s->stream>>>(a);
+  k_born_self<<<nb, kBornThreads, 0, s->stream>>>(a);
   PM_CUDA(cudaGetLastError());
   return PMGPU_OK;
 }

@@ -234,6 +234,10 @@ struct Force {
   size_t fft_work_bytes = 0;
   // simplefull
   int sf_lj = 0, sf_coul = 0;
+  // SCPISM: bulk dielectric (-D); Born radii and self-force switches/cutoffs
+  double scp_D = 80.0;
+  int born_rsw = 3, born_ssw = 3;
+  double born_rcut = 5.0, born_scut = 5.0;
   // gb
   double solute = 1.0, solvent = 80.0;
   // gbace (GBACEForce -solvationparam, -watersphereradius)
@@ -246,7 +250,9 @@ struct Force {
 
 enum { FK_CUTOFF = 1, FK_PME = 2, FK_GB = 3, FK_BONDED = 4,
        FK_SIMPLEFULL = 5, FK_TORSION = 6, FK_GBACE = 7,
-       FK_SIMPLEFULL_SW = 8 /* switched all pairs: terms.mask, lj_sw, coul_sw */ };
+       FK_SIMPLEFULL_SW = 8 /* switched all pairs: terms.mask, lj_sw, coul_sw */,
+       FK_SCPISM = 9 /* LJ + CoulombSCPISM all pairs within the switch cutoffs */,
+       FK_BORN = 10 /* SCPISM BornRadii + BornSelf */ };
 
 // Per-phase CUDA-event timing; events are recorded only when enabled and
 // summed at the next host synchronisation.
@@ -304,6 +310,12 @@ struct System {
   // GB
   double *d_gb_vdwr = nullptr, *d_gb_scale = nullptr, *d_gb_offset = nullptr;
   int *d_water = nullptr;
+  // SCPISM (pmgpu_topology scpism_*): [6][n] sqrt(alpha), alpha, zeta, eta,
+  // C_i, g_i and [3][n] H-bond class, residue, name class; the BornSelf
+  // factor and self energy of each atom [2][n] (per evaluation)
+  double *d_scp = nullptr;
+  int *d_scp_i = nullptr;
+  double *d_born_q = nullptr;
   double gb_obc[3] = {1.0, 0.8, 4.85};
   double *d_gb_born = nullptr, *d_gb_psi = nullptr, *d_gb_partial = nullptr;
   long long *d_gb_fixed = nullptr;  // 2n: burial and partial-sum accumulators
@@ -504,7 +516,8 @@ int fold_pending_slots(System *s);
 int nb_debug_cells(System *s, double cellsize, int *cell_xyz, int *dims);
 int nb_simplefull(System *s, int lj, int coul, int em);
 int nb_simplefull_sw(System *s, const SwitchParams *lj_sw, const SwitchParams *coul_sw,
-                     int em);
+                     int em, int scpism = 0, double dielectric = 80.0);
+int nb_born(System *s, const Force &f, int em);
 // the exclusion tile masks of the FP32 simple-full pass (once per system)
 int nb_simplefull_init(System *s);
 // Launch shape of the FP32 half all-pairs passes (each unordered pair once,

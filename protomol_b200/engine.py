@@ -149,6 +149,12 @@ class GpuSystem:
                 t.gb_obc[i] = float(topo.gb_obc[i])
         if getattr(topo, "water", None) is not None:
             t.water = arr("water", topo.water, np.int32)
+        scp = getattr(topo, "scpism", None)
+        if scp is not None:
+            for key in ("sqrtalpha", "alpha", "zeta", "eta", "c", "g"):
+                setattr(t, "scpism_" + key, arr("scp_" + key, scp["scp_" + key], np.float64))
+            for key in ("hbond", "residue", "name"):
+                setattr(t, "scpism_" + key, arr("scp_" + key, scp["scp_" + key], np.int32))
         h = C.c_void_p()
         L.check(self.lib.pmgpu_system_create(ctx.h, C.byref(t), _PREC[precision], C.byref(h)))
         self.h = h
@@ -382,6 +388,37 @@ class NonbondedSimpleFullSwitchedForce(SystemForce):
         super().__init__(system, fid.value)
 
 
+class ScpismSystemForce(SystemForce):
+    """``[LennardJones] CoulombSCPISM -algorithm NonbondedCutoff|
+    NonbondedSimpleFull``: the SCPISM screened Coulomb term
+    (force/coulomb/CoulombSCPISMForce.h) over every pair within the switch
+    cutoffs, FP64."""
+    keyword = "CoulombSCPISM"
+
+    def __init__(self, system: GpuSystem, lj: L.Switch | None, coulomb: L.Switch,
+                 dielectric: float = 80.0):
+        fid = C.c_int()
+        L.check(system.lib.pmgpu_force_scpism_add(
+            system.h, C.byref(lj) if lj else None, C.byref(coulomb), float(dielectric),
+            C.byref(fid)))
+        super().__init__(system, fid.value)
+
+
+class BornSystemForce(SystemForce):
+    """``BornRadii`` + ``BornSelf`` (force/born/BornRadii.h,
+    BornSelfForce.h): the SCPISM Born radii and self force, evaluated as one
+    term (the radii pass, then the self pass)."""
+    keyword = "BornSelf"
+
+    def __init__(self, system: GpuSystem, radii_switch: int = 3, radii_cutoff: float = 5.0,
+                 self_switch: int = 3, self_cutoff: float = 5.0, dielectric: float = 80.0):
+        fid = C.c_int()
+        L.check(system.lib.pmgpu_force_born_add(system.h, int(radii_switch), float(radii_cutoff),
+                                                int(self_switch), float(self_cutoff),
+                                                float(dielectric), C.byref(fid)))
+        super().__init__(system, fid.value)
+
+
 class NonbondedSimpleFullSystemForce(SystemForce):
     """``LennardJones|Coulomb -algorithm NonbondedSimpleFull`` (vacuum all pairs
     with exclusions)."""
@@ -479,6 +516,7 @@ class ForceFactory:
     def __init__(self, system: GpuSystem, cellsize: float = 0.0):
         self.system = system
         self.cellsize = cellsize
+        self._born_radii = (3, 5.0)  # the last BornRadii line's -bornswitch, -cutoff
 
     @staticmethod
     def parse(line: str):
@@ -523,7 +561,8 @@ class ForceFactory:
             return BondedSystemForce(s, "bond" in names, "angle" in names)
         if names and all(n in ("dihedral", "improper") for n in names):
             return TorsionSystemForce(s, "dihedral" in names, "improper" in names)
-        def term_switches():
+
+        def term_switches(coulomb="coulomb"):
             sws = []
             for k, name in enumerate(names):
                 sw = switches[k] if k < len(switches) else switches[-1]
@@ -531,9 +570,24 @@ class ForceFactory:
                                           sw.get("switchon", 0.0), sw.get("switchoff", 0.0),
                                           sw.get("n", 0.0))))
             lj = next((w for n, w in sws if n == "lennardjones"), None)
-            co = next((w for n, w in sws if n == "coulomb"), None)
+            co = next((w for n, w in sws if n == coulomb), None)
             return sws, lj, co
 
+        if names and names[0] in ("bornradii", "bornself"):
+            bsw = int(p.get("bornswitch", 3))
+            cut = switches[0].get("cutoff", p.get("cutoff", 5.0)) if switches else \
+                p.get("cutoff", 5.0)
+            if names[0] == "bornradii":
+                # its pass runs inside the BornSelf term, which must follow it
+                self._born_radii = (bsw, cut)
+                return _NoOpForce(s, "BornRadii")
+            return BornSystemForce(s, self._born_radii[0], self._born_radii[1], bsw, cut,
+                                   p.get("d", 80.0))
+        if "coulombscpism" in names and algn in ("nonbondedcutoff", "nonbondedsimplefull"):
+            if not switches:
+                raise ValueError(f"CoulombSCPISM needs -switchingFunction: {line}")
+            _, lj, co = term_switches(coulomb="coulombscpism")
+            return ScpismSystemForce(s, lj, co, p.get("d", 80.0))
         if algn in ("nonbondedcutoff", "nonbondedfull"):
             if not switches:
                 raise ValueError(f"{alg} needs -switchingFunction")

@@ -167,8 +167,39 @@ pmgpu_system *systemFor(const GenericTopology *topo) {
       }
     }
   }
+  // SCPISM data as the topology builder formed it (BuildTopology.cpp:757-818)
+  vector<double> scp[6];
+  vector<int> scpi[3];
+  if (topo->doSCPISM) {
+    for (int k = 0; k < 6; k++) scp[k].resize(n);
+    for (int k = 0; k < 3; k++) scpi[k].resize(n);
+    for (int i = 0; i < n; i++) {
+      const Atom &at = topo->atoms[i];
+      const SCPISMAtomTypeParameters *tp = topo->atomTypes[at.type].mySCPISM_T;
+      scp[0][i] = at.mySCPISM_A->sqrtalphaSCPISM;
+      scp[1][i] = tp->alpha;
+      scp[2][i] = at.mySCPISM_A->zeta;
+      scp[3][i] = at.mySCPISM_A->eta;
+      scp[4][i] = tp->C_i;
+      scp[5][i] = tp->g_i;
+      scpi[0][i] = (int)tp->isHbonded;
+      scpi[1][i] = at.residue_seq;
+      scpi[2][i] = at.name == "HN" ? 1 : (at.name == "O" ? 2 : 0);
+    }
+  }
   pmgpu_topology t;
   memset(&t, 0, sizeof(t));
+  if (topo->doSCPISM && n) {
+    t.scpism_sqrtalpha = &scp[0][0];
+    t.scpism_alpha = &scp[1][0];
+    t.scpism_zeta = &scp[2][0];
+    t.scpism_eta = &scp[3][0];
+    t.scpism_c = &scp[4][0];
+    t.scpism_g = &scp[5][0];
+    t.scpism_hbond = &scpi[0][0];
+    t.scpism_residue = &scpi[1][0];
+    t.scpism_name = &scpi[2][0];
+  }
   t.n_atoms = n;
   t.charge = n ? &q[0] : 0;
   t.mass = n ? &m[0] : 0;
@@ -569,6 +600,118 @@ class GbGpuForce : public PmgpuSystemForce {
   int myBlock;
 };
 
+// LennardJones and/or CoulombSCPISM (force/coulomb/CoulombSCPISMForce.h)
+// on NonbondedCutoff or NonbondedSimpleFull (module/NonbondedCutoffForce
+// Module.cpp:91-107, :150-160; NonbondedSimpleFullForceModule.cpp:104-116)
+// on the GPU: the parameters in the reference's order, each force's own
+// (-D for CoulombSCPISM) before its switch's, then the algorithm's.
+class ScpismGpuForce : public PmgpuSystemForce {
+ public:
+  ScpismGpuForce(bool simpleFull, const SwitchSpec *lj, const SwitchSpec &coul)
+      : myFull(simpleFull), myTwo(lj != 0), mySwA(lj ? *lj : coul), mySwB(coul), myD(80.0),
+        myCutoff(8.0), myBlock(64) {
+    memset(&myA, 0, sizeof(myA));
+    memset(&myB, 0, sizeof(myB));
+  }
+  virtual string getKeyword() const {
+    return myFull ? "NonbondedSimpleFullGPU" : "NonbondedCutoffGPU";
+  }
+  virtual string getIdNoAlias() const {
+    string id = myTwo ? "LennardJones CoulombSCPISM" : "CoulombSCPISM";
+    if (myTwo) id += string(" -switchingFunction ") + mySwA.name;
+    id += string(" -switchingFunction ") + mySwB.name;
+    return id + " -algorithm " + getKeyword();
+  }
+  virtual void getParameters(vector<Parameter> &p) const {
+    if (myTwo) switchParameters(mySwA, myA, p);
+    p.push_back(Parameter("-D", Value(myD, ConstraintValueType::NotNegative()), 80.0));
+    switchParameters(mySwB, myB, p);
+    if (myFull)
+      p.push_back(Parameter("-blocksize", Value(myBlock, ConstraintValueType::Positive()), 64));
+    else
+      p.push_back(Parameter("-cutoff", Value(myCutoff, ConstraintValueType::Positive())));
+  }
+
+ private:
+  virtual Force *doMake(const vector<Value> &values) const {
+    ScpismGpuForce *f = new ScpismGpuForce(myFull, myTwo ? &mySwA : 0, mySwB);
+    size_t at = 0;
+    if (myTwo) f->myA = switchMake(mySwA, values, &at);
+    values[at++].get(f->myD);
+    f->myB = switchMake(mySwB, values, &at);
+    if (myFull)
+      values[at].get(f->myBlock);
+    else
+      values[at].get(f->myCutoff);
+    return f;
+  }
+  virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
+    int id = -1;
+    check(pmgpu_force_scpism_add(s, myTwo ? &myA : 0, &myB, myD, &id), getIdNoAlias());
+    return id;
+  }
+  bool myFull, myTwo;
+  SwitchSpec mySwA, mySwB;
+  pmgpu_switch myA, myB;
+  Real myD, myCutoff;
+  int myBlock;
+};
+
+// BornRadii and BornSelf (force/born/BornRadii.h, BornSelfForce.h) with
+// the Cutoff switch on NonbondedCutoff.  The device runs both passes in
+// BornSelf's evaluation: BornRadii only records its -bornswitch and cutoff
+// for the BornSelf line that follows it (it adds no force or energy in the
+// reference either).
+map<pmgpu_system *, pair<int, Real> > &bornRadiiSettings() {
+  static map<pmgpu_system *, pair<int, Real> > m;
+  return m;
+}
+
+class BornGpuForce : public PmgpuSystemForce {
+ public:
+  explicit BornGpuForce(bool self)
+      : mySelf(self), mySwitch(3), myD(80.0), mySwCutoff(5.0), myCutoff(5.0) {}
+  virtual string getKeyword() const { return "NonbondedCutoffGPU"; }
+  virtual string getIdNoAlias() const {
+    return string(mySelf ? "BornSelf" : "BornRadii") +
+           " -switchingFunction Cutoff -algorithm NonbondedCutoffGPU";
+  }
+  virtual void getParameters(vector<Parameter> &p) const {
+    // BornRadii.cpp:9-13, BornSelfForce.cpp:8-16, then the Cutoff switch
+    // and the algorithm's cutoff
+    p.push_back(Parameter("-bornswitch", Value(mySwitch, ConstraintValueType::NotNegative()), 3));
+    if (mySelf) p.push_back(Parameter("-D", Value(myD, ConstraintValueType::NotNegative()), 80.0));
+    p.push_back(Parameter("-cutoff", Value(mySwCutoff, ConstraintValueType::Positive())));
+    p.push_back(Parameter("-cutoff", Value(myCutoff, ConstraintValueType::Positive())));
+  }
+
+ private:
+  virtual Force *doMake(const vector<Value> &values) const {
+    BornGpuForce *f = new BornGpuForce(mySelf);
+    size_t at = 0;
+    values[at++].get(f->mySwitch);
+    if (mySelf) values[at++].get(f->myD);
+    values[at++].get(f->mySwCutoff);
+    values[at].get(f->myCutoff);
+    return f;
+  }
+  virtual int addTo(pmgpu_system *s, const GenericTopology *) const {
+    if (!mySelf) {
+      bornRadiiSettings()[s] = make_pair(mySwitch, mySwCutoff);
+      return -1;
+    }
+    pair<int, Real> r(3, 5.0);
+    if (bornRadiiSettings().count(s)) r = bornRadiiSettings()[s];
+    int id = -1;
+    check(pmgpu_force_born_add(s, r.first, r.second, mySwitch, mySwCutoff, myD, &id),
+          getIdNoAlias());
+    return id;
+  }
+  bool mySelf;
+  int mySwitch;
+  Real myD, mySwCutoff, myCutoff;
+};
+
 // Dihedral / Improper torsions (force/bonded/DihedralSystemForce.h,
 // ImproperSystemForce.h; MTorsionSystemForce) on the GPU.
 class TorsionGpuForce : public PmgpuSystemForce {
@@ -754,6 +897,21 @@ void PmgpuForceModule::registerForces(ProtoMolApp *app) {
   f.registerExemplar(new GbGpuForce("GBACEForce"));
   f.registerExemplar(new TorsionGpuForce(true));
   f.registerExemplar(new TorsionGpuForce(false));
+  // SCPISM (module/NonbondedCutoffForceModule.cpp:91-160,
+  // NonbondedSimpleFullForceModule.cpp:104-116)
+  const SwitchSpec scp[] = {kC1, kC2, kCn, kCmpCnCn};
+  for (int k = 0; k < 4; k++) {
+    f.registerExemplar(new ScpismGpuForce(false, 0, scp[k]));
+    f.registerExemplar(new ScpismGpuForce(true, 0, scp[k]));
+  }
+  const SwitchSpec scp_pairs[][2] = {{kC2, kC1}, {kC2, kC2}, {kCn, kCn}, {kCmpCnCn, kC1},
+                                     {kCn, kC2}};
+  for (int k = 0; k < 5; k++) {
+    f.registerExemplar(new ScpismGpuForce(false, &scp_pairs[k][0], scp_pairs[k][1]));
+    f.registerExemplar(new ScpismGpuForce(true, &scp_pairs[k][0], scp_pairs[k][1]));
+  }
+  f.registerExemplar(new BornGpuForce(false));
+  f.registerExemplar(new BornGpuForce(true));
 }
 
 void PmgpuForceModule::init(ProtoMolApp *app) {

@@ -32,4 +32,4 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_without_device():
     lib = _lib.load()
-    assert lib.pmgpu_abi_version() == 1
+    assert lib.pmgpu_abi_version() == 2
