@@ -82,6 +82,7 @@ __device__ __forceinline__ void bin_body(const BinArgs &A, Blk b) {
   int *__restrict__ status = A.status;
   if (!*A.rebuild) return;
   const int i = b.x * blockDim.x + threadIdx.x;
+  const unsigned vmask = __ballot_sync(0xffffffffu, i < g.n);
   if (i >= g.n) return;
   const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
   double w[3];
@@ -100,7 +101,12 @@ __device__ __forceinline__ void bin_body(const BinArgs &A, Blk b) {
   // non-negative FP32 bits order like the values
   const float zf = finite ? (float)fmin(fmax(w[2] - g.lo[2], 0.0), 1.0e30) : 0.f;
   zkey[i] = __float_as_uint(zf);
-  atomicAdd(&col_count[col], 1);
+  // one atomic per column among the warp's atoms (neighbouring atoms of a
+  // molecule share columns)
+  {
+    const unsigned peers = __match_any_sync(vmask, col);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&col_count[col], __popc(peers));
+  }
   offset[3 * i] = x - w[0];
   offset[3 * i + 1] = y - w[1];
   offset[3 * i + 2] = z - w[2];
@@ -214,10 +220,19 @@ struct ScatterArgs {
 };
 __device__ __forceinline__ void scatter_body(const ScatterArgs &A, Blk b) {
   if (!*A.rebuild) return;
-  int i = b.x * blockDim.x + threadIdx.x;
-  if (i >= A.n) return;
+  const int i = b.x * blockDim.x + threadIdx.x;
+  const bool valid = i < A.n;
+  // one atomic per column among the warp's atoms (a column's atoms are
+  // sorted by (z, atom) afterwards, so their order here does not matter)
+  const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+  if (!valid) return;
   const int c = A.key[i];
-  A.unsorted[A.col_u[c] + atomicAdd(&A.cursor[c], 1)] = i;
+  const unsigned peers = __match_any_sync(vmask, c);
+  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&A.cursor[c], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  A.unsorted[A.col_u[c] + base + __popc(peers & ((1u << lane) - 1u))] = i;
 }
 __global__ void k_scatter(ScatterArgs a) {
   pdl_wait();  // the predecessor's writes are visible from here on
