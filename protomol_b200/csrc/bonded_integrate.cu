@@ -438,6 +438,13 @@ struct UpdateArgs {
   long long *fslot;
   const int *slot_of;
   int ns;
+  // the pair list's slot records of the drifted positions (xw null: none),
+  // written through the current slot order: the list's gather then only
+  // redoes them when the list is rebuilt
+  double4 *xw;
+  float4 *xhi, *xlo;
+  const double *offset;
+  int mixed;
   // the system's state
   const double *mass;
   double *pos, *vel;
@@ -528,6 +535,19 @@ __device__ __forceinline__ void update_body(const UpdateArgs &a, Blk blk) {
       if (!isfinite(x[c])) atomicOr(status, ST_NONFINITE);
     }
     if (a.rec) write_pair_record(a.rec, a.n, i, x[0], x[1], x[2], a.charge[i], a.type[i]);
+    if (a.xw && slot >= 0) {
+      // the wrapped position x - (x_build - x_wrapped at the build), as the
+      // gather forms it, and its FP32 hi/lo split
+      const double wx = x[0] - a.offset[3 * i], wy = x[1] - a.offset[3 * i + 1],
+                   wz = x[2] - a.offset[3 * i + 2];
+      const double q = a.charge[i];
+      a.xw[slot] = make_double4(wx, wy, wz, q);
+      const float hx = (float)wx, hy = (float)wy, hz = (float)wz;
+      a.xhi[slot] = make_float4(hx, hy, hz, (float)q);
+      if (a.mixed)
+        a.xlo[slot] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
+                                  (float)(wz - (double)hz), __int_as_float(a.type[i]));
+    }
   }
   if (slot >= 0)
     for (int c = 0; c < 3; c++) a.fslot[(size_t)c * a.ns + slot] = 0;
@@ -607,6 +627,10 @@ int update_args(System *s, const pmgpu_integrator *it, int phase, int zero_acc,
   a.fslot = nullptr;
   a.slot_of = nullptr;
   a.ns = 0;
+  a.xw = nullptr;
+  a.xhi = a.xlo = nullptr;
+  a.offset = nullptr;
+  a.mixed = s->precision == PMGPU_PREC_MIXED;
   if (list && list->built && s->n) {
     a.fslot = list->d_fslot;
     a.slot_of = list->d_slot_of;
@@ -619,7 +643,11 @@ int update_args(System *s, const pmgpu_integrator *it, int phase, int zero_acc,
     a.ticket = list->d_maxdisp;
     a.rebuild = list->d_rebuild;
     a.half_skin2 = hs * hs;
-    list->decided = 1;
+    a.xw = list->d_xw;
+    a.xhi = list->d_xhi;
+    a.xlo = list->d_xlo;
+    a.offset = list->d_offset;
+    list->decided = 1;  // the decision and the slot records of this step are taken
   }
   a.mass = s->d_mass;
   a.pos = s->d_pos;

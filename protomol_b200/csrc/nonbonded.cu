@@ -353,9 +353,11 @@ struct GatherArgs {
   int *mol_s;
   const int *rebuild;
   float4 *bb;
+  int updated;  // the update kernel of this step wrote the slots: gather on a rebuild only
 };
 template <bool MIXED>
 __device__ __forceinline__ void gather_slots_body(const GatherArgs &A, Blk b) {
+  if (A.updated && !*A.rebuild) return;
   const int ns = A.ns;
   const double *__restrict__ pos = A.pos;
   const double *__restrict__ offset = A.offset;
@@ -1020,7 +1022,7 @@ static void list_args(System *s, NeighborList *nl, ListArgs *L) {
                      nl->d_slot_of, nl->d_key_start, s->d_status};
   L->gather = GatherArgs{nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted, s->d_charge,
                          s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
-                         nl->d_rebuild, nl->d_bb};
+                         nl->d_rebuild, nl->d_bb, 0};
   TileBuildArgs ba;
   ba.nclusters = nl->nclusters;
   ba.periodic = s->box.periodic;
@@ -1056,7 +1058,9 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
   const int nb = (n + T - 1) / T, nbs = (nl->ns_max + T - 1) / T;
   const int first = !nl->built;
   const float hs = (float)(0.5 * nl->skin);
-  // an MD step's update kernel has taken the decision already
+  // an MD step's update kernel has taken the decision already, and written
+  // the slot records of the drifted positions
+  const int updated = nl->decided && !first && !force_rebuild;
   if (!nl->decided || first || force_rebuild)
     PM_CUDA(launch_pdl(k_check_rebuild, nb, kCheckThreads, 0, st, n, s->d_pos, nl->d_xbuild,
                        nl->d_maxdisp, nl->d_rebuild, hs * hs, (force_rebuild || first) ? 1 : 0));
@@ -1068,6 +1072,7 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
     // overlap their launches
     ListArgs la;
     list_args(s, nl, &la);
+    la.gather.updated = updated;
     PM_CUDA(launch_pdl(k_bin, nb, T, 0, q, la.bin));
     PM_CUDA(launch_pdl(k_scan_cols, 1, 1024, 0, q, la.scan));
     PM_CUDA(launch_pdl(k_scatter, nb, T, 0, q, la.scatter));
