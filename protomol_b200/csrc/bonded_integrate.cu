@@ -511,8 +511,12 @@ __device__ __forceinline__ void update_body(const UpdateArgs &a, Blk blk) {
   }
   // The grid-wide decisions come before this thread's stores, so the fences
   // they take wait for no stores of the update.
-  if (a.xbuild) rebuild_decide<kUpdateThreads>(d2, a.ticket, a.rebuild, a.half_skin2, 0, blk.n);
-  if (a.step_inc) {
+  // with a rebuild decision to take, the step counter advances on its
+  // ticket (one grid-wide ticket instead of two)
+  if (a.xbuild)
+    rebuild_decide<kUpdateThreads>(d2, a.ticket, a.rebuild, a.half_skin2, 0, blk.n,
+                                   a.step_inc ? a.step_ptr : nullptr);
+  if (a.step_inc && !a.xbuild) {
     // every block has read the counter before it counts itself done
     __shared__ bool last;
     __syncthreads();

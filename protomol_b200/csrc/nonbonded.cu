@@ -509,6 +509,7 @@ struct BuildArgs {
   uint2 *jlanes;
   int *jl_count;
   int *status;
+  int *work;  // [0] next row, [1] warps done (both back to zero at the end)
 };
 __device__ __forceinline__ void build_body(const BuildArgs &B, Blk blk) {
   const TileBuildArgs &a = B.a;
@@ -531,9 +532,16 @@ __device__ __forceinline__ void build_body(const BuildArgs &B, Blk blk) {
   __shared__ int4 st_o[kBuildWarps][32], st_m[kBuildWarps][32];
   __shared__ int st_h[kBuildWarps][32], st_c[kBuildWarps][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  // the warps of the (resident) grid stride over the rows
-  for (int rw = blk.x * kBuildWarps + wib; rw < a.nclusters * kRowParts;
-       rw += blk.n * kBuildWarps) {
+  // the warps of the (resident) grid take the rows one at a time from a
+  // counter, so the rows' unequal costs spread over the SMs; the output
+  // of a row does not depend on which warp builds it
+  int *const work = B.work;
+  auto next_row = [&]() {
+    int r = 0;
+    if (lane == 0) r = atomicAdd(&work[0], 1);
+    return __shfl_sync(kAll, r, 0);
+  };
+  for (int rw = next_row(); rw < a.nclusters * kRowParts; rw = next_row()) {
   const int ci = rw / kRowParts, part = rw - ci * kRowParts;
   const float4 l0 = bb[4 * ci], h0 = bb[4 * ci + 1], l1 = bb[4 * ci + 2], h1 = bb[4 * ci + 3];
   if (l0.w + l1.w == 0.f) {
@@ -845,6 +853,14 @@ __device__ __forceinline__ void build_body(const BuildArgs &B, Blk blk) {
   }
   __syncwarp();  // the next row reuses the staging
   }  // rows
+  // the last warp of the launch to finish sets the counters back to zero
+  if (lane == 0) {
+    __threadfence();
+    if (atomicAdd(&work[1], 1) == blk.n * kBuildWarps - 1) {
+      work[0] = 0;
+      work[1] = 0;
+    }
+  }
 }
 __global__ void __launch_bounds__(kBuildWarps * 32, 3) k_build_tiles(BuildArgs a) {
   pdl_wait();  // the predecessor's writes are visible from here on
@@ -961,6 +977,8 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   PM_CUDA(cudaMemsetAsync(nl->d_maxdisp, 0, 2 * sizeof(unsigned int), s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_rebuild, 3 * sizeof(int)));
   PM_CUDA(cudaMemsetAsync(nl->d_rebuild, 0, 3 * sizeof(int), s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_build_work, 2 * sizeof(int)));
+  PM_CUDA(cudaMemsetAsync(nl->d_build_work, 0, 2 * sizeof(int), s->stream));
   nl->built = 0;
   return PMGPU_OK;
 }
@@ -971,8 +989,9 @@ int nb_list_free(System *s, NeighborList *nl) {
                   nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
                   nl->d_bb, nl->d_fslot, nl->d_slot_of, nl->d_tiles, nl->d_tmod,
                   nl->d_jlanes, nl->d_jl_count, nl->d_tile_count, nl->d_maxdisp,
-                  nl->d_rebuild};
+                  nl->d_rebuild, nl->d_build_work};
   for (void *p : ptrs) dev_free(s, p);
+  nl->d_build_work = nullptr;
   nl->d_key = nl->d_unsorted = nl->d_col_count = nl->d_col_u = nl->d_col_cursor = nullptr;
   nl->d_col_base = nl->d_key_start = nl->d_sorted = nl->d_mol_s = nl->d_tile_count = nullptr;
   nl->d_zkey = nullptr;
@@ -1045,7 +1064,7 @@ static void list_args(System *s, NeighborList *nl, ListArgs *L) {
   ba.excl_class = s->d_excl_class;
   L->build = BuildArgs{ba, nl->d_rebuild, nl->d_sorted, nl->d_key_start, nl->d_xhi,
                        nl->d_mol_s, nl->d_bb, nl->d_tiles, nl->d_tmod, nl->d_tile_count,
-                       nl->d_jlanes, nl->d_jl_count, s->d_status};
+                       nl->d_jlanes, nl->d_jl_count, s->d_status, nl->d_build_work};
 }
 
 // Sort + (conditional) list build + per-step gather.  Never synchronises

@@ -359,7 +359,8 @@ __device__ __forceinline__ void red_add(long long *p, long long v) {
 // blocks of this system's launch.
 template <int THREADS>
 __device__ __forceinline__ void rebuild_decide(float d2, unsigned *ticket, int *rebuild,
-                                               float half_skin2, int force, int nblocks) {
+                                               float half_skin2, int force, int nblocks,
+                                               unsigned long long *step = nullptr) {
   __shared__ float wmax[THREADS / 32];
   __shared__ bool last;
   if (!(d2 == d2)) d2 = 3.0e38f;  // NaN: rebuild (the binning flags it)
@@ -382,6 +383,9 @@ __device__ __forceinline__ void rebuild_decide(float d2, unsigned *ticket, int *
     rebuild[0] = r;
     if (r) rebuild[1] += 1;
     ticket[0] = 0u;
+    // the caller's step counter, when it rides on this ticket (every block
+    // has read it before counting itself done)
+    if (step) step[0] += 1ull;
   }
 }
 

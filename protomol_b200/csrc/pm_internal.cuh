@@ -204,6 +204,7 @@ struct NeighborList {
   int *d_tile_count = nullptr;   // nrows
   unsigned int *d_maxdisp = nullptr;  // rebuild check: block ticket, max displacement^2 bits
   int *d_rebuild = nullptr;      // rebuild flag, build count, largest row need after an overflow
+  int *d_build_work = nullptr;   // the tile build's row counter and finished-warp count
 };
 
 struct System;
