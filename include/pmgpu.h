@@ -483,6 +483,12 @@ int pmgpu_debug_cell_assign(pmgpu_system *sys, double cellsize,
  * so results equal those of a list that never overflowed.  No counterpart
  * in the reference (its cell lists have no capacity). */
 int pmgpu_debug_set_list_capacity(pmgpu_system *sys, int tiles_per_row);
+/* Fixes the atoms a pair-list column bucket holds (rounded up to a
+ * multiple of 32, at most 4096) for the system's cutoff forces, for testing
+ * the growth path: a build that bins more atoms into one column flags the
+ * overflow internally, the buckets grow to the fullest column's count and
+ * the evaluation or MD segment is repeated from its start. */
+int pmgpu_debug_set_column_capacity(pmgpu_system *sys, int atoms_per_column);
 /* Limits the tiles a list row may hold in the next builds to tiles_per_row
  * without touching the current list, positions or forces: the first later
  * build (an MD step's rebuild) that needs more takes the growth path, which

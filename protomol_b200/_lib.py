@@ -45,7 +45,7 @@ EXPORTED = [
     "pmgpu_ensemble_set_splits", "pmgpu_ensemble_time_pairs", "pmgpu_ensemble_get_info",
     "pmgpu_ensemble_member", "pmgpu_debug_limit_list_rows", "pmgpu_system_set_step",
     "pmgpu_force_full_add", "pmgpu_force_simplefull_switched_add", "pmgpu_force_scpism_add",
-    "pmgpu_force_born_add",
+    "pmgpu_force_born_add", "pmgpu_debug_set_column_capacity",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -151,6 +151,7 @@ def load() -> C.CDLL:
     lib.pmgpu_debug_pair_set.argtypes = [vp, i32, vp, C.c_longlong, C.POINTER(C.c_longlong)]
     lib.pmgpu_debug_set_list_capacity.argtypes = [vp, i32]
     lib.pmgpu_debug_limit_list_rows.argtypes = [vp, i32]
+    lib.pmgpu_debug_set_column_capacity.argtypes = [vp, i32]
     lib.pmgpu_system_set_step.argtypes = [vp, C.c_longlong]
     lib.pmgpu_profile_enable.argtypes = [vp, i32]
     lib.pmgpu_profile_read.argtypes = [vp, vp, vp, i32]

@@ -569,8 +569,7 @@ int evaluate_forces(System *s, int only, int mode, int fold) {
       prof_begin(s, PMGPU_PHASE_LIST);
       int r = nb_prepare(s, &s->lists[f.list_index], 0);
       prof_end(s);
-      PM_CHECK(r);
-      s->kernels += 6;  // check, bin, scan, scatter, sort, gather
+      PM_CHECK(r);  // nb_prepare counts its launches
       prepared[f.list_index] = 1;
     }
   }
@@ -627,17 +626,21 @@ int take_results(System *s, int only, double *energies, double *virial, int add,
   if (st) {
     PM_CUDA(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
     if (st & ST_LIST_OVERFLOW) {
-      // Grow every list to at least its largest row's need (fresh build
-      // next time); this result is incomplete and no output is touched.
+      // Grow every list to at least its largest row's need, and its column
+      // buckets to the fullest column's count (fresh build next time); this
+      // result is incomplete and no output is touched.
       for (auto &nl : s->lists) {
-        int rb[3] = {0, 0, 0};
+        int rb[4] = {0, 0, 0, 0};
         PM_CUDA(cudaMemcpyAsync(rb, nl.d_rebuild, sizeof(rb), cudaMemcpyDeviceToHost, s->stream));
         PM_CUDA(cudaStreamSynchronize(s->stream));
         const int need = rb[2] + rb[2] / 4 + 32;
-        const int cap = (std::max(nl.cap * 2, need) + 31) & ~31;
+        // a column overflow alone leaves the tile capacity as it is
+        const int cap = rb[3] > 0 && rb[2] == 0 ? nl.cap : (std::max(nl.cap * 2, need) + 31) & ~31;
+        if (rb[3] > 0) nl.bcap = std::max(nl.bcap, rb[3] + rb[3] / 4 + 32);
         nb_list_free(s, &nl);
         nl.cap = cap;
         nl.cap_set = 0;
+        nl.bcap_set = 0;
         nl.limit = 0;
         PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
         s->graph_version++;  // captured graphs hold the old list buffers
@@ -1814,6 +1817,23 @@ int pmgpu_debug_set_list_capacity(pmgpu_system *h, int tiles_per_row) {
     nb_list_free(s, &nl);
     nl.cap = 0;
     nl.cap_set = tiles_per_row;
+    PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
+  }
+  s->graph_version++;
+  s->forces_valid = 0;
+  return PMGPU_OK;
+}
+
+int pmgpu_debug_set_column_capacity(pmgpu_system *h, int atoms_per_column) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null system");
+  if (atoms_per_column < 1) return fail(PMGPU_ERR_ARG, "atoms_per_column must be >= 1");
+  System *s = sysp(h);
+  PM_CHECK(run_finish(s));
+  PM_CUDA(cudaSetDevice(s->device));
+  for (auto &nl : s->lists) {
+    nb_list_free(s, &nl);
+    nl.bcap = 0;
+    nl.bcap_set = atoms_per_column;
     PM_CHECK(nb_list_init(s, &nl, nl.cutoff, nl.skin, 0));
   }
   s->graph_version++;

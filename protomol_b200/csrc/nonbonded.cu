@@ -61,69 +61,26 @@ struct ListGrid {
   double inv[3];   // 1 / column width (x, y), 1 / z-bin height
 };
 
+// Column layout of a rebuild, by one block once every atom is binned: the
+// padded column bases (every column a whole number of 8-atom clusters; a
+// column past its bucket counts as a full bucket, and the sort flags it) and
+// the slots past the padded total marked empty.
+struct ScanArgs {
+  int ncol, nkeys, ns_max, bcap;
+  int *col_base, *key_start, *sorted;
+};
+
 struct BinArgs {
   ListGrid g;
   const double *pos;
   const int *rebuild;
-  int *key;
   unsigned *zkey;
-  int *col_count;
+  int *col_count, *bucket;
   double *offset, *xbuild;
   int *status;
+  unsigned *ticket;  // binning blocks done: the last one lays out the columns
+  ScanArgs scan;
 };
-__device__ __forceinline__ void bin_body(const BinArgs &A, Blk b) {
-  const ListGrid &g = A.g;
-  const double *__restrict__ pos = A.pos;
-  int *__restrict__ key = A.key;
-  unsigned *__restrict__ zkey = A.zkey;
-  int *__restrict__ col_count = A.col_count;
-  double *__restrict__ offset = A.offset;
-  double *__restrict__ xbuild = A.xbuild;
-  int *__restrict__ status = A.status;
-  if (!*A.rebuild) return;
-  const int i = b.x * blockDim.x + threadIdx.x;
-  const unsigned vmask = __ballot_sync(0xffffffffu, i < g.n);
-  if (i >= g.n) return;
-  const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-  double w[3];
-  box_minpos(g.box, x, y, z, w[0], w[1], w[2]);
-  const int dims[2] = {g.ncx, g.ncy};
-  int c[2];
-  const bool finite = isfinite(x) && isfinite(y) && isfinite(z);
-  for (int a = 0; a < 2; a++) {
-    const double q = finite ? (w[a] - g.lo[a]) * g.inv[a] : 0.0;
-    int k = (int)floor(fmin(fmax(q, -1.0), (double)dims[a]));
-    c[a] = k < 0 ? 0 : (k >= dims[a] ? dims[a] - 1 : k);
-  }
-  if (!finite) atomicOr(status, ST_NONFINITE);
-  const int col = c[0] * g.ncy + c[1];
-  key[i] = col;
-  // non-negative FP32 bits order like the values
-  const float zf = finite ? (float)fmin(fmax(w[2] - g.lo[2], 0.0), 1.0e30) : 0.f;
-  zkey[i] = __float_as_uint(zf);
-  // one atomic per column among the warp's atoms (neighbouring atoms of a
-  // molecule share columns)
-  {
-    const unsigned peers = __match_any_sync(vmask, col);
-    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&col_count[col], __popc(peers));
-  }
-  offset[3 * i] = x - w[0];
-  offset[3 * i + 1] = y - w[1];
-  offset[3 * i + 2] = z - w[2];
-  xbuild[3 * i] = x;
-  xbuild[3 * i + 1] = y;
-  xbuild[3 * i + 2] = z;
-}
-__global__ void k_bin(BinArgs a) {
-  pdl_wait();  // the predecessor's writes are visible from here on
-  pdl_trigger();
-  bin_body(a, own_blk());
-}
-__global__ void k_bin_batch(const BinArgs *__restrict__ tab, const int *__restrict__ first,
-                            int nm) {
-  const int m = batch_member(first, nm, blockIdx.x);
-  bin_body(tab[m], batch_blk(first, m));
-}
 
 // Exclusive scan of value(k), k < count, by one block; write(k, prefix)
 // receives each prefix and the return value is the total.
@@ -163,129 +120,210 @@ __device__ int block_scan(int count, V value, W write, int *warp_tot, int *carry
   return *carry;
 }
 
-// One block: column starts (unpadded, for the scatter) and padded column
-// bases (every column a whole number of 8-atom clusters); slots past the
-// padded total are marked empty.
-struct ScanArgs {
-  const int *rebuild;
-  const int *col_count;
-  int ncol;
-  int *col_u, *cursor, *col_base, *key_start;
-  int nkeys;
-  int *sorted;
-  int ns_max;
-};
-__device__ __forceinline__ void scan_body(const ScanArgs &A) {
-  const int *__restrict__ col_count = A.col_count;
-  const int ncol = A.ncol, nkeys = A.nkeys, ns_max = A.ns_max;
-  int *__restrict__ col_u = A.col_u;
-  int *__restrict__ cursor = A.cursor;
-  int *__restrict__ col_base = A.col_base;
-  int *__restrict__ key_start = A.key_start;
-  int *__restrict__ sorted = A.sorted;
-  if (!*A.rebuild) return;
+__device__ void scan_columns(const ScanArgs &A, const int *col_count) {
   __shared__ int warp_tot[32];
   __shared__ int carry;
-  block_scan(
-      ncol, [&](int c) { return col_count[c]; },
-      [&](int c, int p) {
-        col_u[c] = p;
-        cursor[c] = 0;
-      },
-      warp_tot, &carry);
+  const int bcap = A.bcap;
+  int *col_base = A.col_base;
+  // the counts come from other blocks' atomics: read them from L2
   const int padded = block_scan(
-      ncol, [&](int c) { return (col_count[c] + 7) & ~7; },
+      A.ncol, [&](int c) { return (min(__ldcg(col_count + c), bcap) + 7) & ~7; },
       [&](int c, int p) { col_base[c] = p; }, warp_tot, &carry);
   if (threadIdx.x == 0) {
-    col_base[ncol] = padded;
-    key_start[nkeys] = padded;
+    col_base[A.ncol] = padded;
+    A.key_start[A.nkeys] = padded;
   }
-  for (int s = padded + threadIdx.x; s < ns_max; s += blockDim.x) sorted[s] = -1;
-}
-__global__ void __launch_bounds__(1024) k_scan_cols(ScanArgs a) {
-  pdl_wait();  // the predecessor's writes are visible from here on
-  pdl_trigger();
-  scan_body(a);
-}
-__global__ void __launch_bounds__(1024)
-k_scan_cols_batch(const ScanArgs *__restrict__ tab, const int *__restrict__ first, int nm) {
-  scan_body(tab[batch_member(first, nm, blockIdx.x)]);
+  for (int s = padded + threadIdx.x; s < A.ns_max; s += blockDim.x) A.sorted[s] = -1;
 }
 
-struct ScatterArgs {
-  const int *rebuild;
-  int n;
-  const int *key, *col_u;
-  int *cursor, *unsorted;
-};
-__device__ __forceinline__ void scatter_body(const ScatterArgs &A, Blk b) {
+// Rebuild steps: each atom's column (its xy cell of the wrapped position),
+// z key and image offset, the atom placed in its column's bucket; the last
+// block to finish lays out the columns (scan_columns).
+__device__ __forceinline__ void bin_body(const BinArgs &A, Blk b) {
   if (!*A.rebuild) return;
+  const ListGrid &g = A.g;
+  const double *__restrict__ pos = A.pos;
+  const int bcap = A.scan.bcap;
   const int i = b.x * blockDim.x + threadIdx.x;
-  const bool valid = i < A.n;
-  // one atomic per column among the warp's atoms (a column's atoms are
-  // sorted by (z, atom) afterwards, so their order here does not matter)
+  const bool valid = i < g.n;
   const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-  if (!valid) return;
-  const int c = A.key[i];
-  const unsigned peers = __match_any_sync(vmask, c);
-  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(&A.cursor[c], __popc(peers));
-  base = __shfl_sync(peers, base, leader);
-  A.unsorted[A.col_u[c] + base + __popc(peers & ((1u << lane) - 1u))] = i;
+  if (valid) {
+    const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    double w[3];
+    box_minpos(g.box, x, y, z, w[0], w[1], w[2]);
+    const int dims[2] = {g.ncx, g.ncy};
+    int c[2];
+    const bool finite = isfinite(x) && isfinite(y) && isfinite(z);
+    for (int a = 0; a < 2; a++) {
+      const double q = finite ? (w[a] - g.lo[a]) * g.inv[a] : 0.0;
+      int k = (int)floor(fmin(fmax(q, -1.0), (double)dims[a]));
+      c[a] = k < 0 ? 0 : (k >= dims[a] ? dims[a] - 1 : k);
+    }
+    if (!finite) atomicOr(A.status, ST_NONFINITE);
+    const int col = c[0] * g.ncy + c[1];
+    // non-negative FP32 bits order like the values
+    const float zf = finite ? (float)fmin(fmax(w[2] - g.lo[2], 0.0), 1.0e30) : 0.f;
+    A.zkey[i] = __float_as_uint(zf);
+    // one atomic per column among the warp's atoms (neighbouring atoms of a
+    // molecule share columns); the count it returns places each atom in its
+    // column's bucket (the order inside a column is sorted afterwards)
+    const unsigned peers = __match_any_sync(vmask, col);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&A.col_count[col], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    const int r = base + __popc(peers & ((1u << lane) - 1u));
+    if (r < bcap) A.bucket[(size_t)col * bcap + r] = i;
+    A.offset[3 * i] = x - w[0];
+    A.offset[3 * i + 1] = y - w[1];
+    A.offset[3 * i + 2] = z - w[2];
+    A.xbuild[3 * i] = x;
+    A.xbuild[3 * i + 1] = y;
+    A.xbuild[3 * i + 2] = z;
+  }
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's counts before its ticket
+    last = atomicAdd(A.ticket, 1u) == (unsigned)(b.n - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  scan_columns(A.scan, A.col_count);
+  if (threadIdx.x == 0) *A.ticket = 0u;  // ready for the next build
 }
-__global__ void k_scatter(ScatterArgs a) {
+__global__ void k_bin(BinArgs a) {
   pdl_wait();  // the predecessor's writes are visible from here on
   pdl_trigger();
-  scatter_body(a, own_blk());
+  bin_body(a, own_blk());
 }
-__global__ void k_scatter_batch(const ScatterArgs *__restrict__ tab, const int *__restrict__ first,
-                                int nm) {
+__global__ void k_bin_batch(const BinArgs *__restrict__ tab, const int *__restrict__ first,
+                            int nm) {
   const int m = batch_member(first, nm, blockIdx.x);
-  scatter_body(tab[m], batch_blk(first, m));
+  bin_body(tab[m], batch_blk(first, m));
+}
+
+// Slot records of the sorted coordinates: xw = x - offset keeps every atom
+// in the image it had at the last build, so tile images stay valid.
+// Padding slots get far-away positions and no charge; no tile pairs them.
+struct GatherArgs {
+  int ns;
+  const double *pos, *offset;
+  const int *sorted;
+  const double *charge;
+  const int *type, *mol;
+  float4 *xhi, *xlo;
+  double4 *xw;
+  int *mol_s;
+  const int *rebuild;
+  float4 *bb;
+};
+
+// Slot s's records for atom i (i < 0: padding): the FP64 wrapped position
+// and charge, the FP32 high part with the charge and, in mixed precision,
+// the FP32 residue with the type bits.  (hx, hy, hz) gets the FP32
+// position of an atom.
+__device__ __forceinline__ void write_slot(const GatherArgs &A, bool mixed, int s, int i,
+                                           float &hx, float &hy, float &hz) {
+  if (i < 0) {
+    const double far = 1.0e5 + 16.0 * s;
+    A.xw[s] = make_double4(far, 1.0e5, 1.0e5, 0.0);
+    A.xhi[s] = make_float4((float)far, 1.0e5f, 1.0e5f, 0.f);
+    if (mixed) A.xlo[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+    A.mol_s[s] = -1;
+    return;
+  }
+  const double x = A.pos[3 * i], y = A.pos[3 * i + 1], z = A.pos[3 * i + 2];
+  const double wx = x - A.offset[3 * i], wy = y - A.offset[3 * i + 1],
+               wz = z - A.offset[3 * i + 2];
+  const double q = A.charge[i];
+  A.xw[s] = make_double4(wx, wy, wz, q);
+  hx = (float)wx;
+  hy = (float)wy;
+  hz = (float)wz;
+  A.xhi[s] = make_float4(hx, hy, hz, (float)q);
+  if (mixed)
+    A.xlo[s] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
+                           (float)(wz - (double)hz), __int_as_float(A.type[i]));
+  A.mol_s[s] = A.mol[i];
+}
+
+// The box of the 4-atom cluster of slots s..s+3 (4 consecutive lanes, the
+// whole warp taking part): lower corner with the number of atoms in .w,
+// upper corner.
+__device__ __forceinline__ void write_cluster_box(float4 *bb, int s, bool in, bool atom,
+                                                  float hx, float hy, float hz) {
+  float lo[3] = {atom ? hx : 3.0e38f, atom ? hy : 3.0e38f, atom ? hz : 3.0e38f};
+  float hi[3] = {atom ? hx : -3.0e38f, atom ? hy : -3.0e38f, atom ? hz : -3.0e38f};
+  int m = atom ? 1 : 0;
+#pragma unroll
+  for (int o = 1; o < 4; o <<= 1) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      lo[c] = fminf(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+      hi[c] = fmaxf(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+    }
+    m += __shfl_xor_sync(0xffffffffu, m, o);
+  }
+  if (in && (s & 3) == 0) {
+    bb[2 * (s >> 2)] = make_float4(lo[0], lo[1], lo[2], (float)m);
+    bb[2 * (s >> 2) + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
+  }
 }
 
 // One block per column: bitonic sort of (z, atom) in shared memory, the
 // column's padded slots written in that order, and the column's z-bin
 // index (first slot of every bin).  A column above kColCap atoms flags
-// ST_CELL_OVERFLOW and is left empty.
+// ST_CELL_OVERFLOW and is left empty; one above its bucket (but within
+// kColCap) flags ST_LIST_OVERFLOW with its count, for the host to grow the
+// buckets and repeat the work.  With gather set (the rebuild of an MD step,
+// whose update kernel writes the slot records on the other steps) the block
+// also writes its slots' records and cluster boxes, and the blocks share
+// the empty slots past the last column.
 constexpr int kSortThreads = 256;
 struct SortArgs {
   const int *rebuild;
-  int nzb;
+  int nzb, ncol, bcap;
   float inv_z;
   int *col_count;
-  const int *col_u, *col_base, *unsorted;
+  const int *col_base, *bucket;
   const unsigned *zkey;
   int *sorted, *slot_of, *key_start, *status;
+  int *need;  // largest column count past the bucket size
+  int gather, mixed;
+  GatherArgs g;
 };
 __device__ __forceinline__ void sort_body(const SortArgs &A, Blk b) {
-  const int nzb = A.nzb;
+  const int nzb = A.nzb, bcap = A.bcap;
   const float inv_z = A.inv_z;
   int *__restrict__ col_count = A.col_count;
-  const int *__restrict__ col_u = A.col_u;
   const int *__restrict__ col_base = A.col_base;
-  const int *__restrict__ unsorted = A.unsorted;
   const unsigned *__restrict__ zkey = A.zkey;
   int *__restrict__ sorted = A.sorted;
   int *__restrict__ slot_of = A.slot_of;
   int *__restrict__ key_start = A.key_start;
-  int *__restrict__ status = A.status;
   if (!*A.rebuild) return;
   __shared__ unsigned long long keys[kColCap];
   const int col = b.x;
   int m = col_count[col];
   const int base = col_base[col], pend = col_base[col + 1];
   if (m > kColCap) {
-    if (threadIdx.x == 0) atomicOr(status, ST_CELL_OVERFLOW);
+    if (threadIdx.x == 0) atomicOr(A.status, ST_CELL_OVERFLOW);
     m = 0;
+  } else if (m > bcap) {
+    if (threadIdx.x == 0) {
+      atomicOr(A.status, ST_LIST_OVERFLOW);
+      atomicMax(A.need, m);
+    }
+    m = bcap;
   }
   int P = 1;
   while (P < m) P <<= 1;
-  const int u = col_u[col];
+  const int *__restrict__ bucket = A.bucket + (size_t)col * bcap;
   for (int k = threadIdx.x; k < P; k += kSortThreads) {
     if (k < m) {
-      const int i = unsorted[u + k];
+      const int i = bucket[k];
       keys[k] = ((unsigned long long)zkey[i] << 32) | (unsigned)i;
     } else {
       keys[k] = ~0ull;
@@ -310,21 +348,44 @@ __device__ __forceinline__ void sort_body(const SortArgs &A, Blk b) {
   }
   auto bin_of = [&](int k) {
     const float zf = __uint_as_float((unsigned)(keys[k] >> 32));
-    const int b = (int)(zf * inv_z);
-    return b < 0 ? 0 : (b >= nzb ? nzb - 1 : b);
+    const int q = (int)(zf * inv_z);
+    return q < 0 ? 0 : (q >= nzb ? nzb - 1 : q);
   };
   int *ks = key_start + (size_t)col * nzb;
-  for (int k = threadIdx.x; k < pend - base; k += kSortThreads) {
-    const int atom = k < m ? (int)(keys[k] & 0xffffffffu) : -1;
-    sorted[base + k] = atom;
-    if (atom >= 0) slot_of[atom] = base + k;
+  // the column's slots (a whole number of clusters: warps stay uniform)
+  const int len = pend - base;
+  for (int k0 = 0; k0 < len; k0 += kSortThreads) {
+    const int k = k0 + threadIdx.x;
+    const bool in = k < len;
+    const int atom = in && k < m ? (int)(keys[k] & 0xffffffffu) : -1;
+    if (in) {
+      sorted[base + k] = atom;
+      if (atom >= 0) slot_of[atom] = base + k;
+    }
+    if (A.gather) {
+      float hx = 0.f, hy = 0.f, hz = 0.f;
+      if (in) write_slot(A.g, A.mixed, base + k, atom, hx, hy, hz);
+      write_cluster_box(A.g.bb, base + k, in, atom >= 0, hx, hy, hz);
+    }
+  }
+  if (A.gather) {
+    // the empty slots past the last column (the padded total is a multiple
+    // of 8, so every cluster lies within one warp's lanes)
+    const int ns = A.g.ns;
+    for (int s0 = col_base[A.ncol] + b.x * kSortThreads; s0 < ns; s0 += b.n * kSortThreads) {
+      const int s = s0 + threadIdx.x;
+      const bool in = s < ns;
+      float hx = 0.f, hy = 0.f, hz = 0.f;
+      if (in) write_slot(A.g, A.mixed, s, -1, hx, hy, hz);
+      write_cluster_box(A.g.bb, s, in, false, hx, hy, hz);
+    }
   }
   for (int k = threadIdx.x; k < m; k += kSortThreads) {
-    const int b = bin_of(k), prev = k ? bin_of(k - 1) : -1;
-    for (int q = prev + 1; q <= b; q++) ks[q] = base + k;
+    const int q = bin_of(k), prev = k ? bin_of(k - 1) : -1;
+    for (int z = prev + 1; z <= q; z++) ks[z] = base + k;
   }
   const int last = m ? bin_of(m - 1) : -1;
-  for (int q = last + 1 + threadIdx.x; q < nzb; q += kSortThreads) ks[q] = base + m;
+  for (int z = last + 1 + threadIdx.x; z < nzb; z += kSortThreads) ks[z] = base + m;
   __syncthreads();
   if (threadIdx.x == 0) col_count[col] = 0;  // ready for the next build
 }
@@ -339,83 +400,16 @@ k_sort_cols_batch(const SortArgs *__restrict__ tab, const int *__restrict__ firs
   sort_body(tab[m], batch_blk(first, m));
 }
 
-// Per-step gather of the sorted coordinates: xw = x - offset keeps every
-// atom in the image it had at the last build, so tile images stay valid.
-// Padding slots get far-away positions and no charge; no tile pairs them.
-struct GatherArgs {
-  int ns;
-  const double *pos, *offset;
-  const int *sorted;
-  const double *charge;
-  const int *type, *mol;
-  float4 *xhi, *xlo;
-  double4 *xw;
-  int *mol_s;
-  const int *rebuild;
-  float4 *bb;
-  int updated;  // the update kernel of this step wrote the slots: gather on a rebuild only
-};
+// The slot records of every slot (evaluations outside MD steps, and the
+// members of an ensemble); the cluster boxes on a rebuild.
 template <bool MIXED>
 __device__ __forceinline__ void gather_slots_body(const GatherArgs &A, Blk b) {
-  if (A.updated && !*A.rebuild) return;
-  const int ns = A.ns;
-  const double *__restrict__ pos = A.pos;
-  const double *__restrict__ offset = A.offset;
-  const int *__restrict__ sorted = A.sorted;
-  const double *__restrict__ charge = A.charge;
-  const int *__restrict__ type = A.type;
-  const int *__restrict__ mol = A.mol;
-  float4 *__restrict__ xhi = A.xhi;
-  float4 *__restrict__ xlo = A.xlo;
-  double4 *__restrict__ xw = A.xw;
-  int *__restrict__ mol_s = A.mol_s;
-  const int *__restrict__ rebuild = A.rebuild;
-  float4 *__restrict__ bb = A.bb;
   const int s = b.x * blockDim.x + threadIdx.x;
-  const bool in = s < ns;
-  const int i = in ? sorted[s] : -1;
+  const bool in = s < A.ns;
+  const int i = in ? A.sorted[s] : -1;
   float hx = 0.f, hy = 0.f, hz = 0.f;
-  if (in && i < 0) {
-    const double far = 1.0e5 + 16.0 * s;
-    xw[s] = make_double4(far, 1.0e5, 1.0e5, 0.0);
-    xhi[s] = make_float4((float)far, 1.0e5f, 1.0e5f, 0.f);
-    if (MIXED) xlo[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
-    mol_s[s] = -1;
-  } else if (in) {
-    const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-    const double wx = x - offset[3 * i], wy = y - offset[3 * i + 1], wz = z - offset[3 * i + 2];
-    const double q = charge[i];
-    xw[s] = make_double4(wx, wy, wz, q);
-    hx = (float)wx;
-    hy = (float)wy;
-    hz = (float)wz;
-    xhi[s] = make_float4(hx, hy, hz, (float)q);
-    if (MIXED)
-      xlo[s] = make_float4((float)(wx - (double)hx), (float)(wy - (double)hy),
-                           (float)(wz - (double)hz), __int_as_float(type[i]));
-    mol_s[s] = mol[i];
-  }
-  // on a rebuild: the box of every 4-atom cluster (4 consecutive lanes;
-  // lower corner with the number of atoms in .w, upper corner)
-  if (*rebuild) {
-    const bool atom = in && i >= 0;
-    float lo[3] = {atom ? hx : 3.0e38f, atom ? hy : 3.0e38f, atom ? hz : 3.0e38f};
-    float hi[3] = {atom ? hx : -3.0e38f, atom ? hy : -3.0e38f, atom ? hz : -3.0e38f};
-    int m = atom ? 1 : 0;
-#pragma unroll
-    for (int o = 1; o < 4; o <<= 1) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        lo[c] = fminf(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
-        hi[c] = fmaxf(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
-      }
-      m += __shfl_xor_sync(0xffffffffu, m, o);
-    }
-    if (in && (s & 3) == 0) {
-      bb[2 * (s >> 2)] = make_float4(lo[0], lo[1], lo[2], (float)m);
-      bb[2 * (s >> 2) + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
-    }
-  }
+  if (in) write_slot(A, MIXED, s, i, hx, hy, hz);
+  if (*A.rebuild) write_cluster_box(A.bb, s, in, in && i >= 0, hx, hy, hz);
 }
 template <bool MIXED>
 __global__ void k_gather(GatherArgs a) {
@@ -943,14 +937,18 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
   if (nl->cap > cap) cap = nl->cap;
   if (nl->cap_set > 0) cap = nl->cap_set;  // a capacity the caller fixed
   nl->cap = cap;
+  // column buckets: four times a column's mean count, at least 256 atoms
+  // (vacuum grids are dense in the middle), at most the sort's kColCap; a
+  // fuller column flags an overflow and the buckets grow to its count
+  int bcap = std::max(256, 4 * ((n + nl->ncol - 1) / nl->ncol));
+  if (nl->bcap > bcap) bcap = nl->bcap;
+  if (nl->bcap_set > 0) bcap = nl->bcap_set;
+  nl->bcap = std::min(kColCap, (bcap + 31) & ~31);
   const size_t nn = std::max(1, n), ns = std::max(8, nl->ns_max);
-  PM_CHECK(dev_alloc(s, &nl->d_key, sizeof(int) * nn));
   PM_CHECK(dev_alloc(s, &nl->d_zkey, sizeof(unsigned) * nn));
-  PM_CHECK(dev_alloc(s, &nl->d_unsorted, sizeof(int) * nn));
+  PM_CHECK(dev_alloc(s, &nl->d_bucket, sizeof(int) * (size_t)nl->bcap * nl->ncol));
   PM_CHECK(dev_alloc(s, &nl->d_col_count, sizeof(int) * nl->ncol));
   PM_CUDA(cudaMemsetAsync(nl->d_col_count, 0, sizeof(int) * nl->ncol, s->stream));
-  PM_CHECK(dev_alloc(s, &nl->d_col_u, sizeof(int) * nl->ncol));
-  PM_CHECK(dev_alloc(s, &nl->d_col_cursor, sizeof(int) * nl->ncol));
   PM_CHECK(dev_alloc(s, &nl->d_col_base, sizeof(int) * (nl->ncol + 1)));
   PM_CHECK(dev_alloc(s, &nl->d_key_start, sizeof(int) * (nl->nkeys + 1)));
   PM_CHECK(dev_alloc(s, &nl->d_sorted, sizeof(int) * ns));
@@ -975,24 +973,24 @@ int nb_list_init(System *s, NeighborList *nl, double cutoff, double skin, double
                           s->stream));
   PM_CHECK(dev_alloc(s, &nl->d_maxdisp, 2 * sizeof(unsigned int)));
   PM_CUDA(cudaMemsetAsync(nl->d_maxdisp, 0, 2 * sizeof(unsigned int), s->stream));
-  PM_CHECK(dev_alloc(s, &nl->d_rebuild, 3 * sizeof(int)));
-  PM_CUDA(cudaMemsetAsync(nl->d_rebuild, 0, 3 * sizeof(int), s->stream));
-  PM_CHECK(dev_alloc(s, &nl->d_build_work, 2 * sizeof(int)));
-  PM_CUDA(cudaMemsetAsync(nl->d_build_work, 0, 2 * sizeof(int), s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_rebuild, 4 * sizeof(int)));
+  PM_CUDA(cudaMemsetAsync(nl->d_rebuild, 0, 4 * sizeof(int), s->stream));
+  PM_CHECK(dev_alloc(s, &nl->d_build_work, 3 * sizeof(int)));
+  PM_CUDA(cudaMemsetAsync(nl->d_build_work, 0, 3 * sizeof(int), s->stream));
   nl->built = 0;
   return PMGPU_OK;
 }
 
 int nb_list_free(System *s, NeighborList *nl) {
-  void *ptrs[] = {nl->d_key, nl->d_zkey, nl->d_unsorted, nl->d_col_count, nl->d_col_u,
-                  nl->d_col_cursor, nl->d_col_base, nl->d_key_start, nl->d_sorted,
+  void *ptrs[] = {nl->d_zkey, nl->d_bucket, nl->d_col_count, nl->d_col_base,
+                  nl->d_key_start, nl->d_sorted,
                   nl->d_offset, nl->d_xbuild, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
                   nl->d_bb, nl->d_fslot, nl->d_slot_of, nl->d_tiles, nl->d_tmod,
                   nl->d_jlanes, nl->d_jl_count, nl->d_tile_count, nl->d_maxdisp,
                   nl->d_rebuild, nl->d_build_work};
   for (void *p : ptrs) dev_free(s, p);
   nl->d_build_work = nullptr;
-  nl->d_key = nl->d_unsorted = nl->d_col_count = nl->d_col_u = nl->d_col_cursor = nullptr;
+  nl->d_bucket = nl->d_col_count = nullptr;
   nl->d_col_base = nl->d_key_start = nl->d_sorted = nl->d_mol_s = nl->d_tile_count = nullptr;
   nl->d_zkey = nullptr;
   nl->d_rebuild = nullptr;
@@ -1013,8 +1011,6 @@ int nb_list_free(System *s, NeighborList *nl) {
 // the tile build).
 struct ListArgs {
   BinArgs bin;
-  ScanArgs scan;
-  ScatterArgs scatter;
   SortArgs sort;
   GatherArgs gather;
   BuildArgs build;
@@ -1030,18 +1026,18 @@ static void list_args(System *s, NeighborList *nl, ListArgs *L) {
     g.lo[a] = nl->lo[a];
     g.inv[a] = 1.0 / nl->cs[a];
   }
-  L->bin = BinArgs{g, s->d_pos, nl->d_rebuild, nl->d_key, nl->d_zkey, nl->d_col_count,
-                   nl->d_offset, nl->d_xbuild, s->d_status};
-  L->scan = ScanArgs{nl->d_rebuild, nl->d_col_count, nl->ncol, nl->d_col_u, nl->d_col_cursor,
-                     nl->d_col_base, nl->d_key_start, nl->nkeys, nl->d_sorted, nl->ns_max};
-  L->scatter = ScatterArgs{nl->d_rebuild, s->n, nl->d_key, nl->d_col_u, nl->d_col_cursor,
-                           nl->d_unsorted};
-  L->sort = SortArgs{nl->d_rebuild, nl->nzb, (float)(1.0 / nl->cs[2]), nl->d_col_count,
-                     nl->d_col_u, nl->d_col_base, nl->d_unsorted, nl->d_zkey, nl->d_sorted,
-                     nl->d_slot_of, nl->d_key_start, s->d_status};
+  const ScanArgs scan{nl->ncol, nl->nkeys, nl->ns_max, nl->bcap,
+                      nl->d_col_base, nl->d_key_start, nl->d_sorted};
+  L->bin = BinArgs{g, s->d_pos, nl->d_rebuild, nl->d_zkey, nl->d_col_count, nl->d_bucket,
+                   nl->d_offset, nl->d_xbuild, s->d_status, (unsigned *)nl->d_build_work + 2,
+                   scan};
   L->gather = GatherArgs{nl->ns_max, s->d_pos, nl->d_offset, nl->d_sorted, s->d_charge,
                          s->d_type, s->d_mol, nl->d_xhi, nl->d_xlo, nl->d_xw, nl->d_mol_s,
-                         nl->d_rebuild, nl->d_bb, 0};
+                         nl->d_rebuild, nl->d_bb};
+  L->sort = SortArgs{nl->d_rebuild, nl->nzb, nl->ncol, nl->bcap, (float)(1.0 / nl->cs[2]),
+                     nl->d_col_count, nl->d_col_base, nl->d_bucket, nl->d_zkey, nl->d_sorted,
+                     nl->d_slot_of, nl->d_key_start, s->d_status, nl->d_rebuild + 3,
+                     0, s->precision == PMGPU_PREC_MIXED ? 1 : 0, L->gather};
   TileBuildArgs ba;
   ba.nclusters = nl->nclusters;
   ba.periodic = s->box.periodic;
@@ -1080,24 +1076,27 @@ int nb_prepare(System *s, NeighborList *nl, int force_rebuild) {
   // an MD step's update kernel has taken the decision already, and written
   // the slot records of the drifted positions
   const int updated = nl->decided && !first && !force_rebuild;
-  if (!nl->decided || first || force_rebuild)
+  if (!nl->decided || first || force_rebuild) {
     PM_CUDA(launch_pdl(k_check_rebuild, nb, kCheckThreads, 0, st, n, s->d_pos, nl->d_xbuild,
                        nl->d_maxdisp, nl->d_rebuild, hs * hs, (force_rebuild || first) ? 1 : 0));
+    s->kernels++;
+  }
   nl->decided = 0;
-  {
-    cudaStream_t q = st;  // the rebuild-only sort
-    // each kernel of the chain launches as a programmatic dependent of the
-    // one before, so on the steps that keep the list their early exits
-    // overlap their launches
-    ListArgs la;
-    list_args(s, nl, &la);
-    la.gather.updated = updated;
-    PM_CUDA(launch_pdl(k_bin, nb, T, 0, q, la.bin));
-    PM_CUDA(launch_pdl(k_scan_cols, 1, 1024, 0, q, la.scan));
-    PM_CUDA(launch_pdl(k_scatter, nb, T, 0, q, la.scatter));
-    PM_CUDA(launch_pdl(k_sort_cols, nl->ncol, kSortThreads, 0, q, la.sort));
+  // each kernel of the chain launches as a programmatic dependent of the
+  // one before, so on the steps that keep the list their early exits
+  // overlap their launches: the binning (with the column layout), the
+  // column sort (with the slot records on an MD step's rebuild) and, outside
+  // MD steps, the slot records of every evaluation
+  ListArgs la;
+  list_args(s, nl, &la);
+  la.sort.gather = updated;
+  PM_CUDA(launch_pdl(k_bin, nb, T, 0, st, la.bin));
+  PM_CUDA(launch_pdl(k_sort_cols, nl->ncol, kSortThreads, 0, st, la.sort));
+  s->kernels += 2;
+  if (!updated) {
     PM_CUDA(launch_pdl(s->precision == PMGPU_PREC_MIXED ? k_gather<true> : k_gather<false>, nbs,
                        T, 0, st, la.gather));
+    s->kernels++;
   }
   PM_CUDA(cudaGetLastError());
   nl->built = 1;  // the slot order exists from here on
@@ -1451,8 +1450,6 @@ int fold_pending_slots(System *s) {
 // those of its own launches.
 struct NbBatch {
   BatchTable<BinArgs> bin;
-  BatchTable<ScanArgs> scan;
-  BatchTable<ScatterArgs> scatter;
   BatchTable<SortArgs> sort;
   BatchTable<GatherArgs> gather;
   BatchTable<BuildArgs> build;
@@ -1472,7 +1469,7 @@ struct NbBatch {
 NbBatch *nb_batch_new() { return new NbBatch(); }
 void nb_batch_free(NbBatch *b) {
   if (!b) return;
-  b->bin.release(); b->scan.release(); b->scatter.release(); b->sort.release();
+  b->bin.release(); b->sort.release();
   b->gather.release(); b->build.release(); b->jl.release(); b->gforce.release();
   b->energy.release(); b->slots.release(); b->probe.release();
   delete b;
@@ -1501,7 +1498,7 @@ int nb_batch_build(NbBatch *b, System *const *m, int n, const PairTerms *terms,
   if (!sms && (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m[0]->device) !=
                    cudaSuccess || sms <= 0))
     sms = 148;
-  b->bin.clear(); b->scan.clear(); b->scatter.clear(); b->sort.clear(); b->gather.clear();
+  b->bin.clear(); b->sort.clear(); b->gather.clear();
   b->build.clear(); b->jl.clear(); b->gforce.clear(); b->energy.clear(); b->slots.clear();
   b->has_form.assign(n, 0);
   b->base.assign(n, PairArgs<float>());
@@ -1518,9 +1515,7 @@ int nb_batch_build(NbBatch *b, System *const *m, int n, const PairTerms *terms,
     list_args(s, nl, &la);
     const int T = 256;
     const int nb = (s->n + T - 1) / T, nbs = (nl->ns_max + T - 1) / T;
-    b->bin.add(la.bin, nb);
-    b->scan.add(la.scan, 1);
-    b->scatter.add(la.scatter, nb);
+    b->bin.add(la.bin, std::max(1, nb));  // its last block lays out the columns
     b->sort.add(la.sort, nl->ncol);
     b->gather.add(la.gather, nbs);
     b->build.add(la.build, std::max(1, std::min((nl->nrows + kBuildWarps - 1) / kBuildWarps,
@@ -1552,8 +1547,6 @@ int nb_batch_build(NbBatch *b, System *const *m, int n, const PairTerms *terms,
   }
   BatchTable<PairArgs<float>> *pt[] = {&b->jl, &b->gforce, &b->energy};
   PM_CUDA(b->bin.upload());
-  PM_CUDA(b->scan.upload());
-  PM_CUDA(b->scatter.upload());
   PM_CUDA(b->sort.upload());
   PM_CUDA(b->gather.upload());
   PM_CUDA(b->build.upload());
@@ -1568,11 +1561,8 @@ int nb_batch_build(NbBatch *b, System *const *m, int n, const PairTerms *terms,
 int nb_batch_list(NbBatch *b, cudaStream_t st, long long *launched) {
   const int nm = b->bin.members();
   if (!nm) return PMGPU_OK;
-  *launched += 4 + (b->bin.total() > 0) + (b->scatter.total() > 0);
-  if (b->bin.total()) k_bin_batch<<<b->bin.total(), 256, 0, st>>>(b->bin.d, b->bin.d_first, nm);
-  k_scan_cols_batch<<<b->scan.total(), 1024, 0, st>>>(b->scan.d, b->scan.d_first, nm);
-  if (b->scatter.total())
-    k_scatter_batch<<<b->scatter.total(), 256, 0, st>>>(b->scatter.d, b->scatter.d_first, nm);
+  *launched += 4;
+  k_bin_batch<<<b->bin.total(), 256, 0, st>>>(b->bin.d, b->bin.d_first, nm);
   k_sort_cols_batch<<<b->sort.total(), kSortThreads, 0, st>>>(b->sort.d, b->sort.d_first, nm);
   k_gather_batch<true><<<b->gather.total(), 256, 0, st>>>(b->gather.d, b->gather.d_first, nm);
   k_build_tiles_batch<<<b->build.total(), kBuildWarps * 32, 0, st>>>(b->build.d,

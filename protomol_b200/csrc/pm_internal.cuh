@@ -170,6 +170,8 @@ struct NeighborList {
   int nrows = 0;                     // nclusters * kRowParts tile rows
   int cap = 0;                       // tiles per row
   int cap_set = 0;                   // tiles per row fixed by the caller (0: sized here)
+  int bcap = 0;                      // atoms a column bucket holds (multiple of 32, <= kColCap)
+  int bcap_set = 0;                  // bucket size fixed by the caller (0: sized here)
   int built = 0;
   int decided = 0;                   // this evaluation's rebuild decision is taken
   // a force-only MD step left its pair forces in d_fslot for the next update
@@ -179,12 +181,9 @@ struct NeighborList {
   int last_form = PMGPU_PAIRK_GENERIC;  // pair-kernel form of the last launch
   long long builds = 0;
   // device
-  int *d_key = nullptr;          // n: column of each atom
   unsigned *d_zkey = nullptr;    // n: z above the grid corner (FP32 bits, >= 0)
-  int *d_unsorted = nullptr;     // n: atoms grouped by column, any order
-  int *d_col_count = nullptr;    // ncol
-  int *d_col_u = nullptr;        // ncol: first entry of each column in d_unsorted
-  int *d_col_cursor = nullptr;   // ncol
+  int *d_bucket = nullptr;       // ncol buckets of bcap atoms: each column's atoms, any order
+  int *d_col_count = nullptr;    // ncol: atoms binned into each column
   int *d_col_base = nullptr;     // ncol + 1: first slot of each column (padded)
   int *d_key_start = nullptr;    // nkeys + 1: first slot of each (column, z bin)
   int *d_sorted = nullptr;       // ns_max: atom of each slot, -1 for padding
@@ -203,8 +202,11 @@ struct NeighborList {
   int *d_jl_count = nullptr;     // entries per row
   int *d_tile_count = nullptr;   // nrows
   unsigned int *d_maxdisp = nullptr;  // rebuild check: block ticket, max displacement^2 bits
-  int *d_rebuild = nullptr;      // rebuild flag, build count, largest row need after an overflow
-  int *d_build_work = nullptr;   // the tile build's row counter and finished-warp count
+  // rebuild flag, build count, largest row need and largest column count
+  // after an overflow
+  int *d_rebuild = nullptr;
+  // the tile build's row counter and finished-warp count; binning blocks done
+  int *d_build_work = nullptr;
 };
 
 struct System;

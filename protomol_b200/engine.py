@@ -261,6 +261,11 @@ class GpuSystem:
         """Fix the pair lists' capacity (testing the growth path)."""
         L.check(self.lib.pmgpu_debug_set_list_capacity(self.h, int(tiles_per_row)))
 
+    def set_column_capacity(self, atoms_per_column: int) -> None:
+        """Fix the atoms a pair-list column bucket holds (testing the growth
+        path)."""
+        L.check(self.lib.pmgpu_debug_set_column_capacity(self.h, int(atoms_per_column)))
+
     def limit_list_rows(self, tiles_per_row: int) -> None:
         """Limit the tiles a list row may hold in later builds, keeping the
         current list and forces (testing the growth path inside segments)."""

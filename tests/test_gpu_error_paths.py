@@ -1,6 +1,7 @@
 """Error paths and the Langevin thermostat, on the GPU without any device
 fault: a pair list whose capacity is too small for the system (the build
-flags the overflow, the host grows the list and repeats the segment), a
+flags the overflow, the host grows the list and repeats the segment), column
+buckets too small for the atoms binned into a column (the same growth), a
 non-finite position handed in from the host (refused before any upload),
 and the statistics of the Langevin noise (Philox4x32-10 + Box-Muller)
 through the integrator."""
@@ -51,6 +52,36 @@ def test_list_overflow_in_single_evaluation(ctx):
     e0, _ = gs.evaluate()
     f0 = gs.forces_total()
     gs.set_list_capacity(1)
+    e1, _ = gs.evaluate()
+    assert np.array_equal(f0, gs.forces_total())
+    assert np.array_equal(e0, e1)
+    gs.close()
+
+
+def test_column_bucket_overflow_retry_is_bit_identical(ctx):
+    """Column buckets fixed at 32 atoms overflow on the first build (the
+    648-atom box bins about 40 atoms into each of its 16 columns); the
+    buckets grow to the fullest column's count, the segment is repeated and
+    the trajectory equals, bit for bit, the run whose buckets never
+    overflowed."""
+    out = []
+    for cap in (None, 32):
+        gs = _c1(ctx)
+        if cap:
+            gs.set_column_capacity(cap)
+        LangevinLeapfrogIntegrator(1.0, 300.0, 5.0, seed=11).run(gs, 30)
+        out.append((gs.positions(), gs.velocities(), gs.energies()[0]))
+        assert gs.forces[0].stats()["list_entries"] > 0
+        gs.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+
+
+def test_column_bucket_overflow_in_single_evaluation(ctx):
+    gs = _c1(ctx)
+    e0, _ = gs.evaluate()
+    f0 = gs.forces_total()
+    gs.set_column_capacity(32)
     e1, _ = gs.evaluate()
     assert np.array_equal(f0, gs.forces_total())
     assert np.array_equal(e0, e1)
