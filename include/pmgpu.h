@@ -361,6 +361,14 @@ int pmgpu_run(pmgpu_system *sys, const pmgpu_integrator *integ, long n_steps);
 int pmgpu_run_async(pmgpu_system *sys, const pmgpu_integrator *integ, long n_steps);
 int pmgpu_run_query(pmgpu_system *sys, int *done);
 int pmgpu_run_wait(pmgpu_system *sys);
+/* Waits for a pending segment and undoes it: positions, velocities,
+ * forces and the step counter return to their values at its start, as if it
+ * had not run (pair lists are rebuilt at the next evaluation).  A device
+ * integrator starts the segment after an output this way before the host
+ * knows it is wanted, so that it runs while the outputs are written, and
+ * discards it when the next run() asks for other steps or the host changed
+ * the state.  No pending segment: nothing to do. */
+int pmgpu_run_discard(pmgpu_system *sys);
 /* Free and total device memory of the context's GPU (admission control). */
 int pmgpu_mem_info(pmgpu_context *ctx, long long *free_bytes, long long *total_bytes);
 /* Estimated device bytes of a periodic system of n_atoms with edges

@@ -45,7 +45,7 @@ EXPORTED = [
     "pmgpu_ensemble_set_splits", "pmgpu_ensemble_time_pairs", "pmgpu_ensemble_get_info",
     "pmgpu_ensemble_member", "pmgpu_debug_limit_list_rows", "pmgpu_system_set_step",
     "pmgpu_force_full_add", "pmgpu_force_simplefull_switched_add", "pmgpu_force_scpism_add",
-    "pmgpu_force_born_add", "pmgpu_debug_set_column_capacity",
+    "pmgpu_force_born_add", "pmgpu_debug_set_column_capacity", "pmgpu_run_discard",
 ]
 PHASES = ["list", "pairs", "pme", "correction", "bonded", "gb", "simplefull", "integrate"]
 
@@ -159,6 +159,7 @@ def load() -> C.CDLL:
     lib.pmgpu_run_async.argtypes = [vp, C.POINTER(Integrator), C.c_long]
     lib.pmgpu_run_query.argtypes = [vp, C.POINTER(i32)]
     lib.pmgpu_run_wait.argtypes = [vp]
+    lib.pmgpu_run_discard.argtypes = [vp]
     lib.pmgpu_mem_info.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     lib.pmgpu_fp32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     lib.pmgpu_footprint_estimate.argtypes = [i32, vp, dbl, vp, C.POINTER(C.c_longlong)]

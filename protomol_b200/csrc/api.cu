@@ -1681,6 +1681,21 @@ int pmgpu_run_wait(pmgpu_system *h) {
   return run_finish(s);
 }
 
+int pmgpu_run_discard(pmgpu_system *h) {
+  if (!h) return fail(PMGPU_ERR_ARG, "null argument");
+  System *s = sysp(h);
+  PM_CUDA(cudaSetDevice(s->device));
+  if (!s->pending.active) return PMGPU_OK;
+  // the segment's own outcome does not matter: it is undone
+  (void)run_finish(s);
+  PM_CHECK(run_snapshot(s, 1));
+  s->step = s->pending.step0;
+  s->forces_valid = s->pending.valid0;
+  for (auto &nl : s->lists) nl.built = 0;  // fresh lists, as for new positions
+  PM_CUDA(cudaStreamSynchronize(s->stream));
+  return PMGPU_OK;
+}
+
 int pmgpu_mem_info(pmgpu_context *ctx, long long *free_bytes, long long *total_bytes) {
   if (!ctx || !free_bytes || !total_bytes) return fail(PMGPU_ERR_ARG, "null argument");
   PM_CUDA(cudaSetDevice(ctx->device));

@@ -674,6 +674,12 @@ class _Integrator:
     def wait(system: GpuSystem) -> None:
         L.check(system.lib.pmgpu_run_wait(system.h))
 
+    @staticmethod
+    def discard(system: GpuSystem) -> None:
+        """Wait for a pending run_async segment and undo it (the state at
+        its start is restored)."""
+        L.check(system.lib.pmgpu_run_discard(system.h))
+
 
 class LeapfrogIntegrator(_Integrator):
     kind = L.INT_LEAPFROG

@@ -32,7 +32,11 @@
 // stay resident, and only at the end of run(n) (ProtoMolApp::step hands
 // run() the steps up to the next output, ProtoMolApp.cpp:486-498) are
 // positions, velocities, forces and energies written back to the app for
-// the outputs and checkpoints.  Every force of their force group must have
+// the outputs and checkpoints.  While ProtoMol writes those outputs the
+// device already runs the next segment, started at the end of run(n) on the
+// guess that it has as many steps; the next run() takes it when it does and
+// the host left the state alone, and discards it (pmgpu_run_discard)
+// otherwise.  Every force of their force group must have
 // a device form: the GPU forces above, and the CPU Bond, Angle, Dihedral and
 // Improper forces, which they map to the device's bonded terms.
 //
@@ -56,6 +60,7 @@
 #include <protomol/type/ScalarStructure.h>
 #include <protomol/type/Vector3DBlock.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -741,10 +746,12 @@ class DeviceIntegrator : public STSIntegrator {
   DeviceIntegrator(int kind, Real timestep, Real temperature, Real gamma, int seed,
                    ForceGroup *fg)
       : STSIntegrator(timestep, fg), myKind(kind), myTemperature(temperature),
-        myGamma(gamma), mySeed(seed), mySystem(0) {}
+        myGamma(gamma), mySeed(seed), mySystem(0), mySpeculated(0) {}
 
   virtual void initialize(ProtoMolApp *app) {
     STSIntegrator::initialize(app);
+    if (mySystem && mySpeculated) check(pmgpu_run_discard(mySystem), getIdNoAlias());
+    mySpeculated = 0;
     mySystem = systemFor(app->topology);
     // every force of the group gets its device form; only those run
     const vector<Force *> forces = myForcesToEvaluate->getForces();
@@ -786,14 +793,22 @@ class DeviceIntegrator : public STSIntegrator {
 
   virtual long run(const long numTimesteps) {
     if (numTimesteps < 1) return 0;
-    upload();
     pmgpu_integrator it;
     it.kind = myKind;
     it.timestep_fs = getTimestep();
     it.temperature = myTemperature;
     it.gamma_ps = myGamma;
     it.seed = (uint64_t)mySeed;
-    check(pmgpu_run(mySystem, &it, numTimesteps), getIdNoAlias());
+    // the segment started at the end of the last run() is these steps if it
+    // has as many and the host left the state as it was handed over
+    if (mySpeculated == numTimesteps && hostUnchanged()) {
+      check(pmgpu_run_wait(mySystem), getIdNoAlias());
+    } else {
+      if (mySpeculated) check(pmgpu_run_discard(mySystem), getIdNoAlias());
+      upload();
+      check(pmgpu_run(mySystem, &it, numTimesteps), getIdNoAlias());
+    }
+    mySpeculated = 0;
     // the simulated time the outputs report, advanced by the steps taken
     // (as the reference's own device integrator does,
     // integrator/openMM/OpenMMIntegrator.cpp:688)
@@ -801,6 +816,18 @@ class DeviceIntegrator : public STSIntegrator {
     double e[PMGPU_E_COUNT];
     check(pmgpu_system_get_energies(mySystem, e, 0), getIdNoAlias());
     download(e);
+    // ProtoMolApp::step writes its outputs from the state just handed back
+    // before it asks for the next steps (ProtoMolApp.cpp:474-500): the next
+    // segment, guessed to be as long as this one, runs on the device
+    // meanwhile.  Only when this integrator is the application's (no other
+    // integrator touches the system between the calls), not past lastStep,
+    // and unless PMGPU_OVERLAP=0.
+    const long next = app->currentStep + numTimesteps;
+    if (overlapEnabled() && app->integrator == this &&
+        (app->lastStep < 0 || next + numTimesteps <= app->lastStep)) {
+      check(pmgpu_run_async(mySystem, &it, numTimesteps), getIdNoAlias());
+      mySpeculated = numTimesteps;
+    }
     return numTimesteps;
   }
 
@@ -826,6 +853,16 @@ class DeviceIntegrator : public STSIntegrator {
     return new DeviceIntegrator(myKind, values[0], values[1], values[2], values[3], fg);
   }
 
+  static bool overlapEnabled() {
+    const char *v = getenv("PMGPU_OVERLAP");
+    return !(v && v[0] == '0');
+  }
+  bool hostUnchanged() const {
+    const size_t n3 = 3 * app->positions.size();
+    return myHostPos.size() == n3 && myHostVel.size() == n3 &&
+           memcmp(&myHostPos[0], app->positions.c, n3 * sizeof(double)) == 0 &&
+           memcmp(&myHostVel[0], app->velocities.c, n3 * sizeof(double)) == 0;
+  }
   // Positions and velocities go to the device only when the host changed
   // them since the last download (a modifier, a restart, the first call).
   void upload() {
@@ -854,6 +891,7 @@ class DeviceIntegrator : public STSIntegrator {
   int mySeed;
   pmgpu_system *mySystem;
   vector<double> myHostPos, myHostVel;
+  long mySpeculated;  // steps of the segment started ahead of the next run() (0: none)
 };
 
 }  // namespace
