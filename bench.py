@@ -197,15 +197,19 @@ def load_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "src": "fallback"}
 
 
-def load_traffic() -> float | None:
-    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
+def load_traffic() -> tuple:
+    """DRAM bytes per pair-kernel launch from the committed ncu summary:
+    a cold-cache launch, and the mean of launches in the MD loop with the
+    L2 as the loop leaves it (None where absent)."""
     p = os.path.join(ROOT, "profiles", "pair_kernel_tip3p23550.json")
     if os.path.exists(p):
         try:
-            return float(json.load(open(p))["dram_bytes_per_launch"])
+            d = json.load(open(p))
+            warm = d.get("warm_l2", {}).get("mean")
+            return float(d["dram_bytes_per_launch"]), (float(warm) if warm is not None else None)
         except Exception:
-            return None
-    return None
+            return None, None
+    return None, None
 
 
 # FP32 flops of one in-cutoff pair in the force-only pair kernel
@@ -838,7 +842,7 @@ def main():
     pair_avg_s = pair_ms / max(1, pair_launches) / 1000.0
     pair_gbs = ab["pairs"] / pair_avg_s / 1e9
     step_s = t_ms / 1000.0 / md_steps / world
-    traffic = load_traffic()
+    traffic, traffic_warm = load_traffic()
     fp32_peak = ctx.fp32_peak()
     pair_tflops = PAIR_FLOPS * pairs / pair_avg_s / 1e12
     forms = run_forms(args, ctx, world, rank, dist) if args.forms else None
@@ -860,7 +864,8 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_pairs_jl (force-only LJ C2 + Ewald real)",
                          "achieved": pair_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": pair_gbs / peaks["hbm_gbs"],
-                         "traffic": traffic, "peak_source": peaks["src"],
+                         "traffic": traffic, "traffic_warm_l2": traffic_warm,
+                         "peak_source": peaks["src"],
                          "algorithmic_bytes_per_launch": ab["pairs"],
                          "avg_launch_us": pair_avg_s * 1e6,
                          "step": {"algorithmic_bytes": ab["total"],
