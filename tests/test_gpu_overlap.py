@@ -79,6 +79,8 @@ def _module_run(workdir, overlap, extra=""):
     out = subprocess.run([GPU, conf], cwd=workdir, capture_output=True, text=True,
                          timeout=600, env=env)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    # every keyword is ProtoMol's (an unknown one is only reported)
+    assert "not recognized" not in out.stdout + out.stderr
     res = {}
     for name in ("w.out.energy", "w.out.pos", "w.out.vel", "w.out.forces"):
         with open(os.path.join(workdir, name)) as fh:
