@@ -147,8 +147,8 @@ constexpr int kEwTabN = kEwTabOctaves << kEwTabSubBits;
 constexpr unsigned kEwTabBase = (unsigned)(127 + kEwTabLoExp) << kEwTabSubBits;
 
 // Device arrays of one cluster-pair list (one per distinct (cutoff, skin)
-// in a system).  Atoms are counting-sorted into ncx x ncy columns of the xy
-// plane and sorted by z inside a column; every column's atoms are
+// in a system).  Atoms are binned into buckets of ncx x ncy columns of the
+// xy plane and sorted by z inside a column; every column's atoms are
 // contiguous and padded to a whole number of 8-atom clusters (padding
 // slots hold no atom).  A per-column index of z bins gives the slot range
 // of a z window.  The list holds, per 8-atom i cluster, tiles against
